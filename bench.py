@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark: HD 512^3 RK steps/s on B200, FP32 fast path vs FP64 plain path.
+
+Workload (forced HD turbulence at 512^3): seeded random solenoidal velocity
+with E(k) ~ k^4 exp(-2(k/2)^2) on 1 <= |k| <= N/3 normalised to <|v|^2> = 1,
+constant random solenoidal forcing on 2 <= |k| <= 3 with f0 = 1, nu = 1e-3,
+dt = 5e-4, RK order 4, 2/3 dealiasing.  A step is one full RK4 step (four
+fused substeps).  Inputs (0.54 GB per FP32 field) are far larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of GHOST's FFTW/OpenMP path on
+the host cores (the reference itself needs Fortran+MPI+FFTW, absent here).
+With torchrun (N > 1) every rank advances its own independent 512^3 run
+(replicas, weak scaling); the slab-decomposed single run is not built.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HD 512³ RK steps/s, FP32 vs FP64 on 1 B200 (rel err ≤1e-5); FFT HBM %peak"
+N = 512
+ORD, DT, NU = 4, 5e-4, 1e-3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ghost_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return None
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_substep_time(n, samples, warmup):
+    """Seconds per RK substep of the oracle (FP32, all host threads)."""
+    import numpy as np
+    from oracle.oracle import Oracle
+    o = Oracle(n, precision="fp32")
+    v, _ = o.random_solenoidal(1000, 1.0, n / 3.0, 1, 1.0)
+    f, _ = o.random_solenoidal(2000, 2.0, 3.0, 0, 1.0)
+    C = [x.copy() for x in v]
+    times = []
+    for s in range(warmup + samples):
+        t0 = time.perf_counter()
+        v = o.hd_rkstep2(ORD - (s % ORD), DT, NU, v, C, f)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+    return float(np.mean(times)), o.nthreads()
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    t, cores = cpu_substep_time(args.n, max(1, args.steps), max(0, args.warmup))
+    val = 1.0 / (ORD * t)
+    sample = (f"{max(1, args.steps)} timed RK substeps at {args.n}^3 FP32 (1/{ORD} of an RK{ORD} step each), "
+              f"after {args.warmup} untimed; steps/s = 1/({ORD} x mean substep time)")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ORD * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"HD forced turbulence {args.n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32",
+                       "runs": "CPU restatement of GHOST's fftp-3 + pseudospec3D_hd path (C, OpenMP)"},
+            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def setup_run(n, prec, rank):
+    from ghost_b200 import Ghost
+    g = Ghost(n, precision=prec)
+    v = [g.czeros() for _ in range(3)]
+    f = [g.czeros() for _ in range(3)]
+    g.init_random_solenoidal(1000 + rank, 1.0, n / 3.0, 1, 1.0, *v)
+    g.init_random_solenoidal(2000 + rank, 2.0, 3.0, 0, 1.0, *f)
+    return g, v, f
+
+
+def timed_steps(g, v, f, steps, warmup, ws, timers=False):
+    import torch
+    for _ in range(warmup):
+        g.hd_run(1, ORD, DT, NU, *v, *f)
+    stream = torch.cuda.current_stream()
+    barrier(ws)
+    torch.cuda.synchronize()
+    if timers:
+        g.enable_timers(True)
+        g.read_timers()
+    n0 = g.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.hd_run(steps, ORD, DT, NU, *v, *f)
+    e1.record(stream)
+    e1.synchronize()
+    launches = g.launch_count() - n0
+    ms = e0.elapsed_time(e1)
+    tm = g.read_timers() if timers else None
+    if timers:
+        g.enable_timers(False)
+    torch.cuda.synchronize()
+    barrier(ws)
+    return max_over_ranks(ws, ms), launches, tm
+
+
+def rel_err_fp32_step(n, rank):
+    """FP32 step against the FP64 step from the same state (relative L2)."""
+    import torch
+    g64, v64, f64 = setup_run(n, "fp64", rank)
+    g64.hd_run(2, ORD, DT, NU, *v64, *f64)  # develop the state
+    g32, v32, f32 = setup_run(n, "fp32", rank)
+    for a, b in zip(v32, v64):
+        a.copy_(b.to(torch.complex64))
+    for a, b in zip(f32, f64):
+        a.copy_(b.to(torch.complex64))
+    errs = []
+    for _ in range(2):
+        g64.hd_run(1, ORD, DT, NU, *v64, *f64)
+        g32.hd_run(1, ORD, DT, NU, *v32, *f32)
+        num = sum(float(torch.sum(torch.abs(a.to(torch.complex128) - b) ** 2)) for a, b in zip(v32, v64))
+        den = sum(float(torch.sum(torch.abs(b) ** 2)) for b in v64)
+        errs.append((num / den) ** 0.5)
+        for a, b in zip(v32, v64):  # restart from the FP64 state: per-step error
+            a.copy_(b.to(torch.complex64))
+    g64.close()
+    g32.close()
+    del v64, f64, v32, f32
+    torch.cuda.empty_cache()
+    return max(errs)
+
+
+def fft_roofline(n, reps=10):
+    """Standalone 3D r2c at n^3 FP32: achieved (R + C) bytes / time."""
+    import torch
+    from ghost_b200 import GHOST_REAL_TO_COMPLEX, Ghost
+    g = Ghost(n, precision="fp32")
+    x = torch.randn((n, n, n), device="cuda", dtype=torch.float32)
+    c = g.czeros()
+    plan = g.fftp3d_create_plan((n, n, n), GHOST_REAL_TO_COMPLEX)
+    for _ in range(3):
+        g.fftp3d_real_to_complex(plan, x, c)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g.enable_timers(True)
+    g.read_timers()
+    e0.record(s)
+    for _ in range(reps):
+        g.fftp3d_real_to_complex(plan, x, c)
+    e1.record(s)
+    e1.synchronize()
+    tm = g.read_timers()
+    g.enable_timers(False)
+    ms = e0.elapsed_time(e1) / reps
+    R = n ** 3 * 4
+    C = (n // 2 + 1) * n * n * 8
+    g.close()
+    del x, c
+    torch.cuda.empty_cache()
+    return {"ms_per_fft": ms, "algorithmic_bytes": R + C, "gbs": (R + C) / (ms * 1e-3) / 1e9,
+            "passes_ms": {k: v[0] / reps for k, v in tm.items()}}
+
+
+def e2e_host(n, steps, rank):
+    """Through the public C ABI with pinned host arrays: every step copies
+    the velocity and forcing in and the velocity out (GHOST's host-array
+    calling convention)."""
+    import torch
+    from ghost_b200 import Ghost
+    g, v, f = setup_run(n, "fp32", rank)
+    hv = [torch.empty(g.sshape, dtype=torch.complex64, pin_memory=True) for _ in range(3)]
+    hf = [torch.empty(g.sshape, dtype=torch.complex64, pin_memory=True) for _ in range(3)]
+    for a, b in zip(hv, v):
+        a.copy_(b)
+    for a, b in zip(hf, f):
+        a.copy_(b)
+    del v, f
+    torch.cuda.empty_cache()
+    nv = [x.numpy() for x in hv]
+    nf = [x.numpy() for x in hf]
+    g.hd_run(1, ORD, DT, NU, *nv, *nf)  # warm-up: staging buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        g.hd_run(1, ORD, DT, NU, *nv, *nf)
+    dt = time.perf_counter() - t0
+    cb = g.nxh * g.ny * g.nz * 8
+    g.close()
+    return steps / dt, 6 * cb, 3 * cb
+
+
+def traffic_from_profiles(kernel):
+    """dram bytes per launch recorded from an ncu capture, if committed."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        p = line.split()
+        if len(p) >= 2 and p[0] == kernel:
+            try:
+                return float(p[1])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    n = args.n
+    peak, peak_kind = peaks()
+    clocks = Clocks(local)
+
+    # FP32 fast path (headline)
+    g32, v32, f32 = setup_run(n, "fp32", rank)
+    clocks.start()
+    ms32, launches, tm = timed_steps(g32, v32, f32, args.steps, args.warmup, ws, timers=True)
+    # FP64 plain path, same workload
+    g32.close()
+    del v32, f32
+    torch.cuda.empty_cache()
+    g64, v64, f64 = setup_run(n, "fp64", rank)
+    ms64, _, tm64 = timed_steps(g64, v64, f64, max(2, args.steps // 2), args.warmup, ws, timers=True)
+    clk = clocks.stop()
+    g64.close()
+    del v64, f64
+    torch.cuda.empty_cache()
+
+    steps32 = args.steps / (ms32 * 1e-3)
+    steps64 = max(2, args.steps // 2) / (ms64 * 1e-3)
+    value = ws * steps32
+
+    # dominant kernel and its roofline (algorithmic bytes per launch)
+    cb = (n // 2 + 1) * n * n * 8
+    per_launch_bytes = {"z_inv": 9 * cb + 3 * cb / ORD, "y_inv": 12 * cb, "x_nl": 9 * cb, "y_fwd": 6 * cb,
+                        "z_fwd": 15 * cb}
+    dom = max(tm, key=lambda k: tm[k][0])
+    dom_ms = tm[dom][0] / tm[dom][1]
+    ach = per_launch_bytes[dom] / (dom_ms * 1e-3) / 1e9
+    kern = {k: {"ms_per_launch": tm[k][0] / tm[k][1], "launches": tm[k][1],
+                "share": tm[k][0] / sum(x[0] for x in tm.values()),
+                "gbs": per_launch_bytes[k] / (tm[k][0] / tm[k][1] * 1e-3) / 1e9 if k in per_launch_bytes else None}
+            for k in tm}
+
+    err = rel_err_fp32_step(n, rank) if rank == 0 else None
+    fft = fft_roofline(n) if rank == 0 else None
+    e2e_val, h2d, d2h = e2e_host(n, args.e2e_steps, rank) if rank == 0 else (None, 0, 0)
+    if ws > 1:
+        e2e_val = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        t, cores = cpu_substep_time(n, 1, 0)
+        cpu = {"value": 1.0 / (ORD * t), "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"1 RK substep at {n}^3 FP32 (1/{ORD} of an RK{ORD} step) of the CPU restatement, "
+                         f"steps/s = 1/({ORD} x substep time)"}
+
+    # SURVEY-defined algorithmic bytes per substep at 512^3: 9 FFTs x (R+C) + 15 C
+    R = n ** 3 * 4
+    survey_bytes = 9 * (R + cb) + 15 * cb
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"HD forced turbulence {n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32 fast path",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (0.54 GB per FP32 field)"},
+            "fp64": {"value": ws * steps64, "unit": "steps/s", "ms_per_step": ms64 / max(2, args.steps // 2)},
+            "fp32_over_fp64": steps32 / steps64,
+            "fp32_rel_err_per_step": err,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_kind": peak_kind,
+                         "traffic": traffic_from_profiles(dom)},
+            "kernels": kern,
+            "fft": None if fft is None else {**fft, "frac": fft["gbs"] / peak},
+            "substep_effective_gbs": survey_bytes / (ms32 / args.steps / ORD * 1e-3) / 1e9,
+            "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+"""ctypes binding of libghost_b200.so (the C ABI of include/ghost_b200.h).
+
+The library is the only compute path: if it is missing or cannot load, this
+module raises, and nothing falls back to another implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libghost_b200.so")
+
+GHOST_OK = 0
+TIMER_NAMES = ["z_inv", "y_inv", "x_nl", "y_fwd", "z_fwd", "z_c2c", "x_c2r", "x_r2c", "pointwise", "reduce"]
+ERRORS = {
+    1: "GHOST_ERR_ARG", 2: "GHOST_ERR_SIZE", 3: "GHOST_ERR_ALLOC", 4: "GHOST_ERR_CUDA",
+    5: "GHOST_ERR_TIMEOUT", 6: "GHOST_ERR_NAN", 7: "GHOST_ERR_STATE", 8: "GHOST_ERR_NODEV",
+}
+GHOST_SINGLE = 4
+GHOST_DOUBLE = 8
+GHOST_REAL_TO_COMPLEX = -1
+GHOST_COMPLEX_TO_REAL = 1
+
+
+class GhostError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GhostInfo(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("precision", ctypes.c_int), ("anis", ctypes.c_int),
+        ("nmax", ctypes.c_int), ("nmaxperp", ctypes.c_int),
+        ("kmax", ctypes.c_double), ("tiny", ctypes.c_double),
+        ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+        ("Dkx", ctypes.c_double), ("Dky", ctypes.c_double), ("Dkz", ctypes.c_double),
+        ("Dkk", ctypes.c_double),
+        ("spectral_elems", ctypes.c_size_t), ("real_elems", ctypes.c_size_t),
+    ]
+
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+D = ctypes.c_double
+PD = ctypes.POINTER(ctypes.c_double)
+
+# name -> argument types (all return int status)
+SIGNATURES = {
+    "ghost_ctx_create": [I, I, I, D, D, D, I, I, ctypes.POINTER(P)],
+    "ghost_ctx_destroy": [P],
+    "ghost_ctx_get_info": [P, ctypes.POINTER(GhostInfo)],
+    "ghost_ctx_set_stream": [P, P],
+    "ghost_ctx_set_kmax": [P, D],
+    "ghost_ctx_synchronize": [P],
+    "ghost_ctx_launch_count": [P, ctypes.POINTER(ctypes.c_longlong)],
+    "ghost_ctx_enable_timers": [P, I],
+    "ghost_ctx_read_timers": [P, PD, ctypes.POINTER(ctypes.c_longlong)],
+    "ghost_fftp3d_create_plan": [P, ctypes.POINTER(ctypes.c_int), I, I, ctypes.POINTER(P)],
+    "ghost_fftp3d_destroy_plan": [P],
+    "ghost_fftp3d_real_to_complex": [P, P, P],
+    "ghost_fftp3d_complex_to_real": [P, P, P],
+    "ghost_derivk3": [P, P, P, I],
+    "ghost_laplak3": [P, P, P],
+    "ghost_rotor3": [P, P, P, P, I],
+    "ghost_prodre3": [P, P, P, P, P, P, P],
+    "ghost_nonlhd3": [P, P, P, P, P, I],
+    "ghost_energy": [P, P, P, P, PD, I],
+    "ghost_helicity": [P, P, P, P, PD],
+    "ghost_cross": [P, P, P, P, P, P, P, PD, I],
+    "ghost_divergence": [P, P, P, P, PD],
+    "ghost_maxabs": [P, P, P, P, PD, I],
+    "ghost_spectrumc": [P, P, P, P, I, I, PD, PD],
+    "ghost_hdcheck": [P, P, P, P, P, P, P, I, I, PD],
+    "ghost_normalize": [P, P, P, P, D, I],
+    "ghost_sharp": [P, P, P, D],
+    "ghost_hd_rkstep1": [P, P, P, P, P, P, P],
+    "ghost_hd_rkstep2": [P, I, D, D, P, P, P, P, P, P, P, P, P],
+    "ghost_hd_run": [P, I, I, D, D, P, P, P, P, P, P, P, P, P],
+    "ghost_advect3": [P, P, P, P, P, P],
+    "ghost_bouss_rkstep2": [P, I, D, D, D, D, D, D] + [P] * 12,
+    "ghost_bouss_run": [P, I, I, D, D, D, D, D, D] + [P] * 8,
+    "ghost_init_random_solenoidal": [P, ctypes.POINTER(ctypes.c_int32), D, D, I, D, P, P, P],
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m ghost_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    lib.ghost_last_error_string.argtypes = []
+    lib.ghost_last_error_string.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str) -> None:
+    if status != GHOST_OK:
+        msg = load().ghost_last_error_string().decode(errors="replace")
+        raise GhostError(status, where, msg)

@@ -1,0 +1,1290 @@
+// api.cu -- the C ABI of include/ghost_b200.h: context, FFT plans,
+// spectral operators, reductions and the fused RK substeps.
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "ic_host.h"
+#include "ops.cuh"
+#include "passes.cuh"
+
+namespace gb {
+
+// ---------------------------------------------------------------------
+// errors
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+
+static bool pow2_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
+
+// ---------------------------------------------------------------------
+// device memory helpers
+static int dalloc(void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(GHOST_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  return GHOST_OK;
+}
+
+// scratch spectral fields 0..n-1 (each cbytes), grown on demand
+static int scratch(ghost_ctx *c, int n, void **out) {
+  while ((int)c->scratch.size() < n) {
+    void *p;
+    GB_CHECK(dalloc(&p, c->cbytes));
+    c->scratch.push_back(p);
+  }
+  for (int q = 0; q < n; ++q) out[q] = c->scratch[q];
+  return GHOST_OK;
+}
+
+static int partials(ghost_ctx *c, size_t n, double **out) {
+  if (c->partials_elems < n) {
+    if (c->partials) cudaFree(c->partials);
+    c->partials = nullptr;
+    c->partials_elems = 0;
+    void *p;
+    GB_CHECK(dalloc(&p, n * sizeof(double)));
+    c->partials = (double *)p;
+    c->partials_elems = n;
+  }
+  *out = c->partials;
+  return GHOST_OK;
+}
+
+// ---------------------------------------------------------------------
+// host-array staging: pointers that are not device memory are copied
+// through context buffers, and the call syncs before returning.
+static bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+struct Staging {
+  ghost_ctx *c;
+  int used = 0;
+  bool any_host = false;
+  struct Back {
+    void *host;
+    const void *dev;
+    size_t bytes;
+  };
+  std::vector<Back> back;
+  explicit Staging(ghost_ctx *ctx) : c(ctx) {}
+  int buffer(void **out) {
+    while ((int)c->stage.size() <= used) {
+      void *p;
+      GB_CHECK(dalloc(&p, c->cbytes));
+      c->stage.push_back(p);
+    }
+    *out = c->stage[used++];
+    return GHOST_OK;
+  }
+  // dir: 1 in, 2 out, 3 in/out
+  template <typename T> int map(T *user, size_t bytes, int dir, T **dev) {
+    if (user == nullptr) {
+      *dev = nullptr;
+      return GHOST_OK;
+    }
+    if (is_device_ptr(user)) {
+      *dev = user;
+      return GHOST_OK;
+    }
+    any_host = true;
+    void *d;
+    GB_CHECK(buffer(&d));
+    if (dir & 1) GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (dir & 2) back.push_back({(void *)user, d, bytes});
+    *dev = (T *)d;
+    return GHOST_OK;
+  }
+  int finish() {
+    for (auto &b : back) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (any_host) GB_CUDA(cudaStreamSynchronize(c->stream));
+    return GHOST_OK;
+  }
+};
+
+template <typename R> const KParams<R> &kparams(const ghost_ctx *c);
+template <> const KParams<float> &kparams<float>(const ghost_ctx *c) { return c->kp32; }
+template <> const KParams<double> &kparams<double>(const ghost_ctx *c) { return c->kp64; }
+
+static int post_launch(ghost_ctx *c) {
+  c->launches++;
+  GB_CUDA(cudaGetLastError());
+  return GHOST_OK;
+}
+
+// ---------------------------------------------------------------------
+// per-kernel timers
+static cudaEvent_t take_event(ghost_ctx *c) {
+  if (!c->ev_free.empty()) {
+    cudaEvent_t e = c->ev_free.back();
+    c->ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records the start event of a launch; returns the pending slot or -1.
+static int timer_begin(ghost_ctx *c, int kind) {
+  if (!c->timers_on) return -1;
+  ghost_ctx::Pending p{kind, take_event(c), take_event(c)};
+  cudaEventRecord(p.a, c->stream);
+  c->ev_pending.push_back(p);
+  return (int)c->ev_pending.size() - 1;
+}
+static void timer_end(ghost_ctx *c, int slot) {
+  if (slot >= 0) cudaEventRecord(c->ev_pending[slot].b, c->stream);
+}
+static int timers_collect(ghost_ctx *c) {
+  if (c->ev_pending.empty()) return GHOST_OK;
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  for (auto &p : c->ev_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      c->t_ms[p.kind] += ms;
+      c->t_n[p.kind] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    c->ev_free.push_back(p.a);
+    c->ev_free.push_back(p.b);
+  }
+  c->ev_pending.clear();
+  return GHOST_OK;
+}
+
+template <class Op> struct ZKind;
+template <typename R, int S> struct ZKind<ZC2C<R, S>> { static constexpr int value = GHOST_TIMER_Z_C2C; };
+template <typename R, int P> struct ZKind<ZInv<R, P>> { static constexpr int value = GHOST_TIMER_Z_INV; };
+template <typename R> struct ZKind<ZFwdHD<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
+template <typename R> struct ZKind<ZFwdBouss<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
+
+static int grid1d(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)std::min<size_t>(b, 148 * 16);
+}
+
+// ---------------------------------------------------------------------
+// pass launchers
+template <typename R> constexpr int xE() { return sizeof(R) == 4 ? 8 : 4; }
+template <typename R> constexpr int xBZ() { return sizeof(R) == 4 ? 8 : 4; }
+
+template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op) {
+  constexpr int E = 8, T = N / E;
+  int lpb = std::max(1, 256 / T);
+  lpb = std::min(lpb, c->ny);
+  const long nlines = (long)c->ny * c->nxh;
+  const size_t smem = (size_t)(N + lpb * ZShape<N, E>::NP) * sizeof(cx<R>);
+  auto kern = zpass_kernel<R, N, E, Op>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ts = timer_begin(c, ZKind<Op>::value);
+  kern<<<(unsigned)(nlines / lpb), lpb * T, smem, c->stream>>>(op, (const cx<R> *)c->tw_z, lpb);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
+template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op) {
+  switch (c->nz) {
+    case 16: return launch_z_n<R, 16>(c, op);
+    case 32: return launch_z_n<R, 32>(c, op);
+    case 64: return launch_z_n<R, 64>(c, op);
+    case 128: return launch_z_n<R, 128>(c, op);
+    case 256: return launch_z_n<R, 256>(c, op);
+    case 512: return launch_z_n<R, 512>(c, op);
+    case 1024: return launch_z_n<R, 1024>(c, op);
+  }
+  return fail(GHOST_ERR_SIZE, "nz=%d unsupported", c->nz);
+}
+
+template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf) {
+  constexpr int E = 8, T = N / E;
+  int bz = sizeof(R) == 4 ? 16 : 8;
+  while (bz * T > 1024) bz >>= 1;
+  bz = std::min(bz, c->nz);
+  const size_t smem = (size_t)(N + bz * N) * sizeof(cx<R>);
+  auto kern = ypass_kernel<R, N, E, S>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(c->nz / bz, c->nxh, nf);
+  const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
+  kern<<<grid, bz * T, smem, c->stream>>>(f, (const cx<R> *)c->tw_y, c->nz, bz);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
+template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int nf) {
+  switch (c->ny) {
+    case 16: return launch_y_n<R, 16, S>(c, f, nf);
+    case 32: return launch_y_n<R, 32, S>(c, f, nf);
+    case 64: return launch_y_n<R, 64, S>(c, f, nf);
+    case 128: return launch_y_n<R, 128, S>(c, f, nf);
+    case 256: return launch_y_n<R, 256, S>(c, f, nf);
+    case 512: return launch_y_n<R, 512, S>(c, f, nf);
+    case 1024: return launch_y_n<R, 1024, S>(c, f, nf);
+  }
+  return fail(GHOST_ERR_SIZE, "ny=%d unsupported", c->ny);
+}
+
+// X pass kinds
+enum XKind { X_HD = 0, X_C2R = 1, X_R2C = 2, X_BOUSS = 3 };
+
+template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void *in, void *out, const void *const *ins,
+                                                       void *const *outs) {
+  constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
+  constexpr int M = NX / 2, T = M / E;
+  // rows of BZ z values; at most 256 threads so the register-resident
+  // real fields of the fused pass fit the register file
+  constexpr int BZ = xBZ<R>() * T <= 256 ? xBZ<R>() : (256 / T > 0 ? 256 / T : 1);
+  constexpr int NT = BZ * T;
+  typedef cx<R> C;
+  dim3 grid(c->nz / BZ, c->ny);
+  const C *tw = (const C *)c->tw_x;
+  const int ts = timer_begin(c, KIND == X_C2R ? GHOST_TIMER_X_C2R : (KIND == X_R2C ? GHOST_TIMER_X_R2C : GHOST_TIMER_X_NL));
+  if (KIND == X_HD || KIND == X_BOUSS) {
+    constexpr int PHYS = KIND == X_HD ? 0 : 1;
+    constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
+    const size_t smem = (size_t)(NX + 2 * (M + 1) * BZ + M * BZ) * sizeof(C);
+    auto kern = xpass_nl_kernel<R, NX, E, BZ, PHYS>;
+    GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CFields<R> fi{};
+    Fields<R> fo{};
+    for (int q = 0; q < NIN; ++q) fi.p[q] = (const C *)ins[q];
+    for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
+    const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+    kern<<<grid, NT, smem, c->stream>>>(fi, fo, tw, c->ny, c->nz, (R)1 / (nn * nn));
+  } else if (KIND == X_C2R) {
+    const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
+    auto kern = xpass_c2r_kernel<R, NX, E, BZ>;
+    GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, NT, smem, c->stream>>>((const C *)in, (R *)out, tw, c->ny, c->nz);
+  } else {
+    const size_t smem = (size_t)(NX + M * BZ) * sizeof(C);
+    auto kern = xpass_r2c_kernel<R, NX, E, BZ>;
+    GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, NT, smem, c->stream>>>((const R *)in, (C *)out, tw, c->ny, c->nz);
+  }
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
+template <typename R, int KIND>
+int launch_x(ghost_ctx *c, const void *in, void *out, const void *const *ins = nullptr, void *const *outs = nullptr) {
+  switch (c->nx) {
+    case 16: return launch_x_n<R, 16, KIND>(c, in, out, ins, outs);
+    case 32: return launch_x_n<R, 32, KIND>(c, in, out, ins, outs);
+    case 64: return launch_x_n<R, 64, KIND>(c, in, out, ins, outs);
+    case 128: return launch_x_n<R, 128, KIND>(c, in, out, ins, outs);
+    case 256: return launch_x_n<R, 256, KIND>(c, in, out, ins, outs);
+    case 512: return launch_x_n<R, 512, KIND>(c, in, out, ins, outs);
+    case 1024: return launch_x_n<R, 1024, KIND>(c, in, out, ins, outs);
+  }
+  return fail(GHOST_ERR_SIZE, "nx=%d unsupported", c->nx);
+}
+
+// ---------------------------------------------------------------------
+// 3D transforms on device pointers
+template <typename R> int r2c_dev(ghost_ctx *c, const void *in, void *out) {
+  GB_CHECK((launch_x<R, X_R2C>(c, in, out)));
+  Fields<R> f{};
+  f.p[0] = (cx<R> *)out;
+  GB_CHECK((launch_y<R, -1>(c, f, 1)));
+  ZC2C<R, -1> op{};
+  op.in.p[0] = (const cx<R> *)out;
+  op.out.p[0] = (cx<R> *)out;
+  op.nf = 1;
+  op.nz = c->nz;
+  return launch_z<R>(c, op);
+}
+
+template <typename R> int c2r_dev(ghost_ctx *c, const void *in, void *out) {
+  void *w[1];
+  GB_CHECK(scratch(c, 1, w));
+  ZC2C<R, +1> op{};
+  op.in.p[0] = (const cx<R> *)in;
+  op.out.p[0] = (cx<R> *)w[0];
+  op.nf = 1;
+  op.nz = c->nz;
+  GB_CHECK(launch_z<R>(c, op));
+  Fields<R> f{};
+  f.p[0] = (cx<R> *)w[0];
+  GB_CHECK((launch_y<R, +1>(c, f, 1)));
+  return launch_x<R, X_C2R>(c, w[0], out);
+}
+
+// prodre3 on device pointers (outputs may alias inputs)
+template <typename R> int prodre3_dev(ghost_ctx *c, const void *a, const void *b, const void *cc, void *d, void *e, void *f) {
+  void *w[6];
+  GB_CHECK(scratch(c, 6, w));
+  ZInv<R, 0> zi{};
+  zi.v.p[0] = (const cx<R> *)a;
+  zi.v.p[1] = (const cx<R> *)b;
+  zi.v.p[2] = (const cx<R> *)cc;
+  for (int q = 0; q < 6; ++q) zi.w.p[q] = (cx<R> *)w[q];
+  zi.kp = kparams<R>(c);
+  zi.copy = 0;
+  GB_CHECK(launch_z<R>(c, zi));
+  Fields<R> fy{};
+  for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
+  GB_CHECK((launch_y<R, +1>(c, fy, 6)));
+  GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 3)));
+  ZC2C<R, -1> zf{};
+  void *outs[3] = {d, e, f};
+  for (int q = 0; q < 3; ++q) {
+    zf.in.p[q] = (const cx<R> *)w[q];
+    zf.out.p[q] = (cx<R> *)outs[q];
+  }
+  zf.nf = 3;
+  zf.nz = c->nz;
+  return launch_z<R>(c, zf);
+}
+
+// One HD substep on device pointers: include/hd_rkstep2.f90 with
+// hd_rkstep1 folded in when copy != 0.
+template <typename R>
+int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], void *const C[3], const void *const f[3],
+                   int copy) {
+  void *w[6];
+  GB_CHECK(scratch(c, 6, w));
+  ZInv<R, 0> zi{};
+  for (int q = 0; q < 3; ++q) {
+    zi.v.p[q] = (const cx<R> *)v[q];
+    zi.cpy.p[q] = (cx<R> *)C[q];
+  }
+  for (int q = 0; q < 6; ++q) zi.w.p[q] = (cx<R> *)w[q];
+  zi.kp = kparams<R>(c);
+  zi.copy = copy;
+  GB_CHECK(launch_z<R>(c, zi));
+  Fields<R> fy{};
+  for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
+  GB_CHECK((launch_y<R, +1>(c, fy, 6)));
+  GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 3)));
+  ZFwdHD<R> zf{};
+  for (int q = 0; q < 3; ++q) {
+    zf.nl.p[q] = (const cx<R> *)w[q];
+    zf.v.p[q] = (cx<R> *)v[q];
+    zf.c0.p[q] = (const cx<R> *)C[q];
+    zf.f.p[q] = f ? (const cx<R> *)f[q] : nullptr;
+  }
+  zf.kp = kparams<R>(c);
+  zf.dt = (R)dt;
+  zf.nu = (R)nu;
+  zf.rmp = (R)1 / (R)o;
+  return launch_z<R>(c, zf);
+}
+
+// One Boussinesq substep (include/rotbouss_rkstep2.f90) on device
+// pointers: v[0..2] velocity, v[3] theta; C[0..3] the RK1 copies (C20 last).
+template <typename R>
+int bouss_substep_dev(ghost_ctx *c, int o, double dt, double nu, double kappa, double omegaz, double xmom,
+                      double xtemp, void *const v[4], void *const C[4], const void *const f[4], int copy) {
+  void *w[9];
+  GB_CHECK(scratch(c, 9, w));
+  ZInv<R, 1> zi{};
+  for (int q = 0; q < 4; ++q) {
+    zi.v.p[q] = (const cx<R> *)v[q];
+    zi.cpy.p[q] = (cx<R> *)C[q];
+  }
+  for (int q = 0; q < 9; ++q) zi.w.p[q] = (cx<R> *)w[q];
+  zi.kp = kparams<R>(c);
+  zi.copy = copy;
+  GB_CHECK(launch_z<R>(c, zi));
+  Fields<R> fy{};
+  for (int q = 0; q < 9; ++q) fy.p[q] = (cx<R> *)w[q];
+  GB_CHECK((launch_y<R, +1>(c, fy, 9)));
+  GB_CHECK((launch_x<R, X_BOUSS>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 4)));
+  ZFwdBouss<R> zf{};
+  for (int q = 0; q < 4; ++q) {
+    zf.nl.p[q] = (const cx<R> *)w[q];
+    zf.v.p[q] = (cx<R> *)v[q];
+    zf.c0.p[q] = (const cx<R> *)C[q];
+    zf.f.p[q] = f ? (const cx<R> *)f[q] : nullptr;
+  }
+  zf.kp = kparams<R>(c);
+  zf.dt = (R)dt;
+  zf.nu = (R)nu;
+  zf.kappa = (R)kappa;
+  zf.omegaz = (R)omegaz;
+  zf.xmom = (R)xmom;
+  zf.xtemp = (R)xtemp;
+  zf.rmp = (R)1 / (R)o;
+  return launch_z<R>(c, zf);
+}
+
+// advect3 on device pointers: e = -(A.grad)d via the fused Boussinesq
+// passes with zero vorticity work discarded (the three omega x v outputs
+// are computed and dropped)
+template <typename R>
+int advect3_dev(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, void *e) {
+  void *w[9];
+  GB_CHECK(scratch(c, 9, w));
+  ZInv<R, 1> zi{};
+  zi.v.p[0] = (const cx<R> *)a;
+  zi.v.p[1] = (const cx<R> *)b;
+  zi.v.p[2] = (const cx<R> *)cc;
+  zi.v.p[3] = (const cx<R> *)d;
+  for (int q = 0; q < 9; ++q) zi.w.p[q] = (cx<R> *)w[q];
+  zi.kp = kparams<R>(c);
+  zi.copy = 0;
+  GB_CHECK(launch_z<R>(c, zi));
+  Fields<R> fy{};
+  for (int q = 0; q < 9; ++q) fy.p[q] = (cx<R> *)w[q];
+  GB_CHECK((launch_y<R, +1>(c, fy, 9)));
+  GB_CHECK((launch_x<R, X_BOUSS>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
+  Fields<R> f1{};
+  f1.p[0] = (cx<R> *)w[3];
+  GB_CHECK((launch_y<R, -1>(c, f1, 1)));
+  ZC2C<R, -1> zf{};
+  zf.in.p[0] = (const cx<R> *)w[3];
+  zf.out.p[0] = (cx<R> *)e;
+  zf.nf = 1;
+  zf.nz = c->nz;
+  return launch_z<R>(c, zf);
+}
+
+// ---------------------------------------------------------------------
+// reductions
+template <typename R>
+int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d, const void *e,
+               const void *f, double *out_host) {
+  const size_t n = c->nspec;
+  const int nb = grid1d(n);
+  double *part;
+  GB_CHECK(partials(c, (size_t)nb + 1, &part));
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, (const cx<R> *)d, (const cx<R> *)e,
+                (const cx<R> *)f};
+  const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
+  reduce_kernel<R><<<nb, 256, 0, c->stream>>>(kparams<R>(c), ra, kind, n, part);
+  GB_CHECK(post_launch(c));
+  finalize_kernel<<<1, 256, 0, c->stream>>>(part, nb, 1, part + nb);
+  timer_end(c, ts);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaMemcpyAsync(out_host, part + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
+template <typename R>
+int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host) {
+  const size_t n = c->nspec;
+  const int nbins = c->nmax / 2 + 1;
+  const int nblk = std::min(grid1d(n), 148 * 4);
+  double *part;
+  GB_CHECK(partials(c, (size_t)(nblk + 1) * nbins, &part));
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
+  const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
+  GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
+  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, part);
+  GB_CHECK(post_launch(c));
+  double *fin = part + (size_t)nblk * nbins;
+  finalize_kernel<<<1, 256, 0, c->stream>>>(part, nblk, nbins, fin);
+  timer_end(c, ts);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * nbins, cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
+// twiddles exp(-2 pi i e/n), e < n, evaluated in extended precision and
+// rounded once to the working precision
+template <typename R> int make_twiddles(int n, void **out) {
+  std::vector<R> h(2 * (size_t)n);
+  const long double tau = 6.283185307179586476925286766559005768L;
+  for (int e = 0; e < n; ++e) {
+    // exact values at multiples of pi/4 (avoid last-bit noise at the axes)
+    long double re, im;
+    if ((8 * e) % n == 0) {
+      const int o = (8 * e) / n;  // multiple of pi/4
+      const long double s = 0.707106781186547524400844362104849039L;
+      const long double tab_re[8] = {1, s, 0, -s, -1, -s, 0, s};
+      const long double tab_im[8] = {0, -s, -1, -s, 0, s, 1, s};
+      re = tab_re[o];
+      im = tab_im[o];
+    } else {
+      const long double a = tau * (long double)e / (long double)n;
+      re = cosl(a);
+      im = -sinl(a);
+    }
+    h[2 * e] = (R)re;
+    h[2 * e + 1] = (R)im;
+  }
+  GB_CHECK(dalloc(out, sizeof(R) * 2 * n));
+  GB_CUDA(cudaMemcpy(*out, h.data(), sizeof(R) * 2 * n, cudaMemcpyHostToDevice));
+  return GHOST_OK;
+}
+
+template <typename R> void fill_kparams(ghost_ctx *c, KParams<R> &kp) {
+  kp.nx = c->nx;
+  kp.ny = c->ny;
+  kp.nz = c->nz;
+  kp.nxh = c->nxh;
+  kp.anis = c->anis;
+  kp.arbsize = c->arbsize;
+  kp.Dkx = (R)c->Dkx;
+  kp.Dky = (R)c->Dky;
+  kp.Dkz = (R)c->Dkz;
+  kp.rmp = kp.rmq = kp.rms = (R)1;
+  if (c->anis) {
+    kp.rmp = (R)1 / ((R)c->nx * (R)c->nx);
+    kp.rmq = (R)1 / ((R)c->ny * (R)c->ny);
+    kp.rms = (R)1 / ((R)c->nz * (R)c->nz);
+  }
+  kp.kmax = (R)c->kmax;
+  kp.tiny = (R)c->tiny;
+  const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+  kp.tmp = (R)1 / (nn * nn);
+}
+
+// kmax, tiny, nmax, Dk of main3D.fpp:881-909,1727-1737 in precision R
+template <typename R> void setup_scalars(ghost_ctx *c, double Lx, double Ly, double Lz) {
+  R lx = 1, ly = 1, lz = 1, dkx = 1, dky = 1, dkz = 1;
+  if (c->arbsize) {
+    lx = (R)Lx;
+    ly = (R)Ly;
+    lz = (R)Lz;
+    dkx = (R)1 / lx;
+    dky = (R)1 / ly;
+    dkz = (R)1 / lz;
+  }
+  R dkk = std::min(dkx, std::min(dky, dkz));
+  R m = std::max((R)c->nx * dkx, std::max((R)c->ny * dky, (R)c->nz * dkz));
+  R mp = std::max((R)c->nx * dkx, (R)c->ny * dky);
+  c->nmax = (int)(m / dkk);
+  c->nmaxperp = (int)(mp / dkk);
+  R kmax = (R)1.0 / (R)9.0;
+  if (!c->arbsize && c->anis == 0) kmax = kmax * ((R)c->nx * (R)c->nx);
+  R t = (R)0.1 / ((R)c->nmax * (R)c->nmax);
+  R tiny = (R)1e-5 < t ? (R)1e-5 : t;
+  c->Lx = lx;
+  c->Ly = ly;
+  c->Lz = lz;
+  c->Dkx = dkx;
+  c->Dky = dky;
+  c->Dkz = dkz;
+  c->Dkk = dkk;
+  c->kmax = kmax;
+  c->tiny = tiny;
+}
+
+template <typename R> int ctx_init_prec(ghost_ctx *c, double Lx, double Ly, double Lz) {
+  setup_scalars<R>(c, Lx, Ly, Lz);
+  GB_CHECK(make_twiddles<R>(c->nx, &c->tw_x));
+  GB_CHECK(make_twiddles<R>(c->ny, &c->tw_y));
+  GB_CHECK(make_twiddles<R>(c->nz, &c->tw_z));
+  return GHOST_OK;
+}
+
+static void refresh_kparams(ghost_ctx *c) {
+  fill_kparams<float>(c, c->kp32);
+  fill_kparams<double>(c, c->kp64);
+}
+
+// ---------------------------------------------------------------------
+// generic dispatch on the context precision
+#define GB_DISPATCH(c, CALL)                           \
+  ((c)->precision == GHOST_SINGLE ? CALL##_impl<float> : CALL##_impl<double>)
+
+template <typename R> int derivk3_impl(ghost_ctx *c, const void *a, void *b, int dir) {
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  derivk3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec, dir);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+template <typename R> int laplak3_impl(ghost_ctx *c, const void *a, void *b) {
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  laplak3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+template <typename R> int rotor3_impl(ghost_ctx *c, const void *a, const void *b, void *o, int dir) {
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  rotor3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
+                                                             (cx<R> *)o, c->nspec, dir);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+template <typename R> int nonlhd3_impl(ghost_ctx *c, const void *a, const void *b, const void *cc, void *g, int dir) {
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  nonlhd3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
+                                                              (const cx<R> *)cc, (cx<R> *)g, c->nspec, dir);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+template <typename R> int sharp_impl(ghost_ctx *c, const void *a, void *b, double delta) {
+  const R pi = (R)3.14159265358979323846;
+  const R cut = (pi / (R)delta) * (pi / (R)delta);
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  sharp_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec, cut);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+template <typename R> int scale3_impl(ghost_ctx *c, void *x, void *y, void *z, double f0, double s) {
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  scale3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>((cx<R> *)x, (cx<R> *)y, (cx<R> *)z, c->nspec, (R)f0, s);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
+template <typename R> int maxabs_impl(ghost_ctx *c, const void *a, const void *b, const void *cc, double *d, int kin) {
+  // scratch 0: the complex-to-real intermediate; 1..3: spectral fields
+  // whose real-space norm is wanted; 4..6: their real-space values
+  void *w[7];
+  GB_CHECK(scratch(c, 7, w));
+  if (kin == 0) {
+    GB_CHECK(rotor3_impl<R>(c, b, cc, w[1], 1));
+    GB_CHECK(rotor3_impl<R>(c, a, cc, w[2], 2));
+    GB_CHECK(rotor3_impl<R>(c, a, b, w[3], 3));
+  } else if (kin == 1) {
+    GB_CHECK(laplak3_impl<R>(c, a, w[1]));
+    GB_CHECK(laplak3_impl<R>(c, b, w[2]));
+    GB_CHECK(laplak3_impl<R>(c, cc, w[3]));
+  } else {
+    GB_CUDA(cudaMemcpyAsync(w[1], a, c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+    GB_CUDA(cudaMemcpyAsync(w[2], b, c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+    GB_CUDA(cudaMemcpyAsync(w[3], cc, c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  for (int q = 0; q < 3; ++q) GB_CHECK(c2r_dev<R>(c, w[1 + q], w[4 + q]));
+  double *part;
+  GB_CHECK(partials(c, 1, &part));
+  GB_CUDA(cudaMemsetAsync(part, 0, sizeof(double), c->stream));
+  maxnorm_kernel<R><<<grid1d(c->nreal), 256, 0, c->stream>>>((const R *)w[4], (const R *)w[5], (const R *)w[6], c->nreal,
+                                                               (unsigned long long *)part);
+  GB_CHECK(post_launch(c));
+  double m;
+  GB_CUDA(cudaMemcpyAsync(&m, part, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+  *d = (double)((R)m / nn);
+  return GHOST_OK;
+}
+
+template <typename R> int init_random_impl(ghost_ctx *c, int32_t *seed, double kdn, double kup, int shape, double amp,
+                                           void *ox, void *oy, void *oz) {
+  Grid g{c->nx, c->ny, c->nz, c->nxh, c->anis, c->arbsize, c->Dkx, c->Dky, c->Dkz};
+  std::vector<R> h1(2 * c->nspec), h2(2 * c->nspec), h3(2 * c->nspec);
+  *seed = random_vpot<R>(g, *seed, kdn, kup, shape, h1.data(), h2.data(), h3.data());
+  void *w[3];
+  GB_CHECK(scratch(c, 3, w));
+  GB_CUDA(cudaMemcpyAsync(w[0], h1.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CUDA(cudaMemcpyAsync(w[1], h2.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CUDA(cudaMemcpyAsync(w[2], h3.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CHECK(rotor3_impl<R>(c, w[1], w[2], ox, 1));
+  GB_CHECK(rotor3_impl<R>(c, w[0], w[2], oy, 2));
+  GB_CHECK(rotor3_impl<R>(c, w[0], w[1], oz, 3));
+  double e;
+  GB_CHECK(reduce_dev<R>(c, RED_ENERGY, ox, oy, oz, nullptr, nullptr, nullptr, &e));
+  return scale3_impl<R>(c, ox, oy, oz, amp, sqrt(e));
+}
+
+}  // namespace gb
+
+using namespace gb;
+
+// =====================================================================
+// C ABI
+// =====================================================================
+#define CTX_CHECK(c) \
+  if (!(c)) return fail(GHOST_ERR_ARG, "null context")
+
+extern "C" {
+
+const char *ghost_last_error_string(void) { return g_err; }
+
+int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, int arbsize, int precision,
+                     ghost_ctx **out) {
+  if (!out) return fail(GHOST_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  if (!pow2_ok(nx) || !pow2_ok(ny) || !pow2_ok(nz))
+    return fail(GHOST_ERR_SIZE, "grid %dx%dx%d: each n must be a power of two in [16,1024]", nx, ny, nz);
+  if (precision != GHOST_SINGLE && precision != GHOST_DOUBLE)
+    return fail(GHOST_ERR_ARG, "precision %d: use GHOST_SINGLE (4) or GHOST_DOUBLE (8)", precision);
+  if (arbsize && !(Lx > 0 && Ly > 0 && Lz > 0)) return fail(GHOST_ERR_ARG, "box lengths must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(GHOST_ERR_NODEV, "no CUDA device");
+  }
+  ghost_ctx *c = new ghost_ctx();
+  c->nx = nx;
+  c->ny = ny;
+  c->nz = nz;
+  c->nxh = nx / 2 + 1;
+  c->precision = precision;
+  c->arbsize = arbsize ? 1 : 0;
+  c->anis = c->arbsize ? 1 : ((nx != ny) || (ny != nz));
+  c->nspec = (size_t)nz * ny * c->nxh;
+  c->nreal = (size_t)nx * ny * nz;
+  const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
+  c->cbytes = c->nspec * 2 * rs;
+  c->rbytes = c->nreal * rs;
+  cudaGetDevice(&c->device);
+  c->stream = nullptr;
+  c->launches = 0;
+  c->tw_x = c->tw_y = c->tw_z = nullptr;
+  c->partials = nullptr;
+  c->partials_elems = 0;
+  for (int q = 0; q < 4; ++q) c->rk[q] = nullptr;
+  c->timers_on = false;
+  for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
+    c->t_ms[k] = 0.0;
+    c->t_n[k] = 0;
+  }
+  int s = precision == GHOST_SINGLE ? ctx_init_prec<float>(c, Lx, Ly, Lz) : ctx_init_prec<double>(c, Lx, Ly, Lz);
+  if (s != GHOST_OK) {
+    ghost_ctx_destroy(c);
+    return s;
+  }
+  refresh_kparams(c);
+  *out = c;
+  return GHOST_OK;
+}
+
+int ghost_ctx_destroy(ghost_ctx *c) {
+  if (!c) return GHOST_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  else cudaDeviceSynchronize();
+  for (void *p : c->scratch) cudaFree(p);
+  for (void *p : c->stage) cudaFree(p);
+  for (int q = 0; q < 4; ++q)
+    if (c->rk[q]) cudaFree(c->rk[q]);
+  cudaFree(c->tw_x);
+  cudaFree(c->tw_y);
+  cudaFree(c->tw_z);
+  cudaFree(c->partials);
+  for (auto &p : c->ev_pending) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (cudaEvent_t e : c->ev_free) cudaEventDestroy(e);
+  delete c;
+  return GHOST_OK;
+}
+
+int ghost_ctx_get_info(const ghost_ctx *c, ghost_info *info) {
+  CTX_CHECK(c);
+  if (!info) return fail(GHOST_ERR_ARG, "null info");
+  info->nx = c->nx;
+  info->ny = c->ny;
+  info->nz = c->nz;
+  info->precision = c->precision;
+  info->anis = c->anis;
+  info->nmax = c->nmax;
+  info->nmaxperp = c->nmaxperp;
+  info->kmax = c->kmax;
+  info->tiny = c->tiny;
+  info->Lx = c->Lx;
+  info->Ly = c->Ly;
+  info->Lz = c->Lz;
+  info->Dkx = c->Dkx;
+  info->Dky = c->Dky;
+  info->Dkz = c->Dkz;
+  info->Dkk = c->Dkk;
+  info->spectral_elems = c->nspec;
+  info->real_elems = c->nreal;
+  return GHOST_OK;
+}
+
+int ghost_ctx_set_stream(ghost_ctx *c, void *stream) {
+  CTX_CHECK(c);
+  c->stream = (cudaStream_t)stream;
+  return GHOST_OK;
+}
+
+int ghost_ctx_set_kmax(ghost_ctx *c, double kmax) {
+  CTX_CHECK(c);
+  c->kmax = c->precision == GHOST_SINGLE ? (double)(float)kmax : kmax;
+  refresh_kparams(c);
+  return GHOST_OK;
+}
+
+int ghost_ctx_synchronize(ghost_ctx *c) {
+  CTX_CHECK(c);
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
+int ghost_ctx_enable_timers(ghost_ctx *c, int enable) {
+  CTX_CHECK(c);
+  GB_CHECK(timers_collect(c));
+  c->timers_on = enable != 0;
+  return GHOST_OK;
+}
+
+int ghost_ctx_read_timers(ghost_ctx *c, double ms[GHOST_TIMER_KINDS], long long launches[GHOST_TIMER_KINDS]) {
+  CTX_CHECK(c);
+  if (!ms || !launches) return fail(GHOST_ERR_ARG, "null output");
+  GB_CHECK(timers_collect(c));
+  for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
+    ms[k] = c->t_ms[k];
+    launches[k] = c->t_n[k];
+    c->t_ms[k] = 0.0;
+    c->t_n[k] = 0;
+  }
+  return GHOST_OK;
+}
+
+int ghost_ctx_launch_count(const ghost_ctx *c, long long *count) {
+  CTX_CHECK(c);
+  if (!count) return fail(GHOST_ERR_ARG, "null count");
+  *count = c->launches;
+  return GHOST_OK;
+}
+
+// ------------------------------------------------------------------ FFT
+int ghost_fftp3d_create_plan(ghost_ctx *c, const int n[3], int fftdir, int flags, ghost_fftplan **plan) {
+  (void)flags;
+  CTX_CHECK(c);
+  if (!n || !plan) return fail(GHOST_ERR_ARG, "null argument");
+  if (fftdir != GHOST_REAL_TO_COMPLEX && fftdir != GHOST_COMPLEX_TO_REAL)
+    return fail(GHOST_ERR_ARG, "fftdir %d: use -1 (real to complex) or +1 (complex to real)", fftdir);
+  if (n[0] != c->nx || n[1] != c->ny || n[2] != c->nz)
+    return fail(GHOST_ERR_SIZE, "plan size %dx%dx%d differs from the context grid", n[0], n[1], n[2]);
+  ghost_fftplan *p = new ghost_fftplan();
+  p->ctx = c;
+  p->fftdir = fftdir;
+  *plan = p;
+  return GHOST_OK;
+}
+
+int ghost_fftp3d_destroy_plan(ghost_fftplan *plan) {
+  delete plan;
+  return GHOST_OK;
+}
+
+int ghost_fftp3d_real_to_complex(ghost_fftplan *plan, const void *in, void *out) {
+  if (!plan || !in || !out) return fail(GHOST_ERR_ARG, "null argument");
+  ghost_ctx *c = plan->ctx;
+  if (plan->fftdir != GHOST_REAL_TO_COMPLEX) return fail(GHOST_ERR_STATE, "plan is not a real-to-complex plan");
+  Staging st(c);
+  const void *din;
+  void *dout;
+  GB_CHECK(st.map(in, c->rbytes, 1, &din));
+  GB_CHECK(st.map(out, c->cbytes, 2, &dout));
+  GB_CHECK(c->precision == GHOST_SINGLE ? r2c_dev<float>(c, din, dout) : r2c_dev<double>(c, din, dout));
+  return st.finish();
+}
+
+int ghost_fftp3d_complex_to_real(ghost_fftplan *plan, const void *in, void *out) {
+  if (!plan || !in || !out) return fail(GHOST_ERR_ARG, "null argument");
+  ghost_ctx *c = plan->ctx;
+  if (plan->fftdir != GHOST_COMPLEX_TO_REAL) return fail(GHOST_ERR_STATE, "plan is not a complex-to-real plan");
+  Staging st(c);
+  const void *din;
+  void *dout;
+  GB_CHECK(st.map(in, c->cbytes, 1, &din));
+  GB_CHECK(st.map(out, c->rbytes, 2, &dout));
+  GB_CHECK(c->precision == GHOST_SINGLE ? c2r_dev<float>(c, din, dout) : c2r_dev<double>(c, din, dout));
+  return st.finish();
+}
+
+// ------------------------------------------------------------ operators
+static int dir_ok(int dir) { return dir >= 1 && dir <= 3; }
+
+int ghost_derivk3(ghost_ctx *c, const void *a, void *b, int dir) {
+  CTX_CHECK(c);
+  if (!a || !b) return fail(GHOST_ERR_ARG, "null field");
+  if (!dir_ok(dir)) return fail(GHOST_ERR_ARG, "dir %d not in 1..3", dir);
+  Staging st(c);
+  const void *da;
+  void *db;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 2, &db));
+  GB_CHECK(GB_DISPATCH(c, derivk3)(c, da, db, dir));
+  return st.finish();
+}
+
+int ghost_laplak3(ghost_ctx *c, const void *a, void *b) {
+  CTX_CHECK(c);
+  if (!a || !b) return fail(GHOST_ERR_ARG, "null field");
+  Staging st(c);
+  const void *da;
+  void *db;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 2, &db));
+  GB_CHECK(GB_DISPATCH(c, laplak3)(c, da, db));
+  return st.finish();
+}
+
+int ghost_rotor3(ghost_ctx *c, const void *a, const void *b, void *o, int dir) {
+  CTX_CHECK(c);
+  if (!a || !b || !o) return fail(GHOST_ERR_ARG, "null field");
+  if (!dir_ok(dir)) return fail(GHOST_ERR_ARG, "dir %d not in 1..3", dir);
+  Staging st(c);
+  const void *da, *db;
+  void *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(o, c->cbytes, 2, &dc));
+  GB_CHECK(GB_DISPATCH(c, rotor3)(c, da, db, dc, dir));
+  return st.finish();
+}
+
+int ghost_prodre3(ghost_ctx *c, const void *a, const void *b, const void *cc, void *d, void *e, void *f) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e || !f) return fail(GHOST_ERR_ARG, "null field");
+  Staging st(c);
+  const void *da, *db, *dc;
+  void *dd, *de, *df;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(st.map(d, c->cbytes, 2, &dd));
+  GB_CHECK(st.map(e, c->cbytes, 2, &de));
+  GB_CHECK(st.map(f, c->cbytes, 2, &df));
+  GB_CHECK(c->precision == GHOST_SINGLE ? prodre3_dev<float>(c, da, db, dc, dd, de, df)
+                                        : prodre3_dev<double>(c, da, db, dc, dd, de, df));
+  return st.finish();
+}
+
+int ghost_nonlhd3(ghost_ctx *c, const void *a, const void *b, const void *cc, void *g, int dir) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !g) return fail(GHOST_ERR_ARG, "null field");
+  if (!dir_ok(dir)) return fail(GHOST_ERR_ARG, "dir %d not in 1..3", dir);
+  Staging st(c);
+  const void *da, *db, *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  // g may alias an input; the kernel reads all three inputs of a mode
+  // before writing g at that mode, so aliasing is safe element-wise
+  void *dg;
+  GB_CHECK(st.map(g, c->cbytes, 2, &dg));
+  GB_CHECK(GB_DISPATCH(c, nonlhd3)(c, da, db, dc, dg, dir));
+  return st.finish();
+}
+
+static int reduce_api(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d,
+                      const void *e, const void *f, double *out) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !out) return fail(GHOST_ERR_ARG, "null argument");
+  Staging st(c);
+  const void *da, *db, *dc, *dd = nullptr, *de = nullptr, *df = nullptr;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  if (d) {
+    GB_CHECK(st.map(d, c->cbytes, 1, &dd));
+    GB_CHECK(st.map(e, c->cbytes, 1, &de));
+    GB_CHECK(st.map(f, c->cbytes, 1, &df));
+  }
+  GB_CHECK(c->precision == GHOST_SINGLE ? reduce_dev<float>(c, kind, da, db, dc, dd, de, df, out)
+                                        : reduce_dev<double>(c, kind, da, db, dc, dd, de, df, out));
+  return st.finish();
+}
+
+int ghost_energy(ghost_ctx *c, const void *a, const void *b, const void *cc, double *d, int kin) {
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  const int kind = kin == 1 ? RED_ENERGY : (kin == 0 ? RED_ENSTROPHY : RED_LAPLACIAN);
+  return reduce_api(c, kind, a, b, cc, nullptr, nullptr, nullptr, d);
+}
+
+int ghost_helicity(ghost_ctx *c, const void *a, const void *b, const void *cc, double *d) {
+  return reduce_api(c, RED_HELICITY, a, b, cc, nullptr, nullptr, nullptr, d);
+}
+
+int ghost_cross(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                const void *f, double *g, int kin) {
+  if (kin != 0 && kin != 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
+  if (!d || !e || !f) return fail(GHOST_ERR_ARG, "null field");
+  return reduce_api(c, kin == 1 ? RED_CROSS : RED_CROSS_K2, a, b, cc, d, e, f, g);
+}
+
+int ghost_divergence(ghost_ctx *c, const void *a, const void *b, const void *cc, double *d) {
+  return reduce_api(c, RED_DIVERGENCE, a, b, cc, nullptr, nullptr, nullptr, d);
+}
+
+int ghost_maxabs(ghost_ctx *c, const void *a, const void *b, const void *cc, double *d, int kin) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d) return fail(GHOST_ERR_ARG, "null argument");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  Staging st(c);
+  const void *da, *db, *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(GB_DISPATCH(c, maxabs)(c, da, db, dc, d, kin));
+  return st.finish();
+}
+
+int ghost_spectrumc(ghost_ctx *c, const void *a, const void *b, const void *cc, int kin, int hel, double *Ek,
+                    double *Hk) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc) return fail(GHOST_ERR_ARG, "null field");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  if (kin <= 1 && !Ek) return fail(GHOST_ERR_ARG, "null Ek");
+  if (hel == 1 && !Hk) return fail(GHOST_ERR_ARG, "null Hk");
+  Staging st(c);
+  const void *da, *db, *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  const bool sp = c->precision == GHOST_SINGLE;
+  if (kin <= 1) {
+    const int kind = kin == 1 ? RED_ENERGY : RED_ENSTROPHY;
+    GB_CHECK(sp ? spectrum_dev<float>(c, kind, da, db, dc, Ek) : spectrum_dev<double>(c, kind, da, db, dc, Ek));
+  }
+  if (hel == 1)
+    GB_CHECK(sp ? spectrum_dev<float>(c, RED_HELICITY, da, db, dc, Hk)
+                : spectrum_dev<double>(c, RED_HELICITY, da, db, dc, Hk));
+  return st.finish();
+}
+
+int ghost_hdcheck(ghost_ctx *c, const void *vx, const void *vy, const void *vz, const void *fx, const void *fy,
+                  const void *fz, int hel, int chk, double out[5]) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz || !fx || !fy || !fz || !out) return fail(GHOST_ERR_ARG, "null argument");
+  Staging st(c);
+  const void *a, *b, *cc, *d, *e, *f;
+  GB_CHECK(st.map(vx, c->cbytes, 1, &a));
+  GB_CHECK(st.map(vy, c->cbytes, 1, &b));
+  GB_CHECK(st.map(vz, c->cbytes, 1, &cc));
+  GB_CHECK(st.map(fx, c->cbytes, 1, &d));
+  GB_CHECK(st.map(fy, c->cbytes, 1, &e));
+  GB_CHECK(st.map(fz, c->cbytes, 1, &f));
+  const bool sp = c->precision == GHOST_SINGLE;
+  auto red = [&](int kind, const void *p, const void *q, const void *r, double *o) {
+    return sp ? reduce_dev<float>(c, kind, a, b, cc, p, q, r, o) : reduce_dev<double>(c, kind, a, b, cc, p, q, r, o);
+  };
+  for (int q = 0; q < 5; ++q) out[q] = 0.0;
+  GB_CHECK(red(RED_ENERGY, nullptr, nullptr, nullptr, &out[0]));
+  GB_CHECK(red(RED_ENSTROPHY, nullptr, nullptr, nullptr, &out[1]));
+  if (hel == 1) GB_CHECK(red(RED_HELICITY, nullptr, nullptr, nullptr, &out[2]));
+  GB_CHECK(red(RED_CROSS, d, e, f, &out[3]));
+  if (chk == 1) GB_CHECK(red(RED_DIVERGENCE, nullptr, nullptr, nullptr, &out[4]));
+  return st.finish();
+}
+
+int ghost_normalize(ghost_ctx *c, void *fx, void *fy, void *fz, double f0, int kin) {
+  CTX_CHECK(c);
+  if (!fx || !fy || !fz) return fail(GHOST_ERR_ARG, "null field");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  Staging st(c);
+  void *a, *b, *cc;
+  GB_CHECK(st.map(fx, c->cbytes, 3, &a));
+  GB_CHECK(st.map(fy, c->cbytes, 3, &b));
+  GB_CHECK(st.map(fz, c->cbytes, 3, &cc));
+  const int kind = kin == 1 ? RED_ENERGY : (kin == 0 ? RED_ENSTROPHY : RED_LAPLACIAN);
+  double tmp;
+  const bool sp = c->precision == GHOST_SINGLE;
+  GB_CHECK(sp ? reduce_dev<float>(c, kind, a, b, cc, nullptr, nullptr, nullptr, &tmp)
+              : reduce_dev<double>(c, kind, a, b, cc, nullptr, nullptr, nullptr, &tmp));
+  GB_CHECK(GB_DISPATCH(c, scale3)(c, a, b, cc, f0, sqrt(tmp)));
+  return st.finish();
+}
+
+int ghost_sharp(ghost_ctx *c, const void *a, void *b, double delta) {
+  CTX_CHECK(c);
+  if (!a || !b) return fail(GHOST_ERR_ARG, "null field");
+  if (!(delta > 0)) return fail(GHOST_ERR_ARG, "delta must be positive");
+  Staging st(c);
+  const void *da;
+  void *db;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 2, &db));
+  GB_CHECK(GB_DISPATCH(c, sharp)(c, da, db, delta));
+  return st.finish();
+}
+
+// ------------------------------------------------------------------- RK
+int ghost_hd_rkstep1(ghost_ctx *c, const void *vx, const void *vy, const void *vz, void *C1, void *C2, void *C3) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz || !C1 || !C2 || !C3) return fail(GHOST_ERR_ARG, "null field");
+  Staging st(c);
+  const void *in[3];
+  void *out[3];
+  const void *src[3] = {vx, vy, vz};
+  void *dst[3] = {C1, C2, C3};
+  for (int q = 0; q < 3; ++q) {
+    GB_CHECK(st.map(src[q], c->cbytes, 1, &in[q]));
+    GB_CHECK(st.map(dst[q], c->cbytes, 2, &out[q]));
+    GB_CUDA(cudaMemcpyAsync(out[q], in[q], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return st.finish();
+}
+
+int ghost_hd_rkstep2(ghost_ctx *c, int o, double dt, double nu, void *vx, void *vy, void *vz, const void *C1,
+                     const void *C2, const void *C3, const void *fx, const void *fy, const void *fz) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz || !C1 || !C2 || !C3) return fail(GHOST_ERR_ARG, "null field");
+  if (o < 1) return fail(GHOST_ERR_ARG, "substep o=%d must be >= 1", o);
+  if ((fx == nullptr) != (fy == nullptr) || (fx == nullptr) != (fz == nullptr))
+    return fail(GHOST_ERR_ARG, "forcing components must be all given or all null");
+  Staging st(c);
+  void *v[3];
+  void *Cd[3];
+  const void *f[3] = {nullptr, nullptr, nullptr};
+  void *vu[3] = {vx, vy, vz};
+  const void *Cu[3] = {C1, C2, C3};
+  const void *fu[3] = {fx, fy, fz};
+  for (int q = 0; q < 3; ++q) {
+    GB_CHECK(st.map(vu[q], c->cbytes, 3, &v[q]));
+    const void *t;
+    GB_CHECK(st.map(Cu[q], c->cbytes, 1, &t));
+    Cd[q] = (void *)t;
+    if (fx) GB_CHECK(st.map(fu[q], c->cbytes, 1, &f[q]));
+  }
+  GB_CHECK(c->precision == GHOST_SINGLE ? hd_substep_dev<float>(c, o, dt, nu, v, Cd, fx ? f : nullptr, 0)
+                                        : hd_substep_dev<double>(c, o, dt, nu, v, Cd, fx ? f : nullptr, 0));
+  return st.finish();
+}
+
+int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *vx, void *vy, void *vz, void *C1,
+                 void *C2, void *C3, const void *fx, const void *fy, const void *fz) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz) return fail(GHOST_ERR_ARG, "null field");
+  if (nsteps < 0 || ord < 1) return fail(GHOST_ERR_ARG, "nsteps=%d ord=%d", nsteps, ord);
+  if ((fx == nullptr) != (fy == nullptr) || (fx == nullptr) != (fz == nullptr))
+    return fail(GHOST_ERR_ARG, "forcing components must be all given or all null");
+  if ((C1 == nullptr) != (C2 == nullptr) || (C1 == nullptr) != (C3 == nullptr))
+    return fail(GHOST_ERR_ARG, "RK storage must be all given or all null");
+  Staging st(c);
+  void *v[3], *Cd[3];
+  const void *f[3] = {nullptr, nullptr, nullptr};
+  void *vu[3] = {vx, vy, vz};
+  void *Cu[3] = {C1, C2, C3};
+  const void *fu[3] = {fx, fy, fz};
+  for (int q = 0; q < 3; ++q) {
+    GB_CHECK(st.map(vu[q], c->cbytes, 3, &v[q]));
+    if (fx) GB_CHECK(st.map(fu[q], c->cbytes, 1, &f[q]));
+    if (C1) {
+      GB_CHECK(st.map(Cu[q], c->cbytes, 3, &Cd[q]));
+    } else {
+      if (!c->rk[q]) GB_CHECK(dalloc(&c->rk[q], c->cbytes));
+      Cd[q] = c->rk[q];
+    }
+  }
+  for (int t = 0; t < nsteps; ++t)
+    for (int o = ord; o >= 1; --o)
+      GB_CHECK(c->precision == GHOST_SINGLE ? hd_substep_dev<float>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord)
+                                            : hd_substep_dev<double>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord));
+  return st.finish();
+}
+
+int ghost_init_random_solenoidal(ghost_ctx *c, int32_t *seed, double kdn, double kup, int shape, double amp, void *ox,
+                                 void *oy, void *oz) {
+  CTX_CHECK(c);
+  if (!seed || !ox || !oy || !oz) return fail(GHOST_ERR_ARG, "null argument");
+  if (shape != 0 && shape != 1) return fail(GHOST_ERR_ARG, "shape %d not in 0..1", shape);
+  Staging st(c);
+  void *a, *b, *cc;
+  GB_CHECK(st.map(ox, c->cbytes, 2, &a));
+  GB_CHECK(st.map(oy, c->cbytes, 2, &b));
+  GB_CHECK(st.map(oz, c->cbytes, 2, &cc));
+  GB_CHECK(c->precision == GHOST_SINGLE ? init_random_impl<float>(c, seed, kdn, kup, shape, amp, a, b, cc)
+                                        : init_random_impl<double>(c, seed, kdn, kup, shape, amp, a, b, cc));
+  return st.finish();
+}
+
+// ----------------------------------------------------------- Boussinesq
+int ghost_advect3(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, void *e) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e) return fail(GHOST_ERR_ARG, "null field");
+  Staging st(c);
+  const void *da, *db, *dc, *dd;
+  void *de;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(st.map(d, c->cbytes, 1, &dd));
+  GB_CHECK(st.map(e, c->cbytes, 2, &de));
+  GB_CHECK(c->precision == GHOST_SINGLE ? advect3_dev<float>(c, da, db, dc, dd, de)
+                                        : advect3_dev<double>(c, da, db, dc, dd, de));
+  return st.finish();
+}
+
+static int bouss_args(ghost_ctx *c, Staging &st, void *vx, void *vy, void *vz, void *th, const void *fx,
+                      const void *fy, const void *fz, const void *fs, void *v[4], const void *f[4], bool *have_f) {
+  if (!vx || !vy || !vz || !th) return fail(GHOST_ERR_ARG, "null field");
+  if ((fx == nullptr) != (fy == nullptr) || (fx == nullptr) != (fz == nullptr))
+    return fail(GHOST_ERR_ARG, "forcing components must be all given or all null");
+  void *vu[4] = {vx, vy, vz, th};
+  const void *fu[4] = {fx, fy, fz, fs};
+  *have_f = fx != nullptr || fs != nullptr;
+  for (int q = 0; q < 4; ++q) {
+    GB_CHECK(st.map(vu[q], c->cbytes, 3, &v[q]));
+    GB_CHECK(st.map(fu[q], c->cbytes, 1, &f[q]));
+  }
+  return GHOST_OK;
+}
+
+int ghost_bouss_rkstep2(ghost_ctx *c, int o, double dt, double nu, double kappa, double omegaz, double xmom,
+                        double xtemp, void *vx, void *vy, void *vz, void *th, const void *C1, const void *C2,
+                        const void *C3, const void *C20, const void *fx, const void *fy, const void *fz,
+                        const void *fs) {
+  CTX_CHECK(c);
+  if (o < 1) return fail(GHOST_ERR_ARG, "substep o=%d must be >= 1", o);
+  if (!C1 || !C2 || !C3 || !C20) return fail(GHOST_ERR_ARG, "null RK storage");
+  Staging st(c);
+  void *v[4], *Cd[4];
+  const void *f[4];
+  bool have_f;
+  GB_CHECK(bouss_args(c, st, vx, vy, vz, th, fx, fy, fz, fs, v, f, &have_f));
+  const void *Cu[4] = {C1, C2, C3, C20};
+  for (int q = 0; q < 4; ++q) {
+    const void *t;
+    GB_CHECK(st.map(Cu[q], c->cbytes, 1, &t));
+    Cd[q] = (void *)t;
+  }
+  GB_CHECK(c->precision == GHOST_SINGLE
+               ? bouss_substep_dev<float>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr, 0)
+               : bouss_substep_dev<double>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr, 0));
+  return st.finish();
+}
+
+int ghost_bouss_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, double kappa, double omegaz,
+                    double xmom, double xtemp, void *vx, void *vy, void *vz, void *th, const void *fx,
+                    const void *fy, const void *fz, const void *fs) {
+  CTX_CHECK(c);
+  if (nsteps < 0 || ord < 1) return fail(GHOST_ERR_ARG, "nsteps=%d ord=%d", nsteps, ord);
+  Staging st(c);
+  void *v[4], *Cd[4];
+  const void *f[4];
+  bool have_f;
+  GB_CHECK(bouss_args(c, st, vx, vy, vz, th, fx, fy, fz, fs, v, f, &have_f));
+  for (int q = 0; q < 4; ++q) {
+    if (!c->rk[q]) GB_CHECK(dalloc(&c->rk[q], c->cbytes));
+    Cd[q] = c->rk[q];
+  }
+  for (int t = 0; t < nsteps; ++t)
+    for (int o = ord; o >= 1; --o)
+      GB_CHECK(c->precision == GHOST_SINGLE
+                   ? bouss_substep_dev<float>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr,
+                                              o == ord)
+                   : bouss_substep_dev<double>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr,
+                                               o == ord));
+  return st.finish();
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// common.cuh -- context state, wavenumber parameters and error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ghost_b200.h"
+#include "fft_core.cuh"
+
+namespace gb {
+
+// Thread-local last error, reported by ghost_last_error_string().
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+
+#define GB_CUDA(call)                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return ::gb::fail(GHOST_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,        \
+                        cudaGetErrorString(e_));                                          \
+  } while (0)
+
+#define GB_CHECK(expr)          \
+  do {                          \
+    int s_ = (expr);            \
+    if (s_ != GHOST_OK) return s_; \
+  } while (0)
+
+// Wavenumber state passed by value to kernels (the kes/ali modules).
+// Wavenumbers are rebuilt from indices with the operation order of
+// main3D.fpp:1746-1800, so they match the host tables bit for bit.
+template <typename R> struct KParams {
+  int nx, ny, nz, nxh;
+  int anis, arbsize;
+  R Dkx, Dky, Dkz;
+  R rmp, rmq, rms;  // per-axis normalisation of kn2 when anis
+  R kmax, tiny;
+  R tmp;            // 1/(nx ny nz)^2
+};
+
+template <typename R> __device__ __forceinline__ R kx_of(const KParams<R> &p, int i) {
+  R v = (R)(i < p.nx / 2 ? i : i - p.nx);
+  return p.arbsize ? v * p.Dkx : v;
+}
+template <typename R> __device__ __forceinline__ R ky_of(const KParams<R> &p, int j) {
+  R v = (R)(j < p.ny / 2 ? j : j - p.ny);
+  return p.arbsize ? v * p.Dky : v;
+}
+template <typename R> __device__ __forceinline__ R kz_of(const KParams<R> &p, int k) {
+  R v = (R)(k < p.nz / 2 ? k : k - p.nz);
+  return p.arbsize ? v * p.Dkz : v;
+}
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+
+// kn2 (dealias measure) with the unfused operation order of main3D.fpp:1778
+template <typename R> __device__ __forceinline__ R kn2_of(const KParams<R> &p, int i, int j, int k) {
+  R a = (R)(i < p.nx / 2 ? i : i - p.nx), b = (R)(j < p.ny / 2 ? j : j - p.ny),
+    c = (R)(k < p.nz / 2 ? k : k - p.nz);
+  if (p.anis)
+    return radd(radd(rmul(p.rmp, rmul(a, a)), rmul(p.rmq, rmul(b, b))), rmul(p.rms, rmul(c, c)));
+  return radd(radd(rmul(a, a), rmul(b, b)), rmul(c, c));
+}
+// kk2 (physical |k|^2), main3D.fpp:1790-1800
+template <typename R> __device__ __forceinline__ R kk2_of(const KParams<R> &p, int i, int j, int k) {
+  if (!p.anis) return kn2_of(p, i, j, k);
+  R a = kx_of(p, i), b = ky_of(p, j), c = kz_of(p, k);
+  return radd(radd(rmul(a, a), rmul(b, b)), rmul(c, c));
+}
+
+struct DeviceBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace gb
+
+// The opaque context of the C ABI.
+struct ghost_ctx {
+  int nx, ny, nz, nxh;
+  int precision;     // GHOST_SINGLE or GHOST_DOUBLE
+  int arbsize, anis;
+  int nmax, nmaxperp;
+  double Lx, Ly, Lz, Dkx, Dky, Dkz, Dkk;
+  double kmax, tiny;
+  size_t nspec, nreal;   // elements per spectral / real field
+  size_t cbytes, rbytes; // bytes per spectral / real field
+  int device;
+  cudaStream_t stream;
+  long long launches;
+  // device twiddle tables exp(-2 pi i e/n) for n = nx, ny, nz (precision of ctx)
+  void *tw_x, *tw_y, *tw_z;
+  // scratch spectral fields (allocated on demand, grow only)
+  std::vector<void *> scratch;
+  // FP64 partial sums for deterministic reductions
+  double *partials;
+  size_t partials_elems;
+  // staging buffers for host-array calls
+  std::vector<void *> stage;
+  // RK storage owned by the context when the caller passes none
+  void *rk[4];
+  gb::KParams<float> kp32;
+  gb::KParams<double> kp64;
+  // per-kernel timers (ghost_ctx_enable_timers)
+  bool timers_on;
+  std::vector<cudaEvent_t> ev_free;
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> ev_pending;
+  double t_ms[GHOST_TIMER_KINDS];
+  long long t_n[GHOST_TIMER_KINDS];
+};
+
+struct ghost_fftplan {
+  ghost_ctx *ctx;
+  int fftdir;
+};

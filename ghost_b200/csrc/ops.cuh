@@ -1,0 +1,264 @@
+// ops.cuh -- pointwise spectral operators and deterministic FP64
+// reductions of pseudo/pseudospec3D_hd.f90.
+#pragma once
+#include "common.cuh"
+
+namespace gb {
+
+// mode index p = k + nz*(j + ny*i)
+template <typename R> __device__ __forceinline__ void unflat(const KParams<R> &kp, size_t p, int &i, int &j, int &k) {
+  k = (int)(p % kp.nz);
+  size_t q = p / kp.nz;
+  j = (int)(q % kp.ny);
+  i = (int)(q / kp.ny);
+}
+
+// i*kd*a as the Fortran expression im*k*a evaluates it
+template <typename C, typename R> __device__ __forceinline__ C ik(R kd, C a) { return mk(-(kd * a.y), kd * a.x); }
+
+template <typename R> __device__ __forceinline__ R kdir(const KParams<R> &kp, int dir, int i, int j, int k) {
+  return dir == 1 ? kx_of(kp, i) : (dir == 2 ? ky_of(kp, j) : kz_of(kp, k));
+}
+
+// curl component dir of (x,y,z) at one mode, rotor3 order (pseudospec3D_hd.f90:155-196)
+template <typename C, typename R>
+__device__ __forceinline__ C curl_at(const KParams<R> &kp, int dir, int i, int j, int k, C x, C y, C z) {
+  const R kx = kx_of(kp, i), ky = ky_of(kp, j), kz = kz_of(kp, k);
+  if (dir == 1) return csub(ik(ky, z), ik(kz, y));
+  if (dir == 2) return csub(ik(kz, x), ik(kx, z));
+  return csub(ik(kx, y), ik(ky, x));
+}
+
+template <typename R>
+__global__ void derivk3_kernel(KParams<R> kp, const cx<R> *a, cx<R> *b, size_t n, int dir) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    b[p] = ik(kdir(kp, dir, i, j, k), a[p]);
+  }
+}
+
+template <typename R>
+__global__ void laplak3_kernel(KParams<R> kp, const cx<R> *a, cx<R> *b, size_t n) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    const R kk2 = kk2_of(kp, i, j, k);
+    const cx<R> v = a[p];
+    b[p] = mk(-kk2 * v.x, -kk2 * v.y);
+  }
+}
+
+// rotor3(a,b,c,dir): the two given components are (a,b) in the order
+// GHOST passes them: dir 1 (vy,vz), dir 2 (vx,vz), dir 3 (vx,vy)
+template <typename R>
+__global__ void rotor3_kernel(KParams<R> kp, const cx<R> *a, const cx<R> *b,
+                              cx<R> *c, size_t n, int dir) {
+  using C = cx<R>;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    const C va = a[p], vb = b[p];
+    const C zero = mk((R)0, (R)0);
+    C r;
+    if (dir == 1) r = curl_at(kp, 1, i, j, k, zero, va, vb);
+    else if (dir == 2) r = curl_at(kp, 2, i, j, k, va, zero, vb);
+    else r = curl_at(kp, 3, i, j, k, va, vb, zero);
+    c[p] = r;
+  }
+}
+
+template <typename R>
+__global__ void nonlhd3_kernel(KParams<R> kp, const cx<R> *a, const cx<R> *b,
+                               const cx<R> *c, cx<R> *g, size_t n, int dir) {
+  using C = cx<R>;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    const C va = a[p], vb = b[p], vc = c[p];
+    const C self = dir == 1 ? va : (dir == 2 ? vb : vc);
+    const int idx = dir == 1 ? i : (dir == 2 ? j : k);
+    C r;
+    if (idx == 0) {
+      r = mk(-self.x, -self.y);
+    } else {
+      const R kx = kx_of(kp, i), ky = ky_of(kp, j), kz = kz_of(kp, k);
+      const R kk2 = kk2_of(kp, i, j, k), kd = kdir(kp, dir, i, j, k);
+      const C s = mk(kx * va.x + ky * vb.x + kz * vc.x, kx * va.y + ky * vb.y + kz * vc.y);
+      r = mk(-self.x + (kd * s.x) / kk2, -self.y + (kd * s.y) / kk2);
+    }
+    g[p] = r;
+  }
+}
+
+template <typename R>
+__global__ void sharp_kernel(KParams<R> kp, const cx<R> *a, cx<R> *b, size_t n, R cut) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    b[p] = kn2_of(kp, i, j, k) <= cut ? a[p] : mk((R)0, (R)0);
+  }
+}
+
+// normalize: f = f*f0/sqrt(tmp) with the division done in FP64 as the
+// mixed-kind Fortran expression of module_dns.f90:35-37 does
+template <typename R>
+__global__ void scale3_kernel(cx<R> *x, cx<R> *y, cx<R> *z, size_t n, R f0, double s) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    cx<R> *f[3] = {x, y, z};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const cx<R> v = f[c][p];
+      f[c][p] = mk((R)((double)(v.x * f0) / s), (R)((double)(v.y * f0) / s));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// FP64 reductions over the half spectrum: sum_p w(i) * term(p), w = 1 on
+// the kx = 0 plane and 2 elsewhere (the Hermitian weighting of
+// pseudospec3D_hd.f90:550-567).  Per-block partials in a fixed grid, then
+// one block sums them in a fixed tree: bitwise reproducible.
+enum RedKind { RED_ENERGY = 0, RED_ENSTROPHY = 1, RED_LAPLACIAN = 2, RED_HELICITY = 3, RED_CROSS = 4,
+               RED_CROSS_K2 = 5, RED_DIVERGENCE = 6 };
+
+template <typename R> struct RedArgs {
+  const cx<R> *a, *b, *c, *d, *e, *f;
+};
+
+template <typename R>
+__device__ __forceinline__ R red_term(const KParams<R> &kp, const RedArgs<R> &ra, int kind, size_t p, int i, int j, int k) {
+  using C = cx<R>;
+  const C va = ra.a[p], vb = ra.b[p], vc = ra.c[p];
+  switch (kind) {
+    case RED_ENERGY:
+      return (va.x * va.x + va.y * va.y + vb.x * vb.x + vb.y * vb.y + vc.x * vc.x + vc.y * vc.y) * kp.tmp;
+    case RED_ENSTROPHY: {
+      const C w1 = curl_at(kp, 1, i, j, k, va, vb, vc), w2 = curl_at(kp, 2, i, j, k, va, vb, vc),
+              w3 = curl_at(kp, 3, i, j, k, va, vb, vc);
+      return (w1.x * w1.x + w1.y * w1.y + w2.x * w2.x + w2.y * w2.y + w3.x * w3.x + w3.y * w3.y) * kp.tmp;
+    }
+    case RED_LAPLACIAN: {
+      const R kk2 = kk2_of(kp, i, j, k);
+      const R s = va.x * va.x + va.y * va.y + vb.x * vb.x + vb.y * vb.y + vc.x * vc.x + vc.y * vc.y;
+      return (kk2 * kk2) * s * kp.tmp;
+    }
+    case RED_HELICITY: {
+      const C w1 = curl_at(kp, 1, i, j, k, va, vb, vc), w2 = curl_at(kp, 2, i, j, k, va, vb, vc),
+              w3 = curl_at(kp, 3, i, j, k, va, vb, vc);
+      return (cmulc(va, w1).x + cmulc(vb, w2).x + cmulc(vc, w3).x) * kp.tmp;
+    }
+    case RED_CROSS:
+    case RED_CROSS_K2: {
+      const C vd = ra.d[p], ve = ra.e[p], vf = ra.f[p];
+      R s = cmulc(va, vd).x + cmulc(vb, ve).x + cmulc(vc, vf).x;
+      if (kind == RED_CROSS_K2) s = s * kk2_of(kp, i, j, k);
+      return s * kp.tmp;
+    }
+    default: {  // RED_DIVERGENCE
+      const C s = cadd(cadd(ik(kx_of(kp, i), va), ik(ky_of(kp, j), vb)), ik(kz_of(kp, k), vc));
+      return (s.x * s.x + s.y * s.y) * kp.tmp;
+    }
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[q];
+  __syncthreads();
+  return s;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) reduce_kernel(KParams<R> kp, RedArgs<R> ra, int kind, size_t n, double *partials) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    const double w = i == 0 ? 1.0 : 2.0;
+    acc += w * (double)red_term(kp, ra, kind, p, i, j, k);
+  }
+  const double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// Sums nparts partials in a fixed order (one block).  Also used for the
+// per-bin spectrum partials with stride.
+__global__ void __launch_bounds__(256) finalize_kernel(const double *partials, int nparts, int nbins, double *out) {
+  __shared__ double sh[32];
+  for (int b = 0; b < nbins; ++b) {
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) acc += partials[(size_t)q * nbins + b];
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) out[b] = s;
+  }
+}
+
+// Shell spectra (spectrumc, pseudospec3D_hd.f90:1190-1415).  Each warp
+// owns a shared histogram; lanes add in lane order, warps are combined in
+// warp order, blocks in block order: reproducible bit for bit.
+template <typename R>
+__global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R> ra, int kind, size_t n, int nb,
+                                                       R Dkk, double *partials) {
+  extern __shared__ double hist[];  // (blockDim/32) * nb
+  const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = threadIdx.x; q < nw * nb; q += blockDim.x) hist[q] = 0.0;
+  __syncthreads();
+  double *hw = hist + (size_t)w * nb;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t start = blockIdx.x * (size_t)blockDim.x + (size_t)w * 32;
+  for (size_t base = start; base < n; base += stride) {
+    const size_t p = base + lane;
+    int bin = -1;
+    double val = 0.0;
+    if (p < n) {
+      int i, j, k;
+      unflat(kp, p, i, j, k);
+      const R kk2 = kk2_of(kp, i, j, k);
+      const int kmn = (int)(sqrt(kk2) / Dkk + (R)0.501f);  // .501 is a default-REAL literal in GHOST
+      if (kmn > 0 && kmn <= nb) {
+        const R wgt = i == 0 ? (R)1 : (R)2;
+        bin = kmn - 1;
+        val = (double)(wgt * red_term(kp, ra, kind, p, i, j, k));
+      }
+    }
+    for (int s = 0; s < 32; ++s) {
+      if (lane == s && bin >= 0) hw[bin] += val;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < nw; ++q) s += hist[(size_t)q * nb + b];
+    partials[(size_t)blockIdx.x * nb + b] = s;
+  }
+}
+
+// max over real space of sqrt(r1^2+r2^2+r3^2) (maxabs); non-negative
+// floats order like their bit patterns, so an integer max is exact.
+template <typename R>
+__global__ void maxnorm_kernel(const R *__restrict__ r1, const R *__restrict__ r2, const R *__restrict__ r3, size_t n,
+                               unsigned long long *out) {
+  R m = 0;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const R s = sqrt(r1[p] * r1[p] + r2[p] * r2[p] + r3[p] * r3[p]);
+    m = s > m ? s : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const R q = __shfl_down_sync(0xffffffffu, m, o);
+    m = q > m ? q : m;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    const double md = (double)m;
+    atomicMax(out, (unsigned long long)__double_as_longlong(md));
+  }
+}
+
+}  // namespace gb

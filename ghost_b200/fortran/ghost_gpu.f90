@@ -1,0 +1,472 @@
+!=================================================================
+! ghost_gpu.f90 -- ISO_C_BINDING interface of libghost_b200 and
+! drop-in replacements for GHOST's HD hot-path routines.
+!
+! MODULE ghost_gpu      : BIND(C) interfaces of include/ghost_b200.h,
+!                         one context per run (ghost_gpu_init).
+! Drop-in subroutines   : fftp3d_create_plan, fftp3d_destroy_plan,
+!                         fftp3d_real_to_complex, fftp3d_complex_to_real
+!                         (replacing fftp-3/fftp3D.fpp), and derivk3,
+!                         laplak3, rotor3, prodre3, nonlhd3, energy,
+!                         helicity, cross, maxabs, spectrumc (replacing
+!                         pseudo/pseudospec3D_hd.f90) with GHOST's argument
+!                         lists.  Arrays are GHOST's host arrays; the library
+!                         stages them through the GPU.  Codes that keep
+!                         their fields on the device call the ghost_* C
+!                         functions with device pointers directly.
+!
+! Build (with gfortran >= 9):
+!   gfortran -c -cpp ghost_gpu.f90
+!   link with -L<repo>/ghost_b200 -lghost_b200 -lcudart
+! GHOST's fprecision module supplies GP; GHOST_GP_KIND below must match
+! (4 = SINGLE, 8 = DOUBLE).
+!=================================================================
+      MODULE ghost_gpu
+      USE ISO_C_BINDING
+      IMPLICIT NONE
+
+      INTEGER(C_INT), PARAMETER :: GHOST_OK = 0
+      INTEGER(C_INT), PARAMETER :: GHOST_SINGLE = 4, GHOST_DOUBLE = 8
+      TYPE(C_PTR), SAVE :: gctx = C_NULL_PTR
+
+      TYPE, BIND(C) :: ghost_info
+         INTEGER(C_INT)    :: nx, ny, nz, precision, anis, nmax, nmaxperp
+         REAL(C_DOUBLE)    :: kmax, tiny, Lx, Ly, Lz, Dkx, Dky, Dkz, Dkk
+         INTEGER(C_SIZE_T) :: spectral_elems, real_elems
+      END TYPE ghost_info
+
+      INTERFACE
+       FUNCTION ghost_ctx_create(nx,ny,nz,Lx,Ly,Lz,arbsize,prec,ctx) &
+                BIND(C,name="ghost_ctx_create") RESULT(s)
+         IMPORT :: C_INT, C_DOUBLE, C_PTR
+         INTEGER(C_INT), VALUE :: nx, ny, nz, arbsize, prec
+         REAL(C_DOUBLE), VALUE :: Lx, Ly, Lz
+         TYPE(C_PTR) :: ctx
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_destroy(ctx) BIND(C,name="ghost_ctx_destroy") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_get_info(ctx,info) BIND(C,name="ghost_ctx_get_info") RESULT(s)
+         IMPORT :: C_INT, C_PTR, ghost_info
+         TYPE(C_PTR), VALUE :: ctx
+         TYPE(ghost_info) :: info
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_set_stream(ctx,stream) BIND(C,name="ghost_ctx_set_stream") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, stream
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_set_kmax(ctx,kmax) BIND(C,name="ghost_ctx_set_kmax") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx
+         REAL(C_DOUBLE), VALUE :: kmax
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_synchronize(ctx) BIND(C,name="ghost_ctx_synchronize") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_launch_count(ctx,n) BIND(C,name="ghost_ctx_launch_count") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_LONG_LONG
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_LONG_LONG) :: n
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_enable_timers(ctx,enable) BIND(C,name="ghost_ctx_enable_timers") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT), VALUE :: enable
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_read_timers(ctx,ms,launches) BIND(C,name="ghost_ctx_read_timers") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE, C_LONG_LONG
+         TYPE(C_PTR), VALUE :: ctx
+         REAL(C_DOUBLE) :: ms(10)
+         INTEGER(C_LONG_LONG) :: launches(10)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_last_error_string() BIND(C,name="ghost_last_error_string") RESULT(p)
+         IMPORT :: C_PTR
+         TYPE(C_PTR) :: p
+       END FUNCTION
+       FUNCTION ghost_fftp3d_create_plan(ctx,n,fftdir,flags,plan) &
+                BIND(C,name="ghost_fftp3d_create_plan") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT) :: n(3)
+         INTEGER(C_INT), VALUE :: fftdir, flags
+         TYPE(C_PTR) :: plan
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_fftp3d_destroy_plan(plan) BIND(C,name="ghost_fftp3d_destroy_plan") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: plan
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_fftp3d_real_to_complex(plan,in,out) &
+                BIND(C,name="ghost_fftp3d_real_to_complex") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: plan, in, out
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_fftp3d_complex_to_real(plan,in,out) &
+                BIND(C,name="ghost_fftp3d_complex_to_real") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: plan, in, out
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_derivk3(ctx,a,b,dir) BIND(C,name="ghost_derivk3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b
+         INTEGER(C_INT), VALUE :: dir
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_laplak3(ctx,a,b) BIND(C,name="ghost_laplak3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_rotor3(ctx,a,b,c,dir) BIND(C,name="ghost_rotor3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: dir
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_prodre3(ctx,a,b,c,d,e,f) BIND(C,name="ghost_prodre3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_nonlhd3(ctx,a,b,c,g,dir) BIND(C,name="ghost_nonlhd3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, g
+         INTEGER(C_INT), VALUE :: dir
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_energy(ctx,a,b,c,d,kin) BIND(C,name="ghost_energy") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         REAL(C_DOUBLE) :: d
+         INTEGER(C_INT), VALUE :: kin
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_helicity(ctx,a,b,c,d) BIND(C,name="ghost_helicity") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         REAL(C_DOUBLE) :: d
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_cross(ctx,a,b,c,d,e,f,g,kin) BIND(C,name="ghost_cross") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         REAL(C_DOUBLE) :: g
+         INTEGER(C_INT), VALUE :: kin
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_divergence(ctx,a,b,c,d) BIND(C,name="ghost_divergence") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         REAL(C_DOUBLE) :: d
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_maxabs(ctx,a,b,c,d,kin) BIND(C,name="ghost_maxabs") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         REAL(C_DOUBLE) :: d
+         INTEGER(C_INT), VALUE :: kin
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_spectrumc(ctx,a,b,c,kin,hel,Ek,Hk) BIND(C,name="ghost_spectrumc") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: kin, hel
+         REAL(C_DOUBLE) :: Ek(*), Hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_hdcheck(ctx,vx,vy,vz,fx,fy,fz,hel,chk,out) BIND(C,name="ghost_hdcheck") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, fx, fy, fz
+         INTEGER(C_INT), VALUE :: hel, chk
+         REAL(C_DOUBLE) :: out(5)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_normalize(ctx,fx,fy,fz,f0,kin) BIND(C,name="ghost_normalize") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, fx, fy, fz
+         REAL(C_DOUBLE), VALUE :: f0
+         INTEGER(C_INT), VALUE :: kin
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_sharp(ctx,a,b,delta) BIND(C,name="ghost_sharp") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b
+         REAL(C_DOUBLE), VALUE :: delta
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_hd_rkstep1(ctx,vx,vy,vz,C1,C2,C3) BIND(C,name="ghost_hd_rkstep1") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, C1, C2, C3
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_hd_rkstep2(ctx,o,dt,nu,vx,vy,vz,C1,C2,C3,fx,fy,fz) &
+                BIND(C,name="ghost_hd_rkstep2") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, C1, C2, C3, fx, fy, fz
+         INTEGER(C_INT), VALUE :: o
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_hd_run(ctx,nsteps,ord,dt,nu,vx,vy,vz,C1,C2,C3,fx,fy,fz) &
+                BIND(C,name="ghost_hd_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, C1, C2, C3, fx, fy, fz
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_advect3(ctx,a,b,c,d,e) BIND(C,name="ghost_advect3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_bouss_rkstep2(ctx,o,dt,nu,kappa,omegaz,xmom,xtemp, &
+                vx,vy,vz,th,C1,C2,C3,C20,fx,fy,fz,fs) &
+                BIND(C,name="ghost_bouss_rkstep2") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, th, C1, C2, C3, C20
+         TYPE(C_PTR), VALUE :: fx, fy, fz, fs
+         INTEGER(C_INT), VALUE :: o
+         REAL(C_DOUBLE), VALUE :: dt, nu, kappa, omegaz, xmom, xtemp
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_bouss_run(ctx,nsteps,ord,dt,nu,kappa,omegaz,xmom,xtemp, &
+                vx,vy,vz,th,fx,fy,fz,fs) BIND(C,name="ghost_bouss_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, th, fx, fy, fz, fs
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt, nu, kappa, omegaz, xmom, xtemp
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_init_random_solenoidal(ctx,seed,kdn,kup,shape,amp,ox,oy,oz) &
+                BIND(C,name="ghost_init_random_solenoidal") RESULT(s)
+         IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, ox, oy, oz
+         INTEGER(C_INT32_T) :: seed
+         REAL(C_DOUBLE), VALUE :: kdn, kup, amp
+         INTEGER(C_INT), VALUE :: shape
+         INTEGER(C_INT) :: s
+       END FUNCTION
+      END INTERFACE
+
+      CONTAINS
+
+      ! Creates the run's context; call once after nx,ny,nz and the box are
+      ! known (main3D.fpp:1721).  Stops on failure, like GHOST's setup.
+      SUBROUTINE ghost_gpu_init(nx,ny,nz,Lx,Ly,Lz,arbsize,gpkind)
+      INTEGER, INTENT(IN) :: nx, ny, nz, arbsize, gpkind
+      DOUBLE PRECISION, INTENT(IN) :: Lx, Ly, Lz
+      CALL ghost_gpu_check(ghost_ctx_create(nx,ny,nz,Lx,Ly,Lz,arbsize,gpkind,gctx), &
+                           'ghost_ctx_create')
+      END SUBROUTINE ghost_gpu_init
+
+      SUBROUTINE ghost_gpu_check(s,where)
+      INTEGER(C_INT), INTENT(IN) :: s
+      CHARACTER(len=*), INTENT(IN) :: where
+      CHARACTER(kind=C_CHAR), POINTER :: msg(:)
+      INTEGER :: n
+      IF (s.ne.GHOST_OK) THEN
+         CALL C_F_POINTER(ghost_last_error_string(), msg, [1024])
+         n = 0
+         DO WHILE (n.lt.1024)
+            IF (msg(n+1).eq.C_NULL_CHAR) EXIT
+            n = n+1
+         END DO
+         PRINT *, where, ': status ', s, ': ', msg(1:n)
+         STOP
+      ENDIF
+      END SUBROUTINE ghost_gpu_check
+
+      END MODULE ghost_gpu
+
+!=================================================================
+! Drop-in replacements with GHOST's interfaces.  They take GHOST's
+! module state (grid, mpivars) for the array shapes; the plan handle
+! travels in FFTPLAN%planr of the fftplans module.
+!=================================================================
+      SUBROUTINE fftp3d_create_plan(plan,n,fftdir,flags)
+      USE fftplans
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(FFTPLAN), INTENT(OUT) :: plan
+      INTEGER, INTENT(IN) :: n(3), fftdir, flags
+      TYPE(C_PTR) :: p
+      INTEGER(C_INT) :: nn(3)
+      nn = n
+      CALL ghost_gpu_check(ghost_fftp3d_create_plan(gctx,nn,fftdir,flags,p), &
+                           'fftp3d_create_plan')
+      plan%planr = TRANSFER(p,plan%planr)
+      plan%nx = n(1)
+      plan%ny = n(2)
+      plan%nz = n(3)
+      END SUBROUTINE fftp3d_create_plan
+
+      SUBROUTINE fftp3d_destroy_plan(plan)
+      USE fftplans
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(FFTPLAN), INTENT(INOUT) :: plan
+      CALL ghost_gpu_check(ghost_fftp3d_destroy_plan(TRANSFER(plan%planr,C_NULL_PTR)), &
+                           'fftp3d_destroy_plan')
+      END SUBROUTINE fftp3d_destroy_plan
+
+      SUBROUTINE fftp3d_real_to_complex(plan,in,out,comm)
+      USE fprecision
+      USE fftplans
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(FFTPLAN), INTENT(IN) :: plan
+      REAL(KIND=GP), INTENT(IN), TARGET :: in(plan%nx,plan%ny,plan%nz)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: out(plan%nz,plan%ny,plan%nx/2+1)
+      INTEGER, INTENT(IN) :: comm
+      CALL ghost_gpu_check(ghost_fftp3d_real_to_complex(TRANSFER(plan%planr,C_NULL_PTR), &
+                           C_LOC(in),C_LOC(out)),'fftp3d_real_to_complex')
+      END SUBROUTINE fftp3d_real_to_complex
+
+      SUBROUTINE fftp3d_complex_to_real(plan,in,out,comm)
+      USE fprecision
+      USE fftplans
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(FFTPLAN), INTENT(IN) :: plan
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: in(plan%nz,plan%ny,plan%nx/2+1)
+      REAL(KIND=GP), INTENT(OUT), TARGET :: out(plan%nx,plan%ny,plan%nz)
+      INTEGER, INTENT(IN) :: comm
+      CALL ghost_gpu_check(ghost_fftp3d_complex_to_real(TRANSFER(plan%planr,C_NULL_PTR), &
+                           C_LOC(in),C_LOC(out)),'fftp3d_complex_to_real')
+      END SUBROUTINE fftp3d_complex_to_real
+
+      SUBROUTINE derivk3(a,b,dir)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: b(nz,ny,nx/2+1)
+      INTEGER, INTENT(IN) :: dir
+      CALL ghost_gpu_check(ghost_derivk3(gctx,C_LOC(a),C_LOC(b),dir),'derivk3')
+      END SUBROUTINE derivk3
+
+      SUBROUTINE laplak3(a,b)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: b(nz,ny,nx/2+1)
+      CALL ghost_gpu_check(ghost_laplak3(gctx,C_LOC(a),C_LOC(b)),'laplak3')
+      END SUBROUTINE laplak3
+
+      SUBROUTINE rotor3(a,b,c,dir)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: c(nz,ny,nx/2+1)
+      INTEGER, INTENT(IN) :: dir
+      CALL ghost_gpu_check(ghost_rotor3(gctx,C_LOC(a),C_LOC(b),C_LOC(c),dir),'rotor3')
+      END SUBROUTINE rotor3
+
+      SUBROUTINE prodre3(a,b,c,d,e,f)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: d(nz,ny,nx/2+1), e(nz,ny,nx/2+1), f(nz,ny,nx/2+1)
+      CALL ghost_gpu_check(ghost_prodre3(gctx,C_LOC(a),C_LOC(b),C_LOC(c), &
+                           C_LOC(d),C_LOC(e),C_LOC(f)),'prodre3')
+      END SUBROUTINE prodre3
+
+      SUBROUTINE nonlhd3(a,b,c,g,dir)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(OUT), TARGET :: g(nz,ny,nx/2+1)
+      INTEGER, INTENT(IN) :: dir
+      CALL ghost_gpu_check(ghost_nonlhd3(gctx,C_LOC(a),C_LOC(b),C_LOC(c),C_LOC(g),dir), &
+                           'nonlhd3')
+      END SUBROUTINE nonlhd3
+
+      SUBROUTINE energy(a,b,c,d,kin)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      DOUBLE PRECISION, INTENT(OUT) :: d
+      INTEGER, INTENT(IN) :: kin
+      REAL(C_DOUBLE) :: dd
+      CALL ghost_gpu_check(ghost_energy(gctx,C_LOC(a),C_LOC(b),C_LOC(c),dd,kin),'energy')
+      d = dd
+      END SUBROUTINE energy
+
+      SUBROUTINE helicity(a,b,c,d)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      DOUBLE PRECISION, INTENT(OUT) :: d
+      REAL(C_DOUBLE) :: dd
+      CALL ghost_gpu_check(ghost_helicity(gctx,C_LOC(a),C_LOC(b),C_LOC(c),dd),'helicity')
+      d = dd
+      END SUBROUTINE helicity
+
+      SUBROUTINE cross(a,b,c,d,e,f,g,kin)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: d(nz,ny,nx/2+1), e(nz,ny,nx/2+1), f(nz,ny,nx/2+1)
+      DOUBLE PRECISION, INTENT(OUT) :: g
+      INTEGER, INTENT(IN) :: kin
+      REAL(C_DOUBLE) :: gg
+      CALL ghost_gpu_check(ghost_cross(gctx,C_LOC(a),C_LOC(b),C_LOC(c),C_LOC(d), &
+                           C_LOC(e),C_LOC(f),gg,kin),'cross')
+      g = gg
+      END SUBROUTINE cross
+
+      SUBROUTINE maxabs(a,b,c,d,kin)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      REAL(KIND=GP), INTENT(OUT) :: d
+      INTEGER, INTENT(IN) :: kin
+      REAL(C_DOUBLE) :: dd
+      CALL ghost_gpu_check(ghost_maxabs(gctx,C_LOC(a),C_LOC(b),C_LOC(c),dd,kin),'maxabs')
+      d = REAL(dd,KIND=GP)
+      END SUBROUTINE maxabs
+
+      SUBROUTINE spectrumc(a,b,c,kin,hel,Ektot,Hktot)
+      USE fprecision
+      USE grid
+      USE kes
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET :: a(nz,ny,nx/2+1), b(nz,ny,nx/2+1), c(nz,ny,nx/2+1)
+      INTEGER, INTENT(IN) :: kin, hel
+      DOUBLE PRECISION, INTENT(OUT), DIMENSION(nmax/2+1) :: Ektot, Hktot
+      CALL ghost_gpu_check(ghost_spectrumc(gctx,C_LOC(a),C_LOC(b),C_LOC(c),kin,hel, &
+                           Ektot,Hktot),'spectrumc')
+      END SUBROUTINE spectrumc

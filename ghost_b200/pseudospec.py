@@ -1,0 +1,274 @@
+"""Host-side mirror of GHOST's fftp / pseudospec3D interface over the C ABI.
+
+The names, argument order and meaning follow GHOST's Fortran routines
+(3D/src/fftp-3/fftp3D.fpp, 3D/src/pseudo/pseudospec3D_hd.f90 and the HD /
+ROTBOUSS include fragments): outputs are passed in, like Fortran INTENT(OUT)
+arrays, and scalar results are returned.
+
+Arrays are either CUDA tensors (torch; kept in HBM, no copies) or numpy
+arrays (host; staged through the library's device buffers), with GHOST's
+column-major layouts written as C-order shapes:
+    spectral a(nz,ny,nx/2+1)  ->  shape (nx//2+1, ny, nz), complex
+    real     r(nx,ny,nz)      ->  shape (nz, ny, nx), real
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import GHOST_COMPLEX_TO_REAL, GHOST_DOUBLE, GHOST_REAL_TO_COMPLEX, GHOST_SINGLE, check
+
+try:  # torch is only needed for device arrays
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_tensor(x) -> bool:
+    return torch is not None and isinstance(x, torch.Tensor)
+
+
+@dataclass
+class FFTPlan:
+    """fftp3d_create_plan's FFTPLAN (fftp-3/fftp_mod.fpp)."""
+    handle: ctypes.c_void_p
+    n: tuple
+    fftdir: int
+
+
+class Ghost:
+    """One GHOST grid: the grid/kes/ali/boxsize module state plus the HD
+    routines, executed by libghost_b200 on the current CUDA device."""
+
+    def __init__(self, nx: int, ny: int | None = None, nz: int | None = None,
+                 Lx: float = 1.0, Ly: float = 1.0, Lz: float = 1.0, arbsize: bool = False,
+                 precision: str = "fp64", stream=None):
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        self.lib = _lib.load()
+        self.precision = precision
+        code = {"fp32": GHOST_SINGLE, "fp64": GHOST_DOUBLE}[precision]
+        h = ctypes.c_void_p()
+        check(self.lib.ghost_ctx_create(nx, ny, nz, Lx, Ly, Lz, int(bool(arbsize)), code, ctypes.byref(h)),
+              "ghost_ctx_create")
+        self.h = h
+        info = _lib.GhostInfo()
+        check(self.lib.ghost_ctx_get_info(self.h, ctypes.byref(info)), "ghost_ctx_get_info")
+        self.info = info
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nxh = nx // 2 + 1
+        self.kmax, self.tiny, self.nmax, self.Dkk = info.kmax, info.tiny, info.nmax, info.Dkk
+        self.rdtype_np = np.float32 if precision == "fp32" else np.float64
+        self.cdtype_np = np.complex64 if precision == "fp32" else np.complex128
+        if stream is None and torch is not None and torch.cuda.is_available():
+            stream = torch.cuda.current_stream().cuda_stream
+        if stream is not None:
+            check(self.lib.ghost_ctx_set_stream(self.h, ctypes.c_void_p(stream)), "ghost_ctx_set_stream")
+        self.stream = stream
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ghost_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------
+    @property
+    def sshape(self):
+        return (self.nxh, self.ny, self.nz)
+
+    @property
+    def rshape(self):
+        return (self.nz, self.ny, self.nx)
+
+    @property
+    def ctorch(self):
+        return torch.complex64 if self.precision == "fp32" else torch.complex128
+
+    @property
+    def rtorch(self):
+        return torch.float32 if self.precision == "fp32" else torch.float64
+
+    def czeros(self, device="cuda"):
+        return torch.zeros(self.sshape, dtype=self.ctorch, device=device)
+
+    def rzeros(self, device="cuda"):
+        return torch.zeros(self.rshape, dtype=self.rtorch, device=device)
+
+    def _ptr(self, x, kind: str):
+        if x is None:
+            return None
+        shape = self.sshape if kind == "c" else self.rshape
+        if _is_tensor(x):
+            want = self.ctorch if kind == "c" else self.rtorch
+            if x.dtype != want or tuple(x.shape) != shape or not x.is_contiguous():
+                raise ValueError(f"expected contiguous {want} {shape}, got {x.dtype} {tuple(x.shape)}")
+            return ctypes.c_void_p(x.data_ptr())
+        if isinstance(x, np.ndarray):
+            want = self.cdtype_np if kind == "c" else self.rdtype_np
+            if x.dtype != want or x.shape != shape or not x.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"expected C-contiguous {np.dtype(want)} {shape}, got {x.dtype} {x.shape}")
+            return ctypes.c_void_p(x.ctypes.data)
+        raise TypeError(f"unsupported array type {type(x)}")
+
+    def launch_count(self) -> int:
+        n = ctypes.c_longlong()
+        check(self.lib.ghost_ctx_launch_count(self.h, ctypes.byref(n)), "ghost_ctx_launch_count")
+        return n.value
+
+    def enable_timers(self, on: bool = True):
+        check(self.lib.ghost_ctx_enable_timers(self.h, int(on)), "ghost_ctx_enable_timers")
+
+    def read_timers(self) -> dict:
+        """{kernel kind: (milliseconds, launches)} since the last read."""
+        n = len(_lib.TIMER_NAMES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        check(self.lib.ghost_ctx_read_timers(self.h, ms, cnt), "ghost_ctx_read_timers")
+        return {name: (ms[k], cnt[k]) for k, name in enumerate(_lib.TIMER_NAMES) if cnt[k]}
+
+    def synchronize(self):
+        check(self.lib.ghost_ctx_synchronize(self.h), "ghost_ctx_synchronize")
+
+    def set_kmax(self, kmax: float):
+        check(self.lib.ghost_ctx_set_kmax(self.h, kmax), "ghost_ctx_set_kmax")
+        info = _lib.GhostInfo()
+        check(self.lib.ghost_ctx_get_info(self.h, ctypes.byref(info)), "ghost_ctx_get_info")
+        self.kmax = info.kmax
+
+    # ---------------------------------------------------------------- fftp
+    def fftp3d_create_plan(self, n, fftdir: int, flags: int = 0) -> FFTPlan:
+        arr = (ctypes.c_int * 3)(*n)
+        h = ctypes.c_void_p()
+        check(self.lib.ghost_fftp3d_create_plan(self.h, arr, fftdir, flags, ctypes.byref(h)),
+              "fftp3d_create_plan")
+        return FFTPlan(h, tuple(n), fftdir)
+
+    def fftp3d_destroy_plan(self, plan: FFTPlan):
+        check(self.lib.ghost_fftp3d_destroy_plan(plan.handle), "fftp3d_destroy_plan")
+
+    def fftp3d_real_to_complex(self, plan: FFTPlan, inp, out):
+        check(self.lib.ghost_fftp3d_real_to_complex(plan.handle, self._ptr(inp, "r"), self._ptr(out, "c")),
+              "fftp3d_real_to_complex")
+
+    def fftp3d_complex_to_real(self, plan: FFTPlan, inp, out):
+        check(self.lib.ghost_fftp3d_complex_to_real(plan.handle, self._ptr(inp, "c"), self._ptr(out, "r")),
+              "fftp3d_complex_to_real")
+
+    # --------------------------------------------------- pseudospec3D_hd
+    def derivk3(self, a, b, dir: int):
+        check(self.lib.ghost_derivk3(self.h, self._ptr(a, "c"), self._ptr(b, "c"), dir), "derivk3")
+
+    def laplak3(self, a, b):
+        check(self.lib.ghost_laplak3(self.h, self._ptr(a, "c"), self._ptr(b, "c")), "laplak3")
+
+    def rotor3(self, a, b, c, dir: int):
+        check(self.lib.ghost_rotor3(self.h, self._ptr(a, "c"), self._ptr(b, "c"), self._ptr(c, "c"), dir),
+              "rotor3")
+
+    def prodre3(self, a, b, c, d, e, f):
+        check(self.lib.ghost_prodre3(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e, f)]), "prodre3")
+
+    def nonlhd3(self, a, b, c, g, dir: int):
+        check(self.lib.ghost_nonlhd3(self.h, *[self._ptr(x, "c") for x in (a, b, c, g)], dir), "nonlhd3")
+
+    def energy(self, a, b, c, kin: int) -> float:
+        d = ctypes.c_double()
+        check(self.lib.ghost_energy(self.h, *[self._ptr(x, "c") for x in (a, b, c)], ctypes.byref(d), kin),
+              "energy")
+        return d.value
+
+    def helicity(self, a, b, c) -> float:
+        d = ctypes.c_double()
+        check(self.lib.ghost_helicity(self.h, *[self._ptr(x, "c") for x in (a, b, c)], ctypes.byref(d)),
+              "helicity")
+        return d.value
+
+    def cross(self, a, b, c, d, e, f, kin: int) -> float:
+        g = ctypes.c_double()
+        check(self.lib.ghost_cross(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e, f)], ctypes.byref(g),
+                                   kin), "cross")
+        return g.value
+
+    def divergence(self, a, b, c) -> float:
+        d = ctypes.c_double()
+        check(self.lib.ghost_divergence(self.h, *[self._ptr(x, "c") for x in (a, b, c)], ctypes.byref(d)),
+              "divergence")
+        return d.value
+
+    def maxabs(self, a, b, c, kin: int) -> float:
+        d = ctypes.c_double()
+        check(self.lib.ghost_maxabs(self.h, *[self._ptr(x, "c") for x in (a, b, c)], ctypes.byref(d), kin),
+              "maxabs")
+        return d.value
+
+    def spectrumc(self, a, b, c, kin: int = 1, hel: int = 0):
+        nb = self.nmax // 2 + 1
+        Ek = np.zeros(nb)
+        Hk = np.zeros(nb)
+        pd = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.ghost_spectrumc(self.h, *[self._ptr(x, "c") for x in (a, b, c)], kin, hel,
+                                       Ek.ctypes.data_as(pd), Hk.ctypes.data_as(pd)), "spectrumc")
+        return Ek, Hk
+
+    def hdcheck(self, vx, vy, vz, fx, fy, fz, hel: int = 1, chk: int = 0):
+        out = np.zeros(5)
+        check(self.lib.ghost_hdcheck(self.h, *[self._ptr(x, "c") for x in (vx, vy, vz, fx, fy, fz)], hel, chk,
+                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "hdcheck")
+        return {"eng": out[0], "ens": out[1], "khe": out[2], "pot": out[3], "div": out[4]}
+
+    def normalize(self, fx, fy, fz, f0: float, kin: int = 1):
+        check(self.lib.ghost_normalize(self.h, *[self._ptr(x, "c") for x in (fx, fy, fz)], f0, kin), "normalize")
+
+    def sharp(self, a, b, delta: float):
+        check(self.lib.ghost_sharp(self.h, self._ptr(a, "c"), self._ptr(b, "c"), delta), "sharp")
+
+    # -------------------------------------------------------------- RK
+    def hd_rkstep1(self, vx, vy, vz, C1, C2, C3):
+        check(self.lib.ghost_hd_rkstep1(self.h, *[self._ptr(x, "c") for x in (vx, vy, vz, C1, C2, C3)]),
+              "hd_rkstep1")
+
+    def hd_rkstep2(self, o: int, dt: float, nu: float, vx, vy, vz, C1, C2, C3, fx=None, fy=None, fz=None):
+        check(self.lib.ghost_hd_rkstep2(self.h, o, dt, nu,
+                                        *[self._ptr(x, "c") for x in (vx, vy, vz, C1, C2, C3, fx, fy, fz)]),
+              "hd_rkstep2")
+
+    def hd_run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None,
+               C=(None, None, None)):
+        check(self.lib.ghost_hd_run(self.h, nsteps, ord, dt, nu,
+                                    *[self._ptr(x, "c") for x in (vx, vy, vz, *C, fx, fy, fz)]), "hd_run")
+
+    # ------------------------------------------------------- Boussinesq
+    def advect3(self, a, b, c, d, e):
+        check(self.lib.ghost_advect3(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e)]), "advect3")
+
+    def bouss_rkstep2(self, o, dt, nu, kappa, omegaz, xmom, xtemp, vx, vy, vz, th, C1, C2, C3, C20,
+                      fx=None, fy=None, fz=None, fs=None):
+        check(self.lib.ghost_bouss_rkstep2(
+            self.h, o, dt, nu, kappa, omegaz, xmom, xtemp,
+            *[self._ptr(x, "c") for x in (vx, vy, vz, th, C1, C2, C3, C20, fx, fy, fz, fs)]), "bouss_rkstep2")
+
+    def bouss_run(self, nsteps, ord, dt, nu, kappa, omegaz, xmom, xtemp, vx, vy, vz, th,
+                  fx=None, fy=None, fz=None, fs=None):
+        check(self.lib.ghost_bouss_run(
+            self.h, nsteps, ord, dt, nu, kappa, omegaz, xmom, xtemp,
+            *[self._ptr(x, "c") for x in (vx, vy, vz, th, fx, fy, fz, fs)]), "bouss_run")
+
+    # ------------------------------------------------------------ ICs
+    def init_random_solenoidal(self, seed: int, kdn: float, kup: float, shape: int, amp: float, ox, oy, oz) -> int:
+        s = ctypes.c_int32(seed)
+        check(self.lib.ghost_init_random_solenoidal(self.h, ctypes.byref(s), kdn, kup, shape, amp,
+                                                    *[self._ptr(x, "c") for x in (ox, oy, oz)]),
+              "init_random_solenoidal")
+        return s.value
+
+
+__all__ = ["Ghost", "FFTPlan", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL"]

@@ -1,0 +1,232 @@
+/*
+ * ghost_b200.h -- C ABI of the B200 (sm_100a) pseudospectral HD library.
+ *
+ * Drop-in boundary for GHOST's 3D HD hot path.  Every entry point names the
+ * GHOST routine it replaces (paths relative to the GHOST tree, 3D/src/).
+ * The Fortran side binds these with ISO_C_BINDING (ghost_b200/fortran/
+ * ghost_gpu.f90); C and Python (ctypes) callers use them directly.
+ *
+ * Conventions
+ *  - Every function returns an int status (GHOST_OK == 0) and never exits
+ *    the process; ghost_last_error_string() describes the last failure on
+ *    the calling thread.
+ *  - Precision is fixed per context: GHOST_SINGLE (4) or GHOST_DOUBLE (8),
+ *    the KIND values of GHOST's GP (fftp-3/fprecision_mod.fpp:14-16).
+ *    "real" below means float or double accordingly; "complex" means two
+ *    interleaved reals (Fortran COMPLEX(KIND=GP) layout).
+ *  - Layouts are GHOST's, column-major:
+ *      spectral a(nz,ny,nx/2+1): offset k + nz*(j + ny*i), z fastest,
+ *               i = kx index 0..nx/2 (the Nyquist index carries kx=-nx/2
+ *               as in main3D.fpp:1746-1749);
+ *      real     r(nx,ny,nz):     offset i + nx*(j + ny*k), x fastest.
+ *  - Field pointers may be device memory (the fast path: no copies) or host
+ *    memory (pageable or pinned).  Host arrays are staged through the
+ *    context's device buffers and the call returns after the results are
+ *    back on the host, as GHOST's fftp-cu path does with every array
+ *    (fftp-cu/fftp3D.fpp:364-402).  Device-pointer calls are asynchronous
+ *    on the context's stream unless they return host scalars.
+ *  - Transforms are unnormalised both ways (c2r(r2c(x)) = nx*ny*nz * x).
+ *  - One context per host thread; calls on one context are not re-entrant.
+ */
+#ifndef GHOST_B200_H
+#define GHOST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GHOST_OK 0
+#define GHOST_ERR_ARG 1     /* bad argument: null pointer, dir/kin/o out of range */
+#define GHOST_ERR_SIZE 2    /* unsupported grid: each n must be a power of two in [16,2048] */
+#define GHOST_ERR_ALLOC 3   /* device allocation failed */
+#define GHOST_ERR_CUDA 4    /* CUDA runtime error (launch or execution) */
+#define GHOST_ERR_TIMEOUT 5 /* a bounded device-side wait gave up */
+#define GHOST_ERR_NAN 6     /* non-finite value detected by a checked call */
+#define GHOST_ERR_STATE 7   /* call not valid in the current state */
+#define GHOST_ERR_NODEV 8   /* no usable CUDA device */
+
+/* precision (GHOST's GP kind values) */
+#define GHOST_SINGLE 4
+#define GHOST_DOUBLE 8
+
+/* FFT directions, FFTW's values as used by fftp3d_create_plan
+ * (fftp-3/fftp3D.fpp:64-66) */
+#define GHOST_REAL_TO_COMPLEX (-1)
+#define GHOST_COMPLEX_TO_REAL (+1)
+
+typedef struct ghost_ctx ghost_ctx;
+typedef struct ghost_fftplan ghost_fftplan;
+
+/* Scalars of the grid, kes, ali and boxsize modules
+ * (pseudo/pseudospec3D_mod.fpp:13-21,53-72,112-120). */
+typedef struct {
+  int nx, ny, nz;
+  int precision;
+  int anis;      /* 1: anisotropic wavenumber normalisation (main3D.fpp:740-749) */
+  int nmax, nmaxperp;
+  double kmax, tiny;
+  double Lx, Ly, Lz, Dkx, Dky, Dkz, Dkk;
+  size_t spectral_elems; /* nz*ny*(nx/2+1) complex values per field */
+  size_t real_elems;     /* nx*ny*nz reals per field */
+} ghost_info;
+
+/* ---------------------------------------------------------------- */
+/* Context: replaces the module state set up in main3D.fpp:1721-1801
+ * (kmax, tiny, nmax, kx/ky/kz, kn2, kk2) and holds the device scratch,
+ * twiddle tables and stream.  arbsize != 0 is GHOST's ARBSIZE build
+ * (box Lx,Ly,Lz in units of 2*pi, main3D.fpp:881-909); arbsize == 0
+ * ignores Lx,Ly,Lz and uses the 2*pi-periodic cube. */
+int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, int arbsize,
+                     int precision, ghost_ctx **ctx);
+int ghost_ctx_destroy(ghost_ctx *ctx);
+int ghost_ctx_get_info(const ghost_ctx *ctx, ghost_info *info);
+/* Run all further work on this cudaStream_t (NULL: the legacy stream). */
+int ghost_ctx_set_stream(ghost_ctx *ctx, void *cuda_stream);
+/* Override the truncation wavenumber kmax, e.g. the EDQNM choice
+ * kmax = (n/2-0.5)^2 of main3D.fpp:1732-1734. */
+int ghost_ctx_set_kmax(ghost_ctx *ctx, double kmax);
+/* Block until the context's stream is idle; reports asynchronous errors. */
+int ghost_ctx_synchronize(ghost_ctx *ctx);
+/* Number of this library's kernels launched on the context so far. */
+int ghost_ctx_launch_count(const ghost_ctx *ctx, long long *count);
+const char *ghost_last_error_string(void);
+
+/* Per-kernel device timers, the role of FFTP's ffttime/tratime/comtime
+ * accumulators (fftp-cu/fftp_mod.fpp:39-45): when enabled, CUDA events are
+ * recorded on the context's stream around every launch, grouped by kernel
+ * kind (GHOST_TIMER_*).  Reading synchronises the stream, returns the
+ * accumulated milliseconds and launch counts per kind, and resets them. */
+#define GHOST_TIMER_Z_INV 0     /* fused inverse z pass (curl / gradient prologue) */
+#define GHOST_TIMER_Y_INV 1     /* inverse y pass */
+#define GHOST_TIMER_X_NL 2      /* fused x pass: c2r, real-space products, r2c */
+#define GHOST_TIMER_Y_FWD 3     /* forward y pass */
+#define GHOST_TIMER_Z_FWD 4     /* fused forward z pass (projection + RK update) */
+#define GHOST_TIMER_Z_C2C 5     /* plain z pass */
+#define GHOST_TIMER_X_C2R 6     /* plain complex-to-real x pass */
+#define GHOST_TIMER_X_R2C 7     /* plain real-to-complex x pass */
+#define GHOST_TIMER_POINTWISE 8 /* pointwise spectral operators */
+#define GHOST_TIMER_REDUCE 9    /* reductions and spectra */
+#define GHOST_TIMER_KINDS 10
+int ghost_ctx_enable_timers(ghost_ctx *ctx, int enable);
+int ghost_ctx_read_timers(ghost_ctx *ctx, double ms[GHOST_TIMER_KINDS], long long launches[GHOST_TIMER_KINDS]);
+
+/* ---------------------------------------------------------------- */
+/* FFTP: fftp-3/fftp3D.fpp and fftp-cu/fftp3D.fpp */
+
+/* fftp3d_create_plan(plan,n,fftdir,flags) (fftp-3/fftp3D.fpp:56-123).
+ * n must equal the context grid; flags is accepted and ignored. */
+int ghost_fftp3d_create_plan(ghost_ctx *ctx, const int n[3], int fftdir, int flags,
+                             ghost_fftplan **plan);
+/* fftp3d_destroy_plan(plan) (fftp-3/fftp3D.fpp:126-155) */
+int ghost_fftp3d_destroy_plan(ghost_fftplan *plan);
+/* fftp3d_real_to_complex(plan,in,out,comm) (fftp-3/fftp3D.fpp:204-315):
+ * in real(nx,ny,nz) -> out complex(nz,ny,nx/2+1), sign -1. */
+int ghost_fftp3d_real_to_complex(ghost_fftplan *plan, const void *in, void *out);
+/* fftp3d_complex_to_real(plan,in,out,comm) (fftp-3/fftp3D.fpp:318-431):
+ * in complex(nz,ny,nx/2+1) -> out real(nx,ny,nz), sign +1.  The input is
+ * left unmodified (GHOST overwrites it; callers rely on neither).  The
+ * imaginary parts of the kx=0 and kx=nx/2 planes are ignored after the z
+ * and y transforms, as a complex-to-real transform of Hermitian data does. */
+int ghost_fftp3d_complex_to_real(ghost_fftplan *plan, const void *in, void *out);
+
+/* ---------------------------------------------------------------- */
+/* Spectral operators: pseudo/pseudospec3D_hd.f90.  All fields complex
+ * (nz,ny,nx/2+1).  Outputs may alias inputs. */
+
+/* derivk3(a,b,dir) (:22-88): b = i k_dir a */
+int ghost_derivk3(ghost_ctx *ctx, const void *a, void *b, int dir);
+/* laplak3(a,b) (:91-121): b = -kk2 a */
+int ghost_laplak3(ghost_ctx *ctx, const void *a, void *b);
+/* rotor3(a,b,c,dir) (:124-200): c = curl component dir of the field whose
+ * other two components are a,b in right-hand order */
+int ghost_rotor3(ghost_ctx *ctx, const void *a, const void *b, void *c, int dir);
+/* prodre3(a,b,c,d,e,f) (:316-396): (d,e,f) = [curl(A) x A] in Fourier space
+ * (normalised by 1/(nx ny nz)^2 in real space, as GHOST does) */
+int ghost_prodre3(ghost_ctx *ctx, const void *a, const void *b, const void *c, void *d, void *e,
+                  void *f);
+/* nonlhd3(a,b,c,g,dir) (:399-509): g = -a_dir + k_dir (k.a)/kk2, the
+ * k_dir = 0 plane gets -a_dir */
+int ghost_nonlhd3(ghost_ctx *ctx, const void *a, const void *b, const void *c, void *g, int dir);
+/* energy(a,b,c,d,kin) (:512-662): kin 1 <|A|^2>, 0 <|curl A|^2>,
+ * 2 <|lap A|^2>; FP64 accumulation, deterministic */
+int ghost_energy(ghost_ctx *ctx, const void *a, const void *b, const void *c, double *d, int kin);
+/* helicity(a,b,c,d) (:665-784): <A . curl A> */
+int ghost_helicity(ghost_ctx *ctx, const void *a, const void *b, const void *c, double *d);
+/* cross(a,b,c,d,e,f,g,kin) (:787-907): kin 1 <A.B>, 0 <kk2 A.B> */
+int ghost_cross(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d,
+                const void *e, const void *f, double *g, int kin);
+/* divergence term of hdcheck(...,chk=1) (:1036-1070): <(div A)^2> */
+int ghost_divergence(ghost_ctx *ctx, const void *a, const void *b, const void *c, double *d);
+/* maxabs(a,b,c,d,kin) (:910-981): kin 0 max|curl A|, 1 max|lap A|,
+ * 2 max|A| in real space, divided by nx ny nz */
+int ghost_maxabs(ghost_ctx *ctx, const void *a, const void *b, const void *c, double *d, int kin);
+/* spectrumc(a,b,c,kin,hel,Ek,Hk) (:1190-1415): shell spectra on
+ * nmax/2+1 bins (host arrays); Ek skipped when kin == 2, Hk computed only
+ * when hel == 1 (Hk may then be NULL otherwise) */
+int ghost_spectrumc(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel,
+                    double *Ek, double *Hk);
+/* hdcheck(a,b,c,d,e,f,t,dt,hel,chk) (:984-1105) without the file output:
+ * out[0]=<|v|^2>, out[1]=<|w|^2>, out[2]=helicity (hel==1), out[3]=<v.f>,
+ * out[4]=<(div v)^2> (chk==1) */
+int ghost_hdcheck(ghost_ctx *ctx, const void *vx, const void *vy, const void *vz, const void *fx,
+                  const void *fy, const void *fz, int hel, int chk, double out[5]);
+/* normalize(fx,fy,fz,f0,kin) (pseudo/module_dns.f90:13-41) */
+int ghost_normalize(ghost_ctx *ctx, void *fx, void *fy, void *fz, double f0, int kin);
+/* sharp(a,b,delta) (pseudo/pseudospec3D_filt.f90:200-241) */
+int ghost_sharp(ghost_ctx *ctx, const void *a, void *b, double delta);
+
+/* ---------------------------------------------------------------- */
+/* Runge-Kutta fragments of the HD solver */
+
+/* hd_rkstep1 (include/hd_rkstep1.f90:4-6): C1..C3 = vx..vz */
+int ghost_hd_rkstep1(ghost_ctx *ctx, const void *vx, const void *vy, const void *vz, void *C1, void *C2,
+                     void *C3);
+/* hd_rkstep2 (include/hd_rkstep2.f90:3-32) for substep o:
+ * v = C + dt*(nu*lap v - P(w x v) + f)/o on tiny <= kn2 <= kmax, else 0.
+ * f may be NULL (no forcing). */
+int ghost_hd_rkstep2(ghost_ctx *ctx, int o, double dt, double nu, void *vx, void *vy, void *vz,
+                     const void *C1, const void *C2, const void *C3, const void *fx, const void *fy,
+                     const void *fz);
+/* nsteps steps of the loop main3D.fpp:3195-3231 (RK1 then DO o=ord,1,-1
+ * RK2), the copy of RK1 fused into the first substep.  C1..C3 are the
+ * RK storage (device, or NULL: context-owned).  f may be NULL. */
+int ghost_hd_run(ghost_ctx *ctx, int nsteps, int ord, double dt, double nu, void *vx, void *vy, void *vz,
+                 void *C1, void *C2, void *C3, const void *fx, const void *fy, const void *fz);
+
+/* ---------------------------------------------------------------- */
+/* Rotating stratified Boussinesq (ROTBOUSS solver) */
+
+/* advect3(a,b,c,d,e) (pseudo/pseudospec3D_phd.f90:23-114): e = -(A.grad)d */
+int ghost_advect3(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, void *e);
+/* rotbouss_rkstep2 (include/rotbouss_rkstep2.f90:12-83); xmom and xtemp
+ * already multiplied by bvfreq (main3D.fpp:973-974).  f, fs may be NULL. */
+int ghost_bouss_rkstep2(ghost_ctx *ctx, int o, double dt, double nu, double kappa, double omegaz,
+                        double xmom, double xtemp, void *vx, void *vy, void *vz, void *th,
+                        const void *C1, const void *C2, const void *C3, const void *C20,
+                        const void *fx, const void *fy, const void *fz, const void *fs);
+/* nsteps steps of rotbouss_rkstep1 (include/rotbouss_rkstep1.f90) + RK2 */
+int ghost_bouss_run(ghost_ctx *ctx, int nsteps, int ord, double dt, double nu, double kappa,
+                    double omegaz, double xmom, double xtemp, void *vx, void *vy, void *vz, void *th,
+                    const void *fx, const void *fy, const void *fz, const void *fs);
+
+/* ---------------------------------------------------------------- */
+/* Seeded initial conditions (host RNG, GHOST's randu of
+ * pseudo/pseudospec3D_mod.fpp:130-148) */
+
+/* Random-phase vector potential on kdn <= |k| <= kup with the loop order,
+ * seeding and Hermitian kx=0 plane of examples/initialfv.f90_random:16-134;
+ * shape 0: amplitude 1/|k| (GHOST's forcing); shape 1: exp(-|k|^2/4)
+ * (velocity with E(k) ~ k^4 exp(-2(k/2)^2)).  Then (out) = curl of it,
+ * normalised to <|out|^2> = amp^2 (initialfv.f90_random:136-139).
+ * *seed is updated as GHOST's seed variable is. */
+int ghost_init_random_solenoidal(ghost_ctx *ctx, int32_t *seed, double kdn, double kup, int shape,
+                                 double amp, void *ox, void *oy, void *oz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GHOST_B200_H */

@@ -1,0 +1,902 @@
+/*
+ * ghost_oracle.c -- CPU restatement of GHOST's 3D HD pseudospectral path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library
+ * under ghost_b200/: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load it.  Nothing in
+ * the product links it.
+ *
+ * Parity status: the reference (Fortran 90 + MPI + FFTW 3.x) cannot be
+ * compiled here (no Fortran compiler, no MPI, no FFTW) and ships no test
+ * vectors, so no reference-run outputs exist.  The restatement is pinned
+ * instead to
+ *   - the DFT definition (direct O(N^2) sums and scipy's pocketfft,
+ *     tests/test_oracle_fft.py), which is exactly what FFTW computes,
+ *   - the reference's own analytic initial conditions (ABC Beltrami flow of
+ *     examples/initialv.f90_abc decays as exp(-nu k^2 t) with zero
+ *     nonlinear term), the energy budget dE/dt = -2 nu Omega + eps of
+ *     3D/src/README:490-502, and div v = 0,
+ * and the reference's source is followed statement by statement below
+ * (file:line citations are relative to the GHOST tree, 3D/src/).
+ *
+ * Layouts are GHOST's (Fortran column-major, 0-based here):
+ *   spectral a(k,j,i): k = z index (fastest), j = y, i = kx index 0..nx/2
+ *                      offset k + nz*(j + ny*i)
+ *   real     r(i,j,k): i = x (fastest), j = y, k = z
+ *                      offset i + nx*(j + ny*k)
+ * Transforms are unnormalised both ways (fftp-3/fftp3D.fpp:204-431).
+ *
+ * Built twice: -DORACLE_FP32 gives GHOST's PRECISION=SINGLE build
+ * (fftp-3/fprecision_mod.fpp:14-16), otherwise PRECISION=DOUBLE.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifdef ORACLE_FP32
+typedef float real;
+#else
+typedef double real;
+#endif
+
+typedef struct { real re, im; } cplx;
+
+static inline cplx cadd(cplx a, cplx b) { cplx r = {a.re + b.re, a.im + b.im}; return r; }
+static inline cplx csub(cplx a, cplx b) { cplx r = {a.re - b.re, a.im - b.im}; return r; }
+static inline cplx cmul(cplx a, cplx b) {
+  cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+  return r;
+}
+static inline cplx cscal(real s, cplx a) { cplx r = {s * a.re, s * a.im}; return r; }
+static inline cplx cconj(cplx a) { cplx r = {a.re, -a.im}; return r; }
+/* im*s*a: the Fortran expression im*kx(i)*a(k,j,i) of derivk3 */
+static inline cplx cimul(real s, cplx a) {
+  cplx ims = {(real)0, s};
+  return cmul(ims, a);
+}
+static inline real cabs2(cplx a) { return a.re * a.re + a.im * a.im; }
+
+/* ------------------------------------------------------------------ */
+/* 1D complex FFT: iterative radix-2, twiddles evaluated in FP64 once and
+ * rounded to the working precision (the role FFTW plays for GHOST,
+ * fftp-3/fftp3D.fpp:92-107). */
+typedef struct {
+  int n, logn;
+  cplx *tw; /* exp(-2 pi i t / n), t < n/2 */
+  int *rev;
+} fft1_t;
+
+static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
+
+static int fft1_init(fft1_t *p, int n) {
+  p->n = n;
+  p->logn = ilog2(n);
+  if ((1 << p->logn) != n) return -1;
+  p->tw = (cplx *)malloc(sizeof(cplx) * (size_t)(n / 2 + 1));
+  p->rev = (int *)malloc(sizeof(int) * (size_t)n);
+  for (int t = 0; t <= n / 2; ++t) {
+    double a = -2.0 * 3.14159265358979323846 * (double)t / (double)n;
+    p->tw[t].re = (real)cos(a);
+    p->tw[t].im = (real)sin(a);
+  }
+  for (int t = 0; t < n; ++t) {
+    int r = 0;
+    for (int b = 0; b < p->logn; ++b) r |= ((t >> b) & 1) << (p->logn - 1 - b);
+    p->rev[t] = r;
+  }
+  return 0;
+}
+static void fft1_free(fft1_t *p) { free(p->tw); free(p->rev); }
+
+/* sign = -1 forward (FFTW_FORWARD), +1 backward; unnormalised */
+static void fft1(const fft1_t *p, cplx *x, int sign) {
+  int n = p->n;
+  for (int t = 0; t < n; ++t) {
+    int r = p->rev[t];
+    if (r > t) { cplx s = x[t]; x[t] = x[r]; x[r] = s; }
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    int half = len >> 1, step = n / len;
+    for (int b = 0; b < n; b += len) {
+      for (int j = 0; j < half; ++j) {
+        cplx w = p->tw[j * step];
+        if (sign > 0) w.im = -w.im;
+        cplx u = x[b + j], v = cmul(w, x[b + j + half]);
+        x[b + j] = cadd(u, v);
+        x[b + j + half] = csub(u, v);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Context: the grid, kes, ali and boxsize modules
+ * (pseudo/pseudospec3D_mod.fpp:13-21,53-72,112-120) set up as in
+ * main3D.fpp:1727-1801. */
+typedef struct {
+  int nx, ny, nz, nxh;
+  int anis, arbsize, nmax, nmaxperp;
+  real Lx, Ly, Lz, Dkx, Dky, Dkz, Dkk;
+  real kmax, tiny;
+  real *kx, *ky, *kz;
+  real *kn2, *kk2; /* (nz,ny,nxh) */
+  fft1_t fx, fy, fz;
+  size_t nspec, nreal;
+} octx;
+
+#define SIDX(c, k, j, i) ((size_t)(k) + (size_t)(c)->nz * ((size_t)(j) + (size_t)(c)->ny * (size_t)(i)))
+
+/* edqnm != 0 selects the EDQNM truncation kmax=(n/2-0.5)^2 of main3D.fpp:1732-1734 */
+octx *o_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz,
+                   int arbsize, int edqnm) {
+  octx *c = (octx *)calloc(1, sizeof(octx));
+  c->nx = nx; c->ny = ny; c->nz = nz; c->nxh = nx / 2 + 1;
+  c->arbsize = arbsize;
+  c->nspec = (size_t)nz * ny * c->nxh;
+  c->nreal = (size_t)nx * ny * nz;
+  /* main3D.fpp:881-909: default box 1,1,1 unless ARBSIZE */
+  if (arbsize) {
+    c->Lx = (real)Lx; c->Ly = (real)Ly; c->Lz = (real)Lz;
+    c->Dkx = (real)1 / c->Lx; c->Dky = (real)1 / c->Ly; c->Dkz = (real)1 / c->Lz;
+  } else {
+    c->Lx = c->Ly = c->Lz = 1; c->Dkx = c->Dky = c->Dkz = 1;
+  }
+  c->Dkk = c->Dkx < c->Dky ? c->Dkx : c->Dky;
+  if (c->Dkz < c->Dkk) c->Dkk = c->Dkz;
+  /* main3D.fpp:740-749 */
+  c->anis = arbsize ? 1 : ((nx != ny) || (ny != nz));
+  /* main3D.fpp:1727-1737 */
+  c->kmax = (real)1.0 / (real)9.0;
+  {
+    real m = (real)nx * c->Dkx;
+    if ((real)ny * c->Dky > m) m = (real)ny * c->Dky;
+    if ((real)nz * c->Dkz > m) m = (real)nz * c->Dkz;
+    c->nmax = (int)(m / c->Dkk);
+    real mp = (real)nx * c->Dkx;
+    if ((real)ny * c->Dky > mp) mp = (real)ny * c->Dky;
+    c->nmaxperp = (int)(mp / c->Dkk);
+  }
+  if (!arbsize && c->anis == 0) c->kmax = c->kmax * ((real)nx * (real)nx);
+  if (edqnm) c->kmax = ((real)nx / (real)2.0 - (real)0.5) * ((real)nx / (real)2.0 - (real)0.5);
+  {
+    real t = (real)0.1 / ((real)c->nmax * (real)c->nmax);
+    c->tiny = (real)1e-5 < t ? (real)1e-5 : t;
+  }
+  /* main3D.fpp:1746-1763 */
+  c->kx = (real *)malloc(sizeof(real) * nx);
+  c->ky = (real *)malloc(sizeof(real) * ny);
+  c->kz = (real *)malloc(sizeof(real) * nz);
+  for (int i = 0; i < nx / 2; ++i) { c->kx[i] = (real)i; c->kx[i + nx / 2] = (real)(i - nx / 2); }
+  for (int j = 0; j < ny / 2; ++j) { c->ky[j] = (real)j; c->ky[j + ny / 2] = (real)(j - ny / 2); }
+  for (int k = 0; k < nz / 2; ++k) { c->kz[k] = (real)k; c->kz[k + nz / 2] = (real)(k - nz / 2); }
+  if (nx == 1) c->kx[0] = 0;
+  if (ny == 1) c->ky[0] = 0;
+  if (nz == 1) c->kz[0] = 0;
+  real rmp = 1, rmq = 1, rms = 1;
+  if (c->anis) {
+    rmp = (real)1 / ((real)nx * (real)nx);
+    rmq = (real)1 / ((real)ny * (real)ny);
+    rms = (real)1 / ((real)nz * (real)nz);
+  }
+  c->kn2 = (real *)malloc(sizeof(real) * c->nspec);
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k)
+        c->kn2[SIDX(c, k, j, i)] = rmp * (c->kx[i] * c->kx[i]) + rmq * (c->ky[j] * c->ky[j]) +
+                                   rms * (c->kz[k] * c->kz[k]);
+  /* main3D.fpp:1785-1800 */
+  if (arbsize) {
+    for (int i = 0; i < nx; ++i) c->kx[i] *= c->Dkx;
+    for (int j = 0; j < ny; ++j) c->ky[j] *= c->Dky;
+    for (int k = 0; k < nz; ++k) c->kz[k] *= c->Dkz;
+  }
+  if (c->anis) {
+    c->kk2 = (real *)malloc(sizeof(real) * c->nspec);
+    for (int i = 0; i < c->nxh; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k)
+          c->kk2[SIDX(c, k, j, i)] = c->kx[i] * c->kx[i] + c->ky[j] * c->ky[j] + c->kz[k] * c->kz[k];
+  } else {
+    c->kk2 = c->kn2;
+  }
+  if (fft1_init(&c->fx, nx) || fft1_init(&c->fy, ny) || fft1_init(&c->fz, nz)) {
+    return NULL;
+  }
+  return c;
+}
+
+void o_ctx_destroy(octx *c) {
+  if (!c) return;
+  if (c->kk2 != c->kn2) free(c->kk2);
+  free(c->kn2); free(c->kx); free(c->ky); free(c->kz);
+  fft1_free(&c->fx); fft1_free(&c->fy); fft1_free(&c->fz);
+  free(c);
+}
+
+/* accessors for the Python wrapper */
+void o_ctx_info(const octx *c, double *out) {
+  out[0] = c->kmax; out[1] = c->tiny; out[2] = c->Dkk; out[3] = c->nmax;
+  out[4] = c->anis; out[5] = c->nmaxperp; out[6] = c->Dkx; out[7] = c->Dky; out[8] = c->Dkz;
+}
+void o_ctx_tables(const octx *c, real *kx, real *ky, real *kz, real *kn2, real *kk2) {
+  memcpy(kx, c->kx, sizeof(real) * c->nx);
+  memcpy(ky, c->ky, sizeof(real) * c->ny);
+  memcpy(kz, c->kz, sizeof(real) * c->nz);
+  memcpy(kn2, c->kn2, sizeof(real) * c->nspec);
+  memcpy(kk2, c->kk2, sizeof(real) * c->nspec);
+}
+int o_nthreads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+void o_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+/* ------------------------------------------------------------------ */
+/* fftp3d_real_to_complex (fftp-3/fftp3D.fpp:204-315):
+ *   2D r2c over (x,y) for each z plane -> carr(nx/2+1,ny,nz)
+ *   transpose -> out(nz,ny,nx/2+1)
+ *   1D c2c along z, direction -1. */
+void o_fftp3d_real_to_complex(const octx *c, const real *in, cplx *out) {
+  int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
+  cplx *carr = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  /* r2c along x: a full complex transform of (x_n + 0i), first nx/2+1 kept */
+#pragma omp parallel
+  {
+    cplx *buf = (cplx *)malloc(sizeof(cplx) * (size_t)(nx > ny ? nx : ny));
+#pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j) {
+        const real *row = in + (size_t)nx * ((size_t)j + (size_t)ny * k);
+        for (int i = 0; i < nx; ++i) { buf[i].re = row[i]; buf[i].im = 0; }
+        fft1(&c->fx, buf, -1);
+        cplx *dst = carr + (size_t)nxh * ((size_t)j + (size_t)ny * k);
+        for (int i = 0; i < nxh; ++i) dst[i] = buf[i];
+      }
+    /* c2c along y */
+#pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k)
+      for (int i = 0; i < nxh; ++i) {
+        cplx *base = carr + (size_t)i + (size_t)nxh * (size_t)ny * k;
+        for (int j = 0; j < ny; ++j) buf[j] = base[(size_t)nxh * j];
+        fft1(&c->fy, buf, -1);
+        for (int j = 0; j < ny; ++j) base[(size_t)nxh * j] = buf[j];
+      }
+    free(buf);
+  }
+  /* transpose (fftp3D.fpp:282-298) out(k,j,i) = c1(i,j,k) */
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < nxh; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k)
+        out[SIDX(c, k, j, i)] = carr[(size_t)i + (size_t)nxh * ((size_t)j + (size_t)ny * k)];
+  /* c2c along z (contiguous) */
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < nxh; ++i)
+    for (int j = 0; j < ny; ++j) fft1(&c->fz, out + SIDX(c, 0, j, i), -1);
+  free(carr);
+}
+
+/* fftp3d_complex_to_real (fftp-3/fftp3D.fpp:318-431).  The input is left
+ * untouched here (GHOST destroys it; callers never rely on its content).
+ * The final c2r along x takes only the real parts of the kx=0 and kx=nx/2
+ * coefficients, as a complex-to-real transform of a Hermitian line does. */
+void o_fftp3d_complex_to_real(const octx *c, const cplx *in, real *out) {
+  int nx = c->nx, ny = c->ny, nz = c->nz, nxh = c->nxh;
+  cplx *tmp = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *carr = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  memcpy(tmp, in, sizeof(cplx) * c->nspec);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < nxh; ++i)
+    for (int j = 0; j < ny; ++j) fft1(&c->fz, tmp + SIDX(c, 0, j, i), +1);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nxh; ++i)
+        carr[(size_t)i + (size_t)nxh * ((size_t)j + (size_t)ny * k)] = tmp[SIDX(c, k, j, i)];
+#pragma omp parallel
+  {
+    cplx *buf = (cplx *)malloc(sizeof(cplx) * (size_t)(nx > ny ? nx : ny));
+#pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k)
+      for (int i = 0; i < nxh; ++i) {
+        cplx *base = carr + (size_t)i + (size_t)nxh * (size_t)ny * k;
+        for (int j = 0; j < ny; ++j) buf[j] = base[(size_t)nxh * j];
+        fft1(&c->fy, buf, +1);
+        for (int j = 0; j < ny; ++j) base[(size_t)nxh * j] = buf[j];
+      }
+#pragma omp for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j) {
+        const cplx *src = carr + (size_t)nxh * ((size_t)j + (size_t)ny * k);
+        if (nx == 1) {
+          out[(size_t)nx * ((size_t)j + (size_t)ny * k)] = src[0].re;
+          continue;
+        }
+        buf[0].re = src[0].re; buf[0].im = 0;
+        buf[nx / 2].re = src[nx / 2].re; buf[nx / 2].im = 0;
+        for (int i = 1; i < nx / 2; ++i) { buf[i] = src[i]; buf[nx - i] = cconj(src[i]); }
+        fft1(&c->fx, buf, +1);
+        real *row = out + (size_t)nx * ((size_t)j + (size_t)ny * k);
+        for (int i = 0; i < nx; ++i) row[i] = buf[i].re;
+      }
+    free(buf);
+  }
+  free(tmp);
+  free(carr);
+}
+
+/* ------------------------------------------------------------------ */
+/* pseudo/pseudospec3D_hd.f90 */
+
+/* derivk3 (pseudospec3D_hd.f90:22-88): b = i k_dir a */
+void o_derivk3(const octx *c, const cplx *a, cplx *b, int dir) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        real kd = dir == 1 ? c->kx[i] : (dir == 2 ? c->ky[j] : c->kz[k]);
+        b[p] = cimul(kd, a[p]);
+      }
+}
+
+/* laplak3 (pseudospec3D_hd.f90:91-121): b = -kk2 a */
+void o_laplak3(const octx *c, const cplx *a, cplx *b) {
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < c->nspec; ++p) b[p] = cscal(-c->kk2[p], a[p]);
+}
+
+/* rotor3 (pseudospec3D_hd.f90:124-200) */
+void o_rotor3(const octx *c, const cplx *a, const cplx *b, cplx *out, int dir) {
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  if (dir == 1) {
+    o_derivk3(c, a, c1, 3); o_derivk3(c, b, c2, 2);
+  } else if (dir == 2) {
+    o_derivk3(c, a, c1, 3); o_derivk3(c, b, c2, 1);
+  } else {
+    o_derivk3(c, a, c1, 2); o_derivk3(c, b, c2, 1);
+  }
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < c->nspec; ++p)
+    out[p] = (dir == 2) ? csub(c1[p], c2[p]) : csub(c2[p], c1[p]);
+  free(c1);
+  free(c2);
+}
+
+/* prodre3 (pseudospec3D_hd.f90:316-396): [curl(A) x A] in Fourier space */
+void o_prodre3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, cplx *d, cplx *e, cplx *f) {
+  size_t nr = c->nreal;
+  real *r[8];
+  for (int q = 1; q <= 7; ++q) r[q] = (real *)malloc(sizeof(real) * nr);
+  cplx *t1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  o_rotor3(c, b, cc, t1, 1); o_fftp3d_complex_to_real(c, t1, r[1]);
+  o_rotor3(c, a, cc, t1, 2); o_fftp3d_complex_to_real(c, t1, r[2]);
+  o_rotor3(c, a, b, t1, 3);  o_fftp3d_complex_to_real(c, t1, r[3]);
+  o_fftp3d_complex_to_real(c, a, r[4]);
+  o_fftp3d_complex_to_real(c, b, r[5]);
+  o_fftp3d_complex_to_real(c, cc, r[6]);
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < nr; ++p) {
+    real r1 = r[1][p], r2 = r[2][p], r3 = r[3][p], r4 = r[4][p], r5 = r[5][p], r6 = r[6][p];
+    r[7][p] = (r2 * r6 - r5 * r3) * tmp;
+    r[3][p] = (r3 * r4 - r6 * r1) * tmp;
+    r[1][p] = (r1 * r5 - r4 * r2) * tmp;
+  }
+  o_fftp3d_real_to_complex(c, r[7], d);
+  o_fftp3d_real_to_complex(c, r[3], e);
+  o_fftp3d_real_to_complex(c, r[1], f);
+  for (int q = 1; q <= 7; ++q) free(r[q]);
+  free(t1);
+}
+
+/* nonlhd3 (pseudospec3D_hd.f90:399-509): g = -a_dir + k_dir (k.a)/k^2,
+ * with the k_dir = 0 plane set to -a_dir.  g may alias a, b or c. */
+void o_nonlhd3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, cplx *g, int dir) {
+  cplx *tmp = (cplx *)malloc(sizeof(cplx) * c->nspec);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        cplx self = dir == 1 ? a[p] : (dir == 2 ? b[p] : cc[p]);
+        int zero_plane = dir == 1 ? (i == 0) : (dir == 2 ? (j == 0) : (k == 0));
+        if (zero_plane) {
+          tmp[p].re = -self.re; tmp[p].im = -self.im;
+        } else {
+          real kd = dir == 1 ? c->kx[i] : (dir == 2 ? c->ky[j] : c->kz[k]);
+          cplx s = cadd(cadd(cscal(c->kx[i], a[p]), cscal(c->ky[j], b[p])), cscal(c->kz[k], cc[p]));
+          cplx q = cscal(kd, s);
+          q.re = q.re / c->kk2[p];
+          q.im = q.im / c->kk2[p];
+          cplx ms = {-self.re, -self.im};
+          tmp[p] = cadd(ms, q);
+        }
+      }
+  memcpy(g, tmp, sizeof(cplx) * c->nspec);
+  free(tmp);
+}
+
+/* energy (pseudospec3D_hd.f90:512-662); kin: 1 field, 0 curl, 2 Laplacian */
+double o_energy(const octx *c, const cplx *a, const cplx *b, const cplx *cc, int kin) {
+  const cplx *x = a, *y = b, *z = cc;
+  cplx *c1 = NULL, *c2 = NULL, *c3 = NULL;
+  if (kin != 1) {
+    c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    if (kin == 0) {
+      o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+    } else {
+      o_laplak3(c, a, c1); o_laplak3(c, b, c2); o_laplak3(c, cc, c3);
+    }
+    x = c1; y = c2; z = c3;
+  }
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  double dloc = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    double w = i == 0 ? 1.0 : 2.0;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        real s = (cabs2(x[p]) + cabs2(y[p]) + cabs2(z[p])) * tmp;
+        dloc += w * (double)s;
+      }
+  }
+  free(c1); free(c2); free(c3);
+  return dloc;
+}
+
+/* helicity (pseudospec3D_hd.f90:665-784) */
+double o_helicity(const octx *c, const cplx *a, const cplx *b, const cplx *cc) {
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  double dloc = 0.0;
+  const cplx *comp[3] = {a, b, cc};
+  for (int d = 1; d <= 3; ++d) {
+    if (d == 1) o_rotor3(c, b, cc, c1, 1);
+    else if (d == 2) o_rotor3(c, a, cc, c1, 2);
+    else o_rotor3(c, a, b, c1, 3);
+    for (int i = 0; i < c->nxh; ++i) {
+      double w = i == 0 ? 1.0 : 2.0;
+      for (int j = 0; j < c->ny; ++j)
+        for (int k = 0; k < c->nz; ++k) {
+          size_t p = SIDX(c, k, j, i);
+          real s = cmul(comp[d - 1][p], cconj(c1[p])).re * tmp;
+          dloc += w * (double)s;
+        }
+    }
+  }
+  free(c1);
+  return dloc;
+}
+
+/* cross (pseudospec3D_hd.f90:787-907); kin 1: <A.B>, 0: weighted by kk2 */
+double o_cross(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d,
+               const cplx *e, const cplx *f, int kin) {
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  double g = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    double w = i == 0 ? 1.0 : 2.0;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        real s = cadd(cadd(cmul(a[p], cconj(d[p])), cmul(b[p], cconj(e[p]))), cmul(cc[p], cconj(f[p]))).re;
+        if (kin == 1) s = s * tmp;
+        else s = s * c->kk2[p] * tmp;
+        g += w * (double)s;
+      }
+  }
+  return g;
+}
+
+/* divergence check of hdcheck (pseudospec3D_hd.f90:1036-1070) */
+double o_divergence(const octx *c, const cplx *a, const cplx *b, const cplx *cc) {
+  real tmq = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  double t = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    double w = i == 0 ? 1.0 : 2.0;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        cplx s = cadd(cadd(cimul(c->kx[i], a[p]), cimul(c->ky[j], b[p])), cimul(c->kz[k], cc[p]));
+        t += w * (double)(cabs2(s) * tmq);
+      }
+  }
+  return t;
+}
+
+/* maxabs (pseudospec3D_hd.f90:910-981); kin 0 curl, 1 Laplacian, 2 field */
+double o_maxabs(const octx *c, const cplx *a, const cplx *b, const cplx *cc, int kin) {
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  if (kin == 0) {
+    o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+  } else if (kin == 1) {
+    o_laplak3(c, a, c1); o_laplak3(c, b, c2); o_laplak3(c, cc, c3);
+  } else {
+    memcpy(c1, a, sizeof(cplx) * c->nspec); memcpy(c2, b, sizeof(cplx) * c->nspec);
+    memcpy(c3, cc, sizeof(cplx) * c->nspec);
+  }
+  real *r1 = (real *)malloc(sizeof(real) * c->nreal);
+  real *r2 = (real *)malloc(sizeof(real) * c->nreal);
+  real *r3 = (real *)malloc(sizeof(real) * c->nreal);
+  o_fftp3d_complex_to_real(c, c1, r1);
+  o_fftp3d_complex_to_real(c, c2, r2);
+  o_fftp3d_complex_to_real(c, c3, r3);
+  real d = 0;
+  for (size_t p = 0; p < c->nreal; ++p) {
+    real s = (real)sqrt(r1[p] * r1[p] + r2[p] * r2[p] + r3[p] * r3[p]);
+    if (s > d) d = s;
+  }
+  d = d / ((real)c->nx * (real)c->ny * (real)c->nz);
+  free(c1); free(c2); free(c3); free(r1); free(r2); free(r3);
+  return (double)d;
+}
+
+/* spectrumc (pseudospec3D_hd.f90:1190-1415).  Ek, Hk have nmax/2+1 bins.
+ * kin: 1 kinetic, 0 curl, 2 skip; hel: 1 helicity spectrum. */
+void o_spectrumc(const octx *c, const cplx *a, const cplx *b, const cplx *cc, int kin, int hel,
+                 double *Ek, double *Hk) {
+  int nb = c->nmax / 2 + 1;
+  cplx *c1 = NULL, *c2 = NULL, *c3 = NULL;
+  if (kin == 0 || hel == 1) {
+    c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+  }
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  if (kin <= 1) {
+    for (int q = 0; q < nb; ++q) Ek[q] = 0.0;
+    const cplx *x = kin == 1 ? a : c1, *y = kin == 1 ? b : c2, *z = kin == 1 ? cc : c3;
+    for (int i = 0; i < c->nxh; ++i) {
+      real w = i == 0 ? (real)1 : (real)2;
+      for (int j = 0; j < c->ny; ++j)
+        for (int k = 0; k < c->nz; ++k) {
+          size_t p = SIDX(c, k, j, i);
+          int kmn = (int)((real)sqrt(c->kk2[p]) / c->Dkk + (real)0.501f);
+          if (kmn > 0 && kmn <= nb) {
+            double tmq = (double)(w * (cabs2(x[p]) + cabs2(y[p]) + cabs2(z[p])) * tmp);
+            Ek[kmn - 1] += tmq;
+          }
+        }
+    }
+  }
+  if (hel == 1) {
+    for (int q = 0; q < nb; ++q) Hk[q] = 0.0;
+    for (int i = 0; i < c->nxh; ++i) {
+      real w = i == 0 ? (real)1 : (real)2;
+      for (int j = 0; j < c->ny; ++j)
+        for (int k = 0; k < c->nz; ++k) {
+          size_t p = SIDX(c, k, j, i);
+          int kmn = (int)((real)sqrt(c->kk2[p]) / c->Dkk + (real)0.501f);
+          if (kmn > 0 && kmn <= nb) {
+            real s = cmul(a[p], cconj(c1[p])).re + cmul(b[p], cconj(c2[p])).re + cmul(cc[p], cconj(c3[p])).re;
+            double tmq = (double)(w * s * tmp);
+            Hk[kmn - 1] += tmq;
+          }
+        }
+    }
+  }
+  free(c1); free(c2); free(c3);
+}
+
+/* ------------------------------------------------------------------ */
+/* Random numbers: randu of pseudo/pseudospec3D_mod.fpp:130-148.  am is the
+ * default-REAL constant 1./im, which is 2^-31 in both precisions. */
+real o_randu(int32_t *idum) {
+  const int32_t iq = 127773, ir = 2836, mask = 123459876, ia = 16807, im = 2147483647;
+  const real am = (real)(1.0f / (float)im);
+  int32_t k;
+  *idum = *idum ^ mask;
+  k = *idum / iq;
+  *idum = ia * (*idum - k * iq) - ir * k;
+  if (*idum < 0) *idum = *idum + im;
+  real r = am * (real)(*idum);
+  r = (r - (real)0.5) * (real)2;
+  *idum = *idum ^ mask;
+  return r;
+}
+
+/* radial amplitude of the random vector potential:
+ *   shape 0: 1/|k|            (examples/initialfv.f90_random:23)
+ *   shape 1: exp(-|k|^2/4)    gives E(k) ~ k^4 exp(-2 (k/2)^2) after the curl */
+static real amp_of(int shape, real kk2v) {
+  if (shape == 0) return (real)1.0 / (real)sqrt(kk2v);
+  return (real)exp(-(double)kk2v / 4.0);
+}
+
+static inline cplx phasor(real phase, real dump) {
+  cplx r = {(real)cos(phase) * dump, (real)sin(phase) * dump};
+  return r;
+}
+
+/* Random-phase vector potential on kdn <= |k| <= kup, with the loop order,
+ * seeding and Hermitian kx=0 plane of examples/initialfv.f90_random:16-134.
+ * Returns the updated seed. */
+int32_t o_random_vpot(const octx *c, int32_t seed, double kdn_d, double kup_d, int shape, cplx *C1, cplx *C2,
+                      cplx *C3) {
+  int ny = c->ny, nz = c->nz;
+  real kdn = (real)kdn_d, kup = (real)kup_d;
+  const real pi = (real)3.14159265358979323846;
+  cplx zero = {0, 0};
+  cplx *Cs[3] = {C1, C2, C3};
+#define INSHELL(p) ((c->kk2[p] <= kup * kup) && (c->kk2[p] >= kdn * kdn))
+  /* kx = 0 plane */
+  for (int q = 0; q < 3; ++q) Cs[q][SIDX(c, 0, 0, 0)] = zero;
+  for (int j = 1; j <= ny / 2; ++j) {
+    size_t p = SIDX(c, 0, j, 0), pc = SIDX(c, 0, ny - j, 0);
+    if (INSHELL(p)) {
+      real dump = amp_of(shape, c->kk2[p]);
+      for (int q = 0; q < 3; ++q) {
+        real phase = 2 * pi * o_randu(&seed);
+        Cs[q][p] = phasor(phase, dump);
+        Cs[q][pc] = cconj(Cs[q][p]);
+      }
+    } else {
+      for (int q = 0; q < 3; ++q) { Cs[q][p] = zero; Cs[q][pc] = zero; }
+    }
+  }
+  for (int k = 1; k <= nz / 2; ++k) {
+    size_t p = SIDX(c, k, 0, 0), pc = SIDX(c, nz - k, 0, 0);
+    if (INSHELL(p)) {
+      real dump = amp_of(shape, c->kk2[p]);
+      for (int q = 0; q < 3; ++q) {
+        real phase = 2 * pi * o_randu(&seed);
+        Cs[q][p] = phasor(phase, dump);
+        Cs[q][pc] = cconj(Cs[q][p]);
+      }
+    } else {
+      for (int q = 0; q < 3; ++q) { Cs[q][p] = zero; Cs[q][pc] = zero; }
+    }
+  }
+  for (int j = 1; j < ny; ++j)
+    for (int k = 1; k <= nz / 2; ++k) {
+      size_t p = SIDX(c, k, j, 0), pc = SIDX(c, nz - k, ny - j, 0);
+      if (INSHELL(p)) {
+        real dump = amp_of(shape, c->kk2[p]);
+        for (int q = 0; q < 3; ++q) {
+          real phase = 2 * pi * o_randu(&seed);
+          Cs[q][p] = phasor(phase, dump);
+          Cs[q][pc] = cconj(Cs[q][p]);
+        }
+      } else {
+        for (int q = 0; q < 3; ++q) { Cs[q][p] = zero; Cs[q][pc] = zero; }
+      }
+    }
+  for (int i = 1; i < c->nxh; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        if (INSHELL(p)) {
+          real dump = amp_of(shape, c->kk2[p]);
+          for (int q = 0; q < 3; ++q) {
+            real phase = 2 * pi * o_randu(&seed);
+            cplx v = phasor(phase, dump);
+            Cs[q][p] = cscal((real)2, v);
+          }
+        } else {
+          for (int q = 0; q < 3; ++q) Cs[q][p] = zero;
+        }
+      }
+#undef INSHELL
+  return seed;
+}
+
+/* normalize (pseudo/module_dns.f90:13-41) */
+void o_normalize(const octx *c, cplx *fx, cplx *fy, cplx *fz, double f0, int kin) {
+  double tmp = o_energy(c, fx, fy, fz, kin);
+  double s = sqrt(tmp);
+  for (size_t p = 0; p < c->nspec; ++p) {
+    fx[p].re = (real)((double)(fx[p].re * (real)f0) / s); fx[p].im = (real)((double)(fx[p].im * (real)f0) / s);
+    fy[p].re = (real)((double)(fy[p].re * (real)f0) / s); fy[p].im = (real)((double)(fy[p].im * (real)f0) / s);
+    fz[p].re = (real)((double)(fz[p].re * (real)f0) / s); fz[p].im = (real)((double)(fz[p].im * (real)f0) / s);
+  }
+}
+
+/* A solenoidal field = curl of the random vector potential, normalised
+ * so that <|v|^2> = amp^2 (examples/initialfv.f90_random:136-139). */
+int32_t o_random_solenoidal(const octx *c, int32_t seed, double kdn, double kup, int shape, double amp, cplx *vx,
+                            cplx *vy, cplx *vz) {
+  size_t n = c->nspec;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n);
+  seed = o_random_vpot(c, seed, kdn, kup, shape, C1, C2, C3);
+  o_rotor3(c, C2, C3, vx, 1);
+  o_rotor3(c, C1, C3, vy, 2);
+  o_rotor3(c, C1, C2, vz, 3);
+  o_normalize(c, vx, vy, vz, amp, 1);
+  free(C1); free(C2); free(C3);
+  return seed;
+}
+
+/* ABC flow of examples/initialv.f90_abc:25-54 (before normalize) */
+void o_abc(const octx *c, double kdn, double kup, double A, double B, double C, real *R1, real *R2, real *R3) {
+  const real pi = (real)3.14159265358979323846;
+  int nx = c->nx, ny = c->ny, nz = c->nz;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        size_t p = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+        real r1 = 0, r2 = 0, r3 = 0;
+        for (int ki = (int)kdn; ki <= (int)kup; ++ki) {
+          real kk = (real)(ki * ki);
+          r1 += ((real)B * (real)cos(2 * pi * ki * (real)j / (real)ny) +
+                 (real)C * (real)sin(2 * pi * ki * (real)k / (real)nz)) / kk;
+          r2 += ((real)A * (real)sin(2 * pi * ki * (real)i / (real)nx) +
+                 (real)C * (real)cos(2 * pi * ki * (real)k / (real)nz)) / kk;
+          r3 += ((real)A * (real)cos(2 * pi * ki * (real)i / (real)nx) +
+                 (real)B * (real)sin(2 * pi * ki * (real)j / (real)ny)) / kk;
+        }
+        R1[p] = r1; R2[p] = r2; R3[p] = r3;
+      }
+}
+
+/* ------------------------------------------------------------------ */
+/* RK: hd_rkstep1 (include/hd_rkstep1.f90:4-6) and hd_rkstep2
+ * (include/hd_rkstep2.f90:3-32) under the DO o = ord,1,-1 loop of
+ * main3D.fpp:3229-3231. */
+void o_hd_rkstep1(const octx *c, const cplx *vx, const cplx *vy, const cplx *vz, cplx *C1, cplx *C2, cplx *C3) {
+  memcpy(C1, vx, sizeof(cplx) * c->nspec);
+  memcpy(C2, vy, sizeof(cplx) * c->nspec);
+  memcpy(C3, vz, sizeof(cplx) * c->nspec);
+}
+
+void o_hd_rkstep2(const octx *c, int o, double dt_d, double nu_d, cplx *vx, cplx *vy, cplx *vz, const cplx *C1,
+                  const cplx *C2, const cplx *C3, const cplx *fx, const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d;
+  cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
+       *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
+       *C8 = (cplx *)malloc(sizeof(cplx) * n);
+  o_prodre3(c, vx, vy, vz, C4, C5, C6);
+  o_nonlhd3(c, C4, C5, C6, C7, 1);
+  o_nonlhd3(c, C4, C5, C6, C8, 2);
+  o_nonlhd3(c, C4, C5, C6, C4, 3);
+  o_laplak3(c, vx, vx);
+  o_laplak3(c, vy, vy);
+  o_laplak3(c, vz, vz);
+  real rmp = (real)1 / (real)o;
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < n; ++p) {
+    if (c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny) {
+      vx[p] = cadd(C1[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vx[p]), C7[p]), fx[p]))));
+      vy[p] = cadd(C2[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vy[p]), C8[p]), fy[p]))));
+      vz[p] = cadd(C3[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vz[p]), C4[p]), fz[p]))));
+    } else {
+      cplx z = {0, 0};
+      vx[p] = z; vy[p] = z; vz[p] = z;
+    }
+  }
+  free(C4); free(C5); free(C6); free(C7); free(C8);
+}
+
+/* nsteps full RK steps of the HD solver (f may be NULL: no forcing) */
+void o_hd_run(const octx *c, int nsteps, int ord, double dt, double nu, cplx *vx, cplx *vy, cplx *vz,
+              const cplx *fx, const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n);
+  cplx *zf = NULL;
+  if (!fx) {
+    zf = (cplx *)calloc(n, sizeof(cplx));
+    fx = fy = fz = zf;
+  }
+  for (int t = 0; t < nsteps; ++t) {
+    o_hd_rkstep1(c, vx, vy, vz, C1, C2, C3);
+    for (int o = ord; o >= 1; --o) o_hd_rkstep2(c, o, dt, nu, vx, vy, vz, C1, C2, C3, fx, fy, fz);
+  }
+  free(C1); free(C2); free(C3); free(zf);
+}
+
+/* ------------------------------------------------------------------ */
+/* Boussinesq: advect3 (pseudo/pseudospec3D_phd.f90:23-114) gives
+ * e = -(A.grad)B in Fourier space. */
+void o_advect3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d, cplx *e) {
+  size_t nr = c->nreal;
+  real *r1 = (real *)malloc(sizeof(real) * nr), *r2 = (real *)malloc(sizeof(real) * nr),
+       *r3 = (real *)malloc(sizeof(real) * nr);
+  cplx *c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  const cplx *comp[3] = {a, b, cc};
+  for (int dir = 1; dir <= 3; ++dir) {
+    o_derivk3(c, d, c2, dir);
+    o_fftp3d_complex_to_real(c, comp[dir - 1], r1);
+    o_fftp3d_complex_to_real(c, c2, r2);
+    if (dir == 1) {
+      for (size_t p = 0; p < nr; ++p) r3[p] = r1[p] * r2[p];
+    } else if (dir == 2) {
+      for (size_t p = 0; p < nr; ++p) r3[p] = r3[p] + r1[p] * r2[p];
+    } else {
+      real tmp = -(real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+      for (size_t p = 0; p < nr; ++p) r3[p] = (r3[p] + r1[p] * r2[p]) * tmp;
+    }
+  }
+  o_fftp3d_real_to_complex(c, r3, e);
+  free(r1); free(r2); free(r3); free(c2);
+}
+
+/* rotbouss_rkstep2 (include/rotbouss_rkstep2.f90:12-83); xmom and xtemp
+ * are already multiplied by bvfreq (main3D.fpp:973-974). */
+void o_bouss_rkstep2(const octx *c, int o, double dt_d, double nu_d, double kappa_d, double omegaz_d,
+                     double xmom_d, double xtemp_d, cplx *vx, cplx *vy, cplx *vz, cplx *th, const cplx *C1,
+                     const cplx *C2, const cplx *C3, const cplx *C20, const cplx *fx, const cplx *fy,
+                     const cplx *fz, const cplx *fs) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d, kappa = (real)kappa_d, omegaz = (real)omegaz_d;
+  real xmom = (real)xmom_d, xtemp = (real)xtemp_d;
+  cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
+       *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
+       *C8 = (cplx *)malloc(sizeof(cplx) * n);
+  o_prodre3(c, vx, vy, vz, C4, C5, C6);
+  for (size_t p = 0; p < n; ++p) {
+    C4[p] = csub(C4[p], cscal(2 * omegaz, vy[p]));
+    C5[p] = cadd(C5[p], cscal(2 * omegaz, vx[p]));
+    C6[p] = cadd(C6[p], cscal(xmom, th[p]));
+  }
+  o_nonlhd3(c, C4, C5, C6, C7, 1);
+  o_nonlhd3(c, C4, C5, C6, C8, 2);
+  o_nonlhd3(c, C4, C5, C6, C4, 3);
+  o_advect3(c, vx, vy, vz, th, C5);
+  for (size_t p = 0; p < n; ++p) C5[p] = cadd(C5[p], cscal(xtemp, vz[p]));
+  o_laplak3(c, vx, vx);
+  o_laplak3(c, vy, vy);
+  o_laplak3(c, vz, vz);
+  o_laplak3(c, th, th);
+  real rmp = (real)1 / (real)o;
+  cplx z = {0, 0};
+  for (size_t p = 0; p < n; ++p) {
+    if (c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny) {
+      vx[p] = cadd(C1[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vx[p]), C7[p]), fx[p]))));
+      vy[p] = cadd(C2[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vy[p]), C8[p]), fy[p]))));
+      vz[p] = cadd(C3[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vz[p]), C4[p]), fz[p]))));
+      th[p] = cadd(C20[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(kappa, th[p]), C5[p]), fs[p]))));
+    } else if (c->kn2[p] > c->kmax) {
+      vx[p] = z; vy[p] = z; vz[p] = z; th[p] = z;
+    } else if (c->kn2[p] < c->tiny) {
+      vx[p] = z; vy[p] = z; vz[p] = z; th[p] = C20[p];
+    }
+  }
+  free(C4); free(C5); free(C6); free(C7); free(C8);
+}
+
+void o_bouss_run(const octx *c, int nsteps, int ord, double dt, double nu, double kappa, double omegaz,
+                 double xmom, double xtemp, cplx *vx, cplx *vy, cplx *vz, cplx *th, const cplx *fx,
+                 const cplx *fy, const cplx *fz, const cplx *fs) {
+  size_t n = c->nspec;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n), *C20 = (cplx *)malloc(sizeof(cplx) * n);
+  cplx *zf = (cplx *)calloc(n, sizeof(cplx));
+  if (!fx) fx = fy = fz = zf;
+  if (!fs) fs = zf;
+  for (int t = 0; t < nsteps; ++t) {
+    memcpy(C1, vx, sizeof(cplx) * n); memcpy(C2, vy, sizeof(cplx) * n);
+    memcpy(C3, vz, sizeof(cplx) * n); memcpy(C20, th, sizeof(cplx) * n);
+    for (int o = ord; o >= 1; --o)
+      o_bouss_rkstep2(c, o, dt, nu, kappa, omegaz, xmom, xtemp, vx, vy, vz, th, C1, C2, C3, C20, fx, fy, fz, fs);
+  }
+  free(C1); free(C2); free(C3); free(C20); free(zf);
+}
+
+/* sharp (pseudo/pseudospec3D_filt.f90:200-241): keep kn2 <= (pi/delta)^2 */
+void o_sharp(const octx *c, const cplx *a, cplx *b, double delta) {
+  const real pi = (real)3.14159265358979323846;
+  real tmp = (pi / (real)delta) * (pi / (real)delta);
+  cplx z = {0, 0};
+  for (size_t p = 0; p < c->nspec; ++p) b[p] = c->kn2[p] <= tmp ? a[p] : z;
+}

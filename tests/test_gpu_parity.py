@@ -1,0 +1,317 @@
+"""Parity of the CUDA library (through the C ABI) with the CPU oracle on the
+same seeded inputs: transforms, spectral operators, reductions, initial
+conditions and the fused RK substeps of the HD and Boussinesq solvers.
+
+Tolerances: FP64 paths rel <= 1e-12 (1e-13 for single operators); the FP32
+path against the FP64 oracle rel <= 1e-5."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from tests.conftest import rel_l2
+from tests.helpers import rand_real, rand_spectral, solenoidal_ic, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def ghost(*args, **kw):
+    from ghost_b200 import Ghost
+    return Ghost(*args, **kw)
+
+
+GRIDS = [(16, 16, 16), (32, 64, 16), (64, 32, 128), (64, 64, 64)]
+
+
+# ------------------------------------------------------------------ FFTs
+@pytest.mark.parametrize("shape", GRIDS)
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_fftp3d_real_to_complex(shape, prec):
+    from ghost_b200 import GHOST_REAL_TO_COMPLEX
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    r = rand_real(o, 1)
+    ref = o.fftp3d_real_to_complex(r)
+    plan = g.fftp3d_create_plan(shape, GHOST_REAL_TO_COMPLEX)
+    out = g.czeros()
+    g.fftp3d_real_to_complex(plan, to_dev(r.astype(g.rdtype_np)), out)
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    assert rel_l2(to_host(out), ref) < tol
+
+
+@pytest.mark.parametrize("shape", GRIDS)
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_fftp3d_complex_to_real(shape, prec):
+    from ghost_b200 import GHOST_COMPLEX_TO_REAL
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    c = rand_spectral(o, 2)  # not Hermitian: exercises the kx=0 / Nyquist rule
+    ref = o.fftp3d_complex_to_real(c)
+    plan = g.fftp3d_create_plan(shape, GHOST_COMPLEX_TO_REAL)
+    cin = to_dev(c.astype(g.cdtype_np))
+    keep = cin.clone()
+    out = g.rzeros()
+    g.fftp3d_complex_to_real(plan, cin, out)
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    assert rel_l2(to_host(out), ref) < tol
+    assert bool((cin == keep).all())  # input left unmodified
+
+
+def test_fft_host_arrays_equal_device_arrays():
+    from ghost_b200 import GHOST_REAL_TO_COMPLEX
+    o = Oracle(32)
+    g = ghost(32)
+    r = rand_real(o, 3)
+    plan = g.fftp3d_create_plan((32, 32, 32), GHOST_REAL_TO_COMPLEX)
+    host_out = np.zeros(o.sshape, np.complex128)
+    g.fftp3d_real_to_complex(plan, r, host_out)
+    dev_out = g.czeros()
+    g.fftp3d_real_to_complex(plan, to_dev(r), dev_out)
+    assert np.array_equal(host_out, to_host(dev_out))
+
+
+def test_fft_round_trip_at_512_fp32():
+    """Size-independent property at the benchmark size: c2r(r2c(x)) = N^3 x."""
+    from ghost_b200 import GHOST_COMPLEX_TO_REAL, GHOST_REAL_TO_COMPLEX
+    import torch
+    n = 512
+    g = ghost(n, precision="fp32")
+    x = torch.randn((n, n, n), device="cuda", dtype=torch.float32, generator=torch.Generator("cuda").manual_seed(0))
+    c = g.czeros()
+    pf = g.fftp3d_create_plan((n, n, n), GHOST_REAL_TO_COMPLEX)
+    pb = g.fftp3d_create_plan((n, n, n), GHOST_COMPLEX_TO_REAL)
+    g.fftp3d_real_to_complex(pf, x, c)
+    # Parseval: sum |x|^2 = (1/N^3) sum_k w_k |X_k|^2
+    w = torch.full((c.shape[0], 1, 1), 2.0, device="cuda", dtype=torch.float64)
+    w[0] = 1.0
+    w[-1] = 1.0
+    lhs = float((x.double() ** 2).sum())
+    rhs = float((w * c.abs().double() ** 2).sum()) / n**3
+    assert abs(lhs - rhs) / lhs < 1e-5
+    y = g.rzeros()
+    g.fftp3d_complex_to_real(pb, c, y)
+    err = float((y / n**3 - x).norm() / x.norm())
+    assert err < 1e-5
+
+
+# ------------------------------------------------------------- operators
+@pytest.fixture(scope="module")
+def pair32():
+    o = Oracle(32, 32, 64)
+    g = ghost(32, 32, 64)
+    a, b, c = (rand_spectral(o, s) for s in (11, 12, 13))
+    return o, g, a, b, c
+
+
+@pytest.mark.parametrize("dir", [1, 2, 3])
+def test_derivk3_rotor3_nonlhd3(pair32, dir):
+    o, g, a, b, c = pair32
+    A, B, Cc = to_dev(a), to_dev(b), to_dev(c)
+    out = g.czeros()
+    g.derivk3(A, out, dir)
+    assert rel_l2(to_host(out), o.derivk3(a, dir)) < 1e-15
+    g.rotor3(A, B, out, dir)
+    assert rel_l2(to_host(out), o.rotor3(a, b, dir)) < 1e-15
+    g.nonlhd3(A, B, Cc, out, dir)
+    assert rel_l2(to_host(out), o.nonlhd3(a, b, c, dir)) < 1e-15
+    # output aliasing an input, as hd_rkstep2 does with nonlhd3(C4,C5,C6,C4,3)
+    A2 = A.clone()
+    g.nonlhd3(A2, B, Cc, A2, dir)
+    assert rel_l2(to_host(A2), o.nonlhd3(a, b, c, dir)) < 1e-15
+
+
+def test_laplak3_sharp(pair32):
+    o, g, a, b, c = pair32
+    A = to_dev(a)
+    out = g.czeros()
+    g.laplak3(A, out)
+    assert rel_l2(to_host(out), o.laplak3(a)) < 1e-15
+    g.sharp(A, out, np.pi / 7.0)
+    assert np.array_equal(to_host(out), o.sharp(a, np.pi / 7.0))
+
+
+def test_prodre3(pair32):
+    o, g, a, b, c = pair32
+    outs = [g.czeros() for _ in range(3)]
+    g.prodre3(to_dev(a), to_dev(b), to_dev(c), *outs)
+    ref = o.prodre3(a, b, c)
+    assert rel_l2([to_host(x) for x in outs], list(ref)) < 1e-13
+
+
+def test_reductions(pair32):
+    o, g, a, b, c = pair32
+    A, B, Cc = to_dev(a), to_dev(b), to_dev(c)
+    for kin in (0, 1, 2):
+        assert g.energy(A, B, Cc, kin) == pytest.approx(o.energy(a, b, c, kin), rel=1e-13)
+    assert g.helicity(A, B, Cc) == pytest.approx(o.helicity(a, b, c), rel=1e-11, abs=1e-14)
+    for kin in (0, 1):
+        assert g.cross(A, B, Cc, B, Cc, A, kin) == pytest.approx(o.cross(a, b, c, b, c, a, kin), rel=1e-11)
+    assert g.divergence(A, B, Cc) == pytest.approx(o.divergence(a, b, c), rel=1e-13)
+    # deterministic: bit-identical on repeat
+    assert g.energy(A, B, Cc, 0) == g.energy(A, B, Cc, 0)
+
+
+@pytest.mark.parametrize("kin", [0, 1, 2])
+def test_maxabs(kin):
+    o = Oracle(32)
+    g = ghost(32)
+    v = solenoidal_ic(o, seed=21)
+    got = g.maxabs(*[to_dev(x) for x in v], kin)
+    assert got == pytest.approx(o.maxabs(*v, kin), rel=1e-13)
+
+
+def test_spectrumc():
+    o = Oracle(64)
+    g = ghost(64)
+    v = solenoidal_ic(o, seed=31)
+    Ek, Hk = g.spectrumc(*[to_dev(x) for x in v], 1, 1)
+    Ek0, Hk0 = o.spectrumc(*v, 1, 1)
+    assert np.allclose(Ek, Ek0, rtol=1e-12, atol=1e-300)
+    assert np.allclose(Hk, Hk0, rtol=1e-9, atol=1e-18)
+    Ew, _ = g.spectrumc(*[to_dev(x) for x in v], 0, 0)
+    Ew0, _ = o.spectrumc(*v, 0, 0)
+    assert np.allclose(Ew, Ew0, rtol=1e-12, atol=1e-300)
+    Ek2, _ = g.spectrumc(*[to_dev(x) for x in v], 1, 0)
+    assert np.array_equal(Ek, Ek2)
+
+
+def test_normalize_and_initial_condition():
+    o = Oracle(64)
+    g = ghost(64)
+    v0 = solenoidal_ic(o, seed=1000)
+    outs = [g.czeros() for _ in range(3)]
+    seed = g.init_random_solenoidal(1000, 1.0, 64 / 3.0, 1, 1.0, *outs)
+    _, seed0 = o.random_solenoidal(1000, 1.0, 64 / 3.0, 1, 1.0)
+    assert seed == seed0
+    assert rel_l2([to_host(x) for x in outs], v0) < 1e-14
+    f0, _ = o.random_solenoidal(5, 2.0, 3.0, 0, 1.0)
+    F = [to_dev(x * 3.0) for x in f0]
+    g.normalize(*F, 1.0, 1)
+    assert rel_l2([to_host(x) for x in F], f0) < 1e-14
+
+
+# ------------------------------------------------------------ RK steps
+def test_hd_cfg0_one_step_and_hundred_steps_fp64():
+    """Config 0: 64^3 FP64, nu=2e-3, dt=1e-3, RK2, unit-energy seeded IC:
+    rel L2 <= 1e-12 after one step and <= 1e-9 after 100 steps."""
+    o = Oracle(64)
+    g = ghost(64)
+    v0 = solenoidal_ic(o, seed=1000)
+    V = [to_dev(x) for x in v0]
+    g.hd_run(1, 2, 1e-3, 2e-3, *V)
+    ref1 = o.hd_run(1, 2, 1e-3, 2e-3, v0)
+    assert rel_l2([to_host(x) for x in V], ref1) < 1e-12
+    g.hd_run(99, 2, 1e-3, 2e-3, *V)
+    ref100 = o.hd_run(99, 2, 1e-3, 2e-3, ref1)
+    assert rel_l2([to_host(x) for x in V], ref100) < 1e-9
+
+
+def test_hd_forced_rk4_fp64_and_fp32_against_fp64_oracle():
+    """Config 1 at reduced size: forcing on 2<=|k|<=3 (f0=1), nu=1e-3,
+    dt=5e-4, RK4; FP32 within 1e-5 of the FP64 oracle per step."""
+    n = 64
+    o = Oracle(n)
+    v0 = solenoidal_ic(o, seed=1001)
+    f, _ = o.random_solenoidal(2001, 2.0, 3.0, 0, 1.0)
+    g64, g32 = ghost(n), ghost(n, precision="fp32")
+    V64 = [to_dev(x) for x in v0]
+    V32 = [to_dev(x.astype(np.complex64)) for x in v0]
+    F64 = [to_dev(x) for x in f]
+    F32 = [to_dev(x.astype(np.complex64)) for x in f]
+    ref = v0
+    for step in range(3):
+        ref = o.hd_run(1, 4, 5e-4, 1e-3, ref, f)
+        g64.hd_run(1, 4, 5e-4, 1e-3, *V64, *F64)
+        g32.hd_run(1, 4, 5e-4, 1e-3, *V32, *F32)
+        assert rel_l2([to_host(x) for x in V64], ref) < 1e-12
+        assert rel_l2([to_host(x).astype(np.complex128) for x in V32], ref) < 1e-5
+        # restart the FP32 run from the oracle state: per-step error
+        V32 = [to_dev(x.astype(np.complex64)) for x in ref]
+
+
+def test_rkstep1_rkstep2_equal_fused_run():
+    o = Oracle(32)
+    g = ghost(32)
+    v0 = solenoidal_ic(o, seed=77)
+    f, _ = o.random_solenoidal(78, 2.0, 3.0, 0, 1.0)
+    A = [to_dev(x) for x in v0]
+    B = [to_dev(x) for x in v0]
+    F = [to_dev(x) for x in f]
+    C = [g.czeros() for _ in range(3)]
+    g.hd_rkstep1(*A, *C)
+    for oo in (3, 2, 1):
+        g.hd_rkstep2(oo, 1e-3, 1e-3, *A, *C, *F)
+    g.hd_run(1, 3, 1e-3, 1e-3, *B, *F)
+    assert all(bool((x == y).all()) for x, y in zip(A, B))
+    ref = o.hd_run(1, 3, 1e-3, 1e-3, v0, f)
+    assert rel_l2([to_host(x) for x in A], ref) < 1e-12
+
+
+def test_hd_host_arrays_drop_in():
+    """GHOST-style host arrays through the same entry points."""
+    o = Oracle(32)
+    g = ghost(32)
+    v0 = solenoidal_ic(o, seed=9)
+    V = [x.copy() for x in v0]
+    g.hd_run(2, 2, 1e-3, 2e-3, *V)
+    ref = o.hd_run(2, 2, 1e-3, 2e-3, v0)
+    assert rel_l2(V, ref) < 1e-12
+
+
+def test_hd_anisotropic_grid():
+    o = Oracle(32, 16, 64)
+    g = ghost(32, 16, 64)
+    v0 = solenoidal_ic(o, seed=17)
+    V = [to_dev(x) for x in v0]
+    g.hd_run(3, 2, 1e-3, 2e-3, *V)
+    ref = o.hd_run(3, 2, 1e-3, 2e-3, v0)
+    assert rel_l2([to_host(x) for x in V], ref) < 1e-12
+
+
+def test_abc_decay_on_gpu():
+    o = Oracle(32)
+    R = o.abc(1, 1, 1.0, 1.0, 1.0)
+    v = list(o.normalize(*[o.fftp3d_real_to_complex(x) for x in R], 1.0))
+    g = ghost(32)
+    V = [to_dev(x) for x in v]
+    E0 = g.energy(*V, 1)
+    g.hd_run(50, 4, 1e-3, 0.01, *V)
+    assert g.energy(*V, 1) / E0 == pytest.approx(np.exp(-2 * 0.01 * 0.05), rel=1e-12)
+
+
+# ------------------------------------------------------------ Boussinesq
+def test_advect3():
+    o = Oracle(32, 32, 16, Lx=1, Ly=1, Lz=0.5, arbsize=True)
+    g = ghost(32, 32, 16, Lx=1, Ly=1, Lz=0.5, arbsize=True)
+    a, b, c, d = (rand_spectral(o, s, 1e-2) for s in (41, 42, 43, 44))
+    out = g.czeros()
+    g.advect3(*[to_dev(x) for x in (a, b, c, d)], out)
+    assert rel_l2(to_host(out), o.advect3(a, b, c, d)) < 1e-13
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_bouss_steps(prec):
+    """Config 2 physics on a small elongated ARBSIZE box (Lz = Lx/4)."""
+    shape = (64, 64, 16)
+    o = Oracle(*shape, Lx=1, Ly=1, Lz=0.25, arbsize=True)
+    g = ghost(*shape, Lx=1, Ly=1, Lz=0.25, arbsize=True, precision=prec)
+    v0, _ = o.random_solenoidal(55, 1.0, 6.0, 1, 1.0)
+    th0 = rand_spectral(o, 56, 0.0)  # zero temperature perturbation
+    args = (4, 2.5e-4, 5e-4, 5e-4, 0.5, 8.0, 8.0)
+    ref_v, ref_th = o.bouss_run(2, *args, v0, th0)
+    cd = g.cdtype_np
+    V = [to_dev(x.astype(cd)) for x in v0]
+    TH = to_dev(th0.astype(cd))
+    g.bouss_run(2, *args, *V, TH)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    assert rel_l2([to_host(x).astype(np.complex128) for x in V] + [to_host(TH).astype(np.complex128)],
+                  list(ref_v) + [ref_th]) < tol
+    # buoyancy couples theta in after one step
+    assert float(TH.abs().max()) > 0
+
+
+def test_native_kernels_ran():
+    g = ghost(32)
+    n0 = g.launch_count()
+    v = [g.czeros() for _ in range(3)]
+    g.hd_run(1, 2, 1e-3, 1e-3, *v)
+    assert g.launch_count() - n0 == 10  # 5 fused passes per substep

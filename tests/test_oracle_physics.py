@@ -1,0 +1,133 @@
+"""The oracle's HD operators and RK step against analytic known answers taken
+from the reference's own example initial conditions and consistency checks."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from tests.conftest import rel_l2
+from tests.helpers import solenoidal_ic
+
+
+def test_wavenumber_tables_follow_main3d():
+    # main3D.fpp:1746-1749: kx(i)=i-1 for i<=n/2, kx(i+n/2)=i-n/2-1
+    o = Oracle(16)
+    kx, ky, kz, kn2, kk2 = o.tables()
+    assert kx.tolist() == [0, 1, 2, 3, 4, 5, 6, 7, -8, -7, -6, -5, -4, -3, -2, -1]
+    assert o.kmax == pytest.approx(16 * 16 / 9.0)
+    assert o.tiny == pytest.approx(min(1e-5, 0.1 / 16**2))
+    assert kn2[3, 2, 1] == 9 + 4 + 1 and np.shares_memory is not None
+    # anisotropic ARBSIZE box: kn2 normalised per axis, kk2 physical
+    a = Oracle(32, 32, 8, Lx=1, Ly=1, Lz=0.25, arbsize=True)
+    kx, ky, kz, kn2, kk2 = a.tables()
+    assert a.anis == 1 and a.kmax == pytest.approx(1 / 9.0)
+    assert kz[1] == 4.0 and a.nmax == 32
+    assert kk2[1, 0, 1] == pytest.approx(1 + 16)
+    assert kn2[1, 0, 1] == pytest.approx(1 / 32**2 + 1 / 8**2)
+
+
+def test_randu_sequence_is_park_miller_with_mask():
+    import ctypes
+    o = Oracle(16)
+    s = ctypes.c_int32(1000)
+    seq = [o.lib.o_randu(ctypes.byref(s)) for _ in range(4)]
+    # recompute the masked Park-Miller sequence independently
+    idum, out = 1000, []
+    for _ in range(4):
+        idum ^= 123459876
+        k = idum // 127773
+        idum = 16807 * (idum - k * 127773) - 2836 * k
+        if idum < 0:
+            idum += 2147483647
+        out.append((idum * 2.0**-31 - 0.5) * 2)
+        idum ^= 123459876
+    assert np.allclose(seq, out, rtol=0, atol=1e-15)
+    assert s.value == idum
+
+
+def test_abc_beltrami_flow_decays_exactly():
+    """examples/initialv.f90_abc with kdn=kup=1 is a Beltrami flow: curl v = v,
+    the projected nonlinear term vanishes and E(t) = E0 exp(-2 nu t)."""
+    o = Oracle(32)
+    R = o.abc(1, 1, 1.0, 1.0, 1.0)
+    v = [o.fftp3d_real_to_complex(x) for x in R]
+    v = list(o.normalize(*v, 1.0))
+    nl = o.prodre3(*v)
+    g = [o.nonlhd3(*nl, d) for d in (1, 2, 3)]
+    vmax = max(np.abs(x).max() for x in v)
+    assert max(np.abs(x).max() for x in g) < 1e-13 * vmax
+    nu, dt, n = 0.01, 1e-3, 50
+    E0 = o.energy(*v, 1)
+    v2 = o.hd_run(n, 4, dt, nu, v)
+    assert o.energy(*v2, 1) / E0 == pytest.approx(np.exp(-2 * nu * n * dt), rel=1e-12)
+
+
+def test_solenoidal_ic_properties():
+    o = Oracle(32)
+    v = solenoidal_ic(o)
+    assert o.energy(*v, 1) == pytest.approx(1.0, rel=1e-13)
+    assert o.divergence(*v) < 1e-28
+    # Hermitian kx=0 plane: v(0,-ky,-kz) = conj v(0,ky,kz)
+    p = v[0][0]
+    flip = np.roll(p[::-1, ::-1], 1, axis=(0, 1))
+    assert np.abs(p - np.conj(flip)).max() < 1e-15
+    Ek, _ = o.spectrumc(*v, 1, 0)
+    assert int(np.argmax(Ek)) + 1 == 2  # E(k) ~ k^4 exp(-k^2/2) peaks at k=2
+
+
+def test_energy_budget_matches_reference_consistency_check():
+    """3D/src/README:490-502: without random forcing dE/dt = -2 nu Omega + eps,
+    with E = <v^2>/2, Omega = <w^2>/2 (balance.txt columns 2-4)."""
+    o = Oracle(32)
+    v = solenoidal_ic(o, seed=7)
+    f, _ = o.random_solenoidal(11, 2.0, 3.0, 0, 1.0)
+    nu, dt = 2e-3, 1e-4
+    e = []
+    vv = v
+    for _ in range(3):
+        e.append((o.energy(*vv, 1), o.energy(*vv, 0), o.cross(*vv, *f, 1)))
+        vv = o.hd_run(1, 4, dt, nu, vv, f)
+    e.append((o.energy(*vv, 1), o.energy(*vv, 0), o.cross(*vv, *f, 1)))
+    dEdt = (e[2][0] - e[0][0]) / 2 / (2 * dt)  # <v^2>/2 centred difference
+    rhs = -nu * e[1][1] + e[1][2]             # -2 nu Omega + eps, Omega=<w^2>/2
+    assert dEdt == pytest.approx(rhs, rel=1e-4)
+
+
+def test_nonlinear_term_is_solenoidal_and_divergence_free_update():
+    o = Oracle(32)
+    v = solenoidal_ic(o, seed=3)
+    nl = o.prodre3(*v)
+    g = [o.nonlhd3(*nl, d) for d in (1, 2, 3)]
+    assert o.divergence(*g) < 1e-24 * o.energy(*g, 1) + 1e-30
+    v2 = o.hd_run(2, 2, 1e-3, 2e-3, v)
+    assert o.divergence(*v2) < 1e-28
+
+
+def test_rk_truncation_zeroes_mean_and_dealiased_modes():
+    o = Oracle(16)
+    v = solenoidal_ic(o, seed=5)
+    v = [x + 1e-3 for x in v]  # pollute every mode
+    C = [x.copy() for x in v]
+    f = [np.zeros_like(x) for x in v]
+    out = o.hd_rkstep2(2, 1e-3, 1e-3, v, C, f)
+    kx, ky, kz, kn2, kk2 = o.tables()
+    mask = (kn2 <= o.kmax) & (kn2 >= o.tiny)
+    for x in out:
+        assert np.all(x[~mask] == 0)
+        assert x[0, 0, 0] == 0
+
+
+def test_fp32_oracle_tracks_fp64():
+    o64, o32 = Oracle(32), Oracle(32, precision="fp32")
+    v = solenoidal_ic(o64)
+    a = o64.hd_run(5, 2, 1e-3, 2e-3, v)
+    b = o32.hd_run(5, 2, 1e-3, 2e-3, [x.astype(np.complex64) for x in v])
+    assert rel_l2(b, a) < 1e-5
+
+
+def test_spectrum_sums_to_energy():
+    o = Oracle(32)
+    v = solenoidal_ic(o)
+    Ek, Hk = o.spectrumc(*v, 1, 1)
+    # shells beyond nmax/2+1 are dropped; the IC lives below N/3
+    assert Ek.sum() == pytest.approx(o.energy(*v, 1), rel=1e-12)
+    assert Hk.sum() == pytest.approx(o.helicity(*v), rel=1e-10, abs=1e-14)
