@@ -73,6 +73,7 @@ SIGNATURES = {
     "ghost_divergence": [P, P, P, P, PD],
     "ghost_maxabs": [P, P, P, P, PD, I],
     "ghost_spectrumc": [P, P, P, P, I, I, PD, PD],
+    "ghost_spectrumc_noalloc": [P, P, P, P, I, I, PD, PD],
     "ghost_hdcheck": [P, P, P, P, P, P, P, I, I, PD],
     "ghost_normalize": [P, P, P, P, D, I],
     "ghost_sharp": [P, P, P, D],

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1285,6 +1286,89 @@ int ghost_bouss_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, dou
                    : bouss_substep_dev<double>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr,
                                                o == ord));
   return st.finish();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- no-allocation spectrum
+// Partial sums of ghost_spectrumc_noalloc: a fixed grid of
+// NOALLOC_BLOCKS blocks writes one histogram row each, then the final row.
+// Every slot a call reads was written earlier by that same call, so
+// nothing needs clearing between calls.
+#define NOALLOC_BLOCKS 64
+static_assert((NOALLOC_BLOCKS + 1) * GHOST_SPECTRUM_NOALLOC_MAX_BINS <= GHOST_SPECTRUM_NOALLOC_DOUBLES,
+              "static spectrum scratch too small for the advertised shell count");
+static __device__ __align__(256) double g_spectrum_scratch[GHOST_SPECTRUM_NOALLOC_DOUBLES];
+
+static std::mutex g_spectrum_scratch_mu;
+static void *g_spectrum_scratch_addr[128];
+
+// Device address of the static array on the current device, looked up
+// once per device (in host code the symbol is only a host-side stand-in).
+static int spectrum_scratch_address(int dev, double **out) {
+  if (dev < 0 || dev >= 128) return fail(GHOST_ERR_STATE, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_spectrum_scratch_mu);
+  if (!g_spectrum_scratch_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_spectrum_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return fail(GHOST_ERR_CUDA, "cudaGetSymbolAddress(spectrum scratch): %s", cudaGetErrorString(e));
+    }
+    g_spectrum_scratch_addr[dev] = p;
+  }
+  *out = (double *)g_spectrum_scratch_addr[dev];
+  return GHOST_OK;
+}
+
+template <typename R>
+static int spectrum_noalloc_dev(ghost_ctx *c, double *scratch, int kind, const void *a, const void *b, const void *cc,
+                                double *out_host) {
+  const int nbins = c->nmax / 2 + 1;
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
+  const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
+  GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  spectrum_kernel<R><<<NOALLOC_BLOCKS, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, c->nspec, nbins, (R)c->Dkk,
+                                                                 scratch);
+  GB_CHECK(post_launch(c));
+  double *fin = scratch + (size_t)NOALLOC_BLOCKS * nbins;
+  finalize_kernel<<<1, 256, 0, c->stream>>>(scratch, NOALLOC_BLOCKS, nbins, fin);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * nbins, cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
+extern "C" {
+
+int ghost_spectrumc_noalloc(ghost_ctx *c, const void *a, const void *b, const void *cc, int kin, int hel, double *Ek,
+                            double *Hk) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc) return fail(GHOST_ERR_ARG, "null field");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  if (kin <= 1 && !Ek) return fail(GHOST_ERR_ARG, "null Ek");
+  if (hel == 1 && !Hk) return fail(GHOST_ERR_ARG, "null Hk");
+  if (!is_device_ptr(a) || !is_device_ptr(b) || !is_device_ptr(cc))
+    return fail(GHOST_ERR_ARG, "ghost_spectrumc_noalloc needs device arrays (host arrays would need staging buffers)");
+  const int nbins = c->nmax / 2 + 1;
+  if (nbins > GHOST_SPECTRUM_NOALLOC_MAX_BINS)
+    return fail(GHOST_ERR_SIZE, "%d spectral shells exceed the static scratch limit of %d (nmax <= %d)", nbins,
+                GHOST_SPECTRUM_NOALLOC_MAX_BINS, 2 * (GHOST_SPECTRUM_NOALLOC_MAX_BINS - 1));
+  int dev = -1;
+  GB_CUDA(cudaGetDevice(&dev));
+  if (dev != c->device) return fail(GHOST_ERR_STATE, "current device %d is not the context's device %d", dev, c->device);
+  double *scratch = nullptr;
+  GB_CHECK(spectrum_scratch_address(dev, &scratch));
+  const bool sp = c->precision == GHOST_SINGLE;
+  if (kin <= 1) {
+    const int kind = kin == 1 ? RED_ENERGY : RED_ENSTROPHY;
+    GB_CHECK(sp ? spectrum_noalloc_dev<float>(c, scratch, kind, a, b, cc, Ek)
+                : spectrum_noalloc_dev<double>(c, scratch, kind, a, b, cc, Ek));
+  }
+  if (hel == 1)
+    GB_CHECK(sp ? spectrum_noalloc_dev<float>(c, scratch, RED_HELICITY, a, b, cc, Hk)
+                : spectrum_noalloc_dev<double>(c, scratch, RED_HELICITY, a, b, cc, Hk));
+  return GHOST_OK;
 }
 
 }  // extern "C"

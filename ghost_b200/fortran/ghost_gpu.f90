@@ -188,6 +188,15 @@
          REAL(C_DOUBLE) :: Ek(*), Hk(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       ! spectra without any allocation (device arrays only; see the C header)
+       FUNCTION ghost_spectrumc_noalloc(ctx,a,b,c,kin,hel,Ek,Hk) &
+                BIND(C,name="ghost_spectrumc_noalloc") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: kin, hel
+         REAL(C_DOUBLE) :: Ek(*), Hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_hdcheck(ctx,vx,vy,vz,fx,fy,fz,hel,chk,out) BIND(C,name="ghost_hdcheck") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE
          TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, fx, fy, fz

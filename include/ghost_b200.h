@@ -169,6 +169,29 @@ int ghost_maxabs(ghost_ctx *ctx, const void *a, const void *b, const void *c, do
  * when hel == 1 (Hk may then be NULL otherwise) */
 int ghost_spectrumc(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel,
                     double *Ek, double *Hk);
+/* ghost_spectrumc_noalloc: the same shell spectra as ghost_spectrumc,
+ * computed without allocating any memory.  It has no counterpart in the
+ * reference; it exists for callers that cannot let the library allocate:
+ * runs that hand the device memory to their own fields at start-up (a GHOST
+ * grid sized to fill HBM, or an application under a fixed memory budget),
+ * where the lazy cudaMalloc of ghost_spectrumc's partial-sum buffer would
+ * fail at the first spectrum output step, and time loops that cannot
+ * afford the device-wide synchronisation an allocation brings.
+ * The partial sums live in a static device array of
+ * GHOST_SPECTRUM_NOALLOC_DOUBLES doubles (512 KiB, held by every GPU that
+ * loads the library until the process exits); a grid with more than
+ * GHOST_SPECTRUM_NOALLOC_MAX_BINS shells (nmax/2+1) is rejected with
+ * GHOST_ERR_SIZE.  a, b, c must be device arrays (host arrays would need
+ * staging buffers: GHOST_ERR_ARG); Ek, Hk are host arrays as above.  The
+ * first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  All
+ * calls share the one array and it keeps the last call's contents: calls
+ * that overlap on the GPU (other streams, other contexts on the device)
+ * race and must be serialised by the caller. */
+#define GHOST_SPECTRUM_NOALLOC_DOUBLES 65536
+#define GHOST_SPECTRUM_NOALLOC_MAX_BINS 1008
+int ghost_spectrumc_noalloc(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel,
+                            double *Ek, double *Hk);
 /* hdcheck(a,b,c,d,e,f,t,dt,hel,chk) (:984-1105) without the file output:
  * out[0]=<|v|^2>, out[1]=<|w|^2>, out[2]=helicity (hel==1), out[3]=<v.f>,
  * out[4]=<(div v)^2> (chk==1) */
