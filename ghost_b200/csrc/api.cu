@@ -87,6 +87,8 @@ static bool is_device_ptr(const void *p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+static int check_status(ghost_ctx *c);
+
 struct Staging {
   ghost_ctx *c;
   int used = 0;
@@ -114,6 +116,9 @@ struct Staging {
       return GHOST_OK;
     }
     if (is_device_ptr(user)) {
+      // the passes move tiles with TMA bulk copies: 16-byte alignment
+      if (((uintptr_t)(const void *)user & 15u) != 0)
+        return fail(GHOST_ERR_ARG, "device array %p is not 16-byte aligned", (const void *)user);
       *dev = user;
       return GHOST_OK;
     }
@@ -125,12 +130,17 @@ struct Staging {
     *dev = (T *)d;
     return GHOST_OK;
   }
-  int finish() {
-    for (auto &b : back) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
-    if (any_host) GB_CUDA(cudaStreamSynchronize(c->stream));
-    return GHOST_OK;
-  }
+  int finish();
 };
+
+int Staging::finish() {
+  for (auto &b : back) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (any_host) {
+    GB_CUDA(cudaStreamSynchronize(c->stream));
+    return check_status(c);
+  }
+  return GHOST_OK;
+}
 
 template <typename R> const KParams<R> &kparams(const ghost_ctx *c);
 template <> const KParams<float> &kparams<float>(const ghost_ctx *c) { return c->kp32; }
@@ -139,6 +149,19 @@ template <> const KParams<double> &kparams<double>(const ghost_ctx *c) { return 
 static int post_launch(ghost_ctx *c) {
   c->launches++;
   GB_CUDA(cudaGetLastError());
+  return GHOST_OK;
+}
+
+// Reads and clears the device status word (caller has synchronised).
+static int check_status(ghost_ctx *c) {
+  if (!c->status) return GHOST_OK;
+  int st = 0;
+  GB_CUDA(cudaMemcpy(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    GB_CUDA(cudaMemset(c->status, 0, sizeof(int)));
+    return fail(GHOST_ERR_TIMEOUT, "a device-side wait gave up (status %d); results of the affected calls are invalid",
+                st);
+  }
   return GHOST_OK;
 }
 
@@ -185,7 +208,7 @@ static int timers_collect(ghost_ctx *c) {
 }
 
 template <class Op> struct ZKind;
-template <typename R, int S> struct ZKind<ZC2C<R, S>> { static constexpr int value = GHOST_TIMER_Z_C2C; };
+template <typename R, int S, int NF> struct ZKind<ZC2C<R, S, NF>> { static constexpr int value = GHOST_TIMER_Z_C2C; };
 template <typename R, int P> struct ZKind<ZInv<R, P>> { static constexpr int value = GHOST_TIMER_Z_INV; };
 template <typename R> struct ZKind<ZFwdHD<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
 template <typename R> struct ZKind<ZFwdBouss<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
@@ -200,57 +223,95 @@ static int grid1d(size_t n) {
 template <typename R> constexpr int xE() { return sizeof(R) == 4 ? 8 : 4; }
 template <typename R> constexpr int xBZ() { return sizeof(R) == 4 ? 8 : 4; }
 
-template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op) {
-  constexpr int E = 8, T = N / E;
-  int lpb = std::max(1, 256 / T);
-  lpb = std::min(lpb, c->ny);
-  const long nlines = (long)c->ny * c->nxh;
-  const size_t smem = (size_t)(N + lpb * ZShape<N, E>::NP) * sizeof(cx<R>);
-  auto kern = zpass_kernel<R, N, E, Op>;
+// Pruning state for one substep: null tables = every line.
+struct Prune {
+  const int *lines = nullptr;
+  int nlines = 0;
+  const int *jpos = nullptr, *jneg = nullptr;
+  int ni = 0;    // kx indices processed by the y passes
+  int rows = 0;  // kx rows present in / written by the x pass
+};
+
+template <typename R> constexpr int zE() { return sizeof(R) == 4 ? 8 : 4; }
+
+static int sm_count(ghost_ctx *c) {
+  if (c->num_sms <= 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, c->device);
+    c->num_sms = n > 0 ? n : 148;
+  }
+  return c->num_sms;
+}
+
+// Persistent grid: as many CTAs as fit on the device at once, or fewer
+// when there are fewer tiles.
+template <class K> static int persistent_grid(ghost_ctx *c, K kern, int threads, size_t smem, long ntiles) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const long g = (long)per_sm * sm_count(c);
+  return (int)std::max<long>(1, std::min<long>(g, ntiles));
+}
+
+static PipeCtl pipe_ctl(ghost_ctx *c) { return PipeCtl{c->status, c->wait_cap}; }
+
+template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
+  constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
+  constexpr int LPB = 256 / T > 0 ? 256 / T : 1;
+  using G = ZGeom<R, N, E, LPB, Op::NLOAD>;
+  constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
+  const size_t smem = G::smem_bytes(STAGES);
+  const int nlines = pr.lines ? pr.nlines : c->ny * c->nxh;
+  auto kern = zpipe_kernel<R, N, E, LPB, STAGES, Op>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = persistent_grid(c, kern, LPB * T, smem, (nlines + LPB - 1) / LPB);
   const int ts = timer_begin(c, ZKind<Op>::value);
-  kern<<<(unsigned)(nlines / lpb), lpb * T, smem, c->stream>>>(op, (const cx<R> *)c->tw_z, lpb);
+  kern<<<grid, LPB * T, smem, c->stream>>>(op, (const cx<R> *)c->tw_z, pr.lines, nlines, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
 }
 
-template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op) {
+template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const Prune &pr = Prune()) {
   switch (c->nz) {
-    case 16: return launch_z_n<R, 16>(c, op);
-    case 32: return launch_z_n<R, 32>(c, op);
-    case 64: return launch_z_n<R, 64>(c, op);
-    case 128: return launch_z_n<R, 128>(c, op);
-    case 256: return launch_z_n<R, 256>(c, op);
-    case 512: return launch_z_n<R, 512>(c, op);
-    case 1024: return launch_z_n<R, 1024>(c, op);
+    case 16: return launch_z_n<R, 16>(c, op, pr);
+    case 32: return launch_z_n<R, 32>(c, op, pr);
+    case 64: return launch_z_n<R, 64>(c, op, pr);
+    case 128: return launch_z_n<R, 128>(c, op, pr);
+    case 256: return launch_z_n<R, 256>(c, op, pr);
+    case 512: return launch_z_n<R, 512>(c, op, pr);
+    case 1024: return launch_z_n<R, 1024>(c, op, pr);
   }
   return fail(GHOST_ERR_SIZE, "nz=%d unsupported", c->nz);
 }
 
-template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf) {
-  constexpr int E = 8, T = N / E;
-  int bz = sizeof(R) == 4 ? 16 : 8;
-  while (bz * T > 1024) bz >>= 1;
-  bz = std::min(bz, c->nz);
-  const size_t smem = (size_t)(N + bz * N) * sizeof(cx<R>);
-  auto kern = ypass_kernel<R, N, E, S>;
+template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
+  constexpr int E = N < 8 ? N : 8, T = N / E;
+  constexpr int BZ0 = sizeof(R) == 4 ? 16 : 8;
+  constexpr int BZ = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
+  using G = YGeom<R, N, E, BZ>;
+  constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
+  if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);
+  const size_t smem = G::smem_bytes(STAGES);
+  auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(c->nz / bz, c->nxh, nf);
+  const int ni = pr.jpos ? pr.ni : c->nxh;
+  const long ntiles = (long)(c->nz / BZ) * ni * nf;
+  const int grid = persistent_grid(c, kern, BZ * T, smem, ntiles);
   const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
-  kern<<<grid, bz * T, smem, c->stream>>>(f, (const cx<R> *)c->tw_y, c->nz, bz);
+  kern<<<grid, BZ * T, smem, c->stream>>>(f, (const cx<R> *)c->tw_y, c->nz, ni, nf, pr.jpos, pr.jneg, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
 }
 
-template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int nf) {
+template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr = Prune()) {
   switch (c->ny) {
-    case 16: return launch_y_n<R, 16, S>(c, f, nf);
-    case 32: return launch_y_n<R, 32, S>(c, f, nf);
-    case 64: return launch_y_n<R, 64, S>(c, f, nf);
-    case 128: return launch_y_n<R, 128, S>(c, f, nf);
-    case 256: return launch_y_n<R, 256, S>(c, f, nf);
-    case 512: return launch_y_n<R, 512, S>(c, f, nf);
-    case 1024: return launch_y_n<R, 1024, S>(c, f, nf);
+    case 16: return launch_y_n<R, 16, S>(c, f, nf, pr);
+    case 32: return launch_y_n<R, 32, S>(c, f, nf, pr);
+    case 64: return launch_y_n<R, 64, S>(c, f, nf, pr);
+    case 128: return launch_y_n<R, 128, S>(c, f, nf, pr);
+    case 256: return launch_y_n<R, 256, S>(c, f, nf, pr);
+    case 512: return launch_y_n<R, 512, S>(c, f, nf, pr);
+    case 1024: return launch_y_n<R, 1024, S>(c, f, nf, pr);
   }
   return fail(GHOST_ERR_SIZE, "ny=%d unsupported", c->ny);
 }
@@ -259,7 +320,7 @@ template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int 
 enum XKind { X_HD = 0, X_C2R = 1, X_R2C = 2, X_BOUSS = 3 };
 
 template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void *in, void *out, const void *const *ins,
-                                                       void *const *outs) {
+                                                       void *const *outs, int rows) {
   constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
   constexpr int M = NX / 2, T = M / E;
   // rows of BZ z values; at most 256 threads so the register-resident
@@ -273,15 +334,19 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
   if (KIND == X_HD || KIND == X_BOUSS) {
     constexpr int PHYS = KIND == X_HD ? 0 : 1;
     constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
-    const size_t smem = (size_t)(NX + 2 * (M + 1) * BZ + M * BZ) * sizeof(C);
-    auto kern = xpass_nl_kernel<R, NX, E, BZ, PHYS>;
+    using G = XGeom<R, NX, BZ>;
+    constexpr int STAGES = G::smem_bytes(4) <= 110 * 1024 ? 4 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
+    const size_t smem = G::smem_bytes(STAGES);
+    auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES>;
     GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CFields<R> fi{};
     Fields<R> fo{};
     for (int q = 0; q < NIN; ++q) fi.p[q] = (const C *)ins[q];
     for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
     const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
-    kern<<<grid, NT, smem, c->stream>>>(fi, fo, tw, c->ny, c->nz, (R)1 / (nn * nn));
+    const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny);
+    kern<<<pgrid, NT, smem, c->stream>>>(fi, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), rows > 0 ? rows : M + 1,
+                                         pipe_ctl(c));
   } else if (KIND == X_C2R) {
     const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
     auto kern = xpass_c2r_kernel<R, NX, E, BZ>;
@@ -298,17 +363,97 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
 }
 
 template <typename R, int KIND>
-int launch_x(ghost_ctx *c, const void *in, void *out, const void *const *ins = nullptr, void *const *outs = nullptr) {
+int launch_x(ghost_ctx *c, const void *in, void *out, const void *const *ins = nullptr, void *const *outs = nullptr,
+             int rows = 0) {
   switch (c->nx) {
-    case 16: return launch_x_n<R, 16, KIND>(c, in, out, ins, outs);
-    case 32: return launch_x_n<R, 32, KIND>(c, in, out, ins, outs);
-    case 64: return launch_x_n<R, 64, KIND>(c, in, out, ins, outs);
-    case 128: return launch_x_n<R, 128, KIND>(c, in, out, ins, outs);
-    case 256: return launch_x_n<R, 256, KIND>(c, in, out, ins, outs);
-    case 512: return launch_x_n<R, 512, KIND>(c, in, out, ins, outs);
-    case 1024: return launch_x_n<R, 1024, KIND>(c, in, out, ins, outs);
+    case 16: return launch_x_n<R, 16, KIND>(c, in, out, ins, outs, rows);
+    case 32: return launch_x_n<R, 32, KIND>(c, in, out, ins, outs, rows);
+    case 64: return launch_x_n<R, 64, KIND>(c, in, out, ins, outs, rows);
+    case 128: return launch_x_n<R, 128, KIND>(c, in, out, ins, outs, rows);
+    case 256: return launch_x_n<R, 256, KIND>(c, in, out, ins, outs, rows);
+    case 512: return launch_x_n<R, 512, KIND>(c, in, out, ins, outs, rows);
+    case 1024: return launch_x_n<R, 1024, KIND>(c, in, out, ins, outs, rows);
   }
   return fail(GHOST_ERR_SIZE, "nx=%d unsupported", c->nx);
+}
+
+// ---------------------------------------------------------------------
+// zero-pruning tables.  After a substep, v is exactly zero outside
+// tiny <= kn2 <= kmax.  kn2 grows with |kz|, so a z-line (j,i) holds live
+// modes iff its kz = 0 entry has kn2 <= kmax; at fixed kx the live ky form
+// a run from j = 0 up and a run from j = ny-1 down.  The tables are built
+// with kn2 evaluated exactly as the kernels evaluate it; if the live set
+// does not have that shape (an unusual kmax), pruning is disabled.
+template <typename R> int build_prune(ghost_ctx *c) {
+  const KParams<R> &kp = kparams<R>(c);
+  auto kn2h = [&](int i, int j) -> R {
+    const R a = (R)(i < kp.nx / 2 ? i : i - kp.nx), b = (R)(j < kp.ny / 2 ? j : j - kp.ny);
+    volatile R aa = a * a, bb = b * b;  // no contraction: same rounding as the kernels
+    if (kp.anis) {
+      volatile R x = kp.rmp * aa, y = kp.rmq * bb;
+      volatile R s = x + y;
+      return s + (R)0;
+    }
+    volatile R s = aa + bb;
+    return s + (R)0;
+  };
+  const int nxh = c->nxh, ny = c->ny;
+  std::vector<int> jpos(nxh, 0), jneg(nxh, 0), lines;
+  bool ok = true;
+  int imax = -1;
+  for (int i = 0; i < nxh; ++i) {
+    int p = 0;
+    while (p < ny / 2 && kn2h(i, p) <= kp.kmax) ++p;
+    int q = 0;
+    while (q < ny - ny / 2 && kn2h(i, ny - 1 - q) <= kp.kmax) ++q;
+    jpos[i] = p;
+    jneg[i] = q;
+    for (int j = 0; j < ny; ++j) {
+      const bool live = kn2h(i, j) <= kp.kmax;
+      const bool said = j < p || j >= ny - q;
+      if (live != said) ok = false;
+      if (live) lines.push_back(j + ny * i);
+    }
+    if (p + q > 0) {
+      if (imax != i - 1) ok = false;  // live kx indices must be 0..imax
+      imax = i;
+    }
+  }
+  c->prune_ok = ok && imax >= 0;
+  c->prune_valid = true;
+  if (!c->prune_ok) return GHOST_OK;
+  const int n = (int)lines.size();
+  const int padded = (n + 255) / 256 * 256;
+  lines.resize(padded, -1);
+  if (c->prune_lines) cudaFree(c->prune_lines);
+  if (c->prune_jpos) cudaFree(c->prune_jpos);
+  if (c->prune_jneg) cudaFree(c->prune_jneg);
+  c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
+  GB_CHECK(dalloc((void **)&c->prune_lines, sizeof(int) * padded));
+  GB_CHECK(dalloc((void **)&c->prune_jpos, sizeof(int) * nxh));
+  GB_CHECK(dalloc((void **)&c->prune_jneg, sizeof(int) * nxh));
+  GB_CUDA(cudaMemcpy(c->prune_lines, lines.data(), sizeof(int) * padded, cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(c->prune_jpos, jpos.data(), sizeof(int) * nxh, cudaMemcpyHostToDevice));
+  GB_CUDA(cudaMemcpy(c->prune_jneg, jneg.data(), sizeof(int) * nxh, cudaMemcpyHostToDevice));
+  c->prune_nlines = n;
+  c->prune_imax = imax;
+  return GHOST_OK;
+}
+
+// Pruning plan for a substep whose input fields are zero outside the
+// truncation; an empty plan (full passes) when want == false.
+template <typename R> int prune_plan(ghost_ctx *c, bool want, Prune *pr) {
+  *pr = Prune();
+  if (!want) return GHOST_OK;
+  if (!c->prune_valid) GB_CHECK(build_prune<R>(c));
+  if (!c->prune_ok) return GHOST_OK;
+  pr->lines = c->prune_lines;
+  pr->nlines = c->prune_nlines;
+  pr->jpos = c->prune_jpos;
+  pr->jneg = c->prune_jneg;
+  pr->ni = c->prune_imax + 1;
+  pr->rows = c->prune_imax + 1;
+  return GHOST_OK;
 }
 
 // ---------------------------------------------------------------------
@@ -318,22 +463,18 @@ template <typename R> int r2c_dev(ghost_ctx *c, const void *in, void *out) {
   Fields<R> f{};
   f.p[0] = (cx<R> *)out;
   GB_CHECK((launch_y<R, -1>(c, f, 1)));
-  ZC2C<R, -1> op{};
+  ZC2C<R, -1, 1> op{};
   op.in.p[0] = (const cx<R> *)out;
   op.out.p[0] = (cx<R> *)out;
-  op.nf = 1;
-  op.nz = c->nz;
   return launch_z<R>(c, op);
 }
 
 template <typename R> int c2r_dev(ghost_ctx *c, const void *in, void *out) {
   void *w[1];
   GB_CHECK(scratch(c, 1, w));
-  ZC2C<R, +1> op{};
+  ZC2C<R, +1, 1> op{};
   op.in.p[0] = (const cx<R> *)in;
   op.out.p[0] = (cx<R> *)w[0];
-  op.nf = 1;
-  op.nz = c->nz;
   GB_CHECK(launch_z<R>(c, op));
   Fields<R> f{};
   f.p[0] = (cx<R> *)w[0];
@@ -358,14 +499,12 @@ template <typename R> int prodre3_dev(ghost_ctx *c, const void *a, const void *b
   GB_CHECK((launch_y<R, +1>(c, fy, 6)));
   GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
   GB_CHECK((launch_y<R, -1>(c, fy, 3)));
-  ZC2C<R, -1> zf{};
+  ZC2C<R, -1, 3> zf{};
   void *outs[3] = {d, e, f};
   for (int q = 0; q < 3; ++q) {
     zf.in.p[q] = (const cx<R> *)w[q];
     zf.out.p[q] = (cx<R> *)outs[q];
   }
-  zf.nf = 3;
-  zf.nz = c->nz;
   return launch_z<R>(c, zf);
 }
 
@@ -373,9 +512,11 @@ template <typename R> int prodre3_dev(ghost_ctx *c, const void *a, const void *b
 // hd_rkstep1 folded in when copy != 0.
 template <typename R>
 int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], void *const C[3], const void *const f[3],
-                   int copy) {
+                   int copy, bool prune = false) {
   void *w[6];
   GB_CHECK(scratch(c, 6, w));
+  Prune pr;
+  GB_CHECK(prune_plan<R>(c, prune, &pr));
   ZInv<R, 0> zi{};
   for (int q = 0; q < 3; ++q) {
     zi.v.p[q] = (const cx<R> *)v[q];
@@ -384,12 +525,12 @@ int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], 
   for (int q = 0; q < 6; ++q) zi.w.p[q] = (cx<R> *)w[q];
   zi.kp = kparams<R>(c);
   zi.copy = copy;
-  GB_CHECK(launch_z<R>(c, zi));
+  GB_CHECK(launch_z<R>(c, zi, pr));
   Fields<R> fy{};
   for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
-  GB_CHECK((launch_y<R, +1>(c, fy, 6)));
-  GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
-  GB_CHECK((launch_y<R, -1>(c, fy, 3)));
+  GB_CHECK((launch_y<R, +1>(c, fy, 6, pr)));
+  GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w, pr.rows)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 3, pr)));
   ZFwdHD<R> zf{};
   for (int q = 0; q < 3; ++q) {
     zf.nl.p[q] = (const cx<R> *)w[q];
@@ -401,16 +542,19 @@ int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], 
   zf.dt = (R)dt;
   zf.nu = (R)nu;
   zf.rmp = (R)1 / (R)o;
-  return launch_z<R>(c, zf);
+  return launch_z<R>(c, zf, pr);
 }
 
 // One Boussinesq substep (include/rotbouss_rkstep2.f90) on device
 // pointers: v[0..2] velocity, v[3] theta; C[0..3] the RK1 copies (C20 last).
 template <typename R>
 int bouss_substep_dev(ghost_ctx *c, int o, double dt, double nu, double kappa, double omegaz, double xmom,
-                      double xtemp, void *const v[4], void *const C[4], const void *const f[4], int copy) {
+                      double xtemp, void *const v[4], void *const C[4], const void *const f[4], int copy,
+                      bool prune = false) {
   void *w[9];
   GB_CHECK(scratch(c, 9, w));
+  Prune pr;
+  GB_CHECK(prune_plan<R>(c, prune, &pr));
   ZInv<R, 1> zi{};
   for (int q = 0; q < 4; ++q) {
     zi.v.p[q] = (const cx<R> *)v[q];
@@ -419,12 +563,12 @@ int bouss_substep_dev(ghost_ctx *c, int o, double dt, double nu, double kappa, d
   for (int q = 0; q < 9; ++q) zi.w.p[q] = (cx<R> *)w[q];
   zi.kp = kparams<R>(c);
   zi.copy = copy;
-  GB_CHECK(launch_z<R>(c, zi));
+  GB_CHECK(launch_z<R>(c, zi, pr));
   Fields<R> fy{};
   for (int q = 0; q < 9; ++q) fy.p[q] = (cx<R> *)w[q];
-  GB_CHECK((launch_y<R, +1>(c, fy, 9)));
-  GB_CHECK((launch_x<R, X_BOUSS>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w)));
-  GB_CHECK((launch_y<R, -1>(c, fy, 4)));
+  GB_CHECK((launch_y<R, +1>(c, fy, 9, pr)));
+  GB_CHECK((launch_x<R, X_BOUSS>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w, pr.rows)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 4, pr)));
   ZFwdBouss<R> zf{};
   for (int q = 0; q < 4; ++q) {
     zf.nl.p[q] = (const cx<R> *)w[q];
@@ -440,7 +584,7 @@ int bouss_substep_dev(ghost_ctx *c, int o, double dt, double nu, double kappa, d
   zf.xmom = (R)xmom;
   zf.xtemp = (R)xtemp;
   zf.rmp = (R)1 / (R)o;
-  return launch_z<R>(c, zf);
+  return launch_z<R>(c, zf, pr);
 }
 
 // advect3 on device pointers: e = -(A.grad)d via the fused Boussinesq
@@ -466,11 +610,9 @@ int advect3_dev(ghost_ctx *c, const void *a, const void *b, const void *cc, cons
   Fields<R> f1{};
   f1.p[0] = (cx<R> *)w[3];
   GB_CHECK((launch_y<R, -1>(c, f1, 1)));
-  ZC2C<R, -1> zf{};
+  ZC2C<R, -1, 1> zf{};
   zf.in.p[0] = (const cx<R> *)w[3];
   zf.out.p[0] = (cx<R> *)e;
-  zf.nf = 1;
-  zf.nz = c->nz;
   return launch_z<R>(c, zf);
 }
 
@@ -493,7 +635,7 @@ int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void 
   GB_CHECK(post_launch(c));
   GB_CUDA(cudaMemcpyAsync(out_host, part + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   GB_CUDA(cudaStreamSynchronize(c->stream));
-  return GHOST_OK;
+  return check_status(c);
 }
 
 template <typename R>
@@ -758,6 +900,12 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->partials_elems = 0;
   for (int q = 0; q < 4; ++q) c->rk[q] = nullptr;
   c->timers_on = false;
+  c->num_sms = 0;
+  c->status = nullptr;
+  c->wait_cap = 1u << 22;
+  c->prune_valid = c->prune_ok = false;
+  c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
+  c->prune_nlines = c->prune_imax = 0;
   for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
     c->t_ms[k] = 0.0;
     c->t_n[k] = 0;
@@ -768,6 +916,10 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
     return s;
   }
   refresh_kparams(c);
+  if (dalloc((void **)&c->status, sizeof(int)) != GHOST_OK || cudaMemset(c->status, 0, sizeof(int)) != cudaSuccess) {
+    ghost_ctx_destroy(c);
+    return fail(GHOST_ERR_ALLOC, "status word allocation failed");
+  }
   *out = c;
   return GHOST_OK;
 }
@@ -784,6 +936,10 @@ int ghost_ctx_destroy(ghost_ctx *c) {
   cudaFree(c->tw_y);
   cudaFree(c->tw_z);
   cudaFree(c->partials);
+  cudaFree(c->status);
+  cudaFree(c->prune_lines);
+  cudaFree(c->prune_jpos);
+  cudaFree(c->prune_jneg);
   for (auto &p : c->ev_pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -827,12 +983,19 @@ int ghost_ctx_set_kmax(ghost_ctx *c, double kmax) {
   CTX_CHECK(c);
   c->kmax = c->precision == GHOST_SINGLE ? (double)(float)kmax : kmax;
   refresh_kparams(c);
+  c->prune_valid = false;
   return GHOST_OK;
 }
 
 int ghost_ctx_synchronize(ghost_ctx *c) {
   CTX_CHECK(c);
   GB_CUDA(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int ghost_ctx_set_wait_cap(ghost_ctx *c, unsigned int cap) {
+  CTX_CHECK(c);
+  c->wait_cap = cap ? cap : (1u << 22);
   return GHOST_OK;
 }
 
@@ -1186,10 +1349,16 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
       Cd[q] = c->rk[q];
     }
   }
+  // The first substep of a call reads v on the whole grid (it may hold
+  // modes outside the truncation); its update leaves v zero there, so the
+  // later substeps skip the known zeros.
   for (int t = 0; t < nsteps; ++t)
-    for (int o = ord; o >= 1; --o)
-      GB_CHECK(c->precision == GHOST_SINGLE ? hd_substep_dev<float>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord)
-                                            : hd_substep_dev<double>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord));
+    for (int o = ord; o >= 1; --o) {
+      const bool prune = !(t == 0 && o == ord);
+      GB_CHECK(c->precision == GHOST_SINGLE
+                   ? hd_substep_dev<float>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord, prune)
+                   : hd_substep_dev<double>(c, o, dt, nu, v, Cd, fx ? f : nullptr, o == ord, prune));
+    }
   return st.finish();
 }
 
@@ -1279,12 +1448,14 @@ int ghost_bouss_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, dou
     Cd[q] = c->rk[q];
   }
   for (int t = 0; t < nsteps; ++t)
-    for (int o = ord; o >= 1; --o)
+    for (int o = ord; o >= 1; --o) {
+      const bool prune = !(t == 0 && o == ord);
       GB_CHECK(c->precision == GHOST_SINGLE
                    ? bouss_substep_dev<float>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr,
-                                              o == ord)
+                                              o == ord, prune)
                    : bouss_substep_dev<double>(c, o, dt, nu, kappa, omegaz, xmom, xtemp, v, Cd, have_f ? f : nullptr,
-                                               o == ord));
+                                               o == ord, prune));
+    }
   return st.finish();
 }
 

@@ -107,6 +107,16 @@ struct ghost_ctx {
   void *rk[4];
   gb::KParams<float> kp32;
   gb::KParams<double> kp64;
+  int num_sms;
+  // device status word written by kernels whose bounded waits ran out
+  int *status;
+  uint32_t wait_cap;
+  // zero-pruning tables of the 2/3 truncation (built on first use):
+  // active (j,i) z-lines padded with -1 to a multiple of 256, the
+  // contiguous live y-wavenumber counts per kx index, and the last live kx
+  bool prune_valid, prune_ok;
+  int *prune_lines, *prune_jpos, *prune_jneg;
+  int prune_nlines, prune_imax;
   // per-kernel timers (ghost_ctx_enable_timers)
   bool timers_on;
   std::vector<cudaEvent_t> ev_free;

@@ -15,6 +15,7 @@
 // spectral -> real (6 fields) -> omega x v -> spectral (3 fields).
 #pragma once
 #include "common.cuh"
+#include "pipeline.cuh"
 
 namespace gb {
 
@@ -37,56 +38,122 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 }
 
 // ====================================================================
-// Z pass
+// Z pass: persistent CTAs stream tiles of LPB z-lines (each line one bulk
+// copy of N values per loaded field) through STAGES shared-memory buffers.
 // ====================================================================
-template <int N, int E> struct ZShape {
+template <typename R, int N, int E, int LPB, int NL> struct ZGeom {
   static constexpr int T = N / E;
-  static constexpr int NP = N + N / 8;  // padded line: idx + idx/8 spreads strided writes over banks
+  static constexpr int NT = LPB * T;
+  static constexpr int NP = N + N / 8;  // padded exchange line: idx + idx/8 spreads strided writes
+  static constexpr size_t stage_elems = (size_t)NL * LPB * N;
+  static constexpr size_t smem_bytes(int stages) {
+    return (stages * stage_elems + N + (size_t)LPB * NP) * sizeof(cx<R>) + 8 * stages;
+  }
 };
 
-// Generic shell: twiddles to shared memory, per-line buffer accessor, then
-// the operation's body.  nlines must be a multiple of LPB (host checks).
-template <typename R, int N, int E, class Op>
-__global__ void __launch_bounds__(256) zpass_kernel(Op op, const cx<R> *__restrict__ twg, int lpb) {
+struct PipeCtl {
+  int *status;    // device status word (GHOST_ERR_TIMEOUT on a timed-out wait)
+  uint32_t cap;   // polls before a wait gives up
+};
+
+// lines != nullptr: the pass covers the listed (j,i) lines only (entries
+// < 0 pad the list); otherwise lines 0..nlines-1.
+template <typename R, int N, int E, int LPB, int STAGES, class Op>
+__global__ void __launch_bounds__(LPB *(N / E)) zpipe_kernel(Op op, const cx<R> *__restrict__ twg,
+                                                              const int *__restrict__ lines, int nlines,
+                                                              PipeCtl ctl) {
   using C = cx<R>;
-  constexpr int T = ZShape<N, E>::T, NP = ZShape<N, E>::NP;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *tw = reinterpret_cast<C *>(smem_raw);
+  using G = ZGeom<R, N, E, LPB, Op::NLOAD>;
+  constexpr int T = G::T, NT = G::NT, NP = G::NP, NL = Op::NLOAD;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C *stage = reinterpret_cast<C *>(smem_raw);
+  C *tw = stage + STAGES * G::stage_elems;
   C *xb = tw + N;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + LPB * NP);
   const int tid = threadIdx.x, lq = tid / T, t = tid - lq * T;
-  for (int e = tid; e < N; e += blockDim.x) tw[e] = twg[e];
+  const int ntiles = (nlines + LPB - 1) / LPB;
+  if (tid == 0) {
+    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    fence_barrier_init();
+  }
+  for (int e = tid; e < N; e += NT) tw[e] = twg[e];
   __syncthreads();
-  const long line = (long)blockIdx.x * lpb + lq;
+  auto line_of = [&](int tile, int l) -> long {
+    const long idx = (long)tile * LPB + l;
+    if (idx >= nlines) return -1;
+    return lines ? (long)lines[idx] : idx;
+  };
+  auto issue = [&](int k) {
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) return;
+    const int s = k % STAGES;
+    if (tid == 0) {
+      uint32_t bytes = 0;
+      for (int l = 0; l < LPB; ++l)
+        if (line_of(tile, l) >= 0) bytes += NL * N * (uint32_t)sizeof(C);
+      mbar_arrive_expect_tx(&bars[s], bytes);
+    }
+    for (int q = tid; q < NL * LPB; q += NT) {
+      const int f = q / LPB, l = q - f * LPB;
+      const long line = line_of(tile, l);
+      if (line >= 0)
+        bulk_g2s(stage + ((size_t)(s * NL + f) * LPB + l) * N, op.load_src(f) + (size_t)line * N,
+                 N * (uint32_t)sizeof(C), &bars[s]);
+    }
+  };
+  for (int k = 0; k < STAGES - 1; ++k) issue(k);
   C *mine = xb + lq * NP;
   auto buf = [mine](int idx) -> C & { return mine[idx + (idx >> 3)]; };
   auto sync = [] { __syncthreads(); };
-  op.template body<N, E>(line, t, tw, buf, sync);
+  for (int k = 0;; ++k) {
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) break;
+    fence_proxy_async();
+    issue(k + STAGES - 1);
+    const int s = k % STAGES;
+    const bool ok = mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) record_timeout(ctl.status);
+      for (int kk = k; kk < k + STAGES; ++kk)
+        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
+      return;
+    }
+    const long line = line_of(tile, lq);
+    const bool act = line >= 0;
+    const C *in0 = stage + ((size_t)(s * NL) * LPB + lq) * N;
+    auto in = [in0](int f) -> const C * { return in0 + (size_t)f * LPB * N; };
+    op.template body<N, E>(act ? line : 0, act, t, tw, buf, sync, in);
+    __syncthreads();
+  }
 }
 
-// In-place (or out-of-place) c2c along z of nf fields.
-template <typename R, int S> struct ZC2C {
+// Plain c2c along z of NF fields (in -> out, may alias).
+template <typename R, int S, int NF> struct ZC2C {
   using C = cx<R>;
+  static constexpr int NLOAD = NF;
   CFields<R> in;
   Fields<R> out;
-  int nf, nz;
-  template <int N, int E, class Buf, class Sync>
-  __device__ __forceinline__ void body(long line, int t, const C *tw, Buf buf, Sync sync) const {
+  __device__ __forceinline__ const C *load_src(int f) const { return in.p[f]; }
+  template <int N, int E, class Buf, class Sync, class In>
+  __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    for (int f = 0; f < nf; ++f) {
-      const C *src = in.p[f] + (size_t)line * N;
-      C *dst = out.p[f] + (size_t)line * N;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
       C x[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = src[t + T * e];
+      for (int e = 0; e < E; ++e) x[e] = src(f)[t + T * e];
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
+      if (act) {
+        C *dst = out.p[f] + (size_t)line * N;
 #pragma unroll
-      for (int e = 0; e < E; ++e) dst[t + T * e] = x[e];
+        for (int e = 0; e < E; ++e) dst[t + T * e] = x[e];
+      }
     }
   }
 };
 
-// Inverse prologue of the fused substep: reads v (and theta for the
-// Boussinesq solver), forms per mode the fields the real-space products
+// Inverse prologue of the fused substep: from v (and theta for the
+// Boussinesq solver) it forms per mode the fields the real-space products
 // need and runs the inverse z transform of each:
 //   PHYS 0 (HD):    v, curl v                       (prodre3 inputs)
 //   PHYS 1 (BOUSS): v, curl v, i k theta            (prodre3 + advect3 inputs)
@@ -96,51 +163,57 @@ template <typename R, int PHYS> struct ZInv {
   using C = cx<R>;
   static constexpr int NIN = PHYS == 0 ? 3 : 4;
   static constexpr int NOUT = PHYS == 0 ? 6 : 9;
+  static constexpr int NLOAD = NIN;
   CFields<R> v;   // NIN
   Fields<R> w;    // NOUT outputs
   Fields<R> cpy;  // NIN (when copy)
   KParams<R> kp;
   int copy;
-  template <int N, int E, class Buf, class Sync>
-  __device__ __forceinline__ void body(long line, int t, const C *tw, Buf buf, Sync sync) const {
+  __device__ __forceinline__ const C *load_src(int f) const { return v.p[f]; }
+  template <int N, int E, class Buf, class Sync, class In>
+  __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
     const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
-    C a[NIN][E];
-#pragma unroll
-    for (int c = 0; c < NIN; ++c)
-#pragma unroll
-      for (int e = 0; e < E; ++e) a[c][e] = v.p[c][(size_t)line * N + t + T * e];
-    if (copy) {
+    if (copy && act) {
 #pragma unroll
       for (int c = 0; c < NIN; ++c)
 #pragma unroll
-        for (int e = 0; e < E; ++e) cpy.p[c][(size_t)line * N + t + T * e] = a[c][e];
+        for (int e = 0; e < E; ++e) cpy.p[c][(size_t)line * N + t + T * e] = src(c)[t + T * e];
     }
-#pragma unroll 1
+#pragma unroll
     for (int f = 0; f < NOUT; ++f) {
       C x[E];
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        const R kz = kz_of(kp, t + T * e);
+        const int k = t + T * e;
+        const R kz = kz_of(kp, k);
         if (f < 3) {
-          x[e] = a[f][e];
+          x[e] = src(f)[k];
         } else if (f < 6) {
           // i k a = (-k a.y, k a.x)
-          const C vx = a[0][e], vy = a[1][e], vz = a[2][e];
-          if (f == 3) x[e] = mk((-ky * vz.y) - (-kz * vy.y), (ky * vz.x) - (kz * vy.x));
-          else if (f == 4) x[e] = mk((-kz * vx.y) - (-kx * vz.y), (kz * vx.x) - (kx * vz.x));
-          else x[e] = mk((-kx * vy.y) - (-ky * vx.y), (kx * vy.x) - (ky * vx.x));
+          if (f == 3) {
+            const C vy = src(1)[k], vz = src(2)[k];
+            x[e] = mk((-ky * vz.y) - (-kz * vy.y), (ky * vz.x) - (kz * vy.x));
+          } else if (f == 4) {
+            const C vx = src(0)[k], vz = src(2)[k];
+            x[e] = mk((-kz * vx.y) - (-kx * vz.y), (kz * vx.x) - (kx * vz.x));
+          } else {
+            const C vx = src(0)[k], vy = src(1)[k];
+            x[e] = mk((-kx * vy.y) - (-ky * vx.y), (kx * vy.x) - (ky * vx.x));
+          }
         } else {
-          const C th = a[NIN - 1][e];
+          const C th = src(NIN - 1)[k];
           const R kd = f == 6 ? kx : (f == 7 ? ky : kz);
           x[e] = mk(-(kd * th.y), kd * th.x);
         }
       }
       line_fft<C, N, E, +1>(x, t, tw, buf, sync);
-      C *dst = w.p[f] + (size_t)line * N;
+      if (act) {
+        C *dst = w.p[f] + (size_t)line * N;
 #pragma unroll
-      for (int e = 0; e < E; ++e) dst[t + T * e] = x[e];
+        for (int e = 0; e < E; ++e) dst[t + T * e] = x[e];
+      }
     }
   }
 };
@@ -150,27 +223,27 @@ template <typename R, int PHYS> struct ZInv {
 // the truncated RK update of include/hd_rkstep2.f90:18-38, written to v.
 template <typename R> struct ZFwdHD {
   using C = cx<R>;
+  static constexpr int NLOAD = 3;
   CFields<R> nl;  // 3 (x and y transformed)
   Fields<R> v;    // 3 in/out
   CFields<R> c0;  // C1..C3
   CFields<R> f;   // forcing or null
   KParams<R> kp;
   R dt, nu, rmp;
-  template <int N, int E, class Buf, class Sync>
-  __device__ __forceinline__ void body(long line, int t, const C *tw, Buf buf, Sync sync) const {
+  __device__ __forceinline__ const C *load_src(int q) const { return nl.p[q]; }
+  template <int N, int E, class Buf, class Sync, class In>
+  __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
     const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     C g[3][E];
-#pragma unroll 1
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
-      C x[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = nl.p[c][(size_t)line * N + t + T * e];
-      line_fft<C, N, E, -1>(x, t, tw, buf, sync);
-#pragma unroll
-      for (int e = 0; e < E; ++e) g[c][e] = x[e];
+      for (int e = 0; e < E; ++e) g[c][e] = src(c)[t + T * e];
+      line_fft<C, N, E, -1>(g[c], t, tw, buf, sync);
     }
+    if (!act) return;
     const bool forced = f.p[0] != nullptr;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -212,27 +285,27 @@ template <typename R> struct ZFwdHD {
 // Laplacians and the three-way truncated update (theta keeps its mean).
 template <typename R> struct ZFwdBouss {
   using C = cx<R>;
+  static constexpr int NLOAD = 4;
   CFields<R> nl;  // 4: (w x v)_xyz, -v.grad(theta)
   Fields<R> v;    // 4 in/out: vx, vy, vz, theta
   CFields<R> c0;  // C1..C3, C20
   CFields<R> f;   // fx, fy, fz, fs (any null: zero)
   KParams<R> kp;
   R dt, nu, kappa, omegaz, xmom, xtemp, rmp;
-  template <int N, int E, class Buf, class Sync>
-  __device__ __forceinline__ void body(long line, int t, const C *tw, Buf buf, Sync sync) const {
+  __device__ __forceinline__ const C *load_src(int q) const { return nl.p[q]; }
+  template <int N, int E, class Buf, class Sync, class In>
+  __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
     const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     C g[4][E];
-#pragma unroll 1
+#pragma unroll
     for (int c = 0; c < 4; ++c) {
-      C x[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = nl.p[c][(size_t)line * N + t + T * e];
-      line_fft<C, N, E, -1>(x, t, tw, buf, sync);
-#pragma unroll
-      for (int e = 0; e < E; ++e) g[c][e] = x[e];
+      for (int e = 0; e < E; ++e) g[c][e] = src(c)[t + T * e];
+      line_fft<C, N, E, -1>(g[c], t, tw, buf, sync);
     }
+    if (!act) return;
     const bool forced = f.p[0] != nullptr, sforced = f.p[3] != nullptr;
     const R two_om = (R)2 * omegaz;
 #pragma unroll
@@ -280,29 +353,117 @@ template <typename R> struct ZFwdBouss {
 };
 
 // ====================================================================
-// Y pass: in place c2c along y of nf fields
+// Y pass: persistent CTAs stream tiles of BZ z-lines x N y-rows of one
+// field at one kx index (row j: BZ contiguous values, one bulk copy).  The
+// tile's stage buffer then serves as the line-interleaved FFT exchange
+// buffer, so a tile costs one trip through shared memory.
+// With jpos/jneg (pruned passes) only rows j < jpos[i] or j >= N - jneg[i]
+// can be non-zero: the inverse pass loads only those, the forward pass
+// writes only those (the rest are never read).
 // ====================================================================
-template <typename R, int N, int E, int S>
-__global__ void __launch_bounds__(1024) ypass_kernel(Fields<R> fld, const cx<R> *__restrict__ twg, int nz,
-                                                     int bz) {
+template <typename R, int N, int E, int BZ> struct YGeom {
+  static constexpr int T = N / E;
+  static constexpr int NT = BZ * T;
+  static constexpr size_t stage_elems = (size_t)BZ * N;
+  static constexpr size_t smem_bytes(int stages) { return (stages * stage_elems + N) * sizeof(cx<R>) + 8 * stages; }
+};
+
+template <typename R, int N, int E, int BZ, int STAGES, int S>
+__global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(Fields<R> fld, const cx<R> *__restrict__ twg, int nz,
+                                                             int ni, int nf, const int *__restrict__ jpos,
+                                                             const int *__restrict__ jneg, PipeCtl ctl) {
   using C = cx<R>;
-  constexpr int T = N / E;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *tw = reinterpret_cast<C *>(smem_raw);
-  C *xb = tw + N;
-  const int tid = threadIdx.x, l = tid % bz, t = tid / bz;
-  for (int e = tid; e < N; e += blockDim.x) tw[e] = twg[e];
+  using G = YGeom<R, N, E, BZ>;
+  constexpr int T = G::T, NT = G::NT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C *stage = reinterpret_cast<C *>(smem_raw);
+  C *tw = stage + STAGES * G::stage_elems;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tw + N);
+  const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
+  const int nzb = nz / BZ;
+  const int ntiles = nzb * ni * nf;
+  if (tid == 0) {
+    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    fence_barrier_init();
+  }
+  for (int e = tid; e < N; e += NT) tw[e] = twg[e];
   __syncthreads();
-  const int z = blockIdx.x * bz + l, i = blockIdx.y;
-  C *base = fld.p[blockIdx.z] + (size_t)z + (size_t)nz * N * i;
-  C x[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) x[e] = base[(size_t)nz * (t + T * e)];
-  auto buf = [xb, bz, l](int idx) -> C & { return xb[idx * bz + l]; };
+  struct Tile {
+    int zb, i, f;
+  };
+  auto tile_of = [&](int tile) {
+    Tile r;
+    r.zb = tile % nzb;
+    const int q = tile / nzb;
+    r.i = q % ni;
+    r.f = q / ni;
+    return r;
+  };
+  auto rows_of = [&](int i, int &jp, int &jn) {
+    if (jpos && S > 0) {
+      jp = jpos[i];
+      jn = jneg[i];
+    } else {
+      jp = N;
+      jn = 0;
+    }
+  };
+  auto issue = [&](int k) {
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) return;
+    const Tile tl = tile_of(tile);
+    int jp, jn;
+    rows_of(tl.i, jp, jn);
+    const int s = k % STAGES;
+    const int nrows = jp + jn;
+    if (tid == 0) mbar_arrive_expect_tx(&bars[s], (uint32_t)nrows * BZ * (uint32_t)sizeof(C));
+    const C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + (size_t)nz * N * tl.i;
+    C *dst = stage + (size_t)s * G::stage_elems;
+    for (int q = tid; q < nrows; q += NT) {
+      const int jj = q < jp ? q : N - jn + (q - jp);
+      bulk_g2s(dst + (size_t)jj * BZ, base + (size_t)nz * jj, BZ * (uint32_t)sizeof(C), &bars[s]);
+    }
+  };
+  for (int k = 0; k < STAGES - 1; ++k) issue(k);
   auto sync = [] { __syncthreads(); };
-  line_fft<C, N, E, S>(x, t, tw, buf, sync);
+  for (int k = 0;; ++k) {
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) break;
+    fence_proxy_async();
+    issue(k + STAGES - 1);
+    const int s = k % STAGES;
+    const bool ok = mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) record_timeout(ctl.status);
+      for (int kk = k; kk < k + STAGES; ++kk)
+        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
+      return;
+    }
+    const Tile tl = tile_of(tile);
+    int jp = N, jn = 0;
+    if (jpos) {
+      jp = jpos[tl.i];
+      jn = jneg[tl.i];
+    }
+    C *sb = stage + (size_t)s * G::stage_elems;
+    C x[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) base[(size_t)nz * (t + T * e)] = x[e];
+    for (int e = 0; e < E; ++e) {
+      const int jj = t + T * e;
+      const bool live = (S < 0) || jj < jp || jj >= N - jn;
+      x[e] = live ? sb[jj * BZ + l] : mk((R)0, (R)0);
+    }
+    __syncthreads();
+    auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
+    line_fft<C, N, E, S>(x, t, tw, buf, sync);
+    C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * tl.i;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int jj = t + T * e;
+      if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
+    }
+    __syncthreads();
+  }
 }
 
 // ====================================================================
@@ -310,9 +471,9 @@ __global__ void __launch_bounds__(1024) ypass_kernel(Fields<R> fld, const cx<R> 
 // ====================================================================
 // Stage the (M+1) x BZ tile of kx rows at (z0.., j) of one field.
 template <typename C, int BZ>
-__device__ __forceinline__ void x_tile_load(C *tile, const C *src, int M, size_t rowstride, int tid, int nthr) {
+__device__ __forceinline__ void x_tile_load(C *tile, const C *src, int rows, size_t rowstride, int tid, int nthr) {
   constexpr int CH = BZ * (int)sizeof(C) / 16;  // 16-byte chunks per row
-  const int nch = (M + 1) * CH;
+  const int nch = rows * CH;
   for (int q = tid; q < nch; q += nthr) {
     const int row = q / CH, c = q - row * CH;
     cp_async16(reinterpret_cast<unsigned char *>(tile + row * BZ) + 16 * c,
@@ -323,9 +484,12 @@ __device__ __forceinline__ void x_tile_load(C *tile, const C *src, int M, size_t
 // complex-to-real packing of the half spectrum for the M = nx/2 point
 // inverse transform:  Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k/nx} (X_k - conj X_{M-k}),
 // with only the real parts of X_0 and X_M taken.
+// rows: kx rows present in the tile (the rest are zero)
 template <typename C>
-__device__ __forceinline__ C c2r_pack(const C *tile, int bz, int l, int k, int M, const C *tw) {
-  C xk = tile[k * bz + l], xm = tile[(M - k) * bz + l];
+__device__ __forceinline__ C c2r_pack(const C *tile, int bz, int l, int k, int M, int rows, const C *tw) {
+  typedef decltype(C{}.x) R;
+  C xk = k < rows ? tile[k * bz + l] : mk((R)0, (R)0);
+  C xm = (M - k) < rows ? tile[(M - k) * bz + l] : mk((R)0, (R)0);
   if (k == 0) {
     xk.y = 0;
     xm.y = 0;
@@ -357,120 +521,142 @@ template <typename C> __device__ __forceinline__ C r2c_unpack(C zk, C zm, C w) {
 //   PHYS 1 (BOUSS): in v, curl v, grad theta (9)
 //                   -> out omega x v (3), -v.grad(theta) (1)
 //                   (prodre3 + advect3, pseudospec3D_phd.f90:23-114)
-// scale is 1/(nx ny nz)^2; outputs may alias in[0..NOUT-1].
+// A persistent CTA walks (z-block, y) tiles; every input field of a tile
+// is one load of `rows` kx rows (BZ contiguous values each, one bulk copy
+// per row) into a STAGES-deep ring, so the next fields (and the next
+// tile) stream in while the current field is transformed.  scale is
+// 1/(nx ny nz)^2; outputs may alias in[0..NOUT-1]; only kx rows < rows are
+// read (the rest are zero) and written (the rest are never read).
 // ====================================================================
-template <typename R, int NX, int E, int BZ, int PHYS>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_nl_kernel(CFields<R> in, Fields<R> out,
-                                                                    const cx<R> *__restrict__ twg, int ny,
-                                                                    int nz, R scale) {
+template <typename R, int NX, int BZ> struct XGeom {
+  static constexpr int M = NX / 2;
+  static constexpr size_t stage_elems = (size_t)(M + 1) * BZ;
+  static constexpr size_t smem_bytes(int stages) {
+    return (stages * stage_elems + NX + (size_t)M * BZ) * sizeof(cx<R>) + 8 * stages;
+  }
+};
+
+template <typename R, int NX, int E, int BZ, int PHYS, int STAGES>
+__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(CFields<R> in, Fields<R> out,
+                                                                    const cx<R> *__restrict__ twg, int ny, int nz,
+                                                                    R scale, int rows, PipeCtl ctl) {
   using C = cx<R>;
+  using G = XGeom<R, NX, BZ>;
   constexpr int M = NX / 2, T = M / E, NT = BZ * T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *tw = reinterpret_cast<C *>(smem_raw);  // NX
-  C *tile0 = tw + NX;                       // (M+1)*BZ
-  C *tile1 = tile0 + (M + 1) * BZ;
-  C *xb = tile1 + (M + 1) * BZ;             // M*BZ
+  constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C *stage = reinterpret_cast<C *>(smem_raw);
+  C *tw = stage + STAGES * G::stage_elems;
+  C *xb = tw + NX;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + (size_t)M * BZ);
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
-  const int z0 = blockIdx.x * BZ, j = blockIdx.y;
+  const int nzb = nz / BZ;
+  const int ntiles = nzb * ny;
   const size_t rowstride = (size_t)nz * ny;
-  const size_t off = (size_t)z0 + (size_t)nz * j;
+  if (tid == 0) {
+    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    fence_barrier_init();
+  }
   for (int e = tid; e < NX; e += NT) tw[e] = twg[e];
-  x_tile_load<C, BZ>(tile0, in.p[0] + off, M, rowstride, tid, NT);
-  cp_async_commit();
+  __syncthreads();
+  auto issue = [&](int L) {
+    const int k = L / NIN, f = L - k * NIN;
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) return;
+    const int s = L % STAGES;
+    if (tid == 0) mbar_arrive_expect_tx(&bars[s], (uint32_t)rows * BZ * (uint32_t)sizeof(C));
+    const C *src = in.p[f] + (size_t)(tile % nzb) * BZ + (size_t)nz * (tile / nzb);
+    C *dst = stage + (size_t)s * G::stage_elems;
+    for (int r = tid; r < rows; r += NT)
+      bulk_g2s(dst + (size_t)r * BZ, src + rowstride * r, BZ * (uint32_t)sizeof(C), &bars[s]);
+  };
+  for (int L = 0; L < STAGES - 1; ++L) issue(L);
   auto buf = [xb, l](int idx) -> C & { return xb[idx * BZ + l]; };
   auto sync = [] { __syncthreads(); };
-  constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
-  C V[3][E], P[NOUT][E];
-#pragma unroll 1
-  for (int f = 0; f < NIN; ++f) {
-    C *tile = (f & 1) ? tile1 : tile0;
-    if (f + 1 < NIN) {
-      x_tile_load<C, BZ>((f & 1) ? tile0 : tile1, in.p[f + 1] + off, M, rowstride, tid, NT);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    C x[E];
+  for (int k = 0;; ++k) {
+    const int tile = blockIdx.x + k * gridDim.x;
+    if (tile >= ntiles) break;
+    C V[3][E], P[NOUT][E];
+    bool failed = false;
 #pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = c2r_pack(tile, BZ, l, t + T * e, M, tw);
-    line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
-    // x[e] = (r_{2m}, r_{2m+1}) at m = t + T*e
-    switch (f) {
-      case 0:
-      case 1:
-      case 2:
+    for (int f = 0; f < NIN; ++f) {
+      const int L = k * NIN + f;
+      fence_proxy_async();
+      issue(L + STAGES - 1);
+      const bool ok = mbar_wait(&bars[L % STAGES], (uint32_t)(L / STAGES) & 1u, ctl.cap);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) record_timeout(ctl.status);
+        for (int LL = L; LL < L + STAGES; ++LL)
+          if (blockIdx.x + (LL / NIN) * gridDim.x < ntiles)
+            mbar_wait(&bars[LL % STAGES], (uint32_t)(LL / STAGES) & 1u, kDrainPolls);
+        failed = true;
+        break;
+      }
+      const C *sb = stage + (size_t)(L % STAGES) * G::stage_elems;
+      C x[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, BZ, l, t + T * e, M, rows, tw);
+      __syncthreads();  // the stage is consumed: it may be refilled
+      line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
+      // x[e] = (r_{2m}, r_{2m+1}) at m = t + T*e
+      if (f < 3) {
 #pragma unroll
         for (int e = 0; e < E; ++e) V[f][e] = x[e];
-        break;
-      case 3:  // wx: (w x v)_y = wz vx - vz wx ; (w x v)_z = wx vy - vx wy
+      } else if (f == 3) {  // wx: (w x v)_y = wz vx - vz wx ; (w x v)_z = wx vy - vx wy
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           P[1][e] = mk(-(V[2][e].x * x[e].x), -(V[2][e].y * x[e].y));
           P[2][e] = mk(x[e].x * V[1][e].x, x[e].y * V[1][e].y);
         }
-        break;
-      case 4:  // wy: (w x v)_x = wy vz - vy wz
+      } else if (f == 4) {  // wy: (w x v)_x = wy vz - vy wz
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           P[0][e] = mk(x[e].x * V[2][e].x, x[e].y * V[2][e].y);
           P[2][e] = mk(P[2][e].x - V[0][e].x * x[e].x, P[2][e].y - V[0][e].y * x[e].y);
         }
-        break;
-      case 5:  // wz
+      } else if (f == 5) {  // wz
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           P[0][e] = mk((P[0][e].x - V[1][e].x * x[e].x) * scale, (P[0][e].y - V[1][e].y * x[e].y) * scale);
           P[1][e] = mk((x[e].x * V[0][e].x + P[1][e].x) * scale, (x[e].y * V[0][e].y + P[1][e].y) * scale);
           P[2][e] = mk(P[2][e].x * scale, P[2][e].y * scale);
         }
-        break;
-      case 6:  // dtheta/dx: advect3 accumulates vx th_x + vy th_y + vz th_z
-        if constexpr (NOUT > 3) {
+      } else if constexpr (NOUT > 3) {
+        // advect3 accumulates vx th_x + vy th_y + vz th_z, then times -1/(nx ny nz)^2
+        if (f == 6) {
 #pragma unroll
-          for (int e = 0; e < E; ++e) P[3][e] = mk(V[0][e].x * x[e].x, V[0][e].y * x[e].y);
-        }
-        break;
-      case 7:
-        if constexpr (NOUT > 3) {
-#pragma unroll
-          for (int e = 0; e < E; ++e) P[3][e] = mk(P[3][e].x + V[1][e].x * x[e].x, P[3][e].y + V[1][e].y * x[e].y);
-        }
-        break;
-      default:  // 8: times -1/(nx ny nz)^2
-        if constexpr (NOUT > 3) {
+          for (int e = 0; e < E; ++e) P[NOUT - 1][e] = mk(V[0][e].x * x[e].x, V[0][e].y * x[e].y);
+        } else if (f == 7) {
 #pragma unroll
           for (int e = 0; e < E; ++e)
-            P[3][e] = mk((P[3][e].x + V[2][e].x * x[e].x) * -scale, (P[3][e].y + V[2][e].y * x[e].y) * -scale);
+            P[NOUT - 1][e] = mk(P[NOUT - 1][e].x + V[1][e].x * x[e].x, P[NOUT - 1][e].y + V[1][e].y * x[e].y);
+        } else {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            P[NOUT - 1][e] = mk((P[NOUT - 1][e].x + V[2][e].x * x[e].x) * -scale,
+                                (P[NOUT - 1][e].y + V[2][e].y * x[e].y) * -scale);
         }
-        break;
-    }
-    __syncthreads();  // every thread is done with this tile before it is refilled
-  }
-  // forward: real-to-complex lines of the products
-#pragma unroll 1
-  for (int c = 0; c < NOUT; ++c) {
-    C x[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = P[c][e];
-    line_fft<C, M, E, -1, 2>(x, t, tw, buf, sync);
-#pragma unroll
-    for (int e = 0; e < E; ++e) buf(t + T * e) = x[e];
-    __syncthreads();
-    C *dst = out.p[c] + off + l;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int k = t + T * e;
-      const C zk = buf(k), zm = buf((M - k) & (M - 1));
-      dst[rowstride * k] = r2c_unpack(zk, zm, tw[k]);
-      if (k == 0) {
-        // X_M = F_0 - G_0
-        const C x0 = r2c_unpack(zk, zm, mk((R)-1, (R)0));
-        dst[rowstride * M] = x0;
       }
     }
-    __syncthreads();
+    if (failed) return;
+    // forward: real-to-complex lines of the products
+    C *obase = nullptr;
+#pragma unroll
+    for (int c = 0; c < NOUT; ++c) {
+      line_fft<C, M, E, -1, 2>(P[c], t, tw, buf, sync);
+#pragma unroll
+      for (int e = 0; e < E; ++e) buf(t + T * e) = P[c][e];
+      __syncthreads();
+      obase = out.p[c] + (size_t)(tile % nzb) * BZ + (size_t)nz * (tile / nzb) + l;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int kk = t + T * e;
+        const C zk = buf(kk), zm = buf((M - kk) & (M - 1));
+        if (kk < rows) obase[rowstride * kk] = r2c_unpack(zk, zm, tw[kk]);
+        if (kk == 0 && M < rows) obase[rowstride * M] = r2c_unpack(zk, zm, mk((R)-1, (R)0));
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -486,7 +672,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_kernel(const cx<R>
                                                                      int nz) {
   using C = cx<R>;
   constexpr int M = NX / 2, T = M / E, NT = BZ * T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
   C *tile = tw + NX;
   C *xb = tile + (M + 1) * BZ;
@@ -494,7 +680,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_kernel(const cx<R>
   const int z0 = blockIdx.x * BZ, j = blockIdx.y;
   const size_t rowstride = (size_t)nz * ny;
   for (int e = tid; e < NX; e += NT) tw[e] = twg[e];
-  x_tile_load<C, BZ>(tile, in + (size_t)z0 + (size_t)nz * j, M, rowstride, tid, NT);
+  x_tile_load<C, BZ>(tile, in + (size_t)z0 + (size_t)nz * j, M + 1, rowstride, tid, NT);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -502,7 +688,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_kernel(const cx<R>
   auto sync = [] { __syncthreads(); };
   C x[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) x[e] = c2r_pack(tile, BZ, l, t + T * e, M, tw);
+  for (int e = 0; e < E; ++e) x[e] = c2r_pack(tile, BZ, l, t + T * e, M, M + 1, tw);
   line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
   // line-major staging: line l, pair m at xb[l*M + m]
 #pragma unroll
@@ -524,7 +710,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_r2c_kernel(const R *__
                                                                      int nz) {
   using C = cx<R>;
   constexpr int M = NX / 2, T = M / E, NT = BZ * T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
   C *xb = tw + NX;  // BZ*M
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;

@@ -1,0 +1,70 @@
+// pipeline.cuh -- asynchronous tile pipeline for the FFT passes.
+//
+// Tiles move HBM -> shared memory with TMA bulk copies (cp.async.bulk,
+// plain global-to-shared form, no multicast) that complete on an mbarrier
+// per stage.  A persistent CTA keeps STAGES-1 tiles in flight while it
+// transforms the current one, so the copy engine, not warp occupancy,
+// hides the HBM latency.
+//
+// Every wait is bounded: after `cap` unsuccessful polls the CTA agrees (by
+// __syncthreads_or) to give up, records GHOST_ERR_TIMEOUT in the context's
+// device status word, drains its own copies still in flight (with a fixed
+// generous bound) and returns.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gb {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// Make the initialised barriers visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// Order this thread's earlier generic shared-memory accesses before later
+// async-proxy writes into the same buffer.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// bytes must be a multiple of 16; both addresses 16-byte aligned.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase `parity` of bar; false after cap polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t cap) {
+  for (uint32_t n = 0; n < cap; ++n)
+    if (mbar_test(bar, parity)) return true;
+  return false;
+}
+
+constexpr uint32_t kDrainPolls = 1u << 24;
+
+// Status word written on a timeout (GHOST_ERR_TIMEOUT).
+__device__ __forceinline__ void record_timeout(int *status) {
+  if (status) atomicExch(status, 5);
+}
+
+}  // namespace gb

@@ -71,6 +71,12 @@
          TYPE(C_PTR), VALUE :: ctx
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_ctx_set_wait_cap(ctx,cap) BIND(C,name="ghost_ctx_set_wait_cap") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT), VALUE :: cap
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_ctx_launch_count(ctx,n) BIND(C,name="ghost_ctx_launch_count") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_LONG_LONG
          TYPE(C_PTR), VALUE :: ctx

@@ -138,6 +138,10 @@ class Ghost:
     def synchronize(self):
         check(self.lib.ghost_ctx_synchronize(self.h), "ghost_ctx_synchronize")
 
+    def set_wait_cap(self, cap: int):
+        """Bound on device-side polls of every pipelined wait (0: default)."""
+        check(self.lib.ghost_ctx_set_wait_cap(self.h, cap), "ghost_ctx_set_wait_cap")
+
     def set_kmax(self, kmax: float):
         check(self.lib.ghost_ctx_set_kmax(self.h, kmax), "ghost_ctx_set_kmax")
         info = _lib.GhostInfo()

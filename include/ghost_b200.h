@@ -91,6 +91,11 @@ int ghost_ctx_set_stream(ghost_ctx *ctx, void *cuda_stream);
 int ghost_ctx_set_kmax(ghost_ctx *ctx, double kmax);
 /* Block until the context's stream is idle; reports asynchronous errors. */
 int ghost_ctx_synchronize(ghost_ctx *ctx);
+/* Bound on the polls of every device-side wait (tile arrivals in the
+ * pipelined passes).  A wait that runs out makes its kernel give up
+ * cleanly and records GHOST_ERR_TIMEOUT, which the next synchronising call
+ * on the context returns.  Default 2^22 polls; 0 restores the default. */
+int ghost_ctx_set_wait_cap(ghost_ctx *ctx, unsigned int cap);
 /* Number of this library's kernels launched on the context so far. */
 int ghost_ctx_launch_count(const ghost_ctx *ctx, long long *count);
 const char *ghost_last_error_string(void);

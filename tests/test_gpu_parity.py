@@ -315,3 +315,44 @@ def test_native_kernels_ran():
     v = [g.czeros() for _ in range(3)]
     g.hd_run(1, 2, 1e-3, 1e-3, *v)
     assert g.launch_count() - n0 == 10  # 5 fused passes per substep
+
+
+def test_bounded_wait_timeout_reports_and_recovers():
+    """Failure detection without a fault: a wait cap of one poll makes the
+    pipelined passes give up on their tile waits; the kernels drain their
+    copies and return, the next synchronising call reports GHOST_ERR_TIMEOUT,
+    and the context then works normally again."""
+    from ghost_b200 import GhostError
+    o = Oracle(64)
+    g = ghost(64)
+    v0 = solenoidal_ic(o, seed=3)
+    V = [to_dev(x) for x in v0]
+    g.set_wait_cap(1)
+    g.hd_run(1, 2, 1e-3, 2e-3, *V)
+    with pytest.raises(GhostError) as err:
+        g.synchronize()
+    assert err.value.code == 5
+    g.set_wait_cap(0)
+    V = [to_dev(x) for x in v0]
+    g.hd_run(1, 2, 1e-3, 2e-3, *V)
+    g.synchronize()
+    ref = o.hd_run(1, 2, 1e-3, 2e-3, v0)
+    assert rel_l2([to_host(x) for x in V], ref) < 1e-12
+
+
+def test_pruned_substeps_are_bitwise_equal_to_full_ones():
+    """hd_run skips the known zeros outside the 2/3 truncation after its
+    first substep; stepping with hd_rkstep2 (always full passes) must give
+    the same bits."""
+    o = Oracle(64)
+    g = ghost(64, precision="fp32")
+    v0 = [x.astype(np.complex64) for x in solenoidal_ic(o, seed=8)]
+    A = [to_dev(x) for x in v0]
+    B = [to_dev(x) for x in v0]
+    C = [g.czeros() for _ in range(3)]
+    g.hd_run(2, 2, 1e-3, 2e-3, *A)
+    for _ in range(2):
+        g.hd_rkstep1(*B, *C)
+        for oo in (2, 1):
+            g.hd_rkstep2(oo, 1e-3, 2e-3, *B, *C)
+    assert all(bool((x == y).all()) for x, y in zip(A, B))
