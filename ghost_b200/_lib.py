@@ -56,6 +56,7 @@ SIGNATURES = {
     "ghost_ctx_set_kmax": [P, D],
     "ghost_ctx_synchronize": [P],
     "ghost_ctx_set_wait_cap": [P, ctypes.c_uint],
+    "ghost_ctx_inject_stall": [P, I],
     "ghost_ctx_launch_count": [P, ctypes.POINTER(ctypes.c_longlong)],
     "ghost_ctx_enable_timers": [P, I],
     "ghost_ctx_read_timers": [P, PD, ctypes.POINTER(ctypes.c_longlong)],

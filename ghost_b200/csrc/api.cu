@@ -9,6 +9,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "ic_host.h"
 #include "ops.cuh"
@@ -253,7 +255,44 @@ template <class K> static int persistent_grid(ghost_ctx *c, K kern, int threads,
   return (int)std::max<long>(1, std::min<long>(g, ntiles));
 }
 
-static PipeCtl pipe_ctl(ghost_ctx *c) { return PipeCtl{c->status, c->wait_cap}; }
+// ---------------------------------------------------------------------
+// TMA tensor maps of spectral fields: a 3D tensor (z in 8-byte units, y,
+// kx) over one field, with the box the pass loads.
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+static std::mutex g_encode_mu;
+
+static int encode_fn(PFN_cuTensorMapEncodeTiled_v12000 *fn) {
+  std::lock_guard<std::mutex> lock(g_encode_mu);
+  if (!g_encode_tiled) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || p == nullptr || q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return fail(GHOST_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    }
+    g_encode_tiled = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  *fn = g_encode_tiled;
+  return GHOST_OK;
+}
+
+static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box1, unsigned box2, CUtensorMap *out) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc;
+  GB_CHECK(encode_fn(&enc));
+  const cuuint64_t U = c->precision == GHOST_SINGLE ? 1 : 2;
+  const cuuint64_t dims[3] = {(cuuint64_t)c->nz * U, (cuuint64_t)c->ny, (cuuint64_t)c->nxh};
+  const cuuint64_t strides[2] = {(cuuint64_t)c->nz * U * 8, (cuuint64_t)c->nz * c->ny * U * 8};
+  const cuuint32_t box[3] = {box0, box1, box2};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(GHOST_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return GHOST_OK;
+}
+
+static PipeCtl pipe_ctl(ghost_ctx *c) { return PipeCtl{c->status, c->wait_cap, c->inject_stall}; }
 
 template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
   constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
@@ -297,8 +336,14 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   const int ni = pr.jpos ? pr.ni : c->nxh;
   const long ntiles = (long)(c->nz / BZ) * ni * nf;
   const int grid = persistent_grid(c, kern, BZ * T, smem, ntiles);
+  // box rows: 32 (or N/2) for the pruned inverse, whole halves otherwise
+  const int rb = (pr.jpos && S > 0) ? std::min(32, N / 2) : std::min(N, 256);
+  const unsigned U = sizeof(R) == 4 ? 1 : 2;
+  FieldMaps maps;
+  for (int q = 0; q < nf; ++q) GB_CHECK(field_map(c, f.p[q], BZ * U, rb, 1, &maps.m[q]));
   const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
-  kern<<<grid, BZ * T, smem, c->stream>>>(f, (const cx<R> *)c->tw_y, c->nz, ni, nf, pr.jpos, pr.jneg, pipe_ctl(c));
+  kern<<<grid, BZ * T, smem, c->stream>>>(maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf, pr.jpos, pr.jneg, rb,
+                                          pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
 }
@@ -339,14 +384,20 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
     const size_t smem = G::smem_bytes(STAGES);
     auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES>;
     GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CFields<R> fi{};
     Fields<R> fo{};
-    for (int q = 0; q < NIN; ++q) fi.p[q] = (const C *)ins[q];
     for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
     const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+    const int nrows = rows > 0 ? rows : M + 1;
+    // tensor boxes: nbox boxes of rb kx-rows; rb keeps every box 128-byte aligned in shared memory
+    const int nbox = (nrows + 255) / 256;
+    const int align = std::max(1, 128 / (BZ * (int)sizeof(C)));
+    const int rb = ((nrows + nbox - 1) / nbox + align - 1) / align * align;
+    if (nbox * rb > M + 8 || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the tile", nbox, rb);
+    const unsigned U = sizeof(R) == 4 ? 1 : 2;
+    FieldMaps maps;
+    for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, 1, rb, &maps.m[q]));
     const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny);
-    kern<<<pgrid, NT, smem, c->stream>>>(fi, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), rows > 0 ? rows : M + 1,
-                                         pipe_ctl(c));
+    kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb, pipe_ctl(c));
   } else if (KIND == X_C2R) {
     const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
     auto kern = xpass_c2r_kernel<R, NX, E, BZ>;
@@ -903,6 +954,7 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->num_sms = 0;
   c->status = nullptr;
   c->wait_cap = 1u << 22;
+  c->inject_stall = 0;
   c->prune_valid = c->prune_ok = false;
   c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
   c->prune_nlines = c->prune_imax = 0;
@@ -991,6 +1043,12 @@ int ghost_ctx_synchronize(ghost_ctx *c) {
   CTX_CHECK(c);
   GB_CUDA(cudaStreamSynchronize(c->stream));
   return check_status(c);
+}
+
+int ghost_ctx_inject_stall(ghost_ctx *c, int enable) {
+  CTX_CHECK(c);
+  c->inject_stall = enable != 0;
+  return GHOST_OK;
 }
 
 int ghost_ctx_set_wait_cap(ghost_ctx *c, unsigned int cap) {

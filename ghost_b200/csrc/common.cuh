@@ -111,6 +111,7 @@ struct ghost_ctx {
   // device status word written by kernels whose bounded waits ran out
   int *status;
   uint32_t wait_cap;
+  int inject_stall;  // fault injection (ghost_ctx_inject_stall)
   // zero-pruning tables of the 2/3 truncation (built on first use):
   // active (j,i) z-lines padded with -1 to a multiple of 256, the
   // contiguous live y-wavenumber counts per kx index, and the last live kx

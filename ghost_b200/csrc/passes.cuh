@@ -47,13 +47,19 @@ template <typename R, int N, int E, int LPB, int NL> struct ZGeom {
   static constexpr int NP = N + N / 8;  // padded exchange line: idx + idx/8 spreads strided writes
   static constexpr size_t stage_elems = (size_t)NL * LPB * N;
   static constexpr size_t smem_bytes(int stages) {
-    return (stages * stage_elems + N + (size_t)LPB * NP) * sizeof(cx<R>) + 8 * stages;
+    return (stages * stage_elems + N + (size_t)LPB * NP) * sizeof(cx<R>) + 8 * (stages + 1);
   }
+};
+
+// One 3D tensor map per field: (z in 8-byte units, y, kx).
+struct FieldMaps {
+  CUtensorMap m[9];
 };
 
 struct PipeCtl {
   int *status;    // device status word (GHOST_ERR_TIMEOUT on a timed-out wait)
   uint32_t cap;   // polls before a wait gives up
+  int stall;      // fault injection: wait on a barrier nothing completes
 };
 
 // lines != nullptr: the pass covers the listed (j,i) lines only (entries
@@ -73,7 +79,7 @@ __global__ void __launch_bounds__(LPB *(N / E)) zpipe_kernel(Op op, const cx<R> 
   const int tid = threadIdx.x, lq = tid / T, t = tid - lq * T;
   const int ntiles = (nlines + LPB - 1) / LPB;
   if (tid == 0) {
-    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
     fence_barrier_init();
   }
   for (int e = tid; e < N; e += NT) tw[e] = twg[e];
@@ -111,7 +117,8 @@ __global__ void __launch_bounds__(LPB *(N / E)) zpipe_kernel(Op op, const cx<R> 
     fence_proxy_async();
     issue(k + STAGES - 1);
     const int s = k % STAGES;
-    const bool ok = mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
+    const bool ok = (!ctl.stall || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
+                    mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
       for (int kk = k; kk < k + STAGES; ++kk)
@@ -365,13 +372,14 @@ template <typename R, int N, int E, int BZ> struct YGeom {
   static constexpr int T = N / E;
   static constexpr int NT = BZ * T;
   static constexpr size_t stage_elems = (size_t)BZ * N;
-  static constexpr size_t smem_bytes(int stages) { return (stages * stage_elems + N) * sizeof(cx<R>) + 8 * stages; }
+  static constexpr size_t smem_bytes(int stages) { return (stages * stage_elems + N) * sizeof(cx<R>) + 8 * (stages + 1); }
 };
 
 template <typename R, int N, int E, int BZ, int STAGES, int S>
-__global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(Fields<R> fld, const cx<R> *__restrict__ twg, int nz,
-                                                             int ni, int nf, const int *__restrict__ jpos,
-                                                             const int *__restrict__ jneg, PipeCtl ctl) {
+__global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
+                                                             const cx<R> *__restrict__ twg, int nz, int ni, int nf,
+                                                             const int *__restrict__ jpos,
+                                                             const int *__restrict__ jneg, int rb, PipeCtl ctl) {
   using C = cx<R>;
   using G = YGeom<R, N, E, BZ>;
   constexpr int T = G::T, NT = G::NT;
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(Fields<R> fld, const
   const int nzb = nz / BZ;
   const int ntiles = nzb * ni * nf;
   if (tid == 0) {
-    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
     fence_barrier_init();
   }
   for (int e = tid; e < N; e += NT) tw[e] = twg[e];
@@ -408,20 +416,26 @@ __global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(Fields<R> fld, const
       jn = 0;
     }
   };
+  // one thread issues TMA tensor loads of rb-row boxes covering the live
+  // rows: [0, jp) from the top and [N - jn, N) from the bottom (boxes may
+  // overlap or overrun into rows that are masked out below)
+  constexpr int U = (int)sizeof(C) / 8;
   auto issue = [&](int k) {
     const int tile = blockIdx.x + k * gridDim.x;
-    if (tile >= ntiles) return;
+    if (tile >= ntiles || tid != 0) return;
     const Tile tl = tile_of(tile);
     int jp, jn;
     rows_of(tl.i, jp, jn);
     const int s = k % STAGES;
-    const int nrows = jp + jn;
-    if (tid == 0) mbar_arrive_expect_tx(&bars[s], (uint32_t)nrows * BZ * (uint32_t)sizeof(C));
-    const C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + (size_t)nz * N * tl.i;
+    const int nb_top = (jp + rb - 1) / rb, nb_bot = (jn + rb - 1) / rb;
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bars[s], (uint32_t)((nb_top + nb_bot) * rb) * BZ * (uint32_t)sizeof(C));
     C *dst = stage + (size_t)s * G::stage_elems;
-    for (int q = tid; q < nrows; q += NT) {
-      const int jj = q < jp ? q : N - jn + (q - jp);
-      bulk_g2s(dst + (size_t)jj * BZ, base + (size_t)nz * jj, BZ * (uint32_t)sizeof(C), &bars[s]);
+    for (int q = 0; q < nb_top; ++q)
+      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[tl.f], tl.zb * BZ * U, q * rb, tl.i, &bars[s]);
+    for (int q = 0; q < nb_bot; ++q) {
+      const int r0 = N - (q + 1) * rb;
+      tma_load_3d(dst + (size_t)r0 * BZ, &maps.m[tl.f], tl.zb * BZ * U, r0, tl.i, &bars[s]);
     }
   };
   for (int k = 0; k < STAGES - 1; ++k) issue(k);
@@ -429,10 +443,10 @@ __global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(Fields<R> fld, const
   for (int k = 0;; ++k) {
     const int tile = blockIdx.x + k * gridDim.x;
     if (tile >= ntiles) break;
-    fence_proxy_async();
     issue(k + STAGES - 1);
     const int s = k % STAGES;
-    const bool ok = mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
+    const bool ok = (!ctl.stall || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
+                    mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
       for (int kk = k; kk < k + STAGES; ++kk)
@@ -521,25 +535,33 @@ template <typename C> __device__ __forceinline__ C r2c_unpack(C zk, C zm, C w) {
 //   PHYS 1 (BOUSS): in v, curl v, grad theta (9)
 //                   -> out omega x v (3), -v.grad(theta) (1)
 //                   (prodre3 + advect3, pseudospec3D_phd.f90:23-114)
-// A persistent CTA walks (z-block, y) tiles; every input field of a tile
-// is one load of `rows` kx rows (BZ contiguous values each, one bulk copy
-// per row) into a STAGES-deep ring, so the next fields (and the next
-// tile) stream in while the current field is transformed.  scale is
-// 1/(nx ny nz)^2; outputs may alias in[0..NOUT-1]; only kx rows < rows are
-// read (the rest are zero) and written (the rest are never read).
+// A persistent CTA walks (z-block, y) tiles.  Every input field of a tile
+// is one TMA tensor load (nbox boxes of rb kx-rows x BZ z-values) into a
+// STAGES-deep ring, so the next fields (and the next tile) stream in while
+// the current field is transformed.  scale is 1/(nx ny nz)^2; outputs may
+// alias the inputs; only kx rows < rows are read (the rest are zero) and
+// written (the rest are never read).
 // ====================================================================
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 template <typename R, int NX, int BZ> struct XGeom {
   static constexpr int M = NX / 2;
-  static constexpr size_t stage_elems = (size_t)(M + 1) * BZ;
+  // TMA boxes may overrun the M+1 rows by a few (zero-filled) rows
+  static constexpr size_t stage_elems = (size_t)(M + 8) * BZ;
   static constexpr size_t smem_bytes(int stages) {
-    return (stages * stage_elems + NX + (size_t)M * BZ) * sizeof(cx<R>) + 8 * stages;
+    return (stages * stage_elems + NX + (size_t)M * BZ) * sizeof(cx<R>) + 8 * (stages + 1);
   }
 };
 
+
+
 template <typename R, int NX, int E, int BZ, int PHYS, int STAGES>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(CFields<R> in, Fields<R> out,
-                                                                    const cx<R> *__restrict__ twg, int ny, int nz,
-                                                                    R scale, int rows, PipeCtl ctl) {
+__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
+                                                                    Fields<R> out, const cx<R> *__restrict__ twg,
+                                                                    int ny, int nz, R scale, int rows, int nbox,
+                                                                    int rb, PipeCtl ctl) {
   using C = cx<R>;
   using G = XGeom<R, NX, BZ>;
   constexpr int M = NX / 2, T = M / E, NT = BZ * T;
@@ -554,21 +576,23 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(CFields<R> i
   const int ntiles = nzb * ny;
   const size_t rowstride = (size_t)nz * ny;
   if (tid == 0) {
-    for (int q = 0; q < STAGES; ++q) mbar_init(&bars[q], 1);
+    for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
     fence_barrier_init();
   }
   for (int e = tid; e < NX; e += NT) tw[e] = twg[e];
   __syncthreads();
+  // one thread issues nbox tensor loads of rb kx-rows x BZ z-values
+  constexpr int U = (int)sizeof(C) / 8;
   auto issue = [&](int L) {
     const int k = L / NIN, f = L - k * NIN;
     const int tile = blockIdx.x + k * gridDim.x;
-    if (tile >= ntiles) return;
+    if (tile >= ntiles || tid != 0) return;
     const int s = L % STAGES;
-    if (tid == 0) mbar_arrive_expect_tx(&bars[s], (uint32_t)rows * BZ * (uint32_t)sizeof(C));
-    const C *src = in.p[f] + (size_t)(tile % nzb) * BZ + (size_t)nz * (tile / nzb);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bars[s], (uint32_t)(nbox * rb) * BZ * (uint32_t)sizeof(C));
     C *dst = stage + (size_t)s * G::stage_elems;
-    for (int r = tid; r < rows; r += NT)
-      bulk_g2s(dst + (size_t)r * BZ, src + rowstride * r, BZ * (uint32_t)sizeof(C), &bars[s]);
+    for (int q = 0; q < nbox; ++q)
+      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[f], (tile % nzb) * BZ * U, tile / nzb, q * rb, &bars[s]);
   };
   for (int L = 0; L < STAGES - 1; ++L) issue(L);
   auto buf = [xb, l](int idx) -> C & { return xb[idx * BZ + l]; };
@@ -581,9 +605,9 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(CFields<R> i
 #pragma unroll
     for (int f = 0; f < NIN; ++f) {
       const int L = k * NIN + f;
-      fence_proxy_async();
       issue(L + STAGES - 1);
-      const bool ok = mbar_wait(&bars[L % STAGES], (uint32_t)(L / STAGES) & 1u, ctl.cap);
+      const bool ok = (!ctl.stall || L > 0 || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
+                      mbar_wait(&bars[L % STAGES], (uint32_t)(L / STAGES) & 1u, ctl.cap);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) record_timeout(ctl.status);
         for (int LL = L; LL < L + STAGES; ++LL)

@@ -11,6 +11,7 @@
 // device status word, drains its own copies still in flight (with a fixed
 // generous bound) and returns.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,6 +44,19 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// TMA tensor load of one box of a 3D tensor map (coordinates innermost
+// first, in elements of the map's data type) into shared memory.  The
+// innermost coordinate times the element size is a multiple of 16 bytes
+// at every call site; dst is 128-byte aligned.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -61,6 +75,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 }
 
 constexpr uint32_t kDrainPolls = 1u << 24;
+
+// With PipeCtl::stall set (fault-injection testing), a pass first waits on a
+// barrier that nothing ever completes, so its bounded wait runs out.
+__device__ __forceinline__ bool injected_stall_wait(uint64_t *never, uint32_t cap) {
+  return mbar_wait(never, 0u, cap);
+}
 
 // Status word written on a timeout (GHOST_ERR_TIMEOUT).
 __device__ __forceinline__ void record_timeout(int *status) {

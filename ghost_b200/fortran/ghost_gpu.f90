@@ -77,6 +77,12 @@
          INTEGER(C_INT), VALUE :: cap
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_ctx_inject_stall(ctx,enable) BIND(C,name="ghost_ctx_inject_stall") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT), VALUE :: enable
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_ctx_launch_count(ctx,n) BIND(C,name="ghost_ctx_launch_count") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_LONG_LONG
          TYPE(C_PTR), VALUE :: ctx

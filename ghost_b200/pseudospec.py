@@ -138,6 +138,10 @@ class Ghost:
     def synchronize(self):
         check(self.lib.ghost_ctx_synchronize(self.h), "ghost_ctx_synchronize")
 
+    def inject_stall(self, on: bool):
+        """Fault injection: pipelined passes wait on a barrier nothing completes."""
+        check(self.lib.ghost_ctx_inject_stall(self.h, int(on)), "ghost_ctx_inject_stall")
+
     def set_wait_cap(self, cap: int):
         """Bound on device-side polls of every pipelined wait (0: default)."""
         check(self.lib.ghost_ctx_set_wait_cap(self.h, cap), "ghost_ctx_set_wait_cap")

@@ -96,6 +96,11 @@ int ghost_ctx_synchronize(ghost_ctx *ctx);
  * cleanly and records GHOST_ERR_TIMEOUT, which the next synchronising call
  * on the context returns.  Default 2^22 polls; 0 restores the default. */
 int ghost_ctx_set_wait_cap(ghost_ctx *ctx, unsigned int cap);
+/* Fault injection for testing failure detection: with enable != 0 every
+ * pipelined pass additionally waits on a barrier that nothing completes,
+ * so its bounded wait runs out and the next synchronising call returns
+ * GHOST_ERR_TIMEOUT.  Nothing faults or hangs; results are not computed. */
+int ghost_ctx_inject_stall(ghost_ctx *ctx, int enable);
 /* Number of this library's kernels launched on the context so far. */
 int ghost_ctx_launch_count(const ghost_ctx *ctx, long long *count);
 const char *ghost_last_error_string(void);

@@ -318,20 +318,23 @@ def test_native_kernels_ran():
 
 
 def test_bounded_wait_timeout_reports_and_recovers():
-    """Failure detection without a fault: a wait cap of one poll makes the
-    pipelined passes give up on their tile waits; the kernels drain their
-    copies and return, the next synchronising call reports GHOST_ERR_TIMEOUT,
-    and the context then works normally again."""
+    """Failure detection without a fault: with the stall injected, every
+    pipelined pass waits on a barrier nothing completes; after the (lowered)
+    wait cap the kernels give up, drain their copies and return, the next
+    synchronising call reports GHOST_ERR_TIMEOUT, and the context then works
+    normally again."""
     from ghost_b200 import GhostError
     o = Oracle(64)
     g = ghost(64)
     v0 = solenoidal_ic(o, seed=3)
     V = [to_dev(x) for x in v0]
-    g.set_wait_cap(1)
+    g.set_wait_cap(1000)
+    g.inject_stall(True)
     g.hd_run(1, 2, 1e-3, 2e-3, *V)
     with pytest.raises(GhostError) as err:
         g.synchronize()
     assert err.value.code == 5
+    g.inject_stall(False)
     g.set_wait_cap(0)
     V = [to_dev(x) for x in v0]
     g.hd_run(1, 2, 1e-3, 2e-3, *V)
