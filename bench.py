@@ -295,6 +295,29 @@ def traffic_from_profiles(kernel):
     return None
 
 
+def prune_fractions(n):
+    """Exact fractions of the spectral grid the pruned passes must touch for a
+    cubic n^3 grid with the 2/3 truncation kn2 <= n^2/9 (kz = 0 decides a
+    z-line; a kx row is live if any of its lines is)."""
+    import numpy as np
+    nxh = n // 2 + 1
+    kmax = np.float32(1.0 / 9.0) * np.float32(n * n)
+    kx = np.arange(nxh, dtype=np.float64)
+    kx[-1] = -(n // 2)
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    k2 = kx[:, None] ** 2 + ky[None, :] ** 2
+    live = k2 <= kmax
+    f_line = live.mean()
+    f_row = live.any(axis=1).mean()
+    kz = np.fft.fftfreq(n, 1.0 / n)
+    kept = 0
+    for i in range(nxh):
+        kk = k2[i][:, None] + kz[None, :] ** 2
+        kept += int(((kk <= kmax) & (kk >= 3.8e-7)).sum())
+    f_keep = kept / (nxh * n * n)
+    return float(f_line), float(f_row), float(f_keep)
+
+
 def run_ours(args, ws, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -321,10 +344,16 @@ def run_ours(args, ws, rank, local):
     steps64 = max(2, args.steps // 2) / (ms64 * 1e-3)
     value = ws * steps32
 
-    # dominant kernel and its roofline (algorithmic bytes per launch)
+    # dominant kernel and its roofline: algorithmic bytes per launch, the
+    # bytes each pass must move once the known zeros of the 2/3 truncation
+    # are skipped (f_line: live z-lines, f_row: live kx rows, f_keep: kept modes)
     cb = (n // 2 + 1) * n * n * 8
-    per_launch_bytes = {"z_inv": 9 * cb + 3 * cb / ORD, "y_inv": 12 * cb, "x_nl": 9 * cb, "y_fwd": 6 * cb,
-                        "z_fwd": 15 * cb}
+    f_line, f_row, f_keep = prune_fractions(n)
+    per_launch_bytes = {"z_inv": (9 + 3 / ORD) * f_line * cb,
+                        "y_inv": 6 * (f_line + f_row) * cb,
+                        "x_nl": 9 * f_row * cb,
+                        "y_fwd": 3 * (f_row + f_line) * cb,
+                        "z_fwd": (6 * f_line + 9 * f_keep) * cb}
     dom = max(tm, key=lambda k: tm[k][0])
     dom_ms = tm[dom][0] / tm[dom][1]
     ach = per_launch_bytes[dom] / (dom_ms * 1e-3) / 1e9
@@ -366,6 +395,8 @@ def run_ours(args, ws, rank, local):
             "kernels": kern,
             "fft": None if fft is None else {**fft, "frac": fft["gbs"] / peak},
             "substep_effective_gbs": survey_bytes / (ms32 / args.steps / ORD * 1e-3) / 1e9,
+            "prune": {"f_line": f_line, "f_row": f_row, "f_keep": f_keep},
+            "substep_bytes": sum(per_launch_bytes.values()),
             "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk,

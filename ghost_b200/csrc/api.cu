@@ -325,8 +325,8 @@ template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const P
 
 template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   constexpr int E = N < 8 ? N : 8, T = N / E;
-  constexpr int BZ0 = sizeof(R) == 4 ? 16 : 8;
-  constexpr int BZ = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
+  constexpr int BZ0 = 8;  // 64-byte (FP32) / 128-byte (FP64) rows; two CTAs per SM
+  constexpr int BZ = BZ0 * T <= 512 ? BZ0 : 512 / T;
   using G = YGeom<R, N, E, BZ>;
   constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
   if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);

@@ -376,7 +376,7 @@ template <typename R, int N, int E, int BZ> struct YGeom {
 };
 
 template <typename R, int N, int E, int BZ, int STAGES, int S>
-__global__ void __launch_bounds__(BZ *(N / E)) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
+__global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
                                                              const cx<R> *__restrict__ twg, int nz, int ni, int nf,
                                                              const int *__restrict__ jpos,
                                                              const int *__restrict__ jneg, int rb, PipeCtl ctl) {
@@ -558,7 +558,7 @@ template <typename R, int NX, int BZ> struct XGeom {
 
 
 template <typename R, int NX, int E, int BZ, int PHYS, int STAGES>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
+__global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
                                                                     Fields<R> out, const cx<R> *__restrict__ twg,
                                                                     int ny, int nz, R scale, int rows, int nbox,
                                                                     int rb, PipeCtl ctl) {
