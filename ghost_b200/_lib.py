@@ -86,6 +86,18 @@ SIGNATURES = {
     "ghost_bouss_rkstep2": [P, I, D, D, D, D, D, D] + [P] * 12,
     "ghost_bouss_run": [P, I, I, D, D, D, D, D, D] + [P] * 8,
     "ghost_init_random_solenoidal": [P, ctypes.POINTER(ctypes.c_int32), D, D, I, D, P, P, P],
+    "ghost_ctx_create_batch": [I, I, I, I, I, ctypes.POINTER(P)],
+    "ghost_batch_set_nu": [P, PD],
+    "ghost_batch_energy": [P, P, P, P, I, PD],
+    "ghost_batch_init_random_solenoidal": [P, ctypes.POINTER(ctypes.c_int32), D, D, I, D, P, P, P],
+    "ghost_ensemble_create": [I, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), I, ctypes.POINTER(P)],
+    "ghost_ensemble_destroy": [P],
+    "ghost_ensemble_fields": [P, I, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)],
+    "ghost_ensemble_class": [P, I, ctypes.POINTER(P)],
+    "ghost_ensemble_init": [P, ctypes.POINTER(ctypes.c_int32), D, D, I, D, PD],
+    "ghost_ensemble_autotune": [P, I, D, ctypes.POINTER(ctypes.c_int)],
+    "ghost_ensemble_run": [P, I, I, D],
+    "ghost_ensemble_energy": [P, I, PD],
 }
 
 _lib = None

@@ -281,7 +281,7 @@ static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box
   PFN_cuTensorMapEncodeTiled_v12000 enc;
   GB_CHECK(encode_fn(&enc));
   const cuuint64_t U = c->precision == GHOST_SINGLE ? 1 : 2;
-  const cuuint64_t dims[3] = {(cuuint64_t)c->nz * U, (cuuint64_t)c->ny, (cuuint64_t)c->nxh};
+  const cuuint64_t dims[3] = {(cuuint64_t)c->nz * U, (cuuint64_t)c->ny, (cuuint64_t)c->nxh * c->nruns};
   const cuuint64_t strides[2] = {(cuuint64_t)c->nz * U * 8, (cuuint64_t)c->nz * c->ny * U * 8};
   const cuuint32_t box[3] = {box0, box1, box2};
   const cuuint32_t estr[3] = {1, 1, 1};
@@ -294,13 +294,12 @@ static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box
 
 static PipeCtl pipe_ctl(ghost_ctx *c) { return PipeCtl{c->status, c->wait_cap, c->inject_stall}; }
 
-template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
+template <typename R, int N, int LPB, class Op> int launch_z_cfg(ghost_ctx *c, const Op &op, const Prune &pr) {
   constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
-  constexpr int LPB = 256 / T > 0 ? 256 / T : 1;
   using G = ZGeom<R, N, E, LPB, Op::NLOAD>;
   constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
   const size_t smem = G::smem_bytes(STAGES);
-  const int nlines = pr.lines ? pr.nlines : c->ny * c->nxh;
+  const int nlines = pr.lines ? pr.nlines : c->ny * c->nxh * c->nruns;
   auto kern = zpipe_kernel<R, N, E, LPB, STAGES, Op>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = persistent_grid(c, kern, LPB * T, smem, (nlines + LPB - 1) / LPB);
@@ -308,6 +307,15 @@ template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op
   kern<<<grid, LPB * T, smem, c->stream>>>(op, (const cx<R> *)c->tw_z, pr.lines, nlines, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
+}
+
+// CTAs of 256 threads, or of 128 threads with tile variant bit 1
+template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
+  constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
+  constexpr int L256 = 256 / T > 0 ? 256 / T : 1;
+  constexpr int L128 = 128 / T > 0 ? 128 / T : 1;
+  if ((c->tile_cfg & 2) && L128 != L256) return launch_z_cfg<R, N, L128>(c, op, pr);
+  return launch_z_cfg<R, N, L256>(c, op, pr);
 }
 
 template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const Prune &pr = Prune()) {
@@ -323,10 +331,10 @@ template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const P
   return fail(GHOST_ERR_SIZE, "nz=%d unsupported", c->nz);
 }
 
-template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
+template <typename R, int N, int S, int BZ0>
+int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   constexpr int E = N < 8 ? N : 8, T = N / E;
-  constexpr int BZ0 = 8;  // 64-byte (FP32) / 128-byte (FP64) rows; two CTAs per SM
-  constexpr int BZ = BZ0 * T <= 512 ? BZ0 : 512 / T;
+  constexpr int BZ = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
   using G = YGeom<R, N, E, BZ>;
   constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
   if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);
@@ -334,7 +342,7 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ni = pr.jpos ? pr.ni : c->nxh;
-  const long ntiles = (long)(c->nz / BZ) * ni * nf;
+  const long ntiles = (long)(c->nz / BZ) * ni * c->nruns * nf;
   const int grid = persistent_grid(c, kern, BZ * T, smem, ntiles);
   // box rows: 32 (or N/2) for the pruned inverse, whole halves otherwise
   const int rb = (pr.jpos && S > 0) ? std::min(32, N / 2) : std::min(N, 256);
@@ -342,10 +350,16 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   FieldMaps maps;
   for (int q = 0; q < nf; ++q) GB_CHECK(field_map(c, f.p[q], BZ * U, rb, 1, &maps.m[q]));
   const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
-  kern<<<grid, BZ * T, smem, c->stream>>>(maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf, pr.jpos, pr.jneg, rb,
-                                          pipe_ctl(c));
+  kern<<<grid, BZ * T, smem, c->stream>>>(maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf, c->nruns, c->nxh, pr.jpos,
+                                          pr.jneg, rb, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
+}
+
+// tiles 8 z-lines wide, or 16 with tile variant bit 0
+template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
+  if ((c->tile_cfg & 1) && c->nz >= 16) return launch_y_cfg<R, N, S, 16>(c, f, nf, pr);
+  return launch_y_cfg<R, N, S, 8>(c, f, nf, pr);
 }
 
 template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr = Prune()) {
@@ -396,8 +410,9 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
     const unsigned U = sizeof(R) == 4 ? 1 : 2;
     FieldMaps maps;
     for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, 1, rb, &maps.m[q]));
-    const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny);
-    kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb, pipe_ctl(c));
+    const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny * c->nruns);
+    kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb, c->nruns,
+                                         c->nxh, pipe_ctl(c));
   } else if (KIND == X_C2R) {
     const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
     auto kern = xpass_c2r_kernel<R, NX, E, BZ>;
@@ -473,6 +488,9 @@ template <typename R> int build_prune(ghost_ctx *c) {
   c->prune_ok = ok && imax >= 0;
   c->prune_valid = true;
   if (!c->prune_ok) return GHOST_OK;
+  const int nrun = (int)lines.size();
+  for (int r = 1; r < c->nruns; ++r)
+    for (int q = 0; q < nrun; ++q) lines.push_back(lines[q] + r * ny * nxh);
   const int n = (int)lines.size();
   const int padded = (n + 255) / 256 * 256;
   lines.resize(padded, -1);
@@ -672,7 +690,7 @@ int advect3_dev(ghost_ctx *c, const void *a, const void *b, const void *cc, cons
 template <typename R>
 int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d, const void *e,
                const void *f, double *out_host) {
-  const size_t n = c->nspec;
+  const size_t n = c->ntot;
   const int nb = grid1d(n);
   double *part;
   GB_CHECK(partials(c, (size_t)nb + 1, &part));
@@ -691,7 +709,7 @@ int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void 
 
 template <typename R>
 int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host) {
-  const size_t n = c->nspec;
+  const size_t n = c->ntot;
   const int nbins = c->nmax / 2 + 1;
   const int nblk = std::min(grid1d(n), 148 * 4);
   double *part;
@@ -759,6 +777,8 @@ template <typename R> void fill_kparams(ghost_ctx *c, KParams<R> &kp) {
   kp.tiny = (R)c->tiny;
   const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
   kp.tmp = (R)1 / (nn * nn);
+  kp.nruns = c->nruns;
+  kp.nu_run = (sizeof(R) == (c->precision == GHOST_SINGLE ? 4 : 8)) ? (const R *)c->nu_run : nullptr;
 }
 
 // kmax, tiny, nmax, Dk of main3D.fpp:881-909,1727-1737 in precision R
@@ -812,27 +832,27 @@ static void refresh_kparams(ghost_ctx *c) {
 
 template <typename R> int derivk3_impl(ghost_ctx *c, const void *a, void *b, int dir) {
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  derivk3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec, dir);
+  derivk3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->ntot, dir);
   timer_end(c, ts);
   return post_launch(c);
 }
 template <typename R> int laplak3_impl(ghost_ctx *c, const void *a, void *b) {
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  laplak3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec);
+  laplak3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->ntot);
   timer_end(c, ts);
   return post_launch(c);
 }
 template <typename R> int rotor3_impl(ghost_ctx *c, const void *a, const void *b, void *o, int dir) {
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  rotor3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
-                                                             (cx<R> *)o, c->nspec, dir);
+  rotor3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
+                                                             (cx<R> *)o, c->ntot, dir);
   timer_end(c, ts);
   return post_launch(c);
 }
 template <typename R> int nonlhd3_impl(ghost_ctx *c, const void *a, const void *b, const void *cc, void *g, int dir) {
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  nonlhd3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
-                                                              (const cx<R> *)cc, (cx<R> *)g, c->nspec, dir);
+  nonlhd3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (const cx<R> *)b,
+                                                              (const cx<R> *)cc, (cx<R> *)g, c->ntot, dir);
   timer_end(c, ts);
   return post_launch(c);
 }
@@ -840,13 +860,13 @@ template <typename R> int sharp_impl(ghost_ctx *c, const void *a, void *b, doubl
   const R pi = (R)3.14159265358979323846;
   const R cut = (pi / (R)delta) * (pi / (R)delta);
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  sharp_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->nspec, cut);
+  sharp_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), (const cx<R> *)a, (cx<R> *)b, c->ntot, cut);
   timer_end(c, ts);
   return post_launch(c);
 }
 template <typename R> int scale3_impl(ghost_ctx *c, void *x, void *y, void *z, double f0, double s) {
   const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
-  scale3_kernel<R><<<grid1d(c->nspec), 256, 0, c->stream>>>((cx<R> *)x, (cx<R> *)y, (cx<R> *)z, c->nspec, (R)f0, s);
+  scale3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>((cx<R> *)x, (cx<R> *)y, (cx<R> *)z, c->ntot, (R)f0, s);
   timer_end(c, ts);
   return post_launch(c);
 }
@@ -902,6 +922,60 @@ template <typename R> int init_random_impl(ghost_ctx *c, int32_t *seed, double k
   return scale3_impl<R>(c, ox, oy, oz, amp, sqrt(e));
 }
 
+
+// ---------------------------------------------------------------------
+// batches of runs
+template <typename R>
+int batch_reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host) {
+  const int nb = std::max(1, std::min(grid1d(c->nspec), 4096 / std::max(1, c->nruns)));
+  double *part;
+  GB_CHECK(partials(c, (size_t)(nb + 1) * c->nruns, &part));
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
+  const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
+  reduce_runs_kernel<R><<<dim3(nb, c->nruns), 256, 0, c->stream>>>(kparams<R>(c), ra, kind, c->nspec, c->nruns, part);
+  GB_CHECK(post_launch(c));
+  double *fin = part + (size_t)nb * c->nruns;
+  finalize_kernel<<<1, 256, 0, c->stream>>>(part, nb, c->nruns, fin);
+  timer_end(c, ts);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * c->nruns, cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+template <typename R>
+int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out, double kdn, double kup, int shape,
+                          double amp, void *ox, void *oy, void *oz) {
+  Grid g{c->nx, c->ny, c->nz, c->nxh, c->anis, c->arbsize, c->Dkx, c->Dky, c->Dkz};
+  const size_t ns = c->nspec;
+  std::vector<R> h1(2 * c->ntot), h2(2 * c->ntot), h3(2 * c->ntot);
+  for (int r = 0; r < c->nruns; ++r) {
+    const int32_t s = random_vpot<R>(g, seeds[r], kdn, kup, shape, h1.data() + 2 * ns * r, h2.data() + 2 * ns * r,
+                                     h3.data() + 2 * ns * r);
+    if (seeds_out) seeds_out[r] = s;
+  }
+  void *w[3];
+  GB_CHECK(scratch(c, 3, w));
+  GB_CUDA(cudaMemcpyAsync(w[0], h1.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CUDA(cudaMemcpyAsync(w[1], h2.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CUDA(cudaMemcpyAsync(w[2], h3.data(), c->cbytes, cudaMemcpyHostToDevice, c->stream));
+  GB_CHECK(rotor3_impl<R>(c, w[1], w[2], ox, 1));
+  GB_CHECK(rotor3_impl<R>(c, w[0], w[2], oy, 2));
+  GB_CHECK(rotor3_impl<R>(c, w[0], w[1], oz, 3));
+  std::vector<double> e(c->nruns);
+  GB_CHECK(batch_reduce_dev<R>(c, RED_ENERGY, ox, oy, oz, e.data()));
+  double *part;
+  GB_CHECK(partials(c, (size_t)c->nruns, &part));
+  GB_CUDA(cudaMemcpyAsync(part, e.data(), sizeof(double) * c->nruns, cudaMemcpyHostToDevice, c->stream));
+  const int ts = timer_begin(c, GHOST_TIMER_POINTWISE);
+  scale3_runs_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>((cx<R> *)ox, (cx<R> *)oy, (cx<R> *)oz, c->nspec,
+                                                                  c->nruns, (R)amp, part);
+  timer_end(c, ts);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
 }  // namespace gb
 
 using namespace gb;
@@ -940,6 +1014,10 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->anis = c->arbsize ? 1 : ((nx != ny) || (ny != nz));
   c->nspec = (size_t)nz * ny * c->nxh;
   c->nreal = (size_t)nx * ny * nz;
+  c->nruns = 1;
+  c->ntot = c->nspec;
+  c->nu_run = nullptr;
+  c->tile_cfg = 0;
   const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
   c->cbytes = c->nspec * 2 * rs;
   c->rbytes = c->nreal * rs;
@@ -989,6 +1067,7 @@ int ghost_ctx_destroy(ghost_ctx *c) {
   cudaFree(c->tw_z);
   cudaFree(c->partials);
   cudaFree(c->status);
+  cudaFree(c->nu_run);
   cudaFree(c->prune_lines);
   cudaFree(c->prune_jpos);
   cudaFree(c->prune_jneg);
@@ -1597,6 +1676,311 @@ int ghost_spectrumc_noalloc(ghost_ctx *c, const void *a, const void *b, const vo
   if (hel == 1)
     GB_CHECK(sp ? spectrum_noalloc_dev<float>(c, scratch, RED_HELICITY, a, b, cc, Hk)
                 : spectrum_noalloc_dev<double>(c, scratch, RED_HELICITY, a, b, cc, Hk));
+  return GHOST_OK;
+}
+
+
+// ------------------------------------------------------------- batches
+int ghost_ctx_create_batch(int nx, int ny, int nz, int nruns, int precision, ghost_ctx **out) {
+  if (nruns < 1) return fail(GHOST_ERR_ARG, "nruns=%d", nruns);
+  GB_CHECK(ghost_ctx_create(nx, ny, nz, 1, 1, 1, 0, precision, out));
+  ghost_ctx *c = *out;
+  c->nruns = nruns;
+  c->ntot = c->nspec * (size_t)nruns;
+  c->cbytes = c->ntot * 2 * (c->precision == GHOST_SINGLE ? 4 : 8);
+  refresh_kparams(c);
+  return GHOST_OK;
+}
+
+int ghost_batch_set_nu(ghost_ctx *c, const double *nu) {
+  CTX_CHECK(c);
+  if (!nu) return fail(GHOST_ERR_ARG, "null nu");
+  const size_t rs = c->precision == GHOST_SINGLE ? 4 : 8;
+  if (!c->nu_run) GB_CHECK(dalloc(&c->nu_run, rs * c->nruns));
+  std::vector<unsigned char> h(rs * c->nruns);
+  for (int r = 0; r < c->nruns; ++r) {
+    if (rs == 4) ((float *)h.data())[r] = (float)nu[r];
+    else ((double *)h.data())[r] = nu[r];
+  }
+  GB_CUDA(cudaMemcpyAsync(c->nu_run, h.data(), h.size(), cudaMemcpyHostToDevice, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  refresh_kparams(c);
+  return GHOST_OK;
+}
+
+int ghost_batch_energy(ghost_ctx *c, const void *a, const void *b, const void *cc, int kin, double *out) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !out) return fail(GHOST_ERR_ARG, "null argument");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  Staging st(c);
+  const void *da, *db, *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  const int kind = kin == 1 ? RED_ENERGY : (kin == 0 ? RED_ENSTROPHY : RED_LAPLACIAN);
+  GB_CHECK(c->precision == GHOST_SINGLE ? batch_reduce_dev<float>(c, kind, da, db, dc, out)
+                                        : batch_reduce_dev<double>(c, kind, da, db, dc, out));
+  return st.finish();
+}
+
+int ghost_batch_init_random_solenoidal(ghost_ctx *c, int32_t *seeds, double kdn, double kup, int shape, double amp,
+                                       void *ox, void *oy, void *oz) {
+  CTX_CHECK(c);
+  if (!seeds || !ox || !oy || !oz) return fail(GHOST_ERR_ARG, "null argument");
+  if (shape != 0 && shape != 1) return fail(GHOST_ERR_ARG, "shape %d not in 0..1", shape);
+  Staging st(c);
+  void *a, *b, *cc;
+  GB_CHECK(st.map(ox, c->cbytes, 2, &a));
+  GB_CHECK(st.map(oy, c->cbytes, 2, &b));
+  GB_CHECK(st.map(oz, c->cbytes, 2, &cc));
+  std::vector<int32_t> in(seeds, seeds + c->nruns);
+  GB_CHECK(c->precision == GHOST_SINGLE
+               ? batch_init_random_dev<float>(c, in.data(), seeds, kdn, kup, shape, amp, a, b, cc)
+               : batch_init_random_dev<double>(c, in.data(), seeds, kdn, kup, shape, amp, a, b, cc));
+  return st.finish();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ ensembles
+struct ghost_ensemble {
+  int ncls = 0, precision = 0;
+  int n[8] = {0}, nruns[8] = {0};
+  ghost_ctx *cls[8] = {nullptr};
+  void *v[8][3] = {{nullptr}};
+  cudaStream_t main = nullptr, streams[8] = {nullptr};
+  cudaEvent_t fork = nullptr, join[8] = {nullptr};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_ord = 0;
+  double graph_dt = 0.0;
+  bool stepped = false;  // one uncaptured step done: fields dealiased, tables and scratch built
+};
+
+namespace gb {
+// one RK step (ord substeps, RK1 copy folded in) of one class on its stream
+static int ensemble_class_step(ghost_ensemble *e, int q, int ord, double dt, bool prune_all) {
+  ghost_ctx *c = e->cls[q];
+  void *v[3] = {e->v[q][0], e->v[q][1], e->v[q][2]};
+  for (int k = 0; k < 3; ++k)
+    if (!c->rk[k]) GB_CHECK(dalloc(&c->rk[k], c->cbytes));
+  void *C[3] = {c->rk[0], c->rk[1], c->rk[2]};
+  for (int o = ord; o >= 1; --o) {
+    const bool prune = prune_all || o != ord;
+    GB_CHECK(c->precision == GHOST_SINGLE ? hd_substep_dev<float>(c, o, dt, 0.0, v, C, nullptr, o == ord, prune)
+                                          : hd_substep_dev<double>(c, o, dt, 0.0, v, C, nullptr, o == ord, prune));
+  }
+  return GHOST_OK;
+}
+
+static int ensemble_capture(ghost_ensemble *e, int ord, double dt) {
+  if (e->exec) {
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  if (e->graph) {
+    cudaGraphDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  GB_CUDA(cudaStreamBeginCapture(e->main, cudaStreamCaptureModeThreadLocal));
+  int st = GHOST_OK;
+  if (cudaEventRecord(e->fork, e->main) != cudaSuccess) st = fail(GHOST_ERR_CUDA, "event record in capture");
+  for (int q = 0; q < e->ncls && st == GHOST_OK; ++q) {
+    if (cudaStreamWaitEvent(e->streams[q], e->fork, 0) != cudaSuccess) {
+      st = fail(GHOST_ERR_CUDA, "stream wait in capture");
+      break;
+    }
+    st = ensemble_class_step(e, q, ord, dt, true);
+    if (st == GHOST_OK && cudaEventRecord(e->join[q], e->streams[q]) != cudaSuccess)
+      st = fail(GHOST_ERR_CUDA, "event record in capture");
+    if (st == GHOST_OK && cudaStreamWaitEvent(e->main, e->join[q], 0) != cudaSuccess)
+      st = fail(GHOST_ERR_CUDA, "join in capture");
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(e->main, &g);
+  if (st != GHOST_OK) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return st;
+  }
+  if (ce != cudaSuccess || !g) {
+    cudaGetLastError();
+    return fail(GHOST_ERR_CUDA, "stream capture of the ensemble step failed: %s", cudaGetErrorString(ce));
+  }
+  e->graph = g;
+  GB_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
+  e->graph_ord = ord;
+  e->graph_dt = dt;
+  return GHOST_OK;
+}
+}  // namespace gb
+
+extern "C" {
+
+int ghost_ensemble_create(int nclasses, const int *n, const int *nruns, int precision, ghost_ensemble **out) {
+  if (!out || !n || !nruns) return fail(GHOST_ERR_ARG, "null argument");
+  if (nclasses < 1 || nclasses > 8) return fail(GHOST_ERR_ARG, "nclasses=%d not in 1..8", nclasses);
+  *out = nullptr;
+  ghost_ensemble *e = new ghost_ensemble();
+  e->ncls = nclasses;
+  e->precision = precision;
+  int st = GHOST_OK;
+  if (cudaStreamCreateWithFlags(&e->main, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+    st = fail(GHOST_ERR_CUDA, "stream/event creation failed");
+  for (int q = 0; q < nclasses && st == GHOST_OK; ++q) {
+    e->n[q] = n[q];
+    e->nruns[q] = nruns[q];
+    st = ghost_ctx_create_batch(n[q], n[q], n[q], nruns[q], precision, &e->cls[q]);
+    if (st != GHOST_OK) break;
+    if (cudaStreamCreateWithFlags(&e->streams[q], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) != cudaSuccess) {
+      st = fail(GHOST_ERR_CUDA, "stream/event creation failed");
+      break;
+    }
+    e->cls[q]->stream = e->streams[q];
+    for (int k = 0; k < 3 && st == GHOST_OK; ++k) {
+      st = dalloc(&e->v[q][k], e->cls[q]->cbytes);
+      if (st == GHOST_OK && cudaMemset(e->v[q][k], 0, e->cls[q]->cbytes) != cudaSuccess)
+        st = fail(GHOST_ERR_CUDA, "memset failed");
+    }
+  }
+  if (st != GHOST_OK) {
+    ghost_ensemble_destroy(e);
+    return st;
+  }
+  *out = e;
+  return GHOST_OK;
+}
+
+int ghost_ensemble_destroy(ghost_ensemble *e) {
+  if (!e) return GHOST_OK;
+  if (e->main) cudaStreamSynchronize(e->main);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (int q = 0; q < e->ncls; ++q) {
+    if (e->streams[q]) cudaStreamSynchronize(e->streams[q]);
+    for (int k = 0; k < 3; ++k) cudaFree(e->v[q][k]);
+    if (e->cls[q]) ghost_ctx_destroy(e->cls[q]);
+    if (e->streams[q]) cudaStreamDestroy(e->streams[q]);
+    if (e->join[q]) cudaEventDestroy(e->join[q]);
+  }
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->main) cudaStreamDestroy(e->main);
+  delete e;
+  return GHOST_OK;
+}
+
+int ghost_ensemble_fields(ghost_ensemble *e, int q, void **vx, void **vy, void **vz) {
+  if (!e || q < 0 || q >= e->ncls || !vx || !vy || !vz) return fail(GHOST_ERR_ARG, "bad argument");
+  *vx = e->v[q][0];
+  *vy = e->v[q][1];
+  *vz = e->v[q][2];
+  return GHOST_OK;
+}
+
+int ghost_ensemble_class(ghost_ensemble *e, int q, ghost_ctx **ctx) {
+  if (!e || q < 0 || q >= e->ncls || !ctx) return fail(GHOST_ERR_ARG, "bad argument");
+  *ctx = e->cls[q];
+  return GHOST_OK;
+}
+
+int ghost_ensemble_init(ghost_ensemble *e, const int32_t *seeds, double kdn, double kup_frac, int shape, double amp,
+                        const double *nu) {
+  if (!e || !seeds || !nu) return fail(GHOST_ERR_ARG, "null argument");
+  int off = 0;
+  for (int q = 0; q < e->ncls; ++q) {
+    std::vector<int32_t> s(seeds + off, seeds + off + e->nruns[q]);
+    GB_CHECK(ghost_batch_init_random_solenoidal(e->cls[q], s.data(), kdn, kup_frac * e->n[q], shape, amp, e->v[q][0],
+                                                e->v[q][1], e->v[q][2]));
+    GB_CHECK(ghost_batch_set_nu(e->cls[q], nu + off));
+    off += e->nruns[q];
+  }
+  e->stepped = false;
+  return GHOST_OK;
+}
+
+int ghost_ensemble_autotune(ghost_ensemble *e, int ord, double dt, int *cfg_out) {
+  if (!e || ord < 1) return fail(GHOST_ERR_ARG, "bad argument");
+  for (int q = 0; q < e->ncls; ++q) {
+    ghost_ctx *c = e->cls[q];
+    // tune on a copy of the state: the ensemble itself does not advance
+    void *save[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; ++k) {
+      GB_CHECK(dalloc(&save[k], c->cbytes));
+      GB_CUDA(cudaMemcpyAsync(save[k], e->v[q][k], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    int best_cfg = 0;
+    int st = GHOST_OK;
+    for (int cfg = 0; cfg < 4 && st == GHOST_OK; ++cfg) {
+      c->tile_cfg = cfg;
+      float tot = 0.f;
+      for (int rep = 0; rep < 3 && st == GHOST_OK; ++rep) {
+        for (int k = 0; k < 3; ++k) cudaMemcpyAsync(e->v[q][k], save[k], c->cbytes, cudaMemcpyDeviceToDevice, c->stream);
+        cudaEventRecord(a, c->stream);
+        st = ensemble_class_step(e, q, ord, dt, false);
+        cudaEventRecord(b, c->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0) tot += ms;  // first repetition warms up
+      }
+      if (tot < best) {
+        best = tot;
+        best_cfg = cfg;
+      }
+    }
+    c->tile_cfg = best_cfg;
+    if (cfg_out) cfg_out[q] = best_cfg;
+    for (int k = 0; k < 3; ++k) cudaMemcpyAsync(e->v[q][k], save[k], c->cbytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+    for (int k = 0; k < 3; ++k) cudaFree(save[k]);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    GB_CHECK(st);
+    GB_CHECK(check_status(c));
+  }
+  if (e->exec) {  // a new tile choice needs a new graph
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  return GHOST_OK;
+}
+
+int ghost_ensemble_run(ghost_ensemble *e, int nsteps, int ord, double dt) {
+  if (!e || nsteps < 0 || ord < 1) return fail(GHOST_ERR_ARG, "bad argument");
+  int done = 0;
+  if (!e->stepped && nsteps > 0) {
+    // one uncaptured step: reads every mode once, builds tables and scratch
+    for (int q = 0; q < e->ncls; ++q) GB_CHECK(ensemble_class_step(e, q, ord, dt, false));
+    for (int q = 0; q < e->ncls; ++q) GB_CUDA(cudaStreamSynchronize(e->streams[q]));
+    e->stepped = true;
+    done = 1;
+  }
+  if (done < nsteps) {
+    if (!e->exec || e->graph_ord != ord || e->graph_dt != dt) GB_CHECK(ensemble_capture(e, ord, dt));
+    for (int q = 0; q < e->ncls; ++q) GB_CUDA(cudaStreamSynchronize(e->streams[q]));
+    for (; done < nsteps; ++done) {
+      GB_CUDA(cudaGraphLaunch(e->exec, e->main));
+      for (int q = 0; q < e->ncls; ++q) e->cls[q]->launches += 10LL * ord / 2;
+    }
+    GB_CUDA(cudaStreamSynchronize(e->main));
+  }
+  for (int q = 0; q < e->ncls; ++q) GB_CHECK(check_status(e->cls[q]));
+  return GHOST_OK;
+}
+
+int ghost_ensemble_energy(ghost_ensemble *e, int kin, double *out) {
+  if (!e || !out) return fail(GHOST_ERR_ARG, "null argument");
+  int off = 0;
+  for (int q = 0; q < e->ncls; ++q) {
+    GB_CHECK(ghost_batch_energy(e->cls[q], e->v[q][0], e->v[q][1], e->v[q][2], kin, out + off));
+    off += e->nruns[q];
+  }
   return GHOST_OK;
 }
 

@@ -40,6 +40,10 @@ template <typename R> struct KParams {
   R rmp, rmq, rms;  // per-axis normalisation of kn2 when anis
   R kmax, tiny;
   R tmp;            // 1/(nx ny nz)^2
+  // batches of independent runs of one grid: fields hold nruns runs one
+  // after the other, i.e. the kx index runs over nxh*nruns
+  int nruns;
+  const R *nu_run;  // per-run viscosity (batched RK), or null
 };
 
 template <typename R> __device__ __forceinline__ R kx_of(const KParams<R> &p, int i) {
@@ -107,6 +111,10 @@ struct ghost_ctx {
   void *rk[4];
   gb::KParams<float> kp32;
   gb::KParams<double> kp64;
+  int nruns;          // runs in a batched context (1 otherwise)
+  size_t ntot;        // nspec * nruns
+  void *nu_run;       // per-run viscosity on the device (precision of ctx), or null
+  int tile_cfg;       // autotuned tile variant (bit 0: y tile 16 wide, bit 1: z CTAs of 128 threads)
   int num_sms;
   // device status word written by kernels whose bounded waits ran out
   int *status;

@@ -10,7 +10,7 @@ template <typename R> __device__ __forceinline__ void unflat(const KParams<R> &k
   k = (int)(p % kp.nz);
   size_t q = p / kp.nz;
   j = (int)(q % kp.ny);
-  i = (int)(q / kp.ny);
+  i = (int)(q / kp.ny) % kp.nxh;  // batched fields: the run index is folded into kx
 }
 
 // i*kd*a as the Fortran expression im*k*a evaluates it
@@ -186,6 +186,39 @@ __global__ void __launch_bounds__(256) reduce_kernel(KParams<R> kp, RedArgs<R> r
   }
   const double s = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// Per-run sums of a batched field: block (x, run) covers run `run`;
+// partials laid out [block][run] for finalize_kernel.
+template <typename R>
+__global__ void __launch_bounds__(256) reduce_runs_kernel(KParams<R> kp, RedArgs<R> ra, int kind, size_t nspec,
+                                                          int nruns, double *partials) {
+  __shared__ double sh[32];
+  const size_t base = (size_t)blockIdx.y * nspec;
+  double acc = 0.0;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < nspec; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, base + p, i, j, k);
+    const double w = i == 0 ? 1.0 : 2.0;
+    acc += w * (double)red_term(kp, ra, kind, base + p, i, j, k);
+  }
+  const double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[(size_t)blockIdx.x * nruns + blockIdx.y] = s;
+}
+
+// f = f*f0/sqrt(e_run) per run of a batched field (normalize, per run)
+template <typename R>
+__global__ void scale3_runs_kernel(cx<R> *x, cx<R> *y, cx<R> *z, size_t nspec, int nruns, R f0, const double *e) {
+  const size_t n = nspec * (size_t)nruns;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const double s = sqrt(e[p / nspec]);
+    cx<R> *f[3] = {x, y, z};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const cx<R> v = f[c][p];
+      f[c][p] = mk((R)((double)(v.x * f0) / s), (R)((double)(v.y * f0) / s));
+    }
+  }
 }
 
 // Sums nparts partials in a fixed order (one block).  Also used for the

@@ -180,7 +180,7 @@ template <typename R, int PHYS> struct ZInv {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
+    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     if (copy && act) {
 #pragma unroll
@@ -241,8 +241,9 @@ template <typename R> struct ZFwdHD {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
+    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
+    const R nuv = kp.nu_run ? kp.nu_run[ir / kp.nxh] : nu;
     C g[3][E];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -270,7 +271,7 @@ template <typename R> struct ZFwdHD {
         for (int c = 0; c < 3; ++c) {
           const C vv = v.p[c][p];
           const C lap = mk(-kk2 * vv.x, -kk2 * vv.y);
-          C sum = mk(nu * lap.x + nl3[c].x, nu * lap.y + nl3[c].y);
+          C sum = mk(nuv * lap.x + nl3[c].x, nuv * lap.y + nl3[c].y);
           if (forced) {
             const C ff = f.p[c][p];
             sum = mk(sum.x + ff.x, sum.y + ff.y);
@@ -303,7 +304,7 @@ template <typename R> struct ZFwdBouss {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny);
+    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     C g[4][E];
 #pragma unroll
@@ -378,7 +379,7 @@ template <typename R, int N, int E, int BZ> struct YGeom {
 template <typename R, int N, int E, int BZ, int STAGES, int S>
 __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
                                                              const cx<R> *__restrict__ twg, int nz, int ni, int nf,
-                                                             const int *__restrict__ jpos,
+                                                             int nruns, int nxh, const int *__restrict__ jpos,
                                                              const int *__restrict__ jneg, int rb, PipeCtl ctl) {
   using C = cx<R>;
   using G = YGeom<R, N, E, BZ>;
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
   uint64_t *bars = reinterpret_cast<uint64_t *>(tw + N);
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
   const int nzb = nz / BZ;
-  const int ntiles = nzb * ni * nf;
+  const int ntiles = nzb * ni * nruns * nf;
   if (tid == 0) {
     for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
     fence_barrier_init();
@@ -397,14 +398,16 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
   for (int e = tid; e < N; e += NT) tw[e] = twg[e];
   __syncthreads();
   struct Tile {
-    int zb, i, f;
+    int zb, ii, i, f;  // ii: kx index within the run, i: plane of the batched field
   };
   auto tile_of = [&](int tile) {
     Tile r;
     r.zb = tile % nzb;
-    const int q = tile / nzb;
-    r.i = q % ni;
-    r.f = q / ni;
+    int q = tile / nzb;
+    r.ii = q % ni;
+    q /= ni;
+    r.i = (q % nruns) * nxh + r.ii;
+    r.f = q / nruns;
     return r;
   };
   auto rows_of = [&](int i, int &jp, int &jn) {
@@ -425,7 +428,7 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
     if (tile >= ntiles || tid != 0) return;
     const Tile tl = tile_of(tile);
     int jp, jn;
-    rows_of(tl.i, jp, jn);
+    rows_of(tl.ii, jp, jn);
     const int s = k % STAGES;
     const int nb_top = (jp + rb - 1) / rb, nb_bot = (jn + rb - 1) / rb;
     fence_proxy_async();
@@ -456,8 +459,8 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
     const Tile tl = tile_of(tile);
     int jp = N, jn = 0;
     if (jpos) {
-      jp = jpos[tl.i];
-      jn = jneg[tl.i];
+      jp = jpos[tl.ii];
+      jn = jneg[tl.ii];
     }
     C *sb = stage + (size_t)s * G::stage_elems;
     C x[E];
@@ -561,7 +564,7 @@ template <typename R, int NX, int E, int BZ, int PHYS, int STAGES>
 __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
                                                                     Fields<R> out, const cx<R> *__restrict__ twg,
                                                                     int ny, int nz, R scale, int rows, int nbox,
-                                                                    int rb, PipeCtl ctl) {
+                                                                    int rb, int nruns, int nxh, PipeCtl ctl) {
   using C = cx<R>;
   using G = XGeom<R, NX, BZ>;
   constexpr int M = NX / 2, T = M / E, NT = BZ * T;
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
   uint64_t *bars = reinterpret_cast<uint64_t *>(xb + (size_t)M * BZ);
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
   const int nzb = nz / BZ;
-  const int ntiles = nzb * ny;
+  const int ntiles = nzb * ny * nruns;
   const size_t rowstride = (size_t)nz * ny;
   if (tid == 0) {
     for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
@@ -592,7 +595,8 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
     mbar_arrive_expect_tx(&bars[s], (uint32_t)(nbox * rb) * BZ * (uint32_t)sizeof(C));
     C *dst = stage + (size_t)s * G::stage_elems;
     for (int q = 0; q < nbox; ++q)
-      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[f], (tile % nzb) * BZ * U, tile / nzb, q * rb, &bars[s]);
+      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[f], (tile % nzb) * BZ * U, (tile / nzb) % ny,
+                  (tile / nzb / ny) * nxh + q * rb, &bars[s]);
   };
   for (int L = 0; L < STAGES - 1; ++L) issue(L);
   auto buf = [xb, l](int idx) -> C & { return xb[idx * BZ + l]; };
@@ -671,7 +675,8 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
 #pragma unroll
       for (int e = 0; e < E; ++e) buf(t + T * e) = P[c][e];
       __syncthreads();
-      obase = out.p[c] + (size_t)(tile % nzb) * BZ + (size_t)nz * (tile / nzb) + l;
+      obase = out.p[c] + (size_t)(tile % nzb) * BZ + (size_t)nz * ((tile / nzb) % ny) +
+              rowstride * (size_t)((tile / nzb / ny) * nxh) + l;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int kk = t + T * e;

@@ -273,6 +273,92 @@
          REAL(C_DOUBLE), VALUE :: dt, nu, kappa, omegaz, xmom, xtemp
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_ctx_create_batch(nx,ny,nz,nruns,prec,ctx) &
+                BIND(C,name="ghost_ctx_create_batch") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         INTEGER(C_INT), VALUE :: nx, ny, nz, nruns, prec
+         TYPE(C_PTR) :: ctx
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_batch_set_nu(ctx,nu) BIND(C,name="ghost_batch_set_nu") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx
+         REAL(C_DOUBLE) :: nu(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_batch_energy(ctx,a,b,c,kin,out) BIND(C,name="ghost_batch_energy") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: out(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_batch_init_random_solenoidal(ctx,seeds,kdn,kup,shape,amp,ox,oy,oz) &
+                BIND(C,name="ghost_batch_init_random_solenoidal") RESULT(s)
+         IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, ox, oy, oz
+         INTEGER(C_INT32_T) :: seeds(*)
+         REAL(C_DOUBLE), VALUE :: kdn, kup, amp
+         INTEGER(C_INT), VALUE :: shape
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_create(ncls,n,nruns,prec,ens) BIND(C,name="ghost_ensemble_create") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         INTEGER(C_INT), VALUE :: ncls, prec
+         INTEGER(C_INT) :: n(*), nruns(*)
+         TYPE(C_PTR) :: ens
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_destroy(ens) BIND(C,name="ghost_ensemble_destroy") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_fields(ens,c,vx,vy,vz) BIND(C,name="ghost_ensemble_fields") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: c
+         TYPE(C_PTR) :: vx, vy, vz
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_class(ens,c,ctx) BIND(C,name="ghost_ensemble_class") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: c
+         TYPE(C_PTR) :: ctx
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_init(ens,seeds,kdn,kupf,shape,amp,nu) BIND(C,name="ghost_ensemble_init") RESULT(s)
+         IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT32_T) :: seeds(*)
+         REAL(C_DOUBLE), VALUE :: kdn, kupf, amp
+         INTEGER(C_INT), VALUE :: shape
+         REAL(C_DOUBLE) :: nu(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_autotune(ens,ord,dt,cfg) BIND(C,name="ghost_ensemble_autotune") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: ord
+         REAL(C_DOUBLE), VALUE :: dt
+         INTEGER(C_INT) :: cfg(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_run(ens,nsteps,ord,dt) BIND(C,name="ghost_ensemble_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_energy(ens,kin,out) BIND(C,name="ghost_ensemble_energy") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: out(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_init_random_solenoidal(ctx,seed,kdn,kup,shape,amp,ox,oy,oz) &
                 BIND(C,name="ghost_init_random_solenoidal") RESULT(s)
          IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE

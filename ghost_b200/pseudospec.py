@@ -45,15 +45,22 @@ class Ghost:
 
     def __init__(self, nx: int, ny: int | None = None, nz: int | None = None,
                  Lx: float = 1.0, Ly: float = 1.0, Lz: float = 1.0, arbsize: bool = False,
-                 precision: str = "fp64", stream=None):
+                 precision: str = "fp64", stream=None, nruns: int = 1, handle=None):
         ny = nx if ny is None else ny
         nz = nx if nz is None else nz
         self.lib = _lib.load()
         self.precision = precision
+        self.nruns = nruns
+        self.owned = handle is None
         code = {"fp32": GHOST_SINGLE, "fp64": GHOST_DOUBLE}[precision]
         h = ctypes.c_void_p()
-        check(self.lib.ghost_ctx_create(nx, ny, nz, Lx, Ly, Lz, int(bool(arbsize)), code, ctypes.byref(h)),
-              "ghost_ctx_create")
+        if handle is not None:
+            h = handle
+        elif nruns > 1:
+            check(self.lib.ghost_ctx_create_batch(nx, ny, nz, nruns, code, ctypes.byref(h)), "ghost_ctx_create_batch")
+        else:
+            check(self.lib.ghost_ctx_create(nx, ny, nz, Lx, Ly, Lz, int(bool(arbsize)), code, ctypes.byref(h)),
+                  "ghost_ctx_create")
         self.h = h
         info = _lib.GhostInfo()
         check(self.lib.ghost_ctx_get_info(self.h, ctypes.byref(info)), "ghost_ctx_get_info")
@@ -63,7 +70,7 @@ class Ghost:
         self.kmax, self.tiny, self.nmax, self.Dkk = info.kmax, info.tiny, info.nmax, info.Dkk
         self.rdtype_np = np.float32 if precision == "fp32" else np.float64
         self.cdtype_np = np.complex64 if precision == "fp32" else np.complex128
-        if stream is None and torch is not None and torch.cuda.is_available():
+        if stream is None and handle is None and torch is not None and torch.cuda.is_available():
             stream = torch.cuda.current_stream().cuda_stream
         if stream is not None:
             check(self.lib.ghost_ctx_set_stream(self.h, ctypes.c_void_p(stream)), "ghost_ctx_set_stream")
@@ -71,7 +78,8 @@ class Ghost:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.ghost_ctx_destroy(self.h)
+            if getattr(self, "owned", True):
+                self.lib.ghost_ctx_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -83,7 +91,7 @@ class Ghost:
     # ------------------------------------------------------------------
     @property
     def sshape(self):
-        return (self.nxh, self.ny, self.nz)
+        return (self.nxh * self.nruns, self.ny, self.nz)
 
     @property
     def rshape(self):
@@ -279,4 +287,96 @@ class Ghost:
         return s.value
 
 
-__all__ = ["Ghost", "FFTPlan", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL"]
+    # ------------------------------------------------------- batches
+    def batch_set_nu(self, nu):
+        arr = np.ascontiguousarray(nu, dtype=np.float64)
+        check(self.lib.ghost_batch_set_nu(self.h, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              "ghost_batch_set_nu")
+
+    def batch_energy(self, a, b, c, kin: int = 1):
+        out = np.zeros(self.nruns)
+        check(self.lib.ghost_batch_energy(self.h, *[self._ptr(x, "c") for x in (a, b, c)], kin,
+                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_batch_energy")
+        return out
+
+    def batch_init_random_solenoidal(self, seeds, kdn, kup, shape, amp, ox, oy, oz):
+        arr = (ctypes.c_int32 * self.nruns)(*seeds)
+        check(self.lib.ghost_batch_init_random_solenoidal(self.h, arr, kdn, kup, shape, amp,
+                                                          *[self._ptr(x, "c") for x in (ox, oy, oz)]),
+              "ghost_batch_init_random_solenoidal")
+        return list(arr)
+
+
+class Ensemble:
+    """Batches of cubic runs of several sizes advanced together: one batched
+    context per size class, one RK step of all classes replayed as a CUDA
+    graph (ghost_ensemble_* of the C ABI)."""
+
+    def __init__(self, sizes, nruns, precision: str = "fp32"):
+        self.lib = _lib.load()
+        self.sizes, self.nruns, self.precision = list(sizes), list(nruns), precision
+        code = {"fp32": GHOST_SINGLE, "fp64": GHOST_DOUBLE}[precision]
+        h = ctypes.c_void_p()
+        n = (ctypes.c_int * len(sizes))(*sizes)
+        r = (ctypes.c_int * len(sizes))(*nruns)
+        check(self.lib.ghost_ensemble_create(len(sizes), n, r, code, ctypes.byref(h)), "ghost_ensemble_create")
+        self.h = h
+        self.total = sum(nruns)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ghost_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, seeds, nu, kdn=1.0, kup_frac=1.0 / 3.0, shape=1, amp=1.0):
+        s = (ctypes.c_int32 * self.total)(*seeds)
+        v = np.ascontiguousarray(nu, dtype=np.float64)
+        check(self.lib.ghost_ensemble_init(self.h, s, kdn, kup_frac, shape, amp,
+                                           v.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_ensemble_init")
+
+    def autotune(self, ord: int, dt: float):
+        cfg = (ctypes.c_int * len(self.sizes))()
+        check(self.lib.ghost_ensemble_autotune(self.h, ord, dt, cfg), "ghost_ensemble_autotune")
+        return list(cfg)
+
+    def run(self, nsteps: int, ord: int, dt: float):
+        check(self.lib.ghost_ensemble_run(self.h, nsteps, ord, dt), "ghost_ensemble_run")
+
+    def energy(self, kin: int = 1):
+        out = np.zeros(self.total)
+        check(self.lib.ghost_ensemble_energy(self.h, kin, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              "ghost_ensemble_energy")
+        return out
+
+    def fields(self, c: int):
+        """Class c's batched velocity as CUDA tensors (nruns*(n/2+1), n, n)."""
+        ptr = [ctypes.c_void_p() for _ in range(3)]
+        check(self.lib.ghost_ensemble_fields(self.h, c, *[ctypes.byref(p) for p in ptr]), "ghost_ensemble_fields")
+        n, r = self.sizes[c], self.nruns[c]
+        shape = (r * (n // 2 + 1), n, n)
+        dt = torch.complex64 if self.precision == "fp32" else torch.complex128
+        return [_tensor_view(p.value, shape, dt) for p in ptr]
+
+    def class_ctx(self, c: int) -> Ghost:
+        h = ctypes.c_void_p()
+        check(self.lib.ghost_ensemble_class(self.h, c, ctypes.byref(h)), "ghost_ensemble_class")
+        n = self.sizes[c]
+        return Ghost(n, precision=self.precision, nruns=self.nruns[c], handle=h)
+
+
+def _tensor_view(ptr: int, shape, dtype):
+    """A CUDA tensor aliasing library-owned device memory (no copy)."""
+    class _Arr:
+        __cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": "<c8" if dtype == torch.complex64 else "<c16",
+            "data": (ptr, False), "version": 3, "strides": None}
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+__all__ = ["Ghost", "Ensemble", "FFTPlan", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL"]

@@ -247,6 +247,46 @@ int ghost_bouss_run(ghost_ctx *ctx, int nsteps, int ord, double dt, double nu, d
                     const void *fx, const void *fy, const void *fz, const void *fs);
 
 /* ---------------------------------------------------------------- */
+/* Batches and ensembles of independent runs (no counterpart in GHOST,
+ * whose runs are separate MPI jobs).  A batched context holds nruns runs of
+ * one grid; its fields are nruns spectral fields one after the other
+ * (nruns*(nx/2+1)*ny*nz complex), so every pass covers the whole batch in
+ * one launch.  ghost_hd_run, the operators and the sums of ghost_energy
+ * act on the whole batch; ghost_batch_* give per-run results. */
+int ghost_ctx_create_batch(int nx, int ny, int nz, int nruns, int precision, ghost_ctx **ctx);
+/* per-run viscosity (host array of nruns); ghost_hd_run then ignores its nu */
+int ghost_batch_set_nu(ghost_ctx *ctx, const double *nu);
+/* per-run energy(kin) into out[nruns] */
+int ghost_batch_energy(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, double *out);
+/* per-run ghost_init_random_solenoidal with seeds[nruns] (updated in place) */
+int ghost_batch_init_random_solenoidal(ghost_ctx *ctx, int32_t *seeds, double kdn, double kup, int shape,
+                                       double amp, void *ox, void *oy, void *oz);
+
+/* An ensemble: batches of cubic runs of several sizes advanced together.
+ * Each class (size n[c], nruns[c] runs) is a batched context on its own
+ * stream; one RK step of every class is captured in a CUDA graph and
+ * replayed.  Runs are numbered class by class. */
+typedef struct ghost_ensemble ghost_ensemble;
+int ghost_ensemble_create(int nclasses, const int *n, const int *nruns, int precision, ghost_ensemble **ens);
+int ghost_ensemble_destroy(ghost_ensemble *ens);
+/* device pointers of class c's batched velocity */
+int ghost_ensemble_fields(ghost_ensemble *ens, int c, void **vx, void **vy, void **vz);
+/* the batched context of class c (for operators and diagnostics) */
+int ghost_ensemble_class(ghost_ensemble *ens, int c, ghost_ctx **ctx);
+/* seeded initial velocities (the recipe of ghost_init_random_solenoidal
+ * with kdn, kup = kup_frac*n, shape, amp) and per-run viscosities */
+int ghost_ensemble_init(ghost_ensemble *ens, const int32_t *seeds, double kdn, double kup_frac, int shape,
+                        double amp, const double *nu);
+/* Times each tile variant of every class on a copy of its state and keeps
+ * the fastest; cfg_out[c] receives the choice (may be NULL). */
+int ghost_ensemble_autotune(ghost_ensemble *ens, int ord, double dt, int *cfg_out);
+/* nsteps RK steps of every run; after one uncaptured step the step is a
+ * replayed CUDA graph */
+int ghost_ensemble_run(ghost_ensemble *ens, int nsteps, int ord, double dt);
+/* per-run energy(kin), runs in class order */
+int ghost_ensemble_energy(ghost_ensemble *ens, int kin, double *out);
+
+/* ---------------------------------------------------------------- */
 /* Seeded initial conditions (host RNG, GHOST's randu of
  * pseudo/pseudospec3D_mod.fpp:130-148) */
 

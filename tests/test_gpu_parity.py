@@ -359,3 +359,56 @@ def test_pruned_substeps_are_bitwise_equal_to_full_ones():
         for oo in (2, 1):
             g.hd_rkstep2(oo, 1e-3, 2e-3, *B, *C)
     assert all(bool((x == y).all()) for x, y in zip(A, B))
+
+
+# ------------------------------------------------------ batches, ensembles
+def test_batched_runs_match_independent_oracle_runs():
+    """A batch of three 32^3 runs with their own seeds and viscosities, one
+    launch per pass, against three oracle runs."""
+    from ghost_b200 import Ghost
+    o = Oracle(32)
+    seeds, nus = [11, 12, 13], [5e-4, 2e-3, 5e-3]
+    g = Ghost(32, precision="fp64", nruns=3)
+    V = [g.czeros() for _ in range(3)]
+    out_seeds = g.batch_init_random_solenoidal(seeds, 1.0, 32 / 3.0, 1, 1.0, *V)
+    g.batch_set_nu(nus)
+    g.hd_run(3, 2, 1e-3, 0.0, *V)
+    nxh = 17
+    for r in range(3):
+        v0, s_after = o.random_solenoidal(seeds[r], 1.0, 32 / 3.0, 1, 1.0)
+        assert out_seeds[r] == s_after
+        ref = o.hd_run(3, 2, 1e-3, nus[r], v0)
+        got = [to_host(x[r * nxh:(r + 1) * nxh]) for x in V]
+        assert rel_l2(got, ref) < 1e-12
+    e = g.batch_energy(*V, 1)
+    assert np.allclose(e, [o.energy(*o.hd_run(3, 2, 1e-3, nus[r], o.random_solenoidal(seeds[r], 1.0, 32 / 3.0, 1, 1.0)[0]), 1)
+                           for r in range(3)], rtol=1e-12)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_ensemble_graph_steps_match_oracle(prec):
+    """Uneven classes (32^3 x 3, 64^3 x 2) stepped by the replayed CUDA graph
+    after autotuning; every run against its own oracle run."""
+    from ghost_b200 import Ensemble
+    sizes, nruns = [32, 64], [3, 2]
+    seeds = [101, 102, 103, 201, 202]
+    nus = [5e-4, 1e-3, 5e-3, 8e-4, 3e-3]
+    ens = Ensemble(sizes, nruns, precision=prec)
+    ens.init(seeds, nus)
+    cfg = ens.autotune(2, 1e-3)
+    assert len(cfg) == 2 and all(0 <= c < 4 for c in cfg)
+    ens.run(4, 2, 1e-3)
+    e = ens.energy(1)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    q = 0
+    for c, (n, r) in enumerate(zip(sizes, nruns)):
+        o = Oracle(n)
+        fields = ens.fields(c)
+        nxh = n // 2 + 1
+        for k in range(r):
+            v0, _ = o.random_solenoidal(seeds[q], 1.0, n / 3.0, 1, 1.0)
+            ref = o.hd_run(4, 2, 1e-3, nus[q], v0)
+            got = [to_host(x[k * nxh:(k + 1) * nxh]).astype(np.complex128) for x in fields]
+            assert rel_l2(got, ref) < tol, (c, k)
+            assert e[q] == pytest.approx(o.energy(*ref, 1), rel=max(tol, 1e-13))
+            q += 1
