@@ -98,6 +98,14 @@ SIGNATURES = {
     "ghost_ensemble_autotune": [P, I, D, ctypes.POINTER(ctypes.c_int)],
     "ghost_ensemble_run": [P, I, I, D],
     "ghost_ensemble_energy": [P, I, PD],
+    "ghost_mlp_create": [I, ctypes.POINTER(P)],
+    "ghost_mlp_destroy": [P],
+    "ghost_mlp_set_stream": [P, P],
+    "ghost_mlp_get_params": [P, P],
+    "ghost_mlp_set_params": [P, P],
+    "ghost_mlp_forward": [P, P, P, I],
+    "ghost_mlp_gradients": [P, P, P, I, P, PD],
+    "ghost_mlp_train_step": [P, P, P, I, ctypes.c_float, PD],
 }
 
 _lib = None

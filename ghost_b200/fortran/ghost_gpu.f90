@@ -359,6 +359,56 @@
          REAL(C_DOUBLE) :: out(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       ! learned subgrid-stress closure (no GHOST counterpart)
+       FUNCTION ghost_mlp_create(seed,mlp) BIND(C,name="ghost_mlp_create") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         INTEGER(C_INT), VALUE :: seed
+         TYPE(C_PTR) :: mlp
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_destroy(mlp) BIND(C,name="ghost_mlp_destroy") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: mlp
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_set_stream(mlp,stream) BIND(C,name="ghost_mlp_set_stream") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: mlp, stream
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_get_params(mlp,params) BIND(C,name="ghost_mlp_get_params") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: mlp
+         REAL(C_FLOAT) :: params(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_set_params(mlp,params) BIND(C,name="ghost_mlp_set_params") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: mlp
+         REAL(C_FLOAT) :: params(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_forward(mlp,x,y,b) BIND(C,name="ghost_mlp_forward") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: mlp, x, y
+         INTEGER(C_INT), VALUE :: b
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_gradients(mlp,x,t,b,grad,loss) BIND(C,name="ghost_mlp_gradients") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: mlp, x, t, grad
+         INTEGER(C_INT), VALUE :: b
+         REAL(C_DOUBLE) :: loss
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mlp_train_step(mlp,x,t,b,lr,loss) BIND(C,name="ghost_mlp_train_step") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT, C_DOUBLE
+         TYPE(C_PTR), VALUE :: mlp, x, t
+         INTEGER(C_INT), VALUE :: b
+         REAL(C_FLOAT), VALUE :: lr
+         REAL(C_DOUBLE) :: loss
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_init_random_solenoidal(ctx,seed,kdn,kup,shape,amp,ox,oy,oz) &
                 BIND(C,name="ghost_init_random_solenoidal") RESULT(s)
          IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE

@@ -299,6 +299,38 @@ int ghost_ensemble_energy(ghost_ensemble *ens, int kin, double *out);
 int ghost_init_random_solenoidal(ghost_ctx *ctx, int32_t *seed, double kdn, double kup, int shape,
                                  double amp, void *ox, void *oy, void *oz);
 
+/* ---------------------------------------------------------------- */
+/* Learned subgrid-stress closure for LES (no counterpart in GHOST; GHOST's
+ * own LES closure is the EDQNM eddy viscosity of 3D/src/edqnm/).
+ * A 10 -> 64 -> 64 -> 6 MLP with GELU activations, BF16 tensor-core
+ * products with FP32 accumulation, FP32 master weights and Adam.
+ * Inputs per grid point: the 9 resolved velocity gradients du_i/dx_j
+ * (row-major i, j) and the filter width; outputs: the 6 independent
+ * components of the subgrid stress (xx, yy, zz, xy, xz, yz).
+ * Parameters (FP32, GHOST_MLP_NPARAM): W1[64][10], b1[64], W2[64][64],
+ * b2[64], W3[6][64], b3[6] (y = W x + b). */
+#define GHOST_MLP_NIN 10
+#define GHOST_MLP_NHID 64
+#define GHOST_MLP_NOUT 6
+#define GHOST_MLP_NPARAM 5254
+typedef struct ghost_mlp ghost_mlp;
+/* Glorot-uniform weights from a seeded host RNG, zero biases; the MLP lives
+ * on the current device */
+int ghost_mlp_create(int seed, ghost_mlp **mlp);
+int ghost_mlp_destroy(ghost_mlp *mlp);
+int ghost_mlp_set_stream(ghost_mlp *mlp, void *stream);
+/* host copies of the FP32 parameters (set resets Adam's moments) */
+int ghost_mlp_get_params(ghost_mlp *mlp, float *params);
+int ghost_mlp_set_params(ghost_mlp *mlp, const float *params);
+/* y[B][6] = mlp(x[B][10]); device arrays */
+int ghost_mlp_forward(ghost_mlp *mlp, const float *x, float *y, int B);
+/* gradient of the mean squared error mean((mlp(x) - t)^2) over B*6 values
+ * (grad and loss on the host, either may be NULL); no update */
+int ghost_mlp_gradients(ghost_mlp *mlp, const float *x, const float *t, int B, float *grad, double *loss);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss; loss may
+ * be NULL (then the call does not synchronise) */
+int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, float lr, double *loss);
+
 #ifdef __cplusplus
 }
 #endif
