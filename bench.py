@@ -37,7 +37,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--grid", type=int, default=N, help="cubic grid size (default 512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     return ap.parse_args()
@@ -96,13 +96,21 @@ class Clocks:
 
 
 def dist_init(args):
+    """One process per GPU from torchrun's environment.  The GPU arm talks
+    over NCCL; the reference arm (host cores only) and GPU-less hosts over
+    gloo."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import datetime
+
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if args.impl == "ours" and torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
@@ -117,7 +125,8 @@ def max_over_ranks(ws, x):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -144,14 +153,14 @@ def cpu_substep_time(n, samples, warmup):
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    t, cores = cpu_substep_time(args.n, max(1, args.steps), max(0, args.warmup))
+    t, cores = cpu_substep_time(args.grid, max(1, args.steps), max(0, args.warmup))
     val = 1.0 / (ORD * t)
-    sample = (f"{max(1, args.steps)} timed RK substeps at {args.n}^3 FP32 (1/{ORD} of an RK{ORD} step each), "
+    sample = (f"{max(1, args.steps)} timed RK substeps at {args.grid}^3 FP32 (1/{ORD} of an RK{ORD} step each), "
               f"after {args.warmup} untimed; steps/s = 1/({ORD} x mean substep time)")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ORD * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": f"HD forced turbulence {args.n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32",
+            "config": {"workload": f"HD forced turbulence {args.grid}^3, RK{ORD}, dt={DT}, nu={NU}, FP32",
                        "runs": "CPU restatement of GHOST's fftp-3 + pseudospec3D_hd path (C, OpenMP)"},
             "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -321,7 +330,7 @@ def prune_fractions(n):
 def run_ours(args, ws, rank, local):
     import torch
     torch.cuda.set_device(local)
-    n = args.n
+    n = args.grid
     peak, peak_kind = peaks()
     clocks = Clocks(local)
 
