@@ -106,6 +106,18 @@ SIGNATURES = {
     "ghost_mlp_forward": [P, P, P, I],
     "ghost_mlp_gradients": [P, P, P, I, P, PD],
     "ghost_mlp_train_step": [P, P, P, I, ctypes.c_float, PD],
+    "ghost_les_create": [P, I, ctypes.POINTER(P)],
+    "ghost_les_destroy": [P],
+    "ghost_les_truncate": [P, P, P, P],
+    "ghost_les_samples": [P, P, P, P, P, ctypes.c_float, P, P],
+    "ghost_les_features": [P, P, P, P, ctypes.c_float, ctypes.c_float, P],
+    "ghost_les_tau_force": [P, P, ctypes.c_float, P, P, P, P, P, P],
+    "ghost_les_set_model": [P, I, P, D, D, D, D],
+    "ghost_les_set_time": [P, D],
+    "ghost_les_closure_force": [P, D, P, P, P, P, P, P, P, P, P],
+    "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
+    "ghost_les_edqnm_last": [P, PD, PD, PD],
+    "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
 }
 
 _lib = None

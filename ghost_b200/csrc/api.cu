@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "ic_host.h"
+#include "internal.cuh"
 #include "ops.cuh"
 #include "passes.cuh"
 
@@ -41,7 +42,7 @@ static bool pow2_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; 
 
 // ---------------------------------------------------------------------
 // device memory helpers
-static int dalloc(void **p, size_t bytes) {
+int dalloc(void **p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -52,7 +53,7 @@ static int dalloc(void **p, size_t bytes) {
 }
 
 // scratch spectral fields 0..n-1 (each cbytes), grown on demand
-static int scratch(ghost_ctx *c, int n, void **out) {
+int scratch(ghost_ctx *c, int n, void **out) {
   while ((int)c->scratch.size() < n) {
     void *p;
     GB_CHECK(dalloc(&p, c->cbytes));
@@ -79,7 +80,7 @@ static int partials(ghost_ctx *c, size_t n, double **out) {
 // ---------------------------------------------------------------------
 // host-array staging: pointers that are not device memory are copied
 // through context buffers, and the call syncs before returning.
-static bool is_device_ptr(const void *p) {
+bool is_device_ptr(const void *p) {
   cudaPointerAttributes a;
   cudaError_t e = cudaPointerGetAttributes(&a, p);
   if (e != cudaSuccess) {
@@ -89,7 +90,7 @@ static bool is_device_ptr(const void *p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-static int check_status(ghost_ctx *c);
+int check_status(ghost_ctx *c);
 
 struct Staging {
   ghost_ctx *c;
@@ -148,14 +149,14 @@ template <typename R> const KParams<R> &kparams(const ghost_ctx *c);
 template <> const KParams<float> &kparams<float>(const ghost_ctx *c) { return c->kp32; }
 template <> const KParams<double> &kparams<double>(const ghost_ctx *c) { return c->kp64; }
 
-static int post_launch(ghost_ctx *c) {
+int post_launch(ghost_ctx *c) {
   c->launches++;
   GB_CUDA(cudaGetLastError());
   return GHOST_OK;
 }
 
 // Reads and clears the device status word (caller has synchronised).
-static int check_status(ghost_ctx *c) {
+int check_status(ghost_ctx *c) {
   if (!c->status) return GHOST_OK;
   int st = 0;
   GB_CUDA(cudaMemcpy(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost));
@@ -215,7 +216,7 @@ template <typename R, int P> struct ZKind<ZInv<R, P>> { static constexpr int val
 template <typename R> struct ZKind<ZFwdHD<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
 template <typename R> struct ZKind<ZFwdBouss<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
 
-static int grid1d(size_t n) {
+int grid1d(size_t n) {
   size_t b = (n + 255) / 256;
   return (int)std::min<size_t>(b, 148 * 16);
 }
@@ -581,7 +582,7 @@ template <typename R> int prodre3_dev(ghost_ctx *c, const void *a, const void *b
 // hd_rkstep1 folded in when copy != 0.
 template <typename R>
 int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], void *const C[3], const void *const f[3],
-                   int copy, bool prune = false) {
+                   int copy, bool prune) {
   void *w[6];
   GB_CHECK(scratch(c, 6, w));
   Prune pr;
@@ -975,6 +976,18 @@ int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out
   GB_CUDA(cudaStreamSynchronize(c->stream));
   return GHOST_OK;
 }
+
+// instantiations used by the other translation units (internal.cuh)
+#define GB_INST(R)                                                                                             \
+  template int r2c_dev<R>(ghost_ctx *, const void *, void *);                                                  \
+  template int c2r_dev<R>(ghost_ctx *, const void *, void *);                                                  \
+  template int derivk3_impl<R>(ghost_ctx *, const void *, void *, int);                                        \
+  template int hd_substep_dev<R>(ghost_ctx *, int, double, double, void *const[3], void *const[3],             \
+                                 const void *const[3], int, bool);                                             \
+  template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);
+GB_INST(float)
+GB_INST(double)
+#undef GB_INST
 
 }  // namespace gb
 

@@ -1,0 +1,724 @@
+// les.cu -- large-eddy simulation on a coarse grid: sharp-filter data from
+// a fine (DNS) grid, the learned subgrid-stress closure (the MLP of
+// mlp.cu) and GHOST's EDQNM eddy viscosity as its fallback.
+//
+// Conventions (GHOST's): spectral fields are unnormalised, a(k,j,i) with z
+// fastest; a field on an n^3 grid carries n^3 times its Fourier
+// coefficients, so moving a mode from the N^3 grid to the n^3 grid scales
+// it by (n/N)^3.  The sharp filter keeps kx^2+ky^2+kz^2 <= kc^2 (GHOST's
+// sharp, pseudospec3D_filt.f90:200-241, with Delta = pi/kc).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/ghost_b200.h"
+#include "common.cuh"
+#include "internal.cuh"
+
+using namespace gb;
+
+namespace les {
+
+constexpr int RED_ENERGY_KIND = 0;
+
+// ---------------------------------------------------------------------
+// kernels
+
+// out (coarse n^3 spectrum) = modes of in (fine N^3 spectrum) with
+// |k|^2 <= kc2, times scale; the rest zero.  One thread per coarse mode.
+template <typename R>
+__global__ void truncate_kernel(const cx<R> *__restrict__ in, cx<R> *__restrict__ out, int n, int N, int kc2, R scale) {
+  const int nxh = n / 2 + 1;
+  const size_t total = (size_t)nxh * n * n;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(p % n), j = (int)((p / n) % n), i = (int)(p / ((size_t)n * n));
+    const int kx = i < n / 2 ? i : i - n, ky = j < n / 2 ? j : j - n, kz = k < n / 2 ? k : k - n;
+    cx<R> v;
+    v.x = 0;
+    v.y = 0;
+    if (kx >= 0 && kx * kx + ky * ky + kz * kz <= kc2) {
+      const int jf = ky >= 0 ? ky : ky + N, kf = kz >= 0 ? kz : kz + N;
+      const cx<R> a = in[((size_t)kx * N + jf) * N + kf];
+      v.x = a.x * scale;
+      v.y = a.y * scale;
+    }
+    out[p] = v;
+  }
+}
+
+// p = (a * sa) (b * sb) on a real grid
+template <typename R>
+__global__ void product_kernel(const R *__restrict__ a, const R *__restrict__ b, R *__restrict__ p, size_t n, R s) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    p[q] = (a[q] * s) * (b[q] * s);
+}
+
+// Inputs of the closure at every grid point q: x[q][3a+b] = du_a/dx_b
+// (g[3a+b] holds n^3 times it) times gs, x[q][9] = delta.
+template <typename R> struct GradFields {
+  const R *g[9];
+};
+template <typename R>
+__global__ void features_kernel(GradFields<R> gf, float *__restrict__ x, size_t n, R inv_n3, float gs, float delta) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    float *row = x + q * GHOST_MLP_NIN;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) row[c] = (float)(gf.g[c][q] * inv_n3) * gs;
+    row[9] = delta;
+  }
+}
+
+// Targets: tau[q][m] = filt(u_a u_b) - ubar_a ubar_b for the pairs m =
+// xx, yy, zz, xy, xz, yz; P[m] holds n^3 filt(u_a u_b), U[a] n^3 ubar_a.
+template <typename R> struct TauFields {
+  const R *P[6];
+  const R *U[3];
+};
+__constant__ int kPairA[6] = {0, 1, 2, 0, 0, 1};
+__constant__ int kPairB[6] = {0, 1, 2, 1, 2, 2};
+template <typename R>
+__global__ void targets_kernel(TauFields<R> tf, float *__restrict__ tau, size_t n, R inv_n3, float ts) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const R u[3] = {tf.U[0][q] * inv_n3, tf.U[1][q] * inv_n3, tf.U[2][q] * inv_n3};
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+      tau[q * GHOST_MLP_NOUT + m] = (float)(tf.P[m][q] * inv_n3 - u[kPairA[m]] * u[kPairB[m]]) * ts;
+  }
+}
+
+// tau rows (closure output, scaled by 1/ts) -> six real fields (physical)
+template <typename R> struct RealOut6 {
+  R *t[6];
+};
+template <typename R>
+__global__ void unpack_tau_kernel(const float *__restrict__ tau, RealOut6<R> o, size_t n, float ts) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) o.t[m][q] = (R)(tau[q * GHOST_MLP_NOUT + m] * ts);
+  }
+}
+
+// o_a = f_a + P(-i k_b T_ab), T the six transformed stresses; P the Leray
+// projection; modes outside tiny <= kn2 <= kmax get f only.
+template <typename R> struct Spec6 {
+  const cx<R> *T[6];
+};
+template <typename R> struct Spec3 {
+  const cx<R> *p[3];
+};
+template <typename R> struct Spec3w {
+  cx<R> *p[3];
+};
+template <typename R>
+__global__ void tau_force_kernel(KParams<R> kp, Spec6<R> T, Spec3<R> f, Spec3w<R> o, size_t total) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
+    const R kn2 = kn2_of(kp, i, j, k);
+    cx<R> F[3] = {{0, 0}, {0, 0}, {0, 0}};
+    if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
+      const R kv[3] = {kx_of(kp, i), ky_of(kp, j), kz_of(kp, k)};
+      // symmetric stress: (a,b) -> slot
+      const int slot[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        R re = 0, im = 0;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const cx<R> t = T.T[slot[a][b]][p];
+          // -i k_b t = k_b (t.y, -t.x)
+          re += kv[b] * t.y;
+          im -= kv[b] * t.x;
+        }
+        F[a].x = re;
+        F[a].y = im;
+      }
+      const R kk2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+      const R dre = (kv[0] * F[0].x + kv[1] * F[1].x + kv[2] * F[2].x) / kk2;
+      const R dim = (kv[0] * F[0].y + kv[1] * F[1].y + kv[2] * F[2].y) / kk2;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        F[a].x -= kv[a] * dre;
+        F[a].y -= kv[a] * dim;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      cx<R> v = F[a];
+      if (f.p[a]) {
+        v.x += f.p[a][p].x;
+        v.y += f.p[a][p].y;
+      }
+      o.p[a][p] = v;
+    }
+  }
+}
+
+// EDQNM eddy viscosity as a force: o_a = f_a - tve(ki) kk2 v_a with
+// ki = int(sqrt(kk2) + 0.501) (include/edqnmhd_rkstep2.f90:45-56 writes
+// (nu + tve(ki)) times the Laplacian); tve 1-based in GHOST, tve[ki-1] here.
+template <typename R>
+__global__ void eddy_force_kernel(KParams<R> kp, Spec3<R> v, Spec3<R> f, Spec3w<R> o, const double *__restrict__ tve,
+                                  int ntve, size_t total) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
+    const R kn2 = kn2_of(kp, i, j, k);
+    R nut = 0, kk2 = 0;
+    if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
+      kk2 = kk2_of(kp, i, j, k);
+      const int ki = (int)(sqrt(kk2) + (R)0.501f);
+      nut = (ki >= 1 && ki <= ntve) ? (R)tve[ki - 1] : (R)0;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const cx<R> u = v.p[a][p];
+      cx<R> r;
+      r.x = -(nut * kk2) * u.x;
+      r.y = -(nut * kk2) * u.y;
+      if (f.p[a]) {
+        r.x += f.p[a][p].x;
+        r.y += f.p[a][p].y;
+      }
+      o.p[a][p] = r;
+    }
+  }
+}
+
+static int blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+// ---------------------------------------------------------------------
+// EDQNM eddy viscosity (host), pseudo/pseudospec3D_edqnm.f90.  R is
+// GHOST's GP kind: the spectra are DOUBLE PRECISION, the fit and the
+// quadrature locals are REAL(GP), and the literals 0.218 and real(k*k) are
+// default (single-precision) reals, as in the Fortran.
+
+// spec_fit (pseudospec3D_edqnm.f90:278-402): log-linear fit of Ein over
+// shells kinf..kc and extrapolation to 3 kc.  Arrays are 0-based copies of
+// GHOST's 1-based ones (Efit[k-1] = Efit(k)).
+template <typename R>
+static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *power_out, R *ddelta_out) {
+  const R tinyf = std::min((R)1e-15, (R)0.1 / ((R)n * (R)n));
+  const int kc = (int)std::sqrt(kmax);
+  const int ktot = 3 * kc, ksup = kc;
+  const int kinf = (int)((R)kc - delk);
+  const int nfit = 3 * (n / 2 + 1);
+  R power = -1, ddelta = -1;
+  for (int k = 0; k < nfit; ++k) Efit[k] = 0;
+  *power_out = power;
+  *ddelta_out = ddelta;
+  if (Ein[ksup - 1] <= (double)tinyf) return;
+  R x = 0, y = 0, z = 0, v = 0, w = 0, m = 0, nn = 0, o = 0, p = 0, expo = 0;
+  for (int i = kinf; i <= ksup; ++i) {
+    const R ii = (R)i, li = std::log(ii);
+    const R le = (R)std::log(Ein[i - 1] + (double)tinyf);
+    x = x + (R)1;
+    y = y + li;
+    z = z + le;
+    v = v + li * le;
+    w = w + li * li;
+    m = m + ii;
+    nn = nn + ii * li;
+    o = o + ii * le;
+    p = p + ii * ii;
+  }
+  R pden = (w * p - nn * nn) * (x * nn - y * m) - (y * nn - w * m) * (y * p - m * nn);
+  R pnum = ((z * nn - v * m) * (y * p - m * nn) - (v * p - o * nn) * (x * nn - y * m));
+  R dden = x * nn - y * m;
+  if (pden != 0 && dden != 0) {
+    power = pnum / pden;
+    expo = ((z * nn - v * m) - power * (w * m - y * nn)) / dden;
+    ddelta = expo * x / m - power * y / m - z / m;
+  }
+  if (power >= 0 && ddelta >= 0) {
+    expo = std::exp(expo);
+    for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+    for (int k = ksup + 1; k <= ktot; ++k) {
+      const R kk = (R)k;
+      Efit[k - 1] = (double)(expo * std::pow(kk, -power) * std::exp(-ddelta * kk));
+    }
+  } else {
+    x = y = z = v = w = 0;
+    for (int i = kinf; i <= ksup; ++i) {
+      const R ii = (R)i, li = std::log(ii);
+      const R le = (R)std::log(Ein[i - 1] + (double)tinyf);
+      x = x + (R)1;
+      y = y + li;
+      z = z + le;
+      v = v + li * le;
+      w = w + li * li;
+    }
+    pden = y * y - w * x;
+    pnum = (v * x - y * z);
+    dden = x * y;
+    if (pden != 0 && dden != 0) {
+      power = pnum / pden;
+      expo = std::exp((y * z + power * y * y) / dden);
+      for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+      for (int k = ksup + 1; k <= ktot; ++k) {
+        const R kk = (R)k;
+        Efit[k - 1] = (double)(expo * std::pow(kk, -power) + tinyf);
+      }
+    } else {
+      for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+    }
+  }
+  *power_out = power;
+  *ddelta_out = ddelta;
+}
+
+// cusp (pseudospec3D_edqnm.f90:95-171): eddy viscosity nut(k) and modal
+// transfer tepq(k), k = 1..kc, from the extrapolated spectrum.
+template <typename R>
+static void cusp(int n, R kmax, R kolmo, const double *Ext, R nu, R t0, double *tepq, double *nut) {
+  const R lambda = (R)0.218f * std::pow(kolmo, (R)1.5);
+  const int kc = (int)std::sqrt(kmax);
+  const int ktot = 3 * kc;
+  if (Ext[kc] == 0.0) return;  // Ext(kc+1)
+  std::vector<R> mu(3 * (n / 2 + 1) + 1, (R)0);
+  R en = 0;
+  for (int k = 1; k <= ktot; ++k) {
+    const R tmp = (R)(float)(k * k);
+    en = (R)((double)en + (double)tmp * Ext[k - 1]);
+    mu[k] = lambda * std::sqrt(en);
+  }
+  for (int k = 1; k <= kc; ++k) {
+    const R kk = (R)k;
+    for (int p = kc + 1; p <= ktot; ++p) {
+      const R pp = (R)p, ppi = (R)1 / pp;
+      for (int q = p - k; q <= p; ++q) {
+        if (q == 0) continue;
+        const R qq = (R)q, qqi = (R)1 / qq;
+        R coeff = (R)0.5;
+        if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
+        const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
+        const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
+        const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
+        const R tvvkp = (R)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
+        const R tvvkpsym = (R)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
+        const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+        const R frac = (R)1 / tmp;
+        const R theta = -std::exp(-tmp * t0) / tmp;
+        nut[k - 1] = nut[k - 1] - (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) /
+                                      ((double)((R)2 * kk * kk) * Ext[k - 1]);
+        tepq[k - 1] = tepq[k - 1] + (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
+      }
+    }
+  }
+}
+
+// evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92)
+template <typename R>
+static void evedqnm(int n, R kmax, R kolmo, const double *Eold, R nu, R time, double *tepq, double *tve,
+                    double *Ext) {
+  const int kc = (int)std::sqrt(kmax);
+  const R delk = (R)3 * (R)kc / (R)4;
+  for (int k = 0; k < n / 2 + 1; ++k) tve[k] = tepq[k] = 0;
+  R power, ddelta;
+  spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
+  if (power > 0) cusp<R>(n, kmax, kolmo, Ext, nu, time, tepq, tve);
+}
+
+}  // namespace les
+
+using namespace les;
+
+struct ghost_les {
+  ghost_ctx *c = nullptr;
+  int kc = 0;
+  int model = GHOST_LES_NONE;
+  ghost_mlp *mlp = nullptr;
+  float gs = 1.f, ts = 1.f, delta = 1.f;
+  double kolmo = 1.4;
+  double t = 0.0;       // time handed to the EDQNM closure (GHOST's (t-1)*dt)
+  double nu_cur = 0.0;  // viscosity of the run in progress
+  std::vector<void *> bufs;  // owned device buffers
+  void *spec[9] = {};        // coarse spectral work fields
+  void *real[9] = {};        // coarse real work fields
+  void *rk[3] = {};          // RK copies
+  void *force[3] = {};       // closure force + forcing
+  float *x = nullptr, *y = nullptr;  // closure inputs / outputs (n^3 rows)
+  double *tve_dev = nullptr;
+  std::vector<double> Ek, tve, tepq, Ext;
+  // fine-grid buffers for ghost_les_samples (size of the last fine grid)
+  size_t fine_rbytes = 0, fine_cbytes = 0;
+  void *fine_real[4] = {};
+  void *fine_spec = nullptr;
+};
+
+static int les_alloc(ghost_les *L, size_t bytes, void **out) {
+  GB_CHECK(dalloc(out, bytes));
+  L->bufs.push_back(*out);
+  return GHOST_OK;
+}
+
+static int les_fine_buffers(ghost_les *L, ghost_ctx *f) {
+  if (L->fine_rbytes == f->rbytes && L->fine_cbytes == f->cbytes) return GHOST_OK;
+  for (void *&p : L->fine_real) {
+    cudaFree(p);
+    p = nullptr;
+  }
+  cudaFree(L->fine_spec);
+  L->fine_spec = nullptr;
+  L->fine_rbytes = L->fine_cbytes = 0;
+  for (void *&p : L->fine_real) GB_CHECK(dalloc(&p, f->rbytes));
+  GB_CHECK(dalloc(&L->fine_spec, f->cbytes));
+  L->fine_rbytes = f->rbytes;
+  L->fine_cbytes = f->cbytes;
+  return GHOST_OK;
+}
+
+template <typename R> static int truncate_dev(ghost_les *L, ghost_ctx *f, const void *in, void *out) {
+  ghost_ctx *c = L->c;
+  const R scale = (R)((double)c->nreal / (double)f->nreal);
+  const size_t total = c->nspec;
+  truncate_kernel<R><<<blocks(total), 256, 0, c->stream>>>((const cx<R> *)in, (cx<R> *)out, c->nx, f->nx,
+                                                           L->kc * L->kc, scale);
+  return post_launch(c);
+}
+
+// the nine n^3-scaled velocity gradients of (vx, vy, vz) into L->real
+template <typename R> static int gradients_dev(ghost_les *L, const void *const v[3]) {
+  ghost_ctx *c = L->c;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      GB_CHECK(derivk3_impl<R>(c, v[a], L->spec[0], b + 1));
+      GB_CHECK(c2r_dev<R>(c, L->spec[0], L->real[3 * a + b]));
+    }
+  return GHOST_OK;
+}
+
+template <typename R> static int features_dev(ghost_les *L, const void *const v[3], float gs, float delta) {
+  ghost_ctx *c = L->c;
+  GB_CHECK(gradients_dev<R>(L, v));
+  GradFields<R> gf;
+  for (int q = 0; q < 9; ++q) gf.g[q] = (const R *)L->real[q];
+  features_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(gf, L->x, c->nreal, (R)(1.0 / (double)c->nreal), gs,
+                                                              delta);
+  return post_launch(c);
+}
+
+template <typename R>
+static int samples_dev(ghost_les *L, ghost_ctx *f, const void *const v[3], float delta, float *x, float *tau) {
+  ghost_ctx *c = L->c;
+  GB_CHECK(les_fine_buffers(L, f));
+  // filtered velocity on the coarse grid, its gradients and real values
+  void *ub[3] = {L->spec[6], L->spec[7], L->spec[8]};
+  for (int a = 0; a < 3; ++a) GB_CHECK(truncate_dev<R>(L, f, v[a], ub[a]));
+  GB_CHECK(gradients_dev<R>(L, ub));
+  GradFields<R> gf;
+  for (int q = 0; q < 9; ++q) gf.g[q] = (const R *)L->real[q];
+  features_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(gf, x, c->nreal, (R)(1.0 / (double)c->nreal), 1.f,
+                                                              delta);
+  GB_CHECK(post_launch(c));
+  // real ubar (n^3-scaled) into real[0..2]; the gradient fields are done
+  for (int a = 0; a < 3; ++a) GB_CHECK(c2r_dev<R>(c, ub[a], L->real[a]));
+  // fine velocity (N^3-scaled) and the six products, filtered to the coarse grid
+  for (int a = 0; a < 3; ++a) GB_CHECK(c2r_dev<R>(f, v[a], L->fine_real[a]));
+  const R sN = (R)(1.0 / (double)f->nreal);
+  for (int m = 0; m < 6; ++m) {
+    const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+    product_kernel<R><<<blocks(f->nreal), 256, 0, f->stream>>>((const R *)L->fine_real[pa[m]],
+                                                               (const R *)L->fine_real[pb[m]], (R *)L->fine_real[3],
+                                                               f->nreal, sN);
+    GB_CHECK(post_launch(f));
+    GB_CHECK(r2c_dev<R>(f, L->fine_real[3], L->fine_spec));
+    GB_CHECK(truncate_dev<R>(L, f, L->fine_spec, L->spec[0]));
+    GB_CHECK(c2r_dev<R>(c, L->spec[0], L->real[3 + m]));
+  }
+  TauFields<R> tf;
+  for (int m = 0; m < 6; ++m) tf.P[m] = (const R *)L->real[3 + m];
+  for (int a = 0; a < 3; ++a) tf.U[a] = (const R *)L->real[a];
+  targets_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(tf, tau, c->nreal, (R)(1.0 / (double)c->nreal), 1.f);
+  return post_launch(c);
+}
+
+// o = f + P(-div tau), tau rows scaled by 1/ts
+template <typename R>
+static int tau_force_dev(ghost_les *L, const float *tau, float ts, const void *const f[3], void *const o[3]) {
+  ghost_ctx *c = L->c;
+  RealOut6<R> ro;
+  for (int m = 0; m < 6; ++m) ro.t[m] = (R *)L->real[m];
+  unpack_tau_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(tau, ro, c->nreal, ts);
+  GB_CHECK(post_launch(c));
+  Spec6<R> T;
+  for (int m = 0; m < 6; ++m) {
+    GB_CHECK(r2c_dev<R>(c, L->real[m], L->spec[m]));
+    T.T[m] = (const cx<R> *)L->spec[m];
+  }
+  Spec3<R> fs;
+  Spec3w<R> os;
+  for (int a = 0; a < 3; ++a) {
+    fs.p[a] = f ? (const cx<R> *)f[a] : nullptr;
+    os.p[a] = (cx<R> *)o[a];
+  }
+  tau_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), T, fs, os, c->nspec);
+  return post_launch(c);
+}
+
+template <typename R>
+static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
+  ghost_ctx *c = L->c;
+  const int nb = c->nx / 2 + 1;
+  L->Ek.assign(nb, 0.0);
+  GB_CHECK(spectrum_dev<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek.data()));
+  L->tve.assign(nb, 0.0);
+  L->tepq.assign(nb, 0.0);
+  L->Ext.assign(3 * nb, 0.0);
+  evedqnm<R>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek.data(), (R)L->nu_cur, (R)L->t, L->tepq.data(), L->tve.data(),
+             L->Ext.data());
+  GB_CUDA(cudaMemcpyAsync(L->tve_dev, L->tve.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
+  Spec3<R> vs, fs;
+  Spec3w<R> os;
+  for (int a = 0; a < 3; ++a) {
+    vs.p[a] = (const cx<R> *)v[a];
+    fs.p[a] = f ? (const cx<R> *)f[a] : nullptr;
+    os.p[a] = (cx<R> *)o[a];
+  }
+  eddy_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vs, fs, os, L->tve_dev, nb, c->nspec);
+  GB_CHECK(post_launch(c));
+  // the host table is reused by the next substep: wait for the upload
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return GHOST_OK;
+}
+
+// closure force of the selected model for the velocity v: o = f + F(v)
+template <typename R>
+static int closure_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
+  ghost_ctx *c = L->c;
+  switch (L->model) {
+    case GHOST_LES_MLP: {
+      GB_CHECK(features_dev<R>(L, v, L->gs, L->delta));
+      GB_CHECK(ghost_mlp_set_stream(L->mlp, c->stream));
+      GB_CHECK(ghost_mlp_forward(L->mlp, L->x, L->y, (int)c->nreal));
+      return tau_force_dev<R>(L, L->y, L->ts, f, o);
+    }
+    case GHOST_LES_EDQNM:
+      return eddy_force_dev<R>(L, v, f, o);
+    default: {
+      // no closure: the forcing alone
+      const size_t b = c->cbytes;
+      for (int a = 0; a < 3; ++a) {
+        if (f && f[a])
+          GB_CUDA(cudaMemcpyAsync(o[a], f[a], b, cudaMemcpyDeviceToDevice, c->stream));
+        else
+          GB_CUDA(cudaMemsetAsync(o[a], 0, b, c->stream));
+      }
+      return GHOST_OK;
+    }
+  }
+}
+
+// nsteps RK steps of the LES: each substep computes the closure force from
+// the current velocity, then runs the fused HD substep with it as forcing
+template <typename R>
+static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, void *const v[3],
+                       const void *const f[3]) {
+  ghost_ctx *c = L->c;
+  L->nu_cur = nu;
+  bool first = true;
+  for (int s = 0; s < nsteps; ++s) {
+    for (int o = ord; o >= 1; --o) {
+      GB_CHECK(closure_force_dev<R>(L, v, f, L->force));
+      GB_CHECK(hd_substep_dev<R>(c, o, dt, nu, v, L->rk, L->force, o == ord ? 1 : 0, !first));
+      first = false;
+    }
+    L->t += dt;
+  }
+  return check_status(c);
+}
+
+#define LES_CHECK(L)                                                            \
+  do {                                                                          \
+    if (!(L) || !(L)->c) return fail(GHOST_ERR_ARG, "null LES handle");        \
+  } while (0)
+
+static int dev3(const void *a, const void *b, const void *c, const char *what) {
+  if (!a || !b || !c) return fail(GHOST_ERR_ARG, "%s: null field", what);
+  if (!is_device_ptr(a) || !is_device_ptr(b) || !is_device_ptr(c))
+    return fail(GHOST_ERR_ARG, "%s: LES calls take device arrays", what);
+  return GHOST_OK;
+}
+
+static int fine_compatible(const ghost_les *L, const ghost_ctx *f) {
+  const ghost_ctx *c = L->c;
+  if (!f) return fail(GHOST_ERR_ARG, "null fine context");
+  if (f->precision != c->precision) return fail(GHOST_ERR_ARG, "fine and coarse precisions differ");
+  if (f->anis || f->nx != f->ny || f->nx != f->nz) return fail(GHOST_ERR_SIZE, "the fine grid must be cubic");
+  if (f->nx < c->nx) return fail(GHOST_ERR_SIZE, "fine grid %d smaller than the LES grid %d", f->nx, c->nx);
+  if (2 * L->kc >= f->nx) return fail(GHOST_ERR_SIZE, "kc %d not below the fine Nyquist %d", L->kc, f->nx / 2);
+  if (f->nruns != 1) return fail(GHOST_ERR_ARG, "batched fine contexts are not supported");
+  return GHOST_OK;
+}
+
+extern "C" {
+
+int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
+  if (!out) return fail(GHOST_ERR_ARG, "null output");
+  *out = nullptr;
+  if (!c) return fail(GHOST_ERR_ARG, "null context");
+  if (c->anis || c->nx != c->ny || c->nx != c->nz) return fail(GHOST_ERR_SIZE, "the LES grid must be cubic");
+  if (c->nruns != 1) return fail(GHOST_ERR_ARG, "batched contexts are not supported");
+  if (kc < 1 || 2 * kc >= c->nx) return fail(GHOST_ERR_ARG, "kc %d must be in [1, n/2)", kc);
+  ghost_les *L = new ghost_les();
+  L->c = c;
+  L->kc = kc;
+  int st = GHOST_OK;
+  for (int q = 0; q < 9 && !st; ++q) st = les_alloc(L, c->cbytes, &L->spec[q]);
+  for (int q = 0; q < 9 && !st; ++q) st = les_alloc(L, c->rbytes, &L->real[q]);
+  for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->rk[q]);
+  for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->force[q]);
+  if (!st) st = les_alloc(L, sizeof(float) * c->nreal * GHOST_MLP_NIN, (void **)&L->x);
+  if (!st) st = les_alloc(L, sizeof(float) * c->nreal * GHOST_MLP_NOUT, (void **)&L->y);
+  if (!st) st = les_alloc(L, sizeof(double) * (c->nx / 2 + 1), (void **)&L->tve_dev);
+  if (st) {
+    ghost_les_destroy(L);
+    return st;
+  }
+  *out = L;
+  return GHOST_OK;
+}
+
+int ghost_les_destroy(ghost_les *L) {
+  if (!L) return GHOST_OK;
+  if (L->c) cudaStreamSynchronize(L->c->stream);
+  for (void *p : L->bufs) cudaFree(p);
+  for (void *p : L->fine_real) cudaFree(p);
+  cudaFree(L->fine_spec);
+  delete L;
+  return GHOST_OK;
+}
+
+int ghost_les_truncate(ghost_les *L, ghost_ctx *f, const void *in, void *out) {
+  LES_CHECK(L);
+  GB_CHECK(fine_compatible(L, f));
+  GB_CHECK(dev3(in, out, out, "ghost_les_truncate"));
+  GB_CUDA(cudaStreamSynchronize(f->stream));
+  int st = L->c->precision == GHOST_SINGLE ? truncate_dev<float>(L, f, in, out) : truncate_dev<double>(L, f, in, out);
+  return st ? st : check_status(L->c);
+}
+
+int ghost_les_samples(ghost_les *L, ghost_ctx *f, const void *vx, const void *vy, const void *vz, float delta,
+                      float *x, float *tau) {
+  LES_CHECK(L);
+  GB_CHECK(fine_compatible(L, f));
+  GB_CHECK(dev3(vx, vy, vz, "ghost_les_samples"));
+  GB_CHECK(dev3(x, tau, tau, "ghost_les_samples"));
+  // the fine and coarse contexts may use different streams: order them
+  GB_CUDA(cudaStreamSynchronize(f->stream));
+  GB_CUDA(cudaStreamSynchronize(L->c->stream));
+  const void *v[3] = {vx, vy, vz};
+  // the fine-grid passes run on the coarse context's stream, so that every
+  // hand-over between the grids is ordered
+  cudaStream_t fs = f->stream;
+  f->stream = L->c->stream;
+  int st = L->c->precision == GHOST_SINGLE ? samples_dev<float>(L, f, v, delta, x, tau)
+                                           : samples_dev<double>(L, f, v, delta, x, tau);
+  f->stream = fs;
+  if (st) return st;
+  GB_CUDA(cudaStreamSynchronize(L->c->stream));
+  return check_status(L->c);
+}
+
+int ghost_les_features(ghost_les *L, const void *vx, const void *vy, const void *vz, float grad_scale, float delta,
+                       float *x) {
+  LES_CHECK(L);
+  GB_CHECK(dev3(vx, vy, vz, "ghost_les_features"));
+  GB_CHECK(dev3(x, x, x, "ghost_les_features"));
+  const void *v[3] = {vx, vy, vz};
+  float *keep = L->x;
+  L->x = x;
+  int st = L->c->precision == GHOST_SINGLE ? features_dev<float>(L, v, grad_scale, delta)
+                                           : features_dev<double>(L, v, grad_scale, delta);
+  L->x = keep;
+  return st;
+}
+
+int ghost_les_tau_force(ghost_les *L, const float *tau, float tau_scale, const void *fx, const void *fy,
+                        const void *fz, void *ox, void *oy, void *oz) {
+  LES_CHECK(L);
+  GB_CHECK(dev3(tau, tau, tau, "ghost_les_tau_force"));
+  GB_CHECK(dev3(ox, oy, oz, "ghost_les_tau_force"));
+  if ((fx || fy || fz) && (!fx || !fy || !fz)) return fail(GHOST_ERR_ARG, "give all three forcing fields or none");
+  if (fx) GB_CHECK(dev3(fx, fy, fz, "ghost_les_tau_force"));
+  const void *f[3] = {fx, fy, fz};
+  void *o[3] = {ox, oy, oz};
+  return L->c->precision == GHOST_SINGLE ? tau_force_dev<float>(L, tau, tau_scale, fx ? f : nullptr, o)
+                                         : tau_force_dev<double>(L, tau, tau_scale, fx ? f : nullptr, o);
+}
+
+int ghost_les_set_model(ghost_les *L, int model, ghost_mlp *mlp, double grad_scale, double tau_scale, double delta,
+                        double kolmo) {
+  LES_CHECK(L);
+  if (model != GHOST_LES_NONE && model != GHOST_LES_EDQNM && model != GHOST_LES_MLP)
+    return fail(GHOST_ERR_ARG, "unknown closure %d", model);
+  if (model == GHOST_LES_MLP && !mlp) return fail(GHOST_ERR_ARG, "the MLP closure needs a network");
+  if (model == GHOST_LES_EDQNM && !(kolmo > 0)) return fail(GHOST_ERR_ARG, "kolmo must be positive");
+  L->model = model;
+  L->mlp = mlp;
+  L->gs = (float)grad_scale;
+  L->ts = (float)tau_scale;
+  L->delta = (float)delta;
+  L->kolmo = kolmo;
+  return GHOST_OK;
+}
+
+int ghost_les_set_time(ghost_les *L, double t) {
+  LES_CHECK(L);
+  L->t = t;
+  return GHOST_OK;
+}
+
+int ghost_les_closure_force(ghost_les *L, double nu, const void *vx, const void *vy, const void *vz, const void *fx,
+                            const void *fy, const void *fz, void *ox, void *oy, void *oz) {
+  LES_CHECK(L);
+  GB_CHECK(dev3(vx, vy, vz, "ghost_les_closure_force"));
+  GB_CHECK(dev3(ox, oy, oz, "ghost_les_closure_force"));
+  if ((fx || fy || fz) && (!fx || !fy || !fz)) return fail(GHOST_ERR_ARG, "give all three forcing fields or none");
+  const void *v[3] = {vx, vy, vz}, *f[3] = {fx, fy, fz};
+  void *o[3] = {ox, oy, oz};
+  L->nu_cur = nu;
+  int st = L->c->precision == GHOST_SINGLE ? closure_force_dev<float>(L, v, fx ? f : nullptr, o)
+                                           : closure_force_dev<double>(L, v, fx ? f : nullptr, o);
+  return st ? st : check_status(L->c);
+}
+
+int ghost_les_run(ghost_les *L, int nsteps, int ord, double dt, double nu, void *vx, void *vy, void *vz,
+                  const void *fx, const void *fy, const void *fz) {
+  LES_CHECK(L);
+  if (nsteps < 0 || ord < 1 || ord > 4) return fail(GHOST_ERR_ARG, "bad nsteps/ord");
+  GB_CHECK(dev3(vx, vy, vz, "ghost_les_run"));
+  if ((fx || fy || fz) && (!fx || !fy || !fz)) return fail(GHOST_ERR_ARG, "give all three forcing fields or none");
+  if (fx) GB_CHECK(dev3(fx, fy, fz, "ghost_les_run"));
+  void *v[3] = {vx, vy, vz};
+  const void *f[3] = {fx, fy, fz};
+  return L->c->precision == GHOST_SINGLE ? les_run_dev<float>(L, nsteps, ord, dt, nu, v, fx ? f : nullptr)
+                                         : les_run_dev<double>(L, nsteps, ord, dt, nu, v, fx ? f : nullptr);
+}
+
+int ghost_les_edqnm_last(ghost_les *L, double *tve, double *tepq, double *Ek) {
+  LES_CHECK(L);
+  const int nb = L->c->nx / 2 + 1;
+  if ((int)L->tve.size() != nb) return fail(GHOST_ERR_STATE, "no EDQNM evaluation yet");
+  if (tve) memcpy(tve, L->tve.data(), sizeof(double) * nb);
+  if (tepq) memcpy(tepq, L->tepq.data(), sizeof(double) * nb);
+  if (Ek) memcpy(Ek, L->Ek.data(), sizeof(double) * nb);
+  return GHOST_OK;
+}
+
+int ghost_evedqnm(int n, int precision, double kmax, double kolmo, const double *Eold, double nu, double time,
+                  double *tepq, double *tve, double *Ext) {
+  if (!Eold || !tepq || !tve || !Ext) return fail(GHOST_ERR_ARG, "null argument");
+  if (n < 16 || (n & (n - 1))) return fail(GHOST_ERR_SIZE, "n %d", n);
+  const int kc = (int)std::sqrt(kmax);
+  if (kc < 2 || kc > n / 2 + 1 || 3 * kc > 3 * (n / 2 + 1)) return fail(GHOST_ERR_ARG, "kmax %g", kmax);
+  if (precision == GHOST_SINGLE)
+    evedqnm<float>(n, (float)kmax, (float)kolmo, Eold, (float)nu, (float)time, tepq, tve, Ext);
+  else if (precision == GHOST_DOUBLE)
+    evedqnm<double>(n, kmax, kolmo, Eold, nu, time, tepq, tve, Ext);
+  else
+    return fail(GHOST_ERR_ARG, "precision %d", precision);
+  return GHOST_OK;
+}
+
+}  // extern "C"

@@ -409,6 +409,82 @@
          REAL(C_DOUBLE) :: loss
          INTEGER(C_INT) :: s
        END FUNCTION
+       ! large-eddy simulation: learned closure and GHOST's EDQNM eddy viscosity
+       FUNCTION ghost_les_create(ctx,kc,les) BIND(C,name="ghost_les_create") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT), VALUE :: kc
+         TYPE(C_PTR) :: les
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_destroy(les) BIND(C,name="ghost_les_destroy") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: les
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_truncate(les,fine,a,b) BIND(C,name="ghost_les_truncate") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: les, fine, a, b
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_samples(les,fine,vx,vy,vz,delta,x,tau) BIND(C,name="ghost_les_samples") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: les, fine, vx, vy, vz, x, tau
+         REAL(C_FLOAT), VALUE :: delta
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_features(les,vx,vy,vz,gs,delta,x) BIND(C,name="ghost_les_features") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: les, vx, vy, vz, x
+         REAL(C_FLOAT), VALUE :: gs, delta
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_tau_force(les,tau,ts,fx,fy,fz,ox,oy,oz) BIND(C,name="ghost_les_tau_force") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: les, tau, fx, fy, fz, ox, oy, oz
+         REAL(C_FLOAT), VALUE :: ts
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_set_model(les,model,mlp,gs,ts,delta,kolmo) BIND(C,name="ghost_les_set_model") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les, mlp
+         INTEGER(C_INT), VALUE :: model
+         REAL(C_DOUBLE), VALUE :: gs, ts, delta, kolmo
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_set_time(les,t) BIND(C,name="ghost_les_set_time") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les
+         REAL(C_DOUBLE), VALUE :: t
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_closure_force(les,nu,vx,vy,vz,fx,fy,fz,ox,oy,oz) &
+                BIND(C,name="ghost_les_closure_force") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les, vx, vy, vz, fx, fy, fz, ox, oy, oz
+         REAL(C_DOUBLE), VALUE :: nu
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_run(les,nsteps,ord,dt,nu,vx,vy,vz,fx,fy,fz) BIND(C,name="ghost_les_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les, vx, vy, vz, fx, fy, fz
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_edqnm_last(les,tve,tepq,ek) BIND(C,name="ghost_les_edqnm_last") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les
+         REAL(C_DOUBLE) :: tve(*), tepq(*), ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_evedqnm(n,prec,kmax,kolmo,eold,nu,time,tepq,tve,ext) BIND(C,name="ghost_evedqnm") RESULT(s)
+         IMPORT :: C_INT, C_DOUBLE
+         INTEGER(C_INT), VALUE :: n, prec
+         REAL(C_DOUBLE), VALUE :: kmax, kolmo, nu, time
+         REAL(C_DOUBLE) :: eold(*), tepq(*), tve(*), ext(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_init_random_solenoidal(ctx,seed,kdn,kup,shape,amp,ox,oy,oz) &
                 BIND(C,name="ghost_init_random_solenoidal") RESULT(s)
          IMPORT :: C_INT, C_INT32_T, C_PTR, C_DOUBLE

@@ -1,8 +1,10 @@
-"""Host mirror of the LES closures: the learned subgrid-stress MLP.
+"""Host mirror of the LES path: the learned subgrid-stress MLP and the LES
+driver with its closures (none, GHOST's EDQNM eddy viscosity, the MLP).
 
 `MLP` wraps the ghost_mlp_* entry points (tensor-core forward, gradients and
-Adam of the 10 -> 64 -> 64 -> 6 GELU network).  Inputs and targets are CUDA
-float32 tensors of shape (B, 10) and (B, 6).
+Adam of the 10 -> 64 -> 64 -> 6 GELU network); inputs and targets are CUDA
+float32 tensors of shape (B, 10) and (B, 6).  `LES` wraps ghost_les_*: a
+cubic coarse grid (a `Ghost` context) with a sharp cutoff kc.
 """
 from __future__ import annotations
 
@@ -90,4 +92,119 @@ class MLP:
         return loss.value if want_loss else None
 
 
-__all__ = ["MLP", "NIN", "NHID", "NOUT", "NPARAM"]
+MODELS = {"none": 0, "edqnm": 1, "mlp": 2}
+
+
+class LES:
+    """LES on the coarse grid of `g` (a cubic `Ghost`) resolving |k| <= kc.
+
+    The context's kmax is set to kc^2 so that the LES keeps exactly the
+    modes of the sharp-filtered DNS."""
+
+    def __init__(self, g, kc: int):
+        self.g = g
+        self.lib = g.lib
+        self.kc = int(kc)
+        check(self.lib.ghost_ctx_set_kmax(g.h, float(self.kc * self.kc)), "ghost_ctx_set_kmax")
+        h = ctypes.c_void_p()
+        check(self.lib.ghost_les_create(g.h, self.kc, ctypes.byref(h)), "ghost_les_create")
+        self.h = h
+        self.n = g.nx
+        self.model = "none"
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ghost_les_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, x):
+        return self.g._ptr(x, "c")
+
+    def _f(self, x, cols):
+        p = _dev(x, cols, "array")
+        if x.shape[0] != self.rows():
+            raise ValueError(f"expected {self.rows()} rows (one per grid point), got {x.shape[0]}")
+        return p
+
+    def rows(self):
+        return self.n ** 3
+
+    def truncate(self, fine, a, out=None):
+        """The modes |k| <= kc of a spectrum on `fine` (a Ghost), on this grid."""
+        out = self.g.czeros() if out is None else out
+        check(self.lib.ghost_les_truncate(self.h, fine.h, fine._ptr(a, "c"), self._c(out)), "ghost_les_truncate")
+        return out
+
+    def samples(self, fine, vx, vy, vz, delta: float = 1.0, x=None, tau=None):
+        """(inputs (n^3, 10), stresses (n^3, 6)) from a fine velocity."""
+        B = self.rows()
+        x = torch.empty((B, NIN), dtype=torch.float32, device="cuda") if x is None else x
+        tau = torch.empty((B, NOUT), dtype=torch.float32, device="cuda") if tau is None else tau
+        check(self.lib.ghost_les_samples(self.h, fine.h, *[fine._ptr(v, "c") for v in (vx, vy, vz)],
+                                         ctypes.c_float(delta), self._f(x, NIN), self._f(tau, NOUT)),
+              "ghost_les_samples")
+        return x, tau
+
+    def features(self, vx, vy, vz, grad_scale: float = 1.0, delta: float = 1.0, x=None):
+        x = torch.empty((self.rows(), NIN), dtype=torch.float32, device="cuda") if x is None else x
+        check(self.lib.ghost_les_features(self.h, *[self._c(v) for v in (vx, vy, vz)], ctypes.c_float(grad_scale),
+                                          ctypes.c_float(delta), self._f(x, NIN)), "ghost_les_features")
+        return x
+
+    def tau_force(self, tau, tau_scale: float = 1.0, f=(None, None, None), out=None):
+        out = [self.g.czeros() for _ in range(3)] if out is None else out
+        check(self.lib.ghost_les_tau_force(self.h, self._f(tau, NOUT), ctypes.c_float(tau_scale),
+                                           *[self._c(x) for x in f], *[self._c(x) for x in out]),
+              "ghost_les_tau_force")
+        return out
+
+    def set_model(self, model: str, mlp: MLP | None = None, grad_scale: float = 1.0, tau_scale: float = 1.0,
+                  delta: float = 1.0, kolmo: float = 1.4):
+        check(self.lib.ghost_les_set_model(self.h, MODELS[model], mlp.h if mlp is not None else None,
+                                           grad_scale, tau_scale, delta, kolmo), "ghost_les_set_model")
+        self.model = model
+        self.mlp = mlp
+
+    def set_time(self, t: float):
+        check(self.lib.ghost_les_set_time(self.h, t), "ghost_les_set_time")
+
+    def closure_force(self, nu, vx, vy, vz, f=(None, None, None), out=None):
+        out = [self.g.czeros() for _ in range(3)] if out is None else out
+        check(self.lib.ghost_les_closure_force(self.h, nu, *[self._c(v) for v in (vx, vy, vz)],
+                                               *[self._c(x) for x in f], *[self._c(x) for x in out]),
+              "ghost_les_closure_force")
+        return out
+
+    def run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None):
+        check(self.lib.ghost_les_run(self.h, nsteps, ord, dt, nu, *[self._c(v) for v in (vx, vy, vz, fx, fy, fz)]),
+              "ghost_les_run")
+
+    def edqnm_last(self):
+        nb = self.n // 2 + 1
+        tve, tepq, Ek = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        P = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.ghost_les_edqnm_last(self.h, tve.ctypes.data_as(P), tepq.ctypes.data_as(P),
+                                            Ek.ctypes.data_as(P)), "ghost_les_edqnm_last")
+        return tve, tepq, Ek
+
+
+def evedqnm(n: int, kmax: float, Eold, nu: float, time: float, kolmo: float = 1.4, precision: str = "fp64"):
+    """GHOST's evedqnm (heli = 0) on the host: (tepq, tve, Ext)."""
+    lib = _lib.load()
+    nb = n // 2 + 1
+    E = np.ascontiguousarray(Eold, dtype=np.float64)
+    tepq, tve, Ext = np.zeros(nb), np.zeros(nb), np.zeros(3 * nb)
+    P = ctypes.POINTER(ctypes.c_double)
+    code = {"fp32": _lib.GHOST_SINGLE, "fp64": _lib.GHOST_DOUBLE}[precision]
+    check(lib.ghost_evedqnm(n, code, kmax, kolmo, E.ctypes.data_as(P), nu, time, tepq.ctypes.data_as(P),
+                            tve.ctypes.data_as(P), Ext.ctypes.data_as(P)), "ghost_evedqnm")
+    return tepq, tve, Ext
+
+
+__all__ = ["MLP", "LES", "evedqnm", "MODELS", "NIN", "NHID", "NOUT", "NPARAM"]

@@ -331,6 +331,69 @@ int ghost_mlp_gradients(ghost_mlp *mlp, const float *x, const float *t, int B, f
  * be NULL (then the call does not synchronise) */
 int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, float lr, double *loss);
 
+/* ---------------------------------------------------------------- */
+/* Large-eddy simulation on a cubic coarse grid n^3 with a sharp spectral
+ * cutoff kc (modes kx^2+ky^2+kz^2 <= kc^2 are resolved; GHOST's sharp,
+ * pseudo/pseudospec3D_filt.f90:200-241, with Delta = pi/kc).  Set the
+ * coarse context's kmax to kc^2 (ghost_ctx_set_kmax) so that the LES
+ * resolves exactly the filtered modes.  All field arguments are device
+ * arrays of the coarse context unless named fine.  Closures:
+ *   GHOST_LES_NONE   no subgrid term;
+ *   GHOST_LES_EDQNM  GHOST's EDQNM eddy viscosity, include/edqnmhd_rkstep2.f90
+ *                    with heli = 0: the kinetic spectrum of the current
+ *                    velocity gives tve(k) (evedqnm: spec_fit + cusp,
+ *                    pseudo/pseudospec3D_edqnm.f90:24-402) and the update
+ *                    uses nu + tve(k); vcorrect is not applied;
+ *   GHOST_LES_MLP    the learned subgrid stress: tau = mlp(inputs) gives
+ *                    the force -P div tau (P the Leray projection). */
+#define GHOST_LES_NONE 0
+#define GHOST_LES_EDQNM 1
+#define GHOST_LES_MLP 2
+typedef struct ghost_les ghost_les;
+int ghost_les_create(ghost_ctx *coarse, int kc, ghost_les **les);
+int ghost_les_destroy(ghost_les *les);
+/* out = the modes |k| <= kc of the fine spectrum in, on the coarse grid
+ * (scaled by (n/N)^3, GHOST's unnormalised convention; analysis/trunc3D.fpp) */
+int ghost_les_truncate(ghost_les *les, ghost_ctx *fine, const void *in, void *out);
+/* Training samples from a fine (DNS) velocity, one per coarse grid point
+ * (real layout, x fastest): x[q][0..8] = d ubar_a / dx_b (a-major),
+ * x[q][9] = delta; tau[q][0..5] = filt(u_a u_b) - ubar_a ubar_b for xx, yy,
+ * zz, xy, xz, yz, ubar = sharp-filtered u, filt(u_a u_b) from the fine
+ * products.  x and tau are float device arrays of n^3 rows. */
+int ghost_les_samples(ghost_les *les, ghost_ctx *fine, const void *vx, const void *vy, const void *vz, float delta,
+                      float *x, float *tau);
+/* the closure inputs of a coarse velocity: gradients times grad_scale, delta */
+int ghost_les_features(ghost_les *les, const void *vx, const void *vy, const void *vz, float grad_scale, float delta,
+                       float *x);
+/* o = f + P(-div tau), tau[q][6] rows scaled by tau_scale (f may be NULL) */
+int ghost_les_tau_force(ghost_les *les, const float *tau, float tau_scale, const void *fx, const void *fy,
+                        const void *fz, void *ox, void *oy, void *oz);
+/* closure selection; the MLP maps inputs scaled by grad_scale (and delta)
+ * to stresses scaled by 1/tau_scale; kolmo is EDQNM's Kolmogorov constant
+ * (GHOST's default 1.4, main3D.fpp:1579).  The MLP is moved to the
+ * context's stream. */
+int ghost_les_set_model(ghost_les *les, int model, ghost_mlp *mlp, double grad_scale, double tau_scale, double delta,
+                        double kolmo);
+/* time handed to the EDQNM closure (GHOST's (t-1)*dt); ghost_les_run
+ * advances it by dt per step */
+int ghost_les_set_time(ghost_les *les, double t);
+/* o = f + the selected closure's force for velocity v (f may be NULL) */
+int ghost_les_closure_force(ghost_les *les, double nu, const void *vx, const void *vy, const void *vz, const void *fx,
+                            const void *fy, const void *fz, void *ox, void *oy, void *oz);
+/* nsteps RK steps (order ord) of the LES; each substep evaluates the
+ * closure on the current velocity and runs the fused HD substep with
+ * f + closure force as its forcing (f may be NULL) */
+int ghost_les_run(ghost_les *les, int nsteps, int ord, double dt, double nu, void *vx, void *vy, void *vz,
+                  const void *fx, const void *fy, const void *fz);
+/* the last EDQNM evaluation (host arrays of n/2+1, GHOST's 1-based index
+ * k stored at k-1); any pointer may be NULL */
+int ghost_les_edqnm_last(ghost_les *les, double *tve, double *tepq, double *Ek);
+/* evedqnm with heli = 0 on the host: Eold[n/2+1] -> tepq, tve[n/2+1] and
+ * the extrapolated spectrum Ext[3(n/2+1)]; precision selects GHOST's GP
+ * kind for the fit and quadrature (GHOST_SINGLE or GHOST_DOUBLE) */
+int ghost_evedqnm(int n, int precision, double kmax, double kolmo, const double *Eold, double nu, double time,
+                  double *tepq, double *tve, double *Ext);
+
 #ifdef __cplusplus
 }
 #endif

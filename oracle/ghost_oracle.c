@@ -900,3 +900,214 @@ void o_sharp(const octx *c, const cplx *a, cplx *b, double delta) {
   cplx z = {0, 0};
   for (size_t p = 0; p < c->nspec; ++p) b[p] = c->kn2[p] <= tmp ? a[p] : z;
 }
+
+/* ------------------------------------------------------------------ */
+/* EDQNM eddy viscosity (pseudo/pseudospec3D_edqnm.f90), heli = 0.
+ * Spectra are DOUBLE PRECISION as in the Fortran; the fit and quadrature
+ * locals are REAL(GP) = real; 0.218 and real(k*k) are default (single)
+ * reals.  Arrays are 0-based copies of the 1-based Fortran ones. */
+
+/* spec_fit (:278-402) */
+static void o_spec_fit(const octx *c, const double *Ein, real delk, double *Efit, real *power_o, real *ddelta_o) {
+  int n = c->nx;
+  real tinyf = (real)1e-15 < (real)0.1 / ((real)c->nmax * (real)c->nmax) ? (real)1e-15
+                                                                             : (real)0.1 / ((real)c->nmax * (real)c->nmax);
+  int kc = (int)sqrt(c->kmax);
+  int ktot = 3 * kc, ksup = kc, kinf = (int)((real)kc - delk);
+  real power = -1, ddelta = -1, expo = 0;
+  for (int k = 0; k < 3 * (n / 2 + 1); ++k) Efit[k] = 0;
+  *power_o = power;
+  *ddelta_o = ddelta;
+  if (Ein[ksup - 1] <= (double)tinyf) return;
+  real x = 0, y = 0, z = 0, v = 0, w = 0, m = 0, nn = 0, o = 0, p = 0;
+  for (int i = kinf; i <= ksup; ++i) {
+    real ii = (real)i;
+    real lg = (real)log(Ein[i - 1] + (double)tinyf);
+    x = x + (real)1.;
+    y = y + (real)log(ii);
+    z = z + lg;
+    v = v + (real)log(ii) * lg;
+    w = w + (real)log(ii) * (real)log(ii);
+    m = m + ii;
+    nn = nn + ii * (real)log(ii);
+    o = o + ii * lg;
+    p = p + ii * ii;
+  }
+  real pden = (w * p - nn * nn) * (x * nn - y * m) - (y * nn - w * m) * (y * p - m * nn);
+  real pnum = ((z * nn - v * m) * (y * p - m * nn) - (v * p - o * nn) * (x * nn - y * m));
+  real dden = x * nn - y * m;
+  if (pden != 0 && dden != 0) {
+    power = pnum / pden;
+    expo = ((z * nn - v * m) - power * (w * m - y * nn)) / dden;
+    ddelta = expo * x / m - power * y / m - z / m;
+  }
+  if (power >= 0 && ddelta >= 0) {
+    expo = (real)exp(expo);
+    for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+    for (int k = ksup + 1; k <= ktot; ++k) {
+      real kk = (real)k;
+      Efit[k - 1] = (double)(expo * (real)pow(kk, -power) * (real)exp(-ddelta * kk));
+    }
+  } else {
+    x = 0; y = 0; z = 0; v = 0; w = 0;
+    for (int i = kinf; i <= ksup; ++i) {
+      real ii = (real)i;
+      real lg = (real)log(Ein[i - 1] + (double)tinyf);
+      x = x + (real)1.;
+      y = y + (real)log(ii);
+      z = z + lg;
+      v = v + (real)log(ii) * lg;
+      w = w + (real)log(ii) * (real)log(ii);
+    }
+    pden = y * y - w * x;
+    pnum = (v * x - y * z);
+    dden = x * y;
+    if (pden != 0 && dden != 0) {
+      power = pnum / pden;
+      expo = (real)exp((y * z + power * y * y) / dden);
+      for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+      for (int k = ksup + 1; k <= ktot; ++k) {
+        real kk = (real)k;
+        Efit[k - 1] = (double)(expo * (real)pow(kk, -power) + tinyf);
+      }
+    } else {
+      for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
+    }
+  }
+  *power_o = power;
+  *ddelta_o = ddelta;
+}
+
+/* cusp (:95-171) */
+static void o_cusp(const octx *c, real kolmo, const double *Ext, real nu, real t0, double *tepq, double *nut) {
+  real lambda = (real)0.218f * (real)pow(kolmo, (real)1.5);
+  int kc = (int)sqrt(c->kmax), ktot = 3 * kc;
+  if (Ext[kc] == 0.) return;
+  real *mu = (real *)calloc((size_t)ktot + 1, sizeof(real));
+  real en = 0;
+  for (int k = 1; k <= ktot; ++k) {
+    real tmp = (real)(float)(k * k);
+    en = (real)((double)en + (double)tmp * Ext[k - 1]);
+    mu[k] = lambda * (real)sqrt(en);
+  }
+  for (int k = 1; k <= kc; ++k) {
+    real kk = (real)k;
+    for (int p = kc + 1; p <= ktot; ++p) {
+      real pp = (real)p, ppi = (real)1.0 / pp;
+      for (int q = p - k; q <= p; ++q) {
+        real qq = (real)q, qqi;
+        if (q == 0) continue;
+        qqi = (real)1.0 / qq;
+        real coeff = (real)0.5;
+        if ((qq - (real)0.5) >= (pp - kk) && (qq + (real)0.5) <= pp) coeff = (real)1.0;
+        real x = (pp * pp + qq * qq - kk * kk) / ((real)2.0 * pp * qq);
+        real y = (kk * kk + qq * qq - pp * pp) / ((real)2.0 * kk * qq);
+        real z = (pp * pp + kk * kk - qq * qq) / ((real)2.0 * pp * kk);
+        real tvvkp = (real)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
+        real tvvkpsym = (real)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
+        real tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+        real frac = (real)1.0 / tmp;
+        real theta = -(real)exp(-tmp * t0) / tmp;
+        nut[k - 1] = nut[k - 1] - (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) /
+                                      ((double)((real)2. * kk * kk) * Ext[k - 1]);
+        tepq[k - 1] = tepq[k - 1] + (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
+      }
+    }
+  }
+  free(mu);
+}
+
+/* evedqnm (:24-92) with hel = 0: Eold[n/2+1] -> tepq, tve[n/2+1], Ext[3(n/2+1)] */
+void o_evedqnm(const octx *c, double kolmo, const double *Eold, double nu, double time, double *tepq, double *tve,
+               double *Ext) {
+  int n = c->nx, kc = (int)sqrt(c->kmax);
+  real delk = (real)3. * (real)kc / (real)4.;
+  for (int k = 0; k < n / 2 + 1; ++k) tve[k] = tepq[k] = 0.;
+  real power, ddelta;
+  o_spec_fit(c, Eold, delk, Ext, &power, &ddelta);
+  if (power > 0) o_cusp(c, (real)kolmo, Ext, (real)nu, (real)time, tepq, tve);
+}
+
+/* include/edqnmhd_rkstep2.f90 with heli = 0, without the closing vcorrect:
+ * the update of :41-58 with (nu + tve(ki)) times the Laplacian */
+void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const double *tve, cplx *vx, cplx *vy, cplx *vz,
+                     const cplx *C1, const cplx *C2, const cplx *C3, const cplx *fx, const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d;
+  cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
+       *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
+       *C8 = (cplx *)malloc(sizeof(cplx) * n);
+  o_prodre3(c, vx, vy, vz, C4, C5, C6);
+  o_nonlhd3(c, C4, C5, C6, C7, 1);
+  o_nonlhd3(c, C4, C5, C6, C8, 2);
+  o_nonlhd3(c, C4, C5, C6, C4, 3);
+  o_laplak3(c, vx, vx);
+  o_laplak3(c, vy, vy);
+  o_laplak3(c, vz, vz);
+  real rmp = (real)1. / (real)o;
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < n; ++p) {
+    if (c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny) {
+      int ki = (int)((real)sqrt(c->kk2[p]) + (real)0.501f);
+      double nt = (double)nu + tve[ki - 1];
+      cplx *v[3] = {&vx[p], &vy[p], &vz[p]};
+      const cplx *C[3] = {&C1[p], &C2[p], &C3[p]}, *N[3] = {&C7[p], &C8[p], &C4[p]}, *F[3] = {&fx[p], &fy[p], &fz[p]};
+      for (int a = 0; a < 3; ++a) {
+        double re = (double)C[a]->re + (double)dt * (nt * v[a]->re + N[a]->re + F[a]->re) * (double)rmp;
+        double im = (double)C[a]->im + (double)dt * (nt * v[a]->im + N[a]->im + F[a]->im) * (double)rmp;
+        v[a]->re = (real)re;
+        v[a]->im = (real)im;
+      }
+    } else {
+      cplx z = {0, 0};
+      vx[p] = z; vy[p] = z; vz[p] = z;
+    }
+  }
+  free(C4); free(C5); free(C6); free(C7); free(C8);
+}
+
+/* nsteps RK steps of the EDQNM LES: per substep spectrumc -> evedqnm at
+ * time t0 + (step index) dt -> edqnm_rkstep2 (f may be NULL) */
+void o_edqnm_run(const octx *c, int nsteps, int ord, double dt, double nu, double kolmo, double t0, cplx *vx,
+                 cplx *vy, cplx *vz, const cplx *fx, const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  int nb = c->nx / 2 + 1;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n), *zf = NULL;
+  double *Ek = (double *)calloc(nb, sizeof(double)), *tepq = (double *)calloc(nb, sizeof(double)),
+         *tve = (double *)calloc(nb, sizeof(double)), *Ext = (double *)calloc(3 * nb, sizeof(double));
+  if (!fx) {
+    zf = (cplx *)calloc(n, sizeof(cplx));
+    fx = fy = fz = zf;
+  }
+  for (int t = 0; t < nsteps; ++t) {
+    o_hd_rkstep1(c, vx, vy, vz, C1, C2, C3);
+    for (int o = ord; o >= 1; --o) {
+      o_spectrumc(c, vx, vy, vz, 1, 0, Ek, NULL);
+      o_evedqnm(c, kolmo, Ek, nu, t0 + t * dt, tepq, tve, Ext);
+      o_edqnm_rkstep2(c, o, dt, nu, tve, vx, vy, vz, C1, C2, C3, fx, fy, fz);
+    }
+  }
+  free(C1); free(C2); free(C3); free(zf); free(Ek); free(tepq); free(tve); free(Ext);
+}
+
+/* Modes |k|^2 <= kc^2 of the fine spectrum (ctx f) on the coarse grid (ctx
+ * c), times (n/N)^3 (analysis/trunc3D.fpp with GHOST's sharp cutoff). */
+void o_les_truncate(const octx *f, const octx *c, const cplx *in, cplx *out, int kc) {
+  int n = c->nx, N = f->nx;
+  real scale = (real)((double)c->nreal / (double)f->nreal);
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        int kx = i < n / 2 ? i : i - n, ky = j < n / 2 ? j : j - n, kz = k < n / 2 ? k : k - n;
+        cplx v = {0, 0};
+        if (kx >= 0 && kx * kx + ky * ky + kz * kz <= kc * kc) {
+          int jf = ky >= 0 ? ky : ky + N, kf = kz >= 0 ? kz : kz + N;
+          v = cscal(scale, in[SIDX(f, kf, jf, kx)]);
+        }
+        out[SIDX(c, k, j, i)] = v;
+      }
+}
+
+/* kmax override (main3D.fpp sets kmax once; LES runs set it to kc^2) */
+void o_ctx_set_kmax(octx *c, double kmax) { c->kmax = (real)kmax; }

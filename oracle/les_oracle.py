@@ -1,0 +1,78 @@
+"""CPU restatement of the LES data path and closure forces.
+
+TEST INFRASTRUCTURE ONLY: tests/ use it as the checker of ghost_b200's LES
+kernels (ghost_b200/csrc/les.cu).  The product never imports it.
+
+Built on the oracle's GHOST restatement (oracle.py): its unnormalised
+transforms, derivk3 and the sharp-cutoff truncation o_les_truncate (GHOST's
+sharp of pseudo/pseudospec3D_filt.f90:200-241 with Delta = pi/kc, then the
+N^3 -> n^3 truncation of analysis/trunc3D.fpp).  The subgrid stress is the
+standard one, tau_ab = filt(u_a u_b) - ubar_a ubar_b, evaluated at the
+coarse grid points; the closure force is -P div tau.
+
+Sample rows follow the real layout r(i,j,k), x fastest, i.e. numpy's
+C-order flattening of shape (nz, ny, nx).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+
+
+def features(co, v, grad_scale=1.0, delta=1.0):
+    """Closure inputs of a coarse velocity: x[q][3a+b] = du_a/dx_b * grad_scale, x[q][9] = delta."""
+    n3 = co.nx * co.ny * co.nz
+    x = np.zeros((n3, 10))
+    for a in range(3):
+        for b in range(3):
+            g = co.fftp3d_complex_to_real(co.derivk3(v[a], b + 1)) / n3
+            x[:, 3 * a + b] = g.ravel() * grad_scale
+    x[:, 9] = delta
+    return x
+
+
+def samples(fo, co, v, kc, delta=1.0):
+    """(inputs, stresses) at the coarse grid points from a fine velocity."""
+    N3 = fo.nx * fo.ny * fo.nz
+    n3 = co.nx * co.ny * co.nz
+    ub = [fo.les_truncate(co, x, kc) for x in v]
+    x = features(co, ub, 1.0, delta)
+    ur = [co.fftp3d_complex_to_real(u) / n3 for u in ub]
+    U = [fo.fftp3d_complex_to_real(u) / N3 for u in v]
+    tau = np.zeros((n3, 6))
+    for m, (a, b) in enumerate(PAIRS):
+        ph = fo.les_truncate(co, fo.fftp3d_real_to_complex(U[a] * U[b]), kc)
+        p = co.fftp3d_complex_to_real(ph) / n3
+        tau[:, m] = (p - ur[a] * ur[b]).ravel()
+    return x, tau
+
+
+def tau_force(co, tau, tau_scale=1.0, f=None):
+    """o = f + P(-i k_b T_ab) on tiny <= kn2 <= kmax (f elsewhere)."""
+    kx, ky, kz, kn2, _ = co.tables()
+    nxh = co.nxh
+    K = [kx[:nxh][:, None, None], ky[None, :, None], kz[None, None, :]]
+    T = {}
+    for m, (a, b) in enumerate(PAIRS):
+        r = (tau[:, m] * tau_scale).reshape(co.rshape)
+        T[(a, b)] = T[(b, a)] = co.fftp3d_real_to_complex(r)
+    F = [sum(-1j * K[b] * T[(a, b)] for b in range(3)) for a in range(3)]
+    kk2 = K[0] ** 2 + K[1] ** 2 + K[2] ** 2
+    mask = (kn2 <= co.kmax) & (kn2 >= co.tiny)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        d = (K[0] * F[0] + K[1] * F[1] + K[2] * F[2]) / kk2
+    out = []
+    for a in range(3):
+        Fa = np.where(mask, F[a] - K[a] * d, 0)
+        out.append(Fa + (f[a] if f is not None else 0))
+    return out
+
+
+def eddy_force(co, v, tve, f=None):
+    """o = f - tve(ki) kk2 v with ki = int(sqrt(kk2) + 0.501) on tiny <= kn2 <= kmax."""
+    _, _, _, kn2, kk2 = co.tables()
+    mask = (kn2 <= co.kmax) & (kn2 >= co.tiny)
+    ki = (np.sqrt(kk2) + np.float32(0.501)).astype(int)
+    nut = np.where(mask & (ki >= 1) & (ki <= len(tve)), np.asarray(tve)[np.clip(ki - 1, 0, len(tve) - 1)], 0.0)
+    return [-(nut * np.where(mask, kk2, 0)) * x + (f[a] if f is not None else 0) for a, x in enumerate(v)]

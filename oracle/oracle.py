@@ -75,6 +75,11 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_bouss_rkstep2": (None, [P, I, D, D, D, D, D, D] + [P] * 12),
         "o_bouss_run": (None, [P, I, I, D, D, D, D, D, D] + [P] * 8),
         "o_sharp": (None, [P, P, P, D]),
+        "o_evedqnm": (None, [P, D, P, D, D, P, P, P]),
+        "o_edqnm_rkstep2": (None, [P, I, D, D, P] + [P] * 9),
+        "o_edqnm_run": (None, [P, I, I, D, D, D, D] + [P] * 6),
+        "o_les_truncate": (None, [P, P, P, P, I]),
+        "o_ctx_set_kmax": (None, [P, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -280,6 +285,33 @@ class Oracle:
                              *([None] * 3 if fk is None else [_ptr(x) for x in fk]),
                              None if fsk is None else _ptr(fsk))
         return v, th
+
+    def set_kmax(self, kmax):
+        self.lib.o_ctx_set_kmax(self.h, kmax)
+        info = np.zeros(9)
+        self.lib.o_ctx_info(self.h, info.ctypes.data)
+        self.kmax = float(info[0])
+
+    # EDQNM LES (pseudo/pseudospec3D_edqnm.f90, include/edqnmhd_rkstep2.f90) --
+    def evedqnm(self, Eold, nu, time, kolmo=1.4):
+        nb = self.nx // 2 + 1
+        E = np.ascontiguousarray(Eold, dtype=np.float64)
+        tepq, tve, Ext = np.zeros(nb), np.zeros(nb), np.zeros(3 * nb)
+        self.lib.o_evedqnm(self.h, kolmo, _ptr(E), nu, time, _ptr(tepq), _ptr(tve), _ptr(Ext))
+        return tepq, tve, Ext
+
+    def edqnm_run(self, nsteps, ord, dt, nu, v, f=None, kolmo=1.4, t0=0.0):
+        v = [self._c(x).copy() for x in v]
+        fk = None if f is None else [self._c(x) for x in f]
+        self.lib.o_edqnm_run(self.h, nsteps, ord, dt, nu, kolmo, t0, *[_ptr(x) for x in v],
+                             *([None] * 3 if fk is None else [_ptr(x) for x in fk]))
+        return v
+
+    def les_truncate(self, coarse: "Oracle", a, kc: int):
+        """Modes |k| <= kc of this (fine) spectrum on the coarse grid, times (n/N)^3."""
+        out = coarse.czeros()
+        self.lib.o_les_truncate(self.h, coarse.h, _ptr(self._c(a)), _ptr(out), kc)
+        return out
 
     def nthreads(self):
         return self.lib.o_nthreads()

@@ -1,0 +1,131 @@
+"""The LES kernels (ghost_les_*) against the oracle: sharp truncation,
+training samples (gradients and subgrid stresses), the closure forces
+(EDQNM eddy viscosity and the MLP stress divergence), the EDQNM LES run,
+and that the closure-free LES is the plain HD run.
+
+Tolerances: FP64 1e-12 (single passes) to 1e-10 (runs of several steps);
+FP32 1e-5; the MLP closure 2e-2 (BF16 network against the oracle network
+with the same BF16 rounding, where accumulation order flips some roundings)."""
+import numpy as np
+import pytest
+
+from oracle import les_oracle as LO
+from oracle import mlp_oracle as M
+from oracle.oracle import Oracle
+from tests.conftest import rel_l2
+from tests.helpers import rand_spectral, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def kolmogorov_field(o, seed, kc):
+    """A solenoidal field with E(k) ~ k^-5/3 on 1 <= |k| <= kc."""
+    v, _ = o.random_solenoidal(seed, 1.0, float(kc), 0, 1.0)
+    _, _, _, _, kk2 = o.tables()
+    s = np.where(kk2 > 0, kk2, 1.0) ** (-11.0 / 12.0)
+    return [(x * s).astype(o.cdt) for x in v]
+
+
+def setup(prec, N=64, n=32, kc=10):
+    from ghost_b200 import Ghost
+    from ghost_b200.les import LES
+    fo, co = Oracle(N, precision=prec), Oracle(n, precision=prec)
+    co.set_kmax(float(kc * kc))
+    gf, gc = Ghost(N, precision=prec), Ghost(n, precision=prec)
+    return fo, co, gf, gc, LES(gc, kc)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_truncate(prec):
+    fo, co, gf, gc, les = setup(prec)
+    a = rand_spectral(fo, 1)
+    out = to_host(les.truncate(gf, to_dev(a)))
+    ref = fo.les_truncate(co, a, 10)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_samples(prec):
+    fo, co, gf, gc, les = setup(prec)
+    fo64, co64 = Oracle(64), Oracle(32)
+    v = kolmogorov_field(fo64, 3, 21)
+    cd = gf.cdtype_np
+    x, tau = les.samples(gf, *[to_dev(a.astype(cd)) for a in v], 1.0)
+    rx, rt = LO.samples(fo64, co64, [a.astype(cd).astype(np.complex128) for a in v], 10)
+    tol = 1e-12 if prec == "fp64" else 2e-5
+    assert rel_l2(to_host(x), rx) <= tol
+    assert rel_l2(to_host(tau), rt) <= tol
+
+
+def test_features_and_tau_force():
+    fo, co, gf, gc, les = setup("fp64")
+    v = kolmogorov_field(co, 4, 10)
+    x = les.features(*[to_dev(a) for a in v], 0.5, 2.0)
+    assert rel_l2(to_host(x), LO.features(co, v, 0.5, 2.0)) <= 1e-12
+    tau = np.random.default_rng(5).standard_normal((32 ** 3, 6)).astype(np.float32)
+    f = [rand_spectral(co, 6 + a) for a in range(3)]
+    F = les.tau_force(to_dev(tau), 0.25, [to_dev(a) for a in f])
+    ref = LO.tau_force(co, tau.astype(np.float64), 0.25, f)
+    assert rel_l2([to_host(a) for a in F], ref) <= 1e-12
+
+
+def test_edqnm_closure_force():
+    fo, co, gf, gc, les = setup("fp64")
+    v = kolmogorov_field(co, 8, 10)
+    les.set_model("edqnm", kolmo=1.4)
+    les.set_time(2.0)
+    F = les.closure_force(1e-3, *[to_dev(a) for a in v])
+    Ek, _ = co.spectrumc(*v, 1, 0)
+    _, tve, _ = co.evedqnm(Ek, 1e-3, 2.0)
+    assert np.max(tve) > 0
+    tve_g, _, Ek_g = les.edqnm_last()
+    assert rel_l2(Ek_g, Ek) <= 1e-13
+    assert rel_l2(tve_g, tve) <= 1e-12
+    assert rel_l2([to_host(a) for a in F], LO.eddy_force(co, v, tve)) <= 1e-12
+
+
+def test_edqnm_les_run():
+    fo, co, gf, gc, les = setup("fp64")
+    v = kolmogorov_field(co, 9, 10)
+    f, _ = co.random_solenoidal(10, 2.0, 3.0, 0, 1.0)
+    les.set_model("edqnm")
+    les.set_time(1.0)
+    V = [to_dev(a) for a in v]
+    les.run(3, 2, 1e-3, 1e-3, *V, *[to_dev(a) for a in f])
+    ref = co.edqnm_run(3, 2, 1e-3, 1e-3, v, f, t0=1.0)
+    assert rel_l2([to_host(a) for a in V], ref) <= 1e-11
+
+
+def test_mlp_closure_force():
+    from ghost_b200.les import MLP
+    fo, co, gf, gc, les = setup("fp32")
+    v = kolmogorov_field(co, 11, 10)
+    p = M.glorot(12)
+    m = MLP(0)
+    m.params = p
+    les.set_model("mlp", m, grad_scale=0.3, tau_scale=0.05, delta=1.0)
+    F = les.closure_force(1e-3, *[to_dev(a) for a in v])
+    co64 = Oracle(32)
+    co64.set_kmax(100.0)
+    v64 = [a.astype(np.complex128) for a in v]
+    x = LO.features(co64, v64, 0.3, 1.0).astype(np.float32)
+    y = M.forward(p, x, emulate=True).astype(np.float64)
+    ref = LO.tau_force(co64, y, 0.05)
+    assert rel_l2([to_host(a).astype(np.complex128) for a in F], ref) <= 2e-2
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_les_without_closure_is_hd_run(prec):
+    from ghost_b200 import Ghost
+    fo, co, gf, gc, les = setup(prec)
+    v = kolmogorov_field(co, 13, 10)
+    f, _ = co.random_solenoidal(14, 2.0, 3.0, 0, 1.0)
+    A = [to_dev(a) for a in v]
+    B = [to_dev(a) for a in v]
+    F = [to_dev(a) for a in f]
+    les.run(4, 4, 1e-3, 1e-3, *A, *F)
+    g2 = Ghost(32, precision=prec)
+    g2.lib.ghost_ctx_set_kmax(g2.h, 100.0)
+    g2.hd_run(4, 4, 1e-3, 1e-3, *B, *F)
+    for a, b in zip(A, B):
+        assert np.array_equal(to_host(a), to_host(b))

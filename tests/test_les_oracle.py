@@ -1,0 +1,84 @@
+"""LES pieces on the CPU: the library's host EDQNM (ghost_evedqnm, no GPU
+needed) against the oracle's restatement of pseudo/pseudospec3D_edqnm.f90,
+the oracle's EDQNM against the properties of the closure, and the sample
+and force restatements against identities of the filtered equations."""
+import numpy as np
+import pytest
+
+from oracle import les_oracle as LO
+from oracle.oracle import Oracle
+from tests.conftest import rel_l2
+
+
+def kolmogorov(n, kc, s=0.02):
+    k = np.arange(1, n // 2 + 2, dtype=float)
+    E = k ** (-5 / 3) * np.exp(-s * k)
+    E[kc:] = 0
+    return E
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n,kc", [(64, 21), (128, 42)])
+def test_library_evedqnm_matches_oracle(prec, n, kc):
+    from ghost_b200.les import evedqnm
+    o = Oracle(n, precision=prec)
+    o.set_kmax(float(kc * kc))
+    E = kolmogorov(n, kc)
+    for t in (0.05, 0.5, 5.0):
+        ref = o.evedqnm(E, 1e-3, t)
+        got = evedqnm(n, float(kc * kc), E, 1e-3, t, precision=prec)
+        tol = 1e-12 if prec == "fp64" else 1e-5
+        for a, b in zip(got, ref):
+            assert rel_l2(a, b) <= tol
+
+
+def test_edqnm_eddy_viscosity_shape():
+    """Positive, cusp-shaped eddy viscosity (rising towards kc); no closure
+    at t = 0 (theta cancels frac) and none when the fit fails."""
+    o = Oracle(128)
+    o.set_kmax(42.0 ** 2)
+    E = kolmogorov(128, 42)
+    _, tve, Ext = o.evedqnm(E, 1e-4, 10.0)
+    assert np.all(tve[:42] > 0) and np.all(tve[42:] == 0)
+    assert tve[41] > 3 * tve[20]
+    assert np.all(Ext[42:126] > 0) and np.all(np.diff(Ext[42:126]) < 0)
+    _, tve0, _ = o.evedqnm(E, 1e-4, 0.0)
+    assert np.all(tve0 == 0)
+    steep = np.exp(-np.arange(1, 66, dtype=float))  # power < 0: no fit, no closure
+    _, tve1, _ = o.evedqnm(steep, 1e-4, 10.0)
+    assert np.all(tve1 == 0)
+
+
+def test_samples_identities():
+    """tau from a field that is already band-limited to kc is zero, and the
+    features are the exact gradients of the filtered field."""
+    fo, co = Oracle(32), Oracle(16)
+    kc = 3
+    v, _ = fo.random_solenoidal(5, 1.0, 3.0, 0, 1.0)
+    # a field with |k| <= 1.5 squares to |k| <= 3 = kc: the filter keeps all of u_a u_b
+    vlow, _ = fo.random_solenoidal(6, 1.0, 1.5, 0, 1.0)
+    x, tau = LO.samples(fo, co, vlow, kc)
+    assert np.max(np.abs(tau)) < 1e-13 * np.max(np.abs(x[:, :9])) ** 2
+    # with kc = 2 part of v (|k| <= 3) is unresolved: the mean trace of tau is
+    # the energy of the removed modes, <|u|^2> - <|ubar|^2>
+    x, tau = LO.samples(fo, co, v, 2)
+    assert np.max(np.abs(tau)) > 1e-3
+    kx, ky, kz, kn2, kk2 = fo.tables()
+    w = np.where(np.arange(fo.nxh)[:, None, None] == 0, 1.0, 2.0)
+    removed = sum(np.sum(w * np.abs(np.where(kk2 > 4, a, 0)) ** 2) for a in v) / (32 ** 3) ** 2
+    assert abs(np.mean(tau[:, 0] + tau[:, 1] + tau[:, 2]) - removed) < 1e-12 * removed
+    # solenoidal filtered field: the trace of the gradient vanishes pointwise
+    assert np.max(np.abs(x[:, 0] + x[:, 4] + x[:, 8])) < 1e-12
+
+
+def test_tau_force_is_solenoidal_and_matches_divergence():
+    co = Oracle(16)
+    rng = np.random.default_rng(3)
+    tau = rng.standard_normal((16 ** 3, 6))
+    F = LO.tau_force(co, tau)
+    assert co.divergence(*F) < 1e-20 + 1e-12 * co.energy(*F, 1)
+    # an isotropic stress (pressure-like) gives no force
+    iso = np.zeros_like(tau)
+    iso[:, :3] = rng.standard_normal((16 ** 3, 1))
+    F0 = LO.tau_force(co, iso)
+    assert max(np.max(np.abs(x)) for x in F0) < 1e-10
