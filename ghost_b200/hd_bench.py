@@ -3,6 +3,11 @@ B200 library: advance the HD solver a number of RK steps from the seeded
 initial condition and report per-step wall time and per-kernel device time.
 
     python -m ghost_b200.hd_bench --n 512 --steps 10 --precision fp32 [--out benchmark.txt]
+    python -m ghost_b200.hd_bench --shape 512,512,64 ...    # a slab of the 512^3 passes
+
+A non-cubic --shape keeps the x and y lines of the cubic run at a fraction of
+its memory (the 2/3 truncation then follows GHOST's anisotropic kn2); it is
+the size used for multi-pass profiler captures of the 512-point passes.
 
 The output file follows benchmark.txt's spirit: grid, steps, then seconds
 per step (device) and the per-pass split measured with the library's
@@ -17,6 +22,7 @@ import time
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--shape", default=None, help="nx,ny,nz (overrides --n)")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--ord", type=int, default=4)
@@ -30,10 +36,11 @@ def main(argv=None):
 
     from ghost_b200 import Ghost
 
-    g = Ghost(a.n, precision=a.precision)
+    nx, ny, nz = (int(x) for x in a.shape.split(",")) if a.shape else (a.n, a.n, a.n)
+    g = Ghost(nx, ny, nz, precision=a.precision)
     v = [g.czeros() for _ in range(3)]
     f = [g.czeros() for _ in range(3)]
-    g.init_random_solenoidal(1000, 1.0, a.n / 3.0, 1, 1.0, *v)
+    g.init_random_solenoidal(1000, 1.0, min(nx, ny, nz) / 3.0, 1, 1.0, *v)
     g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *f)
     for _ in range(a.warmup):
         g.hd_run(1, a.ord, a.dt, a.nu, *v, *f)
@@ -51,7 +58,7 @@ def main(argv=None):
     tm = g.read_timers()
     ms = e0.elapsed_time(e1)
     eng = g.energy(*v, 1)
-    lines = [f"{a.n} {a.n} {a.n} {a.steps} 1 {a.precision} {ms / 1e3 / a.steps:.6e} {wall / a.steps:.6e}"]
+    lines = [f"{nx} {ny} {nz} {a.steps} 1 {a.precision} {ms / 1e3 / a.steps:.6e} {wall / a.steps:.6e}"]
     for k, (t, n) in tm.items():
         lines.append(f"  {k:10s} {t / a.steps:9.3f} ms/step  {n // a.steps:3d} launches/step")
     lines.append(f"  <|v|^2> after run: {eng:.12e}")

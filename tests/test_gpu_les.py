@@ -3,8 +3,8 @@ training samples (gradients and subgrid stresses), the closure forces
 (EDQNM eddy viscosity and the MLP stress divergence), the EDQNM LES run,
 and that the closure-free LES is the plain HD run.
 
-Tolerances: FP64 1e-12 (single passes) to 1e-10 (runs of several steps);
-FP32 1e-5; the MLP closure 2e-2 (BF16 network against the oracle network
+Tolerances: FP64 1e-12 (single passes) to 1e-10 (runs of several steps),
+1e-7 for the float32 sample arrays; FP32 1e-5; the MLP closure 2e-2 (BF16 network against the oracle network
 with the same BF16 rounding, where accumulation order flips some roundings)."""
 import numpy as np
 import pytest
@@ -52,7 +52,9 @@ def test_samples(prec):
     cd = gf.cdtype_np
     x, tau = les.samples(gf, *[to_dev(a.astype(cd)) for a in v], 1.0)
     rx, rt = LO.samples(fo64, co64, [a.astype(cd).astype(np.complex128) for a in v], 10)
-    tol = 1e-12 if prec == "fp64" else 2e-5
+    # x and tau are float32 arrays (the network's input format): the FP64
+    # path is exact up to that final rounding
+    tol = 1e-7 if prec == "fp64" else 2e-5
     assert rel_l2(to_host(x), rx) <= tol
     assert rel_l2(to_host(tau), rt) <= tol
 
@@ -61,7 +63,7 @@ def test_features_and_tau_force():
     fo, co, gf, gc, les = setup("fp64")
     v = kolmogorov_field(co, 4, 10)
     x = les.features(*[to_dev(a) for a in v], 0.5, 2.0)
-    assert rel_l2(to_host(x), LO.features(co, v, 0.5, 2.0)) <= 1e-12
+    assert rel_l2(to_host(x), LO.features(co, v, 0.5, 2.0)) <= 1e-7  # float32 output
     tau = np.random.default_rng(5).standard_normal((32 ** 3, 6)).astype(np.float32)
     f = [rand_spectral(co, 6 + a) for a in range(3)]
     F = les.tau_force(to_dev(tau), 0.25, [to_dev(a) for a in f])
