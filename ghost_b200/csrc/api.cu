@@ -730,6 +730,26 @@ int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const voi
   return GHOST_OK;
 }
 
+// The same shell spectrum left on the device (out_dev[nmax/2+1]); no
+// synchronisation, for closures that consume it in later kernels.
+template <typename R>
+int spectrum_dev_async(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_dev) {
+  const size_t n = c->ntot;
+  const int nbins = c->nmax / 2 + 1;
+  const int nblk = std::min(grid1d(n), 148 * 4);
+  double *part;
+  GB_CHECK(partials(c, (size_t)nblk * nbins, &part));
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
+  const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
+  GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
+  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, part);
+  GB_CHECK(post_launch(c));
+  finalize_kernel<<<1, 256, 0, c->stream>>>(part, nblk, nbins, out_dev);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
 // twiddles exp(-2 pi i e/n), e < n, evaluated in extended precision and
 // rounded once to the working precision
 template <typename R> int make_twiddles(int n, void **out) {
@@ -984,7 +1004,8 @@ int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out
   template int derivk3_impl<R>(ghost_ctx *, const void *, void *, int);                                        \
   template int hd_substep_dev<R>(ghost_ctx *, int, double, double, void *const[3], void *const[3],             \
                                  const void *const[3], int, bool);                                             \
-  template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);
+  template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);          \
+  template int spectrum_dev_async<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);
 GB_INST(float)
 GB_INST(double)
 #undef GB_INST

@@ -28,6 +28,9 @@ int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], 
 // kinetic (kind 1) shell spectrum into out_host[nmax/2+1]
 template <typename R>
 int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host);
+// the same into a device array, without synchronising
+template <typename R>
+int spectrum_dev_async(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_dev);
 
 }  // namespace gb
 

@@ -188,18 +188,29 @@ __global__ void eddy_force_kernel(KParams<R> kp, Spec3<R> v, Spec3<R> f, Spec3w<
 static int blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 // ---------------------------------------------------------------------
-// EDQNM eddy viscosity (host), pseudo/pseudospec3D_edqnm.f90.  R is
-// GHOST's GP kind: the spectra are DOUBLE PRECISION, the fit and the
-// quadrature locals are REAL(GP), and the literals 0.218 and real(k*k) are
-// default (single-precision) reals, as in the Fortran.
+// EDQNM eddy viscosity, pseudo/pseudospec3D_edqnm.f90.  R is GHOST's GP
+// kind: the spectra are DOUBLE PRECISION, the fit and the quadrature locals
+// are REAL(GP), and the literals 0.218 and real(k*k) are default
+// (single-precision) reals, as in the Fortran.  The same functions run on
+// the host (ghost_evedqnm) and in one device block (the LES closure), so
+// the closure needs no host round trip.
+__host__ __device__ inline float mlog(float x) { return logf(x); }
+__host__ __device__ inline double mlog(double x) { return log(x); }
+__host__ __device__ inline float mexp(float x) { return expf(x); }
+__host__ __device__ inline double mexp(double x) { return exp(x); }
+__host__ __device__ inline float mpow(float x, float y) { return powf(x, y); }
+__host__ __device__ inline double mpow(double x, double y) { return pow(x, y); }
+__host__ __device__ inline float msqrt(float x) { return sqrtf(x); }
+__host__ __device__ inline double msqrt(double x) { return sqrt(x); }
 
 // spec_fit (pseudospec3D_edqnm.f90:278-402): log-linear fit of Ein over
 // shells kinf..kc and extrapolation to 3 kc.  Arrays are 0-based copies of
 // GHOST's 1-based ones (Efit[k-1] = Efit(k)).
 template <typename R>
-static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *power_out, R *ddelta_out) {
-  const R tinyf = std::min((R)1e-15, (R)0.1 / ((R)n * (R)n));
-  const int kc = (int)std::sqrt(kmax);
+__host__ __device__ void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *power_out,
+                                  R *ddelta_out) {
+  const R tinyf = (R)1e-15 < (R)0.1 / ((R)n * (R)n) ? (R)1e-15 : (R)0.1 / ((R)n * (R)n);
+  const int kc = (int)msqrt(kmax);
   const int ktot = 3 * kc, ksup = kc;
   const int kinf = (int)((R)kc - delk);
   const int nfit = 3 * (n / 2 + 1);
@@ -210,8 +221,8 @@ static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *
   if (Ein[ksup - 1] <= (double)tinyf) return;
   R x = 0, y = 0, z = 0, v = 0, w = 0, m = 0, nn = 0, o = 0, p = 0, expo = 0;
   for (int i = kinf; i <= ksup; ++i) {
-    const R ii = (R)i, li = std::log(ii);
-    const R le = (R)std::log(Ein[i - 1] + (double)tinyf);
+    const R ii = (R)i, li = mlog(ii);
+    const R le = (R)mlog(Ein[i - 1] + (double)tinyf);
     x = x + (R)1;
     y = y + li;
     z = z + le;
@@ -231,17 +242,17 @@ static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *
     ddelta = expo * x / m - power * y / m - z / m;
   }
   if (power >= 0 && ddelta >= 0) {
-    expo = std::exp(expo);
+    expo = mexp(expo);
     for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
     for (int k = ksup + 1; k <= ktot; ++k) {
       const R kk = (R)k;
-      Efit[k - 1] = (double)(expo * std::pow(kk, -power) * std::exp(-ddelta * kk));
+      Efit[k - 1] = (double)(expo * mpow(kk, -power) * mexp(-ddelta * kk));
     }
   } else {
     x = y = z = v = w = 0;
     for (int i = kinf; i <= ksup; ++i) {
-      const R ii = (R)i, li = std::log(ii);
-      const R le = (R)std::log(Ein[i - 1] + (double)tinyf);
+      const R ii = (R)i, li = mlog(ii);
+      const R le = (R)mlog(Ein[i - 1] + (double)tinyf);
       x = x + (R)1;
       y = y + li;
       z = z + le;
@@ -253,11 +264,11 @@ static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *
     dden = x * y;
     if (pden != 0 && dden != 0) {
       power = pnum / pden;
-      expo = std::exp((y * z + power * y * y) / dden);
+      expo = mexp((y * z + power * y * y) / dden);
       for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
       for (int k = ksup + 1; k <= ktot; ++k) {
         const R kk = (R)k;
-        Efit[k - 1] = (double)(expo * std::pow(kk, -power) + tinyf);
+        Efit[k - 1] = (double)(expo * mpow(kk, -power) + tinyf);
       }
     } else {
       for (int k = 1; k <= ksup; ++k) Efit[k - 1] = Ein[k - 1];
@@ -267,59 +278,91 @@ static void spec_fit(int n, R kmax, const double *Ein, R delk, double *Efit, R *
   *ddelta_out = ddelta;
 }
 
-// cusp (pseudospec3D_edqnm.f90:95-171): eddy viscosity nut(k) and modal
-// transfer tepq(k), k = 1..kc, from the extrapolated spectrum.
+// cusp (pseudospec3D_edqnm.f90:95-171), split in two: the damping rates
+// mu(k) = lambda sqrt(sum_{q<=k} q^2 Ext(q)) for k = 1..3kc (mu[k], 1-based,
+// false when Ext(kc+1) = 0 and cusp returns at once), and the quadrature
+// over p, q for one k, which gives nut(k) and tepq(k) (arrays zeroed before).
 template <typename R>
-static void cusp(int n, R kmax, R kolmo, const double *Ext, R nu, R t0, double *tepq, double *nut) {
-  const R lambda = (R)0.218f * std::pow(kolmo, (R)1.5);
-  const int kc = (int)std::sqrt(kmax);
+__host__ __device__ bool cusp_mu(R kmax, R kolmo, const double *Ext, R *mu) {
+  const R lambda = (R)0.218f * mpow(kolmo, (R)1.5);
+  const int kc = (int)msqrt(kmax);
   const int ktot = 3 * kc;
-  if (Ext[kc] == 0.0) return;  // Ext(kc+1)
-  std::vector<R> mu(3 * (n / 2 + 1) + 1, (R)0);
+  if (Ext[kc] == 0.0) return false;  // Ext(kc+1)
   R en = 0;
+  mu[0] = 0;
   for (int k = 1; k <= ktot; ++k) {
     const R tmp = (R)(float)(k * k);
     en = (R)((double)en + (double)tmp * Ext[k - 1]);
-    mu[k] = lambda * std::sqrt(en);
+    mu[k] = lambda * msqrt(en);
   }
-  for (int k = 1; k <= kc; ++k) {
-    const R kk = (R)k;
-    for (int p = kc + 1; p <= ktot; ++p) {
-      const R pp = (R)p, ppi = (R)1 / pp;
-      for (int q = p - k; q <= p; ++q) {
-        if (q == 0) continue;
-        const R qq = (R)q, qqi = (R)1 / qq;
-        R coeff = (R)0.5;
-        if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
-        const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
-        const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
-        const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
-        const R tvvkp = (R)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
-        const R tvvkpsym = (R)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
-        const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
-        const R frac = (R)1 / tmp;
-        const R theta = -std::exp(-tmp * t0) / tmp;
-        nut[k - 1] = nut[k - 1] - (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) /
-                                      ((double)((R)2 * kk * kk) * Ext[k - 1]);
-        tepq[k - 1] = tepq[k - 1] + (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
-      }
-    }
-  }
+  return true;
 }
 
-// evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92)
+template <typename R>
+__host__ __device__ void cusp_k(int k, R kmax, const double *Ext, const R *mu, R nu, R t0, double *tepq,
+                                double *nut) {
+  const int kc = (int)msqrt(kmax);
+  const int ktot = 3 * kc;
+  const R kk = (R)k;
+  double nk = nut[k - 1], tk = tepq[k - 1];
+  for (int p = kc + 1; p <= ktot; ++p) {
+    const R pp = (R)p, ppi = (R)1 / pp;
+    for (int q = p - k; q <= p; ++q) {
+      if (q == 0) continue;
+      const R qq = (R)q, qqi = (R)1 / qq;
+      R coeff = (R)0.5;
+      if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
+      const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
+      const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
+      const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
+      const R tvvkp = (R)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
+      const R tvvkpsym = (R)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
+      const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+      const R frac = (R)1 / tmp;
+      const R theta = -mexp(-tmp * t0) / tmp;
+      nk = nk - (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) / ((double)((R)2 * kk * kk) * Ext[k - 1]);
+      tk = tk + (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
+    }
+  }
+  nut[k - 1] = nk;
+  tepq[k - 1] = tk;
+}
+
+// evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92), host
 template <typename R>
 static void evedqnm(int n, R kmax, R kolmo, const double *Eold, R nu, R time, double *tepq, double *tve,
                     double *Ext) {
-  const int kc = (int)std::sqrt(kmax);
+  const int kc = (int)msqrt(kmax);
   const R delk = (R)3 * (R)kc / (R)4;
   for (int k = 0; k < n / 2 + 1; ++k) tve[k] = tepq[k] = 0;
   R power, ddelta;
   spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
-  if (power > 0) cusp<R>(n, kmax, kolmo, Ext, nu, time, tepq, tve);
+  if (!(power > 0)) return;
+  std::vector<R> mu(3 * kc + 1);
+  if (!cusp_mu<R>(kmax, kolmo, Ext, mu.data())) return;
+  for (int k = 1; k <= kc; ++k) cusp_k<R>(k, kmax, Ext, mu.data(), nu, time, tepq, tve);
+}
+
+// the same in one block: thread 0 fits and forms mu, the threads share the k
+template <typename R>
+__global__ void __launch_bounds__(128) edqnm_kernel(int n, R kmax, R kolmo, const double *__restrict__ Eold, R nu,
+                                                    R time, double *tepq, double *tve, double *Ext, R *mu) {
+  __shared__ int go;
+  const int nb = n / 2 + 1, kc = (int)msqrt(kmax);
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) tve[k] = tepq[k] = 0;
+  if (threadIdx.x == 0) {
+    const R delk = (R)3 * (R)kc / (R)4;
+    R power, ddelta;
+    spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
+    go = (power > 0) && cusp_mu<R>(kmax, kolmo, Ext, mu);
+  }
+  __syncthreads();
+  if (!go) return;
+  for (int k = 1 + threadIdx.x; k <= kc; k += blockDim.x) cusp_k<R>(k, kmax, Ext, mu, nu, time, tepq, tve);
 }
 
 }  // namespace les
+
 
 using namespace les;
 
@@ -338,8 +381,9 @@ struct ghost_les {
   void *rk[3] = {};          // RK copies
   void *force[3] = {};       // closure force + forcing
   float *x = nullptr, *y = nullptr;  // closure inputs / outputs (n^3 rows)
-  double *tve_dev = nullptr;
-  std::vector<double> Ek, tve, tepq, Ext;
+  // EDQNM closure state on the device (n/2+1 shells; Ext 3(n/2+1); mu 3(n/2+1)+1)
+  double *tve_dev = nullptr, *tepq_dev = nullptr, *Ek_dev = nullptr, *Ext_dev = nullptr, *mu_dev = nullptr;
+  bool edqnm_done = false;
   // fine-grid buffers for ghost_les_samples (size of the last fine grid)
   size_t fine_rbytes = 0, fine_cbytes = 0;
   void *fine_real[4] = {};
@@ -456,18 +500,17 @@ static int tau_force_dev(ghost_les *L, const float *tau, float ts, const void *c
   return post_launch(c);
 }
 
+// EDQNM closure on the device: kinetic spectrum -> evedqnm (one block) ->
+// eddy-viscous force; the host is not involved, so a substep does not wait
 template <typename R>
 static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
   ghost_ctx *c = L->c;
   const int nb = c->nx / 2 + 1;
-  L->Ek.assign(nb, 0.0);
-  GB_CHECK(spectrum_dev<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek.data()));
-  L->tve.assign(nb, 0.0);
-  L->tepq.assign(nb, 0.0);
-  L->Ext.assign(3 * nb, 0.0);
-  evedqnm<R>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek.data(), (R)L->nu_cur, (R)L->t, L->tepq.data(), L->tve.data(),
-             L->Ext.data());
-  GB_CUDA(cudaMemcpyAsync(L->tve_dev, L->tve.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
+  GB_CHECK(spectrum_dev_async<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek_dev));
+  edqnm_kernel<R><<<1, 128, 0, c->stream>>>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek_dev, (R)L->nu_cur, (R)L->t,
+                                            L->tepq_dev, L->tve_dev, L->Ext_dev, (R *)L->mu_dev);
+  GB_CHECK(post_launch(c));
+  L->edqnm_done = true;
   Spec3<R> vs, fs;
   Spec3w<R> os;
   for (int a = 0; a < 3; ++a) {
@@ -476,10 +519,7 @@ static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *cons
     os.p[a] = (cx<R> *)o[a];
   }
   eddy_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vs, fs, os, L->tve_dev, nb, c->nspec);
-  GB_CHECK(post_launch(c));
-  // the host table is reused by the next substep: wait for the upload
-  GB_CUDA(cudaStreamSynchronize(c->stream));
-  return GHOST_OK;
+  return post_launch(c);
 }
 
 // closure force of the selected model for the velocity v: o = f + F(v)
@@ -570,7 +610,12 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->force[q]);
   if (!st) st = les_alloc(L, sizeof(float) * c->nreal * GHOST_MLP_NIN, (void **)&L->x);
   if (!st) st = les_alloc(L, sizeof(float) * c->nreal * GHOST_MLP_NOUT, (void **)&L->y);
-  if (!st) st = les_alloc(L, sizeof(double) * (c->nx / 2 + 1), (void **)&L->tve_dev);
+  const size_t nb = c->nx / 2 + 1;
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->tve_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->tepq_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->Ek_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * 3 * nb, (void **)&L->Ext_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * (3 * nb + 1), (void **)&L->mu_dev);
   if (st) {
     ghost_les_destroy(L);
     return st;
@@ -654,6 +699,8 @@ int ghost_les_set_model(ghost_les *L, int model, ghost_mlp *mlp, double grad_sca
     return fail(GHOST_ERR_ARG, "unknown closure %d", model);
   if (model == GHOST_LES_MLP && !mlp) return fail(GHOST_ERR_ARG, "the MLP closure needs a network");
   if (model == GHOST_LES_EDQNM && !(kolmo > 0)) return fail(GHOST_ERR_ARG, "kolmo must be positive");
+  if (model == GHOST_LES_EDQNM && (int)std::sqrt(L->c->kmax) < 4)
+    return fail(GHOST_ERR_ARG, "the EDQNM closure needs a cutoff of at least 4 shells");
   L->model = model;
   L->mlp = mlp;
   L->gs = (float)grad_scale;
@@ -699,10 +746,11 @@ int ghost_les_run(ghost_les *L, int nsteps, int ord, double dt, double nu, void 
 int ghost_les_edqnm_last(ghost_les *L, double *tve, double *tepq, double *Ek) {
   LES_CHECK(L);
   const int nb = L->c->nx / 2 + 1;
-  if ((int)L->tve.size() != nb) return fail(GHOST_ERR_STATE, "no EDQNM evaluation yet");
-  if (tve) memcpy(tve, L->tve.data(), sizeof(double) * nb);
-  if (tepq) memcpy(tepq, L->tepq.data(), sizeof(double) * nb);
-  if (Ek) memcpy(Ek, L->Ek.data(), sizeof(double) * nb);
+  if (!L->edqnm_done) return fail(GHOST_ERR_STATE, "no EDQNM evaluation yet");
+  GB_CUDA(cudaStreamSynchronize(L->c->stream));
+  if (tve) GB_CUDA(cudaMemcpy(tve, L->tve_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (tepq) GB_CUDA(cudaMemcpy(tepq, L->tepq_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (Ek) GB_CUDA(cudaMemcpy(Ek, L->Ek_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
   return GHOST_OK;
 }
 
@@ -711,7 +759,8 @@ int ghost_evedqnm(int n, int precision, double kmax, double kolmo, const double 
   if (!Eold || !tepq || !tve || !Ext) return fail(GHOST_ERR_ARG, "null argument");
   if (n < 16 || (n & (n - 1))) return fail(GHOST_ERR_SIZE, "n %d", n);
   const int kc = (int)std::sqrt(kmax);
-  if (kc < 2 || kc > n / 2 + 1 || 3 * kc > 3 * (n / 2 + 1)) return fail(GHOST_ERR_ARG, "kmax %g", kmax);
+  // the fit uses shells kc - 3kc/4 .. kc, so kc >= 4 keeps them >= 1
+  if (kc < 4 || kc > n / 2) return fail(GHOST_ERR_ARG, "kmax %g: EDQNM needs 4 <= sqrt(kmax) <= n/2", kmax);
   if (precision == GHOST_SINGLE)
     evedqnm<float>(n, (float)kmax, (float)kolmo, Eold, (float)nu, (float)time, tepq, tve, Ext);
   else if (precision == GHOST_DOUBLE)

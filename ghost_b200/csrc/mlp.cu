@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <random>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ghost_b200.h"
@@ -128,8 +129,25 @@ struct Smem {
 
 constexpr int TMEM_COLS = 256;  // D1/D5 at 0, D2/D4 at 64, D3 at 128
 
-// Loads the FP32 master weights as BF16 operands.
-__device__ void load_weights(Smem &s, const float *__restrict__ P) {
+// Forward-only tile storage (inference): no backward buffers, so four CTAs
+// share an SM; D1 and D3 share tensor-memory columns 0.. (D1 is read before
+// the layer-3 product is issued), D2 sits at 64.
+struct SmemF {
+  __nv_bfloat16 w1[NH * KIN];
+  __nv_bfloat16 w2[NH * NH];
+  __nv_bfloat16 w3[KOUT * NH];
+  __nv_bfloat16 x[ROWS * KIN];
+  __nv_bfloat16 h1[ROWS * NH];
+  __nv_bfloat16 h2[ROWS * NH];
+  float b1[NH], b2[NH], b3[KOUT];
+  uint64_t bar;
+  uint32_t tmem;
+};
+constexpr int TMEM_COLS_F = 128;
+
+// Loads the FP32 master weights as BF16 operands (with the transposed
+// copies of the backward products when BWD).
+template <class S, bool BWD> __device__ void load_weights(S &s, const float *__restrict__ P) {
   for (int q = threadIdx.x; q < NH * KIN; q += THREADS) {
     const int n = q / KIN, k = q % KIN;
     s.w1[core_off(n, k, KIN)] = __float2bfloat16_rn(k < NIN ? P[OW1 + n * NIN + k] : 0.f);
@@ -137,15 +155,17 @@ __device__ void load_weights(Smem &s, const float *__restrict__ P) {
   for (int q = threadIdx.x; q < NH * NH; q += THREADS) {
     const int n = q / NH, k = q % NH;
     s.w2[core_off(n, k, NH)] = __float2bfloat16_rn(P[OW2 + n * NH + k]);
-    s.w2t[core_off(n, k, NH)] = __float2bfloat16_rn(P[OW2 + k * NH + n]);
+    if constexpr (BWD) s.w2t[core_off(n, k, NH)] = __float2bfloat16_rn(P[OW2 + k * NH + n]);
   }
   for (int q = threadIdx.x; q < KOUT * NH; q += THREADS) {
     const int n = q / NH, k = q % NH;  // w3: N = outputs (padded), K = hidden
     s.w3[core_off(n, k, NH)] = __float2bfloat16_rn(n < NOUT ? P[OW3 + n * NH + k] : 0.f);
   }
-  for (int q = threadIdx.x; q < NH * KOUT; q += THREADS) {
-    const int n = q / KOUT, k = q % KOUT;  // w3t: N = hidden, K = outputs
-    s.w3t[core_off(n, k, KOUT)] = __float2bfloat16_rn(k < NOUT ? P[OW3 + k * NH + n] : 0.f);
+  if constexpr (BWD) {
+    for (int q = threadIdx.x; q < NH * KOUT; q += THREADS) {
+      const int n = q / KOUT, k = q % KOUT;  // w3t: N = hidden, K = outputs
+      s.w3t[core_off(n, k, KOUT)] = __float2bfloat16_rn(k < NOUT ? P[OW3 + k * NH + n] : 0.f);
+    }
   }
   for (int q = threadIdx.x; q < NH; q += THREADS) {
     s.b1[q] = P[OB1 + q];
@@ -159,7 +179,8 @@ __device__ void load_weights(Smem &s, const float *__restrict__ P) {
 // along both operands.  On a timeout every thread agrees to give up, the
 // status word is set, and the CTA waits (bounded) for the MMAs in flight so
 // that the tensor memory can be released.
-__device__ bool run_mma(Smem &s, uint32_t dcol, const __nv_bfloat16 *A, const __nv_bfloat16 *B, int K, int N,
+template <class S>
+__device__ bool run_mma(S &s, uint32_t dcol, const __nv_bfloat16 *A, const __nv_bfloat16 *B, int K, int N,
                         uint32_t &phase, uint32_t cap, int *status) {
   // operands written by all threads (generic proxy) -> visible to the tensor cores
   gb::fence_proxy_async();
@@ -185,7 +206,7 @@ __device__ bool run_mma(Smem &s, uint32_t dcol, const __nv_bfloat16 *A, const __
 }
 
 // Reads this row's N accumulators of D at column dcol into v (N multiple of 16).
-template <int N> __device__ void read_row(const Smem &s, uint32_t dcol, float (&v)[N]) {
+template <int N, class S> __device__ void read_row(const S &s, uint32_t dcol, float (&v)[N]) {
   const uint32_t lane_base = (uint32_t)(threadIdx.x & ~31) << 16;
 #pragma unroll
   for (int c = 0; c < N; c += 16) {
@@ -209,23 +230,29 @@ struct Gmlp {
 };
 
 // TRAIN = false: inference (y written); true: loss and gradients.
+// Training uses the full tile storage (one CTA per SM); inference the
+// forward-only layout (four CTAs per SM, 128 tensor-memory columns each).
+template <bool TRAIN> using SmemOf = typename std::conditional<TRAIN, Smem, SmemF>::type;
 template <bool TRAIN>
-__global__ void __launch_bounds__(THREADS, 1) mlp_kernel(Gmlp g) {
+__global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  Smem &s = *reinterpret_cast<Smem *>(smem_raw);
+  using S = SmemOf<TRAIN>;
+  S &s = *reinterpret_cast<S *>(smem_raw);
+  constexpr uint32_t COLS = TRAIN ? TMEM_COLS : TMEM_COLS_F;
+  constexpr uint32_t D3 = TRAIN ? 128 : 0;  // column of the layer-3 accumulator
   const int r = threadIdx.x;
   if (threadIdx.x < 32) {  // warp 0 owns the tensor memory
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(gb::smem_u32(&s.tmem)),
-                 "r"(TMEM_COLS)
+                 "r"(COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   if (threadIdx.x == 0) {
     gb::mbar_init(&s.bar, 1);
     gb::fence_barrier_init();
-    s.loss = 0.0;
+    if constexpr (TRAIN) s.loss = 0.0;
   }
-  load_weights(s, g.P);
+  load_weights<S, TRAIN>(s, g.P);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -256,7 +283,7 @@ __global__ void __launch_bounds__(THREADS, 1) mlp_kernel(Gmlp g) {
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b1[h];
         s.h1[core_off(r, h, NH)] = __float2bfloat16_rn(gelu(zz));
-        if (TRAIN) s.g1[r * NH + h] = gelu_d(zz);
+        if constexpr (TRAIN) s.g1[r * NH + h] = gelu_d(zz);
       }
     }
     // ---- layer 2
@@ -268,13 +295,13 @@ __global__ void __launch_bounds__(THREADS, 1) mlp_kernel(Gmlp g) {
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b2[h];
         s.h2[core_off(r, h, NH)] = __float2bfloat16_rn(gelu(zz));
-        if (TRAIN) s.g2[r * NH + h] = gelu_d(zz);
+        if constexpr (TRAIN) s.g2[r * NH + h] = gelu_d(zz);
       }
     }
     // ---- layer 3
-    if (!run_mma(s, 128, s.h2, s.w3, NH, KOUT, phase, g.cap, g.status)) break;
+    if (!run_mma(s, D3, s.h2, s.w3, NH, KOUT, phase, g.cap, g.status)) break;
     float yv[KOUT];
-    read_row<KOUT>(s, 128, yv);
+    read_row<KOUT>(s, D3, yv);
 #pragma unroll
     for (int o = 0; o < KOUT; ++o) yv[o] += s.b3[o];
     if constexpr (!TRAIN) {
@@ -344,7 +371,8 @@ __global__ void __launch_bounds__(THREADS, 1) mlp_kernel(Gmlp g) {
       __syncthreads();
     }
   }
-  if (TRAIN && g.grad) {
+  if constexpr (TRAIN) {
+  if (g.grad) {
     float *dst = g.grad + (size_t)blockIdx.x * (NPARAM + 1);
 #pragma unroll
     for (int m = 0; m < NOWN; ++m) {
@@ -359,10 +387,11 @@ __global__ void __launch_bounds__(THREADS, 1) mlp_kernel(Gmlp g) {
     }
     if (r == 0) dst[NPARAM] = (float)s.loss;
   }
+  }
   tc_fence_before();
   __syncthreads();
   if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(s.tmem), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(s.tmem), "r"(COLS) : "memory");
 }
 
 // Sums the per-CTA partials in block order and applies Adam to the FP32
@@ -410,18 +439,21 @@ static int mlp_launch(ghost_mlp *m, const float *x, const float *t, float *y, in
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
   const int ntiles = (B + ROWS - 1) / ROWS;
-  const int grid = std::max(1, std::min(ntiles, nsm));
   Gmlp g{m->P, x, t, y, train ? m->partials : nullptr, B, 2.f / ((float)B * (float)NOUT), m->status, m->cap};
-  const size_t smem = sizeof(Smem) + 1024;
   if (train) {
+    // one CTA per SM; the per-CTA gradient partials are summed by the Adam kernel
+    const int grid = std::max(1, std::min(ntiles, nsm));
+    const size_t smem = sizeof(Smem) + 1024;
     MLP_CUDA(cudaFuncSetAttribute(mlp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     mlp_kernel<true><<<grid, THREADS, smem, m->stream>>>(g);
+    m->nparts = grid;
   } else {
+    const int grid = std::max(1, std::min(ntiles, 4 * nsm));
+    const size_t smem = sizeof(SmemF) + 1024;
     MLP_CUDA(cudaFuncSetAttribute(mlp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     mlp_kernel<false><<<grid, THREADS, smem, m->stream>>>(g);
   }
   MLP_CUDA(cudaGetLastError());
-  m->nparts = grid;
   return GHOST_OK;
 }
 

@@ -253,35 +253,57 @@ template <typename R> struct ZFwdHD {
     }
     if (!act) return;
     const bool forced = f.p[0] != nullptr;
+    // The projected nonlinear term replaces g in place; then, component by
+    // component, all of the line's operands (v, C, f at the kept modes) are
+    // loaded before any result is stored, so a thread waits for one round
+    // of loads per component rather than one per element.
+    bool keep[E];
+    R kk2e[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int k = t + T * e;
-      const size_t p = (size_t)line * N + k;
-      const R kz = kz_of(kp, k);
       const R kn2 = kn2_of(kp, i, j, k);
-      if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
+      keep[e] = kn2 <= kp.kmax && kn2 >= kp.tiny;
+      kk2e[e] = (R)0;
+      if (keep[e]) {
+        const R kz = kz_of(kp, k);
         const R kk2 = kk2_of(kp, i, j, k);
+        kk2e[e] = kk2;
         const C a = g[0][e], b = g[1][e], cc = g[2][e];
         const C s = mk(kx * a.x + ky * b.x + kz * cc.x, kx * a.y + ky * b.y + kz * cc.y);
-        C nl3[3];
-        nl3[0] = (i == 0) ? mk(-a.x, -a.y) : mk(-a.x + (kx * s.x) / kk2, -a.y + (kx * s.y) / kk2);
-        nl3[1] = (j == 0) ? mk(-b.x, -b.y) : mk(-b.x + (ky * s.x) / kk2, -b.y + (ky * s.y) / kk2);
-        nl3[2] = (k == 0) ? mk(-cc.x, -cc.y) : mk(-cc.x + (kz * s.x) / kk2, -cc.y + (kz * s.y) / kk2);
+        g[0][e] = (i == 0) ? mk(-a.x, -a.y) : mk(-a.x + (kx * s.x) / kk2, -a.y + (kx * s.y) / kk2);
+        g[1][e] = (j == 0) ? mk(-b.x, -b.y) : mk(-b.x + (ky * s.x) / kk2, -b.y + (ky * s.y) / kk2);
+        g[2][e] = (k == 0) ? mk(-cc.x, -cc.y) : mk(-cc.x + (kz * s.x) / kk2, -cc.y + (kz * s.y) / kk2);
+      }
+    }
+    const size_t base = (size_t)line * N + t;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const C vv = v.p[c][p];
-          const C lap = mk(-kk2 * vv.x, -kk2 * vv.y);
-          C sum = mk(nuv * lap.x + nl3[c].x, nuv * lap.y + nl3[c].y);
-          if (forced) {
-            const C ff = f.p[c][p];
-            sum = mk(sum.x + ff.x, sum.y + ff.y);
-          }
-          const C cc0 = c0.p[c][p];
-          v.p[c][p] = mk(cc0.x + (dt * sum.x) * rmp, cc0.y + (dt * sum.y) * rmp);
+    for (int c = 0; c < 3; ++c) {
+      C vv[E], ff[E], cc0[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        vv[e] = mk((R)0, (R)0);
+        ff[e] = mk((R)0, (R)0);
+        cc0[e] = mk((R)0, (R)0);
+        if (keep[e]) {
+          const size_t p = base + (size_t)T * e;
+          vv[e] = v.p[c][p];
+          cc0[e] = c0.p[c][p];
+          if (forced) ff[e] = f.p[c][p];
         }
-      } else {
+      }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v.p[c][p] = mk((R)0, (R)0);
+      for (int e = 0; e < E; ++e) {
+        const size_t p = base + (size_t)T * e;
+        if (keep[e]) {
+          const R kk2 = kk2e[e];
+          const C lap = mk(-kk2 * vv[e].x, -kk2 * vv[e].y);
+          C sum = mk(nuv * lap.x + g[c][e].x, nuv * lap.y + g[c][e].y);
+          if (forced) sum = mk(sum.x + ff[e].x, sum.y + ff[e].y);
+          v.p[c][p] = mk(cc0[e].x + (dt * sum.x) * rmp, cc0[e].y + (dt * sum.y) * rmp);
+        } else {
+          v.p[c][p] = mk((R)0, (R)0);
+        }
       }
     }
   }
@@ -316,45 +338,70 @@ template <typename R> struct ZFwdBouss {
     if (!act) return;
     const bool forced = f.p[0] != nullptr, sforced = f.p[3] != nullptr;
     const R two_om = (R)2 * omegaz;
+    // As in ZFwdHD: all loads of a round before any store.  mode 0: kept
+    // mode; 1: truncated (all zero); 2: kn2 < tiny (theta keeps its mean).
+    int mode[E];
+    R kk2e[E];
+    C vv[4][E];
+    const size_t base = (size_t)line * N + t;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int k = t + T * e;
-      const size_t p = (size_t)line * N + k;
       const R kn2 = kn2_of(kp, i, j, k);
-      if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
-        const R kz = kz_of(kp, k);
-        const R kk2 = kk2_of(kp, i, j, k);
-        C vv[4];
+      mode[e] = (kn2 <= kp.kmax && kn2 >= kp.tiny) ? 0 : (kn2 > kp.kmax ? 1 : 2);
+      kk2e[e] = (R)0;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) vv[c] = v.p[c][p];
-        const C a = mk(g[0][e].x - two_om * vv[1].x, g[0][e].y - two_om * vv[1].y);
-        const C b = mk(g[1][e].x + two_om * vv[0].x, g[1][e].y + two_om * vv[0].y);
-        const C cc = mk(g[2][e].x + xmom * vv[3].x, g[2][e].y + xmom * vv[3].y);
-        const C s = mk(kx * a.x + ky * b.x + kz * cc.x, kx * a.y + ky * b.y + kz * cc.y);
-        C rhs[4];
-        rhs[0] = (i == 0) ? mk(-a.x, -a.y) : mk(-a.x + (kx * s.x) / kk2, -a.y + (kx * s.y) / kk2);
-        rhs[1] = (j == 0) ? mk(-b.x, -b.y) : mk(-b.x + (ky * s.x) / kk2, -b.y + (ky * s.y) / kk2);
-        rhs[2] = (k == 0) ? mk(-cc.x, -cc.y) : mk(-cc.x + (kz * s.x) / kk2, -cc.y + (kz * s.y) / kk2);
-        rhs[3] = mk(g[3][e].x + xtemp * vv[2].x, g[3][e].y + xtemp * vv[2].y);
+      for (int c = 0; c < 4; ++c) vv[c][e] = mk((R)0, (R)0);
+      if (mode[e] == 0) {
+        const size_t p = base + (size_t)T * e;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const R dif = c < 3 ? nu : kappa;
-          const C lap = mk(-kk2 * vv[c].x, -kk2 * vv[c].y);
-          C sum = mk(dif * lap.x + rhs[c].x, dif * lap.y + rhs[c].y);
-          if (c < 3 ? forced : sforced) {
-            const C ff = f.p[c][p];
-            sum = mk(sum.x + ff.x, sum.y + ff.y);
-          }
-          const C cc0 = c0.p[c][p];
-          v.p[c][p] = mk(cc0.x + (dt * sum.x) * rmp, cc0.y + (dt * sum.y) * rmp);
+        for (int c = 0; c < 4; ++c) vv[c][e] = v.p[c][p];
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if (mode[e] != 0) continue;
+      const int k = t + T * e;
+      const R kz = kz_of(kp, k);
+      const R kk2 = kk2_of(kp, i, j, k);
+      kk2e[e] = kk2;
+      const C a = mk(g[0][e].x - two_om * vv[1][e].x, g[0][e].y - two_om * vv[1][e].y);
+      const C b = mk(g[1][e].x + two_om * vv[0][e].x, g[1][e].y + two_om * vv[0][e].y);
+      const C cc = mk(g[2][e].x + xmom * vv[3][e].x, g[2][e].y + xmom * vv[3][e].y);
+      const C s = mk(kx * a.x + ky * b.x + kz * cc.x, kx * a.y + ky * b.y + kz * cc.y);
+      g[0][e] = (i == 0) ? mk(-a.x, -a.y) : mk(-a.x + (kx * s.x) / kk2, -a.y + (kx * s.y) / kk2);
+      g[1][e] = (j == 0) ? mk(-b.x, -b.y) : mk(-b.x + (ky * s.x) / kk2, -b.y + (ky * s.y) / kk2);
+      g[2][e] = (k == 0) ? mk(-cc.x, -cc.y) : mk(-cc.x + (kz * s.x) / kk2, -cc.y + (kz * s.y) / kk2);
+      g[3][e] = mk(g[3][e].x + xtemp * vv[2][e].x, g[3][e].y + xtemp * vv[2][e].y);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const R dif = c < 3 ? nu : kappa;
+      const bool fc = c < 3 ? forced : sforced;
+      C ff[E], cc0[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        ff[e] = mk((R)0, (R)0);
+        cc0[e] = mk((R)0, (R)0);
+        const size_t p = base + (size_t)T * e;
+        if (mode[e] == 0) {
+          cc0[e] = c0.p[c][p];
+          if (fc) ff[e] = f.p[c][p];
+        } else if (mode[e] == 2 && c == 3) {
+          cc0[e] = c0.p[3][p];
         }
-      } else if (kn2 > kp.kmax) {
+      }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) v.p[c][p] = mk((R)0, (R)0);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v.p[c][p] = mk((R)0, (R)0);
-        v.p[3][p] = c0.p[3][p];
+      for (int e = 0; e < E; ++e) {
+        const size_t p = base + (size_t)T * e;
+        if (mode[e] == 0) {
+          const C lap = mk(-kk2e[e] * vv[c][e].x, -kk2e[e] * vv[c][e].y);
+          C sum = mk(dif * lap.x + g[c][e].x, dif * lap.y + g[c][e].y);
+          if (fc) sum = mk(sum.x + ff[e].x, sum.y + ff[e].y);
+          v.p[c][p] = mk(cc0[e].x + (dt * sum.x) * rmp, cc0[e].y + (dt * sum.y) * rmp);
+        } else {
+          v.p[c][p] = (mode[e] == 2 && c == 3) ? cc0[e] : mk((R)0, (R)0);
+        }
       }
     }
   }

@@ -41,7 +41,7 @@ def spectrum_errors(E_les, E_dns, kc):
 
 def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_ratio=4, ord=4, spinup=4000,
         nsnap=40, snap_every=100, val_snaps=4, train_steps=4000, batch=65536, lr=2e-3, seed=7, kolmo=1.4,
-        models=("none", "edqnm", "mlp"), log=print):
+        models=("none", "edqnm", "mlp", "mlp_cal"), deviatoric=True, log=print):
     import numpy as np
     import torch
 
@@ -57,7 +57,7 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     out = {"config": dict(dns_n=dns_n, les_n=les_n, kc=kc, nu_dns=nu_dns, nu_les=nu_les, dt=dt,
                           les_dt=dt * les_dt_ratio, ord=ord, spinup=spinup, nsnap=nsnap, snap_every=snap_every,
                           val_snaps=val_snaps, train_steps=train_steps, batch=batch, lr=lr, seed=seed,
-                          kolmo=kolmo, precision="fp32")}
+                          kolmo=kolmo, deviatoric=deviatoric, precision="fp32")}
 
     # ---- 1. DNS
     g = Ghost(dns_n, precision="fp32")
@@ -102,6 +102,12 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
 
     # ---- 3. training
     ntr = nsnap - val_snaps
+    if deviatoric:
+        # the isotropic part of tau is a pressure: -P div (q I) = 0, so the
+        # network is trained on the trace-free stress only
+        tr3 = T[:, :, :3].sum(-1, keepdim=True) / 3.0
+        T[:, :, :3] -= tr3
+        del tr3
     gs = float(1.0 / X[:ntr, :, :9].pow(2).mean().sqrt())
     ts = float(1.0 / T[:ntr].pow(2).mean().sqrt())
     X[:, :, :9] *= gs
@@ -141,11 +147,33 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
                        "ms": train_ms, "ms_per_step": train_ms / max(1, train_steps),
                        "grad_scale": gs, "tau_scale": ts, "history": loss_hist,
                        "val_loss": loss_hist[-1][2] if loss_hist else None,
-                       "val_loss_zero_model": float(tv.pow(2).mean())}
+                       "val_loss_zero_model": float(tv.pow(2).mean()),
+                       "val_loss_mean_model": float((tv - Ttr.mean(0)).pow(2).mean())}
     # correlation of predicted and true stresses on the validation set
     yv = mlp.forward(xv)
     corr = [float(torch.corrcoef(torch.stack([yv[:, m], tv[:, m]]))[0, 1]) for m in range(6)]
     out["training"]["val_correlation"] = corr
+    # subgrid dissipation Pi = -tau_ab S_ab (S the resolved strain): the part
+    # of the stress that drains resolved energy; correlation and mean ratio
+    g = xv[:, :9].reshape(-1, 3, 3)
+    S = 0.5 * (g + g.transpose(1, 2))
+    w = torch.tensor([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], device=dev)
+    Sv = torch.stack([S[:, 0, 0], S[:, 1, 1], S[:, 2, 2], S[:, 0, 1], S[:, 0, 2], S[:, 1, 2]], 1)
+    pi_true = -(tv * Sv * w).sum(1)
+    pi_pred = -(yv * Sv * w).sum(1)
+    out["training"]["dissipation_corr"] = float(torch.corrcoef(torch.stack([pi_pred, pi_true]))[0, 1])
+    out["training"]["dissipation_mean_ratio"] = float(pi_pred.mean() / pi_true.mean())
+    # a priori dissipation calibration, on training samples: the factor that
+    # makes the network's mean subgrid dissipation equal the data's
+    cal_idx = torch.randint(0, Xtr.shape[0], (min(Xtr.shape[0], 1 << 20),), generator=gen, device=dev)
+    xc, tc = Xtr[cal_idx].contiguous(), Ttr[cal_idx].contiguous()
+    yc = mlp.forward(xc)
+    gc = xc[:, :9].reshape(-1, 3, 3)
+    Sc = 0.5 * (gc + gc.transpose(1, 2))
+    Scv = torch.stack([Sc[:, 0, 0], Sc[:, 1, 1], Sc[:, 2, 2], Sc[:, 0, 1], Sc[:, 0, 2], Sc[:, 1, 2]], 1)
+    cal = float((tc * Scv * w).sum(1).mean() / (yc * Scv * w).sum(1).mean())
+    out["training"]["dissipation_calibration"] = cal
+    del xc, tc, yc
     log(f"trained {train_steps} steps in {train_ms:.0f} ms: val loss {out['training']['val_loss']:.4f} "
         f"(zero model {out['training']['val_loss_zero_model']:.4f}), corr {np.round(corr, 3).tolist()}")
     del X, T, Xtr, Ttr, Xva, Tva
@@ -159,6 +187,8 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
         vl = [x.clone() for x in v0]
         if model == "mlp":
             les.set_model("mlp", mlp, grad_scale=gs, tau_scale=1.0 / ts, delta=1.0)
+        elif model == "mlp_cal":
+            les.set_model("mlp", mlp, grad_scale=gs, tau_scale=cal / ts, delta=1.0)
         elif model == "edqnm":
             les.set_model("edqnm", kolmo=kolmo)
         else:
@@ -190,6 +220,24 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
             + (f"time-avg spectrum error mean {res['error_time_avg']['mean']:.3f} max {res['error_time_avg']['max']:.3f}"
                if ok else "diverged"))
     out["dns_spectrum_time_avg"] = E_dns[1:].mean(0)[:kc + 1].tolist()
+    # where the learned closure's time goes: inputs, network, stress divergence
+    if "mlp" in models:
+        vl = [x.clone() for x in v0]
+        xf = les.features(*vl, gs, 1.0)
+        yf = mlp.forward(xf)
+        parts = {"features": lambda: les.features(*vl, gs, 1.0, x=xf), "network": lambda: mlp.forward(xf, yf),
+                 "stress_force": lambda: les.tau_force(yf, 1.0 / ts)}
+        timing = {}
+        for name, fn in parts.items():
+            fn()
+            e0.record(stream)
+            for _ in range(10):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            timing[name] = e0.elapsed_time(e1) / 10
+        out["closure_ms_per_substep"] = timing
+        log(f"MLP closure per substep: {timing}")
     # cost per unit of simulated time
     dns_per_t = out["dns"]["ms_per_step"] / dt
     out["cost"] = {"dns_ms_per_time_unit": dns_per_t}
@@ -219,12 +267,15 @@ def main(argv=None):
     ap.add_argument("--train-steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--val-snaps", type=int, default=4)
+    ap.add_argument("--full-stress", action="store_true", help="train on tau with its trace")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     t = time.time()
     res = run(dns_n=a.dns_n, les_n=a.les_n, kc=a.kc, nu_dns=a.nu_dns, nu_les=a.nu_les, dt=a.dt,
               les_dt_ratio=a.les_dt_ratio, spinup=a.spinup, nsnap=a.nsnap, snap_every=a.snap_every,
-              train_steps=a.train_steps, batch=a.batch, lr=a.lr)
+              train_steps=a.train_steps, batch=a.batch, lr=a.lr, val_snaps=a.val_snaps,
+              deviatoric=not a.full_stress)
     res["wall_s"] = time.time() - t
     summary = {k: res[k] for k in ("config", "dns", "cost")}
     summary["training"] = {k: v for k, v in res["training"].items() if k != "history"}
