@@ -213,6 +213,7 @@ static int timers_collect(ghost_ctx *c) {
 template <class Op> struct ZKind;
 template <typename R, int S, int NF> struct ZKind<ZC2C<R, S, NF>> { static constexpr int value = GHOST_TIMER_Z_C2C; };
 template <typename R, int P> struct ZKind<ZInv<R, P>> { static constexpr int value = GHOST_TIMER_Z_INV; };
+template <typename R> struct ZKind<ZGrad<R>> { static constexpr int value = GHOST_TIMER_Z_INV; };
 template <typename R> struct ZKind<ZFwdHD<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
 template <typename R> struct ZKind<ZFwdBouss<R>> { static constexpr int value = GHOST_TIMER_Z_FWD; };
 
@@ -550,6 +551,37 @@ template <typename R> int c2r_dev(ghost_ctx *c, const void *in, void *out) {
   f.p[0] = (cx<R> *)w[0];
   GB_CHECK((launch_y<R, +1>(c, f, 1)));
   return launch_x<R, X_C2R>(c, w[0], out);
+}
+
+// The nine gradients d v_a / d x_b of a spectral velocity as real fields
+// (n^3 times their values, GHOST's unnormalised c2r), in three passes over
+// all nine instead of nine separate derivk3 + c2r: real[3a+b] via spec[3a+b].
+template <typename R> int grad9_dev(ghost_ctx *c, const void *const v[3], void *const spec[9], void *const real[9]) {
+  ZGrad<R> zg{};
+  for (int a = 0; a < 3; ++a) zg.v.p[a] = (const cx<R> *)v[a];
+  for (int q = 0; q < 9; ++q) zg.w.p[q] = (cx<R> *)spec[q];
+  zg.kp = kparams<R>(c);
+  GB_CHECK(launch_z<R>(c, zg));
+  Fields<R> fy{};
+  for (int q = 0; q < 9; ++q) fy.p[q] = (cx<R> *)spec[q];
+  GB_CHECK((launch_y<R, +1>(c, fy, 9)));
+  for (int q = 0; q < 9; ++q) GB_CHECK((launch_x<R, X_C2R>(c, spec[q], real[q])));
+  return GHOST_OK;
+}
+
+// Six real fields to spectra at once (the stresses of the LES closure):
+// x r2c per field, then one y and one z pass over all six.
+template <typename R> int r2c6_dev(ghost_ctx *c, const void *const in[6], void *const out[6]) {
+  for (int q = 0; q < 6; ++q) GB_CHECK((launch_x<R, X_R2C>(c, in[q], out[q])));
+  Fields<R> f{};
+  for (int q = 0; q < 6; ++q) f.p[q] = (cx<R> *)out[q];
+  GB_CHECK((launch_y<R, -1>(c, f, 6)));
+  ZC2C<R, -1, 6> op{};
+  for (int q = 0; q < 6; ++q) {
+    op.in.p[q] = (const cx<R> *)out[q];
+    op.out.p[q] = (cx<R> *)out[q];
+  }
+  return launch_z<R>(c, op);
 }
 
 // prodre3 on device pointers (outputs may alias inputs)
@@ -1002,6 +1034,8 @@ int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out
   template int r2c_dev<R>(ghost_ctx *, const void *, void *);                                                  \
   template int c2r_dev<R>(ghost_ctx *, const void *, void *);                                                  \
   template int derivk3_impl<R>(ghost_ctx *, const void *, void *, int);                                        \
+  template int grad9_dev<R>(ghost_ctx *, const void *const[3], void *const[9], void *const[9]);                \
+  template int r2c6_dev<R>(ghost_ctx *, const void *const[6], void *const[6]);                                 \
   template int hd_substep_dev<R>(ghost_ctx *, int, double, double, void *const[3], void *const[3],             \
                                  const void *const[3], int, bool);                                             \
   template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);          \

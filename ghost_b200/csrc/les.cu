@@ -298,37 +298,35 @@ __host__ __device__ bool cusp_mu(R kmax, R kolmo, const double *Ext, R *mu) {
   return true;
 }
 
+// The quadrature of cusp for one (k, p): the sums over q of the terms that
+// GHOST subtracts from nut(k) and adds to tepq(k) (loop body of :139-166).
 template <typename R>
-__host__ __device__ void cusp_k(int k, R kmax, const double *Ext, const R *mu, R nu, R t0, double *tepq,
-                                double *nut) {
-  const int kc = (int)msqrt(kmax);
-  const int ktot = 3 * kc;
-  const R kk = (R)k;
-  double nk = nut[k - 1], tk = tepq[k - 1];
-  for (int p = kc + 1; p <= ktot; ++p) {
-    const R pp = (R)p, ppi = (R)1 / pp;
-    for (int q = p - k; q <= p; ++q) {
-      if (q == 0) continue;
-      const R qq = (R)q, qqi = (R)1 / qq;
-      R coeff = (R)0.5;
-      if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
-      const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
-      const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
-      const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
-      const R tvvkp = (R)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
-      const R tvvkpsym = (R)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
-      const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
-      const R frac = (R)1 / tmp;
-      const R theta = -mexp(-tmp * t0) / tmp;
-      nk = nk - (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) / ((double)((R)2 * kk * kk) * Ext[k - 1]);
-      tk = tk + (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
-    }
+__host__ __device__ void cusp_kp(int k, int p, const double *Ext, const R *mu, R nu, R t0, double *dnut,
+                                 double *dtepq) {
+  const R kk = (R)k, pp = (R)p, ppi = (R)1 / pp;
+  double sn = 0.0, st = 0.0;
+  for (int q = p - k; q <= p; ++q) {
+    if (q == 0) continue;
+    const R qq = (R)q, qqi = (R)1 / qq;
+    R coeff = (R)0.5;
+    if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
+    const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
+    const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
+    const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
+    const R tvvkp = (R)((double)(-qqi * (x * y + z * z * z) * (pp * pp)) * Ext[q - 1] * Ext[k - 1]);
+    const R tvvkpsym = (R)((double)(-ppi * (x * z + y * y * y) * (qq * qq)) * Ext[p - 1] * Ext[k - 1]);
+    const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+    const R frac = (R)1 / tmp;
+    const R theta = -mexp(-tmp * t0) / tmp;
+    sn += (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym) / ((double)((R)2 * kk * kk) * Ext[k - 1]);
+    st += (double)(coeff * (frac + theta)) * (double)(tvvkp + tvvkpsym);
   }
-  nut[k - 1] = nk;
-  tepq[k - 1] = tk;
+  *dnut = sn;
+  *dtepq = st;
 }
 
-// evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92), host
+// evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92), host: the partial
+// sums of each p are added in p order
 template <typename R>
 static void evedqnm(int n, R kmax, R kolmo, const double *Eold, R nu, R time, double *tepq, double *tve,
                     double *Ext) {
@@ -340,25 +338,60 @@ static void evedqnm(int n, R kmax, R kolmo, const double *Eold, R nu, R time, do
   if (!(power > 0)) return;
   std::vector<R> mu(3 * kc + 1);
   if (!cusp_mu<R>(kmax, kolmo, Ext, mu.data())) return;
-  for (int k = 1; k <= kc; ++k) cusp_k<R>(k, kmax, Ext, mu.data(), nu, time, tepq, tve);
+  for (int k = 1; k <= kc; ++k) {
+    double sn = 0.0, st = 0.0;
+    for (int p = kc + 1; p <= 3 * kc; ++p) {
+      double dn, dt;
+      cusp_kp<R>(k, p, Ext, mu.data(), nu, time, &dn, &dt);
+      sn += dn;
+      st += dt;
+    }
+    tve[k - 1] = -sn;
+    tepq[k - 1] = st;
+  }
 }
 
-// the same in one block: thread 0 fits and forms mu, the threads share the k
+// Device: one thread fits the spectrum and forms mu; then one block per
+// shell k, its threads sharing the p, partial sums combined in thread order.
 template <typename R>
-__global__ void __launch_bounds__(128) edqnm_kernel(int n, R kmax, R kolmo, const double *__restrict__ Eold, R nu,
-                                                    R time, double *tepq, double *tve, double *Ext, R *mu) {
-  __shared__ int go;
+__global__ void __launch_bounds__(128) edqnm_fit_kernel(int n, R kmax, R kolmo, const double *__restrict__ Eold,
+                                                        double *tepq, double *tve, double *Ext, R *mu, int *go) {
   const int nb = n / 2 + 1, kc = (int)msqrt(kmax);
   for (int k = threadIdx.x; k < nb; k += blockDim.x) tve[k] = tepq[k] = 0;
   if (threadIdx.x == 0) {
     const R delk = (R)3 * (R)kc / (R)4;
     R power, ddelta;
     spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
-    go = (power > 0) && cusp_mu<R>(kmax, kolmo, Ext, mu);
+    *go = (power > 0) && cusp_mu<R>(kmax, kolmo, Ext, mu) ? 1 : 0;
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) edqnm_cusp_kernel(R kmax, const double *__restrict__ Ext,
+                                                         const R *__restrict__ mu, R nu, R t0,
+                                                         const int *__restrict__ go, double *tepq, double *tve) {
+  __shared__ double sn[128], st[128];
+  const int kc = (int)msqrt(kmax), k = blockIdx.x + 1;
+  if (k > kc || *go == 0) return;
+  double an = 0.0, at = 0.0;
+  for (int p = kc + 1 + threadIdx.x; p <= 3 * kc; p += blockDim.x) {
+    double dn, dt;
+    cusp_kp<R>(k, p, Ext, mu, nu, t0, &dn, &dt);
+    an += dn;
+    at += dt;
+  }
+  sn[threadIdx.x] = an;
+  st[threadIdx.x] = at;
   __syncthreads();
-  if (!go) return;
-  for (int k = 1 + threadIdx.x; k <= kc; k += blockDim.x) cusp_k<R>(k, kmax, Ext, mu, nu, time, tepq, tve);
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < (int)blockDim.x; ++q) {
+      a += sn[q];
+      b += st[q];
+    }
+    tve[k - 1] = -a;
+    tepq[k - 1] = b;
+  }
 }
 
 }  // namespace les
@@ -376,13 +409,14 @@ struct ghost_les {
   double t = 0.0;       // time handed to the EDQNM closure (GHOST's (t-1)*dt)
   double nu_cur = 0.0;  // viscosity of the run in progress
   std::vector<void *> bufs;  // owned device buffers
-  void *spec[9] = {};        // coarse spectral work fields
+  void *spec[12] = {};       // coarse spectral work fields (9..11: the filtered velocity of samples)
   void *real[9] = {};        // coarse real work fields
   void *rk[3] = {};          // RK copies
   void *force[3] = {};       // closure force + forcing
   float *x = nullptr, *y = nullptr;  // closure inputs / outputs (n^3 rows)
   // EDQNM closure state on the device (n/2+1 shells; Ext 3(n/2+1); mu 3(n/2+1)+1)
   double *tve_dev = nullptr, *tepq_dev = nullptr, *Ek_dev = nullptr, *Ext_dev = nullptr, *mu_dev = nullptr;
+  int *go_dev = nullptr;  // 1 when the fit succeeded and the quadrature runs
   bool edqnm_done = false;
   // fine-grid buffers for ghost_les_samples (size of the last fine grid)
   size_t fine_rbytes = 0, fine_cbytes = 0;
@@ -423,13 +457,7 @@ template <typename R> static int truncate_dev(ghost_les *L, ghost_ctx *f, const 
 
 // the nine n^3-scaled velocity gradients of (vx, vy, vz) into L->real
 template <typename R> static int gradients_dev(ghost_les *L, const void *const v[3]) {
-  ghost_ctx *c = L->c;
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) {
-      GB_CHECK(derivk3_impl<R>(c, v[a], L->spec[0], b + 1));
-      GB_CHECK(c2r_dev<R>(c, L->spec[0], L->real[3 * a + b]));
-    }
-  return GHOST_OK;
+  return grad9_dev<R>(L->c, v, L->spec, L->real);
 }
 
 template <typename R> static int features_dev(ghost_les *L, const void *const v[3], float gs, float delta) {
@@ -447,7 +475,7 @@ static int samples_dev(ghost_les *L, ghost_ctx *f, const void *const v[3], float
   ghost_ctx *c = L->c;
   GB_CHECK(les_fine_buffers(L, f));
   // filtered velocity on the coarse grid, its gradients and real values
-  void *ub[3] = {L->spec[6], L->spec[7], L->spec[8]};
+  void *ub[3] = {L->spec[9], L->spec[10], L->spec[11]};
   for (int a = 0; a < 3; ++a) GB_CHECK(truncate_dev<R>(L, f, v[a], ub[a]));
   GB_CHECK(gradients_dev<R>(L, ub));
   GradFields<R> gf;
@@ -486,10 +514,8 @@ static int tau_force_dev(ghost_les *L, const float *tau, float ts, const void *c
   unpack_tau_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(tau, ro, c->nreal, ts);
   GB_CHECK(post_launch(c));
   Spec6<R> T;
-  for (int m = 0; m < 6; ++m) {
-    GB_CHECK(r2c_dev<R>(c, L->real[m], L->spec[m]));
-    T.T[m] = (const cx<R> *)L->spec[m];
-  }
+  GB_CHECK(r2c6_dev<R>(c, L->real, L->spec));
+  for (int m = 0; m < 6; ++m) T.T[m] = (const cx<R> *)L->spec[m];
   Spec3<R> fs;
   Spec3w<R> os;
   for (int a = 0; a < 3; ++a) {
@@ -507,8 +533,11 @@ static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *cons
   ghost_ctx *c = L->c;
   const int nb = c->nx / 2 + 1;
   GB_CHECK(spectrum_dev_async<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek_dev));
-  edqnm_kernel<R><<<1, 128, 0, c->stream>>>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek_dev, (R)L->nu_cur, (R)L->t,
-                                            L->tepq_dev, L->tve_dev, L->Ext_dev, (R *)L->mu_dev);
+  edqnm_fit_kernel<R><<<1, 128, 0, c->stream>>>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek_dev, L->tepq_dev, L->tve_dev,
+                                                L->Ext_dev, (R *)L->mu_dev, L->go_dev);
+  GB_CHECK(post_launch(c));
+  edqnm_cusp_kernel<R><<<nb, 128, 0, c->stream>>>((R)c->kmax, L->Ext_dev, (const R *)L->mu_dev, (R)L->nu_cur,
+                                                  (R)L->t, L->go_dev, L->tepq_dev, L->tve_dev);
   GB_CHECK(post_launch(c));
   L->edqnm_done = true;
   Spec3<R> vs, fs;
@@ -604,7 +633,7 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   L->c = c;
   L->kc = kc;
   int st = GHOST_OK;
-  for (int q = 0; q < 9 && !st; ++q) st = les_alloc(L, c->cbytes, &L->spec[q]);
+  for (int q = 0; q < 12 && !st; ++q) st = les_alloc(L, c->cbytes, &L->spec[q]);
   for (int q = 0; q < 9 && !st; ++q) st = les_alloc(L, c->rbytes, &L->real[q]);
   for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->rk[q]);
   for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->force[q]);
@@ -616,6 +645,7 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->Ek_dev);
   if (!st) st = les_alloc(L, sizeof(double) * 3 * nb, (void **)&L->Ext_dev);
   if (!st) st = les_alloc(L, sizeof(double) * (3 * nb + 1), (void **)&L->mu_dev);
+  if (!st) st = les_alloc(L, sizeof(int), (void **)&L->go_dev);
   if (st) {
     ghost_les_destroy(L);
     return st;

@@ -107,6 +107,22 @@ __device__ __forceinline__ float gelu_d(float z) {
   return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
+// Eight consecutive K entries of one row are 16 contiguous bytes of a core
+// matrix: round them to BF16 and store them with one 16-byte write.
+__device__ __forceinline__ void store8_bf16(__nv_bfloat16 *dst, const float *v) {
+  uint4 u;
+  __nv_bfloat162 p;
+  p = __floats2bfloat162_rn(v[0], v[1]);
+  u.x = *reinterpret_cast<uint32_t *>(&p);
+  p = __floats2bfloat162_rn(v[2], v[3]);
+  u.y = *reinterpret_cast<uint32_t *>(&p);
+  p = __floats2bfloat162_rn(v[4], v[5]);
+  u.z = *reinterpret_cast<uint32_t *>(&p);
+  p = __floats2bfloat162_rn(v[6], v[7]);
+  u.w = *reinterpret_cast<uint32_t *>(&p);
+  *reinterpret_cast<uint4 *>(dst) = u;
+}
+
 struct Smem {
   __nv_bfloat16 w1[NH * KIN];   // B operands (N x K)
   __nv_bfloat16 w2[NH * NH];
@@ -271,9 +287,13 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
     const int row = tile * ROWS + r;
     const bool live = row < g.B;
     // ---- X
+    {
+      float xv[KIN];
 #pragma unroll
-    for (int k = 0; k < KIN; ++k)
-      s.x[core_off(r, k, KIN)] = __float2bfloat16_rn(live && k < NIN ? g.x[(size_t)row * NIN + k] : 0.f);
+      for (int k = 0; k < KIN; ++k) xv[k] = live && k < NIN ? g.x[(size_t)row * NIN + k] : 0.f;
+#pragma unroll
+      for (int k = 0; k < KIN; k += 8) store8_bf16(&s.x[core_off(r, k, KIN)], xv + k);
+    }
     // ---- layer 1
     if (!run_mma(s, 0, s.x, s.w1, KIN, NH, phase, g.cap, g.status)) break;
     {
@@ -282,9 +302,11 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b1[h];
-        s.h1[core_off(r, h, NH)] = __float2bfloat16_rn(gelu(zz));
+        z[h] = gelu(zz);
         if constexpr (TRAIN) s.g1[r * NH + h] = gelu_d(zz);
       }
+#pragma unroll
+      for (int h = 0; h < NH; h += 8) store8_bf16(&s.h1[core_off(r, h, NH)], z + h);
     }
     // ---- layer 2
     if (!run_mma(s, 64, s.h1, s.w2, NH, NH, phase, g.cap, g.status)) break;
@@ -294,9 +316,11 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b2[h];
-        s.h2[core_off(r, h, NH)] = __float2bfloat16_rn(gelu(zz));
+        z[h] = gelu(zz);
         if constexpr (TRAIN) s.g2[r * NH + h] = gelu_d(zz);
       }
+#pragma unroll
+      for (int h = 0; h < NH; h += 8) store8_bf16(&s.h2[core_off(r, h, NH)], z + h);
     }
     // ---- layer 3
     if (!run_mma(s, D3, s.h2, s.w3, NH, KOUT, phase, g.cap, g.status)) break;
@@ -310,6 +334,7 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
         for (int o = 0; o < NOUT; ++o) g.y[(size_t)row * NOUT + o] = yv[o];
     } else {
       // ---- loss and dY
+      float dyv[KOUT];
 #pragma unroll
       for (int o = 0; o < KOUT; ++o) {
         float d = 0.f;
@@ -318,15 +343,19 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
           lacc += (double)e * (double)e;
           d = e * g.inv_count;
         }
-        s.dy[core_off(r, o, KOUT)] = __float2bfloat16_rn(d);
+        dyv[o] = d;
       }
+#pragma unroll
+      for (int o = 0; o < KOUT; o += 8) store8_bf16(&s.dy[core_off(r, o, KOUT)], dyv + o);
       // ---- dH2 = dY W3  (A = dY: 128 x 16, B = W3^T: 64 x 16)
       if (!run_mma(s, 64, s.dy, s.w3t, KOUT, NH, phase, g.cap, g.status)) break;
       {
         float dh[NH];
         read_row<NH>(s, 64, dh);
 #pragma unroll
-        for (int h = 0; h < NH; ++h) s.dz2[core_off(r, h, NH)] = __float2bfloat16_rn(dh[h] * s.g2[r * NH + h]);
+        for (int h = 0; h < NH; ++h) dh[h] *= s.g2[r * NH + h];
+#pragma unroll
+        for (int h = 0; h < NH; h += 8) store8_bf16(&s.dz2[core_off(r, h, NH)], dh + h);
       }
       // ---- dH1 = dZ2 W2  (B = W2^T)
       if (!run_mma(s, 0, s.dz2, s.w2t, NH, NH, phase, g.cap, g.status)) break;

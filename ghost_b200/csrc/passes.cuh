@@ -225,6 +225,42 @@ template <typename R, int PHYS> struct ZInv {
   }
 };
 
+// The nine velocity gradients (derivk3 of each component along each axis,
+// pseudospec3D_hd.f90:22-88) with their inverse z transforms:
+// w[3a+b] = i k_b v_a, for the inputs of the LES closure.
+template <typename R> struct ZGrad {
+  using C = cx<R>;
+  static constexpr int NLOAD = 3;
+  CFields<R> v;  // 3
+  Fields<R> w;   // 9 outputs
+  KParams<R> kp;
+  __device__ __forceinline__ const C *load_src(int f) const { return v.p[f]; }
+  template <int N, int E, class Buf, class Sync, class In>
+  __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
+    constexpr int T = N / E;
+    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh;
+    const R kx = kx_of(kp, i), ky = ky_of(kp, j);
+#pragma unroll
+    for (int f = 0; f < 9; ++f) {
+      const int a = f / 3, b = f % 3;
+      C x[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = t + T * e;
+        const R kd = b == 0 ? kx : (b == 1 ? ky : kz_of(kp, k));
+        const C u = src(a)[k];
+        x[e] = mk(-(kd * u.y), kd * u.x);
+      }
+      line_fft<C, N, E, +1>(x, t, tw, buf, sync);
+      if (act) {
+        C *dst = w.p[f] + (size_t)line * N;
+#pragma unroll
+        for (int e = 0; e < E; ++e) dst[t + T * e] = x[e];
+      }
+    }
+  }
+};
+
 // HD forward epilogue: forward z transform of the three components of
 // omega x v, then nonlhd3 x3 (pseudospec3D_hd.f90:399-509), laplak3 and
 // the truncated RK update of include/hd_rkstep2.f90:18-38, written to v.

@@ -36,6 +36,9 @@ def spectrum_errors(E_les, E_dns, kc):
     b = np.asarray(E_dns)[:kc]
     r = np.abs(a / b - 1.0)
     return {"mean": float(r.mean()), "max": float(r.max()), "rms": float(np.sqrt(np.mean(r ** 2))),
+            # the same over the inertial shells k <= kc/2, and weighted by energy
+            "mean_k_le_kc_half": float(r[:kc // 2].mean()),
+            "energy_weighted": float(np.abs(a - b).sum() / b.sum()),
             "per_k": r.tolist()}
 
 
