@@ -98,6 +98,9 @@ SIGNATURES = {
     "ghost_ensemble_autotune": [P, I, D, ctypes.POINTER(ctypes.c_int)],
     "ghost_ensemble_run": [P, I, I, D],
     "ghost_ensemble_energy": [P, I, PD],
+    "ghost_ctx_set_tile_cfg": [P, I],
+    "ghost_ctx_get_tile_cfg": [P, ctypes.POINTER(ctypes.c_int)],
+    "ghost_hd_autotune": [P, I, D, D, P, P, P, P, P, P, ctypes.POINTER(ctypes.c_int)],
     "ghost_mlp_create": [I, ctypes.POINTER(P)],
     "ghost_mlp_destroy": [P],
     "ghost_mlp_set_stream": [P, P],

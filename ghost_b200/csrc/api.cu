@@ -296,13 +296,14 @@ static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box
 
 static PipeCtl pipe_ctl(ghost_ctx *c) { return PipeCtl{c->status, c->wait_cap, c->inject_stall}; }
 
-template <typename R, int N, int LPB, class Op> int launch_z_cfg(ghost_ctx *c, const Op &op, const Prune &pr) {
+template <typename R, int N, int LPB, int STAGES0, int MINB, class Op>
+int launch_z_cfg(ghost_ctx *c, const Op &op, const Prune &pr) {
   constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
   using G = ZGeom<R, N, E, LPB, Op::NLOAD>;
-  constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
+  constexpr int STAGES = G::smem_bytes(STAGES0) <= 200 * 1024 ? STAGES0 : 2;
   const size_t smem = G::smem_bytes(STAGES);
   const int nlines = pr.lines ? pr.nlines : c->ny * c->nxh * c->nruns;
-  auto kern = zpipe_kernel<R, N, E, LPB, STAGES, Op>;
+  auto kern = zpipe_kernel<R, N, E, LPB, STAGES, MINB, Op>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = persistent_grid(c, kern, LPB * T, smem, (nlines + LPB - 1) / LPB);
   const int ts = timer_begin(c, ZKind<Op>::value);
@@ -311,13 +312,18 @@ template <typename R, int N, int LPB, class Op> int launch_z_cfg(ghost_ctx *c, c
   return post_launch(c);
 }
 
-// CTAs of 256 threads, or of 128 threads with tile variant bit 1
+// CTAs of 256 threads; with tile variant bit 1 of 128 threads; with bits 1
+// and 2 of 128 threads with a two-stage ring and at most 170 registers, so
+// that three CTAs share an SM (lines of 256 points or more)
 template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
   constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
   constexpr int L256 = 256 / T > 0 ? 256 / T : 1;
   constexpr int L128 = 128 / T > 0 ? 128 / T : 1;
-  if ((c->tile_cfg & 2) && L128 != L256) return launch_z_cfg<R, N, L128>(c, op, pr);
-  return launch_z_cfg<R, N, L256>(c, op, pr);
+  if constexpr (N >= 256 && L128 != L256) {
+    if ((c->tile_cfg & 6) == 6) return launch_z_cfg<R, N, L128, 2, 3>(c, op, pr);
+  }
+  if ((c->tile_cfg & 2) && L128 != L256) return launch_z_cfg<R, N, L128, 3, 1>(c, op, pr);
+  return launch_z_cfg<R, N, L256, 3, 1>(c, op, pr);
 }
 
 template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const Prune &pr = Prune()) {
@@ -1567,6 +1573,80 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
   return st.finish();
 }
 
+// Tile variants tried by the autotuners (bit 0: y tiles 16 z-lines wide;
+// bit 1: z CTAs of 128 threads; bits 1 and 2: two-stage z ring, three CTAs
+// per SM).
+static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7};
+
+int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
+  CTX_CHECK(c);
+  if (cfg < 0 || cfg > 7) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..7", cfg);
+  c->tile_cfg = cfg;
+  return GHOST_OK;
+}
+
+int ghost_ctx_get_tile_cfg(const ghost_ctx *c, int *cfg) {
+  CTX_CHECK(c);
+  if (!cfg) return fail(GHOST_ERR_ARG, "null output");
+  *cfg = c->tile_cfg;
+  return GHOST_OK;
+}
+
+int ghost_hd_autotune(ghost_ctx *c, int ord, double dt, double nu, const void *vx, const void *vy, const void *vz,
+                      const void *fx, const void *fy, const void *fz, int *cfg_out) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz || ord < 1) return fail(GHOST_ERR_ARG, "bad argument");
+  if ((fx == nullptr) != (fy == nullptr) || (fx == nullptr) != (fz == nullptr))
+    return fail(GHOST_ERR_ARG, "forcing components must be all given or all null");
+  const void *vu[3] = {vx, vy, vz}, *fu[3] = {fx, fy, fz};
+  for (int q = 0; q < 3; ++q)
+    if (!is_device_ptr(vu[q]) || (fx && !is_device_ptr(fu[q])))
+      return fail(GHOST_ERR_ARG, "ghost_hd_autotune takes device arrays");
+  // time on a copy: the caller's v does not advance
+  void *w[3] = {nullptr, nullptr, nullptr}, *Cd[3];
+  int st = GHOST_OK;
+  for (int q = 0; q < 3 && !st; ++q) st = dalloc(&w[q], c->cbytes);
+  for (int q = 0; q < 3 && !st; ++q) {
+    if (!c->rk[q]) st = dalloc(&c->rk[q], c->cbytes);
+    Cd[q] = c->rk[q];
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float best = 1e30f;
+  int best_cfg = c->tile_cfg;
+  for (int cfg : kTileCfgs) {
+    if (st) break;
+    c->tile_cfg = cfg;
+    float tot = 0.f;
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      for (int q = 0; q < 3; ++q) cudaMemcpyAsync(w[q], vu[q], c->cbytes, cudaMemcpyDeviceToDevice, c->stream);
+      cudaEventRecord(a, c->stream);
+      for (int o = ord; o >= 1 && !st; --o)
+        st = c->precision == GHOST_SINGLE
+                 ? hd_substep_dev<float>(c, o, dt, nu, w, Cd, fx ? fu : nullptr, o == ord, o != ord)
+                 : hd_substep_dev<double>(c, o, dt, nu, w, Cd, fx ? fu : nullptr, o == ord, o != ord);
+      cudaEventRecord(b, c->stream);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) tot += ms;  // the first repetition warms up
+    }
+    if (!st && tot < best) {
+      best = tot;
+      best_cfg = cfg;
+    }
+  }
+  c->tile_cfg = best_cfg;
+  cudaStreamSynchronize(c->stream);
+  for (void *p : w) cudaFree(p);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  GB_CHECK(st);
+  if (cfg_out) *cfg_out = best_cfg;
+  return check_status(c);
+}
+
 int ghost_init_random_solenoidal(ghost_ctx *c, int32_t *seed, double kdn, double kup, int shape, double amp, void *ox,
                                  void *oy, void *oz) {
   CTX_CHECK(c);
@@ -1984,7 +2064,8 @@ int ghost_ensemble_autotune(ghost_ensemble *e, int ord, double dt, int *cfg_out)
     float best = 1e30f;
     int best_cfg = 0;
     int st = GHOST_OK;
-    for (int cfg = 0; cfg < 4 && st == GHOST_OK; ++cfg) {
+    for (int cfg : kTileCfgs) {
+      if (st != GHOST_OK) break;
       c->tile_cfg = cfg;
       float tot = 0.f;
       for (int rep = 0; rep < 3 && st == GHOST_OK; ++rep) {

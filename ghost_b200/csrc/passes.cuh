@@ -64,8 +64,8 @@ struct PipeCtl {
 
 // lines != nullptr: the pass covers the listed (j,i) lines only (entries
 // < 0 pad the list); otherwise lines 0..nlines-1.
-template <typename R, int N, int E, int LPB, int STAGES, class Op>
-__global__ void __launch_bounds__(LPB *(N / E)) zpipe_kernel(Op op, const cx<R> *__restrict__ twg,
+template <typename R, int N, int E, int LPB, int STAGES, int MINB, class Op>
+__global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const cx<R> *__restrict__ twg,
                                                               const int *__restrict__ lines, int nlines,
                                                               PipeCtl ctl) {
   using C = cx<R>;

@@ -359,6 +359,26 @@
          REAL(C_DOUBLE) :: out(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_ctx_set_tile_cfg(ctx,cfg) BIND(C,name="ghost_ctx_set_tile_cfg") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT), VALUE :: cfg
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ctx_get_tile_cfg(ctx,cfg) BIND(C,name="ghost_ctx_get_tile_cfg") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx
+         INTEGER(C_INT) :: cfg
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_hd_autotune(ctx,ord,dt,nu,vx,vy,vz,fx,fy,fz,cfg) BIND(C,name="ghost_hd_autotune") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, fx, fy, fz
+         INTEGER(C_INT), VALUE :: ord
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         INTEGER(C_INT) :: cfg
+         INTEGER(C_INT) :: s
+       END FUNCTION
        ! learned subgrid-stress closure (no GHOST counterpart)
        FUNCTION ghost_mlp_create(seed,mlp) BIND(C,name="ghost_mlp_create") RESULT(s)
          IMPORT :: C_INT, C_PTR

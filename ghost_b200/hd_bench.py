@@ -29,6 +29,7 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=5e-4)
     ap.add_argument("--nu", type=float, default=1e-3)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--tile-cfg", type=int, default=None, help="tile variant; default: autotune")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
 
@@ -42,6 +43,11 @@ def main(argv=None):
     f = [g.czeros() for _ in range(3)]
     g.init_random_solenoidal(1000, 1.0, min(nx, ny, nz) / 3.0, 1, 1.0, *v)
     g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *f)
+    if a.tile_cfg is None:
+        cfg = g.hd_autotune(a.ord, a.dt, a.nu, *v, *f)
+    else:
+        g.set_tile_cfg(a.tile_cfg)
+        cfg = a.tile_cfg
     for _ in range(a.warmup):
         g.hd_run(1, a.ord, a.dt, a.nu, *v, *f)
     torch.cuda.synchronize()
@@ -62,6 +68,7 @@ def main(argv=None):
     for k, (t, n) in tm.items():
         lines.append(f"  {k:10s} {t / a.steps:9.3f} ms/step  {n // a.steps:3d} launches/step")
     lines.append(f"  <|v|^2> after run: {eng:.12e}")
+    lines.append(f"  tile variant {cfg}")
     text = "\n".join(lines)
     print(text)
     if a.out:

@@ -127,6 +127,21 @@ class Ghost:
             return ctypes.c_void_p(x.ctypes.data)
         raise TypeError(f"unsupported array type {type(x)}")
 
+    def set_tile_cfg(self, cfg: int):
+        check(self.lib.ghost_ctx_set_tile_cfg(self.h, int(cfg)), "ghost_ctx_set_tile_cfg")
+
+    def tile_cfg(self) -> int:
+        c = ctypes.c_int()
+        check(self.lib.ghost_ctx_get_tile_cfg(self.h, ctypes.byref(c)), "ghost_ctx_get_tile_cfg")
+        return c.value
+
+    def hd_autotune(self, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None) -> int:
+        """Pick the fastest tile variant for this run (v does not advance)."""
+        c = ctypes.c_int()
+        check(self.lib.ghost_hd_autotune(self.h, ord, dt, nu, *[self._ptr(x, "c") for x in (vx, vy, vz, fx, fy, fz)],
+                                         ctypes.byref(c)), "ghost_hd_autotune")
+        return c.value
+
     def launch_count(self) -> int:
         n = ctypes.c_longlong()
         check(self.lib.ghost_ctx_launch_count(self.h, ctypes.byref(n)), "ghost_ctx_launch_count")

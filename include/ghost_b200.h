@@ -41,7 +41,7 @@ extern "C" {
 /* status codes */
 #define GHOST_OK 0
 #define GHOST_ERR_ARG 1     /* bad argument: null pointer, dir/kin/o out of range */
-#define GHOST_ERR_SIZE 2    /* unsupported grid: each n must be a power of two in [16,2048] */
+#define GHOST_ERR_SIZE 2    /* unsupported grid: each n must be a power of two in [16,1024] */
 #define GHOST_ERR_ALLOC 3   /* device allocation failed */
 #define GHOST_ERR_CUDA 4    /* CUDA runtime error (launch or execution) */
 #define GHOST_ERR_TIMEOUT 5 /* a bounded device-side wait gave up */
@@ -89,6 +89,17 @@ int ghost_ctx_set_stream(ghost_ctx *ctx, void *cuda_stream);
 /* Override the truncation wavenumber kmax, e.g. the EDQNM choice
  * kmax = (n/2-0.5)^2 of main3D.fpp:1732-1734. */
 int ghost_ctx_set_kmax(ghost_ctx *ctx, double kmax);
+/* Tile variant of the FFT passes (no GHOST counterpart; FFTW's planner
+ * plays this role in fftp-3/fftp3D.fpp:92-107): bit 0 y tiles 16 z-lines
+ * wide instead of 8; bit 1 z-pass CTAs of 128 threads instead of 256; bits
+ * 1 and 2 together a two-stage z ring with three CTAs per SM.  Results do
+ * not depend on the variant. */
+int ghost_ctx_set_tile_cfg(ghost_ctx *ctx, int cfg);
+int ghost_ctx_get_tile_cfg(const ghost_ctx *ctx, int *cfg);
+/* Times one RK step of every tile variant on a copy of v (device arrays;
+ * v does not advance) and keeps the fastest; cfg_out may be NULL. */
+int ghost_hd_autotune(ghost_ctx *ctx, int ord, double dt, double nu, const void *vx, const void *vy,
+                      const void *vz, const void *fx, const void *fy, const void *fz, int *cfg_out);
 /* Block until the context's stream is idle; reports asynchronous errors. */
 int ghost_ctx_synchronize(ghost_ctx *ctx);
 /* Bound on the polls of every device-side wait (tile arrivals in the

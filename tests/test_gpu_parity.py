@@ -412,3 +412,29 @@ def test_ensemble_graph_steps_match_oracle(prec):
             assert rel_l2(got, ref) < tol, (c, k)
             assert e[q] == pytest.approx(o.energy(*ref, 1), rel=max(tol, 1e-13))
             q += 1
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_tile_variants_are_bitwise_identical(prec):
+    """Every tile variant (y tile width, z CTA size, two-stage z ring) gives
+    the same bits, and the autotuner leaves the velocity untouched."""
+    import torch
+    n = 256
+    g = ghost(n, precision=prec)
+    V0 = [g.czeros() for _ in range(3)]
+    F = [g.czeros() for _ in range(3)]
+    g.init_random_solenoidal(1000, 1.0, n / 3.0, 1, 1.0, *V0)
+    g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *F)
+    keep = [x.clone() for x in V0]
+    cfg = g.hd_autotune(4, 5e-4, 1e-3, *V0, *F)
+    assert cfg in (0, 1, 2, 3, 6, 7)
+    assert all(torch.equal(a, b) for a, b in zip(V0, keep))
+    ref = None
+    for c in (0, 1, 2, 3, 6, 7):
+        g.set_tile_cfg(c)
+        V = [x.clone() for x in keep]
+        g.hd_run(2, 4, 5e-4, 1e-3, *V, *F)
+        if ref is None:
+            ref = V
+        else:
+            assert all(torch.equal(a, b) for a, b in zip(V, ref)), c
