@@ -315,10 +315,18 @@ int launch_z_cfg(ghost_ctx *c, const Op &op, const Prune &pr) {
 // CTAs of 256 threads; with tile variant bit 1 of 128 threads; with bits 1
 // and 2 of 128 threads with a two-stage ring and at most 170 registers, so
 // that three CTAs share an SM (lines of 256 points or more)
+// lines per CTA, halved from want until a two-stage ring of NL fields fits
+template <typename R, int N, int NL> constexpr int fit_lines(int want) {
+  int lpb = want;
+  while (lpb > 1 && ((size_t)2 * NL * lpb * N + N + (size_t)2 * lpb * (N + N / 8)) * sizeof(cx<R>) + 24 > 220 * 1024)
+    lpb /= 2;
+  return lpb;
+}
+
 template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op, const Prune &pr) {
   constexpr int E = zE<R>() < N ? zE<R>() : N, T = N / E;
-  constexpr int L256 = 256 / T > 0 ? 256 / T : 1;
-  constexpr int L128 = 128 / T > 0 ? 128 / T : 1;
+  constexpr int L256 = fit_lines<R, N, Op::NLOAD>(256 / T > 0 ? 256 / T : 1);
+  constexpr int L128 = fit_lines<R, N, Op::NLOAD>(128 / T > 0 ? 128 / T : 1);
   if constexpr (N >= 256 && L128 != L256) {
     if ((c->tile_cfg & 6) == 6) return launch_z_cfg<R, N, L128, 2, 3>(c, op, pr);
   }
@@ -366,7 +374,14 @@ int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
 
 // tiles 8 z-lines wide, or 16 with tile variant bit 0
 template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
-  if ((c->tile_cfg & 1) && c->nz >= 16) return launch_y_cfg<R, N, S, 16>(c, f, nf, pr);
+  // the 16-wide tile needs two stages of 16 lines in shared memory; where
+  // that does not fit (FP64, long lines) the variant falls back to 8
+  constexpr int E = N < 8 ? N : 8, T = N / E;
+  constexpr int BZ16 = 16 * T <= 1024 ? 16 : 1024 / T;
+  constexpr bool fits16 = YGeom<R, N, E, BZ16>::smem_bytes(2) <= 227 * 1024;
+  if constexpr (fits16) {
+    if ((c->tile_cfg & 1) && c->nz >= 16) return launch_y_cfg<R, N, S, 16>(c, f, nf, pr);
+  }
   return launch_y_cfg<R, N, S, 8>(c, f, nf, pr);
 }
 
@@ -1091,7 +1106,9 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->nruns = 1;
   c->ntot = c->nspec;
   c->nu_run = nullptr;
-  c->tile_cfg = 0;
+  // two-stage z ring with three CTAs per SM: the fastest variant measured for
+  // 512-point z lines in both precisions (ghost_hd_autotune re-measures)
+  c->tile_cfg = nz >= 256 ? 6 : 0;
   const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
   c->cbytes = c->nspec * 2 * rs;
   c->rbytes = c->nreal * rs;

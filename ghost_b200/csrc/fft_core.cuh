@@ -136,6 +136,23 @@ __device__ __forceinline__ void fft_stage(C (&x)[E], int t, const C *__restrict_
   }
 }
 
+// An exchange buffer in two halves used alternately: a half is written again
+// only after the barrier that follows the other half's write, by which time
+// every thread has read it, so an exchange needs one barrier instead of two.
+// slot(idx, half) gives the thread's slot; the phase lives with the caller
+// and persists across transforms (all threads of the CTA share the schedule).
+template <typename C, class Slot> struct DualBuf {
+  Slot slot;
+  int *ph;
+  __device__ __forceinline__ C &operator()(int idx) const { return slot(idx, *ph); }
+  __device__ __forceinline__ void flip() const { *ph ^= 1; }
+};
+template <class B> struct is_dual_buf { static constexpr bool value = false; };
+template <typename C, class Slot> struct is_dual_buf<DualBuf<C, Slot>> { static constexpr bool value = true; };
+template <typename C, class Slot> __device__ __forceinline__ DualBuf<C, Slot> dual_buf(Slot s, int *ph) {
+  return DualBuf<C, Slot>{s, ph};
+}
+
 // Full N-point transform of the line held in x (pattern t + T*e).
 //   buf(idx) -> C& : this thread's line slot in shared memory
 //   sync()         : barrier over every thread taking part (all lines of
@@ -153,7 +170,10 @@ __device__ __forceinline__ void line_fft(C (&x)[E], int t, const C *__restrict__
     sync();
 #pragma unroll
     for (int e = 0; e < E; ++e) x[e] = buf(t + T * e);
-    sync();
+    if constexpr (is_dual_buf<Buf>::value)
+      buf.flip();
+    else
+      sync();
     line_fft<C, N, E, S, TWS, L * R>(x, t, tw, buf, sync);
   }
 }

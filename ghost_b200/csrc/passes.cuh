@@ -47,7 +47,7 @@ template <typename R, int N, int E, int LPB, int NL> struct ZGeom {
   static constexpr int NP = N + N / 8;  // padded exchange line: idx + idx/8 spreads strided writes
   static constexpr size_t stage_elems = (size_t)NL * LPB * N;
   static constexpr size_t smem_bytes(int stages) {
-    return (stages * stage_elems + N + (size_t)LPB * NP) * sizeof(cx<R>) + 8 * (stages + 1);
+    return (stages * stage_elems + N + 2 * (size_t)LPB * NP) * sizeof(cx<R>) + 8 * (stages + 1);
   }
 };
 
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
   C *stage = reinterpret_cast<C *>(smem_raw);
   C *tw = stage + STAGES * G::stage_elems;
   C *xb = tw + N;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + LPB * NP);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + 2 * LPB * NP);
   const int tid = threadIdx.x, lq = tid / T, t = tid - lq * T;
   const int ntiles = (nlines + LPB - 1) / LPB;
   if (tid == 0) {
@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
   };
   for (int k = 0; k < STAGES - 1; ++k) issue(k);
   C *mine = xb + lq * NP;
-  auto buf = [mine](int idx) -> C & { return mine[idx + (idx >> 3)]; };
+  int ph = 0;
+  auto buf = dual_buf<C>([mine](int idx, int h) -> C & { return mine[h * (LPB * NP) + idx + (idx >> 3)]; }, &ph);
   auto sync = [] { __syncthreads(); };
   for (int k = 0;; ++k) {
     const int tile = blockIdx.x + k * gridDim.x;
@@ -637,7 +638,7 @@ template <typename R, int NX, int BZ> struct XGeom {
   // TMA boxes may overrun the M+1 rows by a few (zero-filled) rows
   static constexpr size_t stage_elems = (size_t)(M + 8) * BZ;
   static constexpr size_t smem_bytes(int stages) {
-    return (stages * stage_elems + NX + (size_t)M * BZ) * sizeof(cx<R>) + 8 * (stages + 1);
+    return (stages * stage_elems + NX + 2 * (size_t)M * BZ) * sizeof(cx<R>) + 8 * (stages + 1);
   }
 };
 
@@ -656,7 +657,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
   C *stage = reinterpret_cast<C *>(smem_raw);
   C *tw = stage + STAGES * G::stage_elems;
   C *xb = tw + NX;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + (size_t)M * BZ);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + 2 * (size_t)M * BZ);
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
   const int nzb = nz / BZ;
   const int ntiles = nzb * ny * nruns;
@@ -682,7 +683,8 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
                   (tile / nzb / ny) * nxh + q * rb, &bars[s]);
   };
   for (int L = 0; L < STAGES - 1; ++L) issue(L);
-  auto buf = [xb, l](int idx) -> C & { return xb[idx * BZ + l]; };
+  int ph = 0;
+  auto buf = dual_buf<C>([xb, l](int idx, int h) -> C & { return xb[(size_t)h * (M * BZ) + idx * BZ + l]; }, &ph);
   auto sync = [] { __syncthreads(); };
   for (int k = 0;; ++k) {
     const int tile = blockIdx.x + k * gridDim.x;
