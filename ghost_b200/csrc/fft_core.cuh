@@ -117,8 +117,25 @@ __device__ __forceinline__ void fft_stage(C (&x)[E], int t, const C *__restrict_
 #pragma unroll
     for (int m = 0; m < R; ++m) v[m] = x[q + m * NB];
     if constexpr (L > 1) {
+      if constexpr (sizeof(C) == 8 && R >= 4) {
+        // FP32: one table load, the other powers by products of depth <= 3
+        // (shared-memory loads, not FMAs, limit these kernels)
+        C w[R];
+        w[1] = tw[(k * (N / (L * R))) * TWS];
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+        if constexpr (R == 8) {
+          w[4] = cmul(w[2], w[2]);
+          w[5] = cmul(w[4], w[1]);
+          w[6] = cmul(w[4], w[2]);
+          w[7] = cmul(w[4], w[3]);
+        }
 #pragma unroll
-      for (int m = 1; m < R; ++m) v[m] = twmul<S>(v[m], tw[(k * m * (N / (L * R))) * TWS]);
+        for (int m = 1; m < R; ++m) v[m] = twmul<S>(v[m], w[m]);
+      } else {
+#pragma unroll
+        for (int m = 1; m < R; ++m) v[m] = twmul<S>(v[m], tw[(k * m * (N / (L * R))) * TWS]);
+      }
     }
     dftR<R, S>(v);
     if constexpr (LAST) {

@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
         if (kk < rows) obase[rowstride * kk] = r2c_unpack(zk, zm, tw[kk]);
         if (kk == 0 && M < rows) obase[rowstride * M] = r2c_unpack(zk, zm, mk((R)-1, (R)0));
       }
-      __syncthreads();
+      buf.flip();  // the next write goes to the other half
     }
   }
 }
