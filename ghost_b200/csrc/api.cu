@@ -347,15 +347,15 @@ template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const P
   return fail(GHOST_ERR_SIZE, "nz=%d unsupported", c->nz);
 }
 
-template <typename R, int N, int S, int BZ0>
+template <typename R, int N, int S, int BZ0, bool DUAL = false>
 int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   constexpr int E = N < 8 ? N : 8, T = N / E;
   constexpr int BZ = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
-  using G = YGeom<R, N, E, BZ>;
-  constexpr int STAGES = G::smem_bytes(3) <= 200 * 1024 ? 3 : 2;
+  using G = YGeom<R, N, E, BZ, DUAL>;
+  constexpr int STAGES = DUAL ? 2 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
   if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);
   const size_t smem = G::smem_bytes(STAGES);
-  auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S>;
+  auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S, DUAL>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ni = pr.jpos ? pr.ni : c->nxh;
   const long ntiles = (long)(c->nz / BZ) * ni * c->nruns * nf;
@@ -381,6 +381,11 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   constexpr bool fits16 = YGeom<R, N, E, BZ16>::smem_bytes(2) <= 227 * 1024;
   if constexpr (fits16) {
     if ((c->tile_cfg & 1) && c->nz >= 16) return launch_y_cfg<R, N, S, 16>(c, f, nf, pr);
+  }
+  // bit 3: two stages and a second exchange buffer (one barrier per exchange)
+  constexpr bool fits_dual = YGeom<R, N, E, 8, true>::smem_bytes(2) <= 113 * 1024;
+  if constexpr (N >= 256 && fits_dual) {
+    if (c->tile_cfg & 8) return launch_y_cfg<R, N, S, 8, true>(c, f, nf, pr);
   }
   return launch_y_cfg<R, N, S, 8>(c, f, nf, pr);
 }
@@ -1106,9 +1111,10 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->nruns = 1;
   c->ntot = c->nspec;
   c->nu_run = nullptr;
-  // two-stage z ring with three CTAs per SM: the fastest variant measured for
-  // 512-point z lines in both precisions (ghost_hd_autotune re-measures)
-  c->tile_cfg = nz >= 256 ? 6 : 0;
+  // the fastest variants measured for 512-point lines (ghost_hd_autotune
+  // re-measures): two-stage z ring with three CTAs per SM, two-stage y ring
+  // with a second exchange buffer (FP32; FP64 tiles do not fit it)
+  c->tile_cfg = (nz >= 256 ? 6 : 0) | (ny >= 256 ? 8 : 0);
   const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
   c->cbytes = c->nspec * 2 * rs;
   c->rbytes = c->nreal * rs;
@@ -1592,12 +1598,12 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
 
 // Tile variants tried by the autotuners (bit 0: y tiles 16 z-lines wide;
 // bit 1: z CTAs of 128 threads; bits 1 and 2: two-stage z ring, three CTAs
-// per SM).
-static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7};
+// per SM; bit 3: two-stage y ring with a second exchange buffer).
+static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14};
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 7) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..7", cfg);
+  if (cfg < 0 || cfg > 15) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..15", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }

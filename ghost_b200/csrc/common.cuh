@@ -114,7 +114,8 @@ struct ghost_ctx {
   int nruns;          // runs in a batched context (1 otherwise)
   size_t ntot;        // nspec * nruns
   void *nu_run;       // per-run viscosity on the device (precision of ctx), or null
-  int tile_cfg;       // tile variant (bit 0: y tile 16 wide, bit 1: z CTAs of 128 threads, bits 1+2: two-stage z ring)
+  int tile_cfg;       // tile variant (bit 0: y tile 16 wide, bit 1: z CTAs of 128 threads, bits 1+2: two-stage z ring,
+                      // bit 3: two-stage y ring with a second exchange buffer)
   int num_sms;
   // device status word written by kernels whose bounded waits ran out
   int *status;

@@ -153,6 +153,15 @@ __device__ __forceinline__ void fft_stage(C (&x)[E], int t, const C *__restrict_
   }
 }
 
+// number of shared-memory exchanges of an N-point transform, E per thread
+template <int N, int E, int L = 1> constexpr int fft_exchanges() {
+  constexpr int R = stage_radix<N, E, L>::value;
+  if constexpr (L * R == N)
+    return 0;
+  else
+    return 1 + fft_exchanges<N, E, L * R>();
+}
+
 // An exchange buffer in two halves used alternately: a half is written again
 // only after the barrier that follows the other half's write, by which time
 // every thread has read it, so an exchange needs one barrier instead of two.

@@ -453,24 +453,29 @@ template <typename R> struct ZFwdBouss {
 // can be non-zero: the inverse pass loads only those, the forward pass
 // writes only those (the rest are never read).
 // ====================================================================
-template <typename R, int N, int E, int BZ> struct YGeom {
+// DUAL: the exchanges alternate between the tile's own stage buffer and a
+// second buffer of the same size, one barrier per exchange.
+template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
   static constexpr int T = N / E;
   static constexpr int NT = BZ * T;
   static constexpr size_t stage_elems = (size_t)BZ * N;
-  static constexpr size_t smem_bytes(int stages) { return (stages * stage_elems + N) * sizeof(cx<R>) + 8 * (stages + 1); }
+  static constexpr size_t smem_bytes(int stages) {
+    return ((stages + (DUAL ? 1 : 0)) * stage_elems + N) * sizeof(cx<R>) + 8 * (stages + 1);
+  }
 };
 
-template <typename R, int N, int E, int BZ, int STAGES, int S>
+template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false>
 __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
                                                              const cx<R> *__restrict__ twg, int nz, int ni, int nf,
                                                              int nruns, int nxh, const int *__restrict__ jpos,
                                                              const int *__restrict__ jneg, int rb, PipeCtl ctl) {
   using C = cx<R>;
-  using G = YGeom<R, N, E, BZ>;
+  using G = YGeom<R, N, E, BZ, DUAL>;
   constexpr int T = G::T, NT = G::NT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C *stage = reinterpret_cast<C *>(smem_raw);
-  C *tw = stage + STAGES * G::stage_elems;
+  C *xb = stage + STAGES * G::stage_elems;  // second exchange buffer (DUAL)
+  C *tw = xb + (DUAL ? G::stage_elems : 0);
   uint64_t *bars = reinterpret_cast<uint64_t *>(tw + N);
   const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
   const int nzb = nz / BZ;
@@ -555,15 +560,25 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
       x[e] = live ? sb[jj * BZ + l] : mk((R)0, (R)0);
     }
     __syncthreads();
-    auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
-    line_fft<C, N, E, S>(x, t, tw, buf, sync);
+    if constexpr (DUAL) {
+      // half 0 is this tile's stage buffer (its data are in registers), half 1
+      // the second buffer; an even number of exchanges ends on half 1, whose
+      // barrier already follows every read of the stage buffer, which may then
+      // be refilled without a barrier at the end of the tile
+      int ph = 0;
+      auto buf = dual_buf<C>([sb, xb, l](int idx, int h) -> C & { return (h ? xb : sb)[idx * BZ + l]; }, &ph);
+      line_fft<C, N, E, S>(x, t, tw, buf, sync);
+    } else {
+      auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
+      line_fft<C, N, E, S>(x, t, tw, buf, sync);
+    }
     C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * tl.i;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int jj = t + T * e;
       if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
     }
-    __syncthreads();
+    if constexpr (!DUAL || fft_exchanges<N, E>() % 2 == 1) __syncthreads();
   }
 }
 
