@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
     const C *in0 = stage + ((size_t)(s * NL) * LPB + lq) * N;
     auto in = [in0](int f) -> const C * { return in0 + (size_t)f * LPB * N; };
     op.template body<N, E>(act ? line : 0, act, t, tw, buf, sync, in);
-    __syncthreads();
+    // the stage is refilled at the top of the next tile: the transforms'
+    // exchange barriers follow every read of it, except without exchanges
+    if constexpr (fft_exchanges<N, E>() == 0) __syncthreads();
   }
 }
 
@@ -724,7 +726,11 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __g
       C x[E];
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, BZ, l, t + T * e, M, rows, tw);
-      __syncthreads();  // the stage is consumed: it may be refilled
+      // The stage may be refilled once every thread has read it: the first
+      // exchange barrier of the transform below comes after these reads and
+      // before the next refill is issued; only a transform without exchanges
+      // needs a barrier of its own.
+      if constexpr (fft_exchanges<M, E>() == 0) __syncthreads();
       line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
       // x[e] = (r_{2m}, r_{2m+1}) at m = t + T*e
       if (f < 3) {
