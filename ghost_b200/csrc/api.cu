@@ -406,6 +406,38 @@ template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int 
 // X pass kinds
 enum XKind { X_HD = 0, X_C2R = 1, X_R2C = 2, X_BOUSS = 3 };
 
+// The fused X pass with tiles of BZ z-values (MINB CTAs per SM).
+template <typename R, int NX, int KIND, int BZ, int MINB>
+int launch_x_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int rows) {
+  constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
+  constexpr int M = NX / 2, T = M / E, NT = BZ * T;
+  typedef cx<R> C;
+  constexpr int PHYS = KIND == X_HD ? 0 : 1;
+  constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
+  using G = XGeom<R, NX, BZ>;
+  constexpr size_t cap = 220 * 1024 / MINB;  // four stages while MINB CTAs fit an SM
+  constexpr int STAGES = G::smem_bytes(4) <= cap ? 4 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
+  const size_t smem = G::smem_bytes(STAGES);
+  auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES, MINB>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Fields<R> fo{};
+  for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
+  const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+  const int nrows = rows > 0 ? rows : M + 1;
+  // tensor boxes: nbox boxes of rb kx-rows; rb keeps every box 128-byte aligned in shared memory
+  const int nbox = (nrows + 255) / 256;
+  const int align = std::max(1, 128 / (BZ * (int)sizeof(C)));
+  const int rb = ((nrows + nbox - 1) / nbox + align - 1) / align * align;
+  if (nbox * rb > M + 8 || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the tile", nbox, rb);
+  const unsigned U = sizeof(R) == 4 ? 1 : 2;
+  FieldMaps maps;
+  for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, 1, rb, &maps.m[q]));
+  const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny * c->nruns);
+  kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, (const C *)c->tw_x, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb,
+                                       c->nruns, c->nxh, pipe_ctl(c));
+  return GHOST_OK;
+}
+
 template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void *in, void *out, const void *const *ins,
                                                        void *const *outs, int rows) {
   constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
@@ -419,28 +451,7 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
   const C *tw = (const C *)c->tw_x;
   const int ts = timer_begin(c, KIND == X_C2R ? GHOST_TIMER_X_C2R : (KIND == X_R2C ? GHOST_TIMER_X_R2C : GHOST_TIMER_X_NL));
   if (KIND == X_HD || KIND == X_BOUSS) {
-    constexpr int PHYS = KIND == X_HD ? 0 : 1;
-    constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
-    using G = XGeom<R, NX, BZ>;
-    constexpr int STAGES = G::smem_bytes(4) <= 110 * 1024 ? 4 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
-    const size_t smem = G::smem_bytes(STAGES);
-    auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES>;
-    GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    Fields<R> fo{};
-    for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
-    const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
-    const int nrows = rows > 0 ? rows : M + 1;
-    // tensor boxes: nbox boxes of rb kx-rows; rb keeps every box 128-byte aligned in shared memory
-    const int nbox = (nrows + 255) / 256;
-    const int align = std::max(1, 128 / (BZ * (int)sizeof(C)));
-    const int rb = ((nrows + nbox - 1) / nbox + align - 1) / align * align;
-    if (nbox * rb > M + 8 || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the tile", nbox, rb);
-    const unsigned U = sizeof(R) == 4 ? 1 : 2;
-    FieldMaps maps;
-    for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, 1, rb, &maps.m[q]));
-    const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny * c->nruns);
-    kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, tw, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb, c->nruns,
-                                         c->nxh, pipe_ctl(c));
+    GB_CHECK((launch_x_fused<R, NX, KIND, BZ, 2>(c, ins, outs, rows)));
   } else if (KIND == X_C2R) {
     const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
     auto kern = xpass_c2r_kernel<R, NX, E, BZ>;

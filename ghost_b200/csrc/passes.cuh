@@ -661,8 +661,8 @@ template <typename R, int NX, int BZ> struct XGeom {
 
 
 
-template <typename R, int NX, int E, int BZ, int PHYS, int STAGES>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E, 2) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
+template <typename R, int NX, int E, int BZ, int PHYS, int STAGES, int MINB = 2>
+__global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
                                                                     Fields<R> out, const cx<R> *__restrict__ twg,
                                                                     int ny, int nz, R scale, int rows, int nbox,
                                                                     int rb, int nruns, int nxh, PipeCtl ctl) {
