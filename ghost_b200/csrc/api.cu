@@ -347,10 +347,19 @@ template <typename R, class Op> int launch_z(ghost_ctx *c, const Op &op, const P
   return fail(GHOST_ERR_SIZE, "nz=%d unsupported", c->nz);
 }
 
+// y tile width: BZ0 z-lines, at most 1024 threads, narrowed until a
+// two-stage ring fits in shared memory (FP64 with 1024-point lines)
+template <typename R, int N, int BZ0> constexpr int y_tile_width() {
+  constexpr int E = N < 8 ? N : 8, T = N / E;
+  int bz = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
+  while (bz > 1 && ((size_t)3 * bz * N + N) * sizeof(cx<R>) + 24 > 220 * 1024) bz /= 2;
+  return bz;
+}
+
 template <typename R, int N, int S, int BZ0, bool DUAL = false>
 int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   constexpr int E = N < 8 ? N : 8, T = N / E;
-  constexpr int BZ = BZ0 * T <= 1024 ? BZ0 : 1024 / T;
+  constexpr int BZ = y_tile_width<R, N, BZ0>();
   using G = YGeom<R, N, E, BZ, DUAL>;
   constexpr int STAGES = DUAL ? 2 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
   if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);

@@ -438,3 +438,20 @@ def test_tile_variants_are_bitwise_identical(prec):
             ref = V
         else:
             assert all(torch.equal(a, b) for a, b in zip(V, ref)), c
+
+
+@pytest.mark.parametrize("shape", [(1024, 16, 16), (16, 1024, 16), (16, 16, 1024)])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_longest_lines(shape, prec):
+    """The maximum line length (1024) along each axis, in both precisions:
+    one forced RK2 step against the oracle."""
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    v0, _ = o.random_solenoidal(31, 1.0, 5.0, 1, 1.0)
+    f, _ = o.random_solenoidal(32, 2.0, 3.0, 0, 1.0)
+    ref = o.hd_run(1, 2, 1e-3, 1e-3, v0, f)
+    cd = g.cdtype_np
+    V = [to_dev(x.astype(cd)) for x in v0]
+    F = [to_dev(x.astype(cd)) for x in f]
+    g.hd_run(1, 2, 1e-3, 1e-3, *V, *F)
+    assert rel_l2([to_host(x) for x in V], ref) <= (1e-12 if prec == "fp64" else 1e-5)
