@@ -185,6 +185,317 @@ __global__ void eddy_force_kernel(KParams<R> kp, Spec3<R> v, Spec3<R> f, Spec3w<
   }
 }
 
+
+// ---------------------------------------------------------------------
+// vcorrect (pseudo/pseudospec3D_edqnm.f90:405-1629) with heli = 0, per mode:
+// after the eddy-viscous update each resolved mode is rescaled so that its
+// energy becomes E = |v|^2 + 2 tepq(km) dt ef / eold(km) while its helicity
+// is kept, by rebuilding the amplitudes and relative phases of the
+// components.  The seven Fortran routines are the geometries where some
+// wavenumber components vanish; the locals are double precision there and
+// here.  v = (vxr,vxi,vyr,vyi,vzr,vzi) already divided by n^3.
+__device__ static double vc_sgn(double x) { return copysign(1.0, x); }
+__device__ static void vc_phase(double r, double im, double eps, double *c, double *s, double *t) {
+  const double pi = 3.14159265358979323846;
+  *c = r / (sqrt(r * r + im * im) + eps);
+  *s = im / (sqrt(r * r + im * im) + eps);
+  *t = *s > 0. ? acos(*c) : 2.0 * pi - acos(*c);
+}
+/* the common energy ratio of the first branches */
+__device__ static double vc_ratio(double E, double H, double v2, double w2, double kk2) {
+  return (E * sqrt(1. - H * H / (0.25 * kk2 * (E * E)))) / (v2 * sqrt(1. - w2 * w2 / (0.25 * kk2 * (v2 * v2))));
+}
+/* the three reconstructions of the three-component geometries */
+__device__ static void vc_rebuild3(double *v, double mx, double my, double mz, double cx, double sx, double cy, double sy,
+                       double cz, double sz, double cxy, double sxy, double czx, double szx, double cyz, double syz,
+                       int bx, int by, int bz) {
+  double tmp;
+  if (bx) {
+    v[0] = mx * cx; v[1] = mx * sx;
+    tmp = my / mx; v[2] = tmp * (cxy * v[0] - sxy * v[1]); v[3] = tmp * (sxy * v[0] + cxy * v[1]);
+    tmp = mz / mx; v[4] = tmp * (szx * v[1] + czx * v[0]); v[5] = tmp * (czx * v[1] - szx * v[0]);
+  }
+  if (by) {
+    v[2] = my * cy; v[3] = my * sy;
+    tmp = mx / my; v[0] = tmp * (cxy * v[2] + sxy * v[3]); v[1] = tmp * (-sxy * v[2] + cxy * v[3]);
+    tmp = mz / my; v[4] = tmp * (-syz * v[3] + cyz * v[2]); v[5] = tmp * (cyz * v[3] + syz * v[2]);
+  }
+  if (bz) {
+    v[4] = mz * cz; v[5] = mz * sz;
+    tmp = mx / mz; v[0] = tmp * (-szx * v[5] + czx * v[4]); v[1] = tmp * (szx * v[4] + czx * v[5]);
+    tmp = my / mz; v[2] = tmp * (cyz * v[4] + syz * v[5]); v[3] = tmp * (-syz * v[4] + cyz * v[5]);
+  }
+}
+
+__device__ static void vc_vcorr_general(double kx, double ky, double kz, double kk2, double E, double H, double v2, double w2,
+                            double cx, double sx, double cy, double sy, double cz, double sz, double txy, double tzx,
+                            double tyz, double *v);
+
+/* One mode.  zx/zy/zz: the wavenumber component is zero (index 1 in the
+ * Fortran).  kx..kz and kk2 are the GP tables; E and H as above. */
+__device__ static void vc_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double tinyf,
+                         double *v) {
+  const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
+  double cx, sx, tx, cy, sy, ty, cz, sz, tz;
+  if (!zx && !zy && !zz) {  /* vcorr_xnynzn: vz from the divergence */
+    v[4] = (-kx * v[0] - ky * v[2]) / kz;
+    v[5] = (-kx * v[1] - ky * v[3]) / kz;
+  } else if (zx && zy) {
+    v[4] = v[5] = 0.;        /* vcorr_x0y0zn */
+  } else if (zx && zz) {
+    v[2] = v[3] = 0.;        /* vcorr_x0ynz0 */
+  } else if (zy && zz) {
+    v[0] = v[1] = 0.;        /* vcorr_xny0z0 */
+  }
+  const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] + v[4] * v[4] + v[5] * v[5];
+  const double w2 = kz * (v[0] * v[3] - v[1] * v[2]) + ky * (v[4] * v[1] - v[5] * v[0]) + kx * (v[2] * v[5] - v[3] * v[4]);
+  const double H = w2;
+  const double eps = (!zx && !zy && zz) ? tinyf : 0.;  /* only vcorr_xnynz0 pads the moduli */
+  if (zx && zy) {            /* x, y only; kz != 0 */
+    vc_phase(v[0], v[1], 0., &cx, &sx, &tx);
+    vc_phase(v[2], v[3], 0., &cy, &sy, &ty);
+    const double txy = ty - tx, tmp = vc_ratio(E, H, v2, w2, kk2);
+    const double vx2 = tmp * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+    const double vy2 = tmp * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+    const double mx = sqrt(fabs(vx2)), my = sqrt(fabs(vy2));
+    double sxy = H;
+    const double dsxy = kz * mx * my;
+    if (vc_sgn(vx2) >= 0. && vc_sgn(vy2) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0.) {
+      sxy = sxy / dsxy;
+      double cxy = sqrt(1. - sxy * sxy);
+      if (cos(txy) < 0.) cxy = -cxy;
+      if (mx >= my) {
+        v[0] = mx * cx; v[1] = mx * sx;
+        const double t2 = my / mx;
+        v[2] = t2 * (cxy * v[0] - sxy * v[1]); v[3] = t2 * (sxy * v[0] + cxy * v[1]);
+      } else {
+        v[2] = my * cy; v[3] = my * sy;
+        const double t2 = mx / my;
+        v[0] = t2 * (cxy * v[2] + sxy * v[3]); v[1] = t2 * (-sxy * v[2] + cxy * v[3]);
+      }
+    }
+  } else if (zx && zz) {     /* x, z only; ky != 0 */
+    vc_phase(v[0], v[1], 0., &cx, &sx, &tx);
+    vc_phase(v[4], v[5], 0., &cz, &sz, &tz);
+    const double tzx = tx - tz, tmp = vc_ratio(E, H, v2, w2, kk2);
+    const double vx2 = tmp * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+    const double vz2 = tmp * (v[4] * v[4] + v[5] * v[5] - 0.5 * v2) + 0.5 * E;
+    const double mx = sqrt(fabs(vx2)), mz = sqrt(fabs(vz2));
+    double szx = H;
+    const double dszx = ky * mx * mz;
+    if (vc_sgn(vx2) >= 0. && vc_sgn(vz2) >= 0. && fabs(szx) <= fabs(dszx) && dszx != 0.) {
+      szx = szx / dszx;
+      double czx = sqrt(1. - szx * szx);
+      if (cos(tzx) < 0.) czx = -czx;
+      if (mx >= mz) {
+        v[0] = mx * cx; v[1] = mx * sx;
+        const double t2 = mz / mx;
+        v[4] = t2 * (szx * v[1] + czx * v[0]); v[5] = t2 * (czx * v[1] - szx * v[0]);
+      } else {
+        v[4] = mz * cz; v[5] = mz * sz;
+        const double t2 = mx / mz;
+        v[0] = t2 * (-szx * v[5] + czx * v[4]); v[1] = t2 * (szx * v[4] + czx * v[5]);
+      }
+    }
+  } else if (zy && zz) {     /* y, z only; kx != 0 */
+    vc_phase(v[2], v[3], 0., &cy, &sy, &ty);
+    vc_phase(v[4], v[5], 0., &cz, &sz, &tz);
+    const double tyz = tz - ty, tmp = vc_ratio(E, H, v2, w2, kk2);
+    const double vy2 = tmp * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+    const double vz2 = tmp * (v[4] * v[4] + v[5] * v[5] - 0.5 * v2) + 0.5 * E;
+    const double my = sqrt(fabs(vy2)), mz = sqrt(fabs(vz2));
+    double syz = H;
+    const double dsyz = kx * mz * my;
+    if (vc_sgn(vy2) >= 0. && vc_sgn(vz2) >= 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0.) {
+      syz = syz / dsyz;
+      double cyz = sqrt(1. - syz * syz);
+      if (cos(tyz) < 0.) cyz = -cyz;
+      if (my >= mz) {
+        v[2] = my * cy; v[3] = my * sy;
+        const double t2 = mz / my;
+        v[4] = t2 * (-syz * v[3] + cyz * v[2]); v[5] = t2 * (cyz * v[3] + syz * v[2]);
+      } else {
+        v[4] = mz * cz; v[5] = mz * sz;
+        const double t2 = my / mz;
+        v[2] = t2 * (cyz * v[4] + syz * v[5]); v[3] = t2 * (-syz * v[4] + cyz * v[5]);
+      }
+    }
+  } else {                   /* three components */
+    vc_phase(v[0], v[1], eps, &cx, &sx, &tx);
+    vc_phase(v[2], v[3], eps, &cy, &sy, &ty);
+    vc_phase(v[4], v[5], eps, &cz, &sz, &tz);
+    const double txy = ty - tx, tzx = tx - tz, tyz = tz - ty;
+    if (zx || zy || zz) {
+      /* one vanishing component of k (vcorr_x0ynzn, vcorr_xny0zn, vcorr_xnynz0):
+       * the mode along that axis takes its share of E, the other two split
+       * the rest in proportion to the other axes' k^2 */
+      const double tmp0 = vc_ratio(E, H, v2, w2, kk2);
+      double ma, mb, mc, tmp3, t1;
+      if (zx) {
+        const double vx2 = tmp0 * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+        t1 = vc_sgn(vx2); ma = sqrt(fabs(vx2)); tmp3 = E - vx2;
+        const double tt = 1. / (ky2 + kz2);
+        mb = sqrt(fabs(tmp3) * kz2 * tt); mc = sqrt(fabs(tmp3) * ky2 * tt);  /* my, mz */
+        const double mx = ma, my = mb, mz = mc;
+        double sxy = kz * H, szx = ky * H;
+        const double dsxy = (ky2 + kz2) * mx * my, dszx = (ky2 + kz2) * mx * mz;
+        if (t1 >= 0. && vc_sgn(tmp3) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. && fabs(szx) <= fabs(dszx) &&
+            dszx != 0.) {
+          sxy = sxy / dsxy; szx = szx / dszx;
+          double cxy = sqrt(1. - sxy * sxy), czx = sqrt(1. - szx * szx);
+          if (cos(txy) < 0.) cxy = -cxy;
+          if (cos(tzx) < 0.) czx = -czx;
+          const double syz = -szx * cxy - sxy * czx, cyz = czx * cxy - szx * sxy;
+          vc_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      } else if (zy) {
+        const double vy2 = tmp0 * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+        t1 = vc_sgn(vy2); mb = sqrt(vy2); tmp3 = E - vy2;
+        const double tt = 1. / (kx2 + kz2);
+        ma = sqrt(fabs(tmp3) * kz2 * tt); mc = sqrt(fabs(tmp3) * kx2 * tt);
+        const double mx = ma, my = mb, mz = mc;
+        double sxy = kz * H, syz = kx * H;
+        const double dsxy = (kx2 + kz2) * mx * my, dsyz = (kx2 + kz2) * my * mz;
+        if (t1 >= 0. && vc_sgn(tmp3) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. && fabs(syz) <= fabs(dsyz) &&
+            dsyz != 0.) {
+          sxy = sxy / dsxy; syz = syz / dsyz;
+          double cxy = sqrt(1. - sxy * sxy), cyz = sqrt(1. - syz * syz);
+          if (cos(txy) < 0.) cxy = -cxy;
+          if (cos(tyz) < 0.) cyz = -cyz;
+          const double szx = -sxy * cyz - syz * cxy, czx = cxy * cyz - sxy * syz;
+          vc_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      } else {
+        const double vz2 = tmp0 * ((v[4] * v[4] + v[5] * v[5]) - 0.5 * v2) + 0.5 * E;
+        t1 = vc_sgn(vz2); mc = sqrt(fabs(vz2)); tmp3 = E - vz2;
+        const double tt = 1. / (kx2 + ky2);
+        ma = sqrt(fabs(tmp3) * ky2 * tt); mb = sqrt(fabs(tmp3) * kx2 * tt);
+        const double mx = ma, my = mb, mz = mc;
+        double szx = ky * H, syz = kx * H;
+        const double dszx = (kx2 + ky2) * mx * mz, dsyz = (kx2 + ky2) * my * mz;
+        if (t1 >= 0. && vc_sgn(tmp3) >= 0. && fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) &&
+            dsyz != 0.) {
+          szx = szx / dszx; syz = syz / dsyz;
+          double czx = sqrt(1. - szx * szx), cyz = sqrt(1. - syz * syz);
+          if (cos(tzx) < 0.) czx = -czx;
+          if (cos(tyz) < 0.) cyz = -cyz;
+          const double sxy = -syz * czx - szx * cyz, cxy = cyz * czx - syz * szx;
+          vc_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      }
+    } else {
+      vc_vcorr_general(kx, ky, kz, kk2, E, H, v2, w2, cx, sx, cy, sy, cz, sz, txy, tzx, tyz, v);
+    }
+  }
+}
+
+// vcorr_xnynzn (:1377-1629): all components of k non-zero
+__device__ static void vc_vcorr_general(double kx, double ky, double kz, double kk2, double E, double H, double v2, double w2,
+                            double cx, double sx, double cy, double sy, double cz, double sz, double txy, double tzx,
+                            double tyz, double *v) {
+  const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
+  const double fx = 1. - kx2 / kk2, fy = 1. - ky2 / kk2, fz = 1. - kz2 / kk2;
+  const double tmq = vc_ratio(E, H, v2, w2, kk2);
+  double vx2 = tmq * (v[0] * v[0] + v[1] * v[1] - fx * 0.5 * v2) + fx * 0.5 * E;
+  const double vy2 = tmq * (v[2] * v[2] + v[3] * v[3] - fy * 0.5 * v2) + fy * 0.5 * E;
+  const double vz2 = tmq * (v[4] * v[4] + v[5] * v[5] - fz * 0.5 * v2) + fz * 0.5 * E;
+  double mx = sqrt(fabs(vx2)), my = sqrt(fabs(vy2)), mz = sqrt(fabs(vz2));
+  double szx = H * ky, dszx = kk2 * mx * mz, sxy = H * kz, dsxy = kk2 * my * mx, syz = H * kx, dsyz = kk2 * my * mz;
+  double czx = (ky2 * E - mx * mx * (kx2 + ky2) - mz * mz * (ky2 + kz2)), dczx = 2. * kx * kz * mx * mz;
+  double cxy = (kz2 * E - mx * mx * (kx2 + kz2) - my * my * (ky2 + kz2)), dcxy = 2. * kx * ky * mx * my;
+  double cyz = (kx2 * E - my * my * (kx2 + ky2) - mz * mz * (kx2 + kz2)), dcyz = 2. * ky * kz * my * mz;
+  if (vc_sgn(vx2) >= 0. && vc_sgn(vy2) >= 0. && vc_sgn(vz2) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. &&
+      fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0. && fabs(cxy) <= fabs(dcxy) &&
+      dcxy != 0. && fabs(cyz) <= fabs(dcyz) && dcyz != 0. && fabs(czx) <= fabs(dczx) && dczx != 0.) {
+    szx /= dszx; sxy /= dsxy; syz /= dsyz; czx /= dczx; cxy /= dcxy; cyz /= dcyz;
+    vc_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+               my > mx && my >= mz, mz > mx && mz > my);
+  } else {
+    const double hh = sqrt(1. - H * H / (0.25 * (E * E) * kk2));
+    const double hi = fx * 0.5 * E * (1. + hh), lo = fx * 0.5 * E * (1. - hh);
+    if (vx2 > hi) vx2 = hi;
+    if (vx2 < lo) vx2 = lo;
+    const double t1 = vc_sgn(vx2);
+    mx = sqrt(fabs(vx2));
+    const double a2 = 2. * ((ky2 + kz2) * (ky2 + kz2)), iq = 1. / a2;
+    double tmp4 = kx2 * ky2 * kz2 *
+                  (-((mx * mx) * (mx * mx)) * kk2 + mx * mx * (ky2 + kz2) * E -
+                   H * H * ((ky2 + kz2) * (ky2 + kz2)) / (kk2 * kk2));
+    const double t0 = vc_sgn(tmp4), delta = 4. * sqrt(fabs(tmp4)) * iq;
+    tmp4 = (-vx2 * (2. * (kx2 + kz2) * (ky2 + kz2) - 4. * kx2 * ky2) + 2. * kz2 * E * (ky2 + kz2)) * iq + delta;
+    const double t2 = vc_sgn(tmp4);
+    my = sqrt(fabs(tmp4));
+    tmp4 = (-vx2 * (2. * (kx2 + ky2) * (ky2 + kz2) - 4. * kx2 * kz2) + 2. * ky2 * E * (ky2 + kz2)) * iq - delta;
+    const double t3 = vc_sgn(tmp4);
+    mz = sqrt(fabs(tmp4));
+    szx = H * ky; dszx = kk2 * mx * mz; sxy = H * kz; dsxy = kk2 * my * mx; syz = H * kx; dsyz = kk2 * my * mz;
+    czx = (ky2 * E - mx * mx * (kx2 + ky2) - mz * mz * (ky2 + kz2)); dczx = 2. * kx * kz * mx * mz;
+    cxy = (kz2 * E - mx * mx * (kx2 + kz2) - my * my * (ky2 + kz2)); dcxy = 2. * kx * ky * mx * my;
+    cyz = (kx2 * E - my * my * (kx2 + ky2) - mz * mz * (kx2 + kz2)); dcyz = 2. * ky * kz * my * mz;
+    if (t0 >= 0. && t1 >= 0. && t2 >= 0. && t3 >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. &&
+        fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0. && fabs(czx) <= fabs(dczx) &&
+        dczx != 0. && fabs(cxy) <= fabs(dcxy) && dcxy != 0. && fabs(cyz) <= fabs(dcyz) && dcyz != 0.) {
+      szx /= dszx; sxy /= dsxy; syz /= dsyz; czx /= dczx; cxy /= dcxy; cyz /= dcyz;
+      vc_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                 my >= mx && my >= mz, mz >= mx && mz >= my);
+    }
+  }
+  (void)txy; (void)tzx; (void)tyz;
+}
+
+
+// Eden of include/edqnmhd_rkstep2.f90:8-10: (|vx|^2+|vy|^2+|vz|^2)/n^6 per mode
+template <typename R>
+__global__ void eden_kernel(Spec3<R> v, R *__restrict__ ef, size_t total, R rmp) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const cx<R> a = v.p[0][p], b = v.p[1][p], c = v.p[2][p];
+    ef[p] = (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + c.x * c.x + c.y * c.y) * rmp;
+  }
+}
+
+// vcorrect over every resolved mode but the origin: tepq and eold are the
+// shell arrays of the substep's start (1-based shells stored at k-1), ef its
+// Eden, dt the substep's dt/o
+template <typename R>
+__global__ void vcorrect_kernel(KParams<R> kp, Spec3w<R> v, const R *__restrict__ ef, const double *__restrict__ tepq,
+                                const double *__restrict__ eold, int nshell, R dt, R tinyf, R norm, size_t total) {
+  const double inorm = 1. / (double)norm;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
+    if (i == 0 && j == 0 && k == 0) continue;
+    if (kn2_of(kp, i, j, k) > kp.kmax) continue;
+    const R kk2 = kk2_of(kp, i, j, k);
+    const int km = (int)(sqrt(kk2) + (R)0.501f);
+    if (km < 1 || km > nshell) continue;
+    const cx<R> a = v.p[0][p], b = v.p[1][p], c = v.p[2][p];
+    double w[6] = {(double)a.x * inorm, (double)a.y * inorm, (double)b.x * inorm,
+                   (double)b.y * inorm, (double)c.x * inorm, (double)c.y * inorm};
+    const int zx = i == 0, zy = j == 0, zz = k == 0;
+    const double kxv = (double)kx_of(kp, i), kyv = (double)ky_of(kp, j), kzv = (double)kz_of(kp, k);
+    double u[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
+    if (!zx && !zy && !zz) {
+      u[4] = (-kxv * u[0] - kyv * u[2]) / kzv;
+      u[5] = (-kxv * u[1] - kyv * u[3]) / kzv;
+    } else if (zx && zy) {
+      u[4] = u[5] = 0.;
+    } else if (zx && zz) {
+      u[2] = u[3] = 0.;
+    } else if (zy && zz) {
+      u[0] = u[1] = 0.;
+    }
+    const double v2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2] + u[3] * u[3] + u[4] * u[4] + u[5] * u[5];
+    const double E = v2 + 2.0 * tepq[km - 1] * (double)dt * (double)ef[p] / eold[km - 1];
+    vc_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)kk2, E, (double)tinyf, w);
+    cx<R> o;
+    o.x = (R)w[0] * norm; o.y = (R)w[1] * norm; v.p[0][p] = o;
+    o.x = (R)w[2] * norm; o.y = (R)w[3] * norm; v.p[1][p] = o;
+    o.x = (R)w[4] * norm; o.y = (R)w[5] * norm; v.p[2][p] = o;
+  }
+}
+
 static int blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 // ---------------------------------------------------------------------
@@ -417,6 +728,7 @@ struct ghost_les {
   // EDQNM closure state on the device (n/2+1 shells; Ext 3(n/2+1); mu 3(n/2+1)+1)
   double *tve_dev = nullptr, *tepq_dev = nullptr, *Ek_dev = nullptr, *Ext_dev = nullptr, *mu_dev = nullptr;
   int *go_dev = nullptr;  // 1 when the fit succeeded and the quadrature runs
+  void *ef = nullptr;      // per-mode energy of the substep's start (vcorrect)
   bool edqnm_done = false;
   // fine-grid buffers for ghost_les_samples (size of the last fine grid)
   size_t fine_rbytes = 0, fine_cbytes = 0;
@@ -586,10 +898,33 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
   ghost_ctx *c = L->c;
   L->nu_cur = nu;
   bool first = true;
+  // GHOST's EDQNM step ends with vcorrect, which needs the per-mode energies
+  // of the substep's start (edqnmhd_rkstep2.f90:8-10,63)
+  const bool vcorr = L->model == GHOST_LES_EDQNM;
+  const int nb = c->nx / 2 + 1;
+  const R n3 = (R)c->nx * (R)c->ny * (R)c->nz;
+  const R rmp = (R)1 / (n3 * n3);
+  const R tinyf = (R)1e-15 < (R)0.1 / ((R)c->nmax * (R)c->nmax) ? (R)1e-15 : (R)0.1 / ((R)c->nmax * (R)c->nmax);
+  Spec3<R> vr;
+  Spec3w<R> vw;
+  for (int a = 0; a < 3; ++a) {
+    vr.p[a] = (const cx<R> *)v[a];
+    vw.p[a] = (cx<R> *)v[a];
+  }
   for (int s = 0; s < nsteps; ++s) {
     for (int o = ord; o >= 1; --o) {
       GB_CHECK(closure_force_dev<R>(L, v, f, L->force));
+      if (vcorr) {
+        eden_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(vr, (R *)L->ef, c->nspec, rmp);
+        GB_CHECK(post_launch(c));
+      }
       GB_CHECK(hd_substep_dev<R>(c, o, dt, nu, v, L->rk, L->force, o == ord ? 1 : 0, !first));
+      if (vcorr) {
+        vcorrect_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vw, (const R *)L->ef, L->tepq_dev,
+                                                                    L->Ek_dev, nb, (R)dt * ((R)1 / (R)o), tinyf, n3,
+                                                                    c->nspec);
+        GB_CHECK(post_launch(c));
+      }
       first = false;
     }
     L->t += dt;
@@ -646,6 +981,7 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   if (!st) st = les_alloc(L, sizeof(double) * 3 * nb, (void **)&L->Ext_dev);
   if (!st) st = les_alloc(L, sizeof(double) * (3 * nb + 1), (void **)&L->mu_dev);
   if (!st) st = les_alloc(L, sizeof(int), (void **)&L->go_dev);
+  if (!st) st = les_alloc(L, c->cbytes, &L->ef);
   if (st) {
     ghost_les_destroy(L);
     return st;

@@ -351,11 +351,12 @@ int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, 
  * resolves exactly the filtered modes.  All field arguments are device
  * arrays of the coarse context unless named fine.  Closures:
  *   GHOST_LES_NONE   no subgrid term;
- *   GHOST_LES_EDQNM  GHOST's EDQNM eddy viscosity, include/edqnmhd_rkstep2.f90
+ *   GHOST_LES_EDQNM  GHOST's EDQNM closure, include/edqnmhd_rkstep2.f90
  *                    with heli = 0: the kinetic spectrum of the current
- *                    velocity gives tve(k) (evedqnm: spec_fit + cusp,
- *                    pseudo/pseudospec3D_edqnm.f90:24-402) and the update
- *                    uses nu + tve(k); vcorrect is not applied;
+ *                    velocity gives tve(k) and tepq(k) (evedqnm: spec_fit +
+ *                    cusp, pseudo/pseudospec3D_edqnm.f90:24-402), the update
+ *                    uses nu + tve(k), and vcorrect (:405-1629) then sets
+ *                    every mode's energy from tepq, keeping its helicity;
  *   GHOST_LES_MLP    the learned subgrid stress: tau = mlp(inputs) gives
  *                    the force -P div tau (P the Leray projection). */
 #define GHOST_LES_NONE 0

@@ -1030,10 +1030,21 @@ void o_evedqnm(const octx *c, double kolmo, const double *Eold, double nu, doubl
 
 /* include/edqnmhd_rkstep2.f90 with heli = 0, without the closing vcorrect:
  * the update of :41-58 with (nu + tve(ki)) times the Laplacian */
-void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const double *tve, cplx *vx, cplx *vy, cplx *vz,
-                     const cplx *C1, const cplx *C2, const cplx *C3, const cplx *fx, const cplx *fy, const cplx *fz) {
+void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const double *tepq, const double *eold,
+                double dt_d);
+
+void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const double *tve, const double *tepq,
+                     const double *eold, int vcorr, cplx *vx, cplx *vy, cplx *vz, const cplx *C1, const cplx *C2,
+                     const cplx *C3, const cplx *fx, const cplx *fy, const cplx *fz) {
   size_t n = c->nspec;
   real dt = (real)dt_d, nu = (real)nu_d;
+  /* Eden of edqnmhd_rkstep2.f90:8-10, from the velocity before the update */
+  real *ef = NULL;
+  if (vcorr) {
+    const real rmp = (real)1 / ((real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx);
+    ef = (real *)malloc(sizeof(real) * n);
+    for (size_t p = 0; p < n; ++p) ef[p] = (cabs2(vx[p]) + cabs2(vy[p]) + cabs2(vz[p])) * rmp;
+  }
   cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
        *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
        *C8 = (cplx *)malloc(sizeof(cplx) * n);
@@ -1064,12 +1075,16 @@ void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const doubl
     }
   }
   free(C4); free(C5); free(C6); free(C7); free(C8);
+  if (vcorr) {
+    o_vcorrect(c, vx, vy, vz, ef, tepq, eold, (double)(dt * rmp));
+    free(ef);
+  }
 }
 
 /* nsteps RK steps of the EDQNM LES: per substep spectrumc -> evedqnm at
  * time t0 + (step index) dt -> edqnm_rkstep2 (f may be NULL) */
-void o_edqnm_run(const octx *c, int nsteps, int ord, double dt, double nu, double kolmo, double t0, cplx *vx,
-                 cplx *vy, cplx *vz, const cplx *fx, const cplx *fy, const cplx *fz) {
+void o_edqnm_run(const octx *c, int nsteps, int ord, double dt, double nu, double kolmo, double t0, int vcorr,
+                 cplx *vx, cplx *vy, cplx *vz, const cplx *fx, const cplx *fy, const cplx *fz) {
   size_t n = c->nspec;
   int nb = c->nx / 2 + 1;
   cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
@@ -1085,7 +1100,7 @@ void o_edqnm_run(const octx *c, int nsteps, int ord, double dt, double nu, doubl
     for (int o = ord; o >= 1; --o) {
       o_spectrumc(c, vx, vy, vz, 1, 0, Ek, NULL);
       o_evedqnm(c, kolmo, Ek, nu, t0 + t * dt, tepq, tve, Ext);
-      o_edqnm_rkstep2(c, o, dt, nu, tve, vx, vy, vz, C1, C2, C3, fx, fy, fz);
+      o_edqnm_rkstep2(c, o, dt, nu, tve, tepq, Ek, vcorr, vx, vy, vz, C1, C2, C3, fx, fy, fz);
     }
   }
   free(C1); free(C2); free(C3); free(zf); free(Ek); free(tepq); free(tve); free(Ext);
@@ -1111,3 +1126,308 @@ void o_les_truncate(const octx *f, const octx *c, const cplx *in, cplx *out, int
 
 /* kmax override (main3D.fpp sets kmax once; LES runs set it to kc^2) */
 void o_ctx_set_kmax(octx *c, double kmax) { c->kmax = (real)kmax; }
+
+/* ------------------------------------------------------------------ */
+/* vcorrect (pseudo/pseudospec3D_edqnm.f90:405-1629), heli = 0: after the
+ * eddy-viscous update, every resolved mode is rescaled so that its energy
+ * becomes E = |v|^2 + 2 tepq(km) dt ef / eold(km) while its helicity H
+ * (hel = 0: the mode's own w2) is kept, by rebuilding the amplitudes and
+ * relative phases of the components.  The seven routines of the Fortran
+ * handle the geometries where some wavenumber components vanish; the
+ * locals are DOUBLE PRECISION there and here.  v6 = (vxr,vxi,vyr,vyi,vzr,vzi)
+ * already divided by n^3. */
+static double o_sgn(double x) { return copysign(1.0, x); }
+static void o_phase(double r, double im, double eps, double *c, double *s, double *t) {
+  const double pi = 3.14159265358979323846;
+  *c = r / (sqrt(r * r + im * im) + eps);
+  *s = im / (sqrt(r * r + im * im) + eps);
+  *t = *s > 0. ? acos(*c) : 2.0 * pi - acos(*c);
+}
+/* the common energy ratio of the first branches */
+static double o_ratio(double E, double H, double v2, double w2, double kk2) {
+  return (E * sqrt(1. - H * H / (0.25 * kk2 * (E * E)))) / (v2 * sqrt(1. - w2 * w2 / (0.25 * kk2 * (v2 * v2))));
+}
+/* the three reconstructions of the three-component geometries */
+static void o_rebuild3(double *v, double mx, double my, double mz, double cx, double sx, double cy, double sy,
+                       double cz, double sz, double cxy, double sxy, double czx, double szx, double cyz, double syz,
+                       int bx, int by, int bz) {
+  double tmp;
+  if (bx) {
+    v[0] = mx * cx; v[1] = mx * sx;
+    tmp = my / mx; v[2] = tmp * (cxy * v[0] - sxy * v[1]); v[3] = tmp * (sxy * v[0] + cxy * v[1]);
+    tmp = mz / mx; v[4] = tmp * (szx * v[1] + czx * v[0]); v[5] = tmp * (czx * v[1] - szx * v[0]);
+  }
+  if (by) {
+    v[2] = my * cy; v[3] = my * sy;
+    tmp = mx / my; v[0] = tmp * (cxy * v[2] + sxy * v[3]); v[1] = tmp * (-sxy * v[2] + cxy * v[3]);
+    tmp = mz / my; v[4] = tmp * (-syz * v[3] + cyz * v[2]); v[5] = tmp * (cyz * v[3] + syz * v[2]);
+  }
+  if (bz) {
+    v[4] = mz * cz; v[5] = mz * sz;
+    tmp = mx / mz; v[0] = tmp * (-szx * v[5] + czx * v[4]); v[1] = tmp * (szx * v[4] + czx * v[5]);
+    tmp = my / mz; v[2] = tmp * (cyz * v[4] + syz * v[5]); v[3] = tmp * (-syz * v[4] + cyz * v[5]);
+  }
+}
+
+static void o_vcorr_general(double kx, double ky, double kz, double kk2, double E, double H, double v2, double w2,
+                            double cx, double sx, double cy, double sy, double cz, double sz, double txy, double tzx,
+                            double tyz, double *v);
+
+/* One mode.  zx/zy/zz: the wavenumber component is zero (index 1 in the
+ * Fortran).  kx..kz and kk2 are the GP tables; E and H as above. */
+static void o_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double tinyf,
+                         double *v) {
+  const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
+  double cx, sx, tx, cy, sy, ty, cz, sz, tz;
+  if (!zx && !zy && !zz) {  /* vcorr_xnynzn: vz from the divergence */
+    v[4] = (-kx * v[0] - ky * v[2]) / kz;
+    v[5] = (-kx * v[1] - ky * v[3]) / kz;
+  } else if (zx && zy) {
+    v[4] = v[5] = 0.;        /* vcorr_x0y0zn */
+  } else if (zx && zz) {
+    v[2] = v[3] = 0.;        /* vcorr_x0ynz0 */
+  } else if (zy && zz) {
+    v[0] = v[1] = 0.;        /* vcorr_xny0z0 */
+  }
+  const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] + v[4] * v[4] + v[5] * v[5];
+  const double w2 = kz * (v[0] * v[3] - v[1] * v[2]) + ky * (v[4] * v[1] - v[5] * v[0]) + kx * (v[2] * v[5] - v[3] * v[4]);
+  const double H = w2;
+  const double eps = (!zx && !zy && zz) ? tinyf : 0.;  /* only vcorr_xnynz0 pads the moduli */
+  if (zx && zy) {            /* x, y only; kz != 0 */
+    o_phase(v[0], v[1], 0., &cx, &sx, &tx);
+    o_phase(v[2], v[3], 0., &cy, &sy, &ty);
+    const double txy = ty - tx, tmp = o_ratio(E, H, v2, w2, kk2);
+    const double vx2 = tmp * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+    const double vy2 = tmp * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+    const double mx = sqrt(fabs(vx2)), my = sqrt(fabs(vy2));
+    double sxy = H;
+    const double dsxy = kz * mx * my;
+    if (o_sgn(vx2) >= 0. && o_sgn(vy2) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0.) {
+      sxy = sxy / dsxy;
+      double cxy = sqrt(1. - sxy * sxy);
+      if (cos(txy) < 0.) cxy = -cxy;
+      if (mx >= my) {
+        v[0] = mx * cx; v[1] = mx * sx;
+        const double t2 = my / mx;
+        v[2] = t2 * (cxy * v[0] - sxy * v[1]); v[3] = t2 * (sxy * v[0] + cxy * v[1]);
+      } else {
+        v[2] = my * cy; v[3] = my * sy;
+        const double t2 = mx / my;
+        v[0] = t2 * (cxy * v[2] + sxy * v[3]); v[1] = t2 * (-sxy * v[2] + cxy * v[3]);
+      }
+    }
+  } else if (zx && zz) {     /* x, z only; ky != 0 */
+    o_phase(v[0], v[1], 0., &cx, &sx, &tx);
+    o_phase(v[4], v[5], 0., &cz, &sz, &tz);
+    const double tzx = tx - tz, tmp = o_ratio(E, H, v2, w2, kk2);
+    const double vx2 = tmp * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+    const double vz2 = tmp * (v[4] * v[4] + v[5] * v[5] - 0.5 * v2) + 0.5 * E;
+    const double mx = sqrt(fabs(vx2)), mz = sqrt(fabs(vz2));
+    double szx = H;
+    const double dszx = ky * mx * mz;
+    if (o_sgn(vx2) >= 0. && o_sgn(vz2) >= 0. && fabs(szx) <= fabs(dszx) && dszx != 0.) {
+      szx = szx / dszx;
+      double czx = sqrt(1. - szx * szx);
+      if (cos(tzx) < 0.) czx = -czx;
+      if (mx >= mz) {
+        v[0] = mx * cx; v[1] = mx * sx;
+        const double t2 = mz / mx;
+        v[4] = t2 * (szx * v[1] + czx * v[0]); v[5] = t2 * (czx * v[1] - szx * v[0]);
+      } else {
+        v[4] = mz * cz; v[5] = mz * sz;
+        const double t2 = mx / mz;
+        v[0] = t2 * (-szx * v[5] + czx * v[4]); v[1] = t2 * (szx * v[4] + czx * v[5]);
+      }
+    }
+  } else if (zy && zz) {     /* y, z only; kx != 0 */
+    o_phase(v[2], v[3], 0., &cy, &sy, &ty);
+    o_phase(v[4], v[5], 0., &cz, &sz, &tz);
+    const double tyz = tz - ty, tmp = o_ratio(E, H, v2, w2, kk2);
+    const double vy2 = tmp * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+    const double vz2 = tmp * (v[4] * v[4] + v[5] * v[5] - 0.5 * v2) + 0.5 * E;
+    const double my = sqrt(fabs(vy2)), mz = sqrt(fabs(vz2));
+    double syz = H;
+    const double dsyz = kx * mz * my;
+    if (o_sgn(vy2) >= 0. && o_sgn(vz2) >= 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0.) {
+      syz = syz / dsyz;
+      double cyz = sqrt(1. - syz * syz);
+      if (cos(tyz) < 0.) cyz = -cyz;
+      if (my >= mz) {
+        v[2] = my * cy; v[3] = my * sy;
+        const double t2 = mz / my;
+        v[4] = t2 * (-syz * v[3] + cyz * v[2]); v[5] = t2 * (cyz * v[3] + syz * v[2]);
+      } else {
+        v[4] = mz * cz; v[5] = mz * sz;
+        const double t2 = my / mz;
+        v[2] = t2 * (cyz * v[4] + syz * v[5]); v[3] = t2 * (-syz * v[4] + cyz * v[5]);
+      }
+    }
+  } else {                   /* three components */
+    o_phase(v[0], v[1], eps, &cx, &sx, &tx);
+    o_phase(v[2], v[3], eps, &cy, &sy, &ty);
+    o_phase(v[4], v[5], eps, &cz, &sz, &tz);
+    const double txy = ty - tx, tzx = tx - tz, tyz = tz - ty;
+    if (zx || zy || zz) {
+      /* one vanishing component of k (vcorr_x0ynzn, vcorr_xny0zn, vcorr_xnynz0):
+       * the mode along that axis takes its share of E, the other two split
+       * the rest in proportion to the other axes' k^2 */
+      const double tmp0 = o_ratio(E, H, v2, w2, kk2);
+      double ma, mb, mc, tmp3, t1;
+      if (zx) {
+        const double vx2 = tmp0 * (v[0] * v[0] + v[1] * v[1] - 0.5 * v2) + 0.5 * E;
+        t1 = o_sgn(vx2); ma = sqrt(fabs(vx2)); tmp3 = E - vx2;
+        const double tt = 1. / (ky2 + kz2);
+        mb = sqrt(fabs(tmp3) * kz2 * tt); mc = sqrt(fabs(tmp3) * ky2 * tt);  /* my, mz */
+        const double mx = ma, my = mb, mz = mc;
+        double sxy = kz * H, szx = ky * H;
+        const double dsxy = (ky2 + kz2) * mx * my, dszx = (ky2 + kz2) * mx * mz;
+        if (t1 >= 0. && o_sgn(tmp3) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. && fabs(szx) <= fabs(dszx) &&
+            dszx != 0.) {
+          sxy = sxy / dsxy; szx = szx / dszx;
+          double cxy = sqrt(1. - sxy * sxy), czx = sqrt(1. - szx * szx);
+          if (cos(txy) < 0.) cxy = -cxy;
+          if (cos(tzx) < 0.) czx = -czx;
+          const double syz = -szx * cxy - sxy * czx, cyz = czx * cxy - szx * sxy;
+          o_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      } else if (zy) {
+        const double vy2 = tmp0 * (v[2] * v[2] + v[3] * v[3] - 0.5 * v2) + 0.5 * E;
+        t1 = o_sgn(vy2); mb = sqrt(vy2); tmp3 = E - vy2;
+        const double tt = 1. / (kx2 + kz2);
+        ma = sqrt(fabs(tmp3) * kz2 * tt); mc = sqrt(fabs(tmp3) * kx2 * tt);
+        const double mx = ma, my = mb, mz = mc;
+        double sxy = kz * H, syz = kx * H;
+        const double dsxy = (kx2 + kz2) * mx * my, dsyz = (kx2 + kz2) * my * mz;
+        if (t1 >= 0. && o_sgn(tmp3) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. && fabs(syz) <= fabs(dsyz) &&
+            dsyz != 0.) {
+          sxy = sxy / dsxy; syz = syz / dsyz;
+          double cxy = sqrt(1. - sxy * sxy), cyz = sqrt(1. - syz * syz);
+          if (cos(txy) < 0.) cxy = -cxy;
+          if (cos(tyz) < 0.) cyz = -cyz;
+          const double szx = -sxy * cyz - syz * cxy, czx = cxy * cyz - sxy * syz;
+          o_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      } else {
+        const double vz2 = tmp0 * ((v[4] * v[4] + v[5] * v[5]) - 0.5 * v2) + 0.5 * E;
+        t1 = o_sgn(vz2); mc = sqrt(fabs(vz2)); tmp3 = E - vz2;
+        const double tt = 1. / (kx2 + ky2);
+        ma = sqrt(fabs(tmp3) * ky2 * tt); mb = sqrt(fabs(tmp3) * kx2 * tt);
+        const double mx = ma, my = mb, mz = mc;
+        double szx = ky * H, syz = kx * H;
+        const double dszx = (kx2 + ky2) * mx * mz, dsyz = (kx2 + ky2) * my * mz;
+        if (t1 >= 0. && o_sgn(tmp3) >= 0. && fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) &&
+            dsyz != 0.) {
+          szx = szx / dszx; syz = syz / dsyz;
+          double czx = sqrt(1. - szx * szx), cyz = sqrt(1. - syz * syz);
+          if (cos(tzx) < 0.) czx = -czx;
+          if (cos(tyz) < 0.) cyz = -cyz;
+          const double sxy = -syz * czx - szx * cyz, cxy = cyz * czx - syz * szx;
+          o_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                     my >= mx && my >= mz, mz >= mx && mz >= my);
+        }
+      }
+    } else {
+      o_vcorr_general(kx, ky, kz, kk2, E, H, v2, w2, cx, sx, cy, sy, cz, sz, txy, tzx, tyz, v);
+    }
+  }
+}
+
+/* vcorr_xnynzn (:1377-1629): all components of k non-zero */
+static void o_vcorr_general(double kx, double ky, double kz, double kk2, double E, double H, double v2, double w2,
+                            double cx, double sx, double cy, double sy, double cz, double sz, double txy, double tzx,
+                            double tyz, double *v) {
+  const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
+  const double fx = 1. - kx2 / kk2, fy = 1. - ky2 / kk2, fz = 1. - kz2 / kk2;
+  const double tmq = o_ratio(E, H, v2, w2, kk2);
+  double vx2 = tmq * (v[0] * v[0] + v[1] * v[1] - fx * 0.5 * v2) + fx * 0.5 * E;
+  const double vy2 = tmq * (v[2] * v[2] + v[3] * v[3] - fy * 0.5 * v2) + fy * 0.5 * E;
+  const double vz2 = tmq * (v[4] * v[4] + v[5] * v[5] - fz * 0.5 * v2) + fz * 0.5 * E;
+  double mx = sqrt(fabs(vx2)), my = sqrt(fabs(vy2)), mz = sqrt(fabs(vz2));
+  double szx = H * ky, dszx = kk2 * mx * mz, sxy = H * kz, dsxy = kk2 * my * mx, syz = H * kx, dsyz = kk2 * my * mz;
+  double czx = (ky2 * E - mx * mx * (kx2 + ky2) - mz * mz * (ky2 + kz2)), dczx = 2. * kx * kz * mx * mz;
+  double cxy = (kz2 * E - mx * mx * (kx2 + kz2) - my * my * (ky2 + kz2)), dcxy = 2. * kx * ky * mx * my;
+  double cyz = (kx2 * E - my * my * (kx2 + ky2) - mz * mz * (kx2 + kz2)), dcyz = 2. * ky * kz * my * mz;
+  if (o_sgn(vx2) >= 0. && o_sgn(vy2) >= 0. && o_sgn(vz2) >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. &&
+      fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0. && fabs(cxy) <= fabs(dcxy) &&
+      dcxy != 0. && fabs(cyz) <= fabs(dcyz) && dcyz != 0. && fabs(czx) <= fabs(dczx) && dczx != 0.) {
+    szx /= dszx; sxy /= dsxy; syz /= dsyz; czx /= dczx; cxy /= dcxy; cyz /= dcyz;
+    o_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+               my > mx && my >= mz, mz > mx && mz > my);
+  } else {
+    const double hh = sqrt(1. - H * H / (0.25 * (E * E) * kk2));
+    const double hi = fx * 0.5 * E * (1. + hh), lo = fx * 0.5 * E * (1. - hh);
+    if (vx2 > hi) vx2 = hi;
+    if (vx2 < lo) vx2 = lo;
+    const double t1 = o_sgn(vx2);
+    mx = sqrt(fabs(vx2));
+    const double a2 = 2. * ((ky2 + kz2) * (ky2 + kz2)), iq = 1. / a2;
+    double tmp4 = kx2 * ky2 * kz2 *
+                  (-((mx * mx) * (mx * mx)) * kk2 + mx * mx * (ky2 + kz2) * E -
+                   H * H * ((ky2 + kz2) * (ky2 + kz2)) / (kk2 * kk2));
+    const double t0 = o_sgn(tmp4), delta = 4. * sqrt(fabs(tmp4)) * iq;
+    tmp4 = (-vx2 * (2. * (kx2 + kz2) * (ky2 + kz2) - 4. * kx2 * ky2) + 2. * kz2 * E * (ky2 + kz2)) * iq + delta;
+    const double t2 = o_sgn(tmp4);
+    my = sqrt(fabs(tmp4));
+    tmp4 = (-vx2 * (2. * (kx2 + ky2) * (ky2 + kz2) - 4. * kx2 * kz2) + 2. * ky2 * E * (ky2 + kz2)) * iq - delta;
+    const double t3 = o_sgn(tmp4);
+    mz = sqrt(fabs(tmp4));
+    szx = H * ky; dszx = kk2 * mx * mz; sxy = H * kz; dsxy = kk2 * my * mx; syz = H * kx; dsyz = kk2 * my * mz;
+    czx = (ky2 * E - mx * mx * (kx2 + ky2) - mz * mz * (ky2 + kz2)); dczx = 2. * kx * kz * mx * mz;
+    cxy = (kz2 * E - mx * mx * (kx2 + kz2) - my * my * (ky2 + kz2)); dcxy = 2. * kx * ky * mx * my;
+    cyz = (kx2 * E - my * my * (kx2 + ky2) - mz * mz * (kx2 + kz2)); dcyz = 2. * ky * kz * my * mz;
+    if (t0 >= 0. && t1 >= 0. && t2 >= 0. && t3 >= 0. && fabs(sxy) <= fabs(dsxy) && dsxy != 0. &&
+        fabs(szx) <= fabs(dszx) && dszx != 0. && fabs(syz) <= fabs(dsyz) && dsyz != 0. && fabs(czx) <= fabs(dczx) &&
+        dczx != 0. && fabs(cxy) <= fabs(dcxy) && dcxy != 0. && fabs(cyz) <= fabs(dcyz) && dcyz != 0.) {
+      szx /= dszx; sxy /= dsxy; syz /= dsyz; czx /= dczx; cxy /= dcxy; cyz /= dcyz;
+      o_rebuild3(v, mx, my, mz, cx, sx, cy, sy, cz, sz, cxy, sxy, czx, szx, cyz, syz, mx >= my && mx >= mz,
+                 my >= mx && my >= mz, mz >= mx && mz >= my);
+    }
+  }
+  (void)txy; (void)tzx; (void)tyz;
+}
+
+/* vcorrect over every resolved mode but the origin; ef: Eden of the
+ * substep's start, (|vx|^2+|vy|^2+|vz|^2)/n^6 per mode (edqnmhd_rkstep2.f90:
+ * 8-10); tepq, eold: 0-based copies of the shell arrays; dt: dt/o. */
+void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const double *tepq, const double *eold,
+                double dt_d) {
+  const real dt = (real)dt_d;
+  const real norm = (real)c->nx * (real)c->nx * (real)c->nx;
+  const double inorm = 1. / (double)norm;
+  const real tinyf = (real)1e-15 < (real)0.1 / ((real)c->nmax * (real)c->nmax) ? (real)1e-15
+                                                                             : (real)0.1 / ((real)c->nmax * (real)c->nmax);
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        if (i == 0 && j == 0 && k == 0) continue;
+        const size_t p = SIDX(c, k, j, i);
+        if (c->kn2[p] > c->kmax) continue;
+        const int km = (int)((real)sqrt(c->kk2[p]) + (real)0.501f);
+        double v[6] = {(double)vx[p].re * inorm, (double)vx[p].im * inorm, (double)vy[p].re * inorm,
+                       (double)vy[p].im * inorm, (double)vz[p].re * inorm, (double)vz[p].im * inorm};
+        /* E needs v2 of the geometry's components: the mode routine sets them
+         * first, so E is formed there from the corrected v2 */
+        double vv[6];
+        memcpy(vv, v, sizeof vv);
+        const int zx = i == 0, zy = j == 0, zz = k == 0;
+        const double kxv = c->kx[i], kyv = c->ky[j], kzv = c->kz[k];
+        if (!zx && !zy && !zz) {
+          vv[4] = (-kxv * vv[0] - kyv * vv[2]) / kzv;
+          vv[5] = (-kxv * vv[1] - kyv * vv[3]) / kzv;
+        } else if (zx && zy) {
+          vv[4] = vv[5] = 0.;
+        } else if (zx && zz) {
+          vv[2] = vv[3] = 0.;
+        } else if (zy && zz) {
+          vv[0] = vv[1] = 0.;
+        }
+        const double v2 = vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2] + vv[3] * vv[3] + vv[4] * vv[4] + vv[5] * vv[5];
+        const double E = v2 + 2.0 * tepq[km - 1] * (double)dt * (double)ef[p] / eold[km - 1];
+        o_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)c->kk2[p], E, (double)tinyf, v);
+        vx[p].re = (real)v[0] * norm; vx[p].im = (real)v[1] * norm;
+        vy[p].re = (real)v[2] * norm; vy[p].im = (real)v[3] * norm;
+        vz[p].re = (real)v[4] * norm; vz[p].im = (real)v[5] * norm;
+      }
+}

@@ -76,8 +76,9 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_bouss_run": (None, [P, I, I, D, D, D, D, D, D] + [P] * 8),
         "o_sharp": (None, [P, P, P, D]),
         "o_evedqnm": (None, [P, D, P, D, D, P, P, P]),
-        "o_edqnm_rkstep2": (None, [P, I, D, D, P] + [P] * 9),
-        "o_edqnm_run": (None, [P, I, I, D, D, D, D] + [P] * 6),
+        "o_edqnm_rkstep2": (None, [P, I, D, D, P, P, P, I] + [P] * 9),
+        "o_edqnm_run": (None, [P, I, I, D, D, D, D, I] + [P] * 6),
+        "o_vcorrect": (None, [P, P, P, P, P, P, P, D]),
         "o_les_truncate": (None, [P, P, P, P, I]),
         "o_ctx_set_kmax": (None, [P, D]),
     }
@@ -300,11 +301,20 @@ class Oracle:
         self.lib.o_evedqnm(self.h, kolmo, _ptr(E), nu, time, _ptr(tepq), _ptr(tve), _ptr(Ext))
         return tepq, tve, Ext
 
-    def edqnm_run(self, nsteps, ord, dt, nu, v, f=None, kolmo=1.4, t0=0.0):
+    def edqnm_run(self, nsteps, ord, dt, nu, v, f=None, kolmo=1.4, t0=0.0, vcorrect=True):
         v = [self._c(x).copy() for x in v]
         fk = None if f is None else [self._c(x) for x in f]
-        self.lib.o_edqnm_run(self.h, nsteps, ord, dt, nu, kolmo, t0, *[_ptr(x) for x in v],
+        self.lib.o_edqnm_run(self.h, nsteps, ord, dt, nu, kolmo, t0, int(vcorrect), *[_ptr(x) for x in v],
                              *([None] * 3 if fk is None else [_ptr(x) for x in fk]))
+        return v
+
+    def vcorrect(self, v, ef, tepq, eold, dt):
+        """vcorrect (heli = 0) of v with the per-mode energies ef of the step's start."""
+        v = [self._c(x).copy() for x in v]
+        ef = np.ascontiguousarray(ef, dtype=self.rdt)
+        t = np.ascontiguousarray(tepq, dtype=np.float64)
+        e = np.ascontiguousarray(eold, dtype=np.float64)
+        self.lib.o_vcorrect(self.h, *[_ptr(x) for x in v], _ptr(ef), _ptr(t), _ptr(e), dt)
         return v
 
     def les_truncate(self, coarse: "Oracle", a, kc: int):

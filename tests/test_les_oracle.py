@@ -82,3 +82,30 @@ def test_tau_force_is_solenoidal_and_matches_divergence():
     iso[:, :3] = rng.standard_normal((16 ** 3, 1))
     F0 = LO.tau_force(co, iso)
     assert max(np.max(np.abs(x)) for x in F0) < 1e-10
+
+
+def test_vcorrect_sets_mode_energy_and_keeps_helicity():
+    """vcorrect (heli = 0) gives every correctable mode the energy
+    E = |v|^2 + 2 tepq dt ef / eold, keeps the helicity of the field and
+    leaves it solenoidal."""
+    o = Oracle(32)
+    o.set_kmax(100.0)
+    v, _ = o.random_solenoidal(8, 1.0, 10.0, 0, 1.0)
+    _, _, _, kn2, kk2 = o.tables()
+    s = np.where(kk2 > 0, kk2, 1.0) ** (-11.0 / 12.0)
+    v = [x * s for x in v]
+    Ek, _ = o.spectrumc(*v, 1, 0)
+    tepq, _, _ = o.evedqnm(Ek, 1e-3, 2.0)
+    n6 = float(32 ** 6)
+    ef = (np.abs(v[0]) ** 2 + np.abs(v[1]) ** 2 + np.abs(v[2]) ** 2) / n6
+    dt = 0.01
+    vc = o.vcorrect(v, ef, tepq, Ek, dt)
+    e_new = (np.abs(vc[0]) ** 2 + np.abs(vc[1]) ** 2 + np.abs(vc[2]) ** 2) / n6
+    km = np.clip((np.sqrt(kk2) + np.float32(0.501)).astype(int) - 1, 0, len(Ek) - 1)
+    mask = (kn2 <= o.kmax) & (kk2 > 0)
+    target = ef + 2 * tepq[km] * dt * ef / Ek[km]
+    hit = np.abs(e_new[mask] / target[mask] - 1) < 1e-9
+    assert hit.mean() > 0.99
+    assert abs(o.helicity(*vc) - o.helicity(*v)) < 1e-12 * abs(o.helicity(*v))
+    assert o.divergence(*vc) < 1e-28
+    assert not any(np.isnan(x).any() for x in vc)
