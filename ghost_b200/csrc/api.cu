@@ -599,10 +599,29 @@ template <typename R> int c2r_dev(ghost_ctx *c, const void *in, void *out) {
   return launch_x<R, X_C2R>(c, w[0], out);
 }
 
-// The nine gradients d v_a / d x_b of a spectral velocity as real fields
-// (n^3 times their values, GHOST's unnormalised c2r), in three passes over
-// all nine instead of nine separate derivk3 + c2r: real[3a+b] via spec[3a+b].
-template <typename R> int grad9_dev(ghost_ctx *c, const void *const v[3], void *const spec[9], void *const real[9]) {
+// The LES closure's input rows from a spectral velocity: the nine gradients
+// through z and y passes over all nine, then one x pass that writes
+// x[q][3a+b] = (d v_a / d x_b) * gs and x[q][9] = delta directly.
+template <typename R, int NX>
+int grad9_features_n(ghost_ctx *c, void *const spec[9], float *x, float gs, float delta) {
+  constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
+  constexpr int M = NX / 2, T = M / E;
+  constexpr int BZ = xBZ<R>() * T <= 256 ? xBZ<R>() : (256 / T > 0 ? 256 / T : 1);
+  typedef cx<R> C;
+  const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
+  auto kern = xpass_c2r_features_kernel<R, NX, E, BZ>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Fields<R> in{};
+  for (int q = 0; q < 9; ++q) in.p[q] = (C *)spec[q];
+  const int ts = timer_begin(c, GHOST_TIMER_X_C2R);
+  kern<<<dim3(c->nz / BZ, c->ny), BZ * T, smem, c->stream>>>(in, x, (const C *)c->tw_x, c->ny, c->nz,
+                                                              (R)(1.0 / (double)c->nreal), gs, delta);
+  timer_end(c, ts);
+  return post_launch(c);
+}
+
+template <typename R>
+int grad9_features_dev(ghost_ctx *c, const void *const v[3], void *const spec[9], float *x, float gs, float delta) {
   ZGrad<R> zg{};
   for (int a = 0; a < 3; ++a) zg.v.p[a] = (const cx<R> *)v[a];
   for (int q = 0; q < 9; ++q) zg.w.p[q] = (cx<R> *)spec[q];
@@ -611,8 +630,16 @@ template <typename R> int grad9_dev(ghost_ctx *c, const void *const v[3], void *
   Fields<R> fy{};
   for (int q = 0; q < 9; ++q) fy.p[q] = (cx<R> *)spec[q];
   GB_CHECK((launch_y<R, +1>(c, fy, 9)));
-  for (int q = 0; q < 9; ++q) GB_CHECK((launch_x<R, X_C2R>(c, spec[q], real[q])));
-  return GHOST_OK;
+  switch (c->nx) {
+    case 16: return grad9_features_n<R, 16>(c, spec, x, gs, delta);
+    case 32: return grad9_features_n<R, 32>(c, spec, x, gs, delta);
+    case 64: return grad9_features_n<R, 64>(c, spec, x, gs, delta);
+    case 128: return grad9_features_n<R, 128>(c, spec, x, gs, delta);
+    case 256: return grad9_features_n<R, 256>(c, spec, x, gs, delta);
+    case 512: return grad9_features_n<R, 512>(c, spec, x, gs, delta);
+    case 1024: return grad9_features_n<R, 1024>(c, spec, x, gs, delta);
+  }
+  return fail(GHOST_ERR_SIZE, "nx=%d unsupported", c->nx);
 }
 
 // Six real fields to spectra at once (the stresses of the LES closure):
@@ -1079,9 +1106,8 @@ int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out
 #define GB_INST(R)                                                                                             \
   template int r2c_dev<R>(ghost_ctx *, const void *, void *);                                                  \
   template int c2r_dev<R>(ghost_ctx *, const void *, void *);                                                  \
-  template int derivk3_impl<R>(ghost_ctx *, const void *, void *, int);                                        \
-  template int grad9_dev<R>(ghost_ctx *, const void *const[3], void *const[9], void *const[9]);                \
   template int r2c6_dev<R>(ghost_ctx *, const void *const[6], void *const[6]);                                 \
+  template int grad9_features_dev<R>(ghost_ctx *, const void *const[3], void *const[9], float *, float, float);     \
   template int hd_substep_dev<R>(ghost_ctx *, int, double, double, void *const[3], void *const[3],             \
                                  const void *const[3], int, bool);                                             \
   template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);          \

@@ -20,10 +20,10 @@ template <typename R> const KParams<R> &kparams(const ghost_ctx *c);
 // unnormalised 3D transforms on device arrays (c2r keeps its input)
 template <typename R> int r2c_dev(ghost_ctx *c, const void *in, void *out);
 template <typename R> int c2r_dev(ghost_ctx *c, const void *in, void *out);
-template <typename R> int derivk3_impl(ghost_ctx *c, const void *a, void *b, int dir);
-// the nine gradients i k_b v_a of a spectral velocity as real fields (n^3
-// times their values), through spectral work fields spec[9]
-template <typename R> int grad9_dev(ghost_ctx *c, const void *const v[3], void *const spec[9], void *const real[9]);
+// the LES closure's input rows x[q][10] (gradients times gs, delta) of a
+// spectral velocity, through spectral work fields spec[9]
+template <typename R>
+int grad9_features_dev(ghost_ctx *c, const void *const v[3], void *const spec[9], float *x, float gs, float delta);
 // six real fields to spectra (x per field, one y and one z pass for all six)
 template <typename R> int r2c6_dev(ghost_ctx *c, const void *const in[6], void *const out[6]);
 // one fused HD substep (include/hd_rkstep2.f90; hd_rkstep1 folded in with copy)

@@ -55,21 +55,6 @@ __global__ void product_kernel(const R *__restrict__ a, const R *__restrict__ b,
     p[q] = (a[q] * s) * (b[q] * s);
 }
 
-// Inputs of the closure at every grid point q: x[q][3a+b] = du_a/dx_b
-// (g[3a+b] holds n^3 times it) times gs, x[q][9] = delta.
-template <typename R> struct GradFields {
-  const R *g[9];
-};
-template <typename R>
-__global__ void features_kernel(GradFields<R> gf, float *__restrict__ x, size_t n, R inv_n3, float gs, float delta) {
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    float *row = x + q * GHOST_MLP_NIN;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) row[c] = (float)(gf.g[c][q] * inv_n3) * gs;
-    row[9] = delta;
-  }
-}
-
 // Targets: tau[q][m] = filt(u_a u_b) - ubar_a ubar_b for the pairs m =
 // xx, yy, zz, xy, xz, yz; P[m] holds n^3 filt(u_a u_b), U[a] n^3 ubar_a.
 template <typename R> struct TauFields {
@@ -767,19 +752,8 @@ template <typename R> static int truncate_dev(ghost_les *L, ghost_ctx *f, const 
   return post_launch(c);
 }
 
-// the nine n^3-scaled velocity gradients of (vx, vy, vz) into L->real
-template <typename R> static int gradients_dev(ghost_les *L, const void *const v[3]) {
-  return grad9_dev<R>(L->c, v, L->spec, L->real);
-}
-
 template <typename R> static int features_dev(ghost_les *L, const void *const v[3], float gs, float delta) {
-  ghost_ctx *c = L->c;
-  GB_CHECK(gradients_dev<R>(L, v));
-  GradFields<R> gf;
-  for (int q = 0; q < 9; ++q) gf.g[q] = (const R *)L->real[q];
-  features_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(gf, L->x, c->nreal, (R)(1.0 / (double)c->nreal), gs,
-                                                              delta);
-  return post_launch(c);
+  return grad9_features_dev<R>(L->c, v, L->spec, L->x, gs, delta);
 }
 
 template <typename R>
@@ -789,12 +763,7 @@ static int samples_dev(ghost_les *L, ghost_ctx *f, const void *const v[3], float
   // filtered velocity on the coarse grid, its gradients and real values
   void *ub[3] = {L->spec[9], L->spec[10], L->spec[11]};
   for (int a = 0; a < 3; ++a) GB_CHECK(truncate_dev<R>(L, f, v[a], ub[a]));
-  GB_CHECK(gradients_dev<R>(L, ub));
-  GradFields<R> gf;
-  for (int q = 0; q < 9; ++q) gf.g[q] = (const R *)L->real[q];
-  features_kernel<R><<<blocks(c->nreal), 256, 0, c->stream>>>(gf, x, c->nreal, (R)(1.0 / (double)c->nreal), 1.f,
-                                                              delta);
-  GB_CHECK(post_launch(c));
+  GB_CHECK(grad9_features_dev<R>(c, ub, L->spec, x, 1.f, delta));
   // real ubar (n^3-scaled) into real[0..2]; the gradient fields are done
   for (int a = 0; a < 3; ++a) GB_CHECK(c2r_dev<R>(c, ub[a], L->real[a]));
   // fine velocity (N^3-scaled) and the six products, filtered to the coarse grid

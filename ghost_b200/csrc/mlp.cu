@@ -164,30 +164,30 @@ constexpr int TMEM_COLS_F = 128;
 // Loads the FP32 master weights as BF16 operands (with the transposed
 // copies of the backward products when BWD).
 template <class S, bool BWD> __device__ void load_weights(S &s, const float *__restrict__ P) {
-  for (int q = threadIdx.x; q < NH * KIN; q += THREADS) {
+  for (int q = threadIdx.x; q < NH * KIN; q += blockDim.x) {
     const int n = q / KIN, k = q % KIN;
     s.w1[core_off(n, k, KIN)] = __float2bfloat16_rn(k < NIN ? P[OW1 + n * NIN + k] : 0.f);
   }
-  for (int q = threadIdx.x; q < NH * NH; q += THREADS) {
+  for (int q = threadIdx.x; q < NH * NH; q += blockDim.x) {
     const int n = q / NH, k = q % NH;
     s.w2[core_off(n, k, NH)] = __float2bfloat16_rn(P[OW2 + n * NH + k]);
     if constexpr (BWD) s.w2t[core_off(n, k, NH)] = __float2bfloat16_rn(P[OW2 + k * NH + n]);
   }
-  for (int q = threadIdx.x; q < KOUT * NH; q += THREADS) {
+  for (int q = threadIdx.x; q < KOUT * NH; q += blockDim.x) {
     const int n = q / NH, k = q % NH;  // w3: N = outputs (padded), K = hidden
     s.w3[core_off(n, k, NH)] = __float2bfloat16_rn(n < NOUT ? P[OW3 + n * NH + k] : 0.f);
   }
   if constexpr (BWD) {
-    for (int q = threadIdx.x; q < NH * KOUT; q += THREADS) {
+    for (int q = threadIdx.x; q < NH * KOUT; q += blockDim.x) {
       const int n = q / KOUT, k = q % KOUT;  // w3t: N = hidden, K = outputs
       s.w3t[core_off(n, k, KOUT)] = __float2bfloat16_rn(k < NOUT ? P[OW3 + k * NH + n] : 0.f);
     }
   }
-  for (int q = threadIdx.x; q < NH; q += THREADS) {
+  for (int q = threadIdx.x; q < NH; q += blockDim.x) {
     s.b1[q] = P[OB1 + q];
     s.b2[q] = P[OB2 + q];
   }
-  for (int q = threadIdx.x; q < KOUT; q += THREADS) s.b3[q] = q < NOUT ? P[OB3 + q] : 0.f;
+  for (int q = threadIdx.x; q < KOUT; q += blockDim.x) s.b3[q] = q < NOUT ? P[OB3 + q] : 0.f;
 }
 
 // One MMA chain D (tmem col `dcol`) = A (rows x K) * B^T (N x K), waited for
@@ -423,6 +423,124 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(s.tmem), "r"(COLS) : "memory");
 }
 
+// Inference on two tiles per CTA (256 threads; warps 0-3 take tile slot 0,
+// warps 4-7 slot 1): one barrier and one MMA completion per layer serve both
+// tiles.  Slot u accumulates in tensor-memory columns u*128 + (0: D1 and D3,
+// 64: D2); the lanes are the rows, so both slots use lanes 0-127.
+struct SmemF2 {
+  __nv_bfloat16 w1[NH * KIN];
+  __nv_bfloat16 w2[NH * NH];
+  __nv_bfloat16 w3[KOUT * NH];
+  __nv_bfloat16 x[2][ROWS * KIN];
+  __nv_bfloat16 h1[2][ROWS * NH];
+  __nv_bfloat16 h2[2][ROWS * NH];
+  float b1[NH], b2[NH], b3[KOUT];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__device__ bool run_mma2(SmemF2 &s, uint32_t dcol, const __nv_bfloat16 *A0, const __nv_bfloat16 *A1,
+                         const __nv_bfloat16 *B, int K, int N, uint32_t &phase, uint32_t cap, int *status) {
+  gb::fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = instr_desc(ROWS, N);
+    for (int u = 0; u < 2; ++u) {
+      const __nv_bfloat16 *A = u ? A1 : A0;
+      for (int ks = 0; ks < K / 16; ++ks)
+        mma_bf16(s.tmem + u * 128 + dcol, smem_desc(A + ks * 128, K), smem_desc(B + ks * 128, K), idesc, ks > 0);
+    }
+    mma_commit(&s.bar);
+  }
+  bool ok = gb::mbar_wait(&s.bar, phase, cap);
+  ok = __syncthreads_and(ok);
+  if (!ok) {
+    if (threadIdx.x == 0) gb::record_timeout(status);
+    gb::mbar_wait(&s.bar, phase, gb::kDrainPolls);
+    __syncthreads();
+  }
+  phase ^= 1u;
+  tc_fence_after();
+  return ok;
+}
+
+template <int N> __device__ void read_row2(const SmemF2 &s, uint32_t dcol, float (&v)[N]) {
+  const uint32_t u = threadIdx.x >> 7;
+  const uint32_t lane_base = (uint32_t)((threadIdx.x & 127) & ~31) << 16;
+#pragma unroll
+  for (int c = 0; c < N; c += 16) {
+    float t[16];
+    tmem_ld16(s.tmem + lane_base + u * 128 + dcol + c, t);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[c + q] = t[q];
+  }
+}
+
+__global__ void __launch_bounds__(2 * THREADS, 2) mlp_infer2_kernel(Gmlp g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  SmemF2 &s = *reinterpret_cast<SmemF2 *>(smem_raw);
+  constexpr uint32_t COLS = 256;
+  const int r = threadIdx.x & 127, u = threadIdx.x >> 7;
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(gb::smem_u32(&s.tmem)),
+                 "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    gb::mbar_init(&s.bar, 1);
+    gb::fence_barrier_init();
+  }
+  load_weights<SmemF2, false>(s, g.P);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  uint32_t phase = 0;
+  const int ntiles = (g.B + ROWS - 1) / ROWS;
+  const int npairs = (ntiles + 1) / 2;
+  for (int pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
+    const int row = (2 * pair + u) * ROWS + r;
+    const bool live = row < g.B;
+    {
+      float xv[KIN];
+#pragma unroll
+      for (int k = 0; k < KIN; ++k) xv[k] = live && k < NIN ? g.x[(size_t)row * NIN + k] : 0.f;
+#pragma unroll
+      for (int k = 0; k < KIN; k += 8) store8_bf16(&s.x[u][core_off(r, k, KIN)], xv + k);
+    }
+    if (!run_mma2(s, 0, s.x[0], s.x[1], s.w1, KIN, NH, phase, g.cap, g.status)) break;
+    {
+      float z[NH];
+      read_row2<NH>(s, 0, z);
+#pragma unroll
+      for (int h = 0; h < NH; ++h) z[h] = gelu(z[h] + s.b1[h]);
+#pragma unroll
+      for (int h = 0; h < NH; h += 8) store8_bf16(&s.h1[u][core_off(r, h, NH)], z + h);
+    }
+    if (!run_mma2(s, 64, s.h1[0], s.h1[1], s.w2, NH, NH, phase, g.cap, g.status)) break;
+    {
+      float z[NH];
+      read_row2<NH>(s, 64, z);
+#pragma unroll
+      for (int h = 0; h < NH; ++h) z[h] = gelu(z[h] + s.b2[h]);
+#pragma unroll
+      for (int h = 0; h < NH; h += 8) store8_bf16(&s.h2[u][core_off(r, h, NH)], z + h);
+    }
+    if (!run_mma2(s, 0, s.h2[0], s.h2[1], s.w3, NH, KOUT, phase, g.cap, g.status)) break;
+    float yv[KOUT];
+    read_row2<KOUT>(s, 0, yv);
+    if (live && g.y)
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) g.y[(size_t)row * NOUT + o] = yv[o] + s.b3[o];
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(s.tmem), "r"(COLS) : "memory");
+}
+
 // Sums the per-CTA partials in block order and applies Adam to the FP32
 // master weights (grad = sum of the partials).
 __global__ void adam_kernel(float *P, float *M, float *V, const float *partials, int nparts, int step, float lr,
@@ -477,10 +595,12 @@ static int mlp_launch(ghost_mlp *m, const float *x, const float *t, float *y, in
     mlp_kernel<true><<<grid, THREADS, smem, m->stream>>>(g);
     m->nparts = grid;
   } else {
-    const int grid = std::max(1, std::min(ntiles, 4 * nsm));
-    const size_t smem = sizeof(SmemF) + 1024;
-    MLP_CUDA(cudaFuncSetAttribute(mlp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mlp_kernel<false><<<grid, THREADS, smem, m->stream>>>(g);
+    // two tiles per CTA, two CTAs per SM
+    const int npairs = (ntiles + 1) / 2;
+    const int grid = std::max(1, std::min(npairs, 2 * nsm));
+    const size_t smem = sizeof(SmemF2) + 1024;
+    MLP_CUDA(cudaFuncSetAttribute(mlp_infer2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mlp_infer2_kernel<<<grid, 2 * THREADS, smem, m->stream>>>(g);
   }
   MLP_CUDA(cudaGetLastError());
   return GHOST_OK;

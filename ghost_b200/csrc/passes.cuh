@@ -838,6 +838,52 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_kernel(const cx<R>
   }
 }
 
+// Complex-to-real x lines of nine fields written straight into the LES
+// closure's input rows: x[q][f] = (real value / (nx ny nz)) * gs for grid
+// point q (real layout, x fastest), f = 0..8, and x[q][9] = delta.
+template <typename R, int NX, int E, int BZ>
+__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_features_kernel(Fields<R> in, float *__restrict__ xrows,
+                                                                              const cx<R> *__restrict__ twg, int ny,
+                                                                              int nz, R inv_n, float gs, float delta) {
+  using C = cx<R>;
+  constexpr int M = NX / 2, T = M / E, NT = BZ * T;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  C *tile = tw + NX;
+  C *xb = tile + (M + 1) * BZ;
+  const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
+  const int z0 = blockIdx.x * BZ, j = blockIdx.y;
+  const size_t rowstride = (size_t)nz * ny;
+  for (int e = tid; e < NX; e += NT) tw[e] = twg[e];
+  auto buf = [xb, l](int idx) -> C & { return xb[idx * BZ + l]; };
+  auto sync = [] { __syncthreads(); };
+  for (int f = 0; f < 9; ++f) {
+    x_tile_load<C, BZ>(tile, in.p[f] + (size_t)z0 + (size_t)nz * j, M + 1, rowstride, tid, NT);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    C x[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = c2r_pack(tile, BZ, l, t + T * e, M, M + 1, tw);
+    line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
+#pragma unroll
+    for (int e = 0; e < E; ++e) xb[l * M + t + T * e] = x[e];
+    __syncthreads();
+    for (int q = tid; q < BZ * M; q += NT) {
+      const int ll = q / M, m = q - ll * M;
+      const C v = xb[q];
+      float *row = xrows + (size_t)10 * ((size_t)NX * ((size_t)j + (size_t)ny * (z0 + ll)) + 2 * m);
+      row[f] = (float)(v.x * inv_n) * gs;
+      row[10 + f] = (float)(v.y * inv_n) * gs;
+      if (f == 8) {
+        row[9] = delta;
+        row[19] = delta;
+      }
+    }
+    __syncthreads();  // the tile and the staging buffer are reused by the next field
+  }
+}
+
 template <typename R, int NX, int E, int BZ>
 __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_r2c_kernel(const R *__restrict__ in,
                                                                      cx<R> *__restrict__ out,
