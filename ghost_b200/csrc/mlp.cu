@@ -1,5 +1,5 @@
 // mlp.cu -- the learned subgrid-stress closure: a 10 -> 64 -> 64 -> 6 MLP
-// (GELU) evaluated and trained with 5th-generation tensor cores.
+// (GELU, tanh form) evaluated and trained with 5th-generation tensor cores.
 //
 // Per CTA tile of 128 grid points (rows):
 //   forward   Z1 = X W1^T + b1, H1 = gelu(Z1); Z2 = H1 W2^T + b2, H2 = gelu(Z2);
@@ -102,9 +102,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel, 2016):
+//   gelu(z) = z/2 (1 + tanh(c (z + a z^3))), c = sqrt(2/pi), a = 0.044715,
+// with the hardware tanh (relative error about 2^-11, below the BF16
+// resolution of the activations it feeds).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(kGeluC * (z + kGeluA * z * z * z));
+  return 0.5f * z * (1.f + t);
+}
 __device__ __forceinline__ float gelu_d(float z) {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float t = tanh_hw(kGeluC * (z + kGeluA * z * z * z));
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * kGeluC * (1.f + 3.f * kGeluA * z * z);
 }
 
 // Eight consecutive K entries of one row are 16 contiguous bytes of a core

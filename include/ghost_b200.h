@@ -313,8 +313,9 @@ int ghost_init_random_solenoidal(ghost_ctx *ctx, int32_t *seed, double kdn, doub
 
 /* ---------------------------------------------------------------- */
 /* Learned subgrid-stress closure for LES (no counterpart in GHOST; GHOST's
- * own LES closure is the EDQNM eddy viscosity of 3D/src/edqnm/).
- * A 10 -> 64 -> 64 -> 6 MLP with GELU activations, BF16 tensor-core
+ * own LES closure is the EDQNM closure of pseudo/pseudospec3D_edqnm.f90).
+ * A 10 -> 64 -> 64 -> 6 MLP with GELU activations (tanh form:
+ * z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))), BF16 tensor-core
  * products with FP32 accumulation, FP32 master weights and Adam.
  * Inputs per grid point: the 9 resolved velocity gradients du_i/dx_j
  * (row-major i, j) and the filter width; outputs: the 6 independent

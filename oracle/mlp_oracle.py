@@ -7,7 +7,8 @@ never imports it.
 The network has no counterpart in GHOST; its definition is the one the
 C-ABI header states (ghost_b200.h, "Learned subgrid-stress closure"):
 parameters packed as W1[64][10], b1[64], W2[64][64], b2[64], W3[6][64],
-b3[6]; y = W x + b; GELU(z) = z/2 (1 + erf(z/sqrt 2)); loss = mean of the
+b3[6]; y = W x + b; GELU(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
+(the tanh form of Hendrycks and Gimpel); loss = mean of the
 squared error over B*6 values; Adam with beta1 0.9, beta2 0.999, eps 1e-8
 and bias correction.
 
@@ -21,7 +22,6 @@ Two modes:
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 NIN, NH, NOUT = 10, 64, 6
 SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NOUT, NH)), ("b3", (NOUT,))]
@@ -48,12 +48,16 @@ def pack(d: dict) -> np.ndarray:
     return np.concatenate([np.asarray(d[name]).ravel() for name, _ in SHAPES])
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def _q(a, emulate):
