@@ -21,7 +21,6 @@
 
 #include <algorithm>
 #include <random>
-#include <type_traits>
 #include <vector>
 
 #include "../../include/ghost_b200.h"
@@ -159,22 +158,6 @@ struct Smem {
 
 constexpr int TMEM_COLS = 256;  // D1/D5 at 0, D2/D4 at 64, D3 at 128
 
-// Forward-only tile storage (inference): no backward buffers, so four CTAs
-// share an SM; D1 and D3 share tensor-memory columns 0.. (D1 is read before
-// the layer-3 product is issued), D2 sits at 64.
-struct SmemF {
-  __nv_bfloat16 w1[NH * KIN];
-  __nv_bfloat16 w2[NH * NH];
-  __nv_bfloat16 w3[KOUT * NH];
-  __nv_bfloat16 x[ROWS * KIN];
-  __nv_bfloat16 h1[ROWS * NH];
-  __nv_bfloat16 h2[ROWS * NH];
-  float b1[NH], b2[NH], b3[KOUT];
-  uint64_t bar;
-  uint32_t tmem;
-};
-constexpr int TMEM_COLS_F = 128;
-
 // Loads the FP32 master weights as BF16 operands (with the transposed
 // copies of the backward products when BWD).
 template <class S, bool BWD> __device__ void load_weights(S &s, const float *__restrict__ P) {
@@ -259,17 +242,13 @@ struct Gmlp {
   uint32_t cap;
 };
 
-// TRAIN = false: inference (y written); true: loss and gradients.
-// Training uses the full tile storage (one CTA per SM); inference the
-// forward-only layout (four CTAs per SM, 128 tensor-memory columns each).
-template <bool TRAIN> using SmemOf = typename std::conditional<TRAIN, Smem, SmemF>::type;
-template <bool TRAIN>
-__global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
+// Loss and gradients of one batch: forward, backward-data and weight-gradient
+// sums per CTA (one CTA per SM).
+__global__ void __launch_bounds__(THREADS, 1) mlp_train_kernel(Gmlp g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  using S = SmemOf<TRAIN>;
-  S &s = *reinterpret_cast<S *>(smem_raw);
-  constexpr uint32_t COLS = TRAIN ? TMEM_COLS : TMEM_COLS_F;
-  constexpr uint32_t D3 = TRAIN ? 128 : 0;  // column of the layer-3 accumulator
+  Smem &s = *reinterpret_cast<Smem *>(smem_raw);
+  constexpr uint32_t COLS = TMEM_COLS;
+  constexpr uint32_t D3 = 128;  // column of the layer-3 accumulator
   const int r = threadIdx.x;
   if (threadIdx.x < 32) {  // warp 0 owns the tensor memory
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(gb::smem_u32(&s.tmem)),
@@ -280,9 +259,9 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
   if (threadIdx.x == 0) {
     gb::mbar_init(&s.bar, 1);
     gb::fence_barrier_init();
-    if constexpr (TRAIN) s.loss = 0.0;
+    s.loss = 0.0;
   }
-  load_weights<S, TRAIN>(s, g.P);
+  load_weights<Smem, true>(s, g.P);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -290,8 +269,8 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
   // FP32 gradient accumulators: thread r owns entries q = r + THREADS*m of
   // the parameter vector (all rows of the tile summed per entry)
   constexpr int NOWN = (NPARAM + THREADS - 1) / THREADS;
-  float acc[TRAIN ? NOWN : 1];
-  if (TRAIN) {
+  float acc[NOWN];
+  {
 #pragma unroll
     for (int m = 0; m < NOWN; ++m) acc[m] = 0.f;
   }
@@ -317,7 +296,7 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b1[h];
         z[h] = gelu(zz);
-        if constexpr (TRAIN) s.g1[r * NH + h] = gelu_d(zz);
+        s.g1[r * NH + h] = gelu_d(zz);
       }
 #pragma unroll
       for (int h = 0; h < NH; h += 8) store8_bf16(&s.h1[core_off(r, h, NH)], z + h);
@@ -331,7 +310,7 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
       for (int h = 0; h < NH; ++h) {
         const float zz = z[h] + s.b2[h];
         z[h] = gelu(zz);
-        if constexpr (TRAIN) s.g2[r * NH + h] = gelu_d(zz);
+        s.g2[r * NH + h] = gelu_d(zz);
       }
 #pragma unroll
       for (int h = 0; h < NH; h += 8) store8_bf16(&s.h2[core_off(r, h, NH)], z + h);
@@ -342,11 +321,7 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
     read_row<KOUT>(s, D3, yv);
 #pragma unroll
     for (int o = 0; o < KOUT; ++o) yv[o] += s.b3[o];
-    if constexpr (!TRAIN) {
-      if (live && g.y)
-#pragma unroll
-        for (int o = 0; o < NOUT; ++o) g.y[(size_t)row * NOUT + o] = yv[o];
-    } else {
+    {
       // ---- loss and dY
       float dyv[KOUT];
 #pragma unroll
@@ -414,7 +389,6 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
       __syncthreads();
     }
   }
-  if constexpr (TRAIN) {
   if (g.grad) {
     float *dst = g.grad + (size_t)blockIdx.x * (NPARAM + 1);
 #pragma unroll
@@ -429,7 +403,6 @@ __global__ void __launch_bounds__(THREADS, TRAIN ? 1 : 4) mlp_kernel(Gmlp g) {
       __syncthreads();
     }
     if (r == 0) dst[NPARAM] = (float)s.loss;
-  }
   }
   tc_fence_before();
   __syncthreads();
@@ -605,8 +578,8 @@ static int mlp_launch(ghost_mlp *m, const float *x, const float *t, float *y, in
     // one CTA per SM; the per-CTA gradient partials are summed by the Adam kernel
     const int grid = std::max(1, std::min(ntiles, nsm));
     const size_t smem = sizeof(Smem) + 1024;
-    MLP_CUDA(cudaFuncSetAttribute(mlp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mlp_kernel<true><<<grid, THREADS, smem, m->stream>>>(g);
+    MLP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mlp_train_kernel<<<grid, THREADS, smem, m->stream>>>(g);
     m->nparts = grid;
   } else {
     // two tiles per CTA, two CTAs per SM
