@@ -116,6 +116,8 @@ SIGNATURES = {
     "ghost_les_features": [P, P, P, P, ctypes.c_float, ctypes.c_float, P],
     "ghost_les_tau_force": [P, P, ctypes.c_float, P, P, P, P, P, P],
     "ghost_les_set_model": [P, I, P, D, D, D, D],
+    "ghost_les_set_fallback": [P, I, D],
+    "ghost_les_status": [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)],
     "ghost_les_set_time": [P, D],
     "ghost_les_closure_force": [P, D, P, P, P, P, P, P, P, P, P],
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],

@@ -1111,6 +1111,8 @@ int batch_init_random_dev(ghost_ctx *c, const int32_t *seeds, int32_t *seeds_out
   template int hd_substep_dev<R>(ghost_ctx *, int, double, double, void *const[3], void *const[3],             \
                                  const void *const[3], int, bool);                                             \
   template int spectrum_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);          \
+  template int reduce_dev<R>(ghost_ctx *, int, const void *, const void *, const void *, const void *,         \
+                             const void *, const void *, double *);                                            \
   template int spectrum_dev_async<R>(ghost_ctx *, int, const void *, const void *, const void *, double *);
 GB_INST(float)
 GB_INST(double)

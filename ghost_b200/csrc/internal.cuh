@@ -30,6 +30,10 @@ template <typename R> int r2c6_dev(ghost_ctx *c, const void *const in[6], void *
 template <typename R>
 int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], void *const C[3], const void *const f[3],
                    int copy, bool prune = false);
+// reductions of ops.cuh (kind 0: <|v|^2>) into one host double
+template <typename R>
+int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d, const void *e,
+               const void *f, double *out_host);
 // kinetic (kind 1) shell spectrum into out_host[nmax/2+1]
 template <typename R>
 int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host);

@@ -714,6 +714,12 @@ struct ghost_les {
   double *tve_dev = nullptr, *tepq_dev = nullptr, *Ek_dev = nullptr, *Ext_dev = nullptr, *mu_dev = nullptr;
   int *go_dev = nullptr;  // 1 when the fit succeeded and the quadrature runs
   void *ef = nullptr;      // per-mode energy of the substep's start (vcorrect)
+  // fallback of the learned closure to EDQNM (ghost_les_set_fallback)
+  bool fallback = false;
+  double blowup = 10.0;
+  long long fell_back_at = -1;  // step of the run at which it happened, or -1
+  long long steps_done = 0;
+  void *save[3] = {};
   bool edqnm_done = false;
   // fine-grid buffers for ghost_les_samples (size of the last fine grid)
   size_t fine_rbytes = 0, fine_cbytes = 0;
@@ -869,7 +875,6 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
   bool first = true;
   // GHOST's EDQNM step ends with vcorrect, which needs the per-mode energies
   // of the substep's start (edqnmhd_rkstep2.f90:8-10,63)
-  const bool vcorr = L->model == GHOST_LES_EDQNM;
   const int nb = c->nx / 2 + 1;
   const R n3 = (R)c->nx * (R)c->ny * (R)c->nz;
   const R rmp = (R)1 / (n3 * n3);
@@ -880,15 +885,27 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
     vr.p[a] = (const cx<R> *)v[a];
     vw.p[a] = (cx<R> *)v[a];
   }
+  // the learned closure's fallback: each step starts from a saved copy, and a
+  // step that ends non-finite or with <|v|^2> above blowup times its value at
+  // the start of the call is redone with GHOST's EDQNM closure, which then
+  // stays in use
+  double e_ref = 0.0;
+  const bool guard = L->fallback && L->model == GHOST_LES_MLP;
+  if (guard) GB_CHECK(reduce_dev<R>(c, 0 /* <|v|^2> */, v[0], v[1], v[2], nullptr, nullptr, nullptr, &e_ref));
   for (int s = 0; s < nsteps; ++s) {
+    const bool guarded = L->fallback && L->model == GHOST_LES_MLP;
+    if (guarded)
+      for (int a = 0; a < 3; ++a)
+        GB_CUDA(cudaMemcpyAsync(L->save[a], v[a], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+    const bool vcorr_step = L->model == GHOST_LES_EDQNM;
     for (int o = ord; o >= 1; --o) {
       GB_CHECK(closure_force_dev<R>(L, v, f, L->force));
-      if (vcorr) {
+      if (vcorr_step) {
         eden_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(vr, (R *)L->ef, c->nspec, rmp);
         GB_CHECK(post_launch(c));
       }
       GB_CHECK(hd_substep_dev<R>(c, o, dt, nu, v, L->rk, L->force, o == ord ? 1 : 0, !first));
-      if (vcorr) {
+      if (vcorr_step) {
         vcorrect_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vw, (const R *)L->ef, L->tepq_dev,
                                                                     L->Ek_dev, nb, (R)dt * ((R)1 / (R)o), tinyf, n3,
                                                                     c->nspec);
@@ -896,7 +913,21 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
       }
       first = false;
     }
+    if (guarded) {
+      double e = 0.0;
+      GB_CHECK(reduce_dev<R>(c, 0 /* <|v|^2> */, v[0], v[1], v[2], nullptr, nullptr, nullptr, &e));
+      if (!std::isfinite(e) || (e_ref > 0.0 && e > L->blowup * e_ref)) {
+        for (int a = 0; a < 3; ++a)
+          GB_CUDA(cudaMemcpyAsync(v[a], L->save[a], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+        L->model = GHOST_LES_EDQNM;
+        L->fell_back_at = L->steps_done;
+        first = true;  // the restored velocity may carry modes outside the truncation
+        --s;           // redo this step
+        continue;
+      }
+    }
     L->t += dt;
+    ++L->steps_done;
   }
   return check_status(c);
 }
@@ -951,6 +982,7 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   if (!st) st = les_alloc(L, sizeof(double) * (3 * nb + 1), (void **)&L->mu_dev);
   if (!st) st = les_alloc(L, sizeof(int), (void **)&L->go_dev);
   if (!st) st = les_alloc(L, c->cbytes, &L->ef);
+  for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->save[q]);
   if (st) {
     ghost_les_destroy(L);
     return st;
@@ -1042,6 +1074,25 @@ int ghost_les_set_model(ghost_les *L, int model, ghost_mlp *mlp, double grad_sca
   L->ts = (float)tau_scale;
   L->delta = (float)delta;
   L->kolmo = kolmo;
+  L->fell_back_at = -1;
+  return GHOST_OK;
+}
+
+int ghost_les_set_fallback(ghost_les *L, int enable, double blowup) {
+  LES_CHECK(L);
+  if (enable && !(blowup > 1.0)) return fail(GHOST_ERR_ARG, "blowup factor must exceed 1");
+  if (enable && !(L->kolmo > 0)) return fail(GHOST_ERR_ARG, "the fallback needs a positive kolmo (ghost_les_set_model)");
+  if (enable && (int)std::sqrt(L->c->kmax) < 4)
+    return fail(GHOST_ERR_ARG, "the EDQNM fallback needs a cutoff of at least 4 shells");
+  L->fallback = enable != 0;
+  L->blowup = blowup;
+  return GHOST_OK;
+}
+
+int ghost_les_status(const ghost_les *L, int *model, long long *fell_back_at) {
+  LES_CHECK(L);
+  if (model) *model = L->model;
+  if (fell_back_at) *fell_back_at = L->fell_back_at;
   return GHOST_OK;
 }
 

@@ -472,6 +472,20 @@
          REAL(C_DOUBLE), VALUE :: gs, ts, delta, kolmo
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_les_set_fallback(les,enable,blowup) BIND(C,name="ghost_les_set_fallback") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les
+         INTEGER(C_INT), VALUE :: enable
+         REAL(C_DOUBLE), VALUE :: blowup
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_status(les,model,fell_back_at) BIND(C,name="ghost_les_status") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_LONG_LONG
+         TYPE(C_PTR), VALUE :: les
+         INTEGER(C_INT) :: model
+         INTEGER(C_LONG_LONG) :: fell_back_at
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_les_set_time(les,t) BIND(C,name="ghost_les_set_time") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE
          TYPE(C_PTR), VALUE :: les

@@ -171,6 +171,16 @@ class LES:
         self.model = model
         self.mlp = mlp
 
+    def set_fallback(self, enable: bool = True, blowup: float = 10.0):
+        """Let ``run`` switch the MLP closure to EDQNM when a step diverges."""
+        check(self.lib.ghost_les_set_fallback(self.h, int(enable), blowup), "ghost_les_set_fallback")
+
+    def status(self):
+        """(selected closure name, step at which the fallback engaged or -1)."""
+        m, at = ctypes.c_int(), ctypes.c_longlong()
+        check(self.lib.ghost_les_status(self.h, ctypes.byref(m), ctypes.byref(at)), "ghost_les_status")
+        return {v: k for k, v in MODELS.items()}[m.value], at.value
+
     def set_time(self, t: float):
         check(self.lib.ghost_les_set_time(self.h, t), "ghost_les_set_time")
 

@@ -388,6 +388,15 @@ int ghost_les_tau_force(ghost_les *les, const float *tau, float tau_scale, const
  * context's stream. */
 int ghost_les_set_model(ghost_les *les, int model, ghost_mlp *mlp, double grad_scale, double tau_scale, double delta,
                         double kolmo);
+/* fallback of the MLP closure to EDQNM in ghost_les_run: every step then
+ * starts from a saved copy of v, and a step that ends with a non-finite
+ * <|v|^2>, or one above blowup (> 1) times its value when the call started,
+ * is redone with the EDQNM closure (kolmo from ghost_les_set_model), which
+ * stays selected.  Costs one energy reduction and a host sync per step. */
+int ghost_les_set_fallback(ghost_les *les, int enable, double blowup);
+/* the selected closure (GHOST_LES_*) and the step count of the LES's runs
+ * at which the fallback switched to EDQNM (-1: it has not) */
+int ghost_les_status(const ghost_les *les, int *model, long long *fell_back_at);
 /* time handed to the EDQNM closure (GHOST's (t-1)*dt); ghost_les_run
  * advances it by dt per step */
 int ghost_les_set_time(ghost_les *les, double t);

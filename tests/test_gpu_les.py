@@ -131,3 +131,58 @@ def test_les_without_closure_is_hd_run(prec):
     g2.hd_run(4, 4, 1e-3, 1e-3, *B, *F)
     for a, b in zip(A, B):
         assert np.array_equal(to_host(a), to_host(b))
+
+
+def _mlp_les(prec, p, fallback):
+    from ghost_b200.les import MLP
+    fo, co, gf, gc, les = setup(prec)
+    m = MLP(0)
+    m.params = p
+    les.set_model("mlp", m, grad_scale=0.3, tau_scale=0.05, delta=1.0, kolmo=1.4)
+    les.set_time(1.0)
+    if fallback:
+        les.set_fallback(True, 10.0)
+    return co, les, m
+
+
+def test_mlp_fallback_to_edqnm():
+    """A network whose stresses overflow makes the first step non-finite: the
+    step is redone with EDQNM, which then matches an EDQNM-only run exactly."""
+    p = M.glorot(12) * np.float32(1e30)
+    co, les, m = _mlp_les("fp32", p, True)
+    v = kolmogorov_field(co, 15, 10)
+    f, _ = co.random_solenoidal(16, 2.0, 3.0, 0, 1.0)
+    A = [to_dev(a) for a in v]
+    F = [to_dev(a) for a in f]
+    les.run(3, 2, 1e-3, 1e-3, *A, *F)
+    assert les.status() == ("edqnm", 0)
+    _, _, _, _, ref = setup("fp32")
+    ref.set_model("edqnm", kolmo=1.4)
+    ref.set_time(1.0)
+    B = [to_dev(a) for a in v]
+    ref.run(3, 2, 1e-3, 1e-3, *B, *F)
+    for a, b in zip(A, B):
+        h = to_host(a)
+        assert np.all(np.isfinite(h))
+        assert np.array_equal(h, to_host(b))
+    # without the fallback the same network leaves a non-finite field
+    _, les2, m2 = _mlp_les("fp32", p, False)
+    C = [to_dev(a) for a in v]
+    les2.run(1, 2, 1e-3, 1e-3, *C, *F)
+    assert not all(np.all(np.isfinite(to_host(a))) for a in C)
+    assert les2.status() == ("mlp", -1)
+
+
+def test_mlp_fallback_idle_on_a_sane_network():
+    """With a working network the guarded run is the unguarded one, bit for bit."""
+    p = M.glorot(12)
+    co, les, m = _mlp_les("fp32", p, True)
+    _, les2, m2 = _mlp_les("fp32", p, False)
+    v = kolmogorov_field(co, 17, 10)
+    A = [to_dev(a) for a in v]
+    B = [to_dev(a) for a in v]
+    les.run(3, 2, 1e-3, 1e-3, *A)
+    les2.run(3, 2, 1e-3, 1e-3, *B)
+    assert les.status() == ("mlp", -1)
+    for a, b in zip(A, B):
+        assert np.array_equal(to_host(a), to_host(b))
