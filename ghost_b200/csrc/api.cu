@@ -16,6 +16,7 @@
 #include "internal.cuh"
 #include "ops.cuh"
 #include "passes.cuh"
+#include "xwarp.cuh"
 
 namespace gb {
 
@@ -279,7 +280,8 @@ static int encode_fn(PFN_cuTensorMapEncodeTiled_v12000 *fn) {
   return GHOST_OK;
 }
 
-static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box1, unsigned box2, CUtensorMap *out) {
+static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box1, unsigned box2, CUtensorMap *out,
+                     CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE) {
   PFN_cuTensorMapEncodeTiled_v12000 enc;
   GB_CHECK(encode_fn(&enc));
   const cuuint64_t U = c->precision == GHOST_SINGLE ? 1 : 2;
@@ -288,7 +290,7 @@ static int field_map(ghost_ctx *c, const void *base, unsigned box0, unsigned box
   const cuuint32_t box[3] = {box0, box1, box2};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(GHOST_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return GHOST_OK;
@@ -447,6 +449,79 @@ int launch_x_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int 
   return GHOST_OK;
 }
 
+// TMA map of a real FP32 field (x fastest) as 8-byte pairs: a box of
+// nx/2 pairs x 1 y-row x 8 z-values, the tiles of the plain x transforms.
+static int real_map(ghost_ctx *c, const void *base, CUtensorMap *out) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc;
+  GB_CHECK(encode_fn(&enc));
+  const cuuint64_t dims[3] = {(cuuint64_t)c->nx / 2, (cuuint64_t)c->ny, (cuuint64_t)c->nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)c->nx * 4, (cuuint64_t)c->nx * c->ny * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)c->nx / 2, 1, 8};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(GHOST_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return GHOST_OK;
+}
+
+// The plain x transforms with one warp per line (FP32, nx = 512, one run).
+static bool xw_plain_ok(const ghost_ctx *c) {
+  return c->precision == GHOST_SINGLE && c->nx == 512 && c->nruns == 1 && c->nz % 8 == 0;
+}
+static int launch_xw_r2c(ghost_ctx *c, const void *in, void *out) {
+  constexpr int NX = 512, M = NX / 2, STAGES = 3;
+  using G = XWPlainGeom<NX, STAGES>;
+  auto kern = xwarp_r2c_kernel<NX, STAGES>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::r2c_bytes));
+  const int rb = ((M + 1 + 1) / 2 + 15) / 16 * 16;  // 2 x 144 rows cover the M+1 kx rows
+  static_assert(2 * (((M + 2) / 2 + 15) / 16 * 16) <= G::OROWS, "r2c store boxes exceed the output tile");
+  CUtensorMap rm, cm;
+  GB_CHECK(real_map(c, in, &rm));
+  GB_CHECK(field_map(c, out, 8, 1, rb, &cm, CU_TENSOR_MAP_SWIZZLE_64B));
+  const int grid = persistent_grid(c, kern, 256, G::r2c_bytes, (long)(c->nz / 8) * c->ny);
+  kern<<<grid, 256, G::r2c_bytes, c->stream>>>(rm, cm, (const float2 *)c->tw_x, c->ny, c->nz, rb, pipe_ctl(c));
+  return GHOST_OK;
+}
+static int launch_xw_c2r(ghost_ctx *c, const void *in, void *out) {
+  constexpr int NX = 512, M = NX / 2, STAGES = 4;
+  using G = XWPlainGeom<NX, STAGES>;
+  auto kern = xwarp_c2r_kernel<NX, STAGES>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::c2r_bytes));
+  const int nbox = 2, rb = ((M + 1 + 1) / 2 + 15) / 16 * 16;  // 2 x 144 rows cover the M+1 kx rows
+  static_assert(2 * (((M + 2) / 2 + 15) / 16 * 16) <= G::SROWS, "c2r box plan exceeds the slot");
+  CUtensorMap m;
+  GB_CHECK(field_map(c, in, 8, 1, rb, &m, CU_TENSOR_MAP_SWIZZLE_64B));
+  const int grid = persistent_grid(c, kern, 256, G::c2r_bytes, (long)(c->nz / 8) * c->ny);
+  kern<<<grid, 256, G::c2r_bytes, c->stream>>>(m, (float *)out, (const float2 *)c->tw_x, c->ny, c->nz, nbox, rb,
+                                               pipe_ctl(c));
+  return GHOST_OK;
+}
+
+// The fused X pass with one warp per line (FP32, nx = 512; tile variant bit 4).
+static int launch_xw_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int rows) {
+  constexpr int NX = 512, M = NX / 2, STAGES = 3;
+  using G = XWGeom<NX, STAGES>;
+  const size_t smem = G::bytes;
+  auto kern = xwarp_nl_kernel<NX, STAGES>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Fields<float> fo{};
+  for (int q = 0; q < 3; ++q) fo.p[q] = (float2 *)outs[q];
+  const float nn = (float)c->nx * (float)c->ny * (float)c->nz;
+  const int nrows = rows > 0 ? rows : M + 1;
+  // one box of up to 256 kx rows, or two; rows in multiples of 16 start
+  // every box on a 1024-byte boundary
+  const int nbox = (nrows + 255) / 256;
+  const int rb = ((nrows + nbox - 1) / nbox + 15) / 16 * 16;
+  if (nbox * rb > G::SROWS || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the slot", nbox, rb);
+  FieldMaps maps;
+  for (int q = 0; q < 6; ++q) GB_CHECK(field_map(c, ins[q], G::BZ, 1, rb, &maps.m[q], CU_TENSOR_MAP_SWIZZLE_64B));
+  const int pgrid = persistent_grid(c, kern, 256, smem, (long)(c->nz / G::BZ) * c->ny * c->nruns);
+  kern<<<pgrid, 256, smem, c->stream>>>(maps, fo, (const float2 *)c->tw_x, c->ny, c->nz, 1.f / (nn * nn), nrows, nbox,
+                                        rb, c->nruns, c->nxh, pipe_ctl(c));
+  return GHOST_OK;
+}
+
 template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void *in, void *out, const void *const *ins,
                                                        void *const *outs, int rows) {
   constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
@@ -459,8 +534,14 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
   dim3 grid(c->nz / BZ, c->ny);
   const C *tw = (const C *)c->tw_x;
   const int ts = timer_begin(c, KIND == X_C2R ? GHOST_TIMER_X_C2R : (KIND == X_R2C ? GHOST_TIMER_X_R2C : GHOST_TIMER_X_NL));
-  if (KIND == X_HD || KIND == X_BOUSS) {
+  if (KIND == X_HD && sizeof(R) == 4 && NX == 512 && (c->tile_cfg & 16) && c->nz % 8 == 0) {
+    GB_CHECK(launch_xw_fused(c, ins, outs, rows));
+  } else if (KIND == X_HD || KIND == X_BOUSS) {
     GB_CHECK((launch_x_fused<R, NX, KIND, BZ, 2>(c, ins, outs, rows)));
+  } else if (KIND == X_C2R && xw_plain_ok(c)) {
+    GB_CHECK(launch_xw_c2r(c, in, out));
+  } else if (KIND == X_R2C && xw_plain_ok(c)) {
+    GB_CHECK(launch_xw_r2c(c, in, out));
   } else if (KIND == X_C2R) {
     const size_t smem = (size_t)(NX + (M + 1) * BZ + M * BZ) * sizeof(C);
     auto kern = xpass_c2r_kernel<R, NX, E, BZ>;
@@ -1651,7 +1732,7 @@ static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14};
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 15) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..15", cfg);
+  if (cfg < 0 || cfg > 31) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..31", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }
