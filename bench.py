@@ -233,35 +233,55 @@ def rel_err_fp32_step(n, rank):
     return max(errs)
 
 
-def fft_roofline(n, reps=10):
-    """Standalone 3D r2c at n^3 FP32: achieved (R + C) bytes / time."""
+def fft_roofline(n, peak, reps=10):
+    """Standalone 3D r2c and c2r at n^3 FP32.  Whole transform: achieved
+    (R + C) bytes / time.  Per pass (the kernels): every pass reads and
+    writes the whole field once (x: R + C, y and z: 2C), against the
+    library's own per-pass CUDA-event timers."""
     import torch
-    from ghost_b200 import GHOST_REAL_TO_COMPLEX, Ghost
+    from ghost_b200 import GHOST_COMPLEX_TO_REAL, GHOST_REAL_TO_COMPLEX, Ghost
     g = Ghost(n, precision="fp32")
     x = torch.randn((n, n, n), device="cuda", dtype=torch.float32)
     c = g.czeros()
-    plan = g.fftp3d_create_plan((n, n, n), GHOST_REAL_TO_COMPLEX)
-    for _ in range(3):
-        g.fftp3d_real_to_complex(plan, x, c)
-    s = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g.enable_timers(True)
-    g.read_timers()
-    e0.record(s)
-    for _ in range(reps):
-        g.fftp3d_real_to_complex(plan, x, c)
-    e1.record(s)
-    e1.synchronize()
-    tm = g.read_timers()
-    g.enable_timers(False)
-    ms = e0.elapsed_time(e1) / reps
+    fwd = g.fftp3d_create_plan((n, n, n), GHOST_REAL_TO_COMPLEX)
+    inv = g.fftp3d_create_plan((n, n, n), GHOST_COMPLEX_TO_REAL)
     R = n ** 3 * 4
     C = (n // 2 + 1) * n * n * 8
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        g.enable_timers(True)
+        g.read_timers()
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        tm = g.read_timers()
+        g.enable_timers(False)
+        return e0.elapsed_time(e1) / reps, tm
+
+    ms_f, tm_f = timed(lambda: g.fftp3d_real_to_complex(fwd, x, c))
+    ms_i, tm_i = timed(lambda: g.fftp3d_complex_to_real(inv, c, x))
     g.close()
     del x, c
     torch.cuda.empty_cache()
-    return {"ms_per_fft": ms, "algorithmic_bytes": R + C, "gbs": (R + C) / (ms * 1e-3) / 1e9,
-            "passes_ms": {k: v[0] / reps for k, v in tm.items()}}
+    passes = {}
+    for tm in (tm_f, tm_i):
+        for k, (t, cnt) in tm.items():
+            if not cnt:
+                continue
+            nbytes = R + C if k.startswith("x_") else 2 * C
+            ms = t / cnt
+            passes[k] = {"ms_per_launch": ms, "bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                         "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
+    return {"ms_per_fft": ms_f, "ms_per_ifft": ms_i, "algorithmic_bytes": R + C,
+            "gbs": (R + C) / (ms_f * 1e-3) / 1e9, "frac": (R + C) / (ms_f * 1e-3) / 1e9 / peak,
+            "passes": passes, "min_pass_frac": min(p["frac"] for p in passes.values())}
 
 
 def e2e_host(n, steps, rank):
@@ -377,7 +397,7 @@ def run_ours(args, ws, rank, local):
             for k in tm}
 
     err = rel_err_fp32_step(n, rank) if rank == 0 else None
-    fft = fft_roofline(n) if rank == 0 else None
+    fft = fft_roofline(n, peak) if rank == 0 else None
     e2e_val, h2d, d2h = e2e_host(n, args.e2e_steps, rank) if rank == 0 else (None, 0, 0)
     if ws > 1:
         e2e_val = None
@@ -409,7 +429,7 @@ def run_ours(args, ws, rank, local):
                          "frac": ach / peak, "peak_kind": peak_kind,
                          "traffic": traffic_from_profiles(dom)},
             "kernels": kern,
-            "fft": None if fft is None else {**fft, "frac": fft["gbs"] / peak},
+            "fft": fft,
             "substep_effective_gbs": survey_bytes / (ms32 / args.steps / ORD * 1e-3) / 1e9,
             "prune": {"f_line": f_line, "f_row": f_row, "f_keep": f_keep},
             "substep_bytes": sum(per_launch_bytes.values()),

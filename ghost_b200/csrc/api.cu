@@ -498,30 +498,6 @@ static int launch_xw_c2r(ghost_ctx *c, const void *in, void *out) {
   return GHOST_OK;
 }
 
-// The fused X pass with one warp per line (FP32, nx = 512; tile variant bit 4).
-static int launch_xw_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int rows) {
-  constexpr int NX = 512, M = NX / 2, STAGES = 3;
-  using G = XWGeom<NX, STAGES>;
-  const size_t smem = G::bytes;
-  auto kern = xwarp_nl_kernel<NX, STAGES>;
-  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  Fields<float> fo{};
-  for (int q = 0; q < 3; ++q) fo.p[q] = (float2 *)outs[q];
-  const float nn = (float)c->nx * (float)c->ny * (float)c->nz;
-  const int nrows = rows > 0 ? rows : M + 1;
-  // one box of up to 256 kx rows, or two; rows in multiples of 16 start
-  // every box on a 1024-byte boundary
-  const int nbox = (nrows + 255) / 256;
-  const int rb = ((nrows + nbox - 1) / nbox + 15) / 16 * 16;
-  if (nbox * rb > G::SROWS || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the slot", nbox, rb);
-  FieldMaps maps;
-  for (int q = 0; q < 6; ++q) GB_CHECK(field_map(c, ins[q], G::BZ, 1, rb, &maps.m[q], CU_TENSOR_MAP_SWIZZLE_64B));
-  const int pgrid = persistent_grid(c, kern, 256, smem, (long)(c->nz / G::BZ) * c->ny * c->nruns);
-  kern<<<pgrid, 256, smem, c->stream>>>(maps, fo, (const float2 *)c->tw_x, c->ny, c->nz, 1.f / (nn * nn), nrows, nbox,
-                                        rb, c->nruns, c->nxh, pipe_ctl(c));
-  return GHOST_OK;
-}
-
 template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void *in, void *out, const void *const *ins,
                                                        void *const *outs, int rows) {
   constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
@@ -534,9 +510,7 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
   dim3 grid(c->nz / BZ, c->ny);
   const C *tw = (const C *)c->tw_x;
   const int ts = timer_begin(c, KIND == X_C2R ? GHOST_TIMER_X_C2R : (KIND == X_R2C ? GHOST_TIMER_X_R2C : GHOST_TIMER_X_NL));
-  if (KIND == X_HD && sizeof(R) == 4 && NX == 512 && (c->tile_cfg & 16) && c->nz % 8 == 0) {
-    GB_CHECK(launch_xw_fused(c, ins, outs, rows));
-  } else if (KIND == X_HD || KIND == X_BOUSS) {
+  if (KIND == X_HD || KIND == X_BOUSS) {
     GB_CHECK((launch_x_fused<R, NX, KIND, BZ, 2>(c, ins, outs, rows)));
   } else if (KIND == X_C2R && xw_plain_ok(c)) {
     GB_CHECK(launch_xw_c2r(c, in, out));
@@ -1732,7 +1706,7 @@ static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14};
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 31) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..31", cfg);
+  if (cfg < 0 || cfg > 15) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..15", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }

@@ -1,35 +1,25 @@
-// xwarp.cuh -- X pass of the fused HD substep with one warp per x line.
+// xwarp.cuh -- plain x transforms with one warp per x line.
 //
-// GHOST's nonlinear term (prodre3, pseudospec3D_hd.f90:316-396, fed by the
-// complex-to-real x transforms of fftp3d_complex_to_real and followed by the
-// real-to-complex ones of fftp3d_real_to_complex) for FP32 data and x lines
-// of NX = 512 points: each line is a 256-point complex transform held by the
-// 32 lanes of one warp, 8 values per lane, so the transform's shared-memory
-// exchanges go through a buffer private to the warp and need __syncwarp
-// only.  The CTA has no barrier inside a transform; its warps meet three
-// times per tile, once per output field.
-//
-// Data movement, per tile of 8 z-values at one (y, run):
-//   in   each of the six input fields (v, curl v) is one or two TMA tensor
-//        boxes of kx rows x 8 z-values (64 bytes, SWIZZLE_64B) into a
-//        STAGES-deep ring.  A slot is refilled by the last warp to finish
-//        reading it (a per-slot arrival counter), so no warp waits for
-//        another to free a slot.
-//   pack X_k comes from the tile, X_{M-k} from lane (32 - t) mod 32 by a
-//        shuffle (lane 0 supplies its own values one register over).
-//   out  the three products' spectra are unpacked the same way into a
-//        swizzled kx-row tile (two alternating buffers) and, after a CTA
-//        barrier, copied out as 16-byte chunks of whole 64-byte rows.
+// GHOST's fftp3d_real_to_complex / fftp3d_complex_to_real x stage (the
+// real-to-complex and complex-to-real FFTW plans of fftp-3/fftp3D.fpp) for
+// FP32 data and x lines of NX = 512 points: each line is a 256-point
+// complex transform held by the 32 lanes of one warp, 8 values per lane, so
+// the transform's shared-memory exchanges go through a buffer private to
+// the warp and need __syncwarp only.
 //
 // Shared-memory layouts (8-byte complex elements):
-//   tiles  element (k, l) at byte 64k + 8l with the 16-byte chunk index
-//          XORed by (k >> 1) & 3 (the TMA SWIZZLE_64B pattern; every tile
-//          base is 1024-byte aligned and every box starts on 16 rows);
+//   tiles  element (k, l) of a kx-row tile (row k = 8 z-values, 64 bytes)
+//          at byte 64k + 8l with the 16-byte chunk index XORed by
+//          (k >> 1) & 3: the TMA SWIZZLE_64B pattern (every tile base is
+//          1024-byte aligned and every box starts on 16 rows);
 //   lines  element i of a warp's exchange buffer at
 //          i ^ ((i >> 4) & 7) ^ ((i >> 3) & 8): the transform's exchange
 //          patterns (t + 32e reads, radix-8 stage writes 8t + r and
 //          64(t/8) + (t%8) + 8r) then touch 16 distinct 8-byte slots per
 //          half-warp, the minimum for 8-byte accesses.
+// The mirror element X_{M-k} (pack) and Z_{M-k} (unpack) of k = t + 32e is
+// register 7-e of lane 32-t (lane 0: its own register 8-e), fetched by
+// shuffles.
 #pragma once
 #include "fft_core.cuh"
 #include "passes.cuh"
@@ -43,21 +33,6 @@ __device__ __forceinline__ uint32_t xw_tile_off(int k, int l) {
   return ((uint32_t)k << 6) + (((uint32_t)(l >> 1) ^ ((uint32_t)(k >> 1) & 3u)) << 4) + ((uint32_t)(l & 1) << 3);
 }
 
-template <int NX, int STAGES> struct XWGeom {
-  static constexpr int M = NX / 2;
-  static constexpr int BZ = 8;                    // z-values per tile = warps per CTA
-  static constexpr int SROWS = M + 32;            // rows of an input slot (boxes overrun M+1 by < 32)
-  static constexpr int OROWS = (M + 1 + 7) / 8 * 8;
-  static constexpr size_t in_bytes = (size_t)SROWS * 64;
-  static constexpr size_t out_bytes = (size_t)OROWS * 64;
-  static constexpr size_t off_out = STAGES * in_bytes;
-  static constexpr size_t off_xw = off_out + 2 * out_bytes;
-  static constexpr size_t off_tw = off_xw + (size_t)BZ * M * 8;
-  static constexpr size_t off_bar = off_tw + (size_t)NX * 8;
-  // STAGES + 1 mbarriers, then STAGES arrival counters and STAGES last-issued loads
-  static constexpr size_t bytes = off_bar + (STAGES + 1) * 8 + STAGES * 8 + 1024;  // + alignment slack
-};
-
 // pack for the inverse: Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k/NX} (X_k - conj X_{M-k})
 __device__ __forceinline__ float2 xw_pack(float2 xk, float2 xm, float2 w) {
   const float2 a = mk(xk.x + xm.x, xk.y - xm.y);
@@ -66,200 +41,9 @@ __device__ __forceinline__ float2 xw_pack(float2 xk, float2 xm, float2 w) {
   return mk(a.x - wb.y, a.y + wb.x);
 }
 
-// Input fields in the order they are transformed: vx, vy, wx, wy, vz, wz
-// (inputs 0-2 = v, 3-5 = curl v).  With (w x v)_z transformed back as soon
-// as it is complete (after wy), at most five real lines are held per lane.
-__device__ __forceinline__ int xw_field(int n) { return n < 2 ? n : (n < 4 ? n + 1 : (n == 4 ? 2 : 5)); }
-
 __device__ __forceinline__ float2 shfl2(float2 v, int src) {
   return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
-
-template <int NX, int STAGES>
-__global__ void __launch_bounds__(256, 2) xwarp_nl_kernel(const __grid_constant__ FieldMaps maps, Fields<float> out,
-                                                          const float2 *__restrict__ twg, int ny, int nz, float scale,
-                                                          int rows, int nbox, int rb, int nruns, int nxh,
-                                                          PipeCtl ctl) {
-  using C = float2;
-  using G = XWGeom<NX, STAGES>;
-  constexpr int M = NX / 2, E = 8, T = 32, BZ = G::BZ, NIN = 6;
-  static_assert(M == E * T, "one warp per line: NX = 512");
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  unsigned char *stage = sm;
-  unsigned char *obuf = sm + G::off_out;
-  C *tw = reinterpret_cast<C *>(sm + G::off_tw);
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + G::off_bar);
-  uint64_t *never = full + STAGES;  // never completed (fault-injection wait)
-  unsigned *cnt = reinterpret_cast<unsigned *>(full + STAGES + 1);
-  int *last_issued = reinterpret_cast<int *>(cnt + STAGES);
-  const int tid = threadIdx.x, lane = tid & 31, l = tid >> 5;
-  C *xw = reinterpret_cast<C *>(sm + G::off_xw) + (size_t)l * M;
-  const int nzb = nz / BZ;
-  const int ntiles = nzb * ny * nruns;
-  const size_t rowstride = (size_t)nz * ny;
-  if (tid == 0) {
-    mbar_init(never, 1);
-    for (int q = 0; q < STAGES; ++q) {
-      mbar_init(&full[q], 1);
-      cnt[q] = 0;
-      last_issued[q] = -1;
-    }
-    fence_barrier_init();
-  }
-  for (int e = tid; e < NX; e += 256) tw[e] = twg[e];
-  __syncthreads();
-  // load L = k*NIN + f: field f of this CTA's k-th tile into slot L % STAGES
-  auto issue = [&](int L) {
-    const int k = L / NIN, f = xw_field(L - k * NIN);
-    const int tile = blockIdx.x + k * gridDim.x;
-    if (tile >= ntiles) return;
-    const int s = L % STAGES;
-    fence_proxy_async();
-    mbar_arrive_expect_tx(&full[s], (uint32_t)(nbox * rb) * 64u);
-    unsigned char *dst = stage + (size_t)s * G::in_bytes;
-    for (int q = 0; q < nbox; ++q)
-      tma_load_3d(dst + (size_t)q * rb * 64, &maps.m[f], (tile % nzb) * BZ, (tile / nzb) % ny,
-                  (tile / nzb / ny) * nxh + q * rb, &full[s]);
-    last_issued[s] = L;
-  };
-  if (tid == 0)
-    for (int L = 0; L < STAGES; ++L) issue(L);
-  auto buf = [xw](int idx) -> C & { return xw[xw_line_swz(idx)]; };
-  auto wsync = [] { __syncwarp(); };
-  bool failed = false;
-  int nout = 0;  // outputs staged so far (selects the output buffer)
-  const int src = (32 - lane) & 31;
-  const bool l0 = lane == 0;
-
-  // complex-to-real line of load L into x (x[e] = (r_{2m}, r_{2m+1}), m = t + 32e)
-  auto inverse = [&](int L, C(&x)[E]) {
-    const int s = L % STAGES;
-    const uint32_t par = (uint32_t)(L / STAGES) & 1u;
-    const bool got = (!ctl.stall || L > 0 || injected_stall_wait(never, ctl.cap)) && mbar_wait(&full[s], par, ctl.cap);
-    if (!got) {
-      // the CTA gives up at its next output barrier; until then the
-      // schedule goes on, and the slot's load is waited for (bounded) so
-      // that its refill never lands on a copy still in flight
-      failed = true;
-      mbar_wait(&full[s], par, kDrainPolls);
-    }
-    const unsigned char *tb = stage + (size_t)s * G::in_bytes + xw_tile_off(lane, l);
-#pragma unroll
-    for (int e = 0; e < E; ++e)  // row lane + 32e sits 2048e bytes after row lane
-      x[e] = lane + T * e < rows ? *reinterpret_cast<const C *>(tb + 2048 * e) : mk(0.f, 0.f);
-    const C xM = (l0 && M < rows) ? *reinterpret_cast<const C *>(tb - xw_tile_off(0, l) + xw_tile_off(M, l))
-                                  : mk(0.f, 0.f);
-    // every lane has read the slot: the last warp to get here refills it
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();
-      const unsigned old = atomicAdd(&cnt[s], 1u);
-      if (old % BZ == BZ - 1) {
-        __threadfence_block();
-        issue(L + STAGES);
-      }
-    }
-    // pack in pairs (e, 7-e).  X_{M-k} for k = t + 32e is register 7-e of
-    // lane 32-t; lane 0 takes it from its own register 8-e (X_M for e = 0),
-    // reading each before the pair that overwrites it (carry).
-    C carry = xM;
-#pragma unroll
-    for (int e = 0; e < E / 2; ++e) {
-      const C a = x[e], b = x[E - 1 - e];
-      const C pa = shfl2(b, src), pb = shfl2(a, src);
-      C xa = a, ma = l0 ? carry : pa;
-      const C mb = l0 ? (e == E / 2 - 1 ? b : x[e + 1]) : pb;
-      carry = b;
-      if (e == 0 && l0) {  // k = 0: real parts of X_0 and X_M
-        xa.y = 0.f;
-        ma.y = 0.f;
-      }
-      x[e] = xw_pack(xa, ma, tw[lane + T * e]);
-      x[E - 1 - e] = xw_pack(b, mb, tw[lane + T * (E - 1 - e)]);
-    }
-    line_fft<C, M, E, +1, 2>(x, lane, tw, buf, wsync);
-  };
-
-  // real-to-complex line of p, unpacked into the output tile; after a CTA
-  // barrier the tile is copied out to component c.  False: the CTA stops.
-  auto forward = [&](C(&p)[E], int c, int zb, int jy, int run) -> bool {
-    line_fft<C, M, E, -1, 2>(p, lane, tw, buf, wsync);
-    unsigned char *ob = obuf + (size_t)(nout & 1) * G::out_bytes;
-    unsigned char *ob0 = ob + xw_tile_off(lane, l);
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int kk = lane + T * e;
-      const C mine = l0 ? p[(8 - e) & 7] : p[7 - e];
-      const C zm = shfl2(mine, src);  // Z_{(M-k) mod M}
-      if (kk < rows) *reinterpret_cast<C *>(ob0 + 2048 * e) = r2c_unpack(p[e], zm, tw[kk]);
-      if (kk == 0 && M < rows)
-        *reinterpret_cast<C *>(ob0 - xw_tile_off(0, l) + xw_tile_off(M, l)) = r2c_unpack(p[e], zm, mk(-1.f, 0.f));
-    }
-    ++nout;
-    if (__syncthreads_or(failed)) {
-      if (tid == 0) {
-        record_timeout(ctl.status);
-        for (int q = 0; q < STAGES; ++q) {
-          const int Li = last_issued[q];
-          if (Li >= 0) mbar_wait(&full[q], (uint32_t)(Li / STAGES) & 1u, kDrainPolls);
-        }
-      }
-      return false;
-    }
-    // thread tid copies 16-byte chunk tid % 4 of rows tid/4, tid/4 + 64, ...;
-    // (row >> 1) & 3 and so the chunk's swizzled place repeat every 64 rows
-    const int orows = rows < M + 1 ? rows : M + 1;
-    const int kr0 = tid >> 2, part = tid & 3;
-    const unsigned char *op = ob + (kr0 << 6) + (((unsigned)part ^ ((unsigned)(kr0 >> 1) & 3u)) << 4);
-    float4 *gp = reinterpret_cast<float4 *>(out.p[c] + (size_t)zb * BZ + (size_t)nz * jy +
-                                            rowstride * ((size_t)run * nxh + kr0) + 2 * part);
-    const size_t gstep = rowstride * 64 / 2;  // 64 rows, in float4 units
-#pragma unroll 1
-    for (int kr = kr0; kr < orows; kr += 64, op += 4096, gp += gstep) *gp = *reinterpret_cast<const float4 *>(op);
-    return true;
-  };
-
-  for (int k = 0;; ++k) {
-    const int tile = blockIdx.x + k * gridDim.x;
-    if (tile >= ntiles) break;
-    const int zb = tile % nzb, jy = (tile / nzb) % ny, run = tile / nzb / ny;
-    const int L0 = k * NIN;
-    // (w x v)_x = wy vz - wz vy ; (w x v)_y = wz vx - wx vz ; (w x v)_z = wx vy - wy vx
-    // (prodre3), times 1/(nx ny nz)^2
-    C vx[E], vy[E], wx[E], wy[E], x[E];
-    inverse(L0 + 0, vx);
-    inverse(L0 + 1, vy);
-    inverse(L0 + 2, wx);
-    inverse(L0 + 3, x);  // wy
-    {
-      C pz[E];
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        pz[e] = mk(wx[e].x * vy[e].x, wx[e].y * vy[e].y);
-        pz[e] = mk((pz[e].x - vx[e].x * x[e].x) * scale, (pz[e].y - vx[e].y * x[e].y) * scale);
-        wy[e] = x[e];
-      }
-      if (!forward(pz, 2, zb, jy, run)) return;
-    }
-    C px[E], py[E];
-    inverse(L0 + 4, x);  // vz
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      px[e] = mk(x[e].x * wy[e].x, x[e].y * wy[e].y);
-      py[e] = mk(-(x[e].x * wx[e].x), -(x[e].y * wx[e].y));
-    }
-    inverse(L0 + 5, x);  // wz
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      px[e] = mk((px[e].x - vy[e].x * x[e].x) * scale, (px[e].y - vy[e].y * x[e].y) * scale);
-      py[e] = mk((x[e].x * vx[e].x + py[e].x) * scale, (x[e].y * vx[e].y + py[e].y) * scale);
-    }
-    if (!forward(px, 0, zb, jy, run)) return;
-    if (!forward(py, 1, zb, jy, run)) return;
-  }
-}
-
 
 // ====================================================================
 // Plain x transforms (fftp3d_real_to_complex / fftp3d_complex_to_real,
