@@ -358,9 +358,9 @@ template <typename R, int N, int BZ0> constexpr int y_tile_width() {
   return bz;
 }
 
-template <typename R, int N, int S, int BZ0, bool DUAL = false>
+template <typename R, int N, int S, int BZ0, bool DUAL = false, int E0 = 8>
 int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
-  constexpr int E = N < 8 ? N : 8, T = N / E;
+  constexpr int E = N < E0 ? N : E0, T = N / E;
   constexpr int BZ = y_tile_width<R, N, BZ0>();
   using G = YGeom<R, N, E, BZ, DUAL>;
   constexpr int STAGES = DUAL ? 2 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
@@ -392,6 +392,14 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   constexpr bool fits16 = YGeom<R, N, E, BZ16>::smem_bytes(2) <= 227 * 1024;
   if constexpr (fits16) {
     if ((c->tile_cfg & 1) && c->nz >= 16) return launch_y_cfg<R, N, S, 16>(c, f, nf, pr);
+  }
+  // bit 4 (FP32, lines of 256 points or more): 16 values per thread, two
+  // radix-8 butterflies per stage, half the threads per line
+  if constexpr (sizeof(R) == 4 && N >= 256) {
+    if (c->tile_cfg & 16) {
+      if (c->tile_cfg & 8) return launch_y_cfg<R, N, S, 8, true, 16>(c, f, nf, pr);
+      return launch_y_cfg<R, N, S, 8, false, 16>(c, f, nf, pr);
+    }
   }
   // bit 3: two stages and a second exchange buffer (one barrier per exchange)
   constexpr bool fits_dual = YGeom<R, N, E, 8, true>::smem_bytes(2) <= 113 * 1024;
@@ -1216,8 +1224,9 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->nu_run = nullptr;
   // the fastest variants measured for 512-point lines (ghost_hd_autotune
   // re-measures): two-stage z ring with three CTAs per SM, two-stage y ring
-  // with a second exchange buffer (FP32; FP64 tiles do not fit it)
-  c->tile_cfg = (nz >= 256 ? 6 : 0) | (ny >= 256 ? 8 : 0);
+  // with a second exchange buffer, and for FP32 y passes with 16 values per
+  // thread
+  c->tile_cfg = (nz >= 256 ? 6 : 0) | (ny >= 256 ? (precision == GHOST_SINGLE ? 24 : 8) : 0);
   const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
   c->cbytes = c->nspec * 2 * rs;
   c->rbytes = c->nreal * rs;
@@ -1702,11 +1711,11 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
 // Tile variants tried by the autotuners (bit 0: y tiles 16 z-lines wide;
 // bit 1: z CTAs of 128 threads; bits 1 and 2: two-stage z ring, three CTAs
 // per SM; bit 3: two-stage y ring with a second exchange buffer).
-static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14};
+static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30};
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 15) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..15", cfg);
+  if (cfg < 0 || cfg > 31) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..31", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }

@@ -94,10 +94,13 @@ template <int R, int S, typename C> __device__ __forceinline__ void dftR(C (&v)[
   }
 }
 
-// radix of the stage with span L for an N-point transform, E per thread
+// radix of the stage with span L for an N-point transform, E per thread:
+// E (at most 8, the largest in-register DFT; with E = 16 a thread runs two
+// radix-8 butterflies per stage), or the remainder 2/4 for the last stage
 template <int N, int E, int L> struct stage_radix {
   static constexpr int rem = N / L;
-  static constexpr int value = (rem % E == 0) ? E : rem;
+  static constexpr int RM = E < 8 ? E : 8;
+  static constexpr int value = (rem % RM == 0) ? RM : rem;
 };
 
 // Butterflies of one stage.  Writes outputs to `dst(idx, val)` unless this

@@ -396,7 +396,7 @@ def test_ensemble_graph_steps_match_oracle(prec):
     ens = Ensemble(sizes, nruns, precision=prec)
     ens.init(seeds, nus)
     cfg = ens.autotune(2, 1e-3)
-    assert len(cfg) == 2 and all(c in (0, 1, 2, 3, 6, 7, 8, 14) for c in cfg)
+    assert len(cfg) == 2 and all(c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30) for c in cfg)
     ens.run(4, 2, 1e-3)
     e = ens.energy(1)
     tol = 1e-12 if prec == "fp64" else 1e-5
@@ -427,10 +427,10 @@ def test_tile_variants_are_bitwise_identical(prec):
     g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *F)
     keep = [x.clone() for x in V0]
     cfg = g.hd_autotune(4, 5e-4, 1e-3, *V0, *F)
-    assert cfg in (0, 1, 2, 3, 6, 7, 8, 14)
+    assert cfg in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30)
     assert all(torch.equal(a, b) for a, b in zip(V0, keep))
     ref = None
-    for c in (0, 1, 2, 3, 6, 7, 8, 14):
+    for c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 30):
         g.set_tile_cfg(c)
         V = [x.clone() for x in keep]
         g.hd_run(2, 4, 5e-4, 1e-3, *V, *F)
@@ -438,6 +438,29 @@ def test_tile_variants_are_bitwise_identical(prec):
             ref = V
         else:
             assert all(torch.equal(a, b) for a, b in zip(V, ref)), c
+
+
+def test_wide_line_variants_at_512():
+    """The FP32 y passes with 16 values per thread (bit 4), alone and with the
+    other variants, give the same bits as the 8-value passes over unpruned
+    and pruned substeps, and match the oracle."""
+    import torch
+    shape = (64, 256, 512)
+    o = Oracle(*shape)
+    v0, _ = o.random_solenoidal(51, 1.0, 10.0, 1, 1.0)
+    f, _ = o.random_solenoidal(52, 2.0, 3.0, 0, 1.0)
+    g = ghost(*shape, precision="fp32")
+    F = [to_dev(x.astype(np.complex64)) for x in f]
+    out = {}
+    for c in (0, 14, 16, 24, 30):
+        g.set_tile_cfg(c)
+        V = [to_dev(x.astype(np.complex64)) for x in v0]
+        g.hd_run(2, 4, 5e-4, 1e-3, *V, *F)
+        out[c] = V
+    for c in (14, 16, 24, 30):
+        assert all(torch.equal(a, b) for a, b in zip(out[c], out[0])), c
+    ref = o.hd_run(2, 4, 5e-4, 1e-3, v0, f)
+    assert rel_l2([to_host(x) for x in out[30]], ref) <= 1e-5
 
 
 @pytest.mark.parametrize("shape", [(1024, 16, 16), (16, 1024, 16), (16, 16, 1024)])
