@@ -5,6 +5,7 @@ C ABI of include/ghost_b200.h); this package is the host-side mirror of
 GHOST's fftp / pseudospec3D interface over that ABI.
 """
 from ._lib import GhostError, load  # noqa: F401
-from .pseudospec import GHOST_COMPLEX_TO_REAL, GHOST_REAL_TO_COMPLEX, Ensemble, FFTPlan, Ghost  # noqa: F401
+from .pseudospec import GHOST_COMPLEX_TO_REAL, GHOST_REAL_TO_COMPLEX, Ensemble, FFTPlan, Ghost, io_filename  # noqa: F401
 
-__all__ = ["Ghost", "Ensemble", "FFTPlan", "GhostError", "load", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL"]
+__all__ = ["Ghost", "Ensemble", "FFTPlan", "GhostError", "load", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL",
+           "io_filename"]

@@ -15,7 +15,7 @@ GHOST_OK = 0
 TIMER_NAMES = ["z_inv", "y_inv", "x_nl", "y_fwd", "z_fwd", "z_c2c", "x_c2r", "x_r2c", "pointwise", "reduce"]
 ERRORS = {
     1: "GHOST_ERR_ARG", 2: "GHOST_ERR_SIZE", 3: "GHOST_ERR_ALLOC", 4: "GHOST_ERR_CUDA",
-    5: "GHOST_ERR_TIMEOUT", 6: "GHOST_ERR_NAN", 7: "GHOST_ERR_STATE", 8: "GHOST_ERR_NODEV",
+    5: "GHOST_ERR_TIMEOUT", 6: "GHOST_ERR_NAN", 7: "GHOST_ERR_STATE", 8: "GHOST_ERR_NODEV", 9: "GHOST_ERR_IO",
 }
 GHOST_SINGLE = 4
 GHOST_DOUBLE = 8
@@ -123,6 +123,11 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_io_filename": [ctypes.c_char_p, ctypes.c_char_p, I, I, ctypes.c_char_p, ctypes.c_size_t],
+    "ghost_io_write": [P, P, ctypes.c_char_p, I],
+    "ghost_io_read": [P, ctypes.c_char_p, I, P],
+    "ghost_io_output": [P, P, ctypes.c_char_p, I],
+    "ghost_io_restart": [P, ctypes.c_char_p, I, P],
 }
 
 _lib = None

@@ -512,6 +512,41 @@
          REAL(C_DOUBLE) :: tve(*), tepq(*), ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_io_filename(dir,name,idx,width,buf,buflen) BIND(C,name="ghost_io_filename") RESULT(s)
+         IMPORT :: C_INT, C_CHAR, C_SIZE_T
+         CHARACTER(KIND=C_CHAR) :: dir(*), name(*), buf(*)
+         INTEGER(C_INT), VALUE :: idx, width
+         INTEGER(C_SIZE_T), VALUE :: buflen
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_io_write(ctx,var,path,swap) BIND(C,name="ghost_io_write") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_CHAR
+         TYPE(C_PTR), VALUE :: ctx, var
+         CHARACTER(KIND=C_CHAR) :: path(*)
+         INTEGER(C_INT), VALUE :: swap
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_io_read(ctx,path,swap,var) BIND(C,name="ghost_io_read") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_CHAR
+         TYPE(C_PTR), VALUE :: ctx, var
+         CHARACTER(KIND=C_CHAR) :: path(*)
+         INTEGER(C_INT), VALUE :: swap
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_io_output(ctx,spec,path,swap) BIND(C,name="ghost_io_output") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_CHAR
+         TYPE(C_PTR), VALUE :: ctx, spec
+         CHARACTER(KIND=C_CHAR) :: path(*)
+         INTEGER(C_INT), VALUE :: swap
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_io_restart(ctx,path,swap,spec) BIND(C,name="ghost_io_restart") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_CHAR
+         TYPE(C_PTR), VALUE :: ctx, spec
+         CHARACTER(KIND=C_CHAR) :: path(*)
+         INTEGER(C_INT), VALUE :: swap
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_evedqnm(n,prec,kmax,kolmo,eold,nu,time,tepq,tve,ext) BIND(C,name="ghost_evedqnm") RESULT(s)
          IMPORT :: C_INT, C_DOUBLE
          INTEGER(C_INT), VALUE :: n, prec
@@ -737,3 +772,41 @@
       CALL ghost_gpu_check(ghost_spectrumc(gctx,C_LOC(a),C_LOC(b),C_LOC(c),kin,hel, &
                            Ektot,Hktot),'spectrumc')
       END SUBROUTINE spectrumc
+
+!-----------------------------------------------------------------
+! io_write / io_read (mpiio/binary_io.f90:13-186) for a single-rank
+! run (ksta = 1, kend = nz): the file name is GHOST's mangled
+! dir/fname.nmb.out; reads byte-swap when iswap > 0, as GHOST's do.
+!-----------------------------------------------------------------
+      SUBROUTINE io_write(unit,dir,fname,nmb,plan,var)
+      USE fprecision
+      USE iovar
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(IOPLAN), INTENT(IN) :: plan
+      REAL(KIND=GP), INTENT(INOUT), TARGET :: var(plan%nx,plan%ny,plan%ksta:plan%kend)
+      INTEGER, INTENT(IN) :: unit
+      CHARACTER(len=100), INTENT(IN) :: dir
+      CHARACTER(len=*), INTENT(IN) :: nmb
+      CHARACTER(len=*), INTENT(IN) :: fname
+      CALL ghost_gpu_check(ghost_io_write(gctx,C_LOC(var), &
+           trim(dir)//'/'//fname//'.'//nmb//'.out'//C_NULL_CHAR,0),'io_write')
+      END SUBROUTINE io_write
+
+      SUBROUTINE io_read(unit,dir,fname,nmb,plan,var)
+      USE fprecision
+      USE iovar
+      USE ghost_gpu
+      IMPLICIT NONE
+      TYPE(IOPLAN), INTENT(IN) :: plan
+      REAL(KIND=GP), INTENT(OUT), TARGET :: var(plan%nx,plan%ny,plan%ksta:plan%kend)
+      INTEGER, INTENT(IN) :: unit
+      CHARACTER(len=100), INTENT(IN) :: dir
+      CHARACTER(len=*), INTENT(IN) :: nmb
+      CHARACTER(len=*), INTENT(IN) :: fname
+      INTEGER(C_INT) :: swap
+      swap = 0
+      IF (iswap.gt.0) swap = 1
+      CALL ghost_gpu_check(ghost_io_read(gctx, &
+           trim(dir)//'/'//fname//'.'//nmb//'.out'//C_NULL_CHAR,swap,C_LOC(var)),'io_read')
+      END SUBROUTINE io_read

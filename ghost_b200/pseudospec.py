@@ -14,6 +14,7 @@ column-major layouts written as C-order shapes:
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -126,6 +127,27 @@ class Ghost:
                 raise ValueError(f"expected C-contiguous {np.dtype(want)} {shape}, got {x.dtype} {x.shape}")
             return ctypes.c_void_p(x.ctypes.data)
         raise TypeError(f"unsupported array type {type(x)}")
+
+    # ---- GHOST's binary field files (mpiio/binary_io.f90)
+    def io_write(self, real, path: str, swap: bool = False):
+        """io_write: a real field (nz, ny, nx), x fastest, to a raw GP file."""
+        check(self.lib.ghost_io_write(self.h, self._ptr(real, "r"), os.fsencode(path), int(swap)), "ghost_io_write")
+
+    def io_read(self, path: str, out=None, swap: bool = False):
+        """io_read: a raw GP file of nx*ny*nz values into a real field."""
+        out = self.rzeros() if out is None else out
+        check(self.lib.ghost_io_read(self.h, os.fsencode(path), int(swap), self._ptr(out, "r")), "ghost_io_read")
+        return out
+
+    def io_output(self, spec, path: str, swap: bool = False):
+        """One field of GHOST's output step: the real field of spec/(nx ny nz)."""
+        check(self.lib.ghost_io_output(self.h, self._ptr(spec, "c"), os.fsencode(path), int(swap)), "ghost_io_output")
+
+    def io_restart(self, path: str, out=None, swap: bool = False):
+        """One field of GHOST's restart: io_read, then the forward transform."""
+        out = self.czeros() if out is None else out
+        check(self.lib.ghost_io_restart(self.h, os.fsencode(path), int(swap), self._ptr(out, "c")), "ghost_io_restart")
+        return out
 
     def set_tile_cfg(self, cfg: int):
         check(self.lib.ghost_ctx_set_tile_cfg(self.h, int(cfg)), "ghost_ctx_set_tile_cfg")
@@ -395,3 +417,11 @@ def _tensor_view(ptr: int, shape, dtype):
 
 
 __all__ = ["Ghost", "Ensemble", "FFTPlan", "GHOST_REAL_TO_COMPLEX", "GHOST_COMPLEX_TO_REAL"]
+
+
+def io_filename(dir: str, name: str, index: int, width: int = 4) -> str:
+    """GHOST's field file name "<dir>/<name>.NNNN.out" (fmtext '(i4.4)')."""
+    buf = ctypes.create_string_buffer(4096)
+    check(_lib.load().ghost_io_filename(os.fsencode(dir), os.fsencode(name), index, width, buf, len(buf)),
+          "ghost_io_filename")
+    return os.fsdecode(buf.value)

@@ -48,6 +48,7 @@ extern "C" {
 #define GHOST_ERR_NAN 6     /* non-finite value detected by a checked call */
 #define GHOST_ERR_STATE 7   /* call not valid in the current state */
 #define GHOST_ERR_NODEV 8   /* no usable CUDA device */
+#define GHOST_ERR_IO 9      /* a field file could not be opened, read or written */
 
 /* precision (GHOST's GP kind values) */
 #define GHOST_SINGLE 4
@@ -417,6 +418,29 @@ int ghost_les_edqnm_last(ghost_les *les, double *tve, double *tepq, double *Ek);
  * kind for the fit and quadrature (GHOST_SINGLE or GHOST_DOUBLE) */
 int ghost_evedqnm(int n, int precision, double kmax, double kolmo, const double *Eold, double nu, double time,
                   double *tepq, double *tve, double *Ext);
+
+/* ------------------------------------------------------------------
+ * GHOST's binary field files (mpiio/binary_io.f90:13-186): one raw file
+ * per field holding r(nx,ny,nz) in Fortran order (x fastest), GP precision
+ * (the context's), native byte order, no header.  swap != 0 reverses the
+ * bytes of every value (GHOST's iswap / oswap).  Fields may be device or
+ * host arrays.  Batched contexts: GHOST_ERR_STATE (one file per run).
+ * ------------------------------------------------------------------ */
+/* "<dir>/<name>.<index>.out", index zero-padded to width digits (GHOST's
+ * fmtext '(i4.4)' is width 4; a wider index prints as width asterisks) */
+int ghost_io_filename(const char *dir, const char *name, int index, int width, char *buf, size_t len);
+/* io_write(unit,dir,fname,nmb,plan,var): a real field to path */
+int ghost_io_write(ghost_ctx *ctx, const void *real, const char *path, int swap);
+/* io_read(unit,dir,fname,nmb,plan,var): path (exactly nx*ny*nz values,
+ * else GHOST_ERR_SIZE) into a real field */
+int ghost_io_read(ghost_ctx *ctx, const char *path, int swap, void *real);
+/* one field of GHOST's output step (main3D.fpp:2678-2709): the real field
+ * of spec/(nx ny nz) (fftp3d_complex_to_real), written as io_write does;
+ * spec is left unmodified */
+int ghost_io_output(ghost_ctx *ctx, const void *spec, const char *path, int swap);
+/* one field of GHOST's restart (main3D.fpp:2155-2161): io_read, then
+ * fftp3d_real_to_complex into spec (so output then restart gives spec back) */
+int ghost_io_restart(ghost_ctx *ctx, const char *path, int swap, void *spec);
 
 #ifdef __cplusplus
 }
