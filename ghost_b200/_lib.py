@@ -123,6 +123,8 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_entrans": [P, P, P, P, P, P, P, I, PD],
+    "ghost_heltrans": [P, P, P, P, P, P, P, I, PD],
     "ghost_io_filename": [ctypes.c_char_p, ctypes.c_char_p, I, I, ctypes.c_char_p, ctypes.c_size_t],
     "ghost_io_write": [P, P, ctypes.c_char_p, I],
     "ghost_io_read": [P, ctypes.c_char_p, I, P],

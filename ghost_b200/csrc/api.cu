@@ -876,14 +876,18 @@ int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void 
   return check_status(c);
 }
 
+// Shell-binned sums of a reduction term over two field triplets (the
+// transfer spectra of entrans / heltrans); spectrum_dev is its one-triplet form.
 template <typename R>
-int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host) {
+int spectrum6_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, double *out_host) {
   const size_t n = c->ntot;
   const int nbins = c->nmax / 2 + 1;
   const int nblk = std::min(grid1d(n), 148 * 4);
   double *part;
   GB_CHECK(partials(c, (size_t)(nblk + 1) * nbins, &part));
-  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, (const cx<R> *)d, (const cx<R> *)e,
+                (const cx<R> *)f};
   const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
   GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
@@ -896,6 +900,11 @@ int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const voi
   GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * nbins, cudaMemcpyDeviceToHost, c->stream));
   GB_CUDA(cudaStreamSynchronize(c->stream));
   return GHOST_OK;
+}
+
+template <typename R>
+int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, double *out_host) {
+  return spectrum6_dev<R>(c, kind, a, b, cc, nullptr, nullptr, nullptr, out_host);
 }
 
 // The same shell spectrum left on the device (out_dev[nmax/2+1]); no
@@ -1569,6 +1578,38 @@ int ghost_spectrumc(ghost_ctx *c, const void *a, const void *b, const void *cc, 
     GB_CHECK(sp ? spectrum_dev<float>(c, RED_HELICITY, da, db, dc, Hk)
                 : spectrum_dev<double>(c, RED_HELICITY, da, db, dc, Hk));
   return st.finish();
+}
+
+// entrans / heltrans (pseudospec3D_hd.f90:1629-1949): the shell-binned
+// transfer Re(x . conj(d,e,f))/(nx ny nz)^2, x = (a,b,c) (times kk2 when
+// entrans' kin is 0) or curl(a,b,c) for heltrans; GHOST's Ektot / Hktot.
+static int transfer(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d,
+                    const void *e, const void *f, double *out) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e || !f || !out) return fail(GHOST_ERR_ARG, "null argument");
+  Staging st(c);
+  const void *da, *db, *dc, *dd, *de, *df;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(st.map(d, c->cbytes, 1, &dd));
+  GB_CHECK(st.map(e, c->cbytes, 1, &de));
+  GB_CHECK(st.map(f, c->cbytes, 1, &df));
+  GB_CHECK(c->precision == GHOST_SINGLE ? spectrum6_dev<float>(c, kind, da, db, dc, dd, de, df, out)
+                                        : spectrum6_dev<double>(c, kind, da, db, dc, dd, de, df, out));
+  return st.finish();
+}
+
+int ghost_entrans(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, int kin, double *Ek) {
+  if (kin < 0 || kin > 4) return fail(GHOST_ERR_ARG, "kin %d not in 0..4", kin);
+  return transfer(c, kin == 0 ? RED_CROSS_K2 : RED_CROSS, a, b, cc, d, e, f, Ek);
+}
+
+int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                   const void *f, int kin, double *Hk) {
+  if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
+  return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
 }
 
 int ghost_hdcheck(ghost_ctx *c, const void *vx, const void *vy, const void *vz, const void *fx, const void *fy,

@@ -120,7 +120,7 @@ __global__ void scale3_kernel(cx<R> *x, cx<R> *y, cx<R> *z, size_t n, R f0, doub
 // pseudospec3D_hd.f90:550-567).  Per-block partials in a fixed grid, then
 // one block sums them in a fixed tree: bitwise reproducible.
 enum RedKind { RED_ENERGY = 0, RED_ENSTROPHY = 1, RED_LAPLACIAN = 2, RED_HELICITY = 3, RED_CROSS = 4,
-               RED_CROSS_K2 = 5, RED_DIVERGENCE = 6 };
+               RED_CROSS_K2 = 5, RED_DIVERGENCE = 6, RED_CURL_CROSS = 7 };
 
 template <typename R> struct RedArgs {
   const cx<R> *a, *b, *c, *d, *e, *f;
@@ -154,6 +154,12 @@ __device__ __forceinline__ R red_term(const KParams<R> &kp, const RedArgs<R> &ra
       R s = cmulc(va, vd).x + cmulc(vb, ve).x + cmulc(vc, vf).x;
       if (kind == RED_CROSS_K2) s = s * kk2_of(kp, i, j, k);
       return s * kp.tmp;
+    }
+    case RED_CURL_CROSS: {  // heltrans: Re(curl(a,b,c) . conj(d,e,f))
+      const C w1 = curl_at(kp, 1, i, j, k, va, vb, vc), w2 = curl_at(kp, 2, i, j, k, va, vb, vc),
+              w3 = curl_at(kp, 3, i, j, k, va, vb, vc);
+      const C vd = ra.d[p], ve = ra.e[p], vf = ra.f[p];
+      return (cmulc(w1, vd).x + cmulc(w2, ve).x + cmulc(w3, vf).x) * kp.tmp;
     }
     default: {  // RED_DIVERGENCE
       const C s = cadd(cadd(ik(kx_of(kp, i), va), ik(ky_of(kp, j), vb)), ik(kz_of(kp, k), vc));

@@ -512,6 +512,20 @@
          REAL(C_DOUBLE) :: tve(*), tepq(*), ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_entrans(ctx,a,b,c,d,e,f,kin,ek) BIND(C,name="ghost_entrans") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_heltrans(ctx,a,b,c,d,e,f,kin,hk) BIND(C,name="ghost_heltrans") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_io_filename(dir,name,idx,width,buf,buflen) BIND(C,name="ghost_io_filename") RESULT(s)
          IMPORT :: C_INT, C_CHAR, C_SIZE_T
          CHARACTER(KIND=C_CHAR) :: dir(*), name(*), buf(*)
@@ -810,3 +824,63 @@
       CALL ghost_gpu_check(ghost_io_read(gctx, &
            trim(dir)//'/'//fname//'.'//nmb//'.out'//C_NULL_CHAR,swap,C_LOC(var)),'io_read')
       END SUBROUTINE io_read
+
+!-----------------------------------------------------------------
+! entrans / heltrans (pseudospec3D_hd.f90:1629-1949): the shell sums
+! on the device, GHOST's text file (Dkk*k, sum/Dkk) written here.
+!-----------------------------------------------------------------
+      SUBROUTINE entrans(a,b,c,d,e,f,nmb,kin)
+      USE fprecision
+      USE grid
+      USE kes
+      USE boxsize
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET, DIMENSION(nz,ny,nx/2+1) :: a,b,c,d,e,f
+      INTEGER, INTENT(IN) :: kin
+      CHARACTER(len=*), INTENT(IN) :: nmb
+      DOUBLE PRECISION, DIMENSION(nmax/2+1) :: Ektot
+      INTEGER :: i
+      CALL ghost_gpu_check(ghost_entrans(gctx,C_LOC(a),C_LOC(b),C_LOC(c),C_LOC(d),C_LOC(e), &
+                           C_LOC(f),kin,Ektot),'entrans')
+      IF (kin.eq.0) THEN
+         OPEN(1,file='mtransfer.' // nmb // '.txt')
+      ELSEIF (kin.eq.1) THEN
+         OPEN(1,file='ktransfer.' // nmb // '.txt')
+      ELSEIF (kin.eq.2) THEN
+         OPEN(1,file='jtransfer.' // nmb // '.txt')
+      ELSEIF (kin.eq.3) THEN
+         OPEN(1,file='mcrostran.' // nmb // '.txt')
+      ELSE
+         OPEN(1,file='kcrostran.' // nmb // '.txt')
+      ENDIF
+      DO i = 1,nmax/2+1
+         WRITE(1,FMT='(E13.6,E23.15)') Dkk*i,Ektot(i)/Dkk
+      END DO
+      CLOSE(1)
+      END SUBROUTINE entrans
+
+      SUBROUTINE heltrans(a,b,c,d,e,f,nmb,kin)
+      USE fprecision
+      USE grid
+      USE kes
+      USE boxsize
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET, DIMENSION(nz,ny,nx/2+1) :: a,b,c,d,e,f
+      INTEGER, INTENT(IN) :: kin
+      CHARACTER(len=*), INTENT(IN) :: nmb
+      DOUBLE PRECISION, DIMENSION(nmax/2+1) :: Hktot
+      INTEGER :: i
+      CALL ghost_gpu_check(ghost_heltrans(gctx,C_LOC(a),C_LOC(b),C_LOC(c),C_LOC(d),C_LOC(e), &
+                           C_LOC(f),kin,Hktot),'heltrans')
+      IF (kin.eq.0) THEN
+         OPEN(1,file='hmtransfer.' // nmb // '.txt')
+      ELSE
+         OPEN(1,file='hktransfer.' // nmb // '.txt')
+      ENDIF
+      DO i = 1,nmax/2+1
+         WRITE(1,FMT='(E13.6,E23.15)') Dkk*i,Hktot(i)/Dkk
+      END DO
+      CLOSE(1)
+      END SUBROUTINE heltrans

@@ -128,6 +128,20 @@ class Ghost:
             return ctypes.c_void_p(x.ctypes.data)
         raise TypeError(f"unsupported array type {type(x)}")
 
+    def entrans(self, a, b, c, d, e, f, kin: int = 1):
+        """entrans: GHOST's Ektot, the shell-binned transfer Re(v . conj(nl))."""
+        Ek = np.zeros(self.nmax // 2 + 1)
+        check(self.lib.ghost_entrans(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e, f)], kin,
+                                     Ek.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_entrans")
+        return Ek
+
+    def heltrans(self, a, b, c, d, e, f, kin: int = 1):
+        """heltrans: GHOST's Hktot, the shell-binned Re(curl v . conj(nl))."""
+        Hk = np.zeros(self.nmax // 2 + 1)
+        check(self.lib.ghost_heltrans(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e, f)], kin,
+                                      Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
+        return Hk
+
     # ---- GHOST's binary field files (mpiio/binary_io.f90)
     def io_write(self, real, path: str, swap: bool = False):
         """io_write: a real field (nz, ny, nx), x fastest, to a raw GP file."""

@@ -193,6 +193,18 @@ int ghost_maxabs(ghost_ctx *ctx, const void *a, const void *b, const void *c, do
  * when hel == 1 (Hk may then be NULL otherwise) */
 int ghost_spectrumc(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel,
                     double *Ek, double *Hk);
+/* entrans(a,b,c,d,e,f,nmb,kin) (pseudospec3D_hd.f90:1629-1820): the shell
+ * sums Ek[nmax/2+1] of Re(a.conj(d) + b.conj(e) + c.conj(f))/(nx ny nz)^2,
+ * times kk2 for kin = 0, doubled off the kx = 0 plane: GHOST's Ektot.  Its
+ * file (ktransfer.NNNN.txt for kin = 1 and the others by kin) holds
+ * (Dkk*k, Ek[k-1]/Dkk).  Ek is a host array. */
+int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                  const void *f, int kin, double *Ek);
+/* heltrans(a,b,c,d,e,f,nmb,kin) (pseudospec3D_hd.f90:1823-1949): the same
+ * with curl(a,b,c) in place of (a,b,c); kin only names GHOST's file
+ * (hmtransfer / hktransfer). */
+int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                   const void *f, int kin, double *Hk);
 /* ghost_spectrumc_noalloc: the same shell spectra as ghost_spectrumc,
  * computed without allocating any memory.  It has no counterpart in the
  * reference; it exists for callers that cannot let the library allocate:

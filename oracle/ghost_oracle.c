@@ -597,6 +597,45 @@ void o_spectrumc(const octx *c, const cplx *a, const cplx *b, const cplx *cc, in
   free(c1); free(c2); free(c3);
 }
 
+/* entrans (pseudospec3D_hd.f90:1629-1820): Ektot, the shell sums of
+ * w Re(a.conj d + b.conj e + c.conj f) tmp (times kk2 for kin = 0), w = 2 off
+ * the kx = 0 plane.  heltrans (:1823-1949) is the same with curl(a,b,c),
+ * through rotor3 as there (curl != 0 selects it). */
+static void o_transfer(const octx *c, const cplx *x, const cplx *y, const cplx *z, const cplx *d,
+                       const cplx *e, const cplx *f, int with_kk2, double *Ek) {
+  int nb = c->nmax / 2 + 1;
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  for (int q = 0; q < nb; ++q) Ek[q] = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        int kmn = (int)((real)sqrt(c->kk2[p]) / c->Dkk + (real)0.501f);
+        if (kmn > 0 && kmn <= nb) {
+          real s = cmul(x[p], cconj(d[p])).re + cmul(y[p], cconj(e[p])).re + cmul(z[p], cconj(f[p])).re;
+          if (with_kk2) s = c->kk2[p] * s;
+          Ek[kmn - 1] += (double)(w * s * tmp);
+        }
+      }
+  }
+}
+
+void o_entrans(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d, const cplx *e,
+               const cplx *f, int kin, double *Ek) {
+  o_transfer(c, a, b, cc, d, e, f, kin == 0, Ek);
+}
+
+void o_heltrans(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d, const cplx *e,
+                const cplx *f, double *Hk) {
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+  o_transfer(c, c1, c2, c3, d, e, f, 0, Hk);
+  free(c1); free(c2); free(c3);
+}
+
 /* ------------------------------------------------------------------ */
 /* Random numbers: randu of pseudo/pseudospec3D_mod.fpp:130-148.  am is the
  * default-REAL constant 1./im, which is 2^-31 in both precisions. */

@@ -63,6 +63,8 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_divergence": (D, [P, P, P, P]),
         "o_maxabs": (D, [P, P, P, P, I]),
         "o_spectrumc": (None, [P, P, P, P, I, I, P, P]),
+        "o_entrans": (None, [P, P, P, P, P, P, P, I, P]),
+        "o_heltrans": (None, [P, P, P, P, P, P, P, P]),
         "o_randu": (ctypes.c_double if precision == "fp64" else ctypes.c_float, [P]),
         "o_random_vpot": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, P, P, P]),
         "o_random_solenoidal": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, D, P, P, P]),
@@ -225,6 +227,20 @@ class Oracle:
         Hk = np.zeros(nb)
         self.lib.o_spectrumc(self.h, _ptr(a), _ptr(b), _ptr(c), kin, hel, _ptr(Ek), _ptr(Hk))
         return Ek, Hk
+
+    def entrans(self, a, b, c, d, e, f, kin=1):
+        """entrans: Ektot (shell sums of the transfer, pseudospec3D_hd.f90:1629-1820)."""
+        arrs = [self._c(x) for x in (a, b, c, d, e, f)]
+        Ek = np.zeros(self.nmax // 2 + 1)
+        self.lib.o_entrans(self.h, *[_ptr(x) for x in arrs], kin, _ptr(Ek))
+        return Ek
+
+    def heltrans(self, a, b, c, d, e, f):
+        """heltrans: Hktot, the same with curl(a,b,c) (:1823-1949)."""
+        arrs = [self._c(x) for x in (a, b, c, d, e, f)]
+        Hk = np.zeros(self.nmax // 2 + 1)
+        self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
+        return Hk
 
     def sharp(self, a, delta):
         a = self._c(a)

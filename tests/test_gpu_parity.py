@@ -478,3 +478,22 @@ def test_longest_lines(shape, prec):
     F = [to_dev(x.astype(cd)) for x in f]
     g.hd_run(1, 2, 1e-3, 1e-3, *V, *F)
     assert rel_l2([to_host(x) for x in V], ref) <= (1e-12 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 32, 16)])
+def test_transfer_spectra(prec, shape):
+    """entrans (kin 1 and 0) and heltrans against the oracle on unrelated
+    fields, and the zero total transfer of the nonlinear term."""
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    a = [rand_spectral(o, 70 + q) for q in range(6)]
+    A = [to_dev(x.astype(g.cdtype_np)) for x in a]
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    for kin in (1, 0):
+        assert rel_l2(g.entrans(*A, kin=kin), o.entrans(*a, kin=kin)) <= tol
+    assert rel_l2(g.heltrans(*A), o.heltrans(*a)) <= tol
+    v = solenoidal_ic(o, seed=71)
+    nl = o.prodre3(*v)
+    T = g.entrans(*[to_dev(x.astype(g.cdtype_np)) for x in (*v, *nl)], kin=1)
+    assert abs(T.sum()) <= (1e-11 if prec == "fp64" else 1e-5) * np.abs(T).sum()

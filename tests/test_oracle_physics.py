@@ -131,3 +131,23 @@ def test_spectrum_sums_to_energy():
     # shells beyond nmax/2+1 are dropped; the IC lives below N/3
     assert Ek.sum() == pytest.approx(o.energy(*v, 1), rel=1e-12)
     assert Hk.sum() == pytest.approx(o.helicity(*v), rel=1e-10, abs=1e-14)
+
+
+def test_transfer_spectra_identities():
+    """entrans / heltrans (pseudospec3D_hd.f90:1629-1949) on the oracle:
+    the nonlinear term moves energy and helicity between shells without
+    creating either (v.(w x v) = w.(w x v) = 0 at every grid point, so the
+    shell sums add up to zero), entrans of a field with itself is its
+    kinetic spectrum, and with kin = 0 its curl spectrum (solenoidal v)."""
+    o = Oracle(32)
+    v = solenoidal_ic(o, seed=7)
+    nl = o.prodre3(*v)
+    T = o.entrans(*v, *nl, kin=1)
+    H = o.heltrans(*v, *nl)
+    Ek, _ = o.spectrumc(*v, 1, 0)
+    Wk, _ = o.spectrumc(*v, 0, 0)
+    assert abs(T.sum()) <= 1e-12 * np.abs(T).sum()
+    assert abs(H.sum()) <= 1e-12 * np.abs(H).sum()
+    assert np.abs(T).sum() > 0 and np.abs(H).sum() > 0
+    assert rel_l2(o.entrans(*v, *v, kin=1), Ek) <= 1e-14
+    assert rel_l2(o.entrans(*v, *v, kin=0), Wk) <= 1e-12
