@@ -123,6 +123,12 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_specpara": [P, P, P, P, I, I, PD, PD],
+    "ghost_specperp": [P, P, P, P, I, I, PD, PD],
+    "ghost_entpara": [P, P, P, P, P, P, P, I, PD],
+    "ghost_entperp": [P, P, P, P, P, P, P, I, PD],
+    "ghost_heltpara": [P, P, P, P, P, P, P, I, PD],
+    "ghost_heltperp": [P, P, P, P, P, P, P, I, PD],
     "ghost_entrans": [P, P, P, P, P, P, P, I, PD],
     "ghost_heltrans": [P, P, P, P, P, P, P, I, PD],
     "ghost_io_filename": [ctypes.c_char_p, ctypes.c_char_p, I, I, ctypes.c_char_p, ctypes.c_size_t],

@@ -907,6 +907,32 @@ int spectrum_dev(ghost_ctx *c, int kind, const void *a, const void *b, const voi
   return spectrum6_dev<R>(c, kind, a, b, cc, nullptr, nullptr, nullptr, out_host);
 }
 
+// Anisotropic sums (aniso_kernel): out_host[3 nb] = total, horizontal, vertical.
+template <typename R>
+int aniso_dev(ghost_ctx *c, int kind, int mode, int nb, const void *a, const void *b, const void *cc, const void *d,
+              const void *e, const void *f, double *out_host) {
+  const size_t n = c->ntot;
+  const int nb3 = 3 * nb;
+  const int nblk = std::min(grid1d(n), 148 * 2);
+  double *part;
+  GB_CHECK(partials(c, (size_t)(nblk + 1) * nb3, &part));
+  RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, (const cx<R> *)d, (const cx<R> *)e,
+                (const cx<R> *)f};
+  const size_t smem = (size_t)(256 / 32) * nb3 * sizeof(double);
+  if (smem > 227 * 1024) return fail(GHOST_ERR_SIZE, "%d bins exceed the shared-memory histogram", nb);
+  GB_CUDA(cudaFuncSetAttribute(aniso_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
+  aniso_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, mode, n, nb, (R)c->Lz, (R)c->Dkk, part);
+  GB_CHECK(post_launch(c));
+  double *fin = part + (size_t)nblk * nb3;
+  finalize_kernel<<<1, 256, 0, c->stream>>>(part, nblk, nb3, fin);
+  timer_end(c, ts);
+  GB_CHECK(post_launch(c));
+  GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * nb3, cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
 // The same shell spectrum left on the device (out_dev[nmax/2+1]); no
 // synchronisation, for closures that consume it in later kernels.
 template <typename R>
@@ -1610,6 +1636,84 @@ int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, c
                    const void *f, int kin, double *Hk) {
   if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
   return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
+}
+
+// specpara / specperp (pseudospec3D_rot.f90:25-686): E[3 nb] and H[3 nb]
+// (total, horizontal, vertical) for kin 0/1 and hel 1
+static int aniso_spec(ghost_ctx *c, int mode, const void *a, const void *b, const void *cc, int kin, int hel,
+                      double *Ek, double *Hk) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc) return fail(GHOST_ERR_ARG, "null field");
+  if (kin < 0 || kin > 2) return fail(GHOST_ERR_ARG, "kin %d not in 0..2", kin);
+  if (kin <= 1 && !Ek) return fail(GHOST_ERR_ARG, "null Ek");
+  if (hel == 1 && !Hk) return fail(GHOST_ERR_ARG, "null Hk");
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts: one spectrum per run");
+  const int nb = mode == 0 ? c->nz / 2 + 1 : c->nmaxperp / 2 + 1;
+  Staging st(c);
+  const void *da, *db, *dc;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  const bool sp = c->precision == GHOST_SINGLE;
+  auto run = [&](int kind, double *o) {
+    return sp ? aniso_dev<float>(c, kind, mode, nb, da, db, dc, nullptr, nullptr, nullptr, o)
+              : aniso_dev<double>(c, kind, mode, nb, da, db, dc, nullptr, nullptr, nullptr, o);
+  };
+  if (kin <= 1) GB_CHECK(run(kin == 1 ? AN_KIN : AN_CURL, Ek));
+  if (hel == 1) GB_CHECK(run(AN_HEL, Hk));
+  return st.finish();
+}
+
+// entpara/entperp/heltpara/heltperp (pseudospec3D_rot.f90:689-1328): the
+// transfer sums binned by |kz| (mode 0) or k_perp (mode 1); out[nb]
+static int aniso_transfer(ghost_ctx *c, int mode, int kind, const void *a, const void *b, const void *cc,
+                          const void *d, const void *e, const void *f, double *out) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e || !f || !out) return fail(GHOST_ERR_ARG, "null argument");
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts: one spectrum per run");
+  const int nb = mode == 0 ? c->nz / 2 + 1 : c->nmaxperp / 2 + 1;
+  Staging st(c);
+  const void *da, *db, *dc, *dd, *de, *df;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(st.map(d, c->cbytes, 1, &dd));
+  GB_CHECK(st.map(e, c->cbytes, 1, &de));
+  GB_CHECK(st.map(f, c->cbytes, 1, &df));
+  std::vector<double> three((size_t)3 * nb);
+  GB_CHECK(c->precision == GHOST_SINGLE ? aniso_dev<float>(c, kind, mode, nb, da, db, dc, dd, de, df, three.data())
+                                        : aniso_dev<double>(c, kind, mode, nb, da, db, dc, dd, de, df, three.data()));
+  for (int q = 0; q < nb; ++q) out[q] = three[q];
+  return st.finish();
+}
+
+int ghost_specpara(ghost_ctx *c, const void *a, const void *b, const void *cc, int kin, int hel, double *Ek,
+                   double *Hk) {
+  return aniso_spec(c, 0, a, b, cc, kin, hel, Ek, Hk);
+}
+int ghost_specperp(ghost_ctx *c, const void *a, const void *b, const void *cc, int kin, int hel, double *Ek,
+                   double *Hk) {
+  return aniso_spec(c, 1, a, b, cc, kin, hel, Ek, Hk);
+}
+int ghost_entpara(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, int kin, double *Ek) {
+  if (kin < 0 || kin > 4) return fail(GHOST_ERR_ARG, "kin %d not in 0..4", kin);
+  return aniso_transfer(c, 0, kin == 0 ? RED_CROSS_K2 : RED_CROSS, a, b, cc, d, e, f, Ek);
+}
+int ghost_entperp(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, int kin, double *Ek) {
+  if (kin < 0 || kin > 4) return fail(GHOST_ERR_ARG, "kin %d not in 0..4", kin);
+  return aniso_transfer(c, 1, kin == 0 ? RED_CROSS_K2 : RED_CROSS, a, b, cc, d, e, f, Ek);
+}
+int ghost_heltpara(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                   const void *f, int kin, double *Hk) {
+  if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
+  return aniso_transfer(c, 0, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
+}
+int ghost_heltperp(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                   const void *f, int kin, double *Hk) {
+  if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
+  return aniso_transfer(c, 1, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
 }
 
 int ghost_hdcheck(ghost_ctx *c, const void *vx, const void *vy, const void *vz, const void *fx, const void *fy,

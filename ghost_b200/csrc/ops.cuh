@@ -280,6 +280,101 @@ __global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R>
   }
 }
 
+// Anisotropic spectra (pseudospec3D_rot.f90): mode 0 bins by |kz|
+// (kmn = int(|kz| Lz + 1): specpara, entpara, heltpara), mode 1 by the
+// perpendicular wavenumber (kmn = int(sqrt(kx^2 + ky^2)/Dkk + 1): specperp,
+// entperp, heltperp).  Three sums per bin, partials laid out
+// [block][3 nb] = total, horizontal, vertical:
+//   AN_KIN  (kin 1): horizontal |a|^2 + |b|^2, vertical |c|^2
+//   AN_CURL (kin 0): the same of curl(a,b,c)
+//   AN_HEL  (hel 1): horizontal Re(a c1*) + Re(b c2*), vertical Re(c c3*),
+//                    (c1,c2,c3) = curl(a,b,c)
+//   red_term kinds (the transfers): the total only.
+// In mode 1 the horizontal and vertical sums take the kz = 0 plane only,
+// and the total of the other planes is one three-term sum, as specperp's.
+enum AnKind { AN_KIN = 100, AN_CURL = 101, AN_HEL = 102 };
+
+template <typename R>
+__device__ __forceinline__ void an_terms(const KParams<R> &kp, const RedArgs<R> &ra, int kind, size_t p, int i, int j,
+                                         int k, R &h, R &v) {
+  using C = cx<R>;
+  const C va = ra.a[p], vb = ra.b[p], vc = ra.c[p];
+  if (kind == AN_KIN) {
+    h = va.x * va.x + va.y * va.y + (vb.x * vb.x + vb.y * vb.y);
+    v = vc.x * vc.x + vc.y * vc.y;
+    return;
+  }
+  const C w1 = curl_at(kp, 1, i, j, k, va, vb, vc), w2 = curl_at(kp, 2, i, j, k, va, vb, vc),
+          w3 = curl_at(kp, 3, i, j, k, va, vb, vc);
+  if (kind == AN_CURL) {
+    h = w1.x * w1.x + w1.y * w1.y + (w2.x * w2.x + w2.y * w2.y);
+    v = w3.x * w3.x + w3.y * w3.y;
+  } else {
+    h = cmulc(va, w1).x + cmulc(vb, w2).x;
+    v = cmulc(vc, w3).x;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra, int kind, int mode, size_t n, int nb,
+                                                    R Lz, R Dkk, double *partials) {
+  extern __shared__ double hist[];  // (blockDim/32) * 3 nb
+  const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nb3 = 3 * nb;
+  for (int q = threadIdx.x; q < nw * nb3; q += blockDim.x) hist[q] = 0.0;
+  __syncthreads();
+  double *hw = hist + (size_t)w * nb3;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t start = blockIdx.x * (size_t)blockDim.x + (size_t)w * 32;
+  for (size_t base = start; base < n; base += stride) {
+    const size_t p = base + lane;
+    int bin = -1;
+    double t = 0.0, hh = 0.0, vv = 0.0;
+    if (p < n) {
+      int i, j, k;
+      unflat(kp, p, i, j, k);
+      int kmn;
+      if (mode == 0) {
+        kmn = (int)(fabs(kz_of(kp, k)) * Lz + (R)1);
+      } else {
+        const R a = kx_of(kp, i), b = ky_of(kp, j);
+        kmn = (int)(sqrt(a * a + b * b) / Dkk + (R)1);
+      }
+      if (kmn > 0 && kmn <= nb) {
+        const R wgt = i == 0 ? (R)1 : (R)2;
+        bin = kmn - 1;
+        if (kind >= AN_KIN) {
+          R h, v;
+          an_terms(kp, ra, kind, p, i, j, k, h, v);
+          if (mode == 0 || k == 0) {
+            hh = (double)(wgt * h * kp.tmp);
+            vv = (double)(wgt * v * kp.tmp);
+            t = hh + vv;
+          } else {
+            t = (double)(wgt * (h + v) * kp.tmp);
+          }
+        } else {
+          t = (double)(wgt * red_term(kp, ra, kind, p, i, j, k));
+        }
+      }
+    }
+    for (int s = 0; s < 32; ++s) {
+      if (lane == s && bin >= 0) {
+        hw[bin] += t;
+        hw[nb + bin] += hh;
+        hw[2 * nb + bin] += vv;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb3; b += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < nw; ++q) s += hist[(size_t)q * nb3 + b];
+    partials[(size_t)blockIdx.x * nb3 + b] = s;
+  }
+}
+
 // max over real space of sqrt(r1^2+r2^2+r3^2) (maxabs); non-negative
 // floats order like their bit patterns, so an integer max is exact.
 template <typename R>

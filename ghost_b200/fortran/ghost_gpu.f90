@@ -526,6 +526,48 @@
          REAL(C_DOUBLE) :: hk(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_specpara(ctx,a,b,c,kin,hel,ek,hk) BIND(C,name="ghost_specpara") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: kin, hel
+         REAL(C_DOUBLE) :: ek(*), hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_specperp(ctx,a,b,c,kin,hel,ek,hk) BIND(C,name="ghost_specperp") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c
+         INTEGER(C_INT), VALUE :: kin, hel
+         REAL(C_DOUBLE) :: ek(*), hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_entpara(ctx,a,b,c,d,e,f,kin,ek) BIND(C,name="ghost_entpara") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_entperp(ctx,a,b,c,d,e,f,kin,ek) BIND(C,name="ghost_entperp") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_heltpara(ctx,a,b,c,d,e,f,kin,ek) BIND(C,name="ghost_heltpara") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_heltperp(ctx,a,b,c,d,e,f,kin,ek) BIND(C,name="ghost_heltperp") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_io_filename(dir,name,idx,width,buf,buflen) BIND(C,name="ghost_io_filename") RESULT(s)
          IMPORT :: C_INT, C_CHAR, C_SIZE_T
          CHARACTER(KIND=C_CHAR) :: dir(*), name(*), buf(*)

@@ -69,6 +69,7 @@ class Ghost:
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nxh = nx // 2 + 1
         self.kmax, self.tiny, self.nmax, self.Dkk = info.kmax, info.tiny, info.nmax, info.Dkk
+        self.nmaxperp = info.nmaxperp
         self.rdtype_np = np.float32 if precision == "fp32" else np.float64
         self.cdtype_np = np.complex64 if precision == "fp32" else np.complex128
         if stream is None and handle is None and torch is not None and torch.cuda.is_available():
@@ -141,6 +142,43 @@ class Ghost:
         check(self.lib.ghost_heltrans(self.h, *[self._ptr(x, "c") for x in (a, b, c, d, e, f)], kin,
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
+
+    def _aniso_nb(self, para: bool) -> int:
+        return self.nz // 2 + 1 if para else self.nmaxperp // 2 + 1
+
+    def _spec_aniso(self, fn, para, a, b, c, kin, hel):
+        nb = self._aniso_nb(para)
+        Ek, Hk = np.zeros(3 * nb), np.zeros(3 * nb)
+        PDt = ctypes.POINTER(ctypes.c_double)
+        check(getattr(self.lib, fn)(self.h, *[self._ptr(x, "c") for x in (a, b, c)], kin, hel,
+                                    Ek.ctypes.data_as(PDt), Hk.ctypes.data_as(PDt)), fn)
+        return Ek.reshape(3, nb), Hk.reshape(3, nb)
+
+    def specpara(self, a, b, c, kin: int = 1, hel: int = 0):
+        """specpara: (3, nz/2+1) arrays (total, horizontal, vertical) of E and H."""
+        return self._spec_aniso("ghost_specpara", True, a, b, c, kin, hel)
+
+    def specperp(self, a, b, c, kin: int = 1, hel: int = 0):
+        """specperp: (3, nmaxperp/2+1) arrays (total, kz=0 horizontal, kz=0 vertical)."""
+        return self._spec_aniso("ghost_specperp", False, a, b, c, kin, hel)
+
+    def _trans_aniso(self, fn, para, fields, kin):
+        out = np.zeros(self._aniso_nb(para))
+        check(getattr(self.lib, fn)(self.h, *[self._ptr(x, "c") for x in fields], kin,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), fn)
+        return out
+
+    def entpara(self, a, b, c, d, e, f, kin: int = 1):
+        return self._trans_aniso("ghost_entpara", True, (a, b, c, d, e, f), kin)
+
+    def entperp(self, a, b, c, d, e, f, kin: int = 1):
+        return self._trans_aniso("ghost_entperp", False, (a, b, c, d, e, f), kin)
+
+    def heltpara(self, a, b, c, d, e, f, kin: int = 1):
+        return self._trans_aniso("ghost_heltpara", True, (a, b, c, d, e, f), kin)
+
+    def heltperp(self, a, b, c, d, e, f, kin: int = 1):
+        return self._trans_aniso("ghost_heltperp", False, (a, b, c, d, e, f), kin)
 
     # ---- GHOST's binary field files (mpiio/binary_io.f90)
     def io_write(self, real, path: str, swap: bool = False):

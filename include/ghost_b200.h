@@ -205,6 +205,28 @@ int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, c
  * (hmtransfer / hktransfer). */
 int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
                    const void *f, int kin, double *Hk);
+/* Anisotropic spectra of rotating flows (pseudospec3D_rot.f90).  specpara
+ * bins by |kz| (kmn = int(|kz| Lz + 1), nb = nz/2+1 bins), specperp by the
+ * perpendicular wavenumber (kmn = int(sqrt(kx^2+ky^2)/Dkk + 1),
+ * nb = nmaxperp/2+1).  Ek and Hk are host arrays of 3 nb doubles: GHOST's
+ * Ektot, then the horizontal (x, y components) and vertical (z component)
+ * sums (specperp: of the kz = 0 plane, as GHOST's Eptot / Eztot).  kin 1
+ * kinetic, 0 of curl(a,b,c), 2 none; hel 1 the helicity Re(v . conj(curl v)).
+ * GHOST's files hold (Dkz (k-1), .5 E Lz) resp. (Dkk (k-1), .5 E/Dkk). */
+int ghost_specpara(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel, double *Ek,
+                   double *Hk);
+int ghost_specperp(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel, double *Ek,
+                   double *Hk);
+/* entpara/entperp, heltpara/heltperp (pseudospec3D_rot.f90:689-1328): the
+ * entrans / heltrans sums binned as specpara / specperp (nb doubles). */
+int ghost_entpara(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                  const void *f, int kin, double *Ek);
+int ghost_entperp(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                  const void *f, int kin, double *Ek);
+int ghost_heltpara(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                   const void *f, int kin, double *Hk);
+int ghost_heltperp(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                   const void *f, int kin, double *Hk);
 /* ghost_spectrumc_noalloc: the same shell spectra as ghost_spectrumc,
  * computed without allocating any memory.  It has no counterpart in the
  * reference; it exists for callers that cannot let the library allocate:

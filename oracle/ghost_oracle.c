@@ -636,6 +636,94 @@ void o_heltrans(const octx *c, const cplx *a, const cplx *b, const cplx *cc, con
   free(c1); free(c2); free(c3);
 }
 
+/* Anisotropic spectra (pseudospec3D_rot.f90).  mode 0 (specpara, entpara,
+ * heltpara, :25-335, 689-875, 1067-1196): kmn = int(|kz| Lz + 1) over
+ * nz/2+1 bins; mode 1 (specperp, entperp, heltperp, :338-686, 878-1064,
+ * 1199-1328): kmn = int(sqrt(kx^2 + ky^2)/Dkk + 1) over nmaxperp/2+1.
+ * The spectra return E[3 nb] = total, horizontal (x, y), vertical (z); in
+ * mode 1 the horizontal and vertical sums hold the kz = 0 plane and the
+ * other planes enter the total as one three-term sum. */
+static int o_an_bin(const octx *c, int mode, int i, int j, int k) {
+  if (mode == 0) return (int)(fabs(c->kz[k]) * c->Lz + (real)1);
+  return (int)((real)sqrt(c->kx[i] * c->kx[i] + c->ky[j] * c->ky[j]) / c->Dkk + (real)1);
+}
+
+/* what: 0 kinetic of (x,y,z), 1 helicity Re(a.conj(x)), x = curl */
+static void o_an_spec(const octx *c, int mode, const cplx *a, const cplx *b, const cplx *cc, const cplx *x,
+                      const cplx *y, const cplx *z, int what, double *E) {
+  int nb = mode == 0 ? c->nz / 2 + 1 : c->nmaxperp / 2 + 1;
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  for (int q = 0; q < 3 * nb; ++q) E[q] = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        int kmn = o_an_bin(c, mode, i, j, k);
+        if (kmn <= 0 || kmn > nb) continue;
+        size_t p = SIDX(c, k, j, i);
+        real h, v;
+        if (what == 0) {
+          h = cabs2(x[p]) + cabs2(y[p]);
+          v = cabs2(z[p]);
+        } else {
+          h = cmul(a[p], cconj(x[p])).re + cmul(b[p], cconj(y[p])).re;
+          v = cmul(cc[p], cconj(z[p])).re;
+        }
+        if (mode == 0 || k == 0) {
+          double tq = (double)(w * h * tmp), tr = (double)(w * v * tmp);
+          E[kmn - 1] += tq + tr;
+          E[nb + kmn - 1] += tq;
+          E[2 * nb + kmn - 1] += tr;
+        } else {
+          E[kmn - 1] += (double)(w * (h + v) * tmp);
+        }
+      }
+  }
+}
+
+void o_spec_aniso(const octx *c, int mode, const cplx *a, const cplx *b, const cplx *cc, int kin, int hel,
+                  double *Ek, double *Hk) {
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  cplx *c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+  if (kin == 1) o_an_spec(c, mode, a, b, cc, a, b, cc, 0, Ek);
+  if (kin == 0) o_an_spec(c, mode, a, b, cc, c1, c2, c3, 0, Ek);
+  if (hel == 1) o_an_spec(c, mode, a, b, cc, c1, c2, c3, 1, Hk);
+  free(c1); free(c2); free(c3);
+}
+
+/* the transfers binned the same way: Re(x.conj d + y.conj e + z.conj f) tmp
+ * (times kk2 with_kk2), x = (a,b,c) or curl(a,b,c) (curl != 0) */
+void o_trans_aniso(const octx *c, int mode, const cplx *a, const cplx *b, const cplx *cc, const cplx *d,
+                   const cplx *e, const cplx *f, int with_kk2, int curl, double *E) {
+  int nb = mode == 0 ? c->nz / 2 + 1 : c->nmaxperp / 2 + 1;
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  const cplx *x = a, *y = b, *z = cc;
+  cplx *c1 = NULL, *c2 = NULL, *c3 = NULL;
+  if (curl) {
+    c1 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c2 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    c3 = (cplx *)malloc(sizeof(cplx) * c->nspec);
+    o_rotor3(c, b, cc, c1, 1); o_rotor3(c, a, cc, c2, 2); o_rotor3(c, a, b, c3, 3);
+    x = c1; y = c2; z = c3;
+  }
+  for (int q = 0; q < nb; ++q) E[q] = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        int kmn = o_an_bin(c, mode, i, j, k);
+        if (kmn <= 0 || kmn > nb) continue;
+        size_t p = SIDX(c, k, j, i);
+        real s = cmul(x[p], cconj(d[p])).re + cmul(y[p], cconj(e[p])).re + cmul(z[p], cconj(f[p])).re;
+        if (with_kk2) s = c->kk2[p] * s;
+        E[kmn - 1] += (double)(w * s * tmp);
+      }
+  }
+  free(c1); free(c2); free(c3);
+}
+
 /* ------------------------------------------------------------------ */
 /* Random numbers: randu of pseudo/pseudospec3D_mod.fpp:130-148.  am is the
  * default-REAL constant 1./im, which is 2^-31 in both precisions. */

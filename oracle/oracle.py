@@ -65,6 +65,8 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_spectrumc": (None, [P, P, P, P, I, I, P, P]),
         "o_entrans": (None, [P, P, P, P, P, P, P, I, P]),
         "o_heltrans": (None, [P, P, P, P, P, P, P, P]),
+        "o_spec_aniso": (None, [P, I, P, P, P, I, I, P, P]),
+        "o_trans_aniso": (None, [P, I, P, P, P, P, P, P, I, I, P]),
         "o_randu": (ctypes.c_double if precision == "fp64" else ctypes.c_float, [P]),
         "o_random_vpot": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, P, P, P]),
         "o_random_solenoidal": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, D, P, P, P]),
@@ -241,6 +243,25 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def _an_nb(self, mode):
+        return self.nz // 2 + 1 if mode == 0 else self.nmaxperp // 2 + 1
+
+    def spec_aniso(self, mode, a, b, c, kin=1, hel=0):
+        """specpara (mode 0) / specperp (mode 1): (3, nb) arrays of E and H."""
+        a, b, c = self._c(a), self._c(b), self._c(c)
+        nb = self._an_nb(mode)
+        Ek, Hk = np.zeros(3 * nb), np.zeros(3 * nb)
+        self.lib.o_spec_aniso(self.h, mode, _ptr(a), _ptr(b), _ptr(c), kin, hel, _ptr(Ek), _ptr(Hk))
+        return Ek.reshape(3, nb), Hk.reshape(3, nb)
+
+    def trans_aniso(self, mode, a, b, c, d, e, f, kin=1, curl=False):
+        """entpara/entperp (curl False; kk2-weighted for kin 0), heltpara/heltperp (curl True)."""
+        arrs = [self._c(x) for x in (a, b, c, d, e, f)]
+        E = np.zeros(self._an_nb(mode))
+        self.lib.o_trans_aniso(self.h, mode, *[_ptr(x) for x in arrs], int(kin == 0 and not curl), int(curl),
+                               _ptr(E))
+        return E
 
     def sharp(self, a, delta):
         a = self._c(a)

@@ -497,3 +497,26 @@ def test_transfer_spectra(prec, shape):
     nl = o.prodre3(*v)
     T = g.entrans(*[to_dev(x.astype(g.cdtype_np)) for x in (*v, *nl)], kin=1)
     assert abs(T.sum()) <= (1e-11 if prec == "fp64" else 1e-5) * np.abs(T).sum()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("box", [dict(), dict(Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)])
+def test_anisotropic_spectra(prec, box):
+    """specpara / specperp (kin 1 and 0, hel 1) and entpara / entperp /
+    heltpara / heltperp against the oracle, on a cubic and an elongated box."""
+    shape = (32, 32, 16)
+    o = Oracle(*shape, **box)
+    g = ghost(*shape, precision=prec, **box)
+    a = [rand_spectral(o, 80 + q) for q in range(6)]
+    A = [to_dev(x.astype(g.cdtype_np)) for x in a]
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    for mode, spec in ((0, g.specpara), (1, g.specperp)):
+        for kin in (1, 0):
+            E, H = spec(*A[:3], kin=kin, hel=1)
+            Eo, Ho = o.spec_aniso(mode, *a[:3], kin=kin, hel=1)
+            assert rel_l2(E, Eo) <= tol, (mode, kin)
+            assert rel_l2(H, Ho) <= tol, (mode, kin)
+    for mode, ent, hel in ((0, g.entpara, g.heltpara), (1, g.entperp, g.heltperp)):
+        for kin in (1, 0):
+            assert rel_l2(ent(*A, kin=kin), o.trans_aniso(mode, *a, kin=kin)) <= tol, (mode, kin)
+        assert rel_l2(hel(*A), o.trans_aniso(mode, *a, curl=True)) <= tol, mode

@@ -151,3 +151,30 @@ def test_transfer_spectra_identities():
     assert np.abs(T).sum() > 0 and np.abs(H).sum() > 0
     assert rel_l2(o.entrans(*v, *v, kin=1), Ek) <= 1e-14
     assert rel_l2(o.entrans(*v, *v, kin=0), Wk) <= 1e-12
+
+
+@pytest.mark.parametrize("box", [dict(), dict(Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)])
+def test_anisotropic_spectra_identities(box):
+    """specpara / specperp and the binned transfers (pseudospec3D_rot.f90)
+    on the oracle: for a truncated zero-mean field every mode lands in a
+    bin, so each anisotropic spectrum sums to its shell-spectrum total;
+    specpara's total is its horizontal plus vertical sums, bin by bin, and
+    specperp's horizontal and vertical sums are the kz = 0 plane's share."""
+    o = Oracle(32, 32, 16, **box)
+    v = solenoidal_ic(o, seed=9)
+    nl = o.prodre3(*v)
+    Ek, _ = o.spectrumc(*v, 1, 0)
+    _, Hk = o.spectrumc(*v, 1, 1)
+    for mode in (0, 1):
+        E, H = o.spec_aniso(mode, *v, kin=1, hel=1)
+        assert abs(E[0].sum() - Ek.sum()) <= 1e-13 * Ek.sum()
+        assert abs(H[0].sum() - Hk.sum()) <= 1e-12 * np.abs(Hk).sum()
+        if mode == 0:
+            assert np.allclose(E[0], E[1] + E[2], rtol=1e-14, atol=0)
+        else:
+            assert (E[1] + E[2]).sum() <= E[0].sum()
+        T = o.entrans(*v, *nl, kin=1)
+        Ta = o.trans_aniso(mode, *v, *nl, kin=1)
+        assert abs(Ta.sum() - T.sum()) <= 1e-12 * np.abs(T).sum()
+        Hta = o.trans_aniso(mode, *v, *nl, curl=True)
+        assert abs(Hta.sum() - o.heltrans(*v, *nl).sum()) <= 1e-12 * np.abs(Hta).sum()
