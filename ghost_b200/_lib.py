@@ -123,6 +123,8 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_havgcomp": [P, P, P, P, P, D, D, I, PD],
+    "ghost_tbouss": [P, P, P, P, P, D, D, PD, PD, PD],
     "ghost_specpara": [P, P, P, P, I, I, PD, PD],
     "ghost_specperp": [P, P, P, P, I, I, PD, PD],
     "ghost_entpara": [P, P, P, P, P, P, P, I, PD],

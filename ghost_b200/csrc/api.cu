@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <vector>
 
@@ -1636,6 +1637,164 @@ int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, c
                    const void *f, int kin, double *Hk) {
   if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
   return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
+}
+
+// havgcomp (pseudospec3D_bouss.f90:19-554): the horizontally averaged
+// profile gsh[nz] of quantity itype (0..10) of the Boussinesq fields u, v,
+// w (velocity) and s (temperature).  Scratch fields 0..8 belong to the
+// transforms and advect3_dev; this uses 9..15.
+extern "C++" {
+template <typename R>
+static int zsum(ghost_ctx *c, int op, const void *r1, const void *r2, const void *r3, R fo, R bv,
+                std::vector<double> &sh) {
+  const size_t plane = (size_t)c->nx * c->ny;
+  const int nsplit = (int)std::max<size_t>(1, std::min<size_t>(64, plane / 4096));
+  double *part;
+  GB_CHECK(partials(c, (size_t)c->nz * nsplit, &part));
+  ZProfArgs<R> za{(const R *)r1, (const R *)r2, (const R *)r3, fo, bv,
+                  1.0 / ((double)c->nx * (double)c->ny * (double)c->nz)};
+  zprof_kernel<R><<<dim3(c->nz, nsplit), 256, 0, c->stream>>>(za, op, plane, part);
+  GB_CHECK(post_launch(c));
+  std::vector<double> host((size_t)c->nz * nsplit);
+  GB_CUDA(cudaMemcpyAsync(host.data(), part, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, c->stream));
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < c->nz; ++k)
+    for (int q = 0; q < nsplit; ++q) sh[k] += host[(size_t)k * nsplit + q];
+  return GHOST_OK;
+}
+
+template <typename R>
+static int havg_dev(ghost_ctx *c, const void *u, const void *v, const void *w, const void *s, R fo, R bv, int itype,
+                    double *gsh) {
+  void *sc[16];
+  GB_CHECK(scratch(c, 16, sc));
+  void *c1 = sc[9], *c2 = sc[10], *c3 = sc[11], *c4 = sc[12], *r1 = sc[13], *r2 = sc[14], *r3 = sc[15];
+  const int nz = c->nz;
+  std::vector<double> sh(nz, 0.0);
+  // 1/(nx^3 ny^3 nz^2): the transforms' N^3 per factor, over nx ny points
+  const double tmp0 = 1.0 / (std::pow((double)c->nx, 3) * std::pow((double)c->ny, 3) * std::pow((double)c->nz, 2));
+  double scale = tmp0;
+  auto c2r = [&](const void *in, void *out) { return c2r_dev<R>(c, in, out); };
+  auto dz = [&](const void *in, void *out) { return derivk3_impl<R>(c, in, out, 3); };
+  auto zs = [&](int op, const void *a, const void *b, const void *cc) {
+    return zsum<R>(c, op, a, b, cc, fo, bv, sh);
+  };
+  // GHOST enters the type-0 branch for itype 9 too and returns from it, so
+  // its column 10 repeats column 1 (the Richardson-number block is not reached)
+  switch (itype == 9 ? 0 : itype) {
+    case 0:  // <(du_perp/dz)^2>_perp
+      GB_CHECK(dz(u, c1)); GB_CHECK(c2r(c1, r1));
+      GB_CHECK(dz(v, c1)); GB_CHECK(c2r(c1, r2));
+      GB_CHECK(zs(ZP_SQ2, r1, r2, nullptr));
+      break;
+    case 1:  // <(dtheta/dz)^2>_perp
+      GB_CHECK(dz(s, c1)); GB_CHECK(c2r(c1, r3));
+      GB_CHECK(zs(ZP_SQ1, r3, nullptr, nullptr));
+      break;
+    case 2:  // <u_z dtheta/dz>_perp (the profile GHOST's comment names)
+      GB_CHECK(dz(s, c1)); GB_CHECK(c2r(c1, r3));
+      GB_CHECK(c2r(w, r2));
+      GB_CHECK(zs(ZP_PROD, r3, r2, nullptr));
+      break;
+    case 3:  // <u^2 + v^2>_perp
+      GB_CHECK(c2r(u, r1)); GB_CHECK(c2r(v, r2));
+      GB_CHECK(zs(ZP_SQ2, r1, r2, nullptr));
+      break;
+    case 4:  // <w^2>_perp
+      GB_CHECK(c2r(w, r1));
+      GB_CHECK(zs(ZP_SQ1, r1, nullptr, nullptr));
+      break;
+    case 5:  // <v du/dz - u dv/dz>_perp
+      GB_CHECK(dz(v, c1)); GB_CHECK(c2r(c1, r2)); GB_CHECK(c2r(u, r1));
+      GB_CHECK(zs(ZP_NEGPROD, r1, r2, nullptr));
+      GB_CHECK(dz(u, c1)); GB_CHECK(c2r(c1, r2)); GB_CHECK(c2r(v, r1));
+      GB_CHECK(zs(ZP_PROD, r1, r2, nullptr));
+      break;
+    case 6:  // <omega_z theta>_perp
+      GB_CHECK(rotor3_impl<R>(c, u, v, c1, 3)); GB_CHECK(c2r(c1, r1));
+      GB_CHECK(c2r(s, r2));
+      GB_CHECK(zs(ZP_PROD, r1, r2, nullptr));
+      break;
+    case 7: {  // <PV^2>_perp
+      GB_CHECK(dz(s, c1)); GB_CHECK(c2r(c1, r1));
+      GB_CHECK(rotor3_impl<R>(c, u, v, c1, 3)); GB_CHECK(c2r(c1, r2));
+      GB_CHECK(rotor3_impl<R>(c, v, w, c1, 1));
+      GB_CHECK(rotor3_impl<R>(c, u, w, c2, 2));
+      GB_CHECK(rotor3_impl<R>(c, u, v, c3, 3));
+      GB_CHECK(advect3_dev<R>(c, c1, c2, c3, s, c4));
+      GB_CHECK(c2r(c4, r3));
+      GB_CHECK(zs(ZP_PV, r1, r2, r3));
+      scale = 1.0 / ((double)c->nx * (double)c->ny);
+      break;
+    }
+    case 8:  // <omega . curl(omega) parts>_perp, three terms r3 (r1 - r2)
+      GB_CHECK(rotor3_impl<R>(c, u, v, c1, 3)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 2)); GB_CHECK(c2r(c2, r1));
+      GB_CHECK(rotor3_impl<R>(c, u, w, c1, 2)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 3)); GB_CHECK(c2r(c2, r2));
+      GB_CHECK(rotor3_impl<R>(c, v, w, c1, 1)); GB_CHECK(c2r(c1, r3));
+      GB_CHECK(zs(ZP_CURLTERM, r1, r2, r3));
+      GB_CHECK(rotor3_impl<R>(c, v, w, c1, 1)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 3)); GB_CHECK(c2r(c2, r1));
+      GB_CHECK(rotor3_impl<R>(c, u, v, c1, 3)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 1)); GB_CHECK(c2r(c2, r2));
+      GB_CHECK(rotor3_impl<R>(c, u, w, c1, 2)); GB_CHECK(c2r(c1, r3));
+      GB_CHECK(zs(ZP_CURLTERM, r1, r2, r3));
+      GB_CHECK(rotor3_impl<R>(c, u, w, c1, 2)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 1)); GB_CHECK(c2r(c2, r1));
+      GB_CHECK(rotor3_impl<R>(c, v, w, c1, 1)); GB_CHECK(derivk3_impl<R>(c, c1, c2, 2)); GB_CHECK(c2r(c2, r2));
+      GB_CHECK(rotor3_impl<R>(c, u, v, c1, 3)); GB_CHECK(c2r(c1, r3));
+      GB_CHECK(zs(ZP_CURLTERM, r1, r2, r3));
+      break;
+    case 10:  // <w theta>_perp
+      GB_CHECK(c2r(w, r1)); GB_CHECK(c2r(s, r2));
+      GB_CHECK(zs(ZP_PROD, r1, r2, nullptr));
+      break;
+    default:
+      return fail(GHOST_ERR_ARG, "itype %d not in 0..10", itype);
+  }
+  for (int k = 0; k < nz; ++k) gsh[k] = sh[k] * scale;
+  return check_status(c);
+}
+}  // extern "C++"
+
+static int havg(ghost_ctx *c, const void *u, const void *v, const void *w, const void *s, double fo, double bv,
+                int itype, double *gsh) {
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts: one profile per run");
+  Staging st(c);
+  const void *du, *dv, *dw, *ds;
+  GB_CHECK(st.map(u, c->cbytes, 1, &du));
+  GB_CHECK(st.map(v, c->cbytes, 1, &dv));
+  GB_CHECK(st.map(w, c->cbytes, 1, &dw));
+  GB_CHECK(st.map(s, c->cbytes, 1, &ds));
+  GB_CHECK(c->precision == GHOST_SINGLE ? havg_dev<float>(c, du, dv, dw, ds, (float)fo, (float)bv, itype, gsh)
+                                        : havg_dev<double>(c, du, dv, dw, ds, fo, bv, itype, gsh));
+  return st.finish();
+}
+
+int ghost_havgcomp(ghost_ctx *c, const void *u, const void *v, const void *w, const void *s, double fo, double bv,
+                   int itype, double *gsh) {
+  CTX_CHECK(c);
+  if (!u || !v || !w || !s || !gsh) return fail(GHOST_ERR_ARG, "null argument");
+  if (itype < 0 || itype > 10) return fail(GHOST_ERR_ARG, "itype %d not in 0..10", itype);
+  return havg(c, u, v, w, s, fo, bv, itype, gsh);
+}
+
+// tbouss (pseudospec3D_bouss.f90:611-711): the z-average, maximum and
+// minimum over z of each of the 11 havgcomp profiles
+int ghost_tbouss(ghost_ctx *c, const void *u, const void *v, const void *w, const void *s, double fo, double bv,
+                 double avg[11], double mx[11], double mn[11]) {
+  CTX_CHECK(c);
+  if (!u || !v || !w || !s || !avg || !mx || !mn) return fail(GHOST_ERR_ARG, "null argument");
+  std::vector<double> gsh(c->nz);
+  for (int q = 0; q < 11; ++q) {
+    GB_CHECK(havg(c, u, v, w, s, fo, bv, q, gsh.data()));
+    double sum = 0.0, hi = gsh[0], lo = gsh[0];
+    for (int k = 0; k < c->nz; ++k) {
+      sum += gsh[k];
+      hi = std::max(hi, gsh[k]);
+      lo = std::min(lo, gsh[k]);
+    }
+    avg[q] = sum / (double)c->nz;
+    mx[q] = hi;
+    mn[q] = lo;
+  }
+  return GHOST_OK;
 }
 
 // specpara / specperp (pseudospec3D_rot.f90:25-686): E[3 nb] and H[3 nb]

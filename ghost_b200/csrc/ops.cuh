@@ -375,6 +375,49 @@ __global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra
   }
 }
 
+// Horizontal (x, y) sums of real fields per z-plane (havgcomp,
+// pseudospec3D_bouss.f90:19-554): block (k, s) sums a strided part of plane k
+// of op(r1, r2, r3) into partials[k * gridDim.y + s].
+enum ZProfOp { ZP_SQ2 = 0, ZP_SQ1 = 1, ZP_PROD = 2, ZP_NEGPROD = 3, ZP_CURLTERM = 4, ZP_PV = 5 };
+template <typename R> struct ZProfArgs {
+  const R *r1, *r2, *r3;
+  R fo, bv;
+  double tmpn;  // 1/(nx ny nz) for ZP_PV
+};
+template <typename R>
+__global__ void __launch_bounds__(256) zprof_kernel(ZProfArgs<R> za, int op, size_t plane, double *partials) {
+  __shared__ double sh[32];
+  const int k = blockIdx.x;
+  const size_t off = (size_t)k * plane;
+  double acc = 0.0;
+  for (size_t q = blockIdx.y * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.y * blockDim.x) {
+    const size_t p = off + q;
+    if (op == ZP_SQ2) {
+      const R a = za.r1[p], b = za.r2[p];
+      acc += (double)(a * a + b * b);
+    } else if (op == ZP_SQ1) {
+      const R a = za.r1[p];
+      acc += (double)(a * a);
+    } else if (op == ZP_PROD) {
+      acc += (double)(za.r1[p] * za.r2[p]);
+    } else if (op == ZP_NEGPROD) {
+      acc -= (double)(za.r1[p] * za.r2[p]);
+    } else if (op == ZP_CURLTERM) {
+      acc += (double)(za.r3[p] * (za.r1[p] - za.r2[p]));
+    } else {
+      // potential vorticity: fo dtheta/dz - bv w_z + w.grad(theta) - fo bv,
+      // each real field carrying the N^3 of the transforms (type 7)
+      R pv = (R)((double)za.fo * (double)za.r1[p] * za.tmpn);
+      pv = (R)((double)pv - (double)za.bv * (double)za.r2[p] * za.tmpn);
+      pv = (R)((double)pv + (double)za.r3[p] * -za.tmpn);
+      pv = pv - za.fo * za.bv;
+      acc += (double)(pv * pv);
+    }
+  }
+  const double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[(size_t)k * gridDim.y + blockIdx.y] = s;
+}
+
 // max over real space of sqrt(r1^2+r2^2+r3^2) (maxabs); non-negative
 // floats order like their bit patterns, so an integer max is exact.
 template <typename R>

@@ -568,6 +568,21 @@
          REAL(C_DOUBLE) :: ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_havgcomp(ctx,u,v,w,th,fo,bv,itype,gsh) BIND(C,name="ghost_havgcomp") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, u, v, w, th
+         REAL(C_DOUBLE), VALUE :: fo, bv
+         INTEGER(C_INT), VALUE :: itype
+         REAL(C_DOUBLE) :: gsh(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_tbouss(ctx,u,v,w,th,fo,bv,avg,mx,mn) BIND(C,name="ghost_tbouss") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, u, v, w, th
+         REAL(C_DOUBLE), VALUE :: fo, bv
+         REAL(C_DOUBLE) :: avg(*), mx(*), mn(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_io_filename(dir,name,idx,width,buf,buflen) BIND(C,name="ghost_io_filename") RESULT(s)
          IMPORT :: C_INT, C_CHAR, C_SIZE_T
          CHARACTER(KIND=C_CHAR) :: dir(*), name(*), buf(*)
@@ -926,3 +941,30 @@
       END DO
       CLOSE(1)
       END SUBROUTINE heltrans
+
+!-----------------------------------------------------------------
+! tbouss (pseudospec3D_bouss.f90:611-711): the profiles on the device,
+! GHOST's three appended text files written here.
+!-----------------------------------------------------------------
+      SUBROUTINE tbouss(u, v, w, s, t, dt, fo, bv)
+      USE fprecision
+      USE grid
+      USE ghost_gpu
+      IMPLICIT NONE
+      COMPLEX(KIND=GP), INTENT(IN), TARGET, DIMENSION(nz,ny,nx/2+1) :: u,v,w,s
+      REAL(KIND=GP), INTENT(IN) :: dt, fo, bv
+      INTEGER, INTENT(IN) :: t
+      DOUBLE PRECISION :: gxavg(11),gxmax(11),gxmin(11)
+      CALL ghost_gpu_check(ghost_tbouss(gctx,C_LOC(u),C_LOC(v),C_LOC(w),C_LOC(s), &
+           DBLE(fo),DBLE(bv),gxavg,gxmax,gxmin),'tbouss')
+      OPEN(1,file='tboussavg.txt',position='append')
+      WRITE(1,20) (t-1)*dt,gxavg
+      CLOSE(1)
+      OPEN(1,file='tboussmax.txt',position='append')
+      WRITE(1,20) (t-1)*dt,gxmax
+      CLOSE(1)
+      OPEN(1,file='tboussmin.txt',position='append')
+      WRITE(1,20) (t-1)*dt,gxmin
+      CLOSE(1)
+   20 FORMAT( E13.6,1x,11(E26.18,1x) )
+      END SUBROUTINE tbouss

@@ -143,6 +143,21 @@ class Ghost:
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
 
+    def havgcomp(self, u, v, w, s, fo: float, bv: float, itype: int):
+        """havgcomp: the horizontally averaged profile (nz,) of quantity itype."""
+        gsh = np.zeros(self.nz)
+        check(self.lib.ghost_havgcomp(self.h, *[self._ptr(x, "c") for x in (u, v, w, s)], fo, bv, itype,
+                                      gsh.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_havgcomp")
+        return gsh
+
+    def tbouss(self, u, v, w, s, fo: float, bv: float):
+        """tbouss: (avg, max, min) over z of the 11 havgcomp profiles."""
+        out = [np.zeros(11) for _ in range(3)]
+        PDt = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.ghost_tbouss(self.h, *[self._ptr(x, "c") for x in (u, v, w, s)], fo, bv,
+                                    *[o.ctypes.data_as(PDt) for o in out]), "ghost_tbouss")
+        return tuple(out)
+
     def _aniso_nb(self, para: bool) -> int:
         return self.nz // 2 + 1 if para else self.nmaxperp // 2 + 1
 

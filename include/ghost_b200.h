@@ -205,6 +205,21 @@ int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, c
  * (hmtransfer / hktransfer). */
 int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
                    const void *f, int kin, double *Hk);
+/* havgcomp(gsh,u,v,w,s,fo,bv,itype) (pseudospec3D_bouss.f90:19-554): the
+ * horizontally averaged profile gsh[nz] of quantity itype of the
+ * Boussinesq fields (velocity u, v, w; temperature s; fo the Coriolis and
+ * bv the Brunt-Vaisala frequency): 0 <(du_perp/dz)^2>, 1 <(ds/dz)^2>,
+ * 2 <w ds/dz>, 3 <u^2+v^2>, 4 <w^2>, 5 <v du/dz - u dv/dz>, 6 <w_z s>,
+ * 7 <PV^2>, 8 the vorticity-gradient term, 9 as GHOST computes it (its type-0
+ * branch also takes itype 9), 10 <w s>.  Type 2 follows the profile GHOST's
+ * comment names; its code reads an array it has not set. */
+int ghost_havgcomp(ghost_ctx *ctx, const void *u, const void *v, const void *w, const void *s, double fo, double bv,
+                   int itype, double *gsh);
+/* tbouss (pseudospec3D_bouss.f90:611-711): per itype 0..10 the z-average,
+ * the maximum and the minimum of the havgcomp profile (host arrays of 11);
+ * GHOST appends them to tboussavg/max/min.txt */
+int ghost_tbouss(ghost_ctx *ctx, const void *u, const void *v, const void *w, const void *s, double fo, double bv,
+                 double *avg, double *mx, double *mn);
 /* Anisotropic spectra of rotating flows (pseudospec3D_rot.f90).  specpara
  * bins by |kz| (kmn = int(|kz| Lz + 1), nb = nz/2+1 bins), specperp by the
  * perpendicular wavenumber (kmn = int(sqrt(kx^2+ky^2)/Dkk + 1),

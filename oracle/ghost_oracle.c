@@ -1558,3 +1558,107 @@ void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, con
         vz[p].re = (real)v[4] * norm; vz[p].im = (real)v[5] * norm;
       }
 }
+
+/* ------------------------------------------------------------------ */
+/* havgcomp (pseudospec3D_bouss.f90:19-554): the horizontal sums per z
+ * plane of the real fields of itype's quantity.  itype 9 enters GHOST's
+ * type-0 branch and returns from it; type 2 uses dtheta/dz for the factor
+ * its code leaves unset (the profile its comment names). */
+static void o_zsum(const octx *c, int op, const real *r1, const real *r2, const real *r3, real fo, real bv,
+                   double *sh) {
+  size_t plane = (size_t)c->nx * c->ny;
+  double tmpn = 1.0 / ((double)c->nx * (double)c->ny * (double)c->nz);
+  for (int k = 0; k < c->nz; ++k)
+    for (size_t q = 0; q < plane; ++q) {
+      size_t p = (size_t)k * plane + q;
+      if (op == 0) sh[k] += (double)(r1[p] * r1[p] + r2[p] * r2[p]);
+      else if (op == 1) sh[k] += (double)(r1[p] * r1[p]);
+      else if (op == 2) sh[k] += (double)(r1[p] * r2[p]);
+      else if (op == 3) sh[k] -= (double)(r1[p] * r2[p]);
+      else if (op == 4) sh[k] += (double)(r3[p] * (r1[p] - r2[p]));
+      else {
+        real pv = 0;
+        pv = (real)((double)pv + (double)fo * (double)r1[p] * tmpn);
+        pv = (real)((double)pv - (double)bv * (double)r2[p] * tmpn);
+        pv = (real)((double)pv + (double)r3[p] * -tmpn);
+        pv = pv - fo * bv;
+        sh[k] += (double)(pv * pv);
+      }
+    }
+}
+
+void o_havgcomp(const octx *c, const cplx *u, const cplx *v, const cplx *w, const cplx *s, double fo_d,
+                double bv_d, int itype, double *gsh) {
+  real fo = (real)fo_d, bv = (real)bv_d;
+  size_t ns = c->nspec, nr = c->nreal;
+  cplx *c1 = (cplx *)malloc(sizeof(cplx) * ns), *c2 = (cplx *)malloc(sizeof(cplx) * ns);
+  cplx *c3 = (cplx *)malloc(sizeof(cplx) * ns), *c4 = (cplx *)malloc(sizeof(cplx) * ns);
+  real *r1 = (real *)malloc(sizeof(real) * nr), *r2 = (real *)malloc(sizeof(real) * nr);
+  real *r3 = (real *)malloc(sizeof(real) * nr);
+  double tmp0 = 1.0 / (pow((double)c->nx, 3) * pow((double)c->ny, 3) * pow((double)c->nz, 2)), scale = tmp0;
+  for (int k = 0; k < c->nz; ++k) gsh[k] = 0.0;
+  switch (itype == 9 ? 0 : itype) {
+    case 0:
+      o_derivk3(c, u, c1, 3); o_fftp3d_complex_to_real(c, c1, r1);
+      o_derivk3(c, v, c1, 3); o_fftp3d_complex_to_real(c, c1, r2);
+      o_zsum(c, 0, r1, r2, NULL, fo, bv, gsh);
+      break;
+    case 1:
+      o_derivk3(c, s, c1, 3); o_fftp3d_complex_to_real(c, c1, r3);
+      o_zsum(c, 1, r3, NULL, NULL, fo, bv, gsh);
+      break;
+    case 2:
+      o_derivk3(c, s, c1, 3); o_fftp3d_complex_to_real(c, c1, r3);
+      o_fftp3d_complex_to_real(c, w, r2);
+      o_zsum(c, 2, r3, r2, NULL, fo, bv, gsh);
+      break;
+    case 3:
+      o_fftp3d_complex_to_real(c, u, r1); o_fftp3d_complex_to_real(c, v, r2);
+      o_zsum(c, 0, r1, r2, NULL, fo, bv, gsh);
+      break;
+    case 4:
+      o_fftp3d_complex_to_real(c, w, r1);
+      o_zsum(c, 1, r1, NULL, NULL, fo, bv, gsh);
+      break;
+    case 5:
+      o_derivk3(c, v, c1, 3); o_fftp3d_complex_to_real(c, c1, r2); o_fftp3d_complex_to_real(c, u, r1);
+      o_zsum(c, 3, r1, r2, NULL, fo, bv, gsh);
+      o_derivk3(c, u, c1, 3); o_fftp3d_complex_to_real(c, c1, r2); o_fftp3d_complex_to_real(c, v, r1);
+      o_zsum(c, 2, r1, r2, NULL, fo, bv, gsh);
+      break;
+    case 6:
+      o_rotor3(c, u, v, c1, 3); o_fftp3d_complex_to_real(c, c1, r1);
+      o_fftp3d_complex_to_real(c, s, r2);
+      o_zsum(c, 2, r1, r2, NULL, fo, bv, gsh);
+      break;
+    case 7:
+      o_derivk3(c, s, c1, 3); o_fftp3d_complex_to_real(c, c1, r1);
+      o_rotor3(c, u, v, c1, 3); o_fftp3d_complex_to_real(c, c1, r2);
+      o_rotor3(c, v, w, c1, 1); o_rotor3(c, u, w, c2, 2); o_rotor3(c, u, v, c3, 3);
+      o_advect3(c, c1, c2, c3, s, c4);
+      o_fftp3d_complex_to_real(c, c4, r3);
+      o_zsum(c, 5, r1, r2, r3, fo, bv, gsh);
+      scale = 1.0 / ((double)c->nx * (double)c->ny);
+      break;
+    case 8:
+      o_rotor3(c, u, v, c1, 3); o_derivk3(c, c1, c2, 2); o_fftp3d_complex_to_real(c, c2, r1);
+      o_rotor3(c, u, w, c1, 2); o_derivk3(c, c1, c2, 3); o_fftp3d_complex_to_real(c, c2, r2);
+      o_rotor3(c, v, w, c1, 1); o_fftp3d_complex_to_real(c, c1, r3);
+      o_zsum(c, 4, r1, r2, r3, fo, bv, gsh);
+      o_rotor3(c, v, w, c1, 1); o_derivk3(c, c1, c2, 3); o_fftp3d_complex_to_real(c, c2, r1);
+      o_rotor3(c, u, v, c1, 3); o_derivk3(c, c1, c2, 1); o_fftp3d_complex_to_real(c, c2, r2);
+      o_rotor3(c, u, w, c1, 2); o_fftp3d_complex_to_real(c, c1, r3);
+      o_zsum(c, 4, r1, r2, r3, fo, bv, gsh);
+      o_rotor3(c, u, w, c1, 2); o_derivk3(c, c1, c2, 1); o_fftp3d_complex_to_real(c, c2, r1);
+      o_rotor3(c, v, w, c1, 1); o_derivk3(c, c1, c2, 2); o_fftp3d_complex_to_real(c, c2, r2);
+      o_rotor3(c, u, v, c1, 3); o_fftp3d_complex_to_real(c, c1, r3);
+      o_zsum(c, 4, r1, r2, r3, fo, bv, gsh);
+      break;
+    default:  /* 10 */
+      o_fftp3d_complex_to_real(c, w, r1); o_fftp3d_complex_to_real(c, s, r2);
+      o_zsum(c, 2, r1, r2, NULL, fo, bv, gsh);
+      break;
+  }
+  for (int k = 0; k < c->nz; ++k) gsh[k] *= scale;
+  free(c1); free(c2); free(c3); free(c4); free(r1); free(r2); free(r3);
+}

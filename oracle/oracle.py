@@ -66,6 +66,7 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_entrans": (None, [P, P, P, P, P, P, P, I, P]),
         "o_heltrans": (None, [P, P, P, P, P, P, P, P]),
         "o_spec_aniso": (None, [P, I, P, P, P, I, I, P, P]),
+        "o_havgcomp": (None, [P, P, P, P, P, D, D, I, P]),
         "o_trans_aniso": (None, [P, I, P, P, P, P, P, P, I, I, P]),
         "o_randu": (ctypes.c_double if precision == "fp64" else ctypes.c_float, [P]),
         "o_random_vpot": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, P, P, P]),
@@ -243,6 +244,13 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def havgcomp(self, u, v, w, s, fo, bv, itype):
+        """havgcomp: the horizontally averaged profile (nz,) of quantity itype."""
+        arrs = [self._c(x) for x in (u, v, w, s)]
+        gsh = np.zeros(self.nz)
+        self.lib.o_havgcomp(self.h, *[_ptr(x) for x in arrs], fo, bv, itype, _ptr(gsh))
+        return gsh
 
     def _an_nb(self, mode):
         return self.nz // 2 + 1 if mode == 0 else self.nmaxperp // 2 + 1

@@ -520,3 +520,27 @@ def test_anisotropic_spectra(prec, box):
         for kin in (1, 0):
             assert rel_l2(ent(*A, kin=kin), o.trans_aniso(mode, *a, kin=kin)) <= tol, (mode, kin)
         assert rel_l2(hel(*A), o.trans_aniso(mode, *a, curl=True)) <= tol, mode
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_havgcomp_and_tbouss(prec):
+    """havgcomp's eleven profiles against the oracle on an elongated
+    Boussinesq box, and tbouss as their z-average, maximum and minimum."""
+    shape = (32, 32, 16)
+    box = dict(Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)
+    o = Oracle(*shape, **box)
+    g = ghost(*shape, precision=prec, **box)
+    v = solenoidal_ic(o, seed=13)
+    s = o.random_solenoidal(14, 1.0, 4.0, 0, 1.0)[0][0]
+    F = [to_dev(x.astype(g.cdtype_np)) for x in (*v, s)]
+    tol = 1e-11 if prec == "fp64" else 1e-5
+    prof = []
+    for t in range(11):
+        got = g.havgcomp(*F, 1.0, 8.0, t)
+        ref = o.havgcomp(*v, s, 1.0, 8.0, t)
+        assert rel_l2(got, ref) <= tol, t
+        prof.append(got)
+    avg, mx, mn = g.tbouss(*F, 1.0, 8.0)
+    for t in range(11):
+        assert np.isclose(avg[t], prof[t].mean(), rtol=1e-12, atol=0)
+        assert mx[t] == prof[t].max() and mn[t] == prof[t].min()

@@ -178,3 +178,22 @@ def test_anisotropic_spectra_identities(box):
         assert abs(Ta.sum() - T.sum()) <= 1e-12 * np.abs(T).sum()
         Hta = o.trans_aniso(mode, *v, *nl, curl=True)
         assert abs(Hta.sum() - o.heltrans(*v, *nl).sum()) <= 1e-12 * np.abs(Hta).sum()
+
+
+def test_havgcomp_profiles_identities():
+    """havgcomp (pseudospec3D_bouss.f90:19-554) on the oracle: the z-means
+    of the horizontal kinetic profiles add up to <|v|^2>, the z-mean of
+    <w s> is the cross term <w s>, and type 9 repeats type 0 as in GHOST."""
+    o = Oracle(32, 32, 16, Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)
+    v = solenoidal_ic(o, seed=11)
+    s = o.random_solenoidal(12, 1.0, 4.0, 0, 1.0)[0][0]
+    z = np.zeros_like(s)
+    h3 = o.havgcomp(*v, s, 1.0, 8.0, 3)
+    h4 = o.havgcomp(*v, s, 1.0, 8.0, 4)
+    assert abs((h3 + h4).mean() - o.energy(*v, 1)) <= 1e-12 * o.energy(*v, 1)
+    h10 = o.havgcomp(*v, s, 1.0, 8.0, 10)
+    ws = o.cross(z, z, v[2], z, z, s, 1)
+    assert abs(h10.mean() - ws) <= 1e-12 * max(abs(ws), 1e-30) + 1e-15
+    assert np.array_equal(o.havgcomp(*v, s, 1.0, 8.0, 9), o.havgcomp(*v, s, 1.0, 8.0, 0))
+    for t in range(11):
+        assert np.all(np.isfinite(o.havgcomp(*v, s, 1.0, 8.0, t)))
