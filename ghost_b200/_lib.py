@@ -123,6 +123,10 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_phd_run": [P, I, I, D, D, D, P, P, P, P, P, P, P, P],
+    "ghost_variance": [P, P, I, PD],
+    "ghost_spectrscc": [P, P, D, PD],
+    "ghost_sctrans": [P, P, P, I, PD],
     "ghost_havgcomp": [P, P, P, P, P, D, D, I, PD],
     "ghost_tbouss": [P, P, P, P, P, D, D, PD, PD, PD],
     "ghost_specpara": [P, P, P, P, I, I, PD, PD],

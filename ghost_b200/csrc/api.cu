@@ -879,9 +879,11 @@ int reduce_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void 
 
 // Shell-binned sums of a reduction term over two field triplets (the
 // transfer spectra of entrans / heltrans); spectrum_dev is its one-triplet form.
+// rnd is the shell rounding: GHOST's spectra add the default-REAL literal
+// .501 (0.501f), spectrscc adds shift + .501 in GP
 template <typename R>
 int spectrum6_dev(ghost_ctx *c, int kind, const void *a, const void *b, const void *cc, const void *d, const void *e,
-                  const void *f, double *out_host) {
+                  const void *f, double *out_host, R rnd = (R)0.501f) {
   const size_t n = c->ntot;
   const int nbins = c->nmax / 2 + 1;
   const int nblk = std::min(grid1d(n), 148 * 4);
@@ -892,7 +894,7 @@ int spectrum6_dev(ghost_ctx *c, int kind, const void *a, const void *b, const vo
   const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
   GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
-  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, part);
+  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, rnd, part);
   GB_CHECK(post_launch(c));
   double *fin = part + (size_t)nblk * nbins;
   finalize_kernel<<<1, 256, 0, c->stream>>>(part, nblk, nbins, fin);
@@ -947,7 +949,7 @@ int spectrum_dev_async(ghost_ctx *c, int kind, const void *a, const void *b, con
   const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
   GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ts = timer_begin(c, GHOST_TIMER_REDUCE);
-  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, part);
+  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, (R)0.501f, part);
   GB_CHECK(post_launch(c));
   finalize_kernel<<<1, 256, 0, c->stream>>>(part, nblk, nbins, out_dev);
   timer_end(c, ts);
@@ -1639,6 +1641,47 @@ int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, c
   return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
 }
 
+// Passive scalar (pseudospec3D_phd.f90): variance (:116-216), spectrscc
+// (:516-609), sctrans (:612-726) of a scalar spectral field.
+int ghost_variance(ghost_ctx *c, const void *a, int kin, double *out) {
+  CTX_CHECK(c);
+  if (!a || !out) return fail(GHOST_ERR_ARG, "null argument");
+  if (kin < 0 || kin > 1) return fail(GHOST_ERR_ARG, "kin %d not in 0..1", kin);
+  Staging st(c);
+  const void *da;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  const int kind = kin == 1 ? RED_SC_VAR : RED_SC_VAR_K2;
+  GB_CHECK(c->precision == GHOST_SINGLE ? reduce_dev<float>(c, kind, da, da, da, nullptr, nullptr, nullptr, out)
+                                        : reduce_dev<double>(c, kind, da, da, da, nullptr, nullptr, nullptr, out));
+  return st.finish();
+}
+
+int ghost_spectrscc(ghost_ctx *c, const void *a, double shift, double *Ek) {
+  CTX_CHECK(c);
+  if (!a || !Ek) return fail(GHOST_ERR_ARG, "null argument");
+  Staging st(c);
+  const void *da;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  // round = shift + .501_GP (a GP literal here, unlike spectrumc's default REAL)
+  GB_CHECK(c->precision == GHOST_SINGLE
+               ? spectrum6_dev<float>(c, RED_SC_VAR, da, da, da, da, da, da, Ek, (float)shift + 0.501f)
+               : spectrum6_dev<double>(c, RED_SC_VAR, da, da, da, da, da, da, Ek, shift + 0.501));
+  return st.finish();
+}
+
+int ghost_sctrans(ghost_ctx *c, const void *a, const void *b, int isc, double *Ek) {
+  CTX_CHECK(c);
+  if (!a || !b || !Ek) return fail(GHOST_ERR_ARG, "null argument");
+  if (isc < 0) return fail(GHOST_ERR_ARG, "isc %d", isc);
+  Staging st(c);
+  const void *da, *db;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(c->precision == GHOST_SINGLE ? spectrum6_dev<float>(c, RED_SC_CROSS, da, da, da, db, db, db, Ek)
+                                        : spectrum6_dev<double>(c, RED_SC_CROSS, da, da, da, db, db, db, Ek));
+  return st.finish();
+}
+
 // havgcomp (pseudospec3D_bouss.f90:19-554): the horizontally averaged
 // profile gsh[nz] of quantity itype (0..10) of the Boussinesq fields u, v,
 // w (velocity) and s (temperature).  Scratch fields 0..8 belong to the
@@ -2157,6 +2200,14 @@ int ghost_bouss_rkstep2(ghost_ctx *c, int o, double dt, double nu, double kappa,
   return st.finish();
 }
 
+// The passive-scalar solver (PHD_SOL, include/phd_rkstep1/2.f90): the
+// rotating Boussinesq step without rotation, buoyancy or heat current is
+// GHOST's PHD step term for term.
+int ghost_phd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, double kappa, void *vx, void *vy, void *vz,
+                  void *th, const void *fx, const void *fy, const void *fz, const void *fs) {
+  return ghost_bouss_run(c, nsteps, ord, dt, nu, kappa, 0.0, 0.0, 0.0, vx, vy, vz, th, fx, fy, fz, fs);
+}
+
 int ghost_bouss_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, double kappa, double omegaz,
                     double xmom, double xtemp, void *vx, void *vy, void *vz, void *th, const void *fx,
                     const void *fy, const void *fz, const void *fs) {
@@ -2224,7 +2275,7 @@ static int spectrum_noalloc_dev(ghost_ctx *c, double *scratch, int kind, const v
   const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
   GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   spectrum_kernel<R><<<NOALLOC_BLOCKS, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, c->nspec, nbins, (R)c->Dkk,
-                                                                 scratch);
+                                                                 (R)0.501f, scratch);
   GB_CHECK(post_launch(c));
   double *fin = scratch + (size_t)NOALLOC_BLOCKS * nbins;
   finalize_kernel<<<1, 256, 0, c->stream>>>(scratch, NOALLOC_BLOCKS, nbins, fin);

@@ -120,7 +120,8 @@ __global__ void scale3_kernel(cx<R> *x, cx<R> *y, cx<R> *z, size_t n, R f0, doub
 // pseudospec3D_hd.f90:550-567).  Per-block partials in a fixed grid, then
 // one block sums them in a fixed tree: bitwise reproducible.
 enum RedKind { RED_ENERGY = 0, RED_ENSTROPHY = 1, RED_LAPLACIAN = 2, RED_HELICITY = 3, RED_CROSS = 4,
-               RED_CROSS_K2 = 5, RED_DIVERGENCE = 6, RED_CURL_CROSS = 7 };
+               RED_CROSS_K2 = 5, RED_DIVERGENCE = 6, RED_CURL_CROSS = 7, RED_SC_CROSS = 8, RED_SC_VAR = 9,
+               RED_SC_VAR_K2 = 10 };
 
 template <typename R> struct RedArgs {
   const cx<R> *a, *b, *c, *d, *e, *f;
@@ -155,6 +156,14 @@ __device__ __forceinline__ R red_term(const KParams<R> &kp, const RedArgs<R> &ra
       if (kind == RED_CROSS_K2) s = s * kk2_of(kp, i, j, k);
       return s * kp.tmp;
     }
+    case RED_SC_CROSS: {  // sctrans: Re(a conj(d)) of two scalars
+      const C vd = ra.d[p];
+      return cmulc(va, vd).x * kp.tmp;
+    }
+    case RED_SC_VAR:  // variance / spectrscc: |a|^2
+      return (va.x * va.x + va.y * va.y) * kp.tmp;
+    case RED_SC_VAR_K2:
+      return kk2_of(kp, i, j, k) * (va.x * va.x + va.y * va.y) * kp.tmp;
     case RED_CURL_CROSS: {  // heltrans: Re(curl(a,b,c) . conj(d,e,f))
       const C w1 = curl_at(kp, 1, i, j, k, va, vb, vc), w2 = curl_at(kp, 2, i, j, k, va, vb, vc),
               w3 = curl_at(kp, 3, i, j, k, va, vb, vc);
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(const double *partials, i
 // warp order, blocks in block order: reproducible bit for bit.
 template <typename R>
 __global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R> ra, int kind, size_t n, int nb,
-                                                       R Dkk, double *partials) {
+                                                       R Dkk, R rnd, double *partials) {
   extern __shared__ double hist[];  // (blockDim/32) * nb
   const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int q = threadIdx.x; q < nw * nb; q += blockDim.x) hist[q] = 0.0;
@@ -260,7 +269,7 @@ __global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R>
       int i, j, k;
       unflat(kp, p, i, j, k);
       const R kk2 = kk2_of(kp, i, j, k);
-      const int kmn = (int)(sqrt(kk2) / Dkk + (R)0.501f);  // .501 is a default-REAL literal in GHOST
+      const int kmn = (int)(sqrt(kk2) / Dkk + rnd);  // rnd: .501 rounding of the caller's GHOST routine
       if (kmn > 0 && kmn <= nb) {
         const R wgt = i == 0 ? (R)1 : (R)2;
         bin = kmn - 1;

@@ -568,6 +568,35 @@
          REAL(C_DOUBLE) :: ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_phd_run(ctx,nsteps,ord,dt,nu,kappa,vx,vy,vz,th,fx,fy,fz,fs) &
+                BIND(C,name="ghost_phd_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, th, fx, fy, fz, fs
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt, nu, kappa
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_variance(ctx,a,kin,b) BIND(C,name="ghost_variance") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a
+         INTEGER(C_INT), VALUE :: kin
+         REAL(C_DOUBLE) :: b
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_spectrscc(ctx,a,shift,ek) BIND(C,name="ghost_spectrscc") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a
+         REAL(C_DOUBLE), VALUE :: shift
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_sctrans(ctx,a,b,isc,ek) BIND(C,name="ghost_sctrans") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a, b
+         INTEGER(C_INT), VALUE :: isc
+         REAL(C_DOUBLE) :: ek(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_havgcomp(ctx,u,v,w,th,fo,bv,itype,gsh) BIND(C,name="ghost_havgcomp") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE
          TYPE(C_PTR), VALUE :: ctx, u, v, w, th

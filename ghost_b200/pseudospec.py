@@ -143,6 +143,28 @@ class Ghost:
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
 
+    # ---- passive scalar (PHD_SOL)
+    def phd_run(self, nsteps, ord, dt, nu, kappa, vx, vy, vz, th, fx=None, fy=None, fz=None, fs=None):
+        check(self.lib.ghost_phd_run(self.h, nsteps, ord, dt, nu, kappa,
+                                     *[self._ptr(x, "c") for x in (vx, vy, vz, th, fx, fy, fz, fs)]), "phd_run")
+
+    def variance(self, a, kin: int = 1) -> float:
+        out = ctypes.c_double()
+        check(self.lib.ghost_variance(self.h, self._ptr(a, "c"), kin, ctypes.byref(out)), "ghost_variance")
+        return out.value
+
+    def spectrscc(self, a, shift: float = 0.0):
+        Ek = np.zeros(self.nmax // 2 + 1)
+        check(self.lib.ghost_spectrscc(self.h, self._ptr(a, "c"), shift,
+                                       Ek.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_spectrscc")
+        return Ek
+
+    def sctrans(self, a, b, isc: int = 0):
+        Ek = np.zeros(self.nmax // 2 + 1)
+        check(self.lib.ghost_sctrans(self.h, self._ptr(a, "c"), self._ptr(b, "c"), isc,
+                                     Ek.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_sctrans")
+        return Ek
+
     def havgcomp(self, u, v, w, s, fo: float, bv: float, itype: int):
         """havgcomp: the horizontally averaged profile (nz,) of quantity itype."""
         gsh = np.zeros(self.nz)

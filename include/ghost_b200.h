@@ -205,6 +205,23 @@ int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, c
  * (hmtransfer / hktransfer). */
 int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
                    const void *f, int kin, double *Hk);
+/* ------------------------------------------------------------------
+ * Passive scalar (PHD_SOL, pseudospec3D_phd.f90).
+ * ------------------------------------------------------------------ */
+/* nsteps RK steps of GHOST's PHD solver (include/phd_rkstep2.f90): the HD
+ * step plus th advanced by -v.grad(th) + kappa lap(th) + fs, with the
+ * three-way truncation (th keeps its mean).  Equal to ghost_bouss_run with
+ * omegaz = xmom = xtemp = 0. */
+int ghost_phd_run(ghost_ctx *ctx, int nsteps, int ord, double dt, double nu, double kappa, void *vx, void *vy,
+                  void *vz, void *th, const void *fx, const void *fy, const void *fz, const void *fs);
+/* variance(a,b,kin) (:116-216): b = <|a|^2> (kin 1) or <k^2 |a|^2> (kin 0) */
+int ghost_variance(ghost_ctx *ctx, const void *a, int kin, double *b);
+/* spectrscc(a,Ektot,shift) (:516-609): the scalar's shell sums with bins
+ * int(|k|/Dkk + shift + .501); Ek[nmax/2+1] */
+int ghost_spectrscc(ghost_ctx *ctx, const void *a, double shift, double *Ek);
+/* sctrans(a,b,nmb,isc) (:612-726): shell sums of Re(a conj(b))/(nx ny nz)^2
+ * (GHOST's Ektot; isc only names its file) */
+int ghost_sctrans(ghost_ctx *ctx, const void *a, const void *b, int isc, double *Ek);
 /* havgcomp(gsh,u,v,w,s,fo,bv,itype) (pseudospec3D_bouss.f90:19-554): the
  * horizontally averaged profile gsh[nz] of quantity itype of the
  * Boussinesq fields (velocity u, v, w; temperature s; fo the Coriolis and

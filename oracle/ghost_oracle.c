@@ -1662,3 +1662,107 @@ void o_havgcomp(const octx *c, const cplx *u, const cplx *v, const cplx *w, cons
   for (int k = 0; k < c->nz; ++k) gsh[k] *= scale;
   free(c1); free(c2); free(c3); free(c4); free(r1); free(r2); free(r3);
 }
+
+/* ------------------------------------------------------------------ */
+/* Passive scalar (PHD_SOL).  phd_rkstep2 (include/phd_rkstep2.f90):
+ * prodre3, three nonlhd3, advect3, four laplak3, the three-way truncated
+ * update in which th keeps its mean. */
+void o_phd_rkstep2(const octx *c, int o, double dt_d, double nu_d, double kappa_d, cplx *vx, cplx *vy, cplx *vz,
+                   cplx *th, const cplx *C1, const cplx *C2, const cplx *C3, const cplx *C20, const cplx *fx,
+                   const cplx *fy, const cplx *fz, const cplx *fs) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d, kappa = (real)kappa_d;
+  cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
+       *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
+       *C8 = (cplx *)malloc(sizeof(cplx) * n);
+  o_prodre3(c, vx, vy, vz, C4, C5, C6);
+  o_nonlhd3(c, C4, C5, C6, C7, 1);
+  o_nonlhd3(c, C4, C5, C6, C8, 2);
+  o_nonlhd3(c, C4, C5, C6, C4, 3);
+  o_advect3(c, vx, vy, vz, th, C5);
+  o_laplak3(c, vx, vx);
+  o_laplak3(c, vy, vy);
+  o_laplak3(c, vz, vz);
+  o_laplak3(c, th, th);
+  real rmp = (real)1 / (real)o;
+  cplx z = {0, 0};
+  for (size_t p = 0; p < n; ++p) {
+    if (c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny) {
+      vx[p] = cadd(C1[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vx[p]), C7[p]), fx[p]))));
+      vy[p] = cadd(C2[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vy[p]), C8[p]), fy[p]))));
+      vz[p] = cadd(C3[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(nu, vz[p]), C4[p]), fz[p]))));
+      th[p] = cadd(C20[p], cscal(rmp, cscal(dt, cadd(cadd(cscal(kappa, th[p]), C5[p]), fs[p]))));
+    } else if (c->kn2[p] > c->kmax) {
+      vx[p] = z; vy[p] = z; vz[p] = z; th[p] = z;
+    } else {
+      vx[p] = z; vy[p] = z; vz[p] = z; th[p] = C20[p];
+    }
+  }
+  free(C4); free(C5); free(C6); free(C7); free(C8);
+}
+
+void o_phd_run(const octx *c, int nsteps, int ord, double dt, double nu, double kappa, cplx *vx, cplx *vy,
+               cplx *vz, cplx *th, const cplx *fx, const cplx *fy, const cplx *fz, const cplx *fs) {
+  size_t n = c->nspec;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n), *C20 = (cplx *)malloc(sizeof(cplx) * n);
+  cplx *zf = (cplx *)calloc(n, sizeof(cplx));
+  if (!fx) fx = fy = fz = zf;
+  if (!fs) fs = zf;
+  for (int t = 0; t < nsteps; ++t) {
+    memcpy(C1, vx, sizeof(cplx) * n); memcpy(C2, vy, sizeof(cplx) * n);
+    memcpy(C3, vz, sizeof(cplx) * n); memcpy(C20, th, sizeof(cplx) * n);
+    for (int o = ord; o >= 1; --o) o_phd_rkstep2(c, o, dt, nu, kappa, vx, vy, vz, th, C1, C2, C3, C20, fx, fy, fz, fs);
+  }
+  free(C1); free(C2); free(C3); free(C20); free(zf);
+}
+
+/* variance (pseudospec3D_phd.f90:116-216): sum of w tmp |a|^2 (times kk2 for kin 0) */
+double o_variance(const octx *c, const cplx *a, int kin) {
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  double b = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        real t = w * tmp;
+        if (kin == 0) t = t * c->kk2[p];
+        b += (double)(t * cabs2(a[p]));
+      }
+  }
+  return b;
+}
+
+/* spectrscc (:516-609, bins int(|k|/Dkk + shift + .501_GP)) and sctrans
+ * (:612-726, Re(a conj b)) */
+void o_spectrscc(const octx *c, const cplx *a, double shift, double *Ek) {
+  int nb = c->nmax / 2 + 1;
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  real rnd = (real)shift + (real)0.501;
+  for (int q = 0; q < nb; ++q) Ek[q] = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        int kmn = (int)((real)sqrt(c->kk2[p]) / c->Dkk + rnd);
+        if (kmn > 0 && kmn <= nb) Ek[kmn - 1] += (double)(w * tmp * cabs2(a[p]));
+      }
+  }
+}
+
+void o_sctrans(const octx *c, const cplx *a, const cplx *b, double *Ek) {
+  int nb = c->nmax / 2 + 1;
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  for (int q = 0; q < nb; ++q) Ek[q] = 0.0;
+  for (int i = 0; i < c->nxh; ++i) {
+    real w = i == 0 ? (real)1 : (real)2;
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        int kmn = (int)((real)sqrt(c->kk2[p]) / c->Dkk + (real)0.501f);
+        if (kmn > 0 && kmn <= nb) Ek[kmn - 1] += (double)(w * tmp * cmul(a[p], cconj(b[p])).re);
+      }
+  }
+}

@@ -67,6 +67,10 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_heltrans": (None, [P, P, P, P, P, P, P, P]),
         "o_spec_aniso": (None, [P, I, P, P, P, I, I, P, P]),
         "o_havgcomp": (None, [P, P, P, P, P, D, D, I, P]),
+        "o_phd_run": (None, [P, I, I, D, D, D] + [P] * 8),
+        "o_variance": (D, [P, P, I]),
+        "o_spectrscc": (None, [P, P, D, P]),
+        "o_sctrans": (None, [P, P, P, P]),
         "o_trans_aniso": (None, [P, I, P, P, P, P, P, P, I, I, P]),
         "o_randu": (ctypes.c_double if precision == "fp64" else ctypes.c_float, [P]),
         "o_random_vpot": (ctypes.c_int32, [P, ctypes.c_int32, D, D, I, P, P, P]),
@@ -244,6 +248,28 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def phd_run(self, nsteps, ord, dt, nu, kappa, v, th, f=None, fs=None):
+        """nsteps RK steps of GHOST's passive-scalar solver (phd_rkstep2.f90)."""
+        v = [self._c(x).copy() for x in v]
+        th = self._c(th).copy()
+        fp = [_ptr(self._c(x)) for x in f] if f is not None else [None] * 3
+        fsp = _ptr(self._c(fs)) if fs is not None else None
+        self.lib.o_phd_run(self.h, nsteps, ord, dt, nu, kappa, *[_ptr(x) for x in v], _ptr(th), *fp, fsp)
+        return v, th
+
+    def variance(self, a, kin=1):
+        return self.lib.o_variance(self.h, _ptr(self._c(a)), kin)
+
+    def spectrscc(self, a, shift=0.0):
+        Ek = np.zeros(self.nmax // 2 + 1)
+        self.lib.o_spectrscc(self.h, _ptr(self._c(a)), shift, _ptr(Ek))
+        return Ek
+
+    def sctrans(self, a, b):
+        Ek = np.zeros(self.nmax // 2 + 1)
+        self.lib.o_sctrans(self.h, _ptr(self._c(a)), _ptr(self._c(b)), _ptr(Ek))
+        return Ek
 
     def havgcomp(self, u, v, w, s, fo, bv, itype):
         """havgcomp: the horizontally averaged profile (nz,) of quantity itype."""

@@ -544,3 +544,32 @@ def test_havgcomp_and_tbouss(prec):
     for t in range(11):
         assert np.isclose(avg[t], prof[t].mean(), rtol=1e-12, atol=0)
         assert mx[t] == prof[t].max() and mn[t] == prof[t].min()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_passive_scalar(prec):
+    """The PHD solver (phd_rkstep2.f90) and the scalar diagnostics
+    (variance, spectrscc, sctrans) against the oracle's restatement."""
+    shape = (32, 32, 16)
+    box = dict(Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)
+    o = Oracle(*shape, **box)
+    g = ghost(*shape, precision=prec, **box)
+    v = solenoidal_ic(o, seed=23)
+    th = o.random_solenoidal(24, 1.0, 4.0, 0, 1.0)[0][0]
+    fs = o.random_solenoidal(25, 2.0, 3.0, 0, 0.5)[0][1]
+    cd = g.cdtype_np
+    V = [to_dev(x.astype(cd)) for x in v]
+    TH, FS = to_dev(th.astype(cd)), to_dev(fs.astype(cd))
+    g.phd_run(3, 2, 1e-3, 1e-3, 2e-3, *V, TH, fs=FS)
+    rv, rth = o.phd_run(3, 2, 1e-3, 1e-3, 2e-3, v, th, fs=fs)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    assert rel_l2([to_host(x) for x in V], rv) <= tol
+    assert rel_l2(to_host(TH), rth) <= tol
+    a, b = rand_spectral(o, 26), rand_spectral(o, 27)
+    A, B = to_dev(a.astype(cd)), to_dev(b.astype(cd))
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    for kin in (1, 0):
+        assert abs(g.variance(A, kin) - o.variance(a, kin)) <= tol * o.variance(a, kin)
+    for shift in (0.0, 0.5):
+        assert rel_l2(g.spectrscc(A, shift), o.spectrscc(a, shift)) <= tol
+    assert rel_l2(g.sctrans(A, B), o.sctrans(a, b)) <= tol

@@ -197,3 +197,22 @@ def test_havgcomp_profiles_identities():
     assert np.array_equal(o.havgcomp(*v, s, 1.0, 8.0, 9), o.havgcomp(*v, s, 1.0, 8.0, 0))
     for t in range(11):
         assert np.all(np.isfinite(o.havgcomp(*v, s, 1.0, 8.0, t)))
+
+
+def test_passive_scalar_identities():
+    """The passive-scalar routines (pseudospec3D_phd.f90, phd_rkstep2.f90)
+    on the oracle: the PHD step is the rotating Boussinesq step with no
+    rotation, buoyancy or heat current; advection moves scalar variance
+    between shells without creating it (sum of sctrans(th, -v.grad th) = 0);
+    the scalar spectrum sums to the variance; variance(kin 0) weights by k^2."""
+    o = Oracle(32, 32, 16, Lx=1.0, Ly=1.0, Lz=0.5, arbsize=True)
+    v = solenoidal_ic(o, seed=21)
+    th = o.random_solenoidal(22, 1.0, 4.0, 0, 1.0)[0][0]
+    vp, thp = o.phd_run(2, 2, 1e-3, 1e-3, 2e-3, v, th)
+    vb, thb = o.bouss_run(2, 2, 1e-3, 1e-3, 2e-3, 0.0, 0.0, 0.0, v, th)
+    assert all(np.array_equal(a, b) for a, b in zip(vp, vb)) and np.array_equal(thp, thb)
+    adv = o.advect3(*v, th)
+    T = o.sctrans(th, adv)
+    assert abs(T.sum()) <= 1e-12 * np.abs(T).sum()
+    assert abs(o.spectrscc(th).sum() - o.variance(th, 1)) <= 1e-13 * o.variance(th, 1)
+    assert o.variance(th, 0) > 0
