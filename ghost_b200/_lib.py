@@ -124,6 +124,10 @@ SIGNATURES = {
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
     "ghost_phd_run": [P, I, I, D, D, D, P, P, P, P, P, P, P, P],
+    "ghost_vector3": [P, P, P, P, P, P, P, P, P, P],
+    "ghost_nonlin3": [P, P, P, P, P, P, P, P, I],
+    "ghost_gauge3": [P, P, P, P, P, I],
+    "ghost_mhd_run": [P, I, I, D, D, D] + [P] * 12,
     "ghost_variance": [P, P, I, PD],
     "ghost_spectrscc": [P, P, D, PD],
     "ghost_sctrans": [P, P, P, I, PD],

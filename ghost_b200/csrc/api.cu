@@ -1641,6 +1641,172 @@ int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, c
   return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
 }
 
+// ---------------------------------------------------------------------
+// MHD (MHD_SOL, pseudospec3D_mhd.f90 and include/mhd_rkstep1/2.f90)
+extern "C++" {
+// vector3(a,b,c,d,e,f,x,y,z) (pseudospec3D_mhd.f90:22-105): (a,b,c) x (d,e,f)
+// through real space, times 1/(nx ny nz)^2.  Uses scratch 37..45.
+template <typename R>
+static int vector3_dev(ghost_ctx *c, const void *const in[6], void *const out[3]) {
+  void *sc[46];
+  GB_CHECK(scratch(c, 46, sc));
+  void **r = sc + 37;  // six real inputs, three real products
+  for (int q = 0; q < 6; ++q) GB_CHECK(c2r_dev<R>(c, in[q], r[q]));
+  const R tmp = (R)1 / (((R)c->nx * (R)c->ny * (R)c->nz) * ((R)c->nx * (R)c->ny * (R)c->nz));
+  cross_real_kernel<R><<<grid1d(c->nreal), 256, 0, c->stream>>>((const R *)r[0], (const R *)r[1], (const R *)r[2],
+                                                                 (const R *)r[3], (const R *)r[4], (const R *)r[5],
+                                                                 (R *)r[6], (R *)r[7], (R *)r[8], c->nreal, tmp);
+  GB_CHECK(post_launch(c));
+  for (int q = 0; q < 3; ++q) GB_CHECK(r2c_dev<R>(c, r[6 + q], out[q]));
+  return GHOST_OK;
+}
+
+// nonlin3(a,b,c,d,e,f,g,dir) (:108-227) = nonlhd3 of (a-d, b-e, c-f);
+// gauge3(a,b,c,g,dir) (:230-336) = -nonlhd3(a,b,c,g,dir).  Scratch 34..36.
+template <typename R>
+static int nonlin3_dev(ghost_ctx *c, const void *const in[6], void *g, int dir) {
+  void *sc[46];
+  GB_CHECK(scratch(c, 46, sc));
+  sub3_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(
+      (const cx<R> *)in[0], (const cx<R> *)in[1], (const cx<R> *)in[2], (const cx<R> *)in[3], (const cx<R> *)in[4],
+      (const cx<R> *)in[5], (cx<R> *)sc[34], (cx<R> *)sc[35], (cx<R> *)sc[36], c->ntot);
+  GB_CHECK(post_launch(c));
+  return nonlhd3_impl<R>(c, sc[34], sc[35], sc[36], g, dir);
+}
+template <typename R> static int gauge3_dev(ghost_ctx *c, const void *a, const void *b, const void *cc, void *g, int dir) {
+  GB_CHECK(nonlhd3_impl<R>(c, a, b, cc, g, dir));
+  neg_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>((cx<R> *)g, c->ntot);
+  return post_launch(c);
+}
+
+// One MHD substep (include/mhd_rkstep2.f90); Cv, Ca the RK copies of v, a
+template <typename R>
+static int mhd_substep_dev(ghost_ctx *c, int o, double dt, double nu, double mu, void *const v[3], void *const a[3],
+                           void *const Cv[3], void *const Ca[3], const void *const f[3], const void *const m[3]) {
+  void *sc[46];
+  GB_CHECK(scratch(c, 46, sc));
+  void *B[3] = {sc[22], sc[23], sc[24]}, *N1[3] = {sc[25], sc[26], sc[27]}, *N2[3] = {sc[28], sc[29], sc[30]};
+  void *G[3] = {sc[31], sc[32], sc[33]};
+  // b = curl a (rotor3(ay,az,C7,1), rotor3(ax,az,C8,2), rotor3(ax,ay,C9,3))
+  GB_CHECK(rotor3_impl<R>(c, a[1], a[2], B[0], 1));
+  GB_CHECK(rotor3_impl<R>(c, a[0], a[2], B[1], 2));
+  GB_CHECK(rotor3_impl<R>(c, a[0], a[1], B[2], 3));
+  GB_CHECK(prodre3_dev<R>(c, v[0], v[1], v[2], N1[0], N1[1], N1[2]));  // w x v
+  GB_CHECK(prodre3_dev<R>(c, B[0], B[1], B[2], N2[0], N2[1], N2[2]));  // j x b
+  const void *nl[6] = {N1[0], N1[1], N1[2], N2[0], N2[1], N2[2]};
+  for (int d = 0; d < 3; ++d) GB_CHECK(nonlin3_dev<R>(c, nl, G[d], d + 1));
+  // v x b into N1, its Coulomb-gauge projection into N2
+  const void *vb[6] = {v[0], v[1], v[2], B[0], B[1], B[2]};
+  GB_CHECK(vector3_dev<R>(c, vb, N1));
+  for (int d = 0; d < 3; ++d) GB_CHECK(gauge3_dev<R>(c, N1[0], N1[1], N1[2], N2[d], d + 1));
+  MhdUpd<R> u{};
+  for (int q = 0; q < 3; ++q) {
+    u.v[q] = (cx<R> *)v[q];
+    u.a[q] = (cx<R> *)a[q];
+    u.cv[q] = (const cx<R> *)Cv[q];
+    u.ca[q] = (const cx<R> *)Ca[q];
+    u.g[q] = (const cx<R> *)G[q];
+    u.h[q] = (const cx<R> *)N2[q];
+    u.f[q] = f ? (const cx<R> *)f[q] : nullptr;
+    u.m[q] = m ? (const cx<R> *)m[q] : nullptr;
+  }
+  mhd_update_kernel<R><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<R>(c), u, c->ntot, (R)dt, (R)nu, (R)mu,
+                                                                (R)1 / (R)o);
+  return post_launch(c);
+}
+
+template <typename R>
+static int mhd_run_dev(ghost_ctx *c, int nsteps, int ord, double dt, double nu, double mu, void *const v[3],
+                       void *const a[3], const void *const f[3], const void *const m[3]) {
+  void *sc[46];
+  GB_CHECK(scratch(c, 46, sc));
+  void *Cv[3] = {sc[16], sc[17], sc[18]}, *Ca[3] = {sc[19], sc[20], sc[21]};
+  for (int s = 0; s < nsteps; ++s) {
+    // mhd_rkstep1: C1..C6 = v, a
+    for (int q = 0; q < 3; ++q) {
+      GB_CUDA(cudaMemcpyAsync(Cv[q], v[q], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+      GB_CUDA(cudaMemcpyAsync(Ca[q], a[q], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    for (int o = ord; o >= 1; --o) GB_CHECK(mhd_substep_dev<R>(c, o, dt, nu, mu, v, a, Cv, Ca, f, m));
+  }
+  return check_status(c);
+}
+}  // extern "C++"
+
+int ghost_vector3(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, void *x, void *y, void *z) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e || !f || !x || !y || !z) return fail(GHOST_ERR_ARG, "null field");
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts are not supported here");
+  Staging st(c);
+  const void *in[6];
+  void *out[3];
+  const void *src[6] = {a, b, cc, d, e, f};
+  void *dst[3] = {x, y, z};
+  for (int q = 0; q < 6; ++q) GB_CHECK(st.map(src[q], c->cbytes, 1, &in[q]));
+  for (int q = 0; q < 3; ++q) GB_CHECK(st.map(dst[q], c->cbytes, 2, &out[q]));
+  GB_CHECK(c->precision == GHOST_SINGLE ? vector3_dev<float>(c, in, out) : vector3_dev<double>(c, in, out));
+  return st.finish();
+}
+
+int ghost_nonlin3(ghost_ctx *c, const void *a, const void *b, const void *cc, const void *d, const void *e,
+                  const void *f, void *g, int dir) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !d || !e || !f || !g) return fail(GHOST_ERR_ARG, "null field");
+  if (!dir_ok(dir)) return fail(GHOST_ERR_ARG, "dir %d not in 1..3", dir);
+  Staging st(c);
+  const void *in[6];
+  void *dg;
+  const void *src[6] = {a, b, cc, d, e, f};
+  for (int q = 0; q < 6; ++q) GB_CHECK(st.map(src[q], c->cbytes, 1, &in[q]));
+  GB_CHECK(st.map(g, c->cbytes, 2, &dg));
+  GB_CHECK(c->precision == GHOST_SINGLE ? nonlin3_dev<float>(c, in, dg, dir) : nonlin3_dev<double>(c, in, dg, dir));
+  return st.finish();
+}
+
+int ghost_gauge3(ghost_ctx *c, const void *a, const void *b, const void *cc, void *g, int dir) {
+  CTX_CHECK(c);
+  if (!a || !b || !cc || !g) return fail(GHOST_ERR_ARG, "null field");
+  if (!dir_ok(dir)) return fail(GHOST_ERR_ARG, "dir %d not in 1..3", dir);
+  Staging st(c);
+  const void *da, *db, *dc;
+  void *dg;
+  GB_CHECK(st.map(a, c->cbytes, 1, &da));
+  GB_CHECK(st.map(b, c->cbytes, 1, &db));
+  GB_CHECK(st.map(cc, c->cbytes, 1, &dc));
+  GB_CHECK(st.map(g, c->cbytes, 2, &dg));
+  GB_CHECK(c->precision == GHOST_SINGLE ? gauge3_dev<float>(c, da, db, dc, dg, dir)
+                                        : gauge3_dev<double>(c, da, db, dc, dg, dir));
+  return st.finish();
+}
+
+int ghost_mhd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, double mu, void *vx, void *vy, void *vz,
+                  void *ax, void *ay, void *az, const void *fx, const void *fy, const void *fz, const void *mx,
+                  const void *my, const void *mz) {
+  CTX_CHECK(c);
+  if (!vx || !vy || !vz || !ax || !ay || !az) return fail(GHOST_ERR_ARG, "null field");
+  if (nsteps < 0 || ord < 1) return fail(GHOST_ERR_ARG, "nsteps %d, ord %d", nsteps, ord);
+  if ((!fx) != (!fy) || (!fx) != (!fz) || (!mx) != (!my) || (!mx) != (!mz))
+    return fail(GHOST_ERR_ARG, "forcing components must all be given or all be null");
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts are not supported here");
+  Staging st(c);
+  void *v[3], *a[3];
+  const void *f[3] = {nullptr, nullptr, nullptr}, *m[3] = {nullptr, nullptr, nullptr};
+  void *vs[3] = {vx, vy, vz}, *as[3] = {ax, ay, az};
+  const void *fs[3] = {fx, fy, fz}, *ms[3] = {mx, my, mz};
+  for (int q = 0; q < 3; ++q) {
+    GB_CHECK(st.map(vs[q], c->cbytes, 3, &v[q]));
+    GB_CHECK(st.map(as[q], c->cbytes, 3, &a[q]));
+    if (fx) GB_CHECK(st.map(fs[q], c->cbytes, 1, &f[q]));
+    if (mx) GB_CHECK(st.map(ms[q], c->cbytes, 1, &m[q]));
+  }
+  GB_CHECK(c->precision == GHOST_SINGLE ? mhd_run_dev<float>(c, nsteps, ord, dt, nu, mu, v, a, fx ? f : nullptr,
+                                                             mx ? m : nullptr)
+                                        : mhd_run_dev<double>(c, nsteps, ord, dt, nu, mu, v, a, fx ? f : nullptr,
+                                                              mx ? m : nullptr));
+  return st.finish();
+}
+
 // Passive scalar (pseudospec3D_phd.f90): variance (:116-216), spectrscc
 // (:516-609), sctrans (:612-726) of a scalar spectral field.
 int ghost_variance(ghost_ctx *c, const void *a, int kin, double *out) {

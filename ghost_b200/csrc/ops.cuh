@@ -384,6 +384,74 @@ __global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra
   }
 }
 
+// vector3's real-space cross product (pseudospec3D_mhd.f90:22-105):
+// x = (b f - e c) tmp, y = (c d - f a) tmp, z = (a e - d b) tmp for the real
+// fields (a, b, c) x (d, e, f), tmp = 1/(nx ny nz)^2
+template <typename R>
+__global__ void cross_real_kernel(const R *__restrict__ a, const R *__restrict__ b, const R *__restrict__ c,
+                                  const R *__restrict__ d, const R *__restrict__ e, const R *__restrict__ f,
+                                  R *__restrict__ x, R *__restrict__ y, R *__restrict__ z, size_t n, R tmp) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const R r1 = a[p], r2 = b[p], r3 = c[p], r4 = d[p], r5 = e[p], r6 = f[p];
+    x[p] = (r2 * r6 - r5 * r3) * tmp;
+    y[p] = (r3 * r4 - r6 * r1) * tmp;
+    z[p] = (r1 * r5 - r4 * r2) * tmp;
+  }
+}
+
+// o = a - d, componentwise over three field pairs (nonlin3's a - d, b - e, c - f)
+template <typename R>
+__global__ void sub3_kernel(const cx<R> *a, const cx<R> *b, const cx<R> *c, const cx<R> *d, const cx<R> *e,
+                            const cx<R> *f, cx<R> *x, cx<R> *y, cx<R> *z, size_t n) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    x[p] = csub(a[p], d[p]);
+    y[p] = csub(b[p], e[p]);
+    z[p] = csub(c[p], f[p]);
+  }
+}
+
+template <typename R>
+__global__ void neg_kernel(cx<R> *x, size_t n) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+    x[p] = mk(-x[p].x, -x[p].y);
+}
+
+// The truncated update of mhd_rkstep2 (include/mhd_rkstep2.f90): with
+// laplak3 inline, v = C + dt (nu lap v + g + f)/o and a = C' + dt (mu lap a
+// + h + m)/o on tiny <= kn2 <= kmax, everything zero elsewhere.
+template <typename R> struct MhdUpd {
+  cx<R> *v[3], *a[3];
+  const cx<R> *cv[3], *ca[3], *g[3], *h[3], *f[3], *m[3];
+};
+template <typename R>
+__global__ void mhd_update_kernel(KParams<R> kp, MhdUpd<R> u, size_t n, R dt, R nu, R mu, R rmp) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    const R kn2 = kn2_of(kp, i, j, k);
+    if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
+      const R kk2 = kk2_of(kp, i, j, k);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const cx<R> vv = u.v[q][p], aa = u.a[q][p];
+        const cx<R> lv = mk(-kk2 * vv.x, -kk2 * vv.y), la = mk(-kk2 * aa.x, -kk2 * aa.y);
+        cx<R> sv = mk(nu * lv.x + u.g[q][p].x, nu * lv.y + u.g[q][p].y);
+        cx<R> sa = mk(mu * la.x + u.h[q][p].x, mu * la.y + u.h[q][p].y);
+        if (u.f[q]) sv = cadd(sv, u.f[q][p]);
+        if (u.m[q]) sa = cadd(sa, u.m[q][p]);
+        u.v[q][p] = mk(u.cv[q][p].x + dt * sv.x * rmp, u.cv[q][p].y + dt * sv.y * rmp);
+        u.a[q][p] = mk(u.ca[q][p].x + dt * sa.x * rmp, u.ca[q][p].y + dt * sa.y * rmp);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        u.v[q][p] = mk((R)0, (R)0);
+        u.a[q][p] = mk((R)0, (R)0);
+      }
+    }
+  }
+}
+
 // Horizontal (x, y) sums of real fields per z-plane (havgcomp,
 // pseudospec3D_bouss.f90:19-554): block (k, s) sums a strided part of plane k
 // of op(r1, r2, r3) into partials[k * gridDim.y + s].

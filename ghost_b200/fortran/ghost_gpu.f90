@@ -568,6 +568,31 @@
          REAL(C_DOUBLE) :: ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_vector3(ctx,a,b,c,d,e,f,x,y,z) BIND(C,name="ghost_vector3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f, x, y, z
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_nonlin3(ctx,a,b,c,d,e,f,g,dir) BIND(C,name="ghost_nonlin3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f, g
+         INTEGER(C_INT), VALUE :: dir
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_gauge3(ctx,a,b,c,g,dir) BIND(C,name="ghost_gauge3") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, a, b, c, g
+         INTEGER(C_INT), VALUE :: dir
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_mhd_run(ctx,nsteps,ord,dt,nu,mu,vx,vy,vz,ax,ay,az,fx,fy,fz,mx,my,mz) &
+                BIND(C,name="ghost_mhd_run") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, vx, vy, vz, ax, ay, az, fx, fy, fz, mx, my, mz
+         INTEGER(C_INT), VALUE :: nsteps, ord
+         REAL(C_DOUBLE), VALUE :: dt, nu, mu
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_phd_run(ctx,nsteps,ord,dt,nu,kappa,vx,vy,vz,th,fx,fy,fz,fs) &
                 BIND(C,name="ghost_phd_run") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE

@@ -143,6 +143,26 @@ class Ghost:
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
 
+    # ---- MHD (MHD_SOL)
+    def vector3(self, a, b, c, d, e, f, x=None, y=None, z=None):
+        out = [self.czeros() if o is None else o for o in (x, y, z)]
+        check(self.lib.ghost_vector3(self.h, *[self._ptr(q, "c") for q in (a, b, c, d, e, f, *out)]), "vector3")
+        return out
+
+    def nonlin3(self, a, b, c, d, e, f, dir: int, g=None):
+        g = self.czeros() if g is None else g
+        check(self.lib.ghost_nonlin3(self.h, *[self._ptr(q, "c") for q in (a, b, c, d, e, f, g)], dir), "nonlin3")
+        return g
+
+    def gauge3(self, a, b, c, dir: int, g=None):
+        g = self.czeros() if g is None else g
+        check(self.lib.ghost_gauge3(self.h, *[self._ptr(q, "c") for q in (a, b, c, g)], dir), "gauge3")
+        return g
+
+    def mhd_run(self, nsteps, ord, dt, nu, mu, vx, vy, vz, ax, ay, az, f=(None, None, None), m=(None, None, None)):
+        check(self.lib.ghost_mhd_run(self.h, nsteps, ord, dt, nu, mu,
+                                     *[self._ptr(q, "c") for q in (vx, vy, vz, ax, ay, az, *f, *m)]), "mhd_run")
+
     # ---- passive scalar (PHD_SOL)
     def phd_run(self, nsteps, ord, dt, nu, kappa, vx, vy, vz, th, fx=None, fy=None, fz=None, fs=None):
         check(self.lib.ghost_phd_run(self.h, nsteps, ord, dt, nu, kappa,

@@ -206,6 +206,28 @@ int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, c
 int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
                    const void *f, int kin, double *Hk);
 /* ------------------------------------------------------------------
+ * MHD (MHD_SOL, pseudospec3D_mhd.f90, include/mhd_rkstep1/2.f90): velocity
+ * v and magnetic vector potential a (b = curl a).
+ * ------------------------------------------------------------------ */
+/* vector3(a,b,c,d,e,f,x,y,z) (:22-105): (a,b,c) x (d,e,f) through real
+ * space, times 1/(nx ny nz)^2 */
+int ghost_vector3(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                  const void *f, void *x, void *y, void *z);
+/* nonlin3(a,b,c,d,e,f,g,dir) (:108-227): g = -(a-d)_dir + k_dir k.(a-d)/k^2,
+ * the projected difference of the two nonlinear terms (w x v and j x b) */
+int ghost_nonlin3(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
+                  const void *f, void *g, int dir);
+/* gauge3(a,b,c,g,dir) (:230-336): g = a_dir - k_dir k.a/k^2 (Coulomb gauge) */
+int ghost_gauge3(ghost_ctx *ctx, const void *a, const void *b, const void *c, void *g, int dir);
+/* nsteps RK steps of GHOST's MHD solver: per substep b = curl a, the
+ * projected (w x v - j x b), the gauged v x b, and the truncated update of
+ * v (viscosity nu, forcing f) and a (diffusivity mu, forcing m); f and m
+ * may be NULL */
+int ghost_mhd_run(ghost_ctx *ctx, int nsteps, int ord, double dt, double nu, double mu, void *vx, void *vy, void *vz,
+                  void *ax, void *ay, void *az, const void *fx, const void *fy, const void *fz, const void *mx,
+                  const void *my, const void *mz);
+
+/* ------------------------------------------------------------------
  * Passive scalar (PHD_SOL, pseudospec3D_phd.f90).
  * ------------------------------------------------------------------ */
 /* nsteps RK steps of GHOST's PHD solver (include/phd_rkstep2.f90): the HD

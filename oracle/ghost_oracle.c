@@ -1766,3 +1766,143 @@ void o_sctrans(const octx *c, const cplx *a, const cplx *b, double *Ek) {
       }
   }
 }
+
+/* ------------------------------------------------------------------ */
+/* MHD (pseudospec3D_mhd.f90, include/mhd_rkstep2.f90). */
+/* vector3 (:22-105): the real fields of (a,b,c) and (d,e,f), their cross
+ * product times 1/(nx ny nz)^2, back to Fourier space */
+void o_vector3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d, const cplx *e,
+               const cplx *f, cplx *x, cplx *y, cplx *z) {
+  size_t nr = c->nreal;
+  real *r[7];
+  for (int q = 0; q < 7; ++q) r[q] = (real *)malloc(sizeof(real) * nr);
+  o_fftp3d_complex_to_real(c, a, r[0]); o_fftp3d_complex_to_real(c, b, r[1]);
+  o_fftp3d_complex_to_real(c, cc, r[2]); o_fftp3d_complex_to_real(c, d, r[3]);
+  o_fftp3d_complex_to_real(c, e, r[4]); o_fftp3d_complex_to_real(c, f, r[5]);
+  real tmp = (real)1 / (((real)c->nx * (real)c->ny * (real)c->nz) * ((real)c->nx * (real)c->ny * (real)c->nz));
+  for (size_t p = 0; p < nr; ++p) {
+    real r1 = r[0][p], r2 = r[1][p], r3 = r[2][p], r4 = r[3][p], r5 = r[4][p], r6 = r[5][p];
+    r[6][p] = (r2 * r6 - r5 * r3) * tmp;
+    r[2][p] = (r3 * r4 - r6 * r1) * tmp;
+    r[0][p] = (r1 * r5 - r4 * r2) * tmp;
+  }
+  o_fftp3d_real_to_complex(c, r[6], x);
+  o_fftp3d_real_to_complex(c, r[2], y);
+  o_fftp3d_real_to_complex(c, r[0], z);
+  for (int q = 0; q < 7; ++q) free(r[q]);
+}
+
+/* nonlin3 (:108-227) and gauge3 (:230-336), statement by statement */
+void o_nonlin3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, const cplx *d, const cplx *e,
+               const cplx *f, cplx *g, int dir) {
+  cplx *out = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        cplx s = dir == 1 ? a[p] : (dir == 2 ? b[p] : cc[p]);
+        cplx t = dir == 1 ? d[p] : (dir == 2 ? e[p] : f[p]);
+        cplx base = cadd(cscal(-1, s), t);
+        int zero_plane = dir == 1 ? (i == 0) : (dir == 2 ? (j == 0) : (k == 0));
+        if (zero_plane) {
+          out[p] = base;
+        } else {
+          real kd = dir == 1 ? c->kx[i] : (dir == 2 ? c->ky[j] : c->kz[k]);
+          cplx q = cadd(cadd(cscal(c->kx[i], csub(a[p], d[p])), cscal(c->ky[j], csub(b[p], e[p]))),
+                        cscal(c->kz[k], csub(cc[p], f[p])));
+          q = cscal(kd, q);
+          q.re = q.re / c->kk2[p];
+          q.im = q.im / c->kk2[p];
+          out[p] = cadd(base, q);
+        }
+      }
+  memcpy(g, out, sizeof(cplx) * c->nspec);
+  free(out);
+}
+
+void o_gauge3(const octx *c, const cplx *a, const cplx *b, const cplx *cc, cplx *g, int dir) {
+  cplx *out = (cplx *)malloc(sizeof(cplx) * c->nspec);
+  for (int i = 0; i < c->nxh; ++i)
+    for (int j = 0; j < c->ny; ++j)
+      for (int k = 0; k < c->nz; ++k) {
+        size_t p = SIDX(c, k, j, i);
+        cplx s = dir == 1 ? a[p] : (dir == 2 ? b[p] : cc[p]);
+        int zero_plane = dir == 1 ? (i == 0) : (dir == 2 ? (j == 0) : (k == 0));
+        if (zero_plane) {
+          out[p] = s;
+        } else {
+          real kd = dir == 1 ? c->kx[i] : (dir == 2 ? c->ky[j] : c->kz[k]);
+          cplx q = cadd(cadd(cscal(c->kx[i], a[p]), cscal(c->ky[j], b[p])), cscal(c->kz[k], cc[p]));
+          q = cscal(kd, q);
+          q.re = q.re / c->kk2[p];
+          q.im = q.im / c->kk2[p];
+          out[p] = csub(s, q);
+        }
+      }
+  memcpy(g, out, sizeof(cplx) * c->nspec);
+  free(out);
+}
+
+/* mhd_rkstep2 (include/mhd_rkstep2.f90) */
+void o_mhd_rkstep2(const octx *c, int o, double dt_d, double nu_d, double mu_d, cplx *vx, cplx *vy, cplx *vz,
+                   cplx *ax, cplx *ay, cplx *az, const cplx *const C[6], const cplx *const fv[3],
+                   const cplx *const fm[3]) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d, mu = (real)mu_d;
+  cplx *W[11];
+  for (int q = 0; q < 11; ++q) W[q] = (cplx *)malloc(sizeof(cplx) * n);
+  cplx *C7 = W[0], *C8 = W[1], *C9 = W[2], *C10 = W[3], *C11 = W[4], *C12 = W[5], *C13 = W[6], *C14 = W[7],
+       *C15 = W[8], *C16 = W[9], *C17 = W[10];
+  o_rotor3(c, ay, az, C7, 1);
+  o_rotor3(c, ax, az, C8, 2);
+  o_rotor3(c, ax, ay, C9, 3);
+  o_prodre3(c, vx, vy, vz, C10, C11, C12);
+  o_prodre3(c, C7, C8, C9, C13, C14, C15);
+  o_nonlin3(c, C10, C11, C12, C13, C14, C15, C16, 1);
+  o_nonlin3(c, C10, C11, C12, C13, C14, C15, C17, 2);
+  o_nonlin3(c, C10, C11, C12, C13, C14, C15, C10, 3);
+  o_vector3(c, vx, vy, vz, C7, C8, C9, C11, C12, C13);
+  o_gauge3(c, C11, C12, C13, C7, 1);
+  o_gauge3(c, C11, C12, C13, C8, 2);
+  o_gauge3(c, C11, C12, C13, C9, 3);
+  o_laplak3(c, vx, vx); o_laplak3(c, vy, vy); o_laplak3(c, vz, vz);
+  o_laplak3(c, ax, ax); o_laplak3(c, ay, ay); o_laplak3(c, az, az);
+  real rmp = (real)1 / (real)o;
+  cplx zc = {0, 0};
+  cplx *vv[3] = {vx, vy, vz}, *aa[3] = {ax, ay, az};
+  const cplx *gv[3] = {C16, C17, C10}, *ga[3] = {C7, C8, C9};
+  for (size_t p = 0; p < n; ++p) {
+    int keep = c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny;
+    for (int q = 0; q < 3; ++q) {
+      if (keep) {
+        cplx sv = cadd(cscal(nu, vv[q][p]), gv[q][p]);
+        if (fv) sv = cadd(sv, fv[q][p]);
+        cplx sa = cadd(cscal(mu, aa[q][p]), ga[q][p]);
+        if (fm) sa = cadd(sa, fm[q][p]);
+        vv[q][p] = cadd(C[q][p], cscal(rmp, cscal(dt, sv)));
+        aa[q][p] = cadd(C[3 + q][p], cscal(rmp, cscal(dt, sa)));
+      } else {
+        vv[q][p] = zc;
+        aa[q][p] = zc;
+      }
+    }
+  }
+  for (int q = 0; q < 11; ++q) free(W[q]);
+}
+
+void o_mhd_run(const octx *c, int nsteps, int ord, double dt, double nu, double mu, cplx *vx, cplx *vy, cplx *vz,
+               cplx *ax, cplx *ay, cplx *az, const cplx *fx, const cplx *fy, const cplx *fz, const cplx *mx,
+               const cplx *my, const cplx *mz) {
+  size_t n = c->nspec;
+  cplx *Cs[6];
+  for (int q = 0; q < 6; ++q) Cs[q] = (cplx *)malloc(sizeof(cplx) * n);
+  const cplx *C[6] = {Cs[0], Cs[1], Cs[2], Cs[3], Cs[4], Cs[5]};
+  const cplx *fv[3] = {fx, fy, fz}, *fm[3] = {mx, my, mz};
+  cplx *src[6] = {vx, vy, vz, ax, ay, az};
+  for (int t = 0; t < nsteps; ++t) {
+    for (int q = 0; q < 6; ++q) memcpy(Cs[q], src[q], sizeof(cplx) * n);
+    for (int o = ord; o >= 1; --o)
+      o_mhd_rkstep2(c, o, dt, nu, mu, vx, vy, vz, ax, ay, az, C, fx ? fv : NULL, mx ? fm : NULL);
+  }
+  for (int q = 0; q < 6; ++q) free(Cs[q]);
+}

@@ -68,6 +68,10 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_spec_aniso": (None, [P, I, P, P, P, I, I, P, P]),
         "o_havgcomp": (None, [P, P, P, P, P, D, D, I, P]),
         "o_phd_run": (None, [P, I, I, D, D, D] + [P] * 8),
+        "o_vector3": (None, [P] * 10),
+        "o_nonlin3": (None, [P] * 8 + [I]),
+        "o_gauge3": (None, [P] * 5 + [I]),
+        "o_mhd_run": (None, [P, I, I, D, D, D] + [P] * 12),
         "o_variance": (D, [P, P, I]),
         "o_spectrscc": (None, [P, P, D, P]),
         "o_sctrans": (None, [P, P, P, P]),
@@ -248,6 +252,33 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def vector3(self, a, b, c, d, e, f):
+        arrs = [self._c(x) for x in (a, b, c, d, e, f)]
+        out = [self.czeros() for _ in range(3)]
+        self.lib.o_vector3(self.h, *[_ptr(x) for x in arrs], *[_ptr(x) for x in out])
+        return out
+
+    def nonlin3(self, a, b, c, d, e, f, dir):
+        arrs = [self._c(x) for x in (a, b, c, d, e, f)]
+        g = self.czeros()
+        self.lib.o_nonlin3(self.h, *[_ptr(x) for x in arrs], _ptr(g), dir)
+        return g
+
+    def gauge3(self, a, b, c, dir):
+        arrs = [self._c(x) for x in (a, b, c)]
+        g = self.czeros()
+        self.lib.o_gauge3(self.h, *[_ptr(x) for x in arrs], _ptr(g), dir)
+        return g
+
+    def mhd_run(self, nsteps, ord, dt, nu, mu, v, a, f=None, m=None):
+        """nsteps RK steps of GHOST's MHD solver (mhd_rkstep2.f90)."""
+        v = [self._c(x).copy() for x in v]
+        a = [self._c(x).copy() for x in a]
+        fp = [_ptr(self._c(x)) for x in f] if f is not None else [None] * 3
+        mp = [_ptr(self._c(x)) for x in m] if m is not None else [None] * 3
+        self.lib.o_mhd_run(self.h, nsteps, ord, dt, nu, mu, *[_ptr(x) for x in v], *[_ptr(x) for x in a], *fp, *mp)
+        return v, a
 
     def phd_run(self, nsteps, ord, dt, nu, kappa, v, th, f=None, fs=None):
         """nsteps RK steps of GHOST's passive-scalar solver (phd_rkstep2.f90)."""

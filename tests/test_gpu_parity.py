@@ -573,3 +573,31 @@ def test_passive_scalar(prec):
     for shift in (0.0, 0.5):
         assert rel_l2(g.spectrscc(A, shift), o.spectrscc(a, shift)) <= tol
     assert rel_l2(g.sctrans(A, B), o.sctrans(a, b)) <= tol
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_mhd(prec):
+    """GHOST's MHD operators (vector3, nonlin3, gauge3) and a forced MHD run
+    (mhd_rkstep2.f90) against the oracle's restatement."""
+    shape = (32, 32, 32)
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    cd = g.cdtype_np
+    v = solenoidal_ic(o, seed=41)
+    a = [0.3 * x for x in solenoidal_ic(o, seed=42)]
+    f = o.random_solenoidal(43, 2.0, 3.0, 0, 1.0)[0]
+    m = o.random_solenoidal(44, 2.0, 3.0, 0, 0.5)[0]
+    r = [rand_spectral(o, 45 + q) for q in range(6)]
+    R = [to_dev(x.astype(cd)) for x in r]
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    assert rel_l2([to_host(x) for x in g.vector3(*R)], o.vector3(*r)) <= tol
+    for d in (1, 2, 3):
+        assert rel_l2(to_host(g.nonlin3(*R, d)), o.nonlin3(*r, d)) <= tol
+        assert rel_l2(to_host(g.gauge3(*R[:3], d)), o.gauge3(*r[:3], d)) <= tol
+    V = [to_dev(x.astype(cd)) for x in v]
+    A = [to_dev(x.astype(cd)) for x in a]
+    g.mhd_run(3, 2, 1e-3, 1e-3, 2e-3, *V, *A, f=[to_dev(x.astype(cd)) for x in f], m=[to_dev(x.astype(cd)) for x in m])
+    rv, ra = o.mhd_run(3, 2, 1e-3, 1e-3, 2e-3, v, a, f=f, m=m)
+    tol = 1e-11 if prec == "fp64" else 1e-5
+    assert rel_l2([to_host(x) for x in V], rv) <= tol
+    assert rel_l2([to_host(x) for x in A], ra) <= tol

@@ -216,3 +216,23 @@ def test_passive_scalar_identities():
     assert abs(T.sum()) <= 1e-12 * np.abs(T).sum()
     assert abs(o.spectrscc(th).sum() - o.variance(th, 1)) <= 1e-13 * o.variance(th, 1)
     assert o.variance(th, 0) > 0
+
+
+def test_mhd_identities():
+    """The MHD routines (pseudospec3D_mhd.f90, mhd_rkstep2.f90) on the
+    oracle: v x v = 0; the gauged field is divergence-free; nonlin3 with no
+    magnetic term is nonlhd3; with a = 0 the MHD run is the HD run."""
+    o = Oracle(32)
+    v = solenoidal_ic(o, seed=31)
+    x = o.vector3(*v, *v)
+    assert all(np.abs(q).max() <= 1e-14 * np.abs(v[0]).max() for q in x)
+    w = [o.random_solenoidal(32 + q, 1.0, 6.0, 0, 1.0)[0][q] for q in range(3)]
+    g = [o.gauge3(*w, d) for d in (1, 2, 3)]
+    assert o.divergence(*g) <= 1e-20 * o.energy(*g, 1) + 1e-30
+    z = [np.zeros_like(v[0]) for _ in range(3)]
+    for d in (1, 2, 3):
+        assert np.allclose(o.nonlin3(*w, *z, d), o.nonlhd3(*w, d), rtol=0, atol=1e-15 * np.abs(w[0]).max())
+    vm, am = o.mhd_run(2, 2, 1e-3, 1e-3, 1e-3, v, z)
+    vh = o.hd_run(2, 2, 1e-3, 1e-3, v)
+    assert rel_l2(vm, vh) <= 1e-14
+    assert all(np.abs(q).max() == 0 for q in am)
