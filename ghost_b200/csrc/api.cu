@@ -1641,6 +1641,23 @@ int ghost_heltrans(ghost_ctx *c, const void *a, const void *b, const void *cc, c
   return transfer(c, RED_CURL_CROSS, a, b, cc, d, e, f, Hk);
 }
 
+int ghost_phaseshift(ghost_ctx *c, void *a, double cre, double cim) {
+  CTX_CHECK(c);
+  if (!a) return fail(GHOST_ERR_ARG, "null field");
+  if (c->nruns != 1) return fail(GHOST_ERR_STATE, "batched contexts are not supported here");
+  Staging st(c);
+  void *da;
+  GB_CHECK(st.map(a, c->cbytes, 3, &da));
+  if (c->precision == GHOST_SINGLE)
+    phaseshift_kernel<float><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<float>(c), (cx<float> *)da, c->ntot,
+                                                                      make_float2((float)cre, (float)cim));
+  else
+    phaseshift_kernel<double><<<grid1d(c->ntot), 256, 0, c->stream>>>(kparams<double>(c), (cx<double> *)da, c->ntot,
+                                                                       make_double2(cre, cim));
+  GB_CHECK(post_launch(c));
+  return st.finish();
+}
+
 // ---------------------------------------------------------------------
 // MHD (MHD_SOL, pseudospec3D_mhd.f90 and include/mhd_rkstep1/2.f90)
 extern "C++" {

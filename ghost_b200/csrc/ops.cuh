@@ -384,6 +384,40 @@ __global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra
   }
 }
 
+// phaseshift (pseudospec3D_hd.f90:2084-2148): a *= c, except on the kx = 0
+// plane, where GHOST's loops multiply the modes of one half by c and their
+// mirrors by conj(c).  The kz = nz/2 and ky = ny/2 lines of that plane are
+// reached by both loops and so take both factors, in the order the loops
+// apply them.
+template <typename R>
+__global__ void phaseshift_kernel(KParams<R> kp, cx<R> *a, size_t n, cx<R> cd) {
+  const cx<R> jd = mk(cd.x, -cd.y);
+  const int nyh = kp.ny / 2, nzh = kp.nz / 2;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflat(kp, p, i, j, k);
+    cx<R> v = a[p];
+    if (i > 0) {
+      v = cmul(v, cd);
+    } else if (k == 0 && j == 0) {
+    } else if (k == 0 || j == 0) {  // the ky = 0 row or the kz = 0 row of the plane
+      const int q = k == 0 ? j : k, h = k == 0 ? nyh : nzh;
+      if (q < h) v = cmul(v, cd);
+      else if (q == h) v = cmul(cmul(v, cd), jd);
+      else v = cmul(v, jd);
+    } else if (k < nzh) {
+      v = cmul(v, cd);
+    } else if (k > nzh) {
+      v = cmul(v, jd);
+    } else if (j <= nyh) {  // k = nz/2: reached as the direct mode first
+      v = cmul(cmul(v, cd), jd);
+    } else {  // reached as a mirror first
+      v = cmul(cmul(v, jd), cd);
+    }
+    a[p] = v;
+  }
+}
+
 // vector3's real-space cross product (pseudospec3D_mhd.f90:22-105):
 // x = (b f - e c) tmp, y = (c d - f a) tmp, z = (a e - d b) tmp for the real
 // fields (a, b, c) x (d, e, f), tmp = 1/(nx ny nz)^2

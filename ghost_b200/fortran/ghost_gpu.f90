@@ -568,6 +568,12 @@
          REAL(C_DOUBLE) :: ek(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_phaseshift(ctx,a,cre,cim) BIND(C,name="ghost_phaseshift") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: ctx, a
+         REAL(C_DOUBLE), VALUE :: cre, cim
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_vector3(ctx,a,b,c,d,e,f,x,y,z) BIND(C,name="ghost_vector3") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f, x, y, z

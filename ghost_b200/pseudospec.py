@@ -143,6 +143,10 @@ class Ghost:
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
 
+    def phaseshift(self, a, cdump: complex):
+        """phaseshift: a *= cdump in place (conj on the kx = 0 mirror half)."""
+        check(self.lib.ghost_phaseshift(self.h, self._ptr(a, "c"), cdump.real, cdump.imag), "phaseshift")
+
     # ---- MHD (MHD_SOL)
     def vector3(self, a, b, c, d, e, f, x=None, y=None, z=None):
         out = [self.czeros() if o is None else o for o in (x, y, z)]

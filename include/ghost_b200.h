@@ -205,6 +205,11 @@ int ghost_entrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, c
  * (hmtransfer / hktransfer). */
 int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, const void *d, const void *e,
                    const void *f, int kin, double *Hk);
+/* phaseshift(a,cdump) (pseudospec3D_hd.f90:2084-2148): a *= cdump in place,
+ * with conj(cdump) on the mirror half of the kx = 0 plane (GHOST's loop
+ * order, including its Nyquist lines that take both factors) */
+int ghost_phaseshift(ghost_ctx *ctx, void *a, double cdump_re, double cdump_im);
+
 /* ------------------------------------------------------------------
  * MHD (MHD_SOL, pseudospec3D_mhd.f90, include/mhd_rkstep1/2.f90): velocity
  * v and magnetic vector potential a (b = curl a).

@@ -1906,3 +1906,26 @@ void o_mhd_run(const octx *c, int nsteps, int ord, double dt, double nu, double 
   }
   for (int q = 0; q < 6; ++q) free(Cs[q]);
 }
+
+/* phaseshift (pseudospec3D_hd.f90:2084-2148), its loops as written (1-based
+ * j, k of the Fortran shifted to 0-based storage) */
+void o_phaseshift(const octx *c, cplx *a, double cre, double cim) {
+  cplx cd = {(real)cre, (real)cim}, jd = {(real)cre, -(real)cim};
+  int ny = c->ny, nz = c->nz;
+  for (int j = 2; j <= ny / 2 + 1; ++j) {
+    a[SIDX(c, 0, j - 1, 0)] = cmul(a[SIDX(c, 0, j - 1, 0)], cd);
+    a[SIDX(c, 0, ny - j + 1, 0)] = cmul(a[SIDX(c, 0, ny - j + 1, 0)], jd);
+  }
+  for (int k = 2; k <= nz / 2 + 1; ++k) {
+    a[SIDX(c, k - 1, 0, 0)] = cmul(a[SIDX(c, k - 1, 0, 0)], cd);
+    a[SIDX(c, nz - k + 1, 0, 0)] = cmul(a[SIDX(c, nz - k + 1, 0, 0)], jd);
+  }
+  for (int j = 2; j <= ny; ++j)
+    for (int k = 2; k <= nz / 2 + 1; ++k) {
+      a[SIDX(c, k - 1, j - 1, 0)] = cmul(a[SIDX(c, k - 1, j - 1, 0)], cd);
+      a[SIDX(c, nz - k + 1, ny - j + 1, 0)] = cmul(a[SIDX(c, nz - k + 1, ny - j + 1, 0)], jd);
+    }
+  for (int i = 1; i < c->nxh; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) a[SIDX(c, k, j, i)] = cmul(a[SIDX(c, k, j, i)], cd);
+}

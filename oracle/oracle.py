@@ -69,6 +69,7 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_havgcomp": (None, [P, P, P, P, P, D, D, I, P]),
         "o_phd_run": (None, [P, I, I, D, D, D] + [P] * 8),
         "o_vector3": (None, [P] * 10),
+        "o_phaseshift": (None, [P, P, D, D]),
         "o_nonlin3": (None, [P] * 8 + [I]),
         "o_gauge3": (None, [P] * 5 + [I]),
         "o_mhd_run": (None, [P, I, I, D, D, D] + [P] * 12),
@@ -252,6 +253,11 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def phaseshift(self, a, cdump):
+        a = self._c(a).copy()
+        self.lib.o_phaseshift(self.h, _ptr(a), cdump.real, cdump.imag)
+        return a
 
     def vector3(self, a, b, c, d, e, f):
         arrs = [self._c(x) for x in (a, b, c, d, e, f)]

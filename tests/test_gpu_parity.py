@@ -601,3 +601,16 @@ def test_mhd(prec):
     tol = 1e-11 if prec == "fp64" else 1e-5
     assert rel_l2([to_host(x) for x in V], rv) <= tol
     assert rel_l2([to_host(x) for x in A], ra) <= tol
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 16, 64)])
+def test_phaseshift(prec, shape):
+    o = Oracle(*shape)
+    g = ghost(*shape, precision=prec)
+    a = rand_spectral(o, 52)
+    cd = 0.6 + 0.8j
+    A = to_dev(a.astype(g.cdtype_np))
+    g.phaseshift(A, cd)
+    ref = o.phaseshift(a, cd)
+    assert rel_l2(to_host(A), ref) <= (1e-15 if prec == "fp64" else 1e-7)

@@ -236,3 +236,18 @@ def test_mhd_identities():
     vh = o.hd_run(2, 2, 1e-3, 1e-3, v)
     assert rel_l2(vm, vh) <= 1e-14
     assert all(np.abs(q).max() == 0 for q in am)
+
+
+def test_phaseshift_keeps_energy_and_hermitian_plane():
+    """phaseshift (pseudospec3D_hd.f90:2084-2148) with |cdump| = 1 on the
+    oracle: the energy is unchanged, and a field that is Hermitian on the
+    kx = 0 plane stays Hermitian there (mirror modes take conj(cdump))."""
+    o = Oracle(16, 16, 32)
+    v = solenoidal_ic(o, seed=51)
+    cd = np.exp(0.7j)
+    w = [o.phaseshift(x, cd) for x in v]
+    assert abs(o.energy(*w, 1) - o.energy(*v, 1)) <= 1e-14 * o.energy(*v, 1)
+    p0 = w[0][0]  # kx = 0 plane (ny, nz)
+    ny, nz = p0.shape
+    mirror = np.conj(p0[(-np.arange(ny)) % ny][:, (-np.arange(nz)) % nz])
+    assert np.allclose(p0, mirror, rtol=0, atol=1e-14 * np.abs(p0).max())
