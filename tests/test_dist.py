@@ -58,3 +58,54 @@ def test_reference_arm_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+
+
+def test_ensemble_shards_partition_the_runs():
+    """The ensemble's shards (runs sharded by index, no communication): every
+    run belongs to exactly one rank, class by class, with balanced counts."""
+    from ghost_b200.ensemble_bench import shard_runs
+    runs = [128, 96, 32]
+    for world in (1, 2, 3, 4, 8):
+        seen = []
+        per = []
+        for rank in range(world):
+            counts, idx = shard_runs(runs, rank, world)
+            assert sum(counts) == len(idx)
+            per.append(counts)
+            seen.extend(idx)
+        assert sorted(seen) == list(range(sum(runs)))
+        for c in range(len(runs)):
+            col = [p[c] for p in per]
+            assert max(col) - min(col) <= 1 and sum(col) == runs[c]
+
+
+def _shard_worker(rank, ws, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws), RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+
+    from ghost_b200.ensemble_bench import shard_runs
+    dist.init_process_group("gloo")
+    _, idx = shard_runs([5, 4, 3], rank, ws)
+    n = torch.tensor([len(idx)])
+    sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(ws)]
+    dist.all_gather(sizes, n)
+    buf = torch.full((12,), -1, dtype=torch.int64)
+    buf[:len(idx)] = torch.tensor(idx)
+    gathered = [torch.zeros(12, dtype=torch.int64) for _ in range(ws)]
+    dist.all_gather(gathered, buf)
+    if rank == 0:
+        allidx = sorted(int(v) for g in gathered for v in g.tolist() if v >= 0)
+        with open(os.path.join(out, "idx"), "w") as f:
+            f.write(repr(allidx))
+    dist.destroy_process_group()
+
+
+def test_ensemble_shards_under_gloo(tmp_path):
+    """Two gloo ranks take their shards independently; together they hold
+    every run once."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_shard_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    assert eval(open(tmp_path / "idx").read()) == list(range(12))
