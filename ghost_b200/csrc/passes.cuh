@@ -467,7 +467,8 @@ template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
 };
 
 template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false>
-__global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps, Fields<R> fld,
+__global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps,
+                                                             const __grid_constant__ Fields<R> fld,
                                                              const cx<R> *__restrict__ twg, int nz, int ni, int nf,
                                                              int nruns, int nxh, const int *__restrict__ jpos,
                                                              const int *__restrict__ jneg, int rb, PipeCtl ctl) {
@@ -842,7 +843,8 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_kernel(const cx<R>
 // closure's input rows: x[q][f] = (real value / (nx ny nz)) * gs for grid
 // point q (real layout, x fastest), f = 0..8, and x[q][9] = delta.
 template <typename R, int NX, int E, int BZ>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_features_kernel(Fields<R> in, float *__restrict__ xrows,
+__global__ void __launch_bounds__(BZ *(NX / 2) / E) xpass_c2r_features_kernel(const __grid_constant__ Fields<R> in,
+                                                                              float *__restrict__ xrows,
                                                                               const cx<R> *__restrict__ twg, int ny,
                                                                               int nz, R inv_n, float gs, float delta) {
   using C = cx<R>;
