@@ -283,6 +283,29 @@ template <typename R> struct ZFwdHD {
     const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     const R nuv = kp.nu_run ? kp.nu_run[ir / kp.nxh] : nu;
+    const bool forced = f.p[0] != nullptr;
+    // The kept modes are known before the transforms: their v, C and f
+    // values are prefetched into L2 while the three lines are transformed.
+    bool keep[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const R kn2 = kn2_of(kp, i, j, t + T * e);
+      keep[e] = act && kn2 <= kp.kmax && kn2 >= kp.tiny;
+    }
+    {
+      const size_t base = (size_t)line * N + t;
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (keep[e]) {
+          const size_t p = base + (size_t)T * e;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            prefetch_l2(v.p[c] + p);
+            prefetch_l2(c0.p[c] + p);
+            if (forced) prefetch_l2(f.p[c] + p);
+          }
+        }
+    }
     C g[3][E];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -291,18 +314,14 @@ template <typename R> struct ZFwdHD {
       line_fft<C, N, E, -1>(g[c], t, tw, buf, sync);
     }
     if (!act) return;
-    const bool forced = f.p[0] != nullptr;
     // The projected nonlinear term replaces g in place; then, component by
     // component, all of the line's operands (v, C, f at the kept modes) are
     // loaded before any result is stored, so a thread waits for one round
     // of loads per component rather than one per element.
-    bool keep[E];
     R kk2e[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int k = t + T * e;
-      const R kn2 = kn2_of(kp, i, j, k);
-      keep[e] = kn2 <= kp.kmax && kn2 >= kp.tiny;
       kk2e[e] = (R)0;
       if (keep[e]) {
         const R kz = kz_of(kp, k);

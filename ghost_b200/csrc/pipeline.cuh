@@ -72,6 +72,11 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 // ... and have completed
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
+// Hint: bring the 32-byte sector holding p into L2.
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
