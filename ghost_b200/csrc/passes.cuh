@@ -474,8 +474,9 @@ template <typename R> struct ZFwdBouss {
 // can be non-zero: the inverse pass loads only those, the forward pass
 // writes only those (the rest are never read).
 // ====================================================================
-// DUAL: the exchanges alternate between the tile's own stage buffer and a
-// second buffer of the same size, one barrier per exchange.
+// DUAL: the exchanges alternate between a second buffer of the same size
+// and the tile's own stage buffer, one barrier per exchange and none other
+// than the tile's first (the stage refill is issued after it).
 template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
   static constexpr int T = N / E;
   static constexpr int NT = BZ * T;
@@ -557,16 +558,20 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
   for (int k = 0;; ++k) {
     const int tile = blockIdx.x + k * gridDim.x;
     if (tile >= ntiles) break;
-    issue(k + STAGES - 1);
+    // DUAL: the refill of the previous tile's slot waits for this tile's
+    // first barrier, which follows every read of that slot (so no barrier
+    // closes a tile)
+    if constexpr (!DUAL) issue(k + STAGES - 1);
     const int s = k % STAGES;
     const bool ok = (!ctl.stall || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
                     mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
-      for (int kk = k; kk < k + STAGES; ++kk)
+      for (int kk = k; kk < k + STAGES - (DUAL ? 1 : 0); ++kk)
         if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
       return;
     }
+    if constexpr (DUAL) issue(k + STAGES - 1);
     const Tile tl = tile_of(tile);
     int jp = N, jn = 0;
     if (jpos) {
@@ -581,16 +586,17 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
       const bool live = (S < 0) || jj < jp || jj >= N - jn;
       x[e] = live ? sb[jj * BZ + l] : mk((R)0, (R)0);
     }
-    __syncthreads();
     if constexpr (DUAL) {
-      // half 0 is this tile's stage buffer (its data are in registers), half 1
-      // the second buffer; an even number of exchanges ends on half 1, whose
-      // barrier already follows every read of the stage buffer, which may then
-      // be refilled without a barrier at the end of the tile
-      int ph = 0;
+      // The exchanges alternate between the second buffer (half 1, first) and
+      // this tile's stage buffer (half 0): the first exchange barrier follows
+      // every thread's reads of the stage, so the second exchange may write
+      // it, and the second buffer's last reads come before the next tile's
+      // first barrier.
+      int ph = 1;
       auto buf = dual_buf<C>([sb, xb, l](int idx, int h) -> C & { return (h ? xb : sb)[idx * BZ + l]; }, &ph);
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
     } else {
+      __syncthreads();  // every read of the stage before the exchanges overwrite it
       auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
     }
@@ -600,7 +606,7 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
       const int jj = t + T * e;
       if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
     }
-    if constexpr (!DUAL || fft_exchanges<N, E>() % 2 == 1) __syncthreads();
+    if constexpr (!DUAL) __syncthreads();  // the stage is read before the next refill
   }
 }
 
