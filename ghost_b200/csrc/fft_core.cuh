@@ -207,4 +207,24 @@ __device__ __forceinline__ void line_fft(C (&x)[E], int t, const C *__restrict__
   }
 }
 
+// line_fft whose first exchange barrier is first() instead of sync(): a
+// pipelined pass folds its wait agreement (__syncthreads_or) and its stage
+// refill into that barrier.  Needs at least one exchange.
+template <typename C, int N, int E, int S, int TWS = 1, class Buf, class Sync0, class Sync>
+__device__ __forceinline__ void line_fft_first(C (&x)[E], int t, const C *__restrict__ tw, Buf buf, Sync0 first,
+                                               Sync sync) {
+  static_assert(fft_exchanges<N, E>() > 0, "no exchange barrier to fold into");
+  constexpr int T = N / E;
+  constexpr int R = stage_radix<N, E, 1>::value;
+  fft_stage<C, N, E, 1, S, TWS>(x, t, tw, [&](int idx, C v) { buf(idx) = v; });
+  first();
+#pragma unroll
+  for (int e = 0; e < E; ++e) x[e] = buf(t + T * e);
+  if constexpr (is_dual_buf<Buf>::value)
+    buf.flip();
+  else
+    sync();
+  line_fft<C, N, E, S, TWS, R>(x, t, tw, buf, sync);
+}
+
 }  // namespace gb

@@ -740,7 +740,22 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
       issue(L + STAGES - 1);
       const bool ok = (!ctl.stall || L > 0 || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
                       mbar_wait(&bars[L % STAGES], (uint32_t)(L / STAGES) & 1u, ctl.cap);
-      if (__syncthreads_or(!ok)) {
+      const C *sb = stage + (size_t)(L % STAGES) * G::stage_elems;
+      C x[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, BZ, l, t + T * e, M, rows, tw);
+      // The CTA agrees on the wait at the transform's first exchange barrier,
+      // which also orders every read of the stage before its next refill (the
+      // exchange halves alternate, so that barrier needs nothing before it).
+      // A stage that timed out is read in bounds and its transform discarded.
+      bool bad;
+      if constexpr (fft_exchanges<M, E>() == 0) {
+        bad = __syncthreads_or(!ok);
+        line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
+      } else {
+        line_fft_first<C, M, E, +1, 2>(x, t, tw, buf, [&] { bad = __syncthreads_or(!ok); }, sync);
+      }
+      if (bad) {
         if (tid == 0) record_timeout(ctl.status);
         for (int LL = L; LL < L + STAGES; ++LL)
           if (blockIdx.x + (LL / NIN) * gridDim.x < ntiles)
@@ -748,16 +763,6 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
         failed = true;
         break;
       }
-      const C *sb = stage + (size_t)(L % STAGES) * G::stage_elems;
-      C x[E];
-#pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, BZ, l, t + T * e, M, rows, tw);
-      // The stage may be refilled once every thread has read it: the first
-      // exchange barrier of the transform below comes after these reads and
-      // before the next refill is issued; only a transform without exchanges
-      // needs a barrier of its own.
-      if constexpr (fft_exchanges<M, E>() == 0) __syncthreads();
-      line_fft<C, M, E, +1, 2>(x, t, tw, buf, sync);
       // x[e] = (r_{2m}, r_{2m+1}) at m = t + T*e
       if (f < 3) {
 #pragma unroll
