@@ -386,6 +386,26 @@ template <typename R> struct ZFwdBouss {
     constexpr int T = N / E;
     const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
+    const bool forced = f.p[0] != nullptr, sforced = f.p[3] != nullptr;
+    const size_t base = (size_t)line * N + t;
+    // mode 0: kept mode; 1: truncated (all zero); 2: kn2 < tiny (theta
+    // keeps its mean).  Known before the transforms: the kept modes' v, C
+    // and f values are prefetched into L2 while the lines are transformed.
+    int mode[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const R kn2 = kn2_of(kp, i, j, t + T * e);
+      mode[e] = (kn2 <= kp.kmax && kn2 >= kp.tiny) ? 0 : (kn2 > kp.kmax ? 1 : 2);
+      if (act && mode[e] == 0) {
+        const size_t p = base + (size_t)T * e;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          prefetch_l2(v.p[c] + p);
+          prefetch_l2(c0.p[c] + p);
+          if (c < 3 ? forced : sforced) prefetch_l2(f.p[c] + p);
+        }
+      }
+    }
     C g[4][E];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -394,20 +414,13 @@ template <typename R> struct ZFwdBouss {
       line_fft<C, N, E, -1>(g[c], t, tw, buf, sync);
     }
     if (!act) return;
-    const bool forced = f.p[0] != nullptr, sforced = f.p[3] != nullptr;
     const R two_om = (R)2 * omegaz;
-    // As in ZFwdHD: all loads of a round before any store.  mode 0: kept
-    // mode; 1: truncated (all zero); 2: kn2 < tiny (theta keeps its mean).
-    int mode[E];
-    R kk2e[E];
+    // As in ZFwdHD: all loads of a round before any store.  The velocity
+    // and theta values enter the projection and the Laplacians, which are
+    // folded into g there, so they are dead before the update loads C and f.
     C vv[4][E];
-    const size_t base = (size_t)line * N + t;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const int k = t + T * e;
-      const R kn2 = kn2_of(kp, i, j, k);
-      mode[e] = (kn2 <= kp.kmax && kn2 >= kp.tiny) ? 0 : (kn2 > kp.kmax ? 1 : 2);
-      kk2e[e] = (R)0;
 #pragma unroll
       for (int c = 0; c < 4; ++c) vv[c][e] = mk((R)0, (R)0);
       if (mode[e] == 0) {
@@ -422,7 +435,6 @@ template <typename R> struct ZFwdBouss {
       const int k = t + T * e;
       const R kz = kz_of(kp, k);
       const R kk2 = kk2_of(kp, i, j, k);
-      kk2e[e] = kk2;
       const C a = mk(g[0][e].x - two_om * vv[1][e].x, g[0][e].y - two_om * vv[1][e].y);
       const C b = mk(g[1][e].x + two_om * vv[0][e].x, g[1][e].y + two_om * vv[0][e].y);
       const C cc = mk(g[2][e].x + xmom * vv[3][e].x, g[2][e].y + xmom * vv[3][e].y);
@@ -431,10 +443,15 @@ template <typename R> struct ZFwdBouss {
       g[1][e] = (j == 0) ? mk(-b.x, -b.y) : mk(-b.x + (ky * s.x) / kk2, -b.y + (ky * s.y) / kk2);
       g[2][e] = (k == 0) ? mk(-cc.x, -cc.y) : mk(-cc.x + (kz * s.x) / kk2, -cc.y + (kz * s.y) / kk2);
       g[3][e] = mk(g[3][e].x + xtemp * vv[2][e].x, g[3][e].y + xtemp * vv[2][e].y);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {  // + dif * Laplacian
+        const R dif = c < 3 ? nu : kappa;
+        const C lap = mk(-kk2 * vv[c][e].x, -kk2 * vv[c][e].y);
+        g[c][e] = mk(dif * lap.x + g[c][e].x, dif * lap.y + g[c][e].y);
+      }
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const R dif = c < 3 ? nu : kappa;
       const bool fc = c < 3 ? forced : sforced;
       C ff[E], cc0[E];
 #pragma unroll
@@ -453,8 +470,7 @@ template <typename R> struct ZFwdBouss {
       for (int e = 0; e < E; ++e) {
         const size_t p = base + (size_t)T * e;
         if (mode[e] == 0) {
-          const C lap = mk(-kk2e[e] * vv[c][e].x, -kk2e[e] * vv[c][e].y);
-          C sum = mk(dif * lap.x + g[c][e].x, dif * lap.y + g[c][e].y);
+          C sum = g[c][e];
           if (fc) sum = mk(sum.x + ff[e].x, sum.y + ff[e].y);
           v.p[c][p] = mk(cc0[e].x + (dt * sum.x) * rmp, cc0[e].y + (dt * sum.y) * rmp);
         } else {
