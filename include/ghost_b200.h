@@ -376,7 +376,10 @@ int ghost_batch_init_random_solenoidal(ghost_ctx *ctx, int32_t *seeds, double kd
 typedef struct ghost_ensemble ghost_ensemble;
 int ghost_ensemble_create(int nclasses, const int *n, const int *nruns, int precision, ghost_ensemble **ens);
 int ghost_ensemble_destroy(ghost_ensemble *ens);
-/* device pointers of class c's batched velocity */
+/* device pointers of class c's batched velocity.  The replayed steps of
+ * ghost_ensemble_run take every mode outside the kept set (kn2 > kmax, and
+ * k = 0) to be zero, as every step leaves it, and do not rewrite it: values
+ * written through these pointers between runs must keep those modes zero. */
 int ghost_ensemble_fields(ghost_ensemble *ens, int c, void **vx, void **vy, void **vz);
 /* the batched context of class c (for operators and diagnostics) */
 int ghost_ensemble_class(ghost_ensemble *ens, int c, ghost_ctx **ctx);
