@@ -46,6 +46,7 @@ P = ctypes.c_void_p
 I = ctypes.c_int
 D = ctypes.c_double
 PD = ctypes.POINTER(ctypes.c_double)
+PP = ctypes.POINTER(ctypes.c_void_p)  # an array of device pointers
 
 # name -> argument types (all return int status)
 SIGNATURES = {
@@ -98,6 +99,17 @@ SIGNATURES = {
     "ghost_ensemble_autotune": [P, I, D, ctypes.POINTER(ctypes.c_int)],
     "ghost_ensemble_run": [P, I, I, D],
     "ghost_ensemble_energy": [P, I, PD],
+    "ghost_slab_range": [I, I, I, I, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    "ghost_slab_create": [I, I, I, D, D, D, I, I, I, I, ctypes.POINTER(ctypes.c_void_p)],
+    "ghost_slab_destroy": [P],
+    "ghost_slab_layout": [P] + [ctypes.POINTER(ctypes.c_int)] * 4,
+    "ghost_slab_set_stream": [P, P],
+    "ghost_slab_synchronize": [P],
+    "ghost_slab_hd_front": [P, PP, PP, I, PP],
+    "ghost_slab_hd_xpass": [P, PP, PP],
+    "ghost_slab_hd_back": [P, I, D, D, PP, PP, PP, PP],
+    "ghost_slab_pack": [P, I, I, PP, P],
+    "ghost_slab_unpack": [P, I, I, P, PP],
     "ghost_ctx_set_tile_cfg": [P, I],
     "ghost_ctx_get_tile_cfg": [P, ctypes.POINTER(ctypes.c_int)],
     "ghost_hd_autotune": [P, I, D, D, P, P, P, P, P, P, ctypes.POINTER(ctypes.c_int)],

@@ -442,7 +442,7 @@ int launch_x_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int 
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Fields<R> fo{};
   for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
-  const R nn = (R)c->nx * (R)c->ny * (R)c->nz;
+  const R nn = (R)c->nx * (R)c->ny * (R)c->nz_glob;
   const int nrows = rows > 0 ? rows : M + 1;
   // tensor boxes: nbox boxes of rb kx-rows; rb keeps every box 128-byte aligned in shared memory
   const int nbox = (nrows + 255) / 256;
@@ -1006,6 +1006,7 @@ template <typename R> void fill_kparams(ghost_ctx *c, KParams<R> &kp) {
   kp.tmp = (R)1 / (nn * nn);
   kp.nruns = c->nruns;
   kp.nu_run = (sizeof(R) == (c->precision == GHOST_SINGLE ? 4 : 8)) ? (const R *)c->nu_run : nullptr;
+  kp.i0 = c->i0;
 }
 
 // kmax, tiny, nmax, Dk of main3D.fpp:881-909,1727-1737 in precision R
@@ -1260,6 +1261,8 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->nruns = 1;
   c->ntot = c->nspec;
   c->nu_run = nullptr;
+  c->i0 = 0;
+  c->nz_glob = nz;
   // the fastest variants measured for 512-point lines (ghost_hd_autotune
   // re-measures): two-stage z ring with three CTAs per SM, two-stage y ring
   // with a second exchange buffer, and for FP32 y passes with 16 values per
@@ -2803,6 +2806,280 @@ int ghost_ensemble_energy(ghost_ensemble *e, int kin, double *out) {
     GB_CHECK(ghost_batch_energy(e->cls[q], e->v[q][0], e->v[q][1], e->v[q][2], kin, out + off));
     off += e->nruns[q];
   }
+  return GHOST_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================
+// Slab decomposition of one run over ranks (GHOST's MPI layout).
+//
+// GHOST splits the spectral arrays into kx-slabs (rows ista..iend of
+// 1..nx/2+1) and the real arrays into z-slabs (planes ksta..kend of 1..nz),
+// both by range() (fftp-3/fftp.f90, main3D.fpp:634-635), and every 3D
+// transform moves data between the two with one all-to-all
+// (fftp-3/fftp3D.fpp:158-201, 255-278, 434-488).  Here a rank holds:
+//   spec: a context over its kx-slab (nz, ny, nxh_loc), kx row i of a local
+//         field being global row i + ista: the Z passes and the Y passes
+//         of the HD substep run on it;
+//   real: a context over its z-slab (nz_loc, ny, nxh): the fused X pass
+//         runs on it, normalised by the global grid.
+// One substep is front (Z inverse, Y inverse on 6 fields) -> pack ->
+// all-to-all -> unpack -> X pass -> pack -> all-to-all -> unpack -> back
+// (Y forward, Z forward and the truncated update).  The exchange itself
+// belongs to the caller (NCCL all-to-all, or copies between ranks held by
+// one process); the library packs and unpacks the blocks.
+// Buffers are peer-major: the chunk for (or from) peer p holds the nf
+// fields' blocks one after the other.
+//   dir 0 (kx-slab -> z-slab): send to p: my rows x all ky x p's planes
+//         (nxh_loc x ny x nz_p); receive from p: p's rows x ny x my planes,
+//         which land as rows ista_p.. of the z-slab field.
+//   dir 1 (z-slab -> kx-slab): the reverse.
+// Slab contexts run the slab entry points only, without zero-pruning.
+// =====================================================================
+struct ghost_slab {
+  ghost_ctx *spec = nullptr;
+  ghost_ctx *real = nullptr;
+  int rank = 0, nranks = 1;
+  std::vector<int> ista, nxhl, ksta, nzl;  // per rank, 0-based starts
+};
+
+namespace gb {
+
+// range() of GHOST (fftp-3/fftp.f90), 1-based inclusive bounds
+static void slab_range(int n1, int n2, int nprocs, int irank, int *ista, int *iend) {
+  const int w1 = (n2 - n1 + 1) / nprocs, w2 = (n2 - n1 + 1) % nprocs;
+  *ista = irank * w1 + n1 + std::min(irank, w2);
+  *iend = *ista + w1 - 1;
+  if (w2 > irank) *iend += 1;
+}
+
+static int slab_dev_ptrs(const void *const *p, int n) {
+  if (!p) return fail(GHOST_ERR_ARG, "null field array");
+  for (int q = 0; q < n; ++q) {
+    if (!p[q]) return fail(GHOST_ERR_ARG, "null field %d", q);
+    if (!is_device_ptr(p[q])) return fail(GHOST_ERR_ARG, "slab fields must be device arrays (field %d)", q);
+    if (((uintptr_t)p[q] & 15u) != 0) return fail(GHOST_ERR_ARG, "field %d is not 16-byte aligned", q);
+  }
+  return GHOST_OK;
+}
+
+template <typename R>
+static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3], int copy, void *const w[6]) {
+  ZInv<R, 0> zi{};
+  for (int q = 0; q < 3; ++q) {
+    zi.v.p[q] = (const cx<R> *)v[q];
+    zi.cpy.p[q] = copy ? (cx<R> *)C[q] : nullptr;
+  }
+  for (int q = 0; q < 6; ++q) zi.w.p[q] = (cx<R> *)w[q];
+  zi.kp = kparams<R>(c);
+  zi.copy = copy;
+  GB_CHECK(launch_z<R>(c, zi));
+  Fields<R> fy{};
+  for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
+  return launch_y<R, +1>(c, fy, 6);
+}
+
+template <typename R>
+static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, void *const w[3], void *const v[3],
+                         const void *const C[3], const void *const f[3]) {
+  Fields<R> fy{};
+  for (int q = 0; q < 3; ++q) fy.p[q] = (cx<R> *)w[q];
+  GB_CHECK((launch_y<R, -1>(c, fy, 3)));
+  ZFwdHD<R> zf{};
+  for (int q = 0; q < 3; ++q) {
+    zf.nl.p[q] = (const cx<R> *)w[q];
+    zf.v.p[q] = (cx<R> *)v[q];
+    zf.c0.p[q] = (const cx<R> *)C[q];
+    zf.f.p[q] = f ? (const cx<R> *)f[q] : nullptr;
+  }
+  zf.kp = kparams<R>(c);
+  zf.dt = (R)dt;
+  zf.nu = (R)nu;
+  zf.rmp = (R)1 / (R)o;
+  return launch_z<R>(c, zf);
+}
+
+}  // namespace gb
+
+#define SLAB_CHECK(s) \
+  do {                \
+    if (!(s)) return fail(GHOST_ERR_ARG, "null slab"); \
+  } while (0)
+
+extern "C" {
+
+int ghost_slab_range(int n1, int n2, int nprocs, int irank, int *ista, int *iend) {
+  if (!ista || !iend) return fail(GHOST_ERR_ARG, "null output");
+  if (nprocs < 1 || irank < 0 || irank >= nprocs || n2 < n1)
+    return fail(GHOST_ERR_ARG, "range(%d,%d,%d,%d)", n1, n2, nprocs, irank);
+  slab_range(n1, n2, nprocs, irank, ista, iend);
+  return GHOST_OK;
+}
+
+int ghost_slab_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, int arbsize, int precision, int rank,
+                      int nranks, ghost_slab **out) {
+  if (!out) return fail(GHOST_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(GHOST_ERR_ARG, "rank %d of %d", rank, nranks);
+  if (!pow2_ok(nx) || !pow2_ok(ny) || !pow2_ok(nz))
+    return fail(GHOST_ERR_SIZE, "grid %dx%dx%d: each n must be a power of two in [16,1024]", nx, ny, nz);
+  const int nxh = nx / 2 + 1;
+  if (nranks > nxh) return fail(GHOST_ERR_SIZE, "%d ranks for %d kx rows", nranks, nxh);
+  ghost_slab *s = new ghost_slab();
+  s->rank = rank;
+  s->nranks = nranks;
+  for (int r = 0; r < nranks; ++r) {
+    int a, b, ka, kb;
+    slab_range(1, nxh, nranks, r, &a, &b);
+    slab_range(1, nz, nranks, r, &ka, &kb);
+    s->ista.push_back(a - 1);
+    s->nxhl.push_back(b - a + 1);
+    s->ksta.push_back(ka - 1);
+    s->nzl.push_back(kb - ka + 1);
+    if ((kb - ka + 1) % 8 != 0) {
+      delete s;
+      return fail(GHOST_ERR_SIZE, "z-slab of %d planes on rank %d: every slab must hold a multiple of 8", kb - ka + 1, r);
+    }
+  }
+  int st = ghost_ctx_create(nx, ny, nz, Lx, Ly, Lz, arbsize, precision, &s->spec);
+  if (st == GHOST_OK) st = ghost_ctx_create(nx, ny, nz, Lx, Ly, Lz, arbsize, precision, &s->real);
+  if (st != GHOST_OK) {
+    ghost_ctx_destroy(s->spec);
+    delete s;
+    return st;
+  }
+  const size_t rs = precision == GHOST_SINGLE ? 4 : 8;
+  ghost_ctx *c = s->spec;  // kx-slab: local rows, global kx through i0
+  c->nxh = s->nxhl[rank];
+  c->i0 = s->ista[rank];
+  c->nspec = c->ntot = (size_t)nz * ny * c->nxh;
+  c->cbytes = c->nspec * 2 * rs;
+  refresh_kparams(c);
+  c = s->real;  // z-slab: local planes, the x pass normalised by the global nz
+  c->nz = s->nzl[rank];
+  c->nspec = c->ntot = (size_t)c->nz * ny * nxh;
+  c->cbytes = c->nspec * 2 * rs;
+  c->nreal = (size_t)nx * ny * c->nz;
+  c->rbytes = c->nreal * rs;
+  refresh_kparams(c);
+  *out = s;
+  return GHOST_OK;
+}
+
+int ghost_slab_destroy(ghost_slab *s) {
+  if (!s) return GHOST_OK;
+  int a = ghost_ctx_destroy(s->spec), b = ghost_ctx_destroy(s->real);
+  delete s;
+  return a != GHOST_OK ? a : b;
+}
+
+int ghost_slab_layout(const ghost_slab *s, int *ista, int *nxh_loc, int *ksta, int *nz_loc) {
+  SLAB_CHECK(s);
+  for (int r = 0; r < s->nranks; ++r) {
+    if (ista) ista[r] = s->ista[r];
+    if (nxh_loc) nxh_loc[r] = s->nxhl[r];
+    if (ksta) ksta[r] = s->ksta[r];
+    if (nz_loc) nz_loc[r] = s->nzl[r];
+  }
+  return GHOST_OK;
+}
+
+int ghost_slab_set_stream(ghost_slab *s, void *stream) {
+  SLAB_CHECK(s);
+  s->spec->stream = s->real->stream = (cudaStream_t)stream;
+  return GHOST_OK;
+}
+
+int ghost_slab_synchronize(ghost_slab *s) {
+  SLAB_CHECK(s);
+  GB_CHECK(ghost_ctx_synchronize(s->spec));
+  return ghost_ctx_synchronize(s->real);
+}
+
+int ghost_slab_hd_front(ghost_slab *s, const void *const v[3], void *const C[3], int copy, void *const w[6]) {
+  SLAB_CHECK(s);
+  GB_CHECK(slab_dev_ptrs(v, 3));
+  GB_CHECK(slab_dev_ptrs((const void *const *)w, 6));
+  if (copy) GB_CHECK(slab_dev_ptrs((const void *const *)C, 3));
+  ghost_ctx *c = s->spec;
+  return c->precision == GHOST_SINGLE ? slab_front_dev<float>(c, v, C, copy, w) : slab_front_dev<double>(c, v, C, copy, w);
+}
+
+int ghost_slab_hd_xpass(ghost_slab *s, const void *const in[6], void *const out[3]) {
+  SLAB_CHECK(s);
+  GB_CHECK(slab_dev_ptrs(in, 6));
+  GB_CHECK(slab_dev_ptrs((const void *const *)out, 3));
+  ghost_ctx *c = s->real;
+  return c->precision == GHOST_SINGLE ? launch_x<float, X_HD>(c, nullptr, nullptr, in, out, 0)
+                                      : launch_x<double, X_HD>(c, nullptr, nullptr, in, out, 0);
+}
+
+int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, void *const w[3], void *const v[3],
+                       const void *const C[3], const void *const f[3]) {
+  SLAB_CHECK(s);
+  if (o < 1) return fail(GHOST_ERR_ARG, "substep o=%d", o);
+  GB_CHECK(slab_dev_ptrs((const void *const *)w, 3));
+  GB_CHECK(slab_dev_ptrs((const void *const *)v, 3));
+  GB_CHECK(slab_dev_ptrs(C, 3));
+  if (f && !f[0]) f = nullptr;  // no forcing (a Fortran caller passes three null pointers)
+  if (f) GB_CHECK(slab_dev_ptrs(f, 3));
+  ghost_ctx *c = s->spec;
+  return c->precision == GHOST_SINGLE ? slab_back_dev<float>(c, o, dt, nu, w, v, C, f)
+                                      : slab_back_dev<double>(c, o, dt, nu, w, v, C, f);
+}
+
+int ghost_slab_pack(ghost_slab *s, int dir, int nf, const void *const *fields, void *send) {
+  SLAB_CHECK(s);
+  if ((dir != 0 && dir != 1) || nf < 1 || nf > 16 || !send) return fail(GHOST_ERR_ARG, "pack dir=%d nf=%d", dir, nf);
+  GB_CHECK(slab_dev_ptrs(fields, nf));
+  if (!is_device_ptr(send)) return fail(GHOST_ERR_ARG, "send buffer must be a device array");
+  ghost_ctx *c = s->spec;
+  const size_t es = c->precision == GHOST_SINGLE ? 8 : 16;
+  const int me = s->rank, ny = c->ny, nz = c->nz_glob;
+  unsigned char *dst = (unsigned char *)send;
+  for (int p = 0; p < s->nranks; ++p)
+    for (int f = 0; f < nf; ++f) {
+      const unsigned char *src = (const unsigned char *)fields[f];
+      if (dir == 0) {  // my kx rows, p's z planes, from a (nxh_loc, ny, nz) field
+        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->nxhl[me] * ny;
+        GB_CUDA(cudaMemcpy2DAsync(dst, w, src + (size_t)s->ksta[p] * es, (size_t)nz * es, w, h,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+        dst += w * h;
+      } else {  // p's kx rows of a (nxh, ny, nz_loc) field: contiguous
+        const size_t n = (size_t)s->nxhl[p] * ny * s->nzl[me] * es;
+        GB_CUDA(cudaMemcpyAsync(dst, src + (size_t)s->ista[p] * ny * s->nzl[me] * es, n, cudaMemcpyDeviceToDevice,
+                                c->stream));
+        dst += n;
+      }
+    }
+  return GHOST_OK;
+}
+
+int ghost_slab_unpack(ghost_slab *s, int dir, int nf, const void *recv, void *const *fields) {
+  SLAB_CHECK(s);
+  if ((dir != 0 && dir != 1) || nf < 1 || nf > 16 || !recv) return fail(GHOST_ERR_ARG, "unpack dir=%d nf=%d", dir, nf);
+  GB_CHECK(slab_dev_ptrs((const void *const *)fields, nf));
+  if (!is_device_ptr(recv)) return fail(GHOST_ERR_ARG, "receive buffer must be a device array");
+  ghost_ctx *c = s->spec;
+  const size_t es = c->precision == GHOST_SINGLE ? 8 : 16;
+  const int me = s->rank, ny = c->ny, nz = c->nz_glob;
+  const unsigned char *src = (const unsigned char *)recv;
+  for (int p = 0; p < s->nranks; ++p)
+    for (int f = 0; f < nf; ++f) {
+      unsigned char *dst = (unsigned char *)fields[f];
+      if (dir == 0) {  // p's kx rows of my z planes: rows ista_p.. of a (nxh, ny, nz_loc) field
+        const size_t n = (size_t)s->nxhl[p] * ny * s->nzl[me] * es;
+        GB_CUDA(cudaMemcpyAsync(dst + (size_t)s->ista[p] * ny * s->nzl[me] * es, src, n, cudaMemcpyDeviceToDevice,
+                                c->stream));
+        src += n;
+      } else {  // my kx rows of p's z planes into a (nxh_loc, ny, nz) field
+        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->nxhl[me] * ny;
+        GB_CUDA(cudaMemcpy2DAsync(dst + (size_t)s->ksta[p] * es, (size_t)nz * es, src, w, w, h,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+        src += w * h;
+      }
+    }
   return GHOST_OK;
 }
 

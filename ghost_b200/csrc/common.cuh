@@ -44,6 +44,9 @@ template <typename R> struct KParams {
   // after the other, i.e. the kx index runs over nxh*nruns
   int nruns;
   const R *nu_run;  // per-run viscosity (batched RK), or null
+  // global index of the first local kx row (a kx-slab of a decomposed
+  // grid; 0 otherwise): the passes' row i of a field is kx row i + i0
+  int i0;
 };
 
 template <typename R> __device__ __forceinline__ R kx_of(const KParams<R> &p, int i) {
@@ -113,6 +116,9 @@ struct ghost_ctx {
   gb::KParams<double> kp64;
   int nruns;          // runs in a batched context (1 otherwise)
   size_t ntot;        // nspec * nruns
+  // slab decomposition: the first kx row of a kx-slab context (0 otherwise),
+  // and the global nz (the normalisation of a z-slab context's x pass)
+  int i0, nz_glob;
   void *nu_run;       // per-run viscosity on the device (precision of ctx), or null
   int tile_cfg;       // tile variant (bit 0: y tile 16 wide, bit 1: z CTAs of 128 threads, bits 1+2: two-stage z ring,
                       // bit 3: two-stage y ring with a second exchange buffer)

@@ -183,7 +183,7 @@ template <typename R, int PHYS> struct ZInv {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh;
+    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh + kp.i0;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     if (copy && act) {
 #pragma unroll
@@ -241,7 +241,7 @@ template <typename R> struct ZGrad {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh;
+    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh + kp.i0;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
@@ -280,7 +280,7 @@ template <typename R> struct ZFwdHD {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh;
+    const int j = (int)(line % kp.ny), ir = (int)(line / kp.ny), i = ir % kp.nxh + kp.i0;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     const R nuv = kp.nu_run ? kp.nu_run[ir / kp.nxh] : nu;
     const bool forced = f.p[0] != nullptr;
@@ -384,7 +384,7 @@ template <typename R> struct ZFwdBouss {
   template <int N, int E, class Buf, class Sync, class In>
   __device__ __forceinline__ void body(long line, bool act, int t, const C *tw, Buf buf, Sync sync, In src) const {
     constexpr int T = N / E;
-    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh;
+    const int j = (int)(line % kp.ny), i = (int)(line / kp.ny) % kp.nxh + kp.i0;
     const R kx = kx_of(kp, i), ky = ky_of(kp, j);
     const bool forced = f.p[0] != nullptr, sforced = f.p[3] != nullptr;
     const size_t base = (size_t)line * N + t;

@@ -359,6 +359,78 @@
          REAL(C_DOUBLE) :: out(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       ! slab decomposition (GHOST's kx-slab / z-slab layout; the caller runs
+       ! the all-to-alls between pack and unpack, e.g. MPI_ALLTOALLV)
+       FUNCTION ghost_slab_range(n1,n2,nprocs,irank,ista,iend) BIND(C,name="ghost_slab_range") RESULT(s)
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: n1, n2, nprocs, irank
+         INTEGER(C_INT) :: ista, iend
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_create(nx,ny,nz,lx,ly,lz,arbsize,prec,rank,nranks,slab) &
+           BIND(C,name="ghost_slab_create") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         INTEGER(C_INT), VALUE :: nx, ny, nz, arbsize, prec, rank, nranks
+         REAL(C_DOUBLE), VALUE :: lx, ly, lz
+         TYPE(C_PTR) :: slab
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_destroy(slab) BIND(C,name="ghost_slab_destroy") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_layout(slab,ista,nxhl,ksta,nzl) BIND(C,name="ghost_slab_layout") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT) :: ista(*), nxhl(*), ksta(*), nzl(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_set_stream(slab,stream) BIND(C,name="ghost_slab_set_stream") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab, stream
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_synchronize(slab) BIND(C,name="ghost_slab_synchronize") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_hd_front(slab,v,c,copy,w) BIND(C,name="ghost_slab_hd_front") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         TYPE(C_PTR) :: v(3), c(3), w(6)
+         INTEGER(C_INT), VALUE :: copy
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_hd_xpass(slab,fin,fout) BIND(C,name="ghost_slab_hd_xpass") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         TYPE(C_PTR) :: fin(6), fout(3)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_hd_back(slab,o,dt,nu,w,v,c,f) BIND(C,name="ghost_slab_hd_back") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: o
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         TYPE(C_PTR) :: w(3), v(3), c(3), f(3)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_pack(slab,dir,nf,fields,send) BIND(C,name="ghost_slab_pack") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab, send
+         INTEGER(C_INT), VALUE :: dir, nf
+         TYPE(C_PTR) :: fields(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_unpack(slab,dir,nf,recv,fields) BIND(C,name="ghost_slab_unpack") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab, recv
+         INTEGER(C_INT), VALUE :: dir, nf
+         TYPE(C_PTR) :: fields(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_ctx_set_tile_cfg(ctx,cfg) BIND(C,name="ghost_ctx_set_tile_cfg") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: ctx

@@ -1,0 +1,54 @@
+"""The slab-decomposed HD run on one GPU: the ranks of a decomposed run
+held by one process (ghost_b200.slab.run_local: the library's slab passes,
+packing and unpacking, with the all-to-alls done by device copies), against
+the undivided run of ghost_hd_run on the same fields.  Uneven kx slabs
+(33 rows over 2 or 4 ranks) included."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(g, seed):
+    v = [g.czeros() for _ in range(3)]
+    g.init_random_solenoidal(seed, 1.0, g.nx / 3.0, 1, 1.0, *v)
+    return v
+
+
+@pytest.mark.parametrize("prec,P,shape", [("fp64", 1, (64, 64, 64)), ("fp64", 2, (64, 64, 64)),
+                                          ("fp64", 4, (64, 64, 64)), ("fp32", 2, (64, 64, 64)),
+                                          ("fp64", 4, (64, 32, 128))])
+def test_slab_run_matches_undivided_run(prec, P, shape):
+    import torch
+
+    from ghost_b200 import Ghost
+    from ghost_b200.slab import Slab, run_local
+    nx, ny, nz = shape
+    arb = shape != (nx, nx, nx)
+    kw = dict(Lx=1.0, Ly=2.0, Lz=0.5, arbsize=True) if arb else {}
+    g = Ghost(nx, ny, nz, precision=prec, **kw)
+    v0, f = _fields(g, 1000), _fields(g, 77)
+    ref = [x.clone() for x in v0]
+    g.hd_run(2, 4, 1e-3, 2e-3, *ref, *f)
+    slabs = [Slab(nx, ny, nz, precision=prec, rank=r, nranks=P, **kw) for r in range(P)]
+    vs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in v0] for r, s in enumerate(slabs)]
+    fs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in f] for r, s in enumerate(slabs)]
+    for _ in range(2):  # two calls in a row: the work arrays carry nothing over
+        vv = [[x.clone() for x in v] for v in vs]
+        run_local(slabs, 2, 4, 1e-3, 2e-3, vv, fs)
+        torch.cuda.synchronize()
+        got = [torch.cat([vv[r][c] for r in range(P)], dim=0) for c in range(3)]
+        for c in range(3):
+            a, b = got[c].cpu().numpy(), ref[c].cpu().numpy()
+            err = np.abs(a - b).max() / np.abs(b).max()
+            assert err <= (1e-12 if prec == "fp64" else 1e-5), (c, err)
+    for s in slabs:
+        s.close()
+
+
+def test_slab_phases_reject_host_and_misshaped_arrays():
+    from ghost_b200.slab import Slab
+    s = Slab(64, precision="fp64", rank=1, nranks=2)
+    with pytest.raises(ValueError):
+        s.front([t[:-1] for t in s.C], True)
+    s.close()

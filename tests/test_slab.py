@@ -1,0 +1,131 @@
+"""Slab decomposition host logic (no GPU): GHOST's range() through the
+library, the exchange counts, and the all-to-all of ghost_b200.slab over a
+two-rank gloo group with blocks packed in the documented peer-major layout
+(the device packing is checked on the GPU in test_gpu_slab.py)."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _range_ref(n1, n2, nprocs, irank):
+    # fftp-3/fftp.f90 SUBROUTINE range, as written there
+    iwork1 = (n2 - n1 + 1) // nprocs
+    iwork2 = (n2 - n1 + 1) % nprocs
+    ista = irank * iwork1 + n1 + min(irank, iwork2)
+    iend = ista + iwork1 - 1
+    if iwork2 > irank:
+        iend += 1
+    return ista, iend
+
+
+@pytest.mark.parametrize("n", [16, 33, 257, 512, 513])
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 7, 8])
+def test_range_is_ghosts_and_tiles_the_axis(n, p):
+    from ghost_b200.slab import slab_range
+    got = [slab_range(1, n, p, r) for r in range(p)]
+    assert got == [_range_ref(1, n, p, r) for r in range(p)]
+    assert got[0][0] == 1 and got[-1][1] == n
+    assert all(got[r][1] + 1 == got[r + 1][0] for r in range(p - 1))
+    sizes = [b - a + 1 for a, b in got]
+    assert max(sizes) - min(sizes) <= 1 and sizes == sorted(sizes, reverse=True)
+
+
+def test_slab_create_rejects_what_it_cannot_split():
+    from ghost_b200 import _lib
+    import ctypes
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    # 64 planes over 3 ranks: 22/21/21, not multiples of 8 (checked before any device is touched)
+    assert lib.ghost_slab_create(64, 64, 64, 1., 1., 1., 0, 8, 0, 3, ctypes.byref(h)) == 2
+    assert lib.ghost_slab_create(64, 64, 64, 1., 1., 1., 0, 8, 3, 3, ctypes.byref(h)) == 1
+
+
+@pytest.mark.parametrize("nx,nz,p", [(64, 64, 2), (64, 64, 4), (512, 512, 8), (32, 128, 4)])
+def test_exchange_counts_match_between_peers(nx, nz, p):
+    from ghost_b200.slab import exchange_counts, slab_layout
+    ista, nxhl, ksta, nzl = slab_layout(nx, nz, p)
+    assert sum(nxhl) == nx // 2 + 1 and sum(nzl) == nz
+    ny = 16
+    for d, nf in ((0, 6), (1, 3)):
+        c = [exchange_counts(nxhl, nzl, ny, r, d, nf) for r in range(p)]
+        for r in range(p):
+            for q in range(p):
+                assert c[r][0][q] == c[q][1][r]     # what r sends q is what q expects from r
+        # every value of the nf fields moves exactly once
+        assert sum(sum(x[0]) for x in c) == nf * (nx // 2 + 1) * ny * nz
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _pack(fields_k, direction, me, ista, nxhl, ksta, nzl):
+    # the documented peer-major layout, restated with numpy
+    out = []
+    for p in range(len(nxhl)):
+        for f in fields_k:
+            if direction == 0:
+                out.append(f[:, :, ksta[p]:ksta[p] + nzl[p]].ravel())
+            else:
+                out.append(f[ista[p]:ista[p] + nxhl[p]].ravel())
+    return np.concatenate(out)
+
+
+def _worker(rank, ws, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws), RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+
+    from ghost_b200.slab import all_to_all, exchange_counts, slab_layout
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    nx, ny, nz, nf = 32, 4, 32, 2
+    ista, nxhl, ksta, nzl = slab_layout(nx, nz, ws)
+    rng = np.random.default_rng(5)
+    glob = [rng.standard_normal((nx // 2 + 1, ny, nz)) + 1j * rng.standard_normal((nx // 2 + 1, ny, nz))
+            for _ in range(nf)]
+    mine_k = [g[ista[rank]:ista[rank] + nxhl[rank]] for g in glob]
+    # kx-slab -> z-slab
+    sc, rc = exchange_counts(nxhl, nzl, ny, rank, 0, nf)
+    send = torch.from_numpy(_pack(mine_k, 0, rank, ista, nxhl, ksta, nzl))
+    recv = torch.zeros(sum(rc), dtype=torch.complex128)
+    all_to_all(recv, send, rc, sc)
+    r = recv.numpy()
+    z = [np.zeros((nx // 2 + 1, ny, nzl[rank]), complex) for _ in range(nf)]
+    off = 0
+    for p in range(ws):
+        for f in range(nf):
+            n = nxhl[p] * ny * nzl[rank]
+            z[f][ista[p]:ista[p] + nxhl[p]] = r[off:off + n].reshape(nxhl[p], ny, nzl[rank])
+            off += n
+    ok0 = all(np.array_equal(z[f], glob[f][:, :, ksta[rank]:ksta[rank] + nzl[rank]]) for f in range(nf))
+    # and back
+    sc, rc = exchange_counts(nxhl, nzl, ny, rank, 1, nf)
+    send = torch.from_numpy(_pack(z, 1, rank, ista, nxhl, ksta, nzl))
+    recv = torch.zeros(sum(rc), dtype=torch.complex128)
+    all_to_all(recv, send, rc, sc)
+    r = recv.numpy()
+    k = [np.zeros_like(m) for m in mine_k]
+    off = 0
+    for p in range(ws):
+        for f in range(nf):
+            n = nxhl[rank] * ny * nzl[p]
+            k[f][:, :, ksta[p]:ksta[p] + nzl[p]] = r[off:off + n].reshape(nxhl[rank], ny, nzl[p])
+            off += n
+    ok1 = all(np.array_equal(k[f], mine_k[f]) for f in range(nf))
+    with open(os.path.join(out, f"r{rank}"), "w") as fh:
+        fh.write(f"{int(ok0)}{int(ok1)}")
+    dist.destroy_process_group()
+
+
+def test_transposes_over_gloo(tmp_path):
+    import torch.multiprocessing as mp
+    mp.start_processes(_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    assert [open(tmp_path / f"r{r}").read() for r in range(2)] == ["11", "11"]
