@@ -103,13 +103,14 @@ SIGNATURES = {
     "ghost_slab_create": [I, I, I, D, D, D, I, I, I, I, ctypes.POINTER(ctypes.c_void_p)],
     "ghost_slab_destroy": [P],
     "ghost_slab_layout": [P] + [ctypes.POINTER(ctypes.c_int)] * 4,
+    "ghost_slab_rows": [P, ctypes.POINTER(ctypes.c_int)],
     "ghost_slab_set_stream": [P, P],
     "ghost_slab_synchronize": [P],
-    "ghost_slab_hd_front": [P, PP, PP, I, PP],
-    "ghost_slab_hd_xpass": [P, PP, PP],
-    "ghost_slab_hd_back": [P, I, D, D, PP, PP, PP, PP],
-    "ghost_slab_pack": [P, I, I, PP, P],
-    "ghost_slab_unpack": [P, I, I, P, PP],
+    "ghost_slab_hd_front": [P, PP, PP, I, I, PP],
+    "ghost_slab_hd_xpass": [P, I, PP, PP],
+    "ghost_slab_hd_back": [P, I, D, D, I, PP, PP, PP, PP],
+    "ghost_slab_pack": [P, I, I, I, PP, P],
+    "ghost_slab_unpack": [P, I, I, I, P, PP],
     "ghost_ctx_set_tile_cfg": [P, I],
     "ghost_ctx_get_tile_cfg": [P, ctypes.POINTER(ctypes.c_int)],
     "ghost_hd_autotune": [P, I, D, D, P, P, P, P, P, P, ctypes.POINTER(ctypes.c_int)],

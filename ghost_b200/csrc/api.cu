@@ -564,7 +564,9 @@ int launch_x(ghost_ctx *c, const void *in, void *out, const void *const *ins = n
 // does not have that shape (an unusual kmax), pruning is disabled.
 template <typename R> int build_prune(ghost_ctx *c) {
   const KParams<R> &kp = kparams<R>(c);
-  auto kn2h = [&](int i, int j) -> R {
+  // local kx row i is global row i + i0 (a kx-slab; 0 otherwise)
+  auto kn2h = [&](int il, int j) -> R {
+    const int i = il + kp.i0;
     const R a = (R)(i < kp.nx / 2 ? i : i - kp.nx), b = (R)(j < kp.ny / 2 ? j : j - kp.ny);
     volatile R aa = a * a, bb = b * b;  // no contraction: same rounding as the kernels
     if (kp.anis) {
@@ -2835,13 +2837,21 @@ int ghost_ensemble_energy(ghost_ensemble *e, int kin, double *out) {
 //         (nxh_loc x ny x nz_p); receive from p: p's rows x ny x my planes,
 //         which land as rows ista_p.. of the z-slab field.
 //   dir 1 (z-slab -> kx-slab): the reverse.
-// Slab contexts run the slab entry points only, without zero-pruning.
+// A pruned substep (every one after the first of a run, as in
+// ghost_hd_run) runs the passes with the pruning tables of the rank's slab
+// and moves only the kx rows below rows_glob, which hold every live mode.
+// Slab contexts run the slab entry points only.
 // =====================================================================
 struct ghost_slab {
   ghost_ctx *spec = nullptr;
   ghost_ctx *real = nullptr;
   int rank = 0, nranks = 1;
   std::vector<int> ista, nxhl, ksta, nzl;  // per rank, 0-based starts
+  int rows_glob = 0;  // kx rows 0..rows_glob-1 hold every mode that survives the truncation
+  // kx rows of rank r that a pruned exchange moves: the live prefix of its slab
+  int live_rows(int r, bool prune) const {
+    return prune ? std::max(0, std::min(rows_glob - ista[r], nxhl[r])) : nxhl[r];
+  }
 };
 
 namespace gb {
@@ -2864,8 +2874,34 @@ static int slab_dev_ptrs(const void *const *p, int n) {
   return GHOST_OK;
 }
 
+// kx rows holding a mode with kn2 <= kmax: row i's smallest kn2 is at ky = 0
+// (the same rounding as the pruning tables and the kernels)
+template <typename R> static int slab_rows_glob(const ghost_ctx *c) {
+  const KParams<R> &kp = kparams<R>(c);
+  int rows = 0;
+  for (int i = 0; i < kp.nx / 2 + 1; ++i) {
+    const R a = (R)(i < kp.nx / 2 ? i : i - kp.nx);
+    volatile R aa = a * a, bb = (R)0;
+    R k2;
+    if (kp.anis) {
+      volatile R x = kp.rmp * aa, y = kp.rmq * bb;
+      volatile R t = x + y;
+      k2 = t + (R)0;
+    } else {
+      volatile R t = aa + bb;
+      k2 = t + (R)0;
+    }
+    if (!(k2 <= kp.kmax)) break;
+    rows = i + 1;
+  }
+  return rows;
+}
+
 template <typename R>
-static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3], int copy, void *const w[6]) {
+static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3], int copy, bool prune,
+                          void *const w[6]) {
+  Prune pr;
+  GB_CHECK(prune_plan<R>(c, prune, &pr));
   ZInv<R, 0> zi{};
   for (int q = 0; q < 3; ++q) {
     zi.v.p[q] = (const cx<R> *)v[q];
@@ -2874,18 +2910,20 @@ static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3]
   for (int q = 0; q < 6; ++q) zi.w.p[q] = (cx<R> *)w[q];
   zi.kp = kparams<R>(c);
   zi.copy = copy;
-  GB_CHECK(launch_z<R>(c, zi));
+  GB_CHECK(launch_z<R>(c, zi, pr));
   Fields<R> fy{};
   for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
-  return launch_y<R, +1>(c, fy, 6);
+  return launch_y<R, +1>(c, fy, 6, pr);
 }
 
 template <typename R>
-static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, void *const w[3], void *const v[3],
+static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, bool prune, void *const w[3], void *const v[3],
                          const void *const C[3], const void *const f[3]) {
+  Prune pr;
+  GB_CHECK(prune_plan<R>(c, prune, &pr));
   Fields<R> fy{};
   for (int q = 0; q < 3; ++q) fy.p[q] = (cx<R> *)w[q];
-  GB_CHECK((launch_y<R, -1>(c, fy, 3)));
+  GB_CHECK((launch_y<R, -1>(c, fy, 3, pr)));
   ZFwdHD<R> zf{};
   for (int q = 0; q < 3; ++q) {
     zf.nl.p[q] = (const cx<R> *)w[q];
@@ -2897,7 +2935,7 @@ static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, void *const 
   zf.dt = (R)dt;
   zf.nu = (R)nu;
   zf.rmp = (R)1 / (R)o;
-  return launch_z<R>(c, zf);
+  return launch_z<R>(c, zf, pr);
 }
 
 }  // namespace gb
@@ -2956,6 +2994,7 @@ int ghost_slab_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, i
   c->nspec = c->ntot = (size_t)nz * ny * c->nxh;
   c->cbytes = c->nspec * 2 * rs;
   refresh_kparams(c);
+  s->rows_glob = precision == GHOST_SINGLE ? slab_rows_glob<float>(c) : slab_rows_glob<double>(c);
   c = s->real;  // z-slab: local planes, the x pass normalised by the global nz
   c->nz = s->nzl[rank];
   c->nspec = c->ntot = (size_t)c->nz * ny * nxh;
@@ -2985,6 +3024,13 @@ int ghost_slab_layout(const ghost_slab *s, int *ista, int *nxh_loc, int *ksta, i
   return GHOST_OK;
 }
 
+int ghost_slab_rows(const ghost_slab *s, int *rows) {
+  SLAB_CHECK(s);
+  if (!rows) return fail(GHOST_ERR_ARG, "null output");
+  *rows = s->rows_glob;
+  return GHOST_OK;
+}
+
 int ghost_slab_set_stream(ghost_slab *s, void *stream) {
   SLAB_CHECK(s);
   s->spec->stream = s->real->stream = (cudaStream_t)stream;
@@ -2997,25 +3043,29 @@ int ghost_slab_synchronize(ghost_slab *s) {
   return ghost_ctx_synchronize(s->real);
 }
 
-int ghost_slab_hd_front(ghost_slab *s, const void *const v[3], void *const C[3], int copy, void *const w[6]) {
+int ghost_slab_hd_front(ghost_slab *s, const void *const v[3], void *const C[3], int copy, int prune,
+                        void *const w[6]) {
   SLAB_CHECK(s);
   GB_CHECK(slab_dev_ptrs(v, 3));
   GB_CHECK(slab_dev_ptrs((const void *const *)w, 6));
   if (copy) GB_CHECK(slab_dev_ptrs((const void *const *)C, 3));
   ghost_ctx *c = s->spec;
-  return c->precision == GHOST_SINGLE ? slab_front_dev<float>(c, v, C, copy, w) : slab_front_dev<double>(c, v, C, copy, w);
+  return c->precision == GHOST_SINGLE ? slab_front_dev<float>(c, v, C, copy, prune != 0, w)
+                                      : slab_front_dev<double>(c, v, C, copy, prune != 0, w);
 }
 
-int ghost_slab_hd_xpass(ghost_slab *s, const void *const in[6], void *const out[3]) {
+int ghost_slab_hd_xpass(ghost_slab *s, int prune, const void *const in[6], void *const out[3]) {
   SLAB_CHECK(s);
   GB_CHECK(slab_dev_ptrs(in, 6));
   GB_CHECK(slab_dev_ptrs((const void *const *)out, 3));
   ghost_ctx *c = s->real;
-  return c->precision == GHOST_SINGLE ? launch_x<float, X_HD>(c, nullptr, nullptr, in, out, 0)
-                                      : launch_x<double, X_HD>(c, nullptr, nullptr, in, out, 0);
+  const int rows = prune ? s->rows_glob : 0;  // a pruned substep reads and writes the live kx rows only
+  if (prune && rows == 0) return GHOST_OK;
+  return c->precision == GHOST_SINGLE ? launch_x<float, X_HD>(c, nullptr, nullptr, in, out, rows)
+                                      : launch_x<double, X_HD>(c, nullptr, nullptr, in, out, rows);
 }
 
-int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, void *const w[3], void *const v[3],
+int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, int prune, void *const w[3], void *const v[3],
                        const void *const C[3], const void *const f[3]) {
   SLAB_CHECK(s);
   if (o < 1) return fail(GHOST_ERR_ARG, "substep o=%d", o);
@@ -3025,11 +3075,11 @@ int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, void *const w
   if (f && !f[0]) f = nullptr;  // no forcing (a Fortran caller passes three null pointers)
   if (f) GB_CHECK(slab_dev_ptrs(f, 3));
   ghost_ctx *c = s->spec;
-  return c->precision == GHOST_SINGLE ? slab_back_dev<float>(c, o, dt, nu, w, v, C, f)
-                                      : slab_back_dev<double>(c, o, dt, nu, w, v, C, f);
+  return c->precision == GHOST_SINGLE ? slab_back_dev<float>(c, o, dt, nu, prune != 0, w, v, C, f)
+                                      : slab_back_dev<double>(c, o, dt, nu, prune != 0, w, v, C, f);
 }
 
-int ghost_slab_pack(ghost_slab *s, int dir, int nf, const void *const *fields, void *send) {
+int ghost_slab_pack(ghost_slab *s, int dir, int nf, int prune, const void *const *fields, void *send) {
   SLAB_CHECK(s);
   if ((dir != 0 && dir != 1) || nf < 1 || nf > 16 || !send) return fail(GHOST_ERR_ARG, "pack dir=%d nf=%d", dir, nf);
   GB_CHECK(slab_dev_ptrs(fields, nf));
@@ -3037,26 +3087,29 @@ int ghost_slab_pack(ghost_slab *s, int dir, int nf, const void *const *fields, v
   ghost_ctx *c = s->spec;
   const size_t es = c->precision == GHOST_SINGLE ? 8 : 16;
   const int me = s->rank, ny = c->ny, nz = c->nz_glob;
+  const bool pr = prune != 0;
   unsigned char *dst = (unsigned char *)send;
   for (int p = 0; p < s->nranks; ++p)
     for (int f = 0; f < nf; ++f) {
       const unsigned char *src = (const unsigned char *)fields[f];
-      if (dir == 0) {  // my kx rows, p's z planes, from a (nxh_loc, ny, nz) field
-        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->nxhl[me] * ny;
-        GB_CUDA(cudaMemcpy2DAsync(dst, w, src + (size_t)s->ksta[p] * es, (size_t)nz * es, w, h,
-                                  cudaMemcpyDeviceToDevice, c->stream));
+      if (dir == 0) {  // my (live) kx rows, p's z planes, from a (nxh_loc, ny, nz) field
+        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->live_rows(me, pr) * ny;
+        if (h > 0)
+          GB_CUDA(cudaMemcpy2DAsync(dst, w, src + (size_t)s->ksta[p] * es, (size_t)nz * es, w, h,
+                                    cudaMemcpyDeviceToDevice, c->stream));
         dst += w * h;
-      } else {  // p's kx rows of a (nxh, ny, nz_loc) field: contiguous
-        const size_t n = (size_t)s->nxhl[p] * ny * s->nzl[me] * es;
-        GB_CUDA(cudaMemcpyAsync(dst, src + (size_t)s->ista[p] * ny * s->nzl[me] * es, n, cudaMemcpyDeviceToDevice,
-                                c->stream));
+      } else {  // p's (live) kx rows of a (nxh, ny, nz_loc) field: contiguous
+        const size_t n = (size_t)s->live_rows(p, pr) * ny * s->nzl[me] * es;
+        if (n > 0)
+          GB_CUDA(cudaMemcpyAsync(dst, src + (size_t)s->ista[p] * ny * s->nzl[me] * es, n, cudaMemcpyDeviceToDevice,
+                                  c->stream));
         dst += n;
       }
     }
   return GHOST_OK;
 }
 
-int ghost_slab_unpack(ghost_slab *s, int dir, int nf, const void *recv, void *const *fields) {
+int ghost_slab_unpack(ghost_slab *s, int dir, int nf, int prune, const void *recv, void *const *fields) {
   SLAB_CHECK(s);
   if ((dir != 0 && dir != 1) || nf < 1 || nf > 16 || !recv) return fail(GHOST_ERR_ARG, "unpack dir=%d nf=%d", dir, nf);
   GB_CHECK(slab_dev_ptrs((const void *const *)fields, nf));
@@ -3064,19 +3117,22 @@ int ghost_slab_unpack(ghost_slab *s, int dir, int nf, const void *recv, void *co
   ghost_ctx *c = s->spec;
   const size_t es = c->precision == GHOST_SINGLE ? 8 : 16;
   const int me = s->rank, ny = c->ny, nz = c->nz_glob;
+  const bool pr = prune != 0;
   const unsigned char *src = (const unsigned char *)recv;
   for (int p = 0; p < s->nranks; ++p)
     for (int f = 0; f < nf; ++f) {
       unsigned char *dst = (unsigned char *)fields[f];
-      if (dir == 0) {  // p's kx rows of my z planes: rows ista_p.. of a (nxh, ny, nz_loc) field
-        const size_t n = (size_t)s->nxhl[p] * ny * s->nzl[me] * es;
-        GB_CUDA(cudaMemcpyAsync(dst + (size_t)s->ista[p] * ny * s->nzl[me] * es, src, n, cudaMemcpyDeviceToDevice,
-                                c->stream));
+      if (dir == 0) {  // p's (live) kx rows of my z planes: rows ista_p.. of a (nxh, ny, nz_loc) field
+        const size_t n = (size_t)s->live_rows(p, pr) * ny * s->nzl[me] * es;
+        if (n > 0)
+          GB_CUDA(cudaMemcpyAsync(dst + (size_t)s->ista[p] * ny * s->nzl[me] * es, src, n, cudaMemcpyDeviceToDevice,
+                                  c->stream));
         src += n;
-      } else {  // my kx rows of p's z planes into a (nxh_loc, ny, nz) field
-        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->nxhl[me] * ny;
-        GB_CUDA(cudaMemcpy2DAsync(dst + (size_t)s->ksta[p] * es, (size_t)nz * es, src, w, w, h,
-                                  cudaMemcpyDeviceToDevice, c->stream));
+      } else {  // my (live) kx rows of p's z planes into a (nxh_loc, ny, nz) field
+        const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->live_rows(me, pr) * ny;
+        if (h > 0)
+          GB_CUDA(cudaMemcpy2DAsync(dst + (size_t)s->ksta[p] * es, (size_t)nz * es, src, w, w, h,
+                                    cudaMemcpyDeviceToDevice, c->stream));
         src += w * h;
       }
     }

@@ -386,6 +386,12 @@
          INTEGER(C_INT) :: ista(*), nxhl(*), ksta(*), nzl(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_slab_rows(slab,rows) BIND(C,name="ghost_slab_rows") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT) :: rows
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_slab_set_stream(slab,stream) BIND(C,name="ghost_slab_set_stream") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab, stream
@@ -396,38 +402,39 @@
          TYPE(C_PTR), VALUE :: slab
          INTEGER(C_INT) :: s
        END FUNCTION
-       FUNCTION ghost_slab_hd_front(slab,v,c,copy,w) BIND(C,name="ghost_slab_hd_front") RESULT(s)
+       FUNCTION ghost_slab_hd_front(slab,v,c,copy,prune,w) BIND(C,name="ghost_slab_hd_front") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab
          TYPE(C_PTR) :: v(3), c(3), w(6)
-         INTEGER(C_INT), VALUE :: copy
+         INTEGER(C_INT), VALUE :: copy, prune
          INTEGER(C_INT) :: s
        END FUNCTION
-       FUNCTION ghost_slab_hd_xpass(slab,fin,fout) BIND(C,name="ghost_slab_hd_xpass") RESULT(s)
+       FUNCTION ghost_slab_hd_xpass(slab,prune,fin,fout) BIND(C,name="ghost_slab_hd_xpass") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: prune
          TYPE(C_PTR) :: fin(6), fout(3)
          INTEGER(C_INT) :: s
        END FUNCTION
-       FUNCTION ghost_slab_hd_back(slab,o,dt,nu,w,v,c,f) BIND(C,name="ghost_slab_hd_back") RESULT(s)
+       FUNCTION ghost_slab_hd_back(slab,o,dt,nu,prune,w,v,c,f) BIND(C,name="ghost_slab_hd_back") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE
          TYPE(C_PTR), VALUE :: slab
-         INTEGER(C_INT), VALUE :: o
+         INTEGER(C_INT), VALUE :: o, prune
          REAL(C_DOUBLE), VALUE :: dt, nu
          TYPE(C_PTR) :: w(3), v(3), c(3), f(3)
          INTEGER(C_INT) :: s
        END FUNCTION
-       FUNCTION ghost_slab_pack(slab,dir,nf,fields,send) BIND(C,name="ghost_slab_pack") RESULT(s)
+       FUNCTION ghost_slab_pack(slab,dir,nf,prune,fields,send) BIND(C,name="ghost_slab_pack") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab, send
-         INTEGER(C_INT), VALUE :: dir, nf
+         INTEGER(C_INT), VALUE :: dir, nf, prune
          TYPE(C_PTR) :: fields(*)
          INTEGER(C_INT) :: s
        END FUNCTION
-       FUNCTION ghost_slab_unpack(slab,dir,nf,recv,fields) BIND(C,name="ghost_slab_unpack") RESULT(s)
+       FUNCTION ghost_slab_unpack(slab,dir,nf,prune,recv,fields) BIND(C,name="ghost_slab_unpack") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab, recv
-         INTEGER(C_INT), VALUE :: dir, nf
+         INTEGER(C_INT), VALUE :: dir, nf, prune
          TYPE(C_PTR) :: fields(*)
          INTEGER(C_INT) :: s
        END FUNCTION

@@ -19,7 +19,9 @@ torch.distributed.all_to_all_single on the default process group (one
 process per GPU over NCCL) in Slab.run, or device copies between the
 ranks that one process holds in run_local.  Fields are torch tensors on
 the device: a rank's kx-slab of a spectral field is (nxh_loc, ny, nz),
-Fortran (nz, ny, ista:iend).
+Fortran (nz, ny, ista:iend).  Every substep after the first of a run is
+zero-pruned as in ghost_hd_run: pruned passes, and exchanges of the kx
+rows below Slab.rows only.
 """
 from __future__ import annotations
 
@@ -56,12 +58,20 @@ def slab_layout(nx: int, nz: int, nranks: int):
     return ista, nxhl, ksta, nzl
 
 
+def live_rows(ista, nxhl, rows):
+    """kx rows of every rank that a pruned exchange moves: the prefix of its
+    slab below the global live rows (None: every row)."""
+    if rows is None:
+        return list(nxhl)
+    return [max(0, min(rows - a, n)) for a, n in zip(ista, nxhl)]
+
+
 def exchange_counts(nxhl, nzl, ny: int, rank: int, direction: int, nf: int):
     """Complex values sent to and received from every peer by `rank` in one
     all-to-all of nf fields.  Direction 0 (kx-slab -> z-slab): the chunk
     for peer p is nf blocks of my kx rows x ny x p's z planes; the chunk
     from p is nf blocks of p's rows x ny x my planes.  Direction 1 is the
-    reverse."""
+    reverse.  For a pruned exchange nxhl is the ranks' live rows."""
     n = len(nxhl)
     mine = [nf * nxhl[rank] * ny * nzl[p] for p in range(n)]
     theirs = [nf * nxhl[p] * ny * nzl[rank] for p in range(n)]
@@ -99,6 +109,9 @@ class Slab:
             stream = torch.cuda.current_stream().cuda_stream
         check(self.lib.ghost_slab_set_stream(self.h, ctypes.c_void_p(stream)), "ghost_slab_set_stream")
         self.ista, self.nxhl, self.ksta, self.nzl = slab_layout(nx, nz, nranks)
+        rows = ctypes.c_int()
+        check(self.lib.ghost_slab_rows(self.h, ctypes.byref(rows)), "ghost_slab_rows")
+        self.rows = rows.value
         self.kshape = (self.nxhl[rank], ny, nz)
         self.zshape = (self.nxh, ny, self.nzl[rank])
         dt = torch.complex64 if precision == "fp32" else torch.complex128
@@ -106,9 +119,12 @@ class Slab:
         self.w = [torch.zeros(self.kshape, dtype=dt, device=dev) for _ in range(6)]   # kx-slab work fields
         self.z = [torch.zeros(self.zshape, dtype=dt, device=dev) for _ in range(6)]   # z-slab work fields
         self.C = [torch.zeros(self.kshape, dtype=dt, device=dev) for _ in range(3)]   # RK copy (hd_rkstep1)
-        self.counts = {d: exchange_counts(self.nxhl, self.nzl, ny, rank, d, 6 if d == 0 else 3) for d in (0, 1)}
-        nsend = max(sum(self.counts[d][0]) for d in (0, 1))
-        nrecv = max(sum(self.counts[d][1]) for d in (0, 1))
+        # (direction, pruned) -> (send counts, receive counts)
+        self.counts = {(d, pr): exchange_counts(live_rows(self.ista, self.nxhl, self.rows if pr else None), self.nzl,
+                                                ny, rank, d, 6 if d == 0 else 3)
+                       for d in (0, 1) for pr in (False, True)}
+        nsend = max(sum(self.counts[d, False][0]) for d in (0, 1))
+        nrecv = max(sum(self.counts[d, False][1]) for d in (0, 1))
         self.send = torch.empty(nsend, dtype=dt, device=dev)
         self.recv = torch.empty(nrecv, dtype=dt, device=dev)
 
@@ -134,60 +150,62 @@ class Slab:
         return v
 
     # -- the phases of one substep ------------------------------------
-    def front(self, v, copy: bool):
-        check(self.lib.ghost_slab_hd_front(self.h, self._pp(self._fields(v)), self._pp(self.C), int(copy),
+    def front(self, v, copy: bool, prune: bool = False):
+        check(self.lib.ghost_slab_hd_front(self.h, self._pp(self._fields(v)), self._pp(self.C), int(copy), int(prune),
                                            self._pp(self.w)), "ghost_slab_hd_front")
 
-    def pack(self, direction: int):
+    def pack(self, direction: int, prune: bool = False):
         fields = self.w if direction == 0 else self.z[:3]
-        check(self.lib.ghost_slab_pack(self.h, direction, len(fields), self._pp(fields),
+        check(self.lib.ghost_slab_pack(self.h, direction, len(fields), int(prune), self._pp(fields),
                                        ctypes.c_void_p(self.send.data_ptr())), "ghost_slab_pack")
 
-    def unpack(self, direction: int):
+    def unpack(self, direction: int, prune: bool = False):
         fields = self.z if direction == 0 else self.w[:3]
-        check(self.lib.ghost_slab_unpack(self.h, direction, len(fields), ctypes.c_void_p(self.recv.data_ptr()),
-                                         self._pp(fields)), "ghost_slab_unpack")
+        check(self.lib.ghost_slab_unpack(self.h, direction, len(fields), int(prune),
+                                         ctypes.c_void_p(self.recv.data_ptr()), self._pp(fields)), "ghost_slab_unpack")
 
-    def xpass(self):
+    def xpass(self, prune: bool = False):
         # one rank: the kx-slab is the whole field and the z-slab layout is the same, so the x pass
         # runs on the front's output in place and no exchange is needed
         z = self.w if self.nranks == 1 else self.z
-        check(self.lib.ghost_slab_hd_xpass(self.h, self._pp(z), self._pp(z[:3])), "ghost_slab_hd_xpass")
+        check(self.lib.ghost_slab_hd_xpass(self.h, int(prune), self._pp(z), self._pp(z[:3])), "ghost_slab_hd_xpass")
 
-    def back(self, o: int, dt: float, nu: float, v, f=None):
+    def back(self, o: int, dt: float, nu: float, v, f=None, prune: bool = False):
         fp = self._pp(self._fields(f)) if f is not None else None
-        check(self.lib.ghost_slab_hd_back(self.h, o, dt, nu, self._pp(self.w[:3]), self._pp(self._fields(v)),
-                                          self._pp(self.C), fp), "ghost_slab_hd_back")
+        check(self.lib.ghost_slab_hd_back(self.h, o, dt, nu, int(prune), self._pp(self.w[:3]),
+                                          self._pp(self._fields(v)), self._pp(self.C), fp), "ghost_slab_hd_back")
 
     # -- runs -----------------------------------------------------------
     def run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None, group=None):
         """nsteps RK steps of order ord (GHOST's RK loop, main3D.fpp:3195-3231)
-        of this rank's kx-slab of v, the transposes as NCCL all-to-alls."""
+        of this rank's kx-slab of v, the transposes as NCCL all-to-alls.
+        Every substep after the first is zero-pruned, as in ghost_hd_run."""
         v, f = [vx, vy, vz], (None if fx is None else [fx, fy, fz])
-        for _ in range(nsteps):
+        for t in range(nsteps):
             for o in range(ord, 0, -1):
-                self.front(v, o == ord)
+                pr = not (t == 0 and o == ord)
+                self.front(v, o == ord, pr)
                 if self.nranks == 1:
-                    self.xpass()
+                    self.xpass(pr)
                 else:
                     for d in (0, 1):
-                        self.pack(d)
-                        all_to_all(self.recv, self.send, self.counts[d][1], self.counts[d][0], group)
-                        self.unpack(d)
+                        self.pack(d, pr)
+                        all_to_all(self.recv, self.send, self.counts[d, pr][1], self.counts[d, pr][0], group)
+                        self.unpack(d, pr)
                         if d == 0:
-                            self.xpass()
-                self.back(o, dt, nu, v, f)
+                            self.xpass(pr)
+                self.back(o, dt, nu, v, f, pr)
 
 
-def _local_exchange(slabs, direction: int):
+def _local_exchange(slabs, direction: int, prune: bool):
     """The all-to-all among ranks held by one process: device copies from
     every peer's send chunk for r into r's receive chunk from that peer."""
     n = len(slabs)
     for r, dst in enumerate(slabs):
         roff = 0
-        rc = dst.counts[direction][1]
+        rc = dst.counts[direction, prune][1]
         for p, src in enumerate(slabs):
-            sc = src.counts[direction][0]
+            sc = src.counts[direction, prune][0]
             soff = sum(sc[:r])
             assert sc[r] == rc[p]
             dst.recv[roff:roff + rc[p]].copy_(src.send[soff:soff + sc[r]])
@@ -200,20 +218,21 @@ def run_local(slabs, nsteps: int, ord: int, dt: float, nu: float, vs, fs=None):
     in rank order, vs[r] / fs[r] rank r's kx-slabs of v and f): the same
     library calls as Slab.run, phase by phase over the ranks, with the
     all-to-alls done by device copies on the current stream."""
-    for _ in range(nsteps):
+    for t in range(nsteps):
         for o in range(ord, 0, -1):
+            pr = not (t == 0 and o == ord)
             for s, v in zip(slabs, vs):
-                s.front(v, o == ord)
+                s.front(v, o == ord, pr)
             if len(slabs) == 1:
-                slabs[0].xpass()
+                slabs[0].xpass(pr)
             for d in (0, 1) if len(slabs) > 1 else ():
                 for s in slabs:
-                    s.pack(d)
-                _local_exchange(slabs, d)
+                    s.pack(d, pr)
+                _local_exchange(slabs, d, pr)
                 for s in slabs:
-                    s.unpack(d)
+                    s.unpack(d, pr)
                 if d == 0:
                     for s in slabs:
-                        s.xpass()
+                        s.xpass(pr)
             for r, (s, v) in enumerate(zip(slabs, vs)):
-                s.back(o, dt, nu, v, None if fs is None else fs[r])
+                s.back(o, dt, nu, v, None if fs is None else fs[r], pr)

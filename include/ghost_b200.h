@@ -556,7 +556,11 @@ int ghost_io_restart(ghost_ctx *ctx, const char *path, int swap, void *spec);
  * blocks of nxh_loc[p] x ny x nz_loc[me]; direction 1 is the reverse.
  * Every z-slab must hold a multiple of 8 planes (GHOST_ERR_SIZE).  All
  * arrays are device arrays; the calls are asynchronous on the slab's
- * stream.  Slab runs are not zero-pruned. */
+ * stream.  prune: a substep whose v is zero outside the truncation (every
+ * substep after the first of a run, as ghost_hd_run does) runs pruned
+ * passes, and its exchanges move only the kx rows below ghost_slab_rows
+ * (a rank's live rows are a prefix of its slab: min(rows - ista_r,
+ * nxh_loc_r) rows, clamped at 0, take the place of nxh_loc_r above). */
 typedef struct ghost_slab ghost_slab;
 /* range(n1,n2,nprocs,irank,ista,iend) of GHOST (1-based, inclusive) */
 int ghost_slab_range(int n1, int n2, int nprocs, int irank, int *ista, int *iend);
@@ -566,27 +570,30 @@ int ghost_slab_destroy(ghost_slab *s);
 /* per-rank 0-based kx-row starts, kx-row counts, z-plane starts, z-plane
  * counts (arrays of nranks ints; any may be NULL) */
 int ghost_slab_layout(const ghost_slab *s, int *ista, int *nxh_loc, int *ksta, int *nz_loc);
+/* the kx rows 0..rows-1 that hold every mode with kn2 <= kmax */
+int ghost_slab_rows(const ghost_slab *s, int *rows);
 int ghost_slab_set_stream(ghost_slab *s, void *stream);
 int ghost_slab_synchronize(ghost_slab *s);
 /* Z inverse and Y inverse of the substep on the kx-slab: v -> w[0..2] = v,
  * w[3..5] = curl v (rotor3), inverse-transformed along z and y; C = v when
  * copy (hd_rkstep1) */
-int ghost_slab_hd_front(ghost_slab *s, const void *const v[3], void *const C[3], int copy, void *const w[6]);
+int ghost_slab_hd_front(ghost_slab *s, const void *const v[3], void *const C[3], int copy, int prune,
+                        void *const w[6]);
 /* the x pass (prodre3's real-space product and the x transforms) on the
  * z-slab: in[0..5] -> out[0..2] = omega x v / (nx ny nz)^2, x transformed
  * back (out may alias in[0..2]) */
-int ghost_slab_hd_xpass(ghost_slab *s, const void *const in[6], void *const out[3]);
+int ghost_slab_hd_xpass(ghost_slab *s, int prune, const void *const in[6], void *const out[3]);
 /* Y forward, Z forward and the truncated update of substep o on the
  * kx-slab: w[0..2] (from the x pass) -> v = C + dt (nu lap v + NL + f)/o
  * (f NULL, or f[0] NULL: no forcing) */
-int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, void *const w[3], void *const v[3],
+int ghost_slab_hd_back(ghost_slab *s, int o, double dt, double nu, int prune, void *const w[3], void *const v[3],
                        const void *const C[3], const void *const f[3]);
 /* the blocks of nf fields for every peer into send (dir 0: from kx-slab
  * fields; dir 1: from z-slab fields) */
-int ghost_slab_pack(ghost_slab *s, int dir, int nf, const void *const *fields, void *send);
+int ghost_slab_pack(ghost_slab *s, int dir, int nf, int prune, const void *const *fields, void *send);
 /* the blocks from every peer out of recv into nf fields (dir 0: z-slab
  * fields; dir 1: kx-slab fields) */
-int ghost_slab_unpack(ghost_slab *s, int dir, int nf, const void *recv, void *const *fields);
+int ghost_slab_unpack(ghost_slab *s, int dir, int nf, int prune, const void *recv, void *const *fields);
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,14 @@ def test_exchange_counts_match_between_peers(nx, nz, p):
                 assert c[r][0][q] == c[q][1][r]     # what r sends q is what q expects from r
         # every value of the nf fields moves exactly once
         assert sum(sum(x[0]) for x in c) == nf * (nx // 2 + 1) * ny * nz
+    # pruned: only the rows below the live count, each exactly once
+    from ghost_b200.slab import live_rows
+    rows = (nx // 3) + 1
+    lr = live_rows(ista, nxhl, rows)
+    assert sum(lr) == rows and all(0 <= a <= b for a, b in zip(lr, nxhl))
+    assert all(lr[r] == nxhl[r] for r in range(p) if ista[r] + nxhl[r] <= rows)
+    c = [exchange_counts(lr, nzl, ny, r, 0, 6) for r in range(p)]
+    assert sum(sum(x[0]) for x in c) == 6 * rows * ny * nz
 
 
 def _free_port():
