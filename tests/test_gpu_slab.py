@@ -52,3 +52,47 @@ def test_slab_phases_reject_host_and_misshaped_arrays():
     with pytest.raises(ValueError):
         s.front([t[:-1] for t in s.C], True)
     s.close()
+
+
+def test_slab_run_without_forcing_and_null_forcing_pointers():
+    """No forcing: f NULL (Python None) and f an array of three null
+    pointers (a Fortran caller's C_NULL_PTRs) both mean none, against the
+    undivided run without forcing.  FP32, 4 ranks (one without live rows)."""
+    import ctypes
+
+    import torch
+
+    from ghost_b200 import Ghost
+    from ghost_b200.slab import Slab, run_local
+    g = Ghost(64, precision="fp32")
+    v0 = _fields(g, 1000)
+    ref = [x.clone() for x in v0]
+    g.hd_run(1, 2, 1e-3, 2e-3, *ref)
+    P = 4
+    slabs = [Slab(64, precision="fp32", rank=r, nranks=P) for r in range(P)]
+    assert slabs[0].rows == 22 and slabs[3].ista[3] >= 22   # the last rank holds no live kx row
+    vs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in v0] for r, s in enumerate(slabs)]
+    run_local(slabs, 1, 2, 1e-3, 2e-3, vs, None)
+    torch.cuda.synchronize()
+    for c in range(3):
+        got = torch.cat([vs[r][c] for r in range(P)], dim=0)
+        err = ((got - ref[c]).abs().max() / ref[c].abs().max()).item()
+        assert err <= 1e-5, (c, err)
+    # one substep's back phase with three null forcing pointers equals it with f = NULL
+    s = Slab(64, precision="fp64", rank=0, nranks=1)
+    g64 = Ghost(64, precision="fp64")
+    v = _fields(g64, 5)
+    outs = []
+    for nullarr in (False, True):
+        w = [x.clone() for x in v]
+        s.front(w, True)
+        s.xpass()
+        f = (ctypes.c_void_p * 3)(None, None, None) if nullarr else None
+        st = s.lib.ghost_slab_hd_back(s.h, 1, 1e-3, 2e-3, 0, s._pp(s.w[:3]), s._pp(w), s._pp(s.C), f)
+        assert st == 0, s.lib.ghost_last_error_string()
+        torch.cuda.synchronize()
+        outs.append([x.clone() for x in w])
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+    for t in slabs + [s]:
+        t.close()
