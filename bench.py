@@ -9,10 +9,14 @@ fused substeps).  Inputs (0.54 GB per FP32 field) are far larger than L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the CPU restatement of GHOST's FFTW/OpenMP path on
-the host cores (the reference itself needs Fortran+MPI+FFTW, absent here).
-With torchrun (N > 1) every rank advances its own independent 512^3 run
-(replicas, weak scaling); the slab-decomposed single run is not built.
+--impl reference times GHOST's CPU path on the host cores: the same steps
+(fftp-3 transforms, prodre3, nonlhd3, the truncated update) with a threaded
+library FFT, as GHOST's FFTW/OpenMP build runs them (GHOST itself needs
+Fortran, MPI and FFTW, none of which exist here).  Each of its steps is a
+bounded sample, one RK substep, so that the run ends within minutes.
+With torchrun (N > 1) the ranks advance ONE 512^3 run split into GHOST's
+kx-slabs / z-slabs, with an NCCL all-to-all per transform direction
+(strong scaling); N = 1 runs the undivided fused step.
 """
 from __future__ import annotations
 
@@ -110,7 +114,7 @@ def dist_init(args):
         backend = "nccl" if args.impl == "ours" and torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
     return ws, rank, local
 
 
@@ -132,36 +136,60 @@ def max_over_ranks(ws, x):
 
 
 # ---------------------------------------------------------------- CPU arm
-def cpu_substep_time(n, samples, warmup):
-    """Seconds per RK substep of the oracle (FP32, all host threads)."""
-    import numpy as np
+def cpu_fields(o):
+    v, _ = o.random_solenoidal(1000, 1.0, o.nx / 3.0, 1, 1.0)
+    f, _ = o.random_solenoidal(2000, 2.0, 3.0, 0, 1.0)
+    return v, f
+
+
+def cpu_substep_times(n, samples, warmup, kind="fftlib", threads=None):
+    """Seconds of each timed RK substep at n^3 FP32 on the host cores.
+    kind "fftlib": GHOST's steps with a threaded library FFT (scipy's
+    pocketfft, all host threads), the stand-in for its FFTW/OpenMP build;
+    kind "oracle": the C restatement (OpenMP, its own textbook FFT)."""
     from oracle.oracle import Oracle
     o = Oracle(n, precision="fp32")
-    v, _ = o.random_solenoidal(1000, 1.0, n / 3.0, 1, 1.0)
-    f, _ = o.random_solenoidal(2000, 2.0, 3.0, 0, 1.0)
+    v, f = cpu_fields(o)
     C = [x.copy() for x in v]
+    if kind == "fftlib":
+        from oracle.fftlib import FFTLibHD
+        lib = FFTLibHD(o, threads)
+        step, cores = lib.hd_rkstep2, lib.threads
+    else:
+        step, cores = o.hd_rkstep2, o.nthreads()
     times = []
     for s in range(warmup + samples):
         t0 = time.perf_counter()
-        v = o.hd_rkstep2(ORD - (s % ORD), DT, NU, v, C, f)
+        v = step(ORD - (s % ORD), DT, NU, v, C, f)
         dt = time.perf_counter() - t0
         if s >= warmup:
             times.append(dt)
-    return float(np.mean(times)), o.nthreads()
+    if kind == "fftlib":
+        lib.close()
+    return times, cores
 
 
 def run_reference(args, ws, rank):
+    """GHOST's CPU path on the host cores.  Each of the K timed steps is one
+    RK substep at 512^3 (a quarter of an RK4 step: a whole RK4 step of the
+    CPU path takes ~10 s, so K of them would not fit the run), after W
+    untimed ones; value = RK4 steps/s = 1 / (4 x mean substep time)."""
     if rank != 0:
         return
-    t, cores = cpu_substep_time(args.grid, max(1, args.steps), max(0, args.warmup))
+    times, cores = cpu_substep_times(args.grid, max(1, args.steps), max(0, args.warmup))
+    t = sum(times) / len(times)
     val = 1.0 / (ORD * t)
-    sample = (f"{max(1, args.steps)} timed RK substeps at {args.grid}^3 FP32 (1/{ORD} of an RK{ORD} step each), "
-              f"after {args.warmup} untimed; steps/s = 1/({ORD} x mean substep time)")
+    sample = (f"each step: 1 RK substep at {args.grid}^3 FP32 (1/{ORD} of an RK{ORD} step) of GHOST's CPU path with a "
+              f"threaded library FFT (scipy pocketfft, {cores} threads), {len(times)} timed after {args.warmup} "
+              f"untimed; value = 1/({ORD} x mean substep time)")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ORD * t, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "ms_per_rk_step": 1e3 * ORD * t,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
             "config": {"workload": f"HD forced turbulence {args.grid}^3, RK{ORD}, dt={DT}, nu={NU}, FP32",
-                       "runs": "CPU restatement of GHOST's fftp-3 + pseudospec3D_hd path (C, OpenMP)"},
+                       "runs": "GHOST's fftp-3 + pseudospec3D_hd steps on the host cores, scipy.fft (pocketfft) "
+                               "in place of FFTW, numpy elementwise work split over the same threads",
+                       "step": "one RK substep sample (ms_per_step); ms_per_rk_step = 4 x that"},
             "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -350,9 +378,50 @@ def prune_fractions(n):
     return float(f_line), float(f_row), float(f_keep)
 
 
+def fp64_vs_cpu_oracle(g64, v64, f64):
+    """One RK4 step of the FP64 plain path at full size (the first substep
+    full, the other three zero-pruned, as timed) against the same step of the
+    CPU FP64 oracle from the same state: relative L2 of v."""
+    import numpy as np
+    import torch
+
+    from oracle.oracle import Oracle
+    o = Oracle(g64.nx, g64.ny, g64.nz, precision="fp64")
+    hv = [x.cpu().numpy() for x in v64]
+    hf = [x.cpu().numpy() for x in f64]
+    g64.hd_run(1, ORD, DT, NU, *v64, *f64)
+    torch.cuda.synchronize()
+    ref = o.hd_run(1, ORD, DT, NU, hv, hf)
+    del hv, hf
+    num = den = 0.0
+    for a, b in zip(v64, ref):
+        d = a.cpu().numpy()
+        num += float(np.sum(np.abs(d - b) ** 2))
+        den += float(np.sum(np.abs(b) ** 2))
+    return (num / den) ** 0.5
+
+
+def cpu_baselines(n):
+    """The host-core rates beside the GPU line: GHOST's CPU path with the
+    threaded library FFT (1 warm-up and 3 timed substeps) and the C oracle
+    restatement (2 timed substeps), both FP32 on all host threads."""
+    t_lib, cores = cpu_substep_times(n, 3, 1, "fftlib")
+    t_or, cores_or = cpu_substep_times(n, 2, 0, "oracle")
+    m_lib, m_or = sum(t_lib) / len(t_lib), sum(t_or) / len(t_or)
+    cpu = {"value": 1.0 / (ORD * m_lib), "unit": "steps/s", "cores": cores, "kind": "port",
+           "sample": f"{len(t_lib)} RK substeps at {n}^3 FP32 (1/{ORD} of an RK{ORD} step each) after 1 untimed, "
+                     f"GHOST's CPU path with scipy pocketfft in place of FFTW on {cores} threads; "
+                     f"steps/s = 1/({ORD} x mean substep time)",
+           "oracle_c": {"value": 1.0 / (ORD * m_or), "unit": "steps/s", "cores": cores_or,
+                        "sample": f"{len(t_or)} RK substeps of the C restatement (textbook FFT, OpenMP)"}}
+    return cpu
+
+
 def run_ours(args, ws, rank, local):
     import torch
     torch.cuda.set_device(local)
+    if ws > 1:
+        return run_slab(args, ws, rank, local)
     n = args.grid
     peak, peak_kind = peaks()
     clocks = Clocks(local)
@@ -367,16 +436,17 @@ def run_ours(args, ws, rank, local):
     del v32, f32
     torch.cuda.empty_cache()
     g64, v64, f64 = setup_run(n, "fp64", rank)
-    ms64, _, tm64 = timed_steps(g64, v64, f64, max(2, args.steps // 2), args.warmup, ws, timers=True)
+    steps64_n = max(2, args.steps // 2)
+    ms64, _, tm64 = timed_steps(g64, v64, f64, steps64_n, args.warmup, ws, timers=True)
     tile64 = g64.tile
     clk = clocks.stop()
+    err64 = fp64_vs_cpu_oracle(g64, v64, f64) if not args.no_cpu_baseline else None
     g64.close()
     del v64, f64
     torch.cuda.empty_cache()
 
     steps32 = args.steps / (ms32 * 1e-3)
-    steps64 = max(2, args.steps // 2) / (ms64 * 1e-3)
-    value = ws * steps32
+    steps64 = steps64_n / (ms64 * 1e-3)
 
     # dominant kernel and its roofline: algorithmic bytes per launch, the
     # bytes each pass must move once the known zeros of the 2/3 truncation
@@ -391,52 +461,154 @@ def run_ours(args, ws, rank, local):
     dom = max(tm, key=lambda k: tm[k][0])
     dom_ms = tm[dom][0] / tm[dom][1]
     ach = per_launch_bytes[dom] / (dom_ms * 1e-3) / 1e9
-    kern = {k: {"ms_per_launch": tm[k][0] / tm[k][1], "launches": tm[k][1],
-                "share": tm[k][0] / sum(x[0] for x in tm.values()),
-                "gbs": per_launch_bytes[k] / (tm[k][0] / tm[k][1] * 1e-3) / 1e9 if k in per_launch_bytes else None}
-            for k in tm}
 
-    err = rel_err_fp32_step(n, rank) if rank == 0 else None
-    fft = fft_roofline(n, peak) if rank == 0 else None
-    e2e_val, h2d, d2h = e2e_host(n, args.e2e_steps, rank) if rank == 0 else (None, 0, 0)
-    if ws > 1:
-        e2e_val = None
+    def kern_table(t, scale):
+        return {k: {"ms_per_launch": t[k][0] / t[k][1], "launches": t[k][1],
+                    "share": t[k][0] / sum(x[0] for x in t.values()),
+                    "gbs": scale * per_launch_bytes[k] / (t[k][0] / t[k][1] * 1e-3) / 1e9
+                    if k in per_launch_bytes else None}
+                for k in t}
 
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        t, cores = cpu_substep_time(n, 1, 0)
-        cpu = {"value": 1.0 / (ORD * t), "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": f"1 RK substep at {n}^3 FP32 (1/{ORD} of an RK{ORD} step) of the CPU restatement, "
-                         f"steps/s = 1/({ORD} x substep time)"}
+    err = rel_err_fp32_step(n, rank)
+    fft = fft_roofline(n, peak)
+    e2e_val, h2d, d2h = e2e_host(n, args.e2e_steps, rank)
+    cpu = cpu_baselines(n) if not args.no_cpu_baseline else None
 
-    # SURVEY-defined algorithmic bytes per substep at 512^3: 9 FFTs x (R+C) + 15 C
+    # algorithmic bytes per substep on the unpruned count 9 FFTs x (R + C) + 15 C
     R = n ** 3 * 4
-    survey_bytes = 9 * (R + cb) + 15 * cb
+    unpruned_bytes = 9 * (R + cb) + 15 * cb
+    line = {
+        "metric": METRIC, "value": steps32, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"HD forced turbulence {n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32 fast path",
+                   "parallelism": "single GPU",
+                   "l2": "inputs larger than L2 (0.54 GB per FP32 field)"},
+        "fp64": {"value": steps64, "unit": "steps/s", "ms_per_step": ms64 / steps64_n,
+                 "tile_cfg": tile64, "kernels": kern_table(tm64, 2.0)},
+        "tile_cfg": tile32,
+        "fp32_over_fp64": steps32 / steps64,
+        "fp32_rel_err_per_step": err,
+        "fp64_rel_err_vs_cpu_oracle": err64,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "peak_kind": peak_kind,
+                     "traffic": traffic_from_profiles(dom)},
+        "kernels": kern_table(tm, 1.0),
+        "fft": fft,
+        "substep_effective_gbs": unpruned_bytes / (ms32 / args.steps / ORD * 1e-3) / 1e9,
+        "prune": {"f_line": f_line, "f_row": f_row, "f_keep": f_keep},
+        "substep_bytes": sum(per_launch_bytes.values()),
+        "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_slab(args, ws, rank, local):
+    """N > 1: one n^3 run split over the ranks in GHOST's slab layout
+    (kx-slabs of the spectral fields, z-slabs for the x pass), two NCCL
+    all-to-alls per substep (ghost_b200.slab).  Every rank generates the
+    same seeded fields as the one-GPU run and keeps its kx-slab."""
+    import torch
+
+    from ghost_b200 import Ghost
+    from ghost_b200.slab import Slab
+    n = args.grid
+    clocks = Clocks(local)
+
+    def setup(prec):
+        g = Ghost(n, precision=prec)
+        v = [g.czeros() for _ in range(3)]
+        f = [g.czeros() for _ in range(3)]
+        g.init_random_solenoidal(1000, 1.0, n / 3.0, 1, 1.0, *v)
+        g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *f)
+        s = Slab(n, precision=prec, rank=rank, nranks=ws)
+        lo, cnt = s.ista[rank], s.nxhl[rank]
+        vs = [x[lo:lo + cnt].clone() for x in v]
+        fs = [x[lo:lo + cnt].clone() for x in f]
+        g.close()
+        del v, f
+        torch.cuda.empty_cache()
+        return s, vs, fs
+
+    def timed(s, vs, fs, steps, warmup):
+        s.run(warmup, ORD, DT, NU, *vs, *fs)
+        barrier(ws)
+        torch.cuda.synchronize()
+        n0 = s.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.run(steps, ORD, DT, NU, *vs, *fs)
+        e1.record()
+        e1.synchronize()
+        launches = s.launch_count() - n0
+        ms = max_over_ranks(ws, e0.elapsed_time(e1))
+        barrier(ws)
+        return ms, launches
+
+    s32, v32, f32 = setup("fp32")
+    clocks.start()
+    ms32, launches = timed(s32, v32, f32, args.steps, args.warmup)
+    # exchange time per substep (a separate, untimed step with events around the all-to-alls)
+    ev = []
+    s32.run(1, ORD, DT, NU, *v32, *f32, exchange_events=ev)
+    torch.cuda.synchronize()
+    xch = max_over_ranks(ws, sum(a.elapsed_time(b) for a, b in ev) / ORD)
+    barrier(ws)
+    # e2e: every step copies this rank's slabs of v and f in from pinned host
+    # memory and v out, around the same library calls
+    hv = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in v32]
+    hf = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in f32]
+    for a, b in zip(hv + hf, v32 + f32):
+        a.copy_(b)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.e2e_steps):
+        for a, b in zip(v32 + f32, hv + hf):
+            a.copy_(b, non_blocking=True)
+        s32.run(1, ORD, DT, NU, *v32, *f32)
+        for a, b in zip(hv, v32):
+            a.copy_(b, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    ms_e2e = max_over_ranks(ws, e0.elapsed_time(e1))
+    cb_loc = v32[0].numel() * v32[0].element_size()
+    tot = torch.tensor([6.0 * cb_loc, 3.0 * cb_loc], dtype=torch.float64, device="cuda")
+    import torch.distributed as dist
+    dist.all_reduce(tot)
+    h2d, d2h = int(tot[0].item()), int(tot[1].item())
+    s32.close()
+    del v32, f32, hv, hf
+    torch.cuda.empty_cache()
+    s64, v64, f64 = setup("fp64")
+    steps64_n = max(2, args.steps // 2)
+    ms64, _ = timed(s64, v64, f64, steps64_n, args.warmup)
+    clk = clocks.stop()
+    s64.close()
+    steps32 = args.steps / (ms32 * 1e-3)
+    steps64 = steps64_n / (ms64 * 1e-3)
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "metric": METRIC, "value": steps32, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": f"HD forced turbulence {n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32 fast path",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (0.54 GB per FP32 field)"},
-            "fp64": {"value": ws * steps64, "unit": "steps/s", "ms_per_step": ms64 / max(2, args.steps // 2),
-                     "tile_cfg": tile64},
-            "tile_cfg": tile32,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"HD forced turbulence {n}^3, RK{ORD}, dt={DT}, nu={NU}, FP32 fast path, one run "
+                                   f"split over {ws} GPUs",
+                       "parallelism": f"slab x{ws} (kx-slabs / z-slabs, NCCL all-to-all per transform direction)",
+                       "l2": "inputs larger than L2"},
+            "fp64": {"value": steps64, "unit": "steps/s", "ms_per_step": ms64 / steps64_n},
             "fp32_over_fp64": steps32 / steps64,
-            "fp32_rel_err_per_step": err,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "peak_kind": peak_kind,
-                         "traffic": traffic_from_profiles(dom)},
-            "kernels": kern,
-            "fft": fft,
-            "substep_effective_gbs": survey_bytes / (ms32 / args.steps / ORD * 1e-3) / 1e9,
-            "prune": {"f_line": f_line, "f_row": f_row, "f_keep": f_keep},
-            "substep_bytes": sum(per_launch_bytes.values()),
-            "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
+            "exchange_ms_per_substep": xch,
+            "e2e": {"value": args.e2e_steps / (ms_e2e * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches * ws,
+            "gpu_launches_per_rank": launches,
             "clocks": clk,
-            "cpu_baseline": cpu,
+            "cpu_baseline": None,
         }
         print(json.dumps(line), flush=True)
 

@@ -104,6 +104,7 @@ SIGNATURES = {
     "ghost_slab_destroy": [P],
     "ghost_slab_layout": [P] + [ctypes.POINTER(ctypes.c_int)] * 4,
     "ghost_slab_rows": [P, ctypes.POINTER(ctypes.c_int)],
+    "ghost_slab_launch_count": [P, ctypes.POINTER(ctypes.c_longlong)],
     "ghost_slab_set_stream": [P, P],
     "ghost_slab_synchronize": [P],
     "ghost_slab_hd_front": [P, PP, PP, I, I, PP],

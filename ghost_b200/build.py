@@ -50,6 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
     ccbin = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else None
+    cmds = []
     for src in SOURCES:
         obj = os.path.join(bdir, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]
@@ -57,8 +58,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd[1:1] = ["-ccbin", ccbin]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units compile independently: one nvcc per source
+    procs = [subprocess.Popen(cmd) for cmd in cmds]
+    bad = [" ".join(cmd) for cmd, p in zip(cmds, procs) if p.wait() != 0]
+    if bad:
+        raise subprocess.CalledProcessError(1, bad[0])
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     if ccbin:

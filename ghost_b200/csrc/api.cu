@@ -2425,13 +2425,17 @@ int ghost_bouss_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, dou
 }  // extern "C"
 
 // ------------------------------------------------- no-allocation spectrum
-// Partial sums of ghost_spectrumc_noalloc: a fixed grid of
-// NOALLOC_BLOCKS blocks writes one histogram row each, then the final row.
-// Every slot a call reads was written earlier by that same call, so
-// nothing needs clearing between calls.
-#define NOALLOC_BLOCKS 64
-static_assert((NOALLOC_BLOCKS + 1) * GHOST_SPECTRUM_NOALLOC_MAX_BINS <= GHOST_SPECTRUM_NOALLOC_DOUBLES,
+// Partial sums of ghost_spectrumc_noalloc: nblk blocks write one
+// histogram row of nbins each, then the final row follows them; nblk is
+// chosen per call so that the (nblk + 1) rows fit the static array.  Every
+// slot a call reads was written earlier by that same call, so nothing needs
+// clearing between calls.
+static_assert(2 * GHOST_SPECTRUM_NOALLOC_MAX_BINS <= GHOST_SPECTRUM_NOALLOC_DOUBLES,
               "static spectrum scratch too small for the advertised shell count");
+static int noalloc_blocks(size_t n, int nbins) {
+  const int fit = GHOST_SPECTRUM_NOALLOC_DOUBLES / nbins - 1;  // rows left after the final one
+  return std::max(1, std::min(std::min(grid1d(n), 148 * 4), fit));
+}
 static __device__ __align__(256) double g_spectrum_scratch[GHOST_SPECTRUM_NOALLOC_DOUBLES];
 
 static std::mutex g_spectrum_scratch_mu;
@@ -2439,6 +2443,9 @@ static void *g_spectrum_scratch_addr[128];
 
 // Device address of the static array on the current device, looked up
 // once per device (in host code the symbol is only a host-side stand-in).
+// The cached address belongs to the device's primary context: after
+// cudaDeviceReset the module reloads elsewhere, so a process that resets a
+// device must not call ghost_spectrumc_noalloc on it again.
 static int spectrum_scratch_address(int dev, double **out) {
   if (dev < 0 || dev >= 128) return fail(GHOST_ERR_STATE, "device ordinal %d out of range", dev);
   std::lock_guard<std::mutex> lock(g_spectrum_scratch_mu);
@@ -2459,14 +2466,17 @@ template <typename R>
 static int spectrum_noalloc_dev(ghost_ctx *c, double *scratch, int kind, const void *a, const void *b, const void *cc,
                                 double *out_host) {
   const int nbins = c->nmax / 2 + 1;
+  // every run of a batched context, as ghost_spectrumc sums them
+  const size_t n = c->ntot;
+  const int nblk = noalloc_blocks(n, nbins);
   RedArgs<R> ra{(const cx<R> *)a, (const cx<R> *)b, (const cx<R> *)cc, nullptr, nullptr, nullptr};
   const size_t smem = (size_t)(256 / 32) * nbins * sizeof(double);
   GB_CUDA(cudaFuncSetAttribute(spectrum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  spectrum_kernel<R><<<NOALLOC_BLOCKS, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, c->nspec, nbins, (R)c->Dkk,
-                                                                 (R)0.501f, scratch);
+  spectrum_kernel<R><<<nblk, 256, smem, c->stream>>>(kparams<R>(c), ra, kind, n, nbins, (R)c->Dkk, (R)0.501f,
+                                                     scratch);
   GB_CHECK(post_launch(c));
-  double *fin = scratch + (size_t)NOALLOC_BLOCKS * nbins;
-  finalize_kernel<<<1, 256, 0, c->stream>>>(scratch, NOALLOC_BLOCKS, nbins, fin);
+  double *fin = scratch + (size_t)nblk * nbins;
+  finalize_kernel<<<1, 256, 0, c->stream>>>(scratch, nblk, nbins, fin);
   GB_CHECK(post_launch(c));
   GB_CUDA(cudaMemcpyAsync(out_host, fin, sizeof(double) * nbins, cudaMemcpyDeviceToHost, c->stream));
   GB_CUDA(cudaStreamSynchronize(c->stream));
@@ -2486,8 +2496,8 @@ int ghost_spectrumc_noalloc(ghost_ctx *c, const void *a, const void *b, const vo
     return fail(GHOST_ERR_ARG, "ghost_spectrumc_noalloc needs device arrays (host arrays would need staging buffers)");
   const int nbins = c->nmax / 2 + 1;
   if (nbins > GHOST_SPECTRUM_NOALLOC_MAX_BINS)
-    return fail(GHOST_ERR_SIZE, "%d spectral shells exceed the static scratch limit of %d (nmax <= %d)", nbins,
-                GHOST_SPECTRUM_NOALLOC_MAX_BINS, 2 * (GHOST_SPECTRUM_NOALLOC_MAX_BINS - 1));
+    return fail(GHOST_ERR_SIZE, "%d spectral shells (nmax/2+1) exceed the static scratch limit of %d (nmax <= %d)",
+                nbins, GHOST_SPECTRUM_NOALLOC_MAX_BINS, 2 * GHOST_SPECTRUM_NOALLOC_MAX_BINS - 1);
   int dev = -1;
   GB_CUDA(cudaGetDevice(&dev));
   if (dev != c->device) return fail(GHOST_ERR_STATE, "current device %d is not the context's device %d", dev, c->device);
@@ -3028,6 +3038,13 @@ int ghost_slab_rows(const ghost_slab *s, int *rows) {
   SLAB_CHECK(s);
   if (!rows) return fail(GHOST_ERR_ARG, "null output");
   *rows = s->rows_glob;
+  return GHOST_OK;
+}
+
+int ghost_slab_launch_count(const ghost_slab *s, long long *count) {
+  SLAB_CHECK(s);
+  if (!count) return fail(GHOST_ERR_ARG, "null output");
+  *count = s->spec->launches + (s->real != s->spec ? s->real->launches : 0);
   return GHOST_OK;
 }
 

@@ -392,6 +392,12 @@
          INTEGER(C_INT) :: rows
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_slab_launch_count(slab,count) BIND(C,name="ghost_slab_launch_count") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_LONG_LONG
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_LONG_LONG) :: count
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_slab_set_stream(slab,stream) BIND(C,name="ghost_slab_set_stream") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: slab, stream

@@ -139,6 +139,12 @@ class Slab:
         except Exception:
             pass
 
+    def launch_count(self) -> int:
+        """Kernels launched by this rank's slab contexts so far."""
+        n = ctypes.c_longlong()
+        check(self.lib.ghost_slab_launch_count(self.h, ctypes.byref(n)), "ghost_slab_launch_count")
+        return n.value
+
     @staticmethod
     def _pp(ts):
         return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
@@ -176,10 +182,13 @@ class Slab:
                                           self._pp(self._fields(v)), self._pp(self.C), fp), "ghost_slab_hd_back")
 
     # -- runs -----------------------------------------------------------
-    def run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None, group=None):
+    def run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None, group=None,
+            exchange_events=None):
         """nsteps RK steps of order ord (GHOST's RK loop, main3D.fpp:3195-3231)
         of this rank's kx-slab of v, the transposes as NCCL all-to-alls.
-        Every substep after the first is zero-pruned, as in ghost_hd_run."""
+        Every substep after the first is zero-pruned, as in ghost_hd_run.
+        exchange_events: a list to which CUDA event pairs bracketing each
+        all-to-all (on the current stream) are appended."""
         v, f = [vx, vy, vz], (None if fx is None else [fx, fy, fz])
         for t in range(nsteps):
             for o in range(ord, 0, -1):
@@ -190,7 +199,14 @@ class Slab:
                 else:
                     for d in (0, 1):
                         self.pack(d, pr)
+                        if exchange_events is not None:
+                            e0 = torch.cuda.Event(enable_timing=True)
+                            e0.record()
                         all_to_all(self.recv, self.send, self.counts[d, pr][1], self.counts[d, pr][0], group)
+                        if exchange_events is not None:
+                            e1 = torch.cuda.Event(enable_timing=True)
+                            e1.record()
+                            exchange_events.append((e0, e1))
                         self.unpack(d, pr)
                         if d == 0:
                             self.xpass(pr)

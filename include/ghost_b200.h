@@ -297,14 +297,22 @@ int ghost_heltperp(ghost_ctx *ctx, const void *a, const void *b, const void *c, 
  * The partial sums live in a static device array of
  * GHOST_SPECTRUM_NOALLOC_DOUBLES doubles (512 KiB, held by every GPU that
  * loads the library until the process exits); a grid with more than
- * GHOST_SPECTRUM_NOALLOC_MAX_BINS shells (nmax/2+1) is rejected with
- * GHOST_ERR_SIZE.  a, b, c must be device arrays (host arrays would need
- * staging buffers: GHOST_ERR_ARG); Ek, Hk are host arrays as above.  The
- * first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  All
- * calls share the one array and it keeps the last call's contents: calls
- * that overlap on the GPU (other streams, other contexts on the device)
- * race and must be serialised by the caller. */
+ * GHOST_SPECTRUM_NOALLOC_MAX_BINS shells (nmax/2+1 <= 1008, i.e.
+ * nmax <= 2015) is rejected with GHOST_ERR_SIZE.  On a batched context
+ * (ghost_ctx_create_batch) the spectra sum every run, as ghost_spectrumc
+ * does.  a, b, c must be device arrays (host arrays would need staging
+ * buffers: GHOST_ERR_ARG); Ek, Hk are host arrays as above.
+ * The array is committed when the library's device code is loaded on a
+ * device, which with CUDA's default lazy module loading happens at the
+ * first library call that launches a kernel there (this one included):
+ * make some library call on each device before filling its memory.  The
+ * first call on a device also looks up the array's device address with
+ * that device current; make that first call before any stream capture.
+ * The address stays valid for the process unless the device is reset
+ * (cudaDeviceReset), after which this entry point must not be used on it.
+ * All calls share the one array and it keeps the last call's contents:
+ * calls that overlap on the GPU (other streams, other contexts on the
+ * device) race and must be serialised by the caller. */
 #define GHOST_SPECTRUM_NOALLOC_DOUBLES 65536
 #define GHOST_SPECTRUM_NOALLOC_MAX_BINS 1008
 int ghost_spectrumc_noalloc(ghost_ctx *ctx, const void *a, const void *b, const void *c, int kin, int hel,
@@ -572,6 +580,8 @@ int ghost_slab_destroy(ghost_slab *s);
 int ghost_slab_layout(const ghost_slab *s, int *ista, int *nxh_loc, int *ksta, int *nz_loc);
 /* the kx rows 0..rows-1 that hold every mode with kn2 <= kmax */
 int ghost_slab_rows(const ghost_slab *s, int *rows);
+/* kernels this rank's slab contexts have launched (ghost_ctx_launch_count) */
+int ghost_slab_launch_count(const ghost_slab *s, long long *count);
 int ghost_slab_set_stream(ghost_slab *s, void *stream);
 int ghost_slab_synchronize(ghost_slab *s);
 /* Z inverse and Y inverse of the substep on the kx-slab: v -> w[0..2] = v,

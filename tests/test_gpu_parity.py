@@ -614,3 +614,42 @@ def test_phaseshift(prec, shape):
     g.phaseshift(A, cd)
     ref = o.phaseshift(a, cd)
     assert rel_l2(to_host(A), ref) <= (1e-15 if prec == "fp64" else 1e-7)
+
+
+# ------------------------------------------- the benchmark's 512-point lines
+# Shapes whose lines along one axis (or two) have 512 points run the same
+# kernel instantiations as the 512^3 benchmark step: xpipe_nl_kernel<*, 512,
+# ...> for nx = 512, ypipe_kernel<*, 512, ...> for ny = 512 and
+# zpipe_kernel<*, 512, ...> for nz = 512.  Tile variant 30 is the FP32
+# benchmark's (two-stage z ring with three CTAs per SM, y passes with 16
+# values per thread and a second exchange buffer); FP64 runs the variants
+# the autotuner picks at 512^3 (22, 6) and the default.
+LINE512 = [(512, 16, 16), (16, 512, 16), (16, 16, 512), (512, 512, 16)]
+
+
+@pytest.mark.parametrize("shape", LINE512)
+@pytest.mark.parametrize("prec,cfgs,tol", [("fp64", (0, 6, 22), 1e-12), ("fp32", (0, 30), 1e-5)])
+def test_forced_rk4_with_512_point_lines(shape, prec, cfgs, tol):
+    """Config 1's step (forced on 2 <= |k| <= 3, nu = 1e-3, dt = 5e-4, RK4)
+    for two steps (the second zero-pruned) against the FP64 oracle; every
+    tile variant gives the same bits."""
+    import torch
+    o = Oracle(*shape)
+    kup = max(shape) / 3.0
+    v0, _ = o.random_solenoidal(1000, 1.0, kup, 1, 1.0)
+    f, _ = o.random_solenoidal(2000, 2.0, 3.0, 0, 1.0)
+    ref = o.hd_run(2, 4, 5e-4, 1e-3, v0, f)
+    g = ghost(*shape, precision=prec)
+    cd = g.cdtype_np
+    F = [to_dev(x.astype(cd)) for x in f]
+    first = None
+    for cfg in cfgs:
+        g.set_tile_cfg(cfg)
+        V = [to_dev(x.astype(cd)) for x in v0]
+        g.hd_run(2, 4, 5e-4, 1e-3, *V, *F)
+        err = rel_l2([to_host(x).astype(np.complex128) for x in V], ref)
+        assert err <= tol, (cfg, err)
+        if first is None:
+            first = V
+        else:
+            assert all(torch.equal(a, b) for a, b in zip(V, first)), cfg

@@ -45,6 +45,31 @@ def test_noalloc_spectrum_matches_allocating_entry_point(prec):
     assert torch.cuda.mem_get_info()[0] == free0
 
 
+def test_noalloc_spectrum_on_a_batched_context_sums_every_run():
+    """A batch of three 32^3 runs: both entry points bin the modes of every
+    run, so the spectra agree with each other and with the sum of the three
+    runs' own spectra."""
+    from ghost_b200 import Ghost, _lib
+    lib = _lib.load()
+    seeds = [21, 22, 23]
+    g = Ghost(32, precision="fp64", nruns=3)
+    v = [g.czeros() for _ in range(3)]
+    g.batch_init_random_solenoidal(seeds, 1.0, 32 / 3.0, 1, 1.0, *v)
+    Ek0, Hk0 = g.spectrumc(*v, 1, 1)
+    for _ in range(2):
+        s, Ek, Hk = _spectra_noalloc(g, lib, v, 1, 1)
+        assert s == 0, lib.ghost_last_error_string()
+        assert np.allclose(Ek, Ek0, rtol=1e-12, atol=0)
+        assert np.allclose(Hk, Hk0, rtol=1e-9, atol=1e-18)
+    one = Ghost(32, precision="fp64")
+    nxh = 17
+    total = np.zeros_like(Ek0)
+    for r in range(3):
+        e, _ = one.spectrumc(*[x[r * nxh:(r + 1) * nxh].contiguous() for x in v], 1, 0)
+        total += e
+    assert np.allclose(Ek, total, rtol=1e-12, atol=0)
+
+
 def test_noalloc_spectrum_rejects_what_it_cannot_do():
     from ghost_b200 import Ghost, _lib
     lib = _lib.load()
