@@ -374,12 +374,18 @@ int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   const int grid = persistent_grid(c, kern, BZ * T, smem, ntiles);
   // box rows: 32 (or N/2) for the pruned inverse, whole halves otherwise
   const int rb = (pr.jpos && S > 0) ? std::min(32, N / 2) : std::min(N, 256);
+  // store boxes of the dual-buffer variant (TMA stores): whole halves for the
+  // inverse, 32 rows for the forward pass, whose pruned tiles store the live
+  // rows only; both divide N
+  const int rbo = S > 0 ? std::min(N, 256) : std::min(N, 32);
   const unsigned U = sizeof(R) == 4 ? 1 : 2;
-  FieldMaps maps;
+  FieldMaps maps, omaps;
   for (int q = 0; q < nf; ++q) GB_CHECK(field_map(c, f.p[q], BZ * U, rb, 1, &maps.m[q]));
+  if (DUAL)
+    for (int q = 0; q < nf; ++q) GB_CHECK(field_map(c, f.p[q], BZ * U, rbo, 1, &omaps.m[q]));
   const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
-  kern<<<grid, BZ * T, smem, c->stream>>>(maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf, c->nruns, c->nxh, pr.jpos,
-                                          pr.jneg, rb, pipe_ctl(c));
+  kern<<<grid, BZ * T, smem, c->stream>>>(maps, DUAL ? omaps : maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf,
+                                          c->nruns, c->nxh, pr.jpos, pr.jneg, rb, rbo, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
 }
@@ -520,6 +526,15 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
   const C *tw = (const C *)c->tw_x;
   const int ts = timer_begin(c, KIND == X_C2R ? GHOST_TIMER_X_C2R : (KIND == X_R2C ? GHOST_TIMER_X_R2C : GHOST_TIMER_X_NL));
   if (KIND == X_HD || KIND == X_BOUSS) {
+    // FP32 512-point lines: tiles of 16 z-values (128-byte rows, one CTA of
+    // 512 threads per SM) where nz allows, else BZ
+    if constexpr (sizeof(R) == 4 && NX == 512 && BZ == 8) {
+      if (c->nz % 16 == 0) {
+        GB_CHECK((launch_x_fused<R, NX, KIND, 16, 1>(c, ins, outs, rows)));
+        timer_end(c, ts);
+        return post_launch(c);
+      }
+    }
     GB_CHECK((launch_x_fused<R, NX, KIND, BZ, 2>(c, ins, outs, rows)));
   } else if (KIND == X_C2R && xw_plain_ok(c)) {
     GB_CHECK(launch_xw_c2r(c, in, out));

@@ -492,7 +492,11 @@ template <typename R> struct ZFwdBouss {
 // ====================================================================
 // DUAL: the exchanges alternate between a second buffer of the same size
 // and the tile's own stage buffer, one barrier per exchange and none other
-// than the tile's first (the stage refill is issued after it).
+// than the tile's first (the stage refill is issued after it).  The tile's
+// result then leaves by TMA tensor stores (omaps, boxes of rbo rows) from
+// whichever of the two buffers the last exchange did not use; one thread
+// issues them and, before the next tile's first barrier, waits until they
+// have read shared memory.
 template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
   static constexpr int T = N / E;
   static constexpr int NT = BZ * T;
@@ -504,10 +508,12 @@ template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
 
 template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false>
 __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps,
+                                                             const __grid_constant__ FieldMaps omaps,
                                                              const __grid_constant__ Fields<R> fld,
                                                              const cx<R> *__restrict__ twg, int nz, int ni, int nf,
                                                              int nruns, int nxh, const int *__restrict__ jpos,
-                                                             const int *__restrict__ jneg, int rb, PipeCtl ctl) {
+                                                             const int *__restrict__ jneg, int rb, int rbo,
+                                                             PipeCtl ctl) {
   using C = cx<R>;
   using G = YGeom<R, N, E, BZ, DUAL>;
   constexpr int T = G::T, NT = G::NT;
@@ -581,10 +587,14 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
     const int s = k % STAGES;
     const bool ok = (!ctl.stall || injected_stall_wait(&bars[STAGES], ctl.cap)) &&
                     mbar_wait(&bars[s], (uint32_t)(k / STAGES) & 1u, ctl.cap);
+    // DUAL: the previous tile's stores have read their buffer before anyone
+    // writes it again (this barrier orders every later write)
+    if (DUAL && tid == 0) bulk_wait_read_all();
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
       for (int kk = k; kk < k + STAGES - (DUAL ? 1 : 0); ++kk)
         if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
+      if (DUAL && tid == 0) bulk_wait_all();
       return;
     }
     if constexpr (DUAL) issue(k + STAGES - 1);
@@ -611,19 +621,42 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
       int ph = 1;
       auto buf = dual_buf<C>([sb, xb, l](int idx, int h) -> C & { return (h ? xb : sb)[idx * BZ + l]; }, &ph);
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
+      // the exchanges used xb, sb, xb, ...: the result goes to the buffer the
+      // last one did not use (its last reads came before that exchange's barrier)
+      C *ob = (fft_exchanges<N, E>() % 2 == 1) ? sb : xb;
+#pragma unroll
+      for (int e = 0; e < E; ++e) ob[(t + T * e) * BZ + l] = x[e];
+      fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        // rows written: all of them, or (pruned forward pass) boxes covering
+        // the live rows; the extra rows of a box hold the transform's own
+        // values, in rows nothing reads
+        if (S > 0 || (jp == N && jn == 0)) {
+          for (int r0 = 0; r0 < N; r0 += rbo) tma_store_3d(&omaps.m[tl.f], ob + (size_t)r0 * BZ, tl.zb * BZ * U, r0, tl.i);
+        } else {
+          for (int r0 = 0; r0 < jp; r0 += rbo) tma_store_3d(&omaps.m[tl.f], ob + (size_t)r0 * BZ, tl.zb * BZ * U, r0, tl.i);
+          for (int q = 0; q * rbo < jn; ++q) {
+            const int r0 = N - (q + 1) * rbo;
+            tma_store_3d(&omaps.m[tl.f], ob + (size_t)r0 * BZ, tl.zb * BZ * U, r0, tl.i);
+          }
+        }
+        bulk_commit();
+      }
     } else {
       __syncthreads();  // every read of the stage before the exchanges overwrite it
       auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
-    }
-    C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * tl.i;
+      C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * tl.i;
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int jj = t + T * e;
-      if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
+      for (int e = 0; e < E; ++e) {
+        const int jj = t + T * e;
+        if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
+      }
+      __syncthreads();  // the stage is read before the next refill
     }
-    if constexpr (!DUAL) __syncthreads();  // the stage is read before the next refill
   }
+  if (DUAL && tid == 0) bulk_wait_all();
 }
 
 // ====================================================================
