@@ -137,6 +137,9 @@ SIGNATURES = {
     "ghost_les_run": [P, I, I, D, D, P, P, P, P, P, P],
     "ghost_les_edqnm_last": [P, PD, PD, PD],
     "ghost_evedqnm": [I, I, D, D, PD, D, D, PD, PD, PD],
+    "ghost_evedqnm_hel": [I, I, D, D, PD, PD, D, D, I, PD, PD, PD, PD, PD, PD],
+    "ghost_les_set_helicity": [P, I],
+    "ghost_les_edqnm_last_hel": [P, PD, PD, PD],
     "ghost_phd_run": [P, I, I, D, D, D, P, P, P, P, P, P, P, P],
     "ghost_phaseshift": [P, P, D, D],
     "ghost_vector3": [P, P, P, P, P, P, P, P, P, P],

@@ -22,6 +22,7 @@ using namespace gb;
 namespace les {
 
 constexpr int RED_ENERGY_KIND = 0;
+constexpr int RED_HELICITY_KIND = 3;  // the reduction kind of spectrumc's helicity spectrum (ops.cuh RED_HELICITY)
 
 // ---------------------------------------------------------------------
 // kernels
@@ -143,24 +144,40 @@ __global__ void tau_force_kernel(KParams<R> kp, Spec6<R> T, Spec3<R> f, Spec3w<R
 // EDQNM eddy viscosity as a force: o_a = f_a - tve(ki) kk2 v_a with
 // ki = int(sqrt(kk2) + 0.501) (include/edqnmhd_rkstep2.f90:45-56 writes
 // (nu + tve(ki)) times the Laplacian); tve 1-based in GHOST, tve[ki-1] here.
+// With tvh (heli = 1) the helicity eddy diffusivity adds tvh(ki) w_a, w =
+// curl v formed as rotor3 does (:25-27, the C5, C6, C19 of the update).
 template <typename R>
 __global__ void eddy_force_kernel(KParams<R> kp, Spec3<R> v, Spec3<R> f, Spec3w<R> o, const double *__restrict__ tve,
-                                  int ntve, size_t total) {
+                                  const double *__restrict__ tvh, int ntve, size_t total) {
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
     const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
     const R kn2 = kn2_of(kp, i, j, k);
-    R nut = 0, kk2 = 0;
+    R nut = 0, kk2 = 0, nuh = 0;
     if (kn2 <= kp.kmax && kn2 >= kp.tiny) {
       kk2 = kk2_of(kp, i, j, k);
       const int ki = (int)(sqrt(kk2) + (R)0.501f);
-      nut = (ki >= 1 && ki <= ntve) ? (R)tve[ki - 1] : (R)0;
+      const bool in = ki >= 1 && ki <= ntve;
+      nut = in ? (R)tve[ki - 1] : (R)0;
+      nuh = (in && tvh) ? (R)tvh[ki - 1] : (R)0;
+    }
+    const cx<R> vx = v.p[0][p], vy = v.p[1][p], vz = v.p[2][p];
+    cx<R> w[3] = {};
+    if (nuh != (R)0) {
+      const R kx = kx_of(kp, i), ky = ky_of(kp, j), kz = kz_of(kp, k);
+      w[0] = mk((-ky * vz.y) - (-kz * vy.y), (ky * vz.x) - (kz * vy.x));
+      w[1] = mk((-kz * vx.y) - (-kx * vz.y), (kz * vx.x) - (kx * vz.x));
+      w[2] = mk((-kx * vy.y) - (-ky * vx.y), (kx * vy.x) - (ky * vx.x));
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const cx<R> u = v.p[a][p];
+      const cx<R> u = a == 0 ? vx : (a == 1 ? vy : vz);
       cx<R> r;
       r.x = -(nut * kk2) * u.x;
       r.y = -(nut * kk2) * u.y;
+      if (nuh != (R)0) {
+        r.x += nuh * w[a].x;
+        r.y += nuh * w[a].y;
+      }
       if (f.p[a]) {
         r.x += f.p[a][p].x;
         r.y += f.p[a][p].y;
@@ -218,8 +235,8 @@ __device__ static void vc_vcorr_general(double kx, double ky, double kz, double 
 
 /* One mode.  zx/zy/zz: the wavenumber component is zero (index 1 in the
  * Fortran).  kx..kz and kk2 are the GP tables; E and H as above. */
-__device__ static void vc_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double tinyf,
-                         double *v) {
+__device__ static void vc_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double dH,
+                         double tinyf, double *v) {
   const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
   double cx, sx, tx, cy, sy, ty, cz, sz, tz;
   if (!zx && !zy && !zz) {  /* vcorr_xnynzn: vz from the divergence */
@@ -234,7 +251,8 @@ __device__ static void vc_vcorr_mode(int zx, int zy, int zz, double kx, double k
   }
   const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] + v[4] * v[4] + v[5] * v[5];
   const double w2 = kz * (v[0] * v[3] - v[1] * v[2]) + ky * (v[4] * v[1] - v[5] * v[0]) + kx * (v[2] * v[5] - v[3] * v[4]);
-  const double H = w2;
+  // heli = 1 targets H = w2 + thpq(km) dt hf / hold(km) (:536-540): dH
+  const double H = w2 + dH;
   const double eps = (!zx && !zy && zz) ? tinyf : 0.;  /* only vcorr_xnynz0 pads the moduli */
   if (zx && zy) {            /* x, y only; kz != 0 */
     vc_phase(v[0], v[1], 0., &cx, &sx, &tx);
@@ -432,21 +450,34 @@ __device__ static void vc_vcorr_general(double kx, double ky, double kz, double 
 }
 
 
-// Eden of include/edqnmhd_rkstep2.f90:8-10: (|vx|^2+|vy|^2+|vz|^2)/n^6 per mode
+// Eden of include/edqnmhd_rkstep2.f90:8-10: (|vx|^2+|vy|^2+|vz|^2)/n^6 per
+// mode; with hf (heli = 1) also Hden of :11-17, 2/n^6 times
+// kz (Re vx Im vy - Re vy Im vx) + ky (Re vz Im vx - Re vx Im vz)
+// + kx (Re vy Im vz - Re vz Im vy)
 template <typename R>
-__global__ void eden_kernel(Spec3<R> v, R *__restrict__ ef, size_t total, R rmp) {
+__global__ void eden_kernel(KParams<R> kp, Spec3<R> v, R *__restrict__ ef, R *__restrict__ hf, size_t total, R rmp) {
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
     const cx<R> a = v.p[0][p], b = v.p[1][p], c = v.p[2][p];
     ef[p] = (a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + c.x * c.x + c.y * c.y) * rmp;
+    if (hf) {
+      const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
+      const R t1 = kz_of(kp, k) * (a.x * b.y - b.x * a.y);
+      const R t2 = ky_of(kp, j) * (c.x * a.y - a.x * c.y);
+      const R t3 = kx_of(kp, i) * (b.x * c.y - c.x * b.y);
+      hf[p] = (R)2 * rmp * (t1 + t2 + t3);
+    }
   }
 }
 
 // vcorrect over every resolved mode but the origin: tepq and eold are the
 // shell arrays of the substep's start (1-based shells stored at k-1), ef its
 // Eden, dt the substep's dt/o
+// heli = 1 also reads hf (Hden of the substep's start), thpq and hold.
 template <typename R>
 __global__ void vcorrect_kernel(KParams<R> kp, Spec3w<R> v, const R *__restrict__ ef, const double *__restrict__ tepq,
-                                const double *__restrict__ eold, int nshell, R dt, R tinyf, R norm, size_t total) {
+                                const double *__restrict__ eold, const R *__restrict__ hf,
+                                const double *__restrict__ thpq, const double *__restrict__ hold, int hel, int nshell,
+                                R dt, R tinyf, R norm, size_t total) {
   const double inorm = 1. / (double)norm;
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
     const int k = (int)(p % kp.nz), j = (int)((p / kp.nz) % kp.ny), i = (int)(p / ((size_t)kp.nz * kp.ny));
@@ -473,7 +504,8 @@ __global__ void vcorrect_kernel(KParams<R> kp, Spec3w<R> v, const R *__restrict_
     }
     const double v2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2] + u[3] * u[3] + u[4] * u[4] + u[5] * u[5];
     const double E = v2 + 2.0 * tepq[km - 1] * (double)dt * (double)ef[p] / eold[km - 1];
-    vc_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)kk2, E, (double)tinyf, w);
+    const double dH = hel == 1 ? thpq[km - 1] * (double)dt * (double)hf[p] / hold[km - 1] : 0.0;
+    vc_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)kk2, E, dH, (double)tinyf, w);
     cx<R> o;
     o.x = (R)w[0] * norm; o.y = (R)w[1] * norm; v.p[0][p] = o;
     o.x = (R)w[2] * norm; o.y = (R)w[3] * norm; v.p[1][p] = o;
@@ -621,6 +653,65 @@ __host__ __device__ void cusp_kp(int k, int p, const double *Ext, const R *mu, R
   *dtepq = st;
 }
 
+// The quadrature of full_cusp (pseudospec3D_edqnm.f90:174-277) for one
+// (k, p), on the halved extrapolations: the sums over q of the terms GHOST
+// subtracts from nut(k) (out[0]) and adds to tepq(k), tvh(k), thpq(k)
+// (out[1..3]).  Every GP product is rounded to GP before it meets a double
+// spectrum value, in GHOST's left-to-right order.
+template <typename R>
+__host__ __device__ void full_cusp_kp(int k, int p, const double *Ext, const double *Hxt, const R *mu, R nu, R t0,
+                                      double *out) {
+  const R kk = (R)k, pp = (R)p, ppi = (R)1 / pp;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const double Ek = Ext[k - 1], Ep = Ext[p - 1], Hk = Hxt[k - 1], Hp = Hxt[p - 1];
+  for (int q = p - k; q <= p; ++q) {
+    if (q == 0) continue;
+    const R qq = (R)q, qqi = (R)1 / qq;
+    R coeff = (R)0.5;
+    if ((qq - (R)0.5) >= (pp - kk) && (qq + (R)0.5) <= pp) coeff = (R)1;
+    const R x = (pp * pp + qq * qq - kk * kk) / ((R)2 * pp * qq);
+    const R y = (kk * kk + qq * qq - pp * pp) / ((R)2 * kk * qq);
+    const R z = (pp * pp + kk * kk - qq * qq) / ((R)2 * pp * kk);
+    const R xyz = x * y + z * z * z, xzy = x * z + y * y * y;
+    const R ym1 = (R)1 - y * y, zm1 = (R)1 - z * z;
+    const double Eq = Ext[q - 1], Hq = Hxt[q - 1];
+    const R tvvkp = (R)((double)(-(qqi * xyz * (pp * pp))) * Eq * Ek);
+    const R tvvpq = (R)((double)(qqi * xyz * (kk * kk)) * Eq * Ep);
+    const R tvvkpsym = (R)((double)(-(ppi * xzy * (qq * qq))) * Ep * Ek);
+    const R tvvpqsym = (R)((double)(ppi * xzy * (kk * kk)) * Eq * Ep);
+    const R twwpq = (R)((double)(-(z * ym1 * kk * kk)) * Hp * Hq / (double)(pp * pp * qq));
+    const R twwkp = (R)((double)(z * ym1) * Hk * Hq * (double)qqi);
+    const R twwpqsym = (R)((double)(-(y * zm1 * kk * kk)) * Hp * Hq / (double)(pp * qq * qq));
+    const R twwkpsym = (R)((double)(y * zm1) * Hk * Hp * (double)ppi);
+    const R tvw = (R)((double)(qqi * xyz * kk * kk) * Eq * Hp + (double)(ppi * xzy * kk * kk) * Hq * Ep -
+                      (double)(qqi * z * ym1 * kk * kk) * Ep * Hq - (double)(ppi * y * zm1 * kk * kk) * Eq * Hp);
+    const R tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+    const R theta = ((R)1 - mexp(-tmp * t0)) / tmp;
+    const R ct = coeff * theta;
+    s0 += (double)(ct * (tvvkp + tvvkpsym)) / ((double)((R)2 * kk * kk) * Ek);
+    s1 += (double)(ct * (tvvpq + tvvpqsym + twwpq + twwpqsym));
+    s2 += (double)(ct * (twwkp + twwkpsym)) / (2.0 * Hk);
+    s3 += (double)(ct * tvw);
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  out[3] = s3;
+}
+
+// full_cusp's halving of the extrapolated spectra (:212-215) and its mu
+// from the halved Ext; false when Ext(kc+1) = 0 (full_cusp returns first).
+template <typename R>
+__host__ __device__ bool full_cusp_prep(R kmax, R kolmo, double *Ext, double *Hxt, R *mu) {
+  const int kc = (int)msqrt(kmax), ktot = 3 * kc;
+  if (Ext[kc] == 0.0) return false;
+  for (int k = 1; k <= ktot; ++k) {
+    Ext[k - 1] = 0.5 * Ext[k - 1];
+    Hxt[k - 1] = 0.5 * Hxt[k - 1];
+  }
+  return cusp_mu<R>(kmax, kolmo, Ext, mu);
+}
+
 // evedqnm with hel = 0 (pseudospec3D_edqnm.f90:24-92), host: the partial
 // sums of each p are added in p order
 template <typename R>
@@ -647,46 +738,127 @@ static void evedqnm(int n, R kmax, R kolmo, const double *Eold, R nu, R time, do
   }
 }
 
-// Device: one thread fits the spectrum and forms mu; then one block per
-// shell k, its threads sharing the p, partial sums combined in thread order.
+// evedqnm with hel (pseudospec3D_edqnm.f90:24-92), host.  hel = 1 fits E
+// over delk - 2 shells and H over delk; full_cusp when both fits have a
+// positive index, cusp when only E's does.  thpq, tvh and Hxt may be null
+// for hel = 0.
+template <typename R>
+static void evedqnm_h(int n, R kmax, R kolmo, const double *Eold, const double *Hold, R nu, R time, int hel,
+                      double *tepq, double *thpq, double *tve, double *tvh, double *Ext, double *Hxt) {
+  if (hel != 1) {
+    evedqnm<R>(n, kmax, kolmo, Eold, nu, time, tepq, tve, Ext);
+    for (int k = 0; k < n / 2 + 1; ++k) {
+      if (thpq) thpq[k] = 0;
+      if (tvh) tvh[k] = 0;
+    }
+    return;
+  }
+  const int kc = (int)msqrt(kmax);
+  const R delk = (R)3 * (R)kc / (R)4;
+  for (int k = 0; k < n / 2 + 1; ++k) tve[k] = tepq[k] = thpq[k] = tvh[k] = 0;
+  R power, ddelta, hpower, hddelta;
+  spec_fit<R>(n, kmax, Eold, delk - (R)2, Ext, &power, &ddelta);
+  spec_fit<R>(n, kmax, Hold, delk, Hxt, &hpower, &hddelta);
+  if (!(power > 0)) return;
+  std::vector<R> mu(3 * kc + 1);
+  if (hpower > 0) {
+    if (!full_cusp_prep<R>(kmax, kolmo, Ext, Hxt, mu.data())) return;
+    for (int k = 1; k <= kc; ++k) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int p = kc + 1; p <= 3 * kc; ++p) {
+        double d[4];
+        full_cusp_kp<R>(k, p, Ext, Hxt, mu.data(), nu, time, d);
+        for (int q = 0; q < 4; ++q) acc[q] += d[q];
+      }
+      tve[k - 1] = -acc[0];
+      tepq[k - 1] = acc[1];
+      tvh[k - 1] = acc[2];
+      thpq[k - 1] = acc[3];
+    }
+  } else {
+    if (!cusp_mu<R>(kmax, kolmo, Ext, mu.data())) return;
+    for (int k = 1; k <= kc; ++k) {
+      double sn = 0.0, st = 0.0;
+      for (int p = kc + 1; p <= 3 * kc; ++p) {
+        double dn, dt;
+        cusp_kp<R>(k, p, Ext, mu.data(), nu, time, &dn, &dt);
+        sn += dn;
+        st += dt;
+      }
+      tve[k - 1] = -sn;
+      tepq[k - 1] = st;
+    }
+  }
+}
+
+// Device: one thread fits the spectra and forms mu (go: 0 no closure, 1
+// cusp, 2 full_cusp); then one block per shell k, its threads sharing the
+// p, partial sums combined in thread order.  Hold, thpq, tvh, Hxt are only
+// touched for hel = 1.
 template <typename R>
 __global__ void __launch_bounds__(128) edqnm_fit_kernel(int n, R kmax, R kolmo, const double *__restrict__ Eold,
-                                                        double *tepq, double *tve, double *Ext, R *mu, int *go) {
+                                                        const double *__restrict__ Hold, int hel, double *tepq,
+                                                        double *thpq, double *tve, double *tvh, double *Ext,
+                                                        double *Hxt, R *mu, int *go) {
   const int nb = n / 2 + 1, kc = (int)msqrt(kmax);
-  for (int k = threadIdx.x; k < nb; k += blockDim.x) tve[k] = tepq[k] = 0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    tve[k] = tepq[k] = 0;
+    if (hel == 1) thpq[k] = tvh[k] = 0;
+  }
   if (threadIdx.x == 0) {
     const R delk = (R)3 * (R)kc / (R)4;
     R power, ddelta;
-    spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
-    *go = (power > 0) && cusp_mu<R>(kmax, kolmo, Ext, mu) ? 1 : 0;
+    if (hel == 1) {
+      R hpower, hddelta;
+      spec_fit<R>(n, kmax, Eold, delk - (R)2, Ext, &power, &ddelta);
+      spec_fit<R>(n, kmax, Hold, delk, Hxt, &hpower, &hddelta);
+      if (!(power > 0))
+        *go = 0;
+      else if (hpower > 0)
+        *go = full_cusp_prep<R>(kmax, kolmo, Ext, Hxt, mu) ? 2 : 0;
+      else
+        *go = cusp_mu<R>(kmax, kolmo, Ext, mu) ? 1 : 0;
+    } else {
+      spec_fit<R>(n, kmax, Eold, delk, Ext, &power, &ddelta);
+      *go = (power > 0) && cusp_mu<R>(kmax, kolmo, Ext, mu) ? 1 : 0;
+    }
   }
 }
 
 template <typename R>
 __global__ void __launch_bounds__(128) edqnm_cusp_kernel(R kmax, const double *__restrict__ Ext,
-                                                         const R *__restrict__ mu, R nu, R t0,
-                                                         const int *__restrict__ go, double *tepq, double *tve) {
-  __shared__ double sn[128], st[128];
+                                                         const double *__restrict__ Hxt, const R *__restrict__ mu,
+                                                         R nu, R t0, const int *__restrict__ go, double *tepq,
+                                                         double *thpq, double *tve, double *tvh) {
+  __shared__ double sh[4][128];
   const int kc = (int)msqrt(kmax), k = blockIdx.x + 1;
-  if (k > kc || *go == 0) return;
-  double an = 0.0, at = 0.0;
+  const int g = *go;
+  if (k > kc || g == 0) return;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int p = kc + 1 + threadIdx.x; p <= 3 * kc; p += blockDim.x) {
-    double dn, dt;
-    cusp_kp<R>(k, p, Ext, mu, nu, t0, &dn, &dt);
-    an += dn;
-    at += dt;
+    if (g == 2) {
+      double d[4];
+      full_cusp_kp<R>(k, p, Ext, Hxt, mu, nu, t0, d);
+      for (int q = 0; q < 4; ++q) acc[q] += d[q];
+    } else {
+      double dn, dt;
+      cusp_kp<R>(k, p, Ext, mu, nu, t0, &dn, &dt);
+      acc[0] += dn;
+      acc[1] += dt;
+    }
   }
-  sn[threadIdx.x] = an;
-  st[threadIdx.x] = at;
+  for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = acc[q];
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int q = 0; q < (int)blockDim.x; ++q) {
-      a += sn[q];
-      b += st[q];
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = 0; t < (int)blockDim.x; ++t)
+      for (int q = 0; q < 4; ++q) a[q] += sh[q][t];
+    tve[k - 1] = -a[0];
+    tepq[k - 1] = a[1];
+    if (g == 2) {
+      tvh[k - 1] = a[2];
+      thpq[k - 1] = a[3];
     }
-    tve[k - 1] = -a;
-    tepq[k - 1] = b;
   }
 }
 
@@ -712,8 +884,12 @@ struct ghost_les {
   float *x = nullptr, *y = nullptr;  // closure inputs / outputs (n^3 rows)
   // EDQNM closure state on the device (n/2+1 shells; Ext 3(n/2+1); mu 3(n/2+1)+1)
   double *tve_dev = nullptr, *tepq_dev = nullptr, *Ek_dev = nullptr, *Ext_dev = nullptr, *mu_dev = nullptr;
-  int *go_dev = nullptr;  // 1 when the fit succeeded and the quadrature runs
+  int *go_dev = nullptr;  // 0: no closure; 1: cusp; 2: full_cusp (heli = 1)
   void *ef = nullptr;      // per-mode energy of the substep's start (vcorrect)
+  // GHOST's heli flag: the helical closure (full_cusp, tvh, vcorrect's helicity)
+  int heli = 0;
+  double *thpq_dev = nullptr, *tvh_dev = nullptr, *Hk_dev = nullptr, *Hxt_dev = nullptr;
+  void *hf = nullptr;      // per-mode helicity of the substep's start (heli = 1)
   // fallback of the learned closure to EDQNM (ghost_les_set_fallback)
   bool fallback = false;
   double blowup = 10.0;
@@ -819,12 +995,16 @@ template <typename R>
 static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
   ghost_ctx *c = L->c;
   const int nb = c->nx / 2 + 1;
+  const int hel = L->heli;
   GB_CHECK(spectrum_dev_async<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek_dev));
-  edqnm_fit_kernel<R><<<1, 128, 0, c->stream>>>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek_dev, L->tepq_dev, L->tve_dev,
-                                                L->Ext_dev, (R *)L->mu_dev, L->go_dev);
+  if (hel == 1) GB_CHECK(spectrum_dev_async<R>(c, RED_HELICITY_KIND, v[0], v[1], v[2], L->Hk_dev));
+  edqnm_fit_kernel<R><<<1, 128, 0, c->stream>>>(c->nx, (R)c->kmax, (R)L->kolmo, L->Ek_dev, L->Hk_dev, hel,
+                                                L->tepq_dev, L->thpq_dev, L->tve_dev, L->tvh_dev, L->Ext_dev,
+                                                L->Hxt_dev, (R *)L->mu_dev, L->go_dev);
   GB_CHECK(post_launch(c));
-  edqnm_cusp_kernel<R><<<nb, 128, 0, c->stream>>>((R)c->kmax, L->Ext_dev, (const R *)L->mu_dev, (R)L->nu_cur,
-                                                  (R)L->t, L->go_dev, L->tepq_dev, L->tve_dev);
+  edqnm_cusp_kernel<R><<<nb, 128, 0, c->stream>>>((R)c->kmax, L->Ext_dev, L->Hxt_dev, (const R *)L->mu_dev,
+                                                  (R)L->nu_cur, (R)L->t, L->go_dev, L->tepq_dev, L->thpq_dev,
+                                                  L->tve_dev, L->tvh_dev);
   GB_CHECK(post_launch(c));
   L->edqnm_done = true;
   Spec3<R> vs, fs;
@@ -834,7 +1014,8 @@ static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *cons
     fs.p[a] = f ? (const cx<R> *)f[a] : nullptr;
     os.p[a] = (cx<R> *)o[a];
   }
-  eddy_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vs, fs, os, L->tve_dev, nb, c->nspec);
+  eddy_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vs, fs, os, L->tve_dev,
+                                                                  hel == 1 ? L->tvh_dev : nullptr, nb, c->nspec);
   return post_launch(c);
 }
 
@@ -900,15 +1081,17 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
     const bool vcorr_step = L->model == GHOST_LES_EDQNM;
     for (int o = ord; o >= 1; --o) {
       GB_CHECK(closure_force_dev<R>(L, v, f, L->force));
+      const int hel = vcorr_step ? L->heli : 0;
       if (vcorr_step) {
-        eden_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(vr, (R *)L->ef, c->nspec, rmp);
+        eden_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vr, (R *)L->ef,
+                                                                hel == 1 ? (R *)L->hf : nullptr, c->nspec, rmp);
         GB_CHECK(post_launch(c));
       }
       GB_CHECK(hd_substep_dev<R>(c, o, dt, nu, v, L->rk, L->force, o == ord ? 1 : 0, !first));
       if (vcorr_step) {
-        vcorrect_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vw, (const R *)L->ef, L->tepq_dev,
-                                                                    L->Ek_dev, nb, (R)dt * ((R)1 / (R)o), tinyf, n3,
-                                                                    c->nspec);
+        vcorrect_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(
+            kparams<R>(c), vw, (const R *)L->ef, L->tepq_dev, L->Ek_dev, (const R *)L->hf, L->thpq_dev, L->Hk_dev, hel,
+            nb, (R)dt * ((R)1 / (R)o), tinyf, n3, c->nspec);
         GB_CHECK(post_launch(c));
       }
       first = false;
@@ -982,6 +1165,11 @@ int ghost_les_create(ghost_ctx *c, int kc, ghost_les **out) {
   if (!st) st = les_alloc(L, sizeof(double) * (3 * nb + 1), (void **)&L->mu_dev);
   if (!st) st = les_alloc(L, sizeof(int), (void **)&L->go_dev);
   if (!st) st = les_alloc(L, c->cbytes, &L->ef);
+  if (!st) st = les_alloc(L, c->cbytes, &L->hf);
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->thpq_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->tvh_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * nb, (void **)&L->Hk_dev);
+  if (!st) st = les_alloc(L, sizeof(double) * 3 * nb, (void **)&L->Hxt_dev);
   for (int q = 0; q < 3 && !st; ++q) st = les_alloc(L, c->cbytes, &L->save[q]);
   if (st) {
     ghost_les_destroy(L);
@@ -1137,6 +1325,45 @@ int ghost_les_edqnm_last(ghost_les *L, double *tve, double *tepq, double *Ek) {
   if (tve) GB_CUDA(cudaMemcpy(tve, L->tve_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
   if (tepq) GB_CUDA(cudaMemcpy(tepq, L->tepq_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
   if (Ek) GB_CUDA(cudaMemcpy(Ek, L->Ek_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  return GHOST_OK;
+}
+
+int ghost_les_set_helicity(ghost_les *L, int heli) {
+  LES_CHECK(L);
+  if (heli != 0 && heli != 1) return fail(GHOST_ERR_ARG, "heli %d not 0 or 1", heli);
+  L->heli = heli;
+  return GHOST_OK;
+}
+
+int ghost_les_edqnm_last_hel(ghost_les *L, double *tvh, double *thpq, double *Hk) {
+  LES_CHECK(L);
+  const int nb = L->c->nx / 2 + 1;
+  if (!L->edqnm_done) return fail(GHOST_ERR_STATE, "no EDQNM evaluation yet");
+  if (L->heli != 1) return fail(GHOST_ERR_STATE, "the helical closure is off (ghost_les_set_helicity)");
+  GB_CUDA(cudaStreamSynchronize(L->c->stream));
+  if (tvh) GB_CUDA(cudaMemcpy(tvh, L->tvh_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (thpq) GB_CUDA(cudaMemcpy(thpq, L->thpq_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  if (Hk) GB_CUDA(cudaMemcpy(Hk, L->Hk_dev, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  return GHOST_OK;
+}
+
+int ghost_evedqnm_hel(int n, int precision, double kmax, double kolmo, const double *Eold, const double *Hold,
+                      double nu, double time, int hel, double *tepq, double *thpq, double *tve, double *tvh,
+                      double *Ext, double *Hxt) {
+  if (!Eold || !tepq || !tve || !Ext) return fail(GHOST_ERR_ARG, "null argument");
+  if (hel != 0 && hel != 1) return fail(GHOST_ERR_ARG, "hel %d not 0 or 1", hel);
+  if (hel == 1 && (!Hold || !thpq || !tvh || !Hxt)) return fail(GHOST_ERR_ARG, "null helicity argument");
+  if (n < 16 || (n & (n - 1))) return fail(GHOST_ERR_SIZE, "n %d", n);
+  const int kc = (int)std::sqrt(kmax);
+  // the energy fit of hel = 1 uses shells kc - (3kc/4 - 2) .. kc
+  if (kc < 4 || kc > n / 2) return fail(GHOST_ERR_ARG, "kmax %g: EDQNM needs 4 <= sqrt(kmax) <= n/2", kmax);
+  if (precision == GHOST_SINGLE)
+    evedqnm_h<float>(n, (float)kmax, (float)kolmo, Eold, Hold, (float)nu, (float)time, hel, tepq, thpq, tve, tvh, Ext,
+                     Hxt);
+  else if (precision == GHOST_DOUBLE)
+    evedqnm_h<double>(n, kmax, kolmo, Eold, Hold, nu, time, hel, tepq, thpq, tve, tvh, Ext, Hxt);
+  else
+    return fail(GHOST_ERR_ARG, "precision %d", precision);
   return GHOST_OK;
 }
 

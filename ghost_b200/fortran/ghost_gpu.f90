@@ -763,6 +763,26 @@
          INTEGER(C_INT), VALUE :: swap
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_evedqnm_hel(n,prec,kmax,kolmo,eold,hold,nu,time,hel,tepq,thpq,tve,tvh,ext,hxt) &
+                BIND(C,name="ghost_evedqnm_hel") RESULT(s)
+         IMPORT :: C_INT, C_DOUBLE
+         INTEGER(C_INT), VALUE :: n, prec, hel
+         REAL(C_DOUBLE), VALUE :: kmax, kolmo, nu, time
+         REAL(C_DOUBLE) :: eold(*), hold(*), tepq(*), thpq(*), tve(*), tvh(*), ext(*), hxt(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_set_helicity(les,heli) BIND(C,name="ghost_les_set_helicity") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: les
+         INTEGER(C_INT), VALUE :: heli
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_les_edqnm_last_hel(les,tvh,thpq,hk) BIND(C,name="ghost_les_edqnm_last_hel") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: les
+         REAL(C_DOUBLE) :: tvh(*), thpq(*), hk(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_evedqnm(n,prec,kmax,kolmo,eold,nu,time,tepq,tve,ext) BIND(C,name="ghost_evedqnm") RESULT(s)
          IMPORT :: C_INT, C_DOUBLE
          INTEGER(C_INT), VALUE :: n, prec

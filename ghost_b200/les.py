@@ -195,6 +195,19 @@ class LES:
         check(self.lib.ghost_les_run(self.h, nsteps, ord, dt, nu, *[self._c(v) for v in (vx, vy, vz, fx, fy, fz)]),
               "ghost_les_run")
 
+    def set_helicity(self, heli: int = 1):
+        """GHOST's heli flag for the EDQNM closure (full_cusp, tvh, helical vcorrect)."""
+        check(self.lib.ghost_les_set_helicity(self.h, int(heli)), "ghost_les_set_helicity")
+
+    def edqnm_last_hel(self):
+        """(tvh, thpq, Hk) of the last helical EDQNM evaluation."""
+        nb = self.n // 2 + 1
+        tvh, thpq, Hk = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        P = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.ghost_les_edqnm_last_hel(self.h, tvh.ctypes.data_as(P), thpq.ctypes.data_as(P),
+                                                Hk.ctypes.data_as(P)), "ghost_les_edqnm_last_hel")
+        return tvh, thpq, Hk
+
     def edqnm_last(self):
         nb = self.n // 2 + 1
         tve, tepq, Ek = np.zeros(nb), np.zeros(nb), np.zeros(nb)
@@ -217,4 +230,20 @@ def evedqnm(n: int, kmax: float, Eold, nu: float, time: float, kolmo: float = 1.
     return tepq, tve, Ext
 
 
-__all__ = ["MLP", "LES", "evedqnm", "MODELS", "NIN", "NHID", "NOUT", "NPARAM"]
+def evedqnm_hel(n: int, kmax: float, Eold, Hold, nu: float, time: float, hel: int = 1, kolmo: float = 1.4,
+                precision: str = "fp64"):
+    """GHOST's evedqnm with its hel flag on the host:
+    (tepq, thpq, tve, tvh, Ext, Hxt)."""
+    lib = _lib.load()
+    nb = n // 2 + 1
+    E = np.ascontiguousarray(Eold, dtype=np.float64)
+    H = np.ascontiguousarray(Hold, dtype=np.float64)
+    out = [np.zeros(nb) for _ in range(4)] + [np.zeros(3 * nb), np.zeros(3 * nb)]
+    P = ctypes.POINTER(ctypes.c_double)
+    code = {"fp32": _lib.GHOST_SINGLE, "fp64": _lib.GHOST_DOUBLE}[precision]
+    check(lib.ghost_evedqnm_hel(n, code, kmax, kolmo, E.ctypes.data_as(P), H.ctypes.data_as(P), nu, time, int(hel),
+                                *[x.ctypes.data_as(P) for x in out]), "ghost_evedqnm_hel")
+    return tuple(out)
+
+
+__all__ = ["MLP", "LES", "evedqnm", "evedqnm_hel", "MODELS", "NIN", "NHID", "NOUT", "NPARAM"]

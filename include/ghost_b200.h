@@ -459,7 +459,7 @@ int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, 
  * arrays of the coarse context unless named fine.  Closures:
  *   GHOST_LES_NONE   no subgrid term;
  *   GHOST_LES_EDQNM  GHOST's EDQNM closure, include/edqnmhd_rkstep2.f90
- *                    with heli = 0: the kinetic spectrum of the current
+ *                    (heli = 0 unless ghost_les_set_helicity): the kinetic spectrum of the current
  *                    velocity gives tve(k) and tepq(k) (evedqnm: spec_fit +
  *                    cusp, pseudo/pseudospec3D_edqnm.f90:24-402), the update
  *                    uses nu + tve(k), and vcorrect (:405-1629) then sets
@@ -517,6 +517,25 @@ int ghost_les_run(ghost_les *les, int nsteps, int ord, double dt, double nu, voi
 /* the last EDQNM evaluation (host arrays of n/2+1, GHOST's 1-based index
  * k stored at k-1); any pointer may be NULL */
 int ghost_les_edqnm_last(ghost_les *les, double *tve, double *tepq, double *Ek);
+/* GHOST's heli flag for the EDQNM closure (include/edqnmhd_rkstep2.f90;
+ * default 0): with heli = 1 the closure also takes the helicity spectrum,
+ * fits E over 3kc/4 - 2 shells and H over 3kc/4, and (when both fits have a
+ * positive index) runs full_cusp (pseudo/pseudospec3D_edqnm.f90:174-277),
+ * which gives the helicity eddy diffusivity tvh(k) and transfer thpq(k);
+ * the update adds tvh(k) curl v and vcorrect sets every mode's helicity to
+ * w2 + thpq(km) dt hf / hold(km) (:536-540) as well as its energy. */
+int ghost_les_set_helicity(ghost_les *les, int heli);
+/* the last helical EDQNM evaluation (host arrays of n/2+1): tvh, thpq and
+ * the helicity spectrum Hk; any pointer may be NULL */
+int ghost_les_edqnm_last_hel(ghost_les *les, double *tvh, double *thpq, double *Hk);
+/* evedqnm(Eold,Hold,nu,time,hel,tepq,thpq,tve,tvh,Ext,Hxt)
+ * (pseudo/pseudospec3D_edqnm.f90:24-92) on the host, GHOST's full
+ * signature: Eold, Hold[n/2+1] -> tepq, thpq, tve, tvh[n/2+1] and the
+ * extrapolations Ext, Hxt[3(n/2+1)] (halved by full_cusp when it runs);
+ * with hel = 0, Hold, thpq, tvh and Hxt may be NULL. */
+int ghost_evedqnm_hel(int n, int precision, double kmax, double kolmo, const double *Eold, const double *Hold,
+                      double nu, double time, int hel, double *tepq, double *thpq, double *tve, double *tvh,
+                      double *Ext, double *Hxt);
 /* evedqnm with heli = 0 on the host: Eold[n/2+1] -> tepq, tve[n/2+1] and
  * the extrapolated spectrum Ext[3(n/2+1)]; precision selects GHOST's GP
  * kind for the fit and quadrature (GHOST_SINGLE or GHOST_DOUBLE) */

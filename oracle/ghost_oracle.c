@@ -1144,6 +1144,88 @@ static void o_cusp(const octx *c, real kolmo, const double *Ext, real nu, real t
   free(mu);
 }
 
+/* full_cusp (:174-277): cusp with helicity.  Ext and Hxt are halved in
+ * place first, as GHOST does.  Every GP product is rounded to GP before it
+ * meets a double spectrum value, in GHOST's left-to-right order. */
+static void o_full_cusp(const octx *c, real kolmo, double *Ext, double *Hxt, real nu, real t0, double *tepq,
+                        double *thpq, double *nut, double *tvh) {
+  real lambda = (real)0.218f * (real)pow(kolmo, (real)1.5);
+  int kc = (int)sqrt(c->kmax), ktot = 3 * kc;
+  if (Ext[kc] == 0.) return;
+  for (int k = 1; k <= ktot; ++k) {
+    Ext[k - 1] = 0.5 * Ext[k - 1];
+    Hxt[k - 1] = 0.5 * Hxt[k - 1];
+  }
+  real *mu = (real *)calloc((size_t)ktot + 1, sizeof(real));
+  real en = 0;
+  for (int k = 1; k <= ktot; ++k) {
+    real tmp = (real)(float)(k * k);
+    en = (real)((double)en + (double)tmp * Ext[k - 1]);
+    mu[k] = lambda * (real)sqrt(en);
+  }
+  for (int k = 1; k <= kc; ++k) {
+    real kk = (real)k;
+    for (int p = kc + 1; p <= ktot; ++p) {
+      real pp = (real)p, ppi = (real)1.0 / pp;
+      for (int q = p - k; q <= p; ++q) {
+        if (q == 0) continue;
+        real qq = (real)q, qqi = (real)1.0 / qq;
+        real coeff = (real)0.5;
+        if ((qq - (real)0.5) >= (pp - kk) && (qq + (real)0.5) <= pp) coeff = (real)1.0;
+        real x = (pp * pp + qq * qq - kk * kk) / ((real)2.0 * pp * qq);
+        real y = (kk * kk + qq * qq - pp * pp) / ((real)2.0 * kk * qq);
+        real z = (pp * pp + kk * kk - qq * qq) / ((real)2.0 * pp * kk);
+        real xyz = x * y + z * z * z, xzy = x * z + y * y * y;
+        real ym1 = (real)1. - y * y, zm1 = (real)1. - z * z;
+        double Eq = Ext[q - 1], Ek = Ext[k - 1], Ep = Ext[p - 1];
+        double Hq = Hxt[q - 1], Hk = Hxt[k - 1], Hp = Hxt[p - 1];
+        real tvvkp = (real)((double)(-(qqi * xyz * (pp * pp))) * Eq * Ek);
+        real tvvpq = (real)((double)(qqi * xyz * (kk * kk)) * Eq * Ep);
+        real tvvkpsym = (real)((double)(-(ppi * xzy * (qq * qq))) * Ep * Ek);
+        real tvvpqsym = (real)((double)(ppi * xzy * (kk * kk)) * Eq * Ep);
+        real twwpq = (real)((double)(-(z * ym1 * kk * kk)) * Hp * Hq / (double)(pp * pp * qq));
+        real twwkp = (real)((double)(z * ym1) * Hk * Hq * (double)qqi);
+        real twwpqsym = (real)((double)(-(y * zm1 * kk * kk)) * Hp * Hq / (double)(pp * qq * qq));
+        real twwkpsym = (real)((double)(y * zm1) * Hk * Hp * (double)ppi);
+        real tvw = (real)((double)(qqi * xyz * kk * kk) * Eq * Hp + (double)(ppi * xzy * kk * kk) * Hq * Ep -
+                          (double)(qqi * z * ym1 * kk * kk) * Ep * Hq - (double)(ppi * y * zm1 * kk * kk) * Eq * Hp);
+        real tmp = mu[k] + mu[p] + mu[q] + nu * (kk * kk + pp * pp + qq * qq);
+        real theta = ((real)1.0 - (real)exp(-tmp * t0)) / tmp;
+        real ct = coeff * theta;
+        nut[k - 1] = nut[k - 1] - (double)(ct * (tvvkp + tvvkpsym)) / ((double)((real)2. * kk * kk) * Ek);
+        tepq[k - 1] = tepq[k - 1] + (double)(ct * (tvvpq + tvvpqsym + twwpq + twwpqsym));
+        tvh[k - 1] = tvh[k - 1] + (double)(ct * (twwkp + twwkpsym)) / (2. * Hk);
+        thpq[k - 1] = thpq[k - 1] + (double)(ct * tvw);
+      }
+    }
+  }
+  free(mu);
+}
+
+/* evedqnm (:24-92): Eold, Hold[n/2+1] -> tepq, thpq, tve, tvh[n/2+1] and
+ * Ext, Hxt[3(n/2+1)].  hel = 1 fits E over delk - 2 shells and H over delk,
+ * then full_cusp when both fits have positive index, else cusp. */
+void o_evedqnm_h(const octx *c, double kolmo, const double *Eold, const double *Hold, double nu, double time, int hel,
+                 double *tepq, double *thpq, double *tve, double *tvh, double *Ext, double *Hxt) {
+  int n = c->nx, kc = (int)sqrt(c->kmax);
+  real delk = (real)3. * (real)kc / (real)4.;
+  for (int k = 0; k < n / 2 + 1; ++k) tve[k] = tvh[k] = tepq[k] = thpq[k] = 0.;
+  real power, ddelta, hpower, hddelta;
+  if (hel == 1) {
+    o_spec_fit(c, Eold, delk - (real)2, Ext, &power, &ddelta);
+    o_spec_fit(c, Hold, delk, Hxt, &hpower, &hddelta);
+    if (power > 0) {
+      if (hpower > 0)
+        o_full_cusp(c, (real)kolmo, Ext, Hxt, (real)nu, (real)time, tepq, thpq, tve, tvh);
+      else
+        o_cusp(c, (real)kolmo, Ext, (real)nu, (real)time, tepq, tve);
+    }
+  } else {
+    o_spec_fit(c, Eold, delk, Ext, &power, &ddelta);
+    if (power > 0) o_cusp(c, (real)kolmo, Ext, (real)nu, (real)time, tepq, tve);
+  }
+}
+
 /* evedqnm (:24-92) with hel = 0: Eold[n/2+1] -> tepq, tve[n/2+1], Ext[3(n/2+1)] */
 void o_evedqnm(const octx *c, double kolmo, const double *Eold, double nu, double time, double *tepq, double *tve,
                double *Ext) {
@@ -1159,6 +1241,8 @@ void o_evedqnm(const octx *c, double kolmo, const double *Eold, double nu, doubl
  * the update of :41-58 with (nu + tve(ki)) times the Laplacian */
 void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const double *tepq, const double *eold,
                 double dt_d);
+void o_vcorrect_h(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const real *hf, const double *tepq,
+                  const double *thpq, const double *eold, const double *hold, double dt_d, int hel);
 
 void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const double *tve, const double *tepq,
                      const double *eold, int vcorr, cplx *vx, cplx *vy, cplx *vz, const cplx *C1, const cplx *C2,
@@ -1206,6 +1290,102 @@ void o_edqnm_rkstep2(const octx *c, int o, double dt_d, double nu_d, const doubl
     o_vcorrect(c, vx, vy, vz, ef, tepq, eold, (double)(dt * rmp));
     free(ef);
   }
+}
+
+/* include/edqnmhd_rkstep2.f90 with heli (:1-63): Eden and Hden of the
+ * velocity before the update, prodre3 and nonlhd3, w = curl v (rotor3), the
+ * update C + dt ((nu + tve(ki)) lap v + NL + tvh(ki) w + f) / o on the kept
+ * modes, then vcorrect with hel (when vcorr).  tvh and thpq are zero arrays
+ * for heli = 0, which leaves the update of o_edqnm_rkstep2 bit for bit. */
+void o_edqnm_rkstep2_h(const octx *c, int o, double dt_d, double nu_d, int hel, const double *tve, const double *tvh,
+                       const double *tepq, const double *thpq, const double *eold, const double *hold, int vcorr,
+                       cplx *vx, cplx *vy, cplx *vz, const cplx *C1, const cplx *C2, const cplx *C3, const cplx *fx,
+                       const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  real dt = (real)dt_d, nu = (real)nu_d;
+  real *ef = NULL, *hf = NULL;
+  if (vcorr) {
+    const real rmp = (real)1 / ((real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx * (real)c->nx);
+    ef = (real *)malloc(sizeof(real) * n);
+    hf = (real *)malloc(sizeof(real) * n);
+    for (int i = 0; i < c->nxh; ++i)
+      for (int j = 0; j < c->ny; ++j)
+        for (int k = 0; k < c->nz; ++k) {
+          const size_t p = SIDX(c, k, j, i);
+          ef[p] = (cabs2(vx[p]) + cabs2(vy[p]) + cabs2(vz[p])) * rmp;
+          real a = c->kz[k] * (vx[p].re * vy[p].im - vy[p].re * vx[p].im);
+          real b = c->ky[j] * (vz[p].re * vx[p].im - vx[p].re * vz[p].im);
+          real d = c->kx[i] * (vy[p].re * vz[p].im - vz[p].re * vy[p].im);
+          hf[p] = (real)2 * rmp * (a + b + d);
+        }
+  }
+  cplx *C4 = (cplx *)malloc(sizeof(cplx) * n), *C5 = (cplx *)malloc(sizeof(cplx) * n),
+       *C6 = (cplx *)malloc(sizeof(cplx) * n), *C7 = (cplx *)malloc(sizeof(cplx) * n),
+       *C8 = (cplx *)malloc(sizeof(cplx) * n), *C19 = (cplx *)malloc(sizeof(cplx) * n);
+  o_prodre3(c, vx, vy, vz, C4, C5, C6);
+  o_nonlhd3(c, C4, C5, C6, C7, 1);
+  o_nonlhd3(c, C4, C5, C6, C8, 2);
+  o_nonlhd3(c, C4, C5, C6, C4, 3);
+  o_rotor3(c, vy, vz, C5, 1);
+  o_rotor3(c, vx, vz, C6, 2);
+  o_rotor3(c, vx, vy, C19, 3);
+  o_laplak3(c, vx, vx);
+  o_laplak3(c, vy, vy);
+  o_laplak3(c, vz, vz);
+  real rmp = (real)1. / (real)o;
+#pragma omp parallel for schedule(static)
+  for (size_t p = 0; p < n; ++p) {
+    if (c->kn2[p] <= c->kmax && c->kn2[p] >= c->tiny) {
+      int ki = (int)((real)sqrt(c->kk2[p]) + (real)0.501f);
+      double nt = (double)nu + tve[ki - 1], th = tvh[ki - 1];
+      cplx *v[3] = {&vx[p], &vy[p], &vz[p]};
+      const cplx *C[3] = {&C1[p], &C2[p], &C3[p]}, *N[3] = {&C7[p], &C8[p], &C4[p]}, *F[3] = {&fx[p], &fy[p], &fz[p]};
+      const cplx *W[3] = {&C5[p], &C6[p], &C19[p]};
+      for (int a = 0; a < 3; ++a) {
+        double re = (double)C[a]->re + (double)dt * (nt * v[a]->re + N[a]->re + th * W[a]->re + F[a]->re) * (double)rmp;
+        double im = (double)C[a]->im + (double)dt * (nt * v[a]->im + N[a]->im + th * W[a]->im + F[a]->im) * (double)rmp;
+        v[a]->re = (real)re;
+        v[a]->im = (real)im;
+      }
+    } else {
+      cplx z = {0, 0};
+      vx[p] = z; vy[p] = z; vz[p] = z;
+    }
+  }
+  free(C4); free(C5); free(C6); free(C7); free(C8); free(C19);
+  if (vcorr) {
+    o_vcorrect_h(c, vx, vy, vz, ef, hf, tepq, thpq, eold, hold, (double)(dt * rmp), hel);
+    free(ef);
+    free(hf);
+  }
+}
+
+/* nsteps RK steps of the EDQNM LES with heli: per substep spectrumc (E and,
+ * for hel = 1, H) -> evedqnm at t0 + (step index) dt -> edqnm_rkstep2 */
+void o_edqnm_run_h(const octx *c, int nsteps, int ord, double dt, double nu, double kolmo, double t0, int vcorr,
+                   int hel, cplx *vx, cplx *vy, cplx *vz, const cplx *fx, const cplx *fy, const cplx *fz) {
+  size_t n = c->nspec;
+  int nb = c->nx / 2 + 1;
+  cplx *C1 = (cplx *)malloc(sizeof(cplx) * n), *C2 = (cplx *)malloc(sizeof(cplx) * n),
+       *C3 = (cplx *)malloc(sizeof(cplx) * n), *zf = NULL;
+  double *Ek = (double *)calloc(nb, sizeof(double)), *Hk = (double *)calloc(nb, sizeof(double)),
+         *tepq = (double *)calloc(nb, sizeof(double)), *thpq = (double *)calloc(nb, sizeof(double)),
+         *tve = (double *)calloc(nb, sizeof(double)), *tvh = (double *)calloc(nb, sizeof(double)),
+         *Ext = (double *)calloc(3 * nb, sizeof(double)), *Hxt = (double *)calloc(3 * nb, sizeof(double));
+  if (!fx) {
+    zf = (cplx *)calloc(n, sizeof(cplx));
+    fx = fy = fz = zf;
+  }
+  for (int t = 0; t < nsteps; ++t) {
+    o_hd_rkstep1(c, vx, vy, vz, C1, C2, C3);
+    for (int o = ord; o >= 1; --o) {
+      o_spectrumc(c, vx, vy, vz, 1, hel, Ek, Hk);
+      o_evedqnm_h(c, kolmo, Ek, Hk, nu, t0 + t * dt, hel, tepq, thpq, tve, tvh, Ext, Hxt);
+      o_edqnm_rkstep2_h(c, o, dt, nu, hel, tve, tvh, tepq, thpq, Ek, Hk, vcorr, vx, vy, vz, C1, C2, C3, fx, fy, fz);
+    }
+  }
+  free(C1); free(C2); free(C3); free(zf); free(Ek); free(Hk); free(tepq); free(thpq); free(tve); free(tvh);
+  free(Ext); free(Hxt);
 }
 
 /* nsteps RK steps of the EDQNM LES: per substep spectrumc -> evedqnm at
@@ -1302,8 +1482,8 @@ static void o_vcorr_general(double kx, double ky, double kz, double kk2, double 
 
 /* One mode.  zx/zy/zz: the wavenumber component is zero (index 1 in the
  * Fortran).  kx..kz and kk2 are the GP tables; E and H as above. */
-static void o_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double tinyf,
-                         double *v) {
+static void o_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz, double kk2, double E, double dH,
+                         double tinyf, double *v) {
   const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
   double cx, sx, tx, cy, sy, ty, cz, sz, tz;
   if (!zx && !zy && !zz) {  /* vcorr_xnynzn: vz from the divergence */
@@ -1318,7 +1498,8 @@ static void o_vcorr_mode(int zx, int zy, int zz, double kx, double ky, double kz
   }
   const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] + v[4] * v[4] + v[5] * v[5];
   const double w2 = kz * (v[0] * v[3] - v[1] * v[2]) + ky * (v[4] * v[1] - v[5] * v[0]) + kx * (v[2] * v[5] - v[3] * v[4]);
-  const double H = w2;
+  /* heli = 1: H = w2 + thpq(km) dt hf / hold(km), the caller's dH (:536-540) */
+  const double H = w2 + dH;
   const double eps = (!zx && !zy && zz) ? tinyf : 0.;  /* only vcorr_xnynz0 pads the moduli */
   if (zx && zy) {            /* x, y only; kz != 0 */
     o_phase(v[0], v[1], 0., &cx, &sx, &tx);
@@ -1518,8 +1699,17 @@ static void o_vcorr_general(double kx, double ky, double kz, double kk2, double 
 /* vcorrect over every resolved mode but the origin; ef: Eden of the
  * substep's start, (|vx|^2+|vy|^2+|vz|^2)/n^6 per mode (edqnmhd_rkstep2.f90:
  * 8-10); tepq, eold: 0-based copies of the shell arrays; dt: dt/o. */
+void o_vcorrect_h(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const real *hf, const double *tepq,
+                  const double *thpq, const double *eold, const double *hold, double dt_d, int hel);
 void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const double *tepq, const double *eold,
                 double dt_d) {
+  o_vcorrect_h(c, vx, vy, vz, ef, NULL, tepq, NULL, eold, NULL, dt_d, 0);
+}
+
+/* vcorrect (:405-470) with hel: hf is Hden of the substep's start, thpq and
+ * hold the helicity transfer and spectrum (hel = 1 only) */
+void o_vcorrect_h(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, const real *hf, const double *tepq,
+                  const double *thpq, const double *eold, const double *hold, double dt_d, int hel) {
   const real dt = (real)dt_d;
   const real norm = (real)c->nx * (real)c->nx * (real)c->nx;
   const double inorm = 1. / (double)norm;
@@ -1552,7 +1742,8 @@ void o_vcorrect(const octx *c, cplx *vx, cplx *vy, cplx *vz, const real *ef, con
         }
         const double v2 = vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2] + vv[3] * vv[3] + vv[4] * vv[4] + vv[5] * vv[5];
         const double E = v2 + 2.0 * tepq[km - 1] * (double)dt * (double)ef[p] / eold[km - 1];
-        o_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)c->kk2[p], E, (double)tinyf, v);
+        const double dH = hel == 1 ? thpq[km - 1] * (double)dt * (double)hf[p] / hold[km - 1] : 0.0;
+        o_vcorr_mode(zx, zy, zz, kxv, kyv, kzv, (double)c->kk2[p], E, dH, (double)tinyf, v);
         vx[p].re = (real)v[0] * norm; vx[p].im = (real)v[1] * norm;
         vy[p].re = (real)v[2] * norm; vy[p].im = (real)v[3] * norm;
         vz[p].re = (real)v[4] * norm; vz[p].im = (real)v[5] * norm;

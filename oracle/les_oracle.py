@@ -69,10 +69,33 @@ def tau_force(co, tau, tau_scale=1.0, f=None):
     return out
 
 
-def eddy_force(co, v, tve, f=None):
-    """o = f - tve(ki) kk2 v with ki = int(sqrt(kk2) + 0.501) on tiny <= kn2 <= kmax."""
+def eddy_force(co, v, tve, f=None, tvh=None):
+    """o = f - tve(ki) kk2 v (+ tvh(ki) curl v, the helical closure of
+    include/edqnmhd_rkstep2.f90:45-56) with ki = int(sqrt(kk2) + 0.501) on
+    tiny <= kn2 <= kmax."""
     _, _, _, kn2, kk2 = co.tables()
     mask = (kn2 <= co.kmax) & (kn2 >= co.tiny)
     ki = (np.sqrt(kk2) + np.float32(0.501)).astype(int)
-    nut = np.where(mask & (ki >= 1) & (ki <= len(tve)), np.asarray(tve)[np.clip(ki - 1, 0, len(tve) - 1)], 0.0)
-    return [-(nut * np.where(mask, kk2, 0)) * x + (f[a] if f is not None else 0) for a, x in enumerate(v)]
+    pick = lambda t: np.where(mask & (ki >= 1) & (ki <= len(t)), np.asarray(t)[np.clip(ki - 1, 0, len(t) - 1)], 0.0)
+    nut = pick(tve)
+    out = [-(nut * np.where(mask, kk2, 0)) * x + (f[a] if f is not None else 0) for a, x in enumerate(v)]
+    if tvh is not None:
+        nuh = pick(tvh)
+        w = [co.rotor3(v[1], v[2], 1), co.rotor3(v[0], v[2], 2), co.rotor3(v[0], v[1], 3)]
+        out = [o + nuh * x for o, x in zip(out, w)]
+    return out
+
+
+def helical(co, v, sign=1):
+    """The helical part of a solenoidal spectral field: (v + sign i k x v / |k|) / 2,
+    a field of helicity density of one sign (zero at k = 0)."""
+    kx, ky, kz, _, kk2 = co.tables()
+    kx = kx[:co.nxh][:, None, None]
+    ky = ky[None, :, None]
+    kz = kz[None, None, :]
+    kn = np.sqrt(np.where(kk2 > 0, kk2, 1.0))
+    cx = 1j * (ky * v[2] - kz * v[1])
+    cy = 1j * (kz * v[0] - kx * v[2])
+    cz = 1j * (kx * v[1] - ky * v[0])
+    h = [0.5 * (a + sign * b / kn) for a, b in zip(v, (cx, cy, cz))]
+    return [np.where(kk2 > 0, x, 0).astype(co.cdt) for x in h]

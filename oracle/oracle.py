@@ -92,6 +92,8 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_evedqnm": (None, [P, D, P, D, D, P, P, P]),
         "o_edqnm_rkstep2": (None, [P, I, D, D, P, P, P, I] + [P] * 9),
         "o_edqnm_run": (None, [P, I, I, D, D, D, D, I] + [P] * 6),
+        "o_evedqnm_h": (None, [P, D, P, P, D, D, I, P, P, P, P, P, P]),
+        "o_edqnm_run_h": (None, [P, I, I, D, D, D, D, I, I] + [P] * 6),
         "o_vcorrect": (None, [P, P, P, P, P, P, P, D]),
         "o_les_truncate": (None, [P, P, P, P, I]),
         "o_ctx_set_kmax": (None, [P, D]),
@@ -409,11 +411,25 @@ class Oracle:
         self.lib.o_evedqnm(self.h, kolmo, _ptr(E), nu, time, _ptr(tepq), _ptr(tve), _ptr(Ext))
         return tepq, tve, Ext
 
-    def edqnm_run(self, nsteps, ord, dt, nu, v, f=None, kolmo=1.4, t0=0.0, vcorrect=True):
+    def evedqnm_h(self, Eold, Hold, nu, time, hel=1, kolmo=1.4):
+        """evedqnm with helicity (pseudospec3D_edqnm.f90:24-92): returns
+        tepq, thpq, tve, tvh [n/2+1] and the extrapolated Ext, Hxt [3(n/2+1)]."""
+        nb = self.nx // 2 + 1
+        E = np.ascontiguousarray(Eold, dtype=np.float64)
+        H = np.ascontiguousarray(Hold, dtype=np.float64)
+        out = [np.zeros(nb) for _ in range(4)] + [np.zeros(3 * nb), np.zeros(3 * nb)]
+        self.lib.o_evedqnm_h(self.h, kolmo, _ptr(E), _ptr(H), nu, time, int(hel), *[_ptr(x) for x in out])
+        return tuple(out)
+
+    def edqnm_run(self, nsteps, ord, dt, nu, v, f=None, kolmo=1.4, t0=0.0, vcorrect=True, hel=0):
         v = [self._c(x).copy() for x in v]
         fk = None if f is None else [self._c(x) for x in f]
-        self.lib.o_edqnm_run(self.h, nsteps, ord, dt, nu, kolmo, t0, int(vcorrect), *[_ptr(x) for x in v],
-                             *([None] * 3 if fk is None else [_ptr(x) for x in fk]))
+        if hel:
+            self.lib.o_edqnm_run_h(self.h, nsteps, ord, dt, nu, kolmo, t0, int(vcorrect), int(hel),
+                                   *[_ptr(x) for x in v], *([None] * 3 if fk is None else [_ptr(x) for x in fk]))
+        else:
+            self.lib.o_edqnm_run(self.h, nsteps, ord, dt, nu, kolmo, t0, int(vcorrect), *[_ptr(x) for x in v],
+                                 *([None] * 3 if fk is None else [_ptr(x) for x in fk]))
         return v
 
     def vcorrect(self, v, ef, tepq, eold, dt):

@@ -98,6 +98,52 @@ def test_edqnm_les_run():
     assert rel_l2([to_host(a) for a in V], ref) <= 1e-11
 
 
+def test_helical_edqnm_closure_force():
+    """heli = 1 on a maximally helical field: the helicity spectrum joins
+    the fit, full_cusp gives tvh and thpq, and the force adds tvh(k) curl v."""
+    fo, co, gf, gc, les = setup("fp64")
+    v = LO.helical(co, kolmogorov_field(co, 8, 10), +1)
+    les.set_model("edqnm", kolmo=1.4)
+    les.set_helicity(1)
+    les.set_time(2.0)
+    F = les.closure_force(1e-3, *[to_dev(a) for a in v])
+    Ek, Hk = co.spectrumc(*v, 1, 1)
+    tepq, thpq, tve, tvh, _, _ = co.evedqnm_h(Ek, Hk, 1e-3, 2.0, hel=1)
+    assert np.max(tve) > 0 and np.any(tvh != 0) and np.any(thpq != 0)  # full_cusp ran
+    tve_g, tepq_g, Ek_g = les.edqnm_last()
+    tvh_g, thpq_g, Hk_g = les.edqnm_last_hel()
+    assert rel_l2(Hk_g, Hk) <= 1e-13
+    for a, b in ((tve_g, tve), (tepq_g, tepq), (tvh_g, tvh), (thpq_g, thpq)):
+        assert rel_l2(a, b) <= 1e-12
+    assert rel_l2([to_host(a) for a in F], LO.eddy_force(co, v, tve, tvh=tvh)) <= 1e-12
+
+
+@pytest.mark.parametrize("shape_seed", [12, 13])
+def test_helical_edqnm_les_run(shape_seed):
+    """Three RK2 steps of the LES with GHOST's helical EDQNM closure
+    (full_cusp, the tvh curl v term, vcorrect's helicity target) against the
+    oracle's restatement of edqnmhd_rkstep2 with heli = 1."""
+    fo, co, gf, gc, les = setup("fp64")
+    # positive helicity in every shell but away from the maximal limit, where
+    # vcorrect's sqrt(1 - H^2 / (k^2 E^2 / 4)) vanishes and rounding dominates
+    u = kolmogorov_field(co, shape_seed, 10)
+    v = [a + 0.4 * b for a, b in zip(LO.helical(co, u, +1), LO.helical(co, u, -1))]
+    _, Hk = co.spectrumc(*v, 1, 1)
+    assert np.all(Hk[:10] > 0)
+    f, _ = co.random_solenoidal(10, 2.0, 3.0, 0, 1.0)
+    f = LO.helical(co, f, +1)
+    les.set_model("edqnm")
+    les.set_helicity(1)
+    les.set_time(1.0)
+    V = [to_dev(a) for a in v]
+    les.run(3, 2, 1e-3, 1e-3, *V, *[to_dev(a) for a in f])
+    ref = co.edqnm_run(3, 2, 1e-3, 1e-3, v, f, t0=1.0, hel=1)
+    assert rel_l2([to_host(a) for a in V], ref) <= 1e-11
+    # the helical closure changed the run
+    plain = co.edqnm_run(3, 2, 1e-3, 1e-3, v, f, t0=1.0, hel=0)
+    assert rel_l2(ref, plain) > 1e-9
+
+
 def test_mlp_closure_force():
     from ghost_b200.les import MLP
     fo, co, gf, gc, les = setup("fp32")

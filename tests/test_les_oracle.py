@@ -109,3 +109,82 @@ def test_vcorrect_sets_mode_energy_and_keeps_helicity():
     assert abs(o.helicity(*vc) - o.helicity(*v)) < 1e-12 * abs(o.helicity(*v))
     assert o.divergence(*vc) < 1e-28
     assert not any(np.isnan(x).any() for x in vc)
+
+
+# ------------------------------------------------- helical EDQNM (heli = 1)
+def test_helical_evedqnm_branches():
+    """evedqnm with hel = 1 (pseudospec3D_edqnm.f90:72-83): a helicity
+    spectrum that cannot be fitted (zero) leaves cusp in charge, so the
+    helicity transfer and diffusivity vanish; a maximally helical-leaning
+    H(k) = a k E(k) takes full_cusp, whose eddy viscosity is positive over
+    the resolved shells and whose helicity terms are non-zero."""
+    n, kc = 128, 42
+    o = Oracle(n)
+    o.set_kmax(float(kc * kc))
+    E = kolmogorov(n, kc)
+    tepq, thpq, tve, tvh, Ext, Hxt = o.evedqnm_h(E, np.zeros_like(E), 1e-4, 10.0, hel=1)
+    assert np.all(thpq == 0) and np.all(tvh == 0)
+    assert np.all(tve[:kc] > 0)
+    H = 0.3 * np.arange(1, n // 2 + 2) * E
+    tepq, thpq, tve, tvh, Ext, Hxt = o.evedqnm_h(E, H, 1e-4, 10.0, hel=1)
+    assert np.all(tve[:kc] > 0) and np.all(tve[kc:] == 0)
+    assert np.any(tvh[:kc] != 0) and np.any(thpq[:kc] != 0)
+    # full_cusp works on the halved extrapolations (:212-215)
+    assert np.all(Ext[kc:3 * kc] > 0) and np.all(Hxt[kc:3 * kc] > 0)
+    # hel = 0 through the helical entry point equals the plain evedqnm
+    t0, _, v0, h0, x0, _ = o.evedqnm_h(E, H, 1e-4, 10.0, hel=0)
+    t1, v1, x1 = o.evedqnm(E, 1e-4, 10.0)
+    assert np.array_equal(t0, t1) and np.array_equal(v0, v1) and np.array_equal(x0, x1) and np.all(h0 == 0)
+
+
+def test_helical_edqnm_run_reduces_to_the_plain_run_without_helicity_flag():
+    """The heli-aware step with hel = 0 is the heli = 0 step bit for bit;
+    with hel = 1 the run stays finite, solenoidal and different."""
+    n, kc = 32, 10
+    o = Oracle(n)
+    o.set_kmax(float(kc * kc))
+    v0, _ = o.random_solenoidal(7, 1.0, 10.0, 1, 1.0)
+    f, _ = o.random_solenoidal(8, 2.0, 3.0, 0, 1.0)
+    a = o.edqnm_run(3, 2, 2e-3, 1e-3, v0, f, t0=0.5)
+    b = o.edqnm_run(3, 2, 2e-3, 1e-3, v0, f, t0=0.5, hel=0)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    lib = o.lib
+    c = [x.copy() for x in v0]
+    lib.o_edqnm_run_h(o.h, 3, 2, 2e-3, 1e-3, 1.4, 0.5, 1, 0, *[x.ctypes.data for x in c],
+                      *[x.ctypes.data for x in f])
+    assert all(np.array_equal(x, y) for x, y in zip(a, c))
+    d = o.edqnm_run(3, 2, 2e-3, 1e-3, v0, f, t0=0.5, hel=1)
+    assert all(np.all(np.isfinite(x)) for x in d)
+    assert o.divergence(*d) < 1e-20 * max(1.0, o.energy(*d, 1))
+    assert rel_l2(d, a) > 0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_library_helical_evedqnm_matches_oracle(prec):
+    """ghost_evedqnm_hel (host) against the oracle's evedqnm with hel = 1,
+    on a spectrum pair that takes full_cusp and on one that falls back to cusp."""
+    from ghost_b200.les import evedqnm_hel
+    n, kc = 128, 42
+    o = Oracle(n, precision=prec)
+    o.set_kmax(float(kc * kc))
+    E = kolmogorov(n, kc)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    for H in (0.3 * np.arange(1, n // 2 + 2) * E, np.zeros_like(E)):
+        for t in (0.5, 5.0):
+            ref = o.evedqnm_h(E, H, 1e-3, t, hel=1)
+            got = evedqnm_hel(n, float(kc * kc), E, H, 1e-3, t, hel=1, precision=prec)
+            for a, b in zip(got, ref):
+                assert rel_l2(a, b) <= tol
+
+
+def test_helical_projection_has_one_sign_of_helicity():
+    o = Oracle(32)
+    v, _ = o.random_solenoidal(3, 1.0, 10.0, 1, 1.0)
+    h = LO.helical(o, v, +1)
+    _, Hk = o.spectrumc(*h, 1, 1)
+    Ek, _ = o.spectrumc(*h, 1, 0)
+    kk = np.arange(1, len(Hk) + 1)
+    live = Ek > 1e-20
+    # maximal helicity: H(k) = k E(k) in spectrumc's normalisation (up to shell rounding)
+    assert np.all(Hk[live] > 0) and np.allclose(Hk[live], kk[live] * Ek[live], rtol=0.3)
+    assert o.divergence(*h) < 1e-20
