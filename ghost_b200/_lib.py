@@ -142,6 +142,7 @@ SIGNATURES = {
     "ghost_les_edqnm_last_hel": [P, PD, PD, PD],
     "ghost_phd_run": [P, I, I, D, D, D, P, P, P, P, P, P, P, P],
     "ghost_phaseshift": [P, P, D, D],
+    "ghost_forcing_slow": [P, I, I, P, P, P, P, P, P, P, P, P],
     "ghost_vector3": [P, P, P, P, P, P, P, P, P, P],
     "ghost_nonlin3": [P, P, P, P, P, P, P, P, I],
     "ghost_gauge3": [P, P, P, P, P, I],

@@ -1678,6 +1678,49 @@ int ghost_phaseshift(ghost_ctx *c, void *a, double cre, double cim) {
   return st.finish();
 }
 
+// The rand = 2 forcing of main3D.fpp:2581-2657: between two random
+// forcings (regenerated every fstep steps by initialfv), each step uses
+// f = (1 - rmp) fold + rmp fnew with rmp = FLOAT(timef+1)/float(fstep),
+// evaluated in default (single-precision) REAL as GHOST does.
+int ghost_forcing_slow(ghost_ctx *c, int timef, int fstep, const void *fxold, const void *fyold, const void *fzold,
+                       const void *fxnew, const void *fynew, const void *fznew, void *fx, void *fy, void *fz) {
+  CTX_CHECK(c);
+  if (fstep < 1) return fail(GHOST_ERR_ARG, "fstep %d must be positive", fstep);
+  if (timef < 0 || timef >= fstep) return fail(GHOST_ERR_ARG, "timef %d not in 0..fstep-1", timef);
+  const void *in[6] = {fxold, fyold, fzold, fxnew, fynew, fznew};
+  void *out[3] = {fx, fy, fz};
+  for (const void *p : in)
+    if (!p) return fail(GHOST_ERR_ARG, "null field");
+  for (void *p : out)
+    if (!p) return fail(GHOST_ERR_ARG, "null field");
+  Staging st(c);
+  const void *din[6];
+  void *dout[3];
+  for (int q = 0; q < 6; ++q) GB_CHECK(st.map(in[q], c->cbytes, 1, &din[q]));
+  for (int q = 0; q < 3; ++q) GB_CHECK(st.map(out[q], c->cbytes, 2, &dout[q]));
+  const float rmpf = (float)(timef + 1) / (float)fstep;
+  if (c->precision == GHOST_SINGLE) {
+    Blend3<float> b;
+    for (int q = 0; q < 3; ++q) {
+      b.old[q] = (const cx<float> *)din[q];
+      b.nw[q] = (const cx<float> *)din[3 + q];
+      b.out[q] = (cx<float> *)dout[q];
+    }
+    blend3_kernel<float><<<grid1d(c->ntot), 256, 0, c->stream>>>(b, c->ntot, 1.0f - rmpf, rmpf);
+  } else {
+    Blend3<double> b;
+    for (int q = 0; q < 3; ++q) {
+      b.old[q] = (const cx<double> *)din[q];
+      b.nw[q] = (const cx<double> *)din[3 + q];
+      b.out[q] = (cx<double> *)dout[q];
+    }
+    const double rmp = (double)rmpf;
+    blend3_kernel<double><<<grid1d(c->ntot), 256, 0, c->stream>>>(b, c->ntot, 1.0 - rmp, rmp);
+  }
+  GB_CHECK(post_launch(c));
+  return st.finish();
+}
+
 // ---------------------------------------------------------------------
 // MHD (MHD_SOL, pseudospec3D_mhd.f90 and include/mhd_rkstep1/2.f90)
 extern "C++" {

@@ -384,6 +384,27 @@ __global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra
   }
 }
 
+// The slowly varying forcing of main3D.fpp:2646-2657 (rand = 2): per mode
+// f = (1 - rmp) fold + rmp fnew, products and sum rounded one by one (no
+// contraction), as GHOST's Fortran evaluates them.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+template <typename R> struct Blend3 {
+  const cx<R> *old[3], *nw[3];
+  cx<R> *out[3];
+};
+template <typename R> __global__ void blend3_kernel(Blend3<R> b, size_t n, R w0, R w1) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const cx<R> u = b.old[a][p], v = b.nw[a][p];
+      b.out[a][p] = mk(add_rn(mul_rn(w0, u.x), mul_rn(w1, v.x)), add_rn(mul_rn(w0, u.y), mul_rn(w1, v.y)));
+    }
+  }
+}
+
 // phaseshift (pseudospec3D_hd.f90:2084-2148): a *= c, except on the kx = 0
 // plane, where GHOST's loops multiply the modes of one half by c and their
 // mirrors by conj(c).  The kz = nz/2 and ky = ny/2 lines of that plane are

@@ -659,6 +659,13 @@
          REAL(C_DOUBLE), VALUE :: cre, cim
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_forcing_slow(ctx,timef,fstep,fxold,fyold,fzold,fxnew,fynew,fznew,fx,fy,fz) &
+                BIND(C,name="ghost_forcing_slow") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ctx, fxold, fyold, fzold, fxnew, fynew, fznew, fx, fy, fz
+         INTEGER(C_INT), VALUE :: timef, fstep
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_vector3(ctx,a,b,c,d,e,f,x,y,z) BIND(C,name="ghost_vector3") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: ctx, a, b, c, d, e, f, x, y, z

@@ -143,6 +143,12 @@ class Ghost:
                                       Hk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "ghost_heltrans")
         return Hk
 
+    def forcing_slow(self, timef: int, fstep: int, fold, fnew, f):
+        """GHOST's rand = 2 forcing: f = (1 - rmp) fold + rmp fnew, rmp = (timef+1)/fstep."""
+        check(self.lib.ghost_forcing_slow(self.h, int(timef), int(fstep), *[self._ptr(x, "c") for x in fold],
+                                          *[self._ptr(x, "c") for x in fnew], *[self._ptr(x, "c") for x in f]),
+              "forcing_slow")
+
     def phaseshift(self, a, cdump: complex):
         """phaseshift: a *= cdump in place (conj on the kx = 0 mirror half)."""
         check(self.lib.ghost_phaseshift(self.h, self._ptr(a, "c"), cdump.real, cdump.imag), "phaseshift")

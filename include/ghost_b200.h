@@ -209,6 +209,15 @@ int ghost_heltrans(ghost_ctx *ctx, const void *a, const void *b, const void *c, 
  * with conj(cdump) on the mirror half of the kx = 0 plane (GHOST's loop
  * order, including its Nyquist lines that take both factors) */
 int ghost_phaseshift(ghost_ctx *ctx, void *a, double cdump_re, double cdump_im);
+/* The rand = 2 (slowly varying) forcing update of main3D.fpp:2581-2657,
+ * which GHOST inlines in its time loop: f = (1-rmp) fold + rmp fnew with
+ * rmp = FLOAT(timef+1)/float(fstep) (default REAL), timef in 0..fstep-1
+ * the steps since the last regeneration.  Every fstep steps the caller
+ * copies f to fold and draws a new random forcing into fnew (initialfv:
+ * ghost_init_random_solenoidal continuing the seed), as GHOST does.  The
+ * outputs may alias either input. */
+int ghost_forcing_slow(ghost_ctx *ctx, int timef, int fstep, const void *fxold, const void *fyold, const void *fzold,
+                       const void *fxnew, const void *fynew, const void *fznew, void *fx, void *fy, void *fz);
 
 /* ------------------------------------------------------------------
  * MHD (MHD_SOL, pseudospec3D_mhd.f90, include/mhd_rkstep1/2.f90): velocity

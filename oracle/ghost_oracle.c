@@ -914,6 +914,20 @@ void o_hd_rkstep2(const octx *c, int o, double dt_d, double nu_d, cplx *vx, cplx
   free(C4); free(C5); free(C6); free(C7); free(C8);
 }
 
+/* The rand = 2 forcing update of main3D.fpp:2646-2657: f = (1-rmp) fold +
+ * rmp fnew with rmp = FLOAT(timef+1)/float(fstep) in default REAL. */
+void o_forcing_slow(const octx *c, int timef, int fstep, const cplx *const fold[3], const cplx *const fnew[3],
+                    cplx *const f[3]) {
+  const real rmp = (real)((float)(timef + 1) / (float)fstep);
+  const real w0 = (real)1 - rmp;
+  for (int a = 0; a < 3; ++a)
+    for (size_t p = 0; p < c->nspec; ++p) {
+      cplx o = fold[a][p], nw = fnew[a][p];
+      f[a][p].re = w0 * o.re + rmp * nw.re;
+      f[a][p].im = w0 * o.im + rmp * nw.im;
+    }
+}
+
 /* nsteps full RK steps of the HD solver (f may be NULL: no forcing) */
 void o_hd_run(const octx *c, int nsteps, int ord, double dt, double nu, cplx *vx, cplx *vy, cplx *vz,
               const cplx *fx, const cplx *fy, const cplx *fz) {

@@ -70,6 +70,7 @@ def _declare(lib: ctypes.CDLL, precision: str) -> None:
         "o_phd_run": (None, [P, I, I, D, D, D] + [P] * 8),
         "o_vector3": (None, [P] * 10),
         "o_phaseshift": (None, [P, P, D, D]),
+        "o_forcing_slow": (None, [P, I, I, P, P, P]),
         "o_nonlin3": (None, [P] * 8 + [I]),
         "o_gauge3": (None, [P] * 5 + [I]),
         "o_mhd_run": (None, [P, I, I, D, D, D] + [P] * 12),
@@ -255,6 +256,15 @@ class Oracle:
         Hk = np.zeros(self.nmax // 2 + 1)
         self.lib.o_heltrans(self.h, *[_ptr(x) for x in arrs], _ptr(Hk))
         return Hk
+
+    def forcing_slow(self, timef, fstep, fold, fnew):
+        """main3D.fpp's rand = 2 update: (1 - rmp) fold + rmp fnew."""
+        fo = [self._c(x) for x in fold]
+        fn = [self._c(x) for x in fnew]
+        out = [self.czeros() for _ in range(3)]
+        arr = lambda xs: (ctypes.c_void_p * 3)(*[x.ctypes.data for x in xs])
+        self.lib.o_forcing_slow(self.h, int(timef), int(fstep), arr(fo), arr(fn), arr(out))
+        return out
 
     def phaseshift(self, a, cdump):
         a = self._c(a).copy()

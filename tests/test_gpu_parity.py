@@ -679,3 +679,67 @@ def test_bouss_fp32_with_512_point_x_lines(shape):
             first = V + [TH]
         else:
             assert all(torch.equal(a, b) for a, b in zip(V + [TH], first)), cfg
+
+
+# ------------------------------------------------ rand = 2 forcing update
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_forcing_slow_matches_oracle(prec):
+    """main3D.fpp:2646-2657 through ghost_forcing_slow: bit for bit with the
+    oracle (no contraction), host and device arrays, output aliasing fold."""
+    o = Oracle(32, precision=prec)
+    g = ghost(32, precision=prec)
+    a, _ = o.random_solenoidal(3, 2.0, 3.0, 0, 1.0)
+    b, _ = o.random_solenoidal(4, 2.0, 3.0, 0, 1.0)
+    a = [x.astype(o.cdt) for x in a]
+    b = [x.astype(o.cdt) for x in b]
+    for timef in (0, 2, 4):
+        ref = o.forcing_slow(timef, 5, a, b)
+        A = [to_dev(x) for x in a]
+        out = [g.czeros() for _ in range(3)]
+        g.forcing_slow(timef, 5, A, [to_dev(x) for x in b], out)
+        assert all(np.array_equal(to_host(x), y) for x, y in zip(out, ref))
+        g.forcing_slow(timef, 5, A, [to_dev(x) for x in b], A)  # in place over fold
+        assert all(np.array_equal(to_host(x), y) for x, y in zip(A, ref))
+        h = [np.zeros(o.sshape, o.cdt) for _ in range(3)]
+        g.forcing_slow(timef, 5, a, b, h)  # host arrays
+        assert all(np.array_equal(x, y) for x, y in zip(h, ref))
+
+
+def test_rand2_forced_run_matches_oracle_loop():
+    """GHOST's time loop with rand = 2 (main3D.fpp:2541-2657): every fstep
+    steps the forcing is saved as fold and a new random forcing drawn with the
+    continuing seed (initialfv), each step blends them; 7 forced RK2 steps at
+    32^3 FP64 against the same loop on the oracle."""
+    n, fstep, dt, nu = 32, 3, 1e-3, 2e-3
+    o = Oracle(n)
+    g = ghost(n)
+    v0, _ = o.random_solenoidal(1000, 1.0, n / 3.0, 1, 1.0)
+    f0, seed = o.random_solenoidal(2000, 2.0, 3.0, 0, 1.0)
+    # oracle loop
+    v, f, s, timef = v0, f0, seed, fstep
+    fold = fnew = None
+    for _ in range(7):
+        if timef == fstep:
+            timef = 0
+            fold = [x.copy() for x in f]
+            fnew, s = o.random_solenoidal(s, 2.0, 3.0, 0, 1.0)
+        f = o.forcing_slow(timef, fstep, fold, fnew)
+        v = o.hd_run(1, 2, dt, nu, v, f)
+        timef += 1
+    # library loop
+    V = [to_dev(x) for x in v0]
+    F = [to_dev(x) for x in f0]
+    Fold = [g.czeros() for _ in range(3)]
+    Fnew = [g.czeros() for _ in range(3)]
+    s, timef = seed, fstep
+    for _ in range(7):
+        if timef == fstep:
+            timef = 0
+            for a, b in zip(Fold, F):
+                a.copy_(b)
+            s = g.init_random_solenoidal(s, 2.0, 3.0, 0, 1.0, *Fnew)
+        g.forcing_slow(timef, fstep, Fold, Fnew, F)
+        g.hd_run(1, 2, dt, nu, *V, *F)
+        timef += 1
+    assert rel_l2([to_host(x) for x in F], f) < 1e-14
+    assert rel_l2([to_host(x) for x in V], v) < 1e-12

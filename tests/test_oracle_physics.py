@@ -251,3 +251,18 @@ def test_phaseshift_keeps_energy_and_hermitian_plane():
     ny, nz = p0.shape
     mirror = np.conj(p0[(-np.arange(ny)) % ny][:, (-np.arange(nz)) % nz])
     assert np.allclose(p0, mirror, rtol=0, atol=1e-14 * np.abs(p0).max())
+
+
+def test_slowly_varying_forcing_interpolates():
+    """rand = 2 (main3D.fpp:2646-2657): the forcing moves linearly from the
+    old to the new random forcing over fstep steps and reaches it."""
+    o = Oracle(16)
+    a, _ = o.random_solenoidal(3, 2.0, 3.0, 0, 1.0)
+    b, _ = o.random_solenoidal(4, 2.0, 3.0, 0, 1.0)
+    fstep = 4
+    for timef in range(fstep):
+        f = o.forcing_slow(timef, fstep, a, b)
+        w = np.float32(timef + 1) / np.float32(fstep)
+        assert all(np.allclose(x, (1 - w) * p + w * q, rtol=0, atol=1e-15) for x, p, q in zip(f, a, b))
+    last = o.forcing_slow(fstep - 1, fstep, a, b)
+    assert all(np.array_equal(x, q) for x, q in zip(last, b))
