@@ -251,6 +251,33 @@ __global__ void __launch_bounds__(256) finalize_kernel(const double *partials, i
 // Shell spectra (spectrumc, pseudospec3D_hd.f90:1190-1415).  Each warp
 // owns a shared histogram; lanes add in lane order, warps are combined in
 // warp order, blocks in block order: reproducible bit for bit.
+// One warp's contribution to a shared-memory histogram: every lane with
+// bin >= 0 adds its NV values to hw[bin + q * stride].  Lanes that share a bin
+// are summed in lane order through shuffles and the group's lowest lane adds
+// the sum, so distinct lanes never touch one slot and the result does not
+// depend on scheduling (the order is fixed: lane order within a chunk, chunk
+// order across the loop).
+template <int NV>
+__device__ __forceinline__ void warp_bin_add(double *hw, int stride, int bin, const double (&v)[NV], int lane) {
+  double s[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) s[q] = 0.0;
+  for (int src = 0; src < 32; ++src) {
+    const int b = __shfl_sync(0xffffffffu, bin, src);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      const double x = __shfl_sync(0xffffffffu, v[q], src);
+      if (b == bin) s[q] += x;
+    }
+  }
+  const unsigned peers = __match_any_sync(0xffffffffu, bin);
+  if (bin >= 0 && lane == __ffs(peers) - 1) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) hw[(size_t)q * stride + bin] += s[q];
+  }
+  __syncwarp();
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R> ra, int kind, size_t n, int nb,
                                                        R Dkk, R rnd, double *partials) {
@@ -276,10 +303,8 @@ __global__ void __launch_bounds__(256) spectrum_kernel(KParams<R> kp, RedArgs<R>
         val = (double)(wgt * red_term(kp, ra, kind, p, i, j, k));
       }
     }
-    for (int s = 0; s < 32; ++s) {
-      if (lane == s && bin >= 0) hw[bin] += val;
-      __syncwarp();
-    }
+    const double vals[1] = {val};
+    warp_bin_add<1>(hw, nb, bin, vals, lane);
   }
   __syncthreads();
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
@@ -367,14 +392,8 @@ __global__ void __launch_bounds__(256) aniso_kernel(KParams<R> kp, RedArgs<R> ra
         }
       }
     }
-    for (int s = 0; s < 32; ++s) {
-      if (lane == s && bin >= 0) {
-        hw[bin] += t;
-        hw[nb + bin] += hh;
-        hw[2 * nb + bin] += vv;
-      }
-      __syncwarp();
-    }
+    const double vals[3] = {t, hh, vv};
+    warp_bin_add<3>(hw, nb, bin, vals, lane);
   }
   __syncthreads();
   for (int b = threadIdx.x; b < nb3; b += blockDim.x) {
