@@ -98,6 +98,8 @@ SIGNATURES = {
     "ghost_ensemble_init": [P, ctypes.POINTER(ctypes.c_int32), D, D, I, D, PD],
     "ghost_ensemble_autotune": [P, I, D, ctypes.POINTER(ctypes.c_int)],
     "ghost_ensemble_run": [P, I, I, D],
+    "ghost_ensemble_set_mode": [P, I],
+    "ghost_ensemble_get_mode": [P, ctypes.POINTER(ctypes.c_int)],
     "ghost_ensemble_energy": [P, I, PD],
     "ghost_slab_range": [I, I, I, I, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "ghost_slab_create": [I, I, I, D, D, D, I, I, I, I, ctypes.POINTER(ctypes.c_void_p)],

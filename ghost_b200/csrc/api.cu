@@ -18,6 +18,7 @@
 #include "ops.cuh"
 #include "passes.cuh"
 #include "xwarp.cuh"
+#include "ensemble.cuh"
 
 namespace gb {
 
@@ -359,19 +360,26 @@ template <typename R, int N, int BZ0> constexpr int y_tile_width() {
   return bz;
 }
 
+// kx indices per y tile: short lines put several kx in one tile so that a
+// CTA has at least 128 threads (not with the second exchange buffer)
+template <int N, int E, int BZ, bool DUAL> constexpr int y_kb() {
+  return (DUAL || BZ * (N / E) >= 128) ? 1 : 128 / (BZ * (N / E));
+}
+
 template <typename R, int N, int S, int BZ0, bool DUAL = false, int E0 = 8>
 int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   constexpr int E = N < E0 ? N : E0, T = N / E;
   constexpr int BZ = y_tile_width<R, N, BZ0>();
-  using G = YGeom<R, N, E, BZ, DUAL>;
+  constexpr int KB = y_kb<N, E, BZ, DUAL>();
+  using G = YGeom<R, N, E, BZ, DUAL, KB>;
   constexpr int STAGES = DUAL ? 2 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
   if (c->nz < BZ) return fail(GHOST_ERR_SIZE, "nz=%d below the y-pass tile width %d", c->nz, BZ);
   const size_t smem = G::smem_bytes(STAGES);
-  auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S, DUAL>;
+  auto kern = ypipe_kernel<R, N, E, BZ, STAGES, S, DUAL, KB>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int ni = pr.jpos ? pr.ni : c->nxh;
-  const long ntiles = (long)(c->nz / BZ) * ni * c->nruns * nf;
-  const int grid = persistent_grid(c, kern, BZ * T, smem, ntiles);
+  const long ntiles = (long)(c->nz / BZ) * ((ni + KB - 1) / KB) * c->nruns * nf;
+  const int grid = persistent_grid(c, kern, KB * BZ * T, smem, ntiles);
   // box rows: 32 (or N/2) for the pruned inverse, whole halves otherwise
   const int rb = (pr.jpos && S > 0) ? std::min(32, N / 2) : std::min(N, 256);
   // store boxes of the dual-buffer variant (TMA stores): whole halves for the
@@ -384,7 +392,7 @@ int launch_y_cfg(ghost_ctx *c, const Fields<R> &f, int nf, const Prune &pr) {
   if (DUAL)
     for (int q = 0; q < nf; ++q) GB_CHECK(field_map(c, f.p[q], BZ * U, rbo, 1, &omaps.m[q]));
   const int ts = timer_begin(c, S > 0 ? GHOST_TIMER_Y_INV : GHOST_TIMER_Y_FWD);
-  kern<<<grid, BZ * T, smem, c->stream>>>(maps, DUAL ? omaps : maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf,
+  kern<<<grid, KB * BZ * T, smem, c->stream>>>(maps, DUAL ? omaps : maps, f, (const cx<R> *)c->tw_y, c->nz, ni, nf,
                                           c->nruns, c->nxh, pr.jpos, pr.jneg, rb, rbo, pipe_ctl(c));
   timer_end(c, ts);
   return post_launch(c);
@@ -432,19 +440,28 @@ template <typename R, int S> int launch_y(ghost_ctx *c, const Fields<R> &f, int 
 // X pass kinds
 enum XKind { X_HD = 0, X_C2R = 1, X_R2C = 2, X_BOUSS = 3 };
 
+// y rows per x tile: short lines put several y rows in one tile so that a
+// CTA has at least 128 threads
+template <typename R, int NX, int BZ> constexpr int x_yb() {
+  constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
+  return BZ * (NX / 2 / E) >= 128 ? 1 : 128 / (BZ * (NX / 2 / E));
+}
+
 // The fused X pass with tiles of BZ z-values (MINB CTAs per SM).
 template <typename R, int NX, int KIND, int BZ, int MINB>
 int launch_x_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int rows) {
   constexpr int E = xE<R>() < NX / 2 ? xE<R>() : NX / 2;
-  constexpr int M = NX / 2, T = M / E, NT = BZ * T;
+  constexpr int YB = x_yb<R, NX, BZ>();
+  if (c->ny % YB != 0) return fail(GHOST_ERR_SIZE, "ny=%d not a multiple of the x tile's %d rows", c->ny, YB);
+  constexpr int M = NX / 2, T = M / E, NT = YB * BZ * T;
   typedef cx<R> C;
   constexpr int PHYS = KIND == X_HD ? 0 : 1;
   constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
-  using G = XGeom<R, NX, BZ>;
+  using G = XGeom<R, NX, BZ, YB>;
   constexpr size_t cap = 220 * 1024 / MINB;  // four stages while MINB CTAs fit an SM
   constexpr int STAGES = G::smem_bytes(4) <= cap ? 4 : (G::smem_bytes(3) <= 200 * 1024 ? 3 : 2);
   const size_t smem = G::smem_bytes(STAGES);
-  auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES, MINB>;
+  auto kern = xpipe_nl_kernel<R, NX, E, BZ, PHYS, STAGES, MINB, YB>;
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Fields<R> fo{};
   for (int q = 0; q < NOUT; ++q) fo.p[q] = (C *)outs[q];
@@ -452,13 +469,13 @@ int launch_x_fused(ghost_ctx *c, const void *const *ins, void *const *outs, int 
   const int nrows = rows > 0 ? rows : M + 1;
   // tensor boxes: nbox boxes of rb kx-rows; rb keeps every box 128-byte aligned in shared memory
   const int nbox = (nrows + 255) / 256;
-  const int align = std::max(1, 128 / (BZ * (int)sizeof(C)));
+  const int align = std::max(1, 128 / (YB * BZ * (int)sizeof(C)));
   const int rb = ((nrows + nbox - 1) / nbox + align - 1) / align * align;
   if (nbox * rb > M + 8 || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the tile", nbox, rb);
   const unsigned U = sizeof(R) == 4 ? 1 : 2;
   FieldMaps maps;
-  for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, 1, rb, &maps.m[q]));
-  const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * c->ny * c->nruns);
+  for (int q = 0; q < NIN; ++q) GB_CHECK(field_map(c, ins[q], BZ * U, YB, rb, &maps.m[q]));
+  const int pgrid = persistent_grid(c, kern, NT, smem, (long)(c->nz / BZ) * (c->ny / YB) * c->nruns);
   kern<<<pgrid, NT, smem, c->stream>>>(maps, fo, (const C *)c->tw_x, c->ny, c->nz, (R)1 / (nn * nn), nrows, nbox, rb,
                                        c->nruns, c->nxh, pipe_ctl(c));
   return GHOST_OK;
@@ -2639,6 +2656,9 @@ int ghost_batch_init_random_solenoidal(ghost_ctx *c, int32_t *seeds, double kdn,
 // ------------------------------------------------------------ ensembles
 struct ghost_ensemble {
   int ncls = 0, precision = 0;
+  // 1: each pass is one launch over every class (ensemble.cuh); 0: each
+  // class runs its own launches on its own stream
+  int multi = 0;
   int n[8] = {0}, nruns[8] = {0};
   ghost_ctx *cls[8] = {nullptr};
   void *v[8][3] = {{nullptr}};
@@ -2667,6 +2687,264 @@ static int ensemble_class_step(ghost_ensemble *e, int q, int ord, double dt, boo
   return GHOST_OK;
 }
 
+// ---- one launch per pass over all classes (ensemble.cuh)
+// Persistent CTAs of a multi-class launch: the occupancy of the kernel times
+// the SM count, shared among the classes in proportion to their tiles (each
+// gets at least one, none more than it has tiles).
+template <int MAXC>
+static int ens_split(ghost_ctx *c0, int per_sm, int ncls, const long *tiles, int *b0, int *nb) {
+  long tot_tiles = 0;
+  for (int q = 0; q < ncls; ++q) tot_tiles += tiles[q];
+  const long total = std::max<long>(ncls, (long)std::max(1, per_sm) * sm_count(c0));
+  int start = 0;
+  for (int q = 0; q < ncls; ++q) {
+    long k = tot_tiles > 0 ? (long)((double)total * (double)tiles[q] / (double)tot_tiles) : 1;
+    k = std::max<long>(1, std::min<long>(k, tiles[q]));
+    b0[q] = start;
+    nb[q] = (int)k;
+    start += (int)k;
+  }
+  return start;
+}
+
+template <typename R> static int ens_T(int N, int E) { return N / (E < N ? E : N); }
+
+template <typename R, class Op>
+static int ens_launch_z(ghost_ensemble *e, ZMulti<R, Op> &P, const long *tiles) {
+  size_t smem = 0;
+  for (int q = 0; q < P.ncls; ++q) {
+    switch (P.n[q]) {
+      case 16: smem = std::max(smem, ens_z_smem<R, 16, Op>(2)); break;
+      case 32: smem = std::max(smem, ens_z_smem<R, 32, Op>(2)); break;
+      case 64: smem = std::max(smem, ens_z_smem<R, 64, Op>(2)); break;
+      case 128: smem = std::max(smem, ens_z_smem<R, 128, Op>(2)); break;
+      default: return fail(GHOST_ERR_STATE, "no multi-class z pass for %d-point lines", P.n[q]);
+    }
+  }
+  auto kern = zmulti_kernel<R, Op>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per = 0;
+  GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
+  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  kern<<<grid, kEnsThreads, smem, e->main>>>(P);
+  return post_launch(e->cls[0]);
+}
+
+template <typename R, int S> static int ens_launch_y(ghost_ensemble *e, YMulti<R> &P, const long *tiles) {
+  size_t smem = 0;
+  for (int q = 0; q < P.ncls; ++q) {
+    switch (P.n[q]) {
+      case 16: smem = std::max(smem, ens_y_smem<R, 16>()); break;
+      case 32: smem = std::max(smem, ens_y_smem<R, 32>()); break;
+      case 64: smem = std::max(smem, ens_y_smem<R, 64>()); break;
+      case 128: smem = std::max(smem, ens_y_smem<R, 128>()); break;
+      default: return fail(GHOST_ERR_STATE, "no multi-class y pass for %d-point lines", P.n[q]);
+    }
+  }
+  auto kern = ymulti_kernel<R, S>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per = 0;
+  GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
+  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  kern<<<grid, kEnsThreads, smem, e->main>>>(P);
+  return post_launch(e->cls[0]);
+}
+
+template <typename R> static int ens_launch_x(ghost_ensemble *e, XMulti<R> &P, const long *tiles) {
+  size_t smem = 0;
+  for (int q = 0; q < P.ncls; ++q) {
+    switch (P.n[q]) {
+      case 16: smem = std::max(smem, ens_x_smem<R, 16>()); break;
+      case 32: smem = std::max(smem, ens_x_smem<R, 32>()); break;
+      case 64: smem = std::max(smem, ens_x_smem<R, 64>()); break;
+      case 128: smem = std::max(smem, ens_x_smem<R, 128>()); break;
+      default: return fail(GHOST_ERR_STATE, "no multi-class x pass for %d-point lines", P.n[q]);
+    }
+  }
+  auto kern = xmulti_kernel<R>;
+  GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per = 0;
+  GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
+  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  kern<<<grid, kEnsThreads, smem, e->main>>>(P);
+  return post_launch(e->cls[0]);
+}
+
+// x-pass tile parameters of a class (its own launch_x_fused would use the same)
+template <typename R> static int ens_x_yb_of(int NX) {
+  switch (NX) {
+    case 16: return ens_x_yb<R, 16>();
+    case 32: return ens_x_yb<R, 32>();
+    case 64: return ens_x_yb<R, 64>();
+    case 128: return ens_x_yb<R, 128>();
+  }
+  return 1;
+}
+static int ens_y_kb_of(int N) {
+  switch (N) {
+    case 16: return ens_y_kb<16>();
+    case 32: return ens_y_kb<32>();
+    case 64: return ens_y_kb<64>();
+    case 128: return ens_y_kb<128>();
+  }
+  return 1;
+}
+
+// One substep (include/hd_rkstep2.f90, hd_rkstep1 folded in when copy) of
+// every class: the five passes of hd_substep_dev, each one launch over all
+// classes on the ensemble's main stream.
+template <typename R> static int ens_substep_multi(ghost_ensemble *e, int o, double dt, int copy, bool prune) {
+  const int nc = e->ncls;
+  void *w[kEnsMaxCls][6];
+  Prune pr[kEnsMaxCls];
+  void *C[kEnsMaxCls][3];
+  const unsigned U = sizeof(R) == 4 ? 1 : 2;
+  for (int q = 0; q < nc; ++q) {
+    ghost_ctx *c = e->cls[q];
+    GB_CHECK(scratch(c, 6, w[q]));
+    GB_CHECK(prune_plan<R>(c, prune, &pr[q]));
+    for (int k = 0; k < 3; ++k) {
+      if (!c->rk[k]) GB_CHECK(dalloc(&c->rk[k], c->cbytes));
+      C[q][k] = c->rk[k];
+    }
+  }
+  long tiles[kEnsMaxCls];
+  // Z inverse
+  {
+    ZMulti<R, ZInv<R, 0>> P{};
+    P.ncls = nc;
+    for (int q = 0; q < nc; ++q) {
+      ghost_ctx *c = e->cls[q];
+      ZInv<R, 0> &zi = P.cl[q].op;
+      for (int k = 0; k < 3; ++k) {
+        zi.v.p[k] = (const cx<R> *)e->v[q][k];
+        zi.cpy.p[k] = (cx<R> *)C[q][k];
+      }
+      for (int k = 0; k < 6; ++k) zi.w.p[k] = (cx<R> *)w[q][k];
+      zi.kp = kparams<R>(c);
+      zi.copy = copy;
+      P.n[q] = c->nz;
+      P.cl[q].tw = (const cx<R> *)c->tw_z;
+      P.cl[q].lines = pr[q].lines;
+      P.cl[q].nlines = pr[q].lines ? pr[q].nlines : c->ny * c->nxh * c->nruns;
+      P.cl[q].ctl = pipe_ctl(c);
+      const int lpb = kEnsThreads / ens_T<R>(c->nz, zE<R>());
+      tiles[q] = (P.cl[q].nlines + lpb - 1) / lpb;
+    }
+    GB_CHECK((ens_launch_z<R, ZInv<R, 0>>(e, P, tiles)));
+  }
+  // Y inverse (6 fields) and, below, Y forward (3 fields)
+  auto ypass = [&](auto sgn, int nf) -> int {
+    constexpr int S = decltype(sgn)::value;
+    YMulti<R> P{};
+    P.ncls = nc;
+    for (int q = 0; q < nc; ++q) {
+      ghost_ctx *c = e->cls[q];
+      YClass<R> &k = P.cl[q];
+      const int N = c->ny, kb = ens_y_kb_of(N);
+      k.rb = (pr[q].jpos && S > 0) ? std::min(32, N / 2) : std::min(N, 256);
+      for (int f = 0; f < nf; ++f) {
+        k.fld.p[f] = (cx<R> *)w[q][f];
+        GB_CHECK(field_map(c, w[q][f], kEnsYBZ * U, k.rb, 1, &k.maps.m[f]));
+      }
+      k.tw = (const cx<R> *)c->tw_y;
+      k.nz = c->nz;
+      k.ni = pr[q].jpos ? pr[q].ni : c->nxh;
+      k.nf = nf;
+      k.nruns = c->nruns;
+      k.nxh = c->nxh;
+      k.jpos = pr[q].jpos;
+      k.jneg = pr[q].jneg;
+      k.ctl = pipe_ctl(c);
+      P.n[q] = N;
+      tiles[q] = (long)(c->nz / kEnsYBZ) * ((k.ni + kb - 1) / kb) * c->nruns * nf;
+    }
+    return ens_launch_y<R, S>(e, P, tiles);
+  };
+  GB_CHECK(ypass(std::integral_constant<int, +1>(), 6));
+  // X: omega x v
+  {
+    XMulti<R> P{};
+    P.ncls = nc;
+    for (int q = 0; q < nc; ++q) {
+      ghost_ctx *c = e->cls[q];
+      XClass<R> &k = P.cl[q];
+      const int M = c->nx / 2, yb = ens_x_yb_of<R>(c->nx), bz = ens_xBZ<R>();
+      if (c->ny % yb != 0) return fail(GHOST_ERR_SIZE, "ny=%d not a multiple of the x tile's %d rows", c->ny, yb);
+      const int nrows = pr[q].rows > 0 ? pr[q].rows : M + 1;
+      const int nbox = (nrows + 255) / 256;
+      const int align = std::max(1, 128 / (yb * bz * (int)sizeof(cx<R>)));
+      const int rb = ((nrows + nbox - 1) / nbox + align - 1) / align * align;
+      if (nbox * rb > M + 8 || rb > 256) return fail(GHOST_ERR_STATE, "x-pass box plan %d x %d exceeds the tile", nbox, rb);
+      for (int f = 0; f < 6; ++f) GB_CHECK(field_map(c, w[q][f], bz * U, yb, rb, &k.maps.m[f]));
+      for (int f = 0; f < 3; ++f) k.out.p[f] = (cx<R> *)w[q][f];
+      const R nn = (R)c->nx * (R)c->ny * (R)c->nz_glob;
+      k.scale = (R)1 / (nn * nn);
+      k.tw = (const cx<R> *)c->tw_x;
+      k.ny = c->ny;
+      k.nz = c->nz;
+      k.rows = nrows;
+      k.nbox = nbox;
+      k.rb = rb;
+      k.nruns = c->nruns;
+      k.nxh = c->nxh;
+      k.ctl = pipe_ctl(c);
+      P.n[q] = c->nx;
+      tiles[q] = (long)(c->nz / bz) * (c->ny / yb) * c->nruns;
+    }
+    GB_CHECK(ens_launch_x<R>(e, P, tiles));
+  }
+  GB_CHECK(ypass(std::integral_constant<int, -1>(), 3));
+  // Z forward: nonlhd3, laplak3 and the truncated update
+  {
+    ZMulti<R, ZFwdHD<R>> P{};
+    P.ncls = nc;
+    for (int q = 0; q < nc; ++q) {
+      ghost_ctx *c = e->cls[q];
+      ZFwdHD<R> &zf = P.cl[q].op;
+      for (int k = 0; k < 3; ++k) {
+        zf.nl.p[k] = (const cx<R> *)w[q][k];
+        zf.v.p[k] = (cx<R> *)e->v[q][k];
+        zf.c0.p[k] = (const cx<R> *)C[q][k];
+        zf.f.p[k] = nullptr;
+      }
+      zf.kp = kparams<R>(c);
+      zf.dt = (R)dt;
+      zf.nu = (R)0;
+      zf.rmp = (R)1 / (R)o;
+      P.n[q] = c->nz;
+      P.cl[q].tw = (const cx<R> *)c->tw_z;
+      P.cl[q].lines = pr[q].lines;
+      P.cl[q].nlines = pr[q].lines ? pr[q].nlines : c->ny * c->nxh * c->nruns;
+      P.cl[q].ctl = pipe_ctl(c);
+      const int lpb = kEnsThreads / ens_T<R>(c->nz, zE<R>());
+      tiles[q] = (P.cl[q].nlines + lpb - 1) / lpb;
+    }
+    GB_CHECK((ens_launch_z<R, ZFwdHD<R>>(e, P, tiles)));
+  }
+  e->cls[0]->launches += 5;
+  return GHOST_OK;
+}
+
+// The ensemble can run its passes as multi-class launches: at most
+// kEnsMaxCls classes, cubic grids of 16..128 points per side.
+static bool ens_multi_ok(const ghost_ensemble *e) {
+  if (e->ncls > kEnsMaxCls) return false;
+  for (int q = 0; q < e->ncls; ++q)
+    if (e->n[q] < 16 || e->n[q] > 128) return false;
+  return true;
+}
+
+// one RK step of every class in multi-class mode
+static int ensemble_multi_step(ghost_ensemble *e, int ord, double dt, bool prune_all) {
+  for (int o = ord; o >= 1; --o) {
+    const bool prune = prune_all || o != ord;
+    GB_CHECK(e->precision == GHOST_SINGLE ? ens_substep_multi<float>(e, o, dt, o == ord ? 1 : 0, prune)
+                                          : ens_substep_multi<double>(e, o, dt, o == ord ? 1 : 0, prune));
+  }
+  return GHOST_OK;
+}
+
 static int ensemble_capture(ghost_ensemble *e, int ord, double dt) {
   if (e->exec) {
     cudaGraphExecDestroy(e->exec);
@@ -2678,8 +2956,12 @@ static int ensemble_capture(ghost_ensemble *e, int ord, double dt) {
   }
   GB_CUDA(cudaStreamBeginCapture(e->main, cudaStreamCaptureModeThreadLocal));
   int st = GHOST_OK;
-  if (cudaEventRecord(e->fork, e->main) != cudaSuccess) st = fail(GHOST_ERR_CUDA, "event record in capture");
-  for (int q = 0; q < e->ncls && st == GHOST_OK; ++q) {
+  if (e->multi) {
+    st = ensemble_multi_step(e, ord, dt, true);
+  } else if (cudaEventRecord(e->fork, e->main) != cudaSuccess) {
+    st = fail(GHOST_ERR_CUDA, "event record in capture");
+  }
+  for (int q = 0; q < e->ncls && st == GHOST_OK && !e->multi; ++q) {
     if (cudaStreamWaitEvent(e->streams[q], e->fork, 0) != cudaSuccess) {
       st = fail(GHOST_ERR_CUDA, "stream wait in capture");
       break;
@@ -2743,7 +3025,27 @@ int ghost_ensemble_create(int nclasses, const int *n, const int *nruns, int prec
     ghost_ensemble_destroy(e);
     return st;
   }
+  e->multi = ens_multi_ok(e) ? 1 : 0;
   *out = e;
+  return GHOST_OK;
+}
+
+int ghost_ensemble_set_mode(ghost_ensemble *e, int multi) {
+  if (!e) return fail(GHOST_ERR_ARG, "null ensemble");
+  if (multi != 0 && multi != 1) return fail(GHOST_ERR_ARG, "mode %d not 0 or 1", multi);
+  if (multi && !ens_multi_ok(e))
+    return fail(GHOST_ERR_ARG, "one launch per pass needs at most %d classes of 16..128 points per side", kEnsMaxCls);
+  if (multi != e->multi && e->exec) {  // the captured step belongs to the other mode
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  e->multi = multi;
+  return GHOST_OK;
+}
+
+int ghost_ensemble_get_mode(const ghost_ensemble *e, int *multi) {
+  if (!e || !multi) return fail(GHOST_ERR_ARG, "null argument");
+  *multi = e->multi;
   return GHOST_OK;
 }
 
@@ -2851,7 +3153,12 @@ int ghost_ensemble_run(ghost_ensemble *e, int nsteps, int ord, double dt) {
   int done = 0;
   if (!e->stepped && nsteps > 0) {
     // one uncaptured step: reads every mode once, builds tables and scratch
-    for (int q = 0; q < e->ncls; ++q) GB_CHECK(ensemble_class_step(e, q, ord, dt, false));
+    if (e->multi) {
+      GB_CHECK(ensemble_multi_step(e, ord, dt, false));
+      GB_CUDA(cudaStreamSynchronize(e->main));
+    } else {
+      for (int q = 0; q < e->ncls; ++q) GB_CHECK(ensemble_class_step(e, q, ord, dt, false));
+    }
     for (int q = 0; q < e->ncls; ++q) GB_CUDA(cudaStreamSynchronize(e->streams[q]));
     e->stepped = true;
     done = 1;
@@ -2861,7 +3168,10 @@ int ghost_ensemble_run(ghost_ensemble *e, int nsteps, int ord, double dt) {
     for (int q = 0; q < e->ncls; ++q) GB_CUDA(cudaStreamSynchronize(e->streams[q]));
     for (; done < nsteps; ++done) {
       GB_CUDA(cudaGraphLaunch(e->exec, e->main));
-      for (int q = 0; q < e->ncls; ++q) e->cls[q]->launches += 10LL * ord / 2;
+      if (e->multi)
+        e->cls[0]->launches += 5LL * ord;
+      else
+        for (int q = 0; q < e->ncls; ++q) e->cls[q]->launches += 5LL * ord;
     }
     GB_CUDA(cudaStreamSynchronize(e->main));
   }

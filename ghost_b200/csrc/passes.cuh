@@ -63,11 +63,12 @@ struct PipeCtl {
 };
 
 // lines != nullptr: the pass covers the listed (j,i) lines only (entries
-// < 0 pad the list); otherwise lines 0..nlines-1.
-template <typename R, int N, int E, int LPB, int STAGES, int MINB, class Op>
-__global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const cx<R> *__restrict__ twg,
-                                                              const int *__restrict__ lines, int nlines,
-                                                              PipeCtl ctl) {
+// < 0 pad the list); otherwise lines 0..nlines-1.  The body takes the CTA's
+// index vb among the nvb CTAs working on this pass (blockIdx.x / gridDim.x
+// for a launch of its own; a share of a launch shared by several grids).
+template <typename R, int N, int E, int LPB, int STAGES, class Op>
+__device__ __forceinline__ void zpipe_body(int vb, int nvb, const Op &op, const cx<R> *__restrict__ twg,
+                                           const int *__restrict__ lines, int nlines, PipeCtl ctl) {
   using C = cx<R>;
   using G = ZGeom<R, N, E, LPB, Op::NLOAD>;
   constexpr int T = G::T, NT = G::NT, NP = G::NP, NL = Op::NLOAD;
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
     return lines ? (long)lines[idx] : idx;
   };
   auto issue = [&](int k) {
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles) return;
     const int s = k % STAGES;
     if (tid == 0) {
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
   auto buf = dual_buf<C>([mine](int idx, int h) -> C & { return mine[h * (LPB * NP) + idx + (idx >> 3)]; }, &ph);
   auto sync = [] { __syncthreads(); };
   for (int k = 0;; ++k) {
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles) break;
     fence_proxy_async();
     issue(k + STAGES - 1);
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
       for (int kk = k; kk < k + STAGES; ++kk)
-        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
+        if (vb + kk * nvb < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
       return;
     }
     const long line = line_of(tile, lq);
@@ -135,6 +136,13 @@ __global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const 
     // exchange barriers follow every read of it, except without exchanges
     if constexpr (fft_exchanges<N, E>() == 0) __syncthreads();
   }
+}
+
+template <typename R, int N, int E, int LPB, int STAGES, int MINB, class Op>
+__global__ void __launch_bounds__(LPB *(N / E), MINB) zpipe_kernel(Op op, const cx<R> *__restrict__ twg,
+                                                              const int *__restrict__ lines, int nlines,
+                                                              PipeCtl ctl) {
+  zpipe_body<R, N, E, LPB, STAGES>(blockIdx.x, gridDim.x, op, twg, lines, nlines, ctl);
 }
 
 // Plain c2c along z of NF fields (in -> out, may alias).
@@ -497,34 +505,36 @@ template <typename R> struct ZFwdBouss {
 // whichever of the two buffers the last exchange did not use; one thread
 // issues them and, before the next tile's first barrier, waits until they
 // have read shared memory.
-template <typename R, int N, int E, int BZ, bool DUAL = false> struct YGeom {
+// KB > 1 (short lines, and only without DUAL): a tile holds BZ z-lines of
+// KB consecutive kx indices, one block of BZ x N per kx, so that a CTA of
+// KB BZ N/E threads has enough threads; thread (l, t, kb) with l fastest.
+template <typename R, int N, int E, int BZ, bool DUAL = false, int KB = 1> struct YGeom {
   static constexpr int T = N / E;
-  static constexpr int NT = BZ * T;
-  static constexpr size_t stage_elems = (size_t)BZ * N;
+  static constexpr int NT = KB * BZ * T;
+  static constexpr size_t stage_elems = (size_t)KB * BZ * N;
   static constexpr size_t smem_bytes(int stages) {
     return ((stages + (DUAL ? 1 : 0)) * stage_elems + N) * sizeof(cx<R>) + 8 * (stages + 1);
   }
 };
 
-template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false>
-__global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps,
-                                                             const __grid_constant__ FieldMaps omaps,
-                                                             const __grid_constant__ Fields<R> fld,
-                                                             const cx<R> *__restrict__ twg, int nz, int ni, int nf,
-                                                             int nruns, int nxh, const int *__restrict__ jpos,
-                                                             const int *__restrict__ jneg, int rb, int rbo,
-                                                             PipeCtl ctl) {
+template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false, int KB = 1>
+__device__ __forceinline__ void ypipe_body(int vb, int nvb, const FieldMaps &maps, const FieldMaps &omaps,
+                                           const Fields<R> &fld, const cx<R> *__restrict__ twg, int nz, int ni,
+                                           int nf, int nruns, int nxh, const int *__restrict__ jpos,
+                                           const int *__restrict__ jneg, int rb, int rbo, PipeCtl ctl) {
+  static_assert(KB == 1 || !DUAL, "several kx per tile only without the second buffer");
   using C = cx<R>;
-  using G = YGeom<R, N, E, BZ, DUAL>;
+  using G = YGeom<R, N, E, BZ, DUAL, KB>;
   constexpr int T = G::T, NT = G::NT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C *stage = reinterpret_cast<C *>(smem_raw);
   C *xb = stage + STAGES * G::stage_elems;  // second exchange buffer (DUAL)
   C *tw = xb + (DUAL ? G::stage_elems : 0);
   uint64_t *bars = reinterpret_cast<uint64_t *>(tw + N);
-  const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
+  const int tid = threadIdx.x, l = tid % BZ, t = (tid / BZ) % T, kb = tid / (BZ * T);
   const int nzb = nz / BZ;
-  const int ntiles = nzb * ni * nruns * nf;
+  const int nig = (ni + KB - 1) / KB;  // groups of KB kx indices
+  const int ntiles = nzb * nig * nruns * nf;
   if (tid == 0) {
     for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
     fence_barrier_init();
@@ -532,14 +542,14 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
   for (int e = tid; e < N; e += NT) tw[e] = twg[e];
   __syncthreads();
   struct Tile {
-    int zb, ii, i, f;  // ii: kx index within the run, i: plane of the batched field
+    int zb, ii, i, f;  // ii: first kx index of the tile within the run, i: its plane of the batched field
   };
   auto tile_of = [&](int tile) {
     Tile r;
     r.zb = tile % nzb;
     int q = tile / nzb;
-    r.ii = q % ni;
-    q /= ni;
+    r.ii = (q % nig) * KB;
+    q /= nig;
     r.i = (q % nruns) * nxh + r.ii;
     r.f = q / nruns;
     return r;
@@ -554,31 +564,39 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
     }
   };
   // one thread issues TMA tensor loads of rb-row boxes covering the live
-  // rows: [0, jp) from the top and [N - jn, N) from the bottom (boxes may
-  // overlap or overrun into rows that are masked out below)
+  // rows of each of the tile's kx: [0, jp) from the top and [N - jn, N) from
+  // the bottom (boxes may overlap or overrun into rows that are masked out below)
   constexpr int U = (int)sizeof(C) / 8;
   auto issue = [&](int k) {
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles || tid != 0) return;
     const Tile tl = tile_of(tile);
-    int jp, jn;
-    rows_of(tl.ii, jp, jn);
     const int s = k % STAGES;
-    const int nb_top = (jp + rb - 1) / rb, nb_bot = (jn + rb - 1) / rb;
+    uint32_t nbox = 0;
+    for (int b = 0; b < KB && tl.ii + b < ni; ++b) {
+      int jp, jn;
+      rows_of(tl.ii + b, jp, jn);
+      nbox += (jp + rb - 1) / rb + (jn + rb - 1) / rb;
+    }
     fence_proxy_async();
-    mbar_arrive_expect_tx(&bars[s], (uint32_t)((nb_top + nb_bot) * rb) * BZ * (uint32_t)sizeof(C));
-    C *dst = stage + (size_t)s * G::stage_elems;
-    for (int q = 0; q < nb_top; ++q)
-      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[tl.f], tl.zb * BZ * U, q * rb, tl.i, &bars[s]);
-    for (int q = 0; q < nb_bot; ++q) {
-      const int r0 = N - (q + 1) * rb;
-      tma_load_3d(dst + (size_t)r0 * BZ, &maps.m[tl.f], tl.zb * BZ * U, r0, tl.i, &bars[s]);
+    mbar_arrive_expect_tx(&bars[s], nbox * (uint32_t)rb * BZ * (uint32_t)sizeof(C));
+    for (int b = 0; b < KB && tl.ii + b < ni; ++b) {
+      int jp, jn;
+      rows_of(tl.ii + b, jp, jn);
+      C *dst = stage + (size_t)s * G::stage_elems + (size_t)b * BZ * N;
+      const int nb_top = (jp + rb - 1) / rb, nb_bot = (jn + rb - 1) / rb;
+      for (int q = 0; q < nb_top; ++q)
+        tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[tl.f], tl.zb * BZ * U, q * rb, tl.i + b, &bars[s]);
+      for (int q = 0; q < nb_bot; ++q) {
+        const int r0 = N - (q + 1) * rb;
+        tma_load_3d(dst + (size_t)r0 * BZ, &maps.m[tl.f], tl.zb * BZ * U, r0, tl.i + b, &bars[s]);
+      }
     }
   };
   for (int k = 0; k < STAGES - 1; ++k) issue(k);
   auto sync = [] { __syncthreads(); };
   for (int k = 0;; ++k) {
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles) break;
     // DUAL: the refill of the previous tile's slot waits for this tile's
     // first barrier, which follows every read of that slot (so no barrier
@@ -593,23 +611,26 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
     if (__syncthreads_or(!ok)) {
       if (tid == 0) record_timeout(ctl.status);
       for (int kk = k; kk < k + STAGES - (DUAL ? 1 : 0); ++kk)
-        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
+        if (vb + kk * nvb < ntiles) mbar_wait(&bars[kk % STAGES], (uint32_t)(kk / STAGES) & 1u, kDrainPolls);
       if (DUAL && tid == 0) bulk_wait_all();
       return;
     }
     if constexpr (DUAL) issue(k + STAGES - 1);
     const Tile tl = tile_of(tile);
+    // this thread's kx: beyond the last one (a short last group) its line is
+    // transformed from zeros and not stored
+    const bool act = tl.ii + kb < ni;
     int jp = N, jn = 0;
-    if (jpos) {
-      jp = jpos[tl.ii];
-      jn = jneg[tl.ii];
+    if (jpos && act) {
+      jp = jpos[tl.ii + kb];
+      jn = jneg[tl.ii + kb];
     }
-    C *sb = stage + (size_t)s * G::stage_elems;
+    C *sb = stage + (size_t)s * G::stage_elems + (size_t)kb * BZ * N;
     C x[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int jj = t + T * e;
-      const bool live = (S < 0) || jj < jp || jj >= N - jn;
+      const bool live = act && ((S < 0) || jj < jp || jj >= N - jn);
       x[e] = live ? sb[jj * BZ + l] : mk((R)0, (R)0);
     }
     if constexpr (DUAL) {
@@ -647,16 +668,29 @@ __global__ void __launch_bounds__(BZ *(N / E), 2) ypipe_kernel(const __grid_cons
       __syncthreads();  // every read of the stage before the exchanges overwrite it
       auto buf = [sb, l](int idx) -> C & { return sb[idx * BZ + l]; };
       line_fft<C, N, E, S>(x, t, tw, buf, sync);
-      C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * tl.i;
+      C *base = fld.p[tl.f] + (size_t)tl.zb * BZ + l + (size_t)nz * N * (tl.i + kb);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int jj = t + T * e;
-        if (S > 0 || jj < jp || jj >= N - jn) base[(size_t)nz * jj] = x[e];
+        if (act && (S > 0 || jj < jp || jj >= N - jn)) base[(size_t)nz * jj] = x[e];
       }
       __syncthreads();  // the stage is read before the next refill
     }
   }
   if (DUAL && tid == 0) bulk_wait_all();
+}
+
+template <typename R, int N, int E, int BZ, int STAGES, int S, bool DUAL = false, int KB = 1>
+__global__ void __launch_bounds__(KB *BZ *(N / E), 2) ypipe_kernel(const __grid_constant__ FieldMaps maps,
+                                                                 const __grid_constant__ FieldMaps omaps,
+                                                                 const __grid_constant__ Fields<R> fld,
+                                                                 const cx<R> *__restrict__ twg, int nz, int ni,
+                                                                 int nf, int nruns, int nxh,
+                                                                 const int *__restrict__ jpos,
+                                                                 const int *__restrict__ jneg, int rb, int rbo,
+                                                                 PipeCtl ctl) {
+  ypipe_body<R, N, E, BZ, STAGES, S, DUAL, KB>(blockIdx.x, gridDim.x, maps, omaps, fld, twg, nz, ni, nf, nruns, nxh,
+                                                jpos, jneg, rb, rbo, ctl);
 }
 
 // ====================================================================
@@ -725,34 +759,39 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-template <typename R, int NX, int BZ> struct XGeom {
+// YB > 1 (short lines): a tile holds the BZ z-values of YB consecutive y
+// rows, so that a CTA of YB BZ (NX/2)/E threads has enough threads; the
+// stage holds rows [kx][y][z] (one TMA box of BZ x YB x rb per field) and
+// the lines (y, z) interleave in the exchange buffer.
+template <typename R, int NX, int BZ, int YB = 1> struct XGeom {
   static constexpr int M = NX / 2;
   // TMA boxes may overrun the M+1 rows by a few (zero-filled) rows
-  static constexpr size_t stage_elems = (size_t)(M + 8) * BZ;
+  static constexpr size_t stage_elems = (size_t)(M + 8) * BZ * YB;
   static constexpr size_t smem_bytes(int stages) {
-    return (stages * stage_elems + NX + 2 * (size_t)M * BZ) * sizeof(cx<R>) + 8 * (stages + 1);
+    return (stages * stage_elems + NX + 2 * (size_t)M * BZ * YB) * sizeof(cx<R>) + 8 * (stages + 1);
   }
 };
 
 
 
-template <typename R, int NX, int E, int BZ, int PHYS, int STAGES, int MINB = 2>
-__global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
-                                                                    Fields<R> out, const cx<R> *__restrict__ twg,
-                                                                    int ny, int nz, R scale, int rows, int nbox,
-                                                                    int rb, int nruns, int nxh, PipeCtl ctl) {
+template <typename R, int NX, int E, int BZ, int PHYS, int STAGES, int YB = 1>
+__device__ __forceinline__ void xpipe_nl_body(int vb, int nvb, const FieldMaps &maps, const Fields<R> &out,
+                                              const cx<R> *__restrict__ twg, int ny, int nz, R scale, int rows,
+                                              int nbox, int rb, int nruns, int nxh, PipeCtl ctl) {
   using C = cx<R>;
-  using G = XGeom<R, NX, BZ>;
-  constexpr int M = NX / 2, T = M / E, NT = BZ * T;
+  using G = XGeom<R, NX, BZ, YB>;
+  constexpr int M = NX / 2, T = M / E, NT = YB * BZ * T;
+  constexpr int LW = YB * BZ;  // lines of a tile: (y, z) with z fastest
   constexpr int NIN = PHYS == 0 ? 6 : 9, NOUT = PHYS == 0 ? 3 : 4;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C *stage = reinterpret_cast<C *>(smem_raw);
   C *tw = stage + STAGES * G::stage_elems;
   C *xb = tw + NX;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + 2 * (size_t)M * BZ);
-  const int tid = threadIdx.x, l = tid % BZ, t = tid / BZ;
-  const int nzb = nz / BZ;
-  const int ntiles = nzb * ny * nruns;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xb + 2 * (size_t)M * LW);
+  const int tid = threadIdx.x, l = tid % BZ, t = (tid / BZ) % T, yb = tid / (BZ * T);
+  const int lw = yb * BZ + l;  // this thread's line within the tile
+  const int nzb = nz / BZ, nyg = ny / YB;
+  const int ntiles = nzb * nyg * nruns;
   const size_t rowstride = (size_t)nz * ny;
   if (tid == 0) {
     for (int q = 0; q <= STAGES; ++q) mbar_init(&bars[q], 1);  // bars[STAGES]: never completed
@@ -764,22 +803,22 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
   constexpr int U = (int)sizeof(C) / 8;
   auto issue = [&](int L) {
     const int k = L / NIN, f = L - k * NIN;
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles || tid != 0) return;
     const int s = L % STAGES;
     fence_proxy_async();
-    mbar_arrive_expect_tx(&bars[s], (uint32_t)(nbox * rb) * BZ * (uint32_t)sizeof(C));
+    mbar_arrive_expect_tx(&bars[s], (uint32_t)(nbox * rb) * LW * (uint32_t)sizeof(C));
     C *dst = stage + (size_t)s * G::stage_elems;
     for (int q = 0; q < nbox; ++q)
-      tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[f], (tile % nzb) * BZ * U, (tile / nzb) % ny,
-                  (tile / nzb / ny) * nxh + q * rb, &bars[s]);
+      tma_load_3d(dst + (size_t)q * rb * LW, &maps.m[f], (tile % nzb) * BZ * U, ((tile / nzb) % nyg) * YB,
+                  (tile / nzb / nyg) * nxh + q * rb, &bars[s]);
   };
   for (int L = 0; L < STAGES - 1; ++L) issue(L);
   int ph = 0;
-  auto buf = dual_buf<C>([xb, l](int idx, int h) -> C & { return xb[(size_t)h * (M * BZ) + idx * BZ + l]; }, &ph);
+  auto buf = dual_buf<C>([xb, lw](int idx, int h) -> C & { return xb[(size_t)h * (M * LW) + idx * LW + lw]; }, &ph);
   auto sync = [] { __syncthreads(); };
   for (int k = 0;; ++k) {
-    const int tile = blockIdx.x + k * gridDim.x;
+    const int tile = vb + k * nvb;
     if (tile >= ntiles) break;
     C V[3][E], P[NOUT][E];
     bool failed = false;
@@ -792,7 +831,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
       const C *sb = stage + (size_t)(L % STAGES) * G::stage_elems;
       C x[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, BZ, l, t + T * e, M, rows, tw);
+      for (int e = 0; e < E; ++e) x[e] = c2r_pack(sb, LW, lw, t + T * e, M, rows, tw);
       // The CTA agrees on the wait at the transform's first exchange barrier,
       // which also orders every read of the stage before its next refill (the
       // exchange halves alternate, so that barrier needs nothing before it).
@@ -807,7 +846,7 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
       if (bad) {
         if (tid == 0) record_timeout(ctl.status);
         for (int LL = L; LL < L + STAGES; ++LL)
-          if (blockIdx.x + (LL / NIN) * gridDim.x < ntiles)
+          if (vb + (LL / NIN) * nvb < ntiles)
             mbar_wait(&bars[LL % STAGES], (uint32_t)(LL / STAGES) & 1u, kDrainPolls);
         failed = true;
         break;
@@ -861,8 +900,8 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
 #pragma unroll
       for (int e = 0; e < E; ++e) buf(t + T * e) = P[c][e];
       __syncthreads();
-      obase = out.p[c] + (size_t)(tile % nzb) * BZ + (size_t)nz * ((tile / nzb) % ny) +
-              rowstride * (size_t)((tile / nzb / ny) * nxh) + l;
+      obase = out.p[c] + (size_t)(tile % nzb) * BZ + (size_t)nz * (((tile / nzb) % nyg) * YB + yb) +
+              rowstride * (size_t)((tile / nzb / nyg) * nxh) + l;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int kk = t + T * e;
@@ -873,6 +912,15 @@ __global__ void __launch_bounds__(BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const 
       buf.flip();  // the next write goes to the other half
     }
   }
+}
+
+template <typename R, int NX, int E, int BZ, int PHYS, int STAGES, int MINB = 2, int YB = 1>
+__global__ void __launch_bounds__(YB *BZ *(NX / 2) / E, MINB) xpipe_nl_kernel(const __grid_constant__ FieldMaps maps,
+                                                                         Fields<R> out, const cx<R> *__restrict__ twg,
+                                                                         int ny, int nz, R scale, int rows, int nbox,
+                                                                         int rb, int nruns, int nxh, PipeCtl ctl) {
+  xpipe_nl_body<R, NX, E, BZ, PHYS, STAGES, YB>(blockIdx.x, gridDim.x, maps, out, twg, ny, nz, scale, rows, nbox, rb,
+                                                nruns, nxh, ctl);
 }
 
 // ====================================================================

@@ -345,6 +345,18 @@
          INTEGER(C_INT) :: cfg(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_ensemble_set_mode(ens,multi) BIND(C,name="ghost_ensemble_set_mode") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT), VALUE :: multi
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_ensemble_get_mode(ens,multi) BIND(C,name="ghost_ensemble_get_mode") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: ens
+         INTEGER(C_INT) :: multi
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_ensemble_run(ens,nsteps,ord,dt) BIND(C,name="ghost_ensemble_run") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_DOUBLE
          TYPE(C_PTR), VALUE :: ens

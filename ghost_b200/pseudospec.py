@@ -504,6 +504,15 @@ class Ensemble:
     def run(self, nsteps: int, ord: int, dt: float):
         check(self.lib.ghost_ensemble_run(self.h, nsteps, ord, dt), "ghost_ensemble_run")
 
+    def set_mode(self, multi: bool):
+        """True: each pass one launch over every class; False: per-class launches on per-class streams."""
+        check(self.lib.ghost_ensemble_set_mode(self.h, int(bool(multi))), "ghost_ensemble_set_mode")
+
+    def mode(self) -> bool:
+        m = ctypes.c_int()
+        check(self.lib.ghost_ensemble_get_mode(self.h, ctypes.byref(m)), "ghost_ensemble_get_mode")
+        return bool(m.value)
+
     def energy(self, kin: int = 1):
         out = np.zeros(self.total)
         check(self.lib.ghost_ensemble_energy(self.h, kin, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),

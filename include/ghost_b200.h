@@ -410,6 +410,15 @@ int ghost_ensemble_autotune(ghost_ensemble *ens, int ord, double dt, int *cfg_ou
 /* nsteps RK steps of every run; after one uncaptured step the step is a
  * replayed CUDA graph */
 int ghost_ensemble_run(ghost_ensemble *ens, int nsteps, int ord, double dt);
+/* How the ensemble runs its passes: multi = 1 (the default where allowed:
+ * at most 4 classes of 16..128 points per side) makes each of the five
+ * passes of a substep one kernel launch over every class, each CTA working
+ * for one class (a tile table splits the persistent CTAs in proportion to
+ * the classes' tiles); multi = 0 runs every class's own launches on its own
+ * stream (the per-class tile variants of ghost_ensemble_autotune apply
+ * there).  Both give the same bits. */
+int ghost_ensemble_set_mode(ghost_ensemble *ens, int multi);
+int ghost_ensemble_get_mode(const ghost_ensemble *ens, int *multi);
 /* per-run energy(kin), runs in class order */
 int ghost_ensemble_energy(ghost_ensemble *ens, int kin, double *out);
 

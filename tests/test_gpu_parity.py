@@ -743,3 +743,37 @@ def test_rand2_forced_run_matches_oracle_loop():
         timef += 1
     assert rel_l2([to_host(x) for x in F], f) < 1e-14
     assert rel_l2([to_host(x) for x in V], v) < 1e-12
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_ensemble_one_launch_per_pass_equals_per_class_launches(prec):
+    """Every pass one launch over all classes (CTAs assigned to classes by a
+    tile table) against each class's own launches on its own stream: the
+    same bits for four uneven classes, and each run against the oracle."""
+    import torch
+    from ghost_b200 import Ensemble
+    sizes, nruns = [16, 32, 64, 128], [5, 3, 2, 1]
+    seeds = list(range(301, 312))
+    nus = [5e-4 * (1.3 ** q) for q in range(11)]
+    out = {}
+    for multi in (True, False):
+        ens = Ensemble(sizes, nruns, precision=prec)
+        ens.set_mode(multi)
+        assert ens.mode() == multi
+        ens.init(seeds, nus)
+        ens.run(3, 2, 1e-3)
+        out[multi] = [[x.clone() for x in ens.fields(c)] for c in range(len(sizes))]
+        ens.close()
+    for c in range(len(sizes)):
+        assert all(torch.equal(a, b) for a, b in zip(out[True][c], out[False][c])), c
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    q = 0
+    for c, (n, r) in enumerate(zip(sizes, nruns)):
+        o = Oracle(n)
+        nxh = n // 2 + 1
+        for k in range(r):
+            v0, _ = o.random_solenoidal(seeds[q], 1.0, n / 3.0, 1, 1.0)
+            ref = o.hd_run(3, 2, 1e-3, nus[q], v0)
+            got = [to_host(x[k * nxh:(k + 1) * nxh]).astype(np.complex128) for x in out[True][c]]
+            assert rel_l2(got, ref) < tol, (c, k)
+            q += 1
