@@ -130,6 +130,7 @@ SIGNATURES = {
     "ghost_les_truncate": [P, P, P, P],
     "ghost_les_samples": [P, P, P, P, P, ctypes.c_float, P, P],
     "ghost_les_features": [P, P, P, P, ctypes.c_float, ctypes.c_float, P],
+    "ghost_les_spectral_features": [P, P, P],
     "ghost_les_tau_force": [P, P, ctypes.c_float, P, P, P, P, P, P],
     "ghost_les_set_model": [P, I, P, D, D, D, D],
     "ghost_les_set_fallback": [P, I, D],

@@ -187,6 +187,53 @@ __global__ void eddy_force_kernel(KParams<R> kp, Spec3<R> v, Spec3<R> f, Spec3w<
   }
 }
 
+// ---------------------------------------------------------------------
+// The spectral network's inputs, one row per resolved shell k = 1..kc (row
+// k-1), from the kinetic spectrum E (spectrumc's kin = 1 sums, E[k-1] the
+// shell k); non-positive shell energies count as 1e-30 of the resolved sum:
+//   x0 = k/kc, x1 = (k/kc)^2, x2 = ln(E(k)/E(kc)) / 8,
+//   x3 = d ln E / d ln k at k (centred; one-sided at k = 1 and k = kc) / 4,
+//   x4 = the log-slope from kc/2 to kc / 4,
+//   x5 = ln(kc E(kc) / sum_{k<=kc} E(k)) / 8,
+//   x6 = exp(-(kc - k)/2), x7 = exp(-(kc - k)/8), x8 = x9 = 0.
+// Every thread forms the resolved sum itself, in shell order.
+__device__ inline double spec_e(const double *E, int k, double floor_) { return fmax(E[k - 1], floor_); }
+
+__global__ void spec_features_kernel(const double *__restrict__ E, int kc, float *__restrict__ x) {
+  double tot = 0.0;
+  for (int k = 1; k <= kc; ++k) tot += fmax(E[k - 1], 0.0);
+  const double fl = 1e-30 * fmax(tot, 1e-300);
+  const double ec = spec_e(E, kc, fl);
+  const int kh = kc / 2 > 1 ? kc / 2 : 1;
+  const double slope_c = kh < kc ? log(ec / spec_e(E, kh, fl)) / log((double)kc / (double)kh) : 0.0;
+  const double frac = log((double)kc * ec / fmax(tot, fl));
+  for (int k = 1 + (int)threadIdx.x; k <= kc; k += (int)blockDim.x) {
+    const double r = (double)k / (double)kc;
+    const int ka = k > 1 ? k - 1 : k, kb = k < kc ? k + 1 : k;
+    const double sl = ka < kb ? log(spec_e(E, kb, fl) / spec_e(E, ka, fl)) / log((double)kb / (double)ka) : 0.0;
+    float *row = x + (size_t)(k - 1) * GHOST_MLP_NIN;
+    row[0] = (float)r;
+    row[1] = (float)(r * r);
+    row[2] = (float)(log(spec_e(E, k, fl) / ec) / 8.0);
+    row[3] = (float)(sl / 4.0);
+    row[4] = (float)(slope_c / 4.0);
+    row[5] = (float)(frac / 8.0);
+    row[6] = (float)exp(-(double)(kc - k) / 2.0);
+    row[7] = (float)exp(-(double)(kc - k) / 8.0);
+    row[8] = 0.f;
+    row[9] = 0.f;
+  }
+}
+
+// tve(k) of the spectral network: the first output of row k-1 times
+// out_scale sqrt(E(kc)/kc) (Kraichnan's scaling of a spectral eddy
+// viscosity at the cutoff) for k <= kc, zero beyond
+__global__ void spec_tve_kernel(const float *__restrict__ y, const double *__restrict__ E, int kc, int nb,
+                                double out_scale, double *__restrict__ tve) {
+  const double s = out_scale * sqrt(fmax(E[kc - 1], 0.0) / (double)kc);
+  for (int k = 1 + (int)threadIdx.x; k <= nb; k += (int)blockDim.x)
+    tve[k - 1] = k <= kc ? (double)y[(size_t)(k - 1) * GHOST_MLP_NOUT] * s : 0.0;
+}
 
 // ---------------------------------------------------------------------
 // vcorrect (pseudo/pseudospec3D_edqnm.f90:405-1629) with heli = 0, per mode:
@@ -1019,6 +1066,31 @@ static int eddy_force_dev(ghost_les *L, const void *const v[3], const void *cons
   return post_launch(c);
 }
 
+// The spectral network as a closure: kinetic spectrum -> shell inputs ->
+// network (kc rows) -> tve(k) -> the eddy-viscous force, all on the stream
+template <typename R>
+static int spectral_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
+  ghost_ctx *c = L->c;
+  const int nb = c->nx / 2 + 1;
+  GB_CHECK(spectrum_dev_async<R>(c, RED_ENERGY_KIND, v[0], v[1], v[2], L->Ek_dev));
+  spec_features_kernel<<<1, 64, 0, c->stream>>>(L->Ek_dev, L->kc, L->x);
+  GB_CHECK(post_launch(c));
+  GB_CHECK(ghost_mlp_set_stream(L->mlp, c->stream));
+  GB_CHECK(ghost_mlp_forward(L->mlp, L->x, L->y, L->kc));
+  spec_tve_kernel<<<1, 64, 0, c->stream>>>(L->y, L->Ek_dev, L->kc, nb, (double)L->ts, L->tve_dev);
+  GB_CHECK(post_launch(c));
+  Spec3<R> vs, fs;
+  Spec3w<R> os;
+  for (int a = 0; a < 3; ++a) {
+    vs.p[a] = (const cx<R> *)v[a];
+    fs.p[a] = f ? (const cx<R> *)f[a] : nullptr;
+    os.p[a] = (cx<R> *)o[a];
+  }
+  eddy_force_kernel<R><<<blocks(c->nspec), 256, 0, c->stream>>>(kparams<R>(c), vs, fs, os, L->tve_dev, nullptr, nb,
+                                                                  c->nspec);
+  return post_launch(c);
+}
+
 // closure force of the selected model for the velocity v: o = f + F(v)
 template <typename R>
 static int closure_force_dev(ghost_les *L, const void *const v[3], const void *const f[3], void *const o[3]) {
@@ -1032,6 +1104,8 @@ static int closure_force_dev(ghost_les *L, const void *const v[3], const void *c
     }
     case GHOST_LES_EDQNM:
       return eddy_force_dev<R>(L, v, f, o);
+    case GHOST_LES_MLP_SPECTRAL:
+      return spectral_force_dev<R>(L, v, f, o);
     default: {
       // no closure: the forcing alone
       const size_t b = c->cbytes;
@@ -1071,10 +1145,11 @@ static int les_run_dev(ghost_les *L, int nsteps, int ord, double dt, double nu, 
   // the start of the call is redone with GHOST's EDQNM closure, which then
   // stays in use
   double e_ref = 0.0;
-  const bool guard = L->fallback && L->model == GHOST_LES_MLP;
+  auto learned = [L] { return L->model == GHOST_LES_MLP || L->model == GHOST_LES_MLP_SPECTRAL; };
+  const bool guard = L->fallback && learned();
   if (guard) GB_CHECK(reduce_dev<R>(c, 0 /* <|v|^2> */, v[0], v[1], v[2], nullptr, nullptr, nullptr, &e_ref));
   for (int s = 0; s < nsteps; ++s) {
-    const bool guarded = L->fallback && L->model == GHOST_LES_MLP;
+    const bool guarded = L->fallback && learned();
     if (guarded)
       for (int a = 0; a < 3; ++a)
         GB_CUDA(cudaMemcpyAsync(L->save[a], v[a], c->cbytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -1234,6 +1309,16 @@ int ghost_les_features(ghost_les *L, const void *vx, const void *vy, const void 
   return st;
 }
 
+int ghost_les_spectral_features(ghost_les *L, const double *E, float *x) {
+  LES_CHECK(L);
+  if (!E || !x || !is_device_ptr(E) || !is_device_ptr(x))
+    return fail(GHOST_ERR_ARG, "ghost_les_spectral_features needs device arrays");
+  spec_features_kernel<<<1, 64, 0, L->c->stream>>>(E, L->kc, x);
+  GB_CHECK(post_launch(L->c));
+  GB_CUDA(cudaStreamSynchronize(L->c->stream));
+  return check_status(L->c);
+}
+
 int ghost_les_tau_force(ghost_les *L, const float *tau, float tau_scale, const void *fx, const void *fy,
                         const void *fz, void *ox, void *oy, void *oz) {
   LES_CHECK(L);
@@ -1250,9 +1335,13 @@ int ghost_les_tau_force(ghost_les *L, const float *tau, float tau_scale, const v
 int ghost_les_set_model(ghost_les *L, int model, ghost_mlp *mlp, double grad_scale, double tau_scale, double delta,
                         double kolmo) {
   LES_CHECK(L);
-  if (model != GHOST_LES_NONE && model != GHOST_LES_EDQNM && model != GHOST_LES_MLP)
+  if (model != GHOST_LES_NONE && model != GHOST_LES_EDQNM && model != GHOST_LES_MLP &&
+      model != GHOST_LES_MLP_SPECTRAL)
     return fail(GHOST_ERR_ARG, "unknown closure %d", model);
-  if (model == GHOST_LES_MLP && !mlp) return fail(GHOST_ERR_ARG, "the MLP closure needs a network");
+  if ((model == GHOST_LES_MLP || model == GHOST_LES_MLP_SPECTRAL) && !mlp)
+    return fail(GHOST_ERR_ARG, "the MLP closure needs a network");
+  if (model == GHOST_LES_MLP_SPECTRAL && L->kc < 4)
+    return fail(GHOST_ERR_ARG, "the spectral closure needs a cutoff of at least 4 shells");
   if (model == GHOST_LES_EDQNM && !(kolmo > 0)) return fail(GHOST_ERR_ARG, "kolmo must be positive");
   if (model == GHOST_LES_EDQNM && (int)std::sqrt(L->c->kmax) < 4)
     return fail(GHOST_ERR_ARG, "the EDQNM closure needs a cutoff of at least 4 shells");

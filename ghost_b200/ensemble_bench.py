@@ -10,6 +10,13 @@ within each size class, with the seeds and viscosities of the whole
 ensemble), with no communication; the time is the maximum over ranks and
 the rates are those of the whole ensemble.
 
+Two ways to run one substep of the ensemble are timed back to back (--mode
+both, the default): "multi", each of the five passes one launch over all
+size classes (a CTA picks its class from a per-class tile table), and
+"per-class", each class's own launches on its own stream, with the tile
+shapes the autotuner picked for that class.  The top-level rates are those
+of the faster mode.
+
 Default workload: 128 runs at 32^3, 96 at 64^3, 32 at 128^3 (96.5M grid
 points), seeds 1000+r, nu log-uniform in [5e-4, 5e-3] from a seeded host
 RNG, the config-0 initial spectrum, RK2, dt = 1e-3.  Prints one JSON line
@@ -43,6 +50,7 @@ def main(argv=None):
     ap.add_argument("--ord", type=int, default=2)
     ap.add_argument("--dt", type=float, default=1e-3)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--mode", default="both", choices=["both", "multi", "per-class"])
     a = ap.parse_args(argv)
 
     import numpy as np
@@ -73,32 +81,49 @@ def main(argv=None):
     ens.init([seeds[r] for r in mine], nu[mine])
     cfg = ens.autotune(a.ord, a.dt)
     setup = time.perf_counter() - t0
-    ens.run(1, a.ord, a.dt)  # uncaptured first step, graph capture
-    ens.run(1, a.ord, a.dt)
-    torch.cuda.synchronize()
-    e0 = ens.energy(1)
-    s = torch.cuda.current_stream()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0.record(s)
-    ens.run(a.steps, a.ord, a.dt)
-    ev1.record(s)
-    ev1.synchronize()
-    wall = ev0.elapsed_time(ev1) * 1e-3
-    if world > 1:
-        t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        wall = float(t.item())
+    e0 = None
+    modes = {"both": ["multi", "per-class"], "multi": ["multi"], "per-class": ["per-class"]}[a.mode]
+    timing = {}
+    for m in modes:
+        try:
+            ens.set_mode(m == "multi")
+        except RuntimeError:
+            if a.mode == "multi":
+                raise
+            continue  # classes outside the multi-class launches: per-class only
+        ens.run(1, a.ord, a.dt)  # uncaptured first step, graph capture
+        ens.run(1, a.ord, a.dt)
+        torch.cuda.synchronize()
+        if e0 is None:
+            e0 = ens.energy(1)
+        s = torch.cuda.current_stream()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(s)
+        ens.run(a.steps, a.ord, a.dt)
+        ev1.record(s)
+        ev1.synchronize()
+        wall = ev0.elapsed_time(ev1) * 1e-3
+        if world > 1:
+            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        timing[m] = wall
     e1 = ens.energy(1)
     points = sum(r * n ** 3 for n, r in zip(sizes, runs))
+    best = min(timing, key=timing.get)
+    wall = timing[best]
     if rank == 0:
         print(json.dumps({
             "workload": f"ensemble {'+'.join(f'{r}x{n}^3' for n, r in zip(sizes, runs))}, RK{a.ord}, dt={a.dt}, "
                         f"{a.precision}",
             "gpus": world, "steps": a.steps, "seconds": wall, "run_steps_per_s": total * a.steps / wall,
             "ensemble_steps_per_s": a.steps / wall, "gridpoint_steps_per_s": points * a.steps / wall,
+            "mode": best,
+            "modes": {m: {"seconds": w, "run_steps_per_s": total * a.steps / w,
+                          "gridpoint_steps_per_s": points * a.steps / w} for m, w in timing.items()},
             "tile_cfg": cfg, "setup_s": setup,
             "energy_decay_min_max": [float((e1 / e0).min()), float((e1 / e0).max())],
         }))

@@ -556,6 +556,11 @@
          REAL(C_FLOAT), VALUE :: gs, delta
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_les_spectral_features(les,e,x) BIND(C,name="ghost_les_spectral_features") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: les, e, x
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_les_tau_force(les,tau,ts,fx,fy,fz,ox,oy,oz) BIND(C,name="ghost_les_tau_force") RESULT(s)
          IMPORT :: C_INT, C_PTR, C_FLOAT
          TYPE(C_PTR), VALUE :: les, tau, fx, fy, fz, ox, oy, oz

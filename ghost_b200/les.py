@@ -1,5 +1,6 @@
 """Host mirror of the LES path: the learned subgrid-stress MLP and the LES
-driver with its closures (none, GHOST's EDQNM eddy viscosity, the MLP).
+driver with its closures (none, GHOST's EDQNM eddy viscosity, the MLP as a
+pointwise stress model or as a spectral eddy viscosity).
 
 `MLP` wraps the ghost_mlp_* entry points (tensor-core forward, gradients and
 Adam of the 10 -> 64 -> 64 -> 6 GELU network); inputs and targets are CUDA
@@ -92,7 +93,7 @@ class MLP:
         return loss.value if want_loss else None
 
 
-MODELS = {"none": 0, "edqnm": 1, "mlp": 2}
+MODELS = {"none": 0, "edqnm": 1, "mlp": 2, "mlp_spectral": 3}
 
 
 class LES:
@@ -157,6 +158,20 @@ class LES:
                                           ctypes.c_float(delta), self._f(x, NIN)), "ghost_les_features")
         return x
 
+    def spectral_features(self, E, x=None):
+        """Inputs of the spectral network, (kc, 10), from a kinetic spectrum
+        E: a CUDA float64 tensor of the n/2+1 shell sums (spectrumc, kin = 1)."""
+        if not isinstance(E, torch.Tensor) or not E.is_cuda or E.dtype != torch.float64 or E.dim() != 1 \
+                or E.shape[0] != self.n // 2 + 1 or not E.is_contiguous():
+            raise ValueError(f"E: expected a contiguous CUDA float64 tensor of {self.n // 2 + 1} shells")
+        x = torch.empty((self.kc, NIN), dtype=torch.float32, device=E.device) if x is None else x
+        p = _dev(x, NIN, "x")
+        if x.shape[0] != self.kc:
+            raise ValueError(f"x: expected {self.kc} rows, got {x.shape[0]}")
+        check(self.lib.ghost_les_spectral_features(self.h, ctypes.c_void_p(E.data_ptr()), p),
+              "ghost_les_spectral_features")
+        return x
+
     def tau_force(self, tau, tau_scale: float = 1.0, f=(None, None, None), out=None):
         out = [self.g.czeros() for _ in range(3)] if out is None else out
         check(self.lib.ghost_les_tau_force(self.h, self._f(tau, NOUT), ctypes.c_float(tau_scale),
@@ -166,6 +181,10 @@ class LES:
 
     def set_model(self, model: str, mlp: MLP | None = None, grad_scale: float = 1.0, tau_scale: float = 1.0,
                   delta: float = 1.0, kolmo: float = 1.4):
+        """Select the closure.  "mlp": the stresses are the network's outputs
+        for the inputs (gradients times grad_scale, delta), times tau_scale;
+        "mlp_spectral": tve(k) is the network's first output for shell k
+        (inputs from spectral_features) times tau_scale sqrt(E(kc)/kc)."""
         check(self.lib.ghost_les_set_model(self.h, MODELS[model], mlp.h if mlp is not None else None,
                                            grad_scale, tau_scale, delta, kolmo), "ghost_les_set_model")
         self.model = model

@@ -13,10 +13,15 @@
    reference the LES is judged against.
 3. Training: the tensor-core MLP (ghost_mlp_*) with Adam on random batches
    of the samples (inputs scaled by their rms, stresses by theirs), the last
-   snapshots held out for validation.
+   snapshots held out for validation.  A second network of the same shape
+   learns a spectral eddy viscosity: from the shell inputs of each
+   snapshot's filtered spectrum (ghost_les_spectral_features) to the
+   a-priori nu_t(k) = -S(k)/D(k) of that snapshot, S the subgrid energy
+   transfer of shell k and D its sum of k^2 |ubar|^2, in units of
+   sqrt(E(kc)/kc).
 4. LES: from the filtered first snapshot, the coarse grid is advanced over
    the same time window with no closure, GHOST's EDQNM eddy viscosity, and
-   the trained network; spectra at the snapshot times.
+   the trained networks; spectra at the snapshot times.
 5. Report: spectrum errors of each LES against the filtered DNS
    (|E_les(k)/E_dns(k) - 1| over 1 <= k <= kc, time-averaged spectra), and
    the device time per unit of simulated time of the DNS and of each LES.
@@ -44,12 +49,15 @@ def spectrum_errors(E_les, E_dns, kc):
 
 def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_ratio=4, ord=4, spinup=4000,
         nsnap=40, snap_every=100, val_snaps=4, train_steps=4000, batch=65536, lr=2e-3, seed=7, kolmo=1.4,
-        models=("none", "edqnm", "mlp", "mlp_cal"), deviatoric=True, log=print):
+        models=("none", "edqnm", "mlp", "mlp_cal", "mlp_spectral"), deviatoric=True, spec_train_steps=3000,
+        spec_lr=3e-3, log=print):
     import numpy as np
     import torch
 
     from ghost_b200 import Ghost
     from ghost_b200.les import LES, MLP
+
+    to_np = lambda t: t.detach().cpu().numpy()  # noqa: E731
 
     nu_les = nu_dns if nu_les is None else nu_les
     if snap_every % les_dt_ratio:
@@ -60,7 +68,8 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     out = {"config": dict(dns_n=dns_n, les_n=les_n, kc=kc, nu_dns=nu_dns, nu_les=nu_les, dt=dt,
                           les_dt=dt * les_dt_ratio, ord=ord, spinup=spinup, nsnap=nsnap, snap_every=snap_every,
                           val_snaps=val_snaps, train_steps=train_steps, batch=batch, lr=lr, seed=seed,
-                          kolmo=kolmo, deviatoric=deviatoric, precision="fp32")}
+                          kolmo=kolmo, deviatoric=deviatoric, spec_train_steps=spec_train_steps, spec_lr=spec_lr,
+                          precision="fp32")}
 
     # ---- 1. DNS
     g = Ghost(dns_n, precision="fp32")
@@ -85,6 +94,7 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     X = torch.empty((nsnap, rows, 10), dtype=torch.float32, device=dev)
     T = torch.empty((nsnap, rows, 6), dtype=torch.float32, device=dev)
     E_dns = []
+    S_sgs, D_sgs = [], []
     v0 = None
     fl = [les.truncate(g, x) for x in f]
     for s in range(nsnap):
@@ -93,10 +103,19 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
         les.samples(g, *v, 1.0, X[s], T[s])
         ub = [les.truncate(g, x) for x in v]
         E_dns.append(c.spectrumc(*ub, 1, 0)[0])
+        # the subgrid energy transfer of each shell, S(k) = sum Re(ubar . conj F)
+        # with F = P(-div tau), and D(k) = sum k^2 |ubar|^2 (entrans's kin = 1
+        # and kin = 0 sums): an eddy force -nu_t(k) k^2 ubar transfers
+        # -nu_t(k) D(k), so nu_t(k) = -S(k)/D(k) reproduces it shell by shell
+        Fs = les.tau_force(T[s], 1.0)
+        S_sgs.append(c.entrans(*ub, *Fs, 1))
+        D_sgs.append(c.entrans(*ub, *ub, 0))
+        del Fs
         if s == 0:
             v0 = [x.clone() for x in ub]
     torch.cuda.synchronize()
     E_dns = np.array(E_dns)
+    S_sgs, D_sgs = np.array(S_sgs), np.array(D_sgs)
     t0 = spinup * dt
     # release the DNS grid before training and the LES runs
     del v, f
@@ -182,6 +201,38 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     del X, T, Xtr, Ttr, Xva, Tva
     torch.cuda.empty_cache()
 
+    # ---- 3b. the spectral network: shell inputs of each snapshot's filtered
+    # spectrum -> nu_t(k) / sqrt(E(kc)/kc), trained on the a-priori eddy
+    # viscosity of the training snapshots
+    nu_ap = -S_sgs[:, :kc] / D_sgs[:, :kc]
+    vel = np.sqrt(np.maximum(E_dns[:, kc - 1], 0.0) / kc)
+    xs = torch.cat([les.spectral_features(torch.tensor(E_dns[q], device=dev)) for q in range(nsnap)])
+    ys0 = nu_ap / vel[:, None]
+    so = float(1.0 / np.sqrt(np.mean(ys0[:ntr] ** 2)))
+    ys = torch.zeros((nsnap * kc, 6), dtype=torch.float32, device=dev)
+    ys[:, 0] = torch.tensor((ys0 * so).ravel(), dtype=torch.float32, device=dev)
+    xs_tr, ys_tr = xs[:ntr * kc].contiguous(), ys[:ntr * kc].contiguous()
+    xs_va, ys_va = xs[ntr * kc:].contiguous(), ys[ntr * kc:].contiguous()
+    mlp_s = MLP(seed + 1)
+    e0.record(stream)
+    for step in range(spec_train_steps):
+        lr_s = spec_lr * 0.5 * (1.0 + np.cos(np.pi * step / spec_train_steps))
+        mlp_s.train_step(xs_tr, ys_tr, lr_s, want_loss=False)
+    e1.record(stream)
+    e1.synchronize()
+    pred = to_np(mlp_s.forward(xs))[:, 0].reshape(nsnap, kc) / so
+    _, lva = mlp_s.gradients(xs_va, ys_va)
+    out["training_spectral"] = {
+        "samples": int(ntr * kc), "steps": spec_train_steps, "ms": e0.elapsed_time(e1), "out_scale": 1.0 / so,
+        # the losses count the five unused (zero-target) outputs too
+        "val_loss": lva, "val_loss_zero_model": float(ys_va.pow(2).mean()),
+        "nu_t_apriori_mean": (nu_ap[:ntr].mean(0)).tolist(),
+        "nu_t_apriori_std": (nu_ap[:ntr].std(0)).tolist(),
+        "nu_t_pred_val_mean": (pred[ntr:] * vel[ntr:, None]).mean(0).tolist(),
+    }
+    log(f"spectral network: val loss {lva:.4g} (zero model {out['training_spectral']['val_loss_zero_model']:.4g}); "
+        f"a-priori nu_t(kc) {nu_ap[:ntr, -1].mean():.4g}")
+
     # ---- 4. LES runs over the snapshot window
     les_dt = dt * les_dt_ratio
     sub = snap_every // les_dt_ratio
@@ -192,6 +243,8 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
             les.set_model("mlp", mlp, grad_scale=gs, tau_scale=1.0 / ts, delta=1.0)
         elif model == "mlp_cal":
             les.set_model("mlp", mlp, grad_scale=gs, tau_scale=cal / ts, delta=1.0)
+        elif model == "mlp_spectral":
+            les.set_model("mlp_spectral", mlp_s, tau_scale=1.0 / so)
         elif model == "edqnm":
             les.set_model("edqnm", kolmo=kolmo)
         else:
@@ -249,9 +302,11 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
         out["cost"][f"{model}_ms_per_time_unit"] = les_per_t
         out["cost"][f"{model}_speedup_vs_dns"] = dns_per_t / les_per_t if les_per_t > 0 else None
     out["mlp_params"] = mlp.params.tolist()
+    out["mlp_spectral_params"] = mlp_s.params.tolist()
     les.close()
     c.close()
     mlp.close()
+    mlp_s.close()
     return out
 
 
@@ -282,6 +337,7 @@ def main(argv=None):
     res["wall_s"] = time.time() - t
     summary = {k: res[k] for k in ("config", "dns", "cost")}
     summary["training"] = {k: v for k, v in res["training"].items() if k != "history"}
+    summary["training_spectral"] = {k: v for k, v in res["training_spectral"].items() if not isinstance(v, list)}
     summary["les"] = {m: {k: v for k, v in r.items() if k not in ("spectrum_time_avg",)} for m, r in res["les"].items()}
     for m in summary["les"].values():
         for k in ("error_time_avg", "error_final"):

@@ -483,10 +483,16 @@ int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, 
  *                    uses nu + tve(k), and vcorrect (:405-1629) then sets
  *                    every mode's energy from tepq, keeping its helicity;
  *   GHOST_LES_MLP    the learned subgrid stress: tau = mlp(inputs) gives
- *                    the force -P div tau (P the Leray projection). */
+ *                    the force -P div tau (P the Leray projection);
+ *   GHOST_LES_MLP_SPECTRAL  a learned spectral eddy viscosity: the network
+ *                    maps each resolved shell's inputs (ghost_les_spectral_features,
+ *                    from the current kinetic spectrum) to tve(k) = y0
+ *                    tau_scale sqrt(E(kc)/kc), applied as EDQNM's tve is
+ *                    (the update uses nu + tve(k)), without vcorrect. */
 #define GHOST_LES_NONE 0
 #define GHOST_LES_EDQNM 1
 #define GHOST_LES_MLP 2
+#define GHOST_LES_MLP_SPECTRAL 3
 typedef struct ghost_les ghost_les;
 int ghost_les_create(ghost_ctx *coarse, int kc, ghost_les **les);
 int ghost_les_destroy(ghost_les *les);
@@ -503,6 +509,14 @@ int ghost_les_samples(ghost_les *les, ghost_ctx *fine, const void *vx, const voi
 /* the closure inputs of a coarse velocity: gradients times grad_scale, delta */
 int ghost_les_features(ghost_les *les, const void *vx, const void *vy, const void *vz, float grad_scale, float delta,
                        float *x);
+/* the spectral network's inputs: E a device array of the n/2+1 shell sums
+ * of ghost_spectrumc (kin = 1; shell k at k-1), x a device float array of kc
+ * rows of GHOST_MLP_NIN, row k-1 for shell k: k/kc, (k/kc)^2,
+ * ln(E(k)/E(kc))/8, the local log-slope d ln E/d ln k /4 (centred, one-sided
+ * at k = 1 and kc), the log-slope from kc/2 to kc /4, ln(kc E(kc)/sum E)/8,
+ * exp(-(kc-k)/2), exp(-(kc-k)/8), 0, 0 (shell energies floored at 1e-30 of
+ * the resolved sum) */
+int ghost_les_spectral_features(ghost_les *les, const double *E, float *x);
 /* o = f + P(-div tau), tau[q][6] rows scaled by tau_scale (f may be NULL) */
 int ghost_les_tau_force(ghost_les *les, const float *tau, float tau_scale, const void *fx, const void *fy,
                         const void *fz, void *ox, void *oy, void *oz);

@@ -99,3 +99,32 @@ def helical(co, v, sign=1):
     cz = 1j * (kx * v[1] - ky * v[0])
     h = [0.5 * (a + sign * b / kn) for a, b in zip(v, (cx, cy, cz))]
     return [np.where(kk2 > 0, x, 0).astype(co.cdt) for x in h]
+
+
+def spectral_features(E, kc):
+    """Inputs of the spectral network (kc rows of 10, float32) from the shell
+    sums E (E[k-1] the shell k), as ghost_les_spectral_features defines them."""
+    E = np.asarray(E, dtype=np.float64)
+    tot = float(np.sum(np.maximum(E[:kc], 0.0)))
+    fl = 1e-30 * max(tot, 1e-300)
+    e = lambda k: max(E[k - 1], fl)  # noqa: E731
+    ec = e(kc)
+    kh = max(kc // 2, 1)
+    slope_c = np.log(ec / e(kh)) / np.log(kc / kh) if kh < kc else 0.0
+    frac = np.log(kc * ec / max(tot, fl))
+    x = np.zeros((kc, 10))
+    for k in range(1, kc + 1):
+        r = k / kc
+        ka, kb = (k - 1 if k > 1 else k), (k + 1 if k < kc else k)
+        sl = np.log(e(kb) / e(ka)) / np.log(kb / ka) if ka < kb else 0.0
+        x[k - 1, :8] = [r, r * r, np.log(e(k) / ec) / 8.0, sl / 4.0, slope_c / 4.0, frac / 8.0,
+                        np.exp(-(kc - k) / 2.0), np.exp(-(kc - k) / 8.0)]
+    return x.astype(np.float32)
+
+
+def spectral_tve(y0, E, kc, nb, out_scale):
+    """tve of the spectral closure: y0[k-1] out_scale sqrt(E(kc)/kc) for k <= kc, 0 beyond."""
+    s = out_scale * np.sqrt(max(float(E[kc - 1]), 0.0) / kc)
+    t = np.zeros(nb)
+    t[:kc] = np.asarray(y0, dtype=np.float64)[:kc] * s
+    return t

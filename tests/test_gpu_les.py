@@ -1,6 +1,7 @@
 """The LES kernels (ghost_les_*) against the oracle: sharp truncation,
 training samples (gradients and subgrid stresses), the closure forces
-(EDQNM eddy viscosity and the MLP stress divergence), the EDQNM LES run,
+(EDQNM eddy viscosity, the MLP stress divergence and the MLP spectral eddy
+viscosity), the EDQNM LES run,
 and that the closure-free LES is the plain HD run.
 
 Tolerances: FP64 1e-12 (single passes) to 1e-10 (runs of several steps),
@@ -160,6 +161,65 @@ def test_mlp_closure_force():
     y = M.forward(p, x, emulate=True).astype(np.float64)
     ref = LO.tau_force(co64, y, 0.05)
     assert rel_l2([to_host(a).astype(np.complex128) for a in F], ref) <= 2e-2
+
+
+def test_spectral_features():
+    import torch
+    fo, co, gf, gc, les = setup("fp64")
+    v = kolmogorov_field(co, 21, 10)
+    Ek, _ = co.spectrumc(*v, 1, 0)
+    x = les.spectral_features(torch.tensor(Ek, device="cuda"))
+    ref = LO.spectral_features(Ek, 10)
+    assert x.shape == (10, 10)
+    assert rel_l2(to_host(x), ref) <= 1e-7  # float32 output
+    assert np.all(ref[:, 8:] == 0) and ref[-1, 6] == 1.0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_spectral_closure_force(prec):
+    """The spectral closure: device spectrum -> shell inputs -> network ->
+    tve -> eddy-viscous force, against the oracle's eddy force with the tve
+    of the same chain (exact up to the force's arithmetic), and against the
+    oracle network (BF16 emulated) end to end."""
+    import torch
+    from ghost_b200.les import MLP
+    fo, co, gf, gc, les = setup(prec)
+    v = kolmogorov_field(co, 22, 10)
+    f = [rand_spectral(co, 23 + a) for a in range(3)]
+    p = M.glorot(24)
+    m = MLP(0)
+    m.params = p
+    les.set_model("mlp_spectral", m, tau_scale=0.02)
+    V = [to_dev(a) for a in v]
+    F = les.closure_force(1e-3, *V, [to_dev(a) for a in f])
+    Eg, _ = gc.spectrumc(*V, 1, 0)
+    yg = to_host(m.forward(les.spectral_features(torch.tensor(Eg, device="cuda"))))
+    tve = LO.spectral_tve(yg[:, 0], Eg, 10, 17, 0.02)
+    assert np.count_nonzero(tve) == 10
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    ref = LO.eddy_force(co, v, tve, f)
+    assert rel_l2([to_host(a) for a in F], ref) <= tol
+    # end to end against the oracle's spectrum, inputs and network
+    co64 = Oracle(32)
+    co64.set_kmax(100.0)
+    v64 = [a.astype(np.complex128) for a in v]
+    E64, _ = co64.spectrumc(*v64, 1, 0)
+    y64 = M.forward(p, LO.spectral_features(E64, 10), emulate=True).astype(np.float64)
+    tve64 = LO.spectral_tve(y64[:, 0], E64, 10, 17, 0.02)
+    ref64 = LO.eddy_force(co64, v64, tve64, [a.astype(np.complex128) for a in f])
+    assert rel_l2([to_host(a).astype(np.complex128) for a in F], ref64) <= 2e-2
+
+
+def test_spectral_closure_arguments():
+    from ghost_b200 import Ghost
+    from ghost_b200._lib import GhostError
+    from ghost_b200.les import LES, MLP
+    fo, co, gf, gc, les = setup("fp32")
+    with pytest.raises(GhostError):
+        les.set_model("mlp_spectral")  # no network
+    g3 = Ghost(32, precision="fp32")
+    with pytest.raises(GhostError):
+        LES(g3, 3).set_model("mlp_spectral", MLP(0))  # fewer than 4 shells
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
