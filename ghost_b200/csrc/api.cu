@@ -2688,23 +2688,40 @@ static int ensemble_class_step(ghost_ensemble *e, int q, int ord, double dt, boo
 }
 
 // ---- one launch per pass over all classes (ensemble.cuh)
-// Persistent CTAs of a multi-class launch: the occupancy of the kernel times
-// the SM count, shared among the classes in proportion to their tiles (each
-// gets at least one, none more than it has tiles).
-template <int MAXC>
-static int ens_split(ghost_ctx *c0, int per_sm, int ncls, const long *tiles, int *b0, int *nb) {
-  long tot_tiles = 0;
-  for (int q = 0; q < ncls; ++q) tot_tiles += tiles[q];
-  const long total = std::max<long>(ncls, (long)std::max(1, per_sm) * sm_count(c0));
-  int start = 0;
-  for (int q = 0; q < ncls; ++q) {
-    long k = tot_tiles > 0 ? (long)((double)total * (double)tiles[q] / (double)tot_tiles) : 1;
-    k = std::max<long>(1, std::min<long>(k, tiles[q]));
-    b0[q] = start;
-    nb[q] = (int)k;
-    start += (int)k;
+// Persistent CTAs of a multi-class launch: per_sm CTAs on each SM; the SM
+// slots are shared among the classes in proportion to their tiles (each
+// class gets at least one).  Returns the grid, per_sm times the SM count.
+template <class P> static int ens_split(ghost_ctx *c0, int per_sm, const long *tiles, P &p) {
+  const int nsm = sm_count(c0), nc = p.ncls;
+  long tot = 0;
+  for (int q = 0; q < nc; ++q) tot += tiles[q];
+  int sum = 0;
+  for (int q = 0; q < nc; ++q) {
+    p.nb[q] = std::max(1, (int)((double)nsm * (double)tiles[q] / (double)std::max<long>(1, tot)));
+    sum += p.nb[q];
   }
-  return start;
+  while (sum > nsm) {  // take slots from the class with the most
+    int m = 0;
+    for (int q = 1; q < nc; ++q)
+      if (p.nb[q] > p.nb[m]) m = q;
+    --p.nb[m];
+    --sum;
+  }
+  while (sum < nsm) {  // give slots to the class with the most tiles per slot
+    int m = 0;
+    for (int q = 1; q < nc; ++q)
+      if ((double)tiles[q] / p.nb[q] > (double)tiles[m] / p.nb[m]) m = q;
+    ++p.nb[m];
+    ++sum;
+  }
+  int start = 0;
+  for (int q = 0; q < nc; ++q) {
+    p.b0[q] = start;
+    start += p.nb[q];
+  }
+  p.nsm = nsm;
+  p.per = std::max(1, per_sm);
+  return p.per * nsm;
 }
 
 template <typename R> static int ens_T(int N, int E) { return N / (E < N ? E : N); }
@@ -2725,7 +2742,7 @@ static int ens_launch_z(ghost_ensemble *e, ZMulti<R, Op> &P, const long *tiles) 
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per = 0;
   GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
-  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  const int grid = ens_split(e->cls[0], per, tiles, P);
   kern<<<grid, kEnsThreads, smem, e->main>>>(P);
   return post_launch(e->cls[0]);
 }
@@ -2745,7 +2762,7 @@ template <typename R, int S> static int ens_launch_y(ghost_ensemble *e, YMulti<R
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per = 0;
   GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
-  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  const int grid = ens_split(e->cls[0], per, tiles, P);
   kern<<<grid, kEnsThreads, smem, e->main>>>(P);
   return post_launch(e->cls[0]);
 }
@@ -2765,7 +2782,7 @@ template <typename R> static int ens_launch_x(ghost_ensemble *e, XMulti<R> &P, c
   GB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per = 0;
   GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kEnsThreads, smem));
-  const int grid = ens_split<kEnsMaxCls>(e->cls[0], per, P.ncls, tiles, P.b0, P.nb);
+  const int grid = ens_split(e->cls[0], per, tiles, P);
   kern<<<grid, kEnsThreads, smem, e->main>>>(P);
   return post_launch(e->cls[0]);
 }
@@ -3025,7 +3042,7 @@ int ghost_ensemble_create(int nclasses, const int *n, const int *nruns, int prec
     ghost_ensemble_destroy(e);
     return st;
   }
-  e->multi = ens_multi_ok(e) ? 1 : 0;
+  e->multi = 0;  // ghost_ensemble_autotune keeps the faster mode
   *out = e;
   return GHOST_OK;
 }
@@ -3096,6 +3113,62 @@ int ghost_ensemble_init(ghost_ensemble *e, const int32_t *seeds, double kdn, dou
   return GHOST_OK;
 }
 
+// Times one step of every class in each mode (the classes' own launches on
+// their streams, and one launch per pass over all classes) on a copy of the
+// state and keeps the faster mode.
+static int ensemble_pick_mode(ghost_ensemble *e, int ord, double dt) {
+  void *save[kEnsMaxCls][3] = {};
+  int st = GHOST_OK;
+  for (int q = 0; q < e->ncls && st == GHOST_OK; ++q)
+    for (int k = 0; k < 3 && st == GHOST_OK; ++k) {
+      st = dalloc(&save[q][k], e->cls[q]->cbytes);
+      if (st == GHOST_OK && cudaMemcpyAsync(save[q][k], e->v[q][k], e->cls[q]->cbytes, cudaMemcpyDeviceToDevice,
+                                            e->main) != cudaSuccess)
+        st = fail(GHOST_ERR_CUDA, "state copy failed");
+    }
+  auto restore = [&] {
+    for (int q = 0; q < e->ncls; ++q)
+      for (int k = 0; k < 3; ++k)
+        if (save[q][k]) cudaMemcpyAsync(e->v[q][k], save[q][k], e->cls[q]->cbytes, cudaMemcpyDeviceToDevice, e->main);
+  };
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (st == GHOST_OK && (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess))
+    st = fail(GHOST_ERR_CUDA, "event creation failed");
+  float t[2] = {0.f, 0.f};
+  for (int multi = 0; multi < 2 && st == GHOST_OK; ++multi) {
+    for (int rep = 0; rep < 3 && st == GHOST_OK; ++rep) {
+      restore();
+      cudaEventRecord(a, e->main);
+      if (multi) {
+        st = ensemble_multi_step(e, ord, dt, true);
+      } else {
+        cudaEventRecord(e->fork, e->main);
+        for (int q = 0; q < e->ncls && st == GHOST_OK; ++q) {
+          cudaStreamWaitEvent(e->streams[q], e->fork, 0);
+          st = ensemble_class_step(e, q, ord, dt, true);
+          cudaEventRecord(e->join[q], e->streams[q]);
+          cudaStreamWaitEvent(e->main, e->join[q], 0);
+        }
+      }
+      cudaEventRecord(b, e->main);
+      if (cudaEventSynchronize(b) != cudaSuccess) st = fail(GHOST_ERR_CUDA, "mode timing failed");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) t[multi] += ms;  // the first repetition warms up
+    }
+  }
+  restore();
+  cudaStreamSynchronize(e->main);
+  for (int q = 0; q < e->ncls; ++q)
+    for (int k = 0; k < 3; ++k) cudaFree(save[q][k]);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  GB_CHECK(st);
+  e->multi = t[1] < t[0] ? 1 : 0;
+  for (int q = 0; q < e->ncls; ++q) GB_CHECK(check_status(e->cls[q]));
+  return GHOST_OK;
+}
+
 int ghost_ensemble_autotune(ghost_ensemble *e, int ord, double dt, int *cfg_out) {
   if (!e || ord < 1) return fail(GHOST_ERR_ARG, "bad argument");
   for (int q = 0; q < e->ncls; ++q) {
@@ -3141,6 +3214,7 @@ int ghost_ensemble_autotune(ghost_ensemble *e, int ord, double dt, int *cfg_out)
     GB_CHECK(st);
     GB_CHECK(check_status(c));
   }
+  if (ens_multi_ok(e)) GB_CHECK(ensemble_pick_mode(e, ord, dt));
   if (e->exec) {  // a new tile choice needs a new graph
     cudaGraphExecDestroy(e->exec);
     e->exec = nullptr;

@@ -3,10 +3,14 @@
 // An ensemble holds batched contexts of different grids (config 3: 128 runs
 // of 32^3, 96 of 64^3, 32 of 128^3).  Each pass of the fused substep (Z
 // inverse, Y inverse, X, Y forward, Z forward) runs as ONE kernel over all
-// classes: CTA b works for the class c whose range [b0[c], b0[c] + nb[c])
-// holds it, as CTA b - b0[c] of that class's nb[c] persistent CTAs, with the
-// class's own line length (a switch over the supported lengths picks the
-// templated pass body).  Every class runs the same CTA size, NTH threads:
+// classes.  The launch has per CTAs for each of nsm SM slots; class c owns
+// the slots [b0[c], b0[c] + nb[c]), and CTA b (slot b % nsm, round b / nsm)
+// works for the class owning its slot, as CTA round nb[c] + slot - b0[c] of
+// that class's per nb[c] persistent CTAs, with the class's own line length
+// (a switch over the supported lengths picks the templated pass body).  The
+// hardware fills the SMs slot by slot, round after round, so the CTAs
+// resident on one SM tend to run one class's code: the instruction cache
+// then holds one pass body per SM instead of several.  Every class runs the same CTA size, NTH threads:
 //   Z pass: NTH / (N/E) lines of N points per tile;
 //   Y pass: BZ z-lines of NTH / (BZ N/E) consecutive kx per tile;
 //   X pass: BZ z-values of NTH / (BZ (N/2)/E) consecutive y per tile;
@@ -23,12 +27,17 @@ template <typename R> constexpr int ens_zE() { return sizeof(R) == 4 ? 8 : 4; }
 template <typename R> constexpr int ens_xE() { return sizeof(R) == 4 ? 8 : 4; }
 template <typename R> constexpr int ens_xBZ() { return sizeof(R) == 4 ? 8 : 4; }
 constexpr int kEnsYBZ = 8;
+constexpr int kEnsXStages = 4;  // the X pass's ring: four fields in flight, as the classes' own launches
 
-// the class a CTA works for, and its index within that class's CTAs
-__device__ __forceinline__ int ens_class(const int *b0, int ncls) {
+// the class a CTA works for, its index among that class's CTAs, and their number
+struct EnsCta {
+  int c, vb, nvb;
+};
+template <class P> __device__ __forceinline__ EnsCta ens_cta(const P &p) {
+  const int slot = (int)blockIdx.x % p.nsm, round = (int)blockIdx.x / p.nsm;
   int c = 0;
-  while (c + 1 < ncls && (int)blockIdx.x >= b0[c + 1]) ++c;
-  return c;
+  while (c + 1 < p.ncls && slot >= p.b0[c + 1]) ++c;
+  return EnsCta{c, round * p.nb[c] + (slot - p.b0[c]), p.per * p.nb[c]};
 }
 
 // ------------------------------------------------------------------ Z
@@ -40,7 +49,7 @@ template <typename R, class Op> struct ZClass {
   PipeCtl ctl;
 };
 template <typename R, class Op> struct ZMulti {
-  int ncls;
+  int ncls, nsm, per;
   int n[kEnsMaxCls], b0[kEnsMaxCls], nb[kEnsMaxCls];
   ZClass<R, Op> cl[kEnsMaxCls];
 };
@@ -57,13 +66,12 @@ template <typename R, int N, class Op> __device__ __forceinline__ void ens_z_run
 
 template <typename R, class Op>
 __global__ void __launch_bounds__(kEnsThreads) zmulti_kernel(const __grid_constant__ ZMulti<R, Op> P) {
-  const int c = ens_class(P.b0, P.ncls);
-  const int vb = (int)blockIdx.x - P.b0[c];
-  switch (P.n[c]) {
-    case 16: ens_z_run<R, 16>(P.cl[c], vb, P.nb[c]); break;
-    case 32: ens_z_run<R, 32>(P.cl[c], vb, P.nb[c]); break;
-    case 64: ens_z_run<R, 64>(P.cl[c], vb, P.nb[c]); break;
-    case 128: ens_z_run<R, 128>(P.cl[c], vb, P.nb[c]); break;
+  const EnsCta k = ens_cta(P);
+  switch (P.n[k.c]) {
+    case 16: ens_z_run<R, 16>(P.cl[k.c], k.vb, k.nvb); break;
+    case 32: ens_z_run<R, 32>(P.cl[k.c], k.vb, k.nvb); break;
+    case 64: ens_z_run<R, 64>(P.cl[k.c], k.vb, k.nvb); break;
+    case 128: ens_z_run<R, 128>(P.cl[k.c], k.vb, k.nvb); break;
   }
 }
 
@@ -77,7 +85,7 @@ template <typename R> struct YClass {
   PipeCtl ctl;
 };
 template <typename R> struct YMulti {
-  int ncls;
+  int ncls, nsm, per;
   int n[kEnsMaxCls], b0[kEnsMaxCls], nb[kEnsMaxCls];
   YClass<R> cl[kEnsMaxCls];
 };
@@ -98,13 +106,12 @@ template <typename R, int N, int S> __device__ __forceinline__ void ens_y_run(co
 
 template <typename R, int S>
 __global__ void __launch_bounds__(kEnsThreads) ymulti_kernel(const __grid_constant__ YMulti<R> P) {
-  const int c = ens_class(P.b0, P.ncls);
-  const int vb = (int)blockIdx.x - P.b0[c];
-  switch (P.n[c]) {
-    case 16: ens_y_run<R, 16, S>(P.cl[c], vb, P.nb[c]); break;
-    case 32: ens_y_run<R, 32, S>(P.cl[c], vb, P.nb[c]); break;
-    case 64: ens_y_run<R, 64, S>(P.cl[c], vb, P.nb[c]); break;
-    case 128: ens_y_run<R, 128, S>(P.cl[c], vb, P.nb[c]); break;
+  const EnsCta k = ens_cta(P);
+  switch (P.n[k.c]) {
+    case 16: ens_y_run<R, 16, S>(P.cl[k.c], k.vb, k.nvb); break;
+    case 32: ens_y_run<R, 32, S>(P.cl[k.c], k.vb, k.nvb); break;
+    case 64: ens_y_run<R, 64, S>(P.cl[k.c], k.vb, k.nvb); break;
+    case 128: ens_y_run<R, 128, S>(P.cl[k.c], k.vb, k.nvb); break;
   }
 }
 
@@ -118,7 +125,7 @@ template <typename R> struct XClass {
   PipeCtl ctl;
 };
 template <typename R> struct XMulti {
-  int ncls;
+  int ncls, nsm, per;
   int n[kEnsMaxCls], b0[kEnsMaxCls], nb[kEnsMaxCls];
   XClass<R> cl[kEnsMaxCls];
 };
@@ -127,23 +134,22 @@ template <typename R, int NX> constexpr int ens_x_yb() {
   return kEnsThreads / (ens_xBZ<R>() * (NX / 2 / ens_x_E<R, NX>()));
 }
 template <typename R, int NX> constexpr size_t ens_x_smem() {
-  return XGeom<R, NX, ens_xBZ<R>(), ens_x_yb<R, NX>()>::smem_bytes(3);
+  return XGeom<R, NX, ens_xBZ<R>(), ens_x_yb<R, NX>()>::smem_bytes(kEnsXStages);
 }
 
 template <typename R, int NX> __device__ __forceinline__ void ens_x_run(const XClass<R> &k, int vb, int nvb) {
-  xpipe_nl_body<R, NX, ens_x_E<R, NX>(), ens_xBZ<R>(), 0, 3, ens_x_yb<R, NX>()>(
+  xpipe_nl_body<R, NX, ens_x_E<R, NX>(), ens_xBZ<R>(), 0, kEnsXStages, ens_x_yb<R, NX>()>(
       vb, nvb, k.maps, k.out, k.tw, k.ny, k.nz, k.scale, k.rows, k.nbox, k.rb, k.nruns, k.nxh, k.ctl);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(kEnsThreads) xmulti_kernel(const __grid_constant__ XMulti<R> P) {
-  const int c = ens_class(P.b0, P.ncls);
-  const int vb = (int)blockIdx.x - P.b0[c];
-  switch (P.n[c]) {
-    case 16: ens_x_run<R, 16>(P.cl[c], vb, P.nb[c]); break;
-    case 32: ens_x_run<R, 32>(P.cl[c], vb, P.nb[c]); break;
-    case 64: ens_x_run<R, 64>(P.cl[c], vb, P.nb[c]); break;
-    case 128: ens_x_run<R, 128>(P.cl[c], vb, P.nb[c]); break;
+  const EnsCta k = ens_cta(P);
+  switch (P.n[k.c]) {
+    case 16: ens_x_run<R, 16>(P.cl[k.c], k.vb, k.nvb); break;
+    case 32: ens_x_run<R, 32>(P.cl[k.c], k.vb, k.nvb); break;
+    case 64: ens_x_run<R, 64>(P.cl[k.c], k.vb, k.nvb); break;
+    case 128: ens_x_run<R, 128>(P.cl[k.c], k.vb, k.nvb); break;
   }
 }
 

@@ -80,6 +80,7 @@ def main(argv=None):
     ens = Ensemble([sizes[q] for q in keep], [counts[q] for q in keep], precision=a.precision)
     ens.init([seeds[r] for r in mine], nu[mine])
     cfg = ens.autotune(a.ord, a.dt)
+    tuned_mode = "multi" if ens.mode() else "per-class"
     setup = time.perf_counter() - t0
     e0 = None
     modes = {"both": ["multi", "per-class"], "multi": ["multi"], "per-class": ["per-class"]}[a.mode]
@@ -121,7 +122,7 @@ def main(argv=None):
                         f"{a.precision}",
             "gpus": world, "steps": a.steps, "seconds": wall, "run_steps_per_s": total * a.steps / wall,
             "ensemble_steps_per_s": a.steps / wall, "gridpoint_steps_per_s": points * a.steps / wall,
-            "mode": best,
+            "mode": best, "autotuned_mode": tuned_mode,
             "modes": {m: {"seconds": w, "run_steps_per_s": total * a.steps / w,
                           "gridpoint_steps_per_s": points * a.steps / w} for m, w in timing.items()},
             "tile_cfg": cfg, "setup_s": setup,

@@ -405,18 +405,21 @@ int ghost_ensemble_class(ghost_ensemble *ens, int c, ghost_ctx **ctx);
 int ghost_ensemble_init(ghost_ensemble *ens, const int32_t *seeds, double kdn, double kup_frac, int shape,
                         double amp, const double *nu);
 /* Times each tile variant of every class on a copy of its state and keeps
- * the fastest; cfg_out[c] receives the choice (may be NULL). */
+ * the fastest; cfg_out[c] receives the choice (may be NULL).  Then, where
+ * one launch per pass is allowed (ghost_ensemble_set_mode), times a step in
+ * each mode and keeps the faster (ghost_ensemble_get_mode reports it). */
 int ghost_ensemble_autotune(ghost_ensemble *ens, int ord, double dt, int *cfg_out);
 /* nsteps RK steps of every run; after one uncaptured step the step is a
  * replayed CUDA graph */
 int ghost_ensemble_run(ghost_ensemble *ens, int nsteps, int ord, double dt);
-/* How the ensemble runs its passes: multi = 1 (the default where allowed:
- * at most 4 classes of 16..128 points per side) makes each of the five
- * passes of a substep one kernel launch over every class, each CTA working
- * for one class (a tile table splits the persistent CTAs in proportion to
- * the classes' tiles); multi = 0 runs every class's own launches on its own
- * stream (the per-class tile variants of ghost_ensemble_autotune apply
- * there).  Both give the same bits. */
+/* How the ensemble runs its passes: multi = 1 (allowed for at most 4
+ * classes of 16..128 points per side) makes each of the five passes of a
+ * substep one kernel launch over every class, each CTA working for one
+ * class (a tile table splits the persistent CTAs in proportion to the
+ * classes' tiles); multi = 0 (the default) runs every class's own launches
+ * on its own stream, with the per-class tile variants of
+ * ghost_ensemble_autotune.  Both give the same bits.  Where multi = 1 is
+ * allowed, ghost_ensemble_autotune times both modes and keeps the faster. */
 int ghost_ensemble_set_mode(ghost_ensemble *ens, int multi);
 int ghost_ensemble_get_mode(const ghost_ensemble *ens, int *multi);
 /* per-run energy(kin), runs in class order */

@@ -194,7 +194,8 @@ def test_spectral_closure_force(prec):
     F = les.closure_force(1e-3, *V, [to_dev(a) for a in f])
     Eg, _ = gc.spectrumc(*V, 1, 0)
     yg = to_host(m.forward(les.spectral_features(torch.tensor(Eg, device="cuda"))))
-    tve = LO.spectral_tve(yg[:, 0], Eg, 10, 17, 0.02)
+    # the closure holds tau_scale as a float
+    tve = LO.spectral_tve(yg[:, 0], Eg, 10, 17, float(np.float32(0.02)))
     assert np.count_nonzero(tve) == 10
     tol = 1e-12 if prec == "fp64" else 1e-5
     ref = LO.eddy_force(co, v, tve, f)
