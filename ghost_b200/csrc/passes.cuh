@@ -531,7 +531,9 @@ __device__ __forceinline__ void ypipe_body(int vb, int nvb, const FieldMaps &map
   C *xb = stage + STAGES * G::stage_elems;  // second exchange buffer (DUAL)
   C *tw = xb + (DUAL ? G::stage_elems : 0);
   uint64_t *bars = reinterpret_cast<uint64_t *>(tw + N);
-  const int tid = threadIdx.x, l = tid % BZ, t = (tid / BZ) % T, kb = tid / (BZ * T);
+  // with one kx per tile the kx offset is the constant 0 and every line is live
+  const int tid = threadIdx.x, l = tid % BZ, t = KB == 1 ? tid / BZ : (tid / BZ) % T;
+  const int kb = KB == 1 ? 0 : tid / (BZ * T);
   const int nzb = nz / BZ;
   const int nig = (ni + KB - 1) / KB;  // groups of KB kx indices
   const int ntiles = nzb * nig * nruns * nf;
@@ -572,19 +574,21 @@ __device__ __forceinline__ void ypipe_body(int vb, int nvb, const FieldMaps &map
     if (tile >= ntiles || tid != 0) return;
     const Tile tl = tile_of(tile);
     const int s = k % STAGES;
+    // live rows of each kx of the tile, read once (none past the last kx)
+    int jp[KB], jn[KB];
     uint32_t nbox = 0;
-    for (int b = 0; b < KB && tl.ii + b < ni; ++b) {
-      int jp, jn;
-      rows_of(tl.ii + b, jp, jn);
-      nbox += (jp + rb - 1) / rb + (jn + rb - 1) / rb;
+#pragma unroll
+    for (int b = 0; b < KB; ++b) {
+      jp[b] = jn[b] = 0;
+      if (KB == 1 || tl.ii + b < ni) rows_of(tl.ii + b, jp[b], jn[b]);
+      nbox += (jp[b] + rb - 1) / rb + (jn[b] + rb - 1) / rb;
     }
     fence_proxy_async();
     mbar_arrive_expect_tx(&bars[s], nbox * (uint32_t)rb * BZ * (uint32_t)sizeof(C));
-    for (int b = 0; b < KB && tl.ii + b < ni; ++b) {
-      int jp, jn;
-      rows_of(tl.ii + b, jp, jn);
+#pragma unroll
+    for (int b = 0; b < KB; ++b) {
       C *dst = stage + (size_t)s * G::stage_elems + (size_t)b * BZ * N;
-      const int nb_top = (jp + rb - 1) / rb, nb_bot = (jn + rb - 1) / rb;
+      const int nb_top = (jp[b] + rb - 1) / rb, nb_bot = (jn[b] + rb - 1) / rb;
       for (int q = 0; q < nb_top; ++q)
         tma_load_3d(dst + (size_t)q * rb * BZ, &maps.m[tl.f], tl.zb * BZ * U, q * rb, tl.i + b, &bars[s]);
       for (int q = 0; q < nb_bot; ++q) {
@@ -619,7 +623,7 @@ __device__ __forceinline__ void ypipe_body(int vb, int nvb, const FieldMaps &map
     const Tile tl = tile_of(tile);
     // this thread's kx: beyond the last one (a short last group) its line is
     // transformed from zeros and not stored
-    const bool act = tl.ii + kb < ni;
+    const bool act = KB == 1 || tl.ii + kb < ni;
     int jp = N, jn = 0;
     if (jpos && act) {
       jp = jpos[tl.ii + kb];
@@ -788,7 +792,8 @@ __device__ __forceinline__ void xpipe_nl_body(int vb, int nvb, const FieldMaps &
   C *tw = stage + STAGES * G::stage_elems;
   C *xb = tw + NX;
   uint64_t *bars = reinterpret_cast<uint64_t *>(xb + 2 * (size_t)M * LW);
-  const int tid = threadIdx.x, l = tid % BZ, t = (tid / BZ) % T, yb = tid / (BZ * T);
+  const int tid = threadIdx.x, l = tid % BZ, t = YB == 1 ? tid / BZ : (tid / BZ) % T;
+  const int yb = YB == 1 ? 0 : tid / (BZ * T);
   const int lw = yb * BZ + l;  // this thread's line within the tile
   const int nzb = nz / BZ, nyg = ny / YB;
   const int ntiles = nzb * nyg * nruns;
