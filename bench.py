@@ -508,8 +508,10 @@ def run_ours(args, ws, rank, local):
 
 def run_slab(args, ws, rank, local):
     """N > 1: one n^3 run split over the ranks in GHOST's slab layout
-    (kx-slabs of the spectral fields, z-slabs for the x pass), two NCCL
-    all-to-alls per substep (ghost_b200.slab).  Every rank generates the
+    (kx-slabs of the spectral fields, z-slabs for the x pass), NCCL
+    all-to-alls per substep in field groups overlapped with the Y passes
+    (ghost_b200.slab; the plain schedule of two all-to-alls per substep is
+    timed beside it).  Every rank generates the
     same seeded fields as the one-GPU run and keeps its kx-slab."""
     import torch
 
@@ -551,12 +553,17 @@ def run_slab(args, ws, rank, local):
     s32, v32, f32 = setup("fp32")
     clocks.start()
     ms32, launches = timed(s32, v32, f32, args.steps, args.warmup)
-    # exchange time per substep (a separate, untimed step with events around the all-to-alls)
+    # the plain schedule (one synchronous all-to-all per direction, own block
+    # through the buffers) for comparison, and its exchange time per substep
+    # (an extra step with events around the all-to-alls)
+    s32.set_overlap(False)
+    ms32_plain, _ = timed(s32, v32, f32, args.steps, 1)
     ev = []
     s32.run(1, ORD, DT, NU, *v32, *f32, exchange_events=ev)
     torch.cuda.synchronize()
     xch = max_over_ranks(ws, sum(a.elapsed_time(b) for a, b in ev) / ORD)
     barrier(ws)
+    s32.set_overlap(True)
     # e2e: every step copies this rank's slabs of v and f in from pinned host
     # memory and v out, around the same library calls
     hv = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in v32]
@@ -603,6 +610,9 @@ def run_slab(args, ws, rank, local):
             "fp64": {"value": steps64, "unit": "steps/s", "ms_per_step": ms64 / steps64_n},
             "fp32_over_fp64": steps32 / steps64,
             "exchange_ms_per_substep": xch,
+            "schedule": "overlapped: v and curl v exchanged as two asynchronous all-to-alls, the products one field "
+                        "at a time, each behind the Y passes of the others; own block copied field to field",
+            "plain_schedule_ms_per_step": ms32_plain / args.steps,
             "e2e": {"value": args.e2e_steps / (ms_e2e * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches * ws,

@@ -114,6 +114,11 @@ SIGNATURES = {
     "ghost_slab_hd_back": [P, I, D, D, I, PP, PP, PP, PP],
     "ghost_slab_pack": [P, I, I, I, PP, P],
     "ghost_slab_unpack": [P, I, I, I, P, PP],
+    "ghost_slab_set_self_direct": [P, I],
+    "ghost_slab_exchange_self": [P, I, I, I, PP, PP],
+    "ghost_slab_hd_front_z": [P, PP, PP, I, I, PP],
+    "ghost_slab_ypass": [P, I, I, I, PP],
+    "ghost_slab_hd_back_z": [P, I, D, D, I, PP, PP, PP, PP],
     "ghost_ctx_set_tile_cfg": [P, I],
     "ghost_ctx_get_tile_cfg": [P, ctypes.POINTER(ctypes.c_int)],
     "ghost_hd_autotune": [P, I, D, D, P, P, P, P, P, P, ctypes.POINTER(ctypes.c_int)],

@@ -3300,6 +3300,7 @@ struct ghost_slab {
   int rank = 0, nranks = 1;
   std::vector<int> ista, nxhl, ksta, nzl;  // per rank, 0-based starts
   int rows_glob = 0;  // kx rows 0..rows_glob-1 hold every mode that survives the truncation
+  bool self_direct = false;  // pack/unpack skip the rank's own block (ghost_slab_exchange_self moves it)
   // kx rows of rank r that a pruned exchange moves: the live prefix of its slab
   int live_rows(int r, bool prune) const {
     return prune ? std::max(0, std::min(rows_glob - ista[r], nxhl[r])) : nxhl[r];
@@ -3351,7 +3352,7 @@ template <typename R> static int slab_rows_glob(const ghost_ctx *c) {
 
 template <typename R>
 static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3], int copy, bool prune,
-                          void *const w[6]) {
+                          void *const w[6], bool with_y = true) {
   Prune pr;
   GB_CHECK(prune_plan<R>(c, prune, &pr));
   ZInv<R, 0> zi{};
@@ -3363,19 +3364,28 @@ static int slab_front_dev(ghost_ctx *c, const void *const v[3], void *const C[3]
   zi.kp = kparams<R>(c);
   zi.copy = copy;
   GB_CHECK(launch_z<R>(c, zi, pr));
+  if (!with_y) return GHOST_OK;
   Fields<R> fy{};
   for (int q = 0; q < 6; ++q) fy.p[q] = (cx<R> *)w[q];
   return launch_y<R, +1>(c, fy, 6, pr);
 }
 
+// the Y pass of nf fields of the kx-slab (sign +1 inverse, -1 forward)
 template <typename R>
-static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, bool prune, void *const w[3], void *const v[3],
-                         const void *const C[3], const void *const f[3]) {
+static int slab_y_dev(ghost_ctx *c, int sign, int nf, bool prune, void *const *w) {
   Prune pr;
   GB_CHECK(prune_plan<R>(c, prune, &pr));
   Fields<R> fy{};
-  for (int q = 0; q < 3; ++q) fy.p[q] = (cx<R> *)w[q];
-  GB_CHECK((launch_y<R, -1>(c, fy, 3, pr)));
+  for (int q = 0; q < nf; ++q) fy.p[q] = (cx<R> *)w[q];
+  return sign > 0 ? launch_y<R, +1>(c, fy, nf, pr) : launch_y<R, -1>(c, fy, nf, pr);
+}
+
+// Z forward and the truncated update (the back phase without its Y pass)
+template <typename R>
+static int slab_back_z_dev(ghost_ctx *c, int o, double dt, double nu, bool prune, void *const w[3], void *const v[3],
+                           const void *const C[3], const void *const f[3]) {
+  Prune pr;
+  GB_CHECK(prune_plan<R>(c, prune, &pr));
   ZFwdHD<R> zf{};
   for (int q = 0; q < 3; ++q) {
     zf.nl.p[q] = (const cx<R> *)w[q];
@@ -3388,6 +3398,13 @@ static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, bool prune, 
   zf.nu = (R)nu;
   zf.rmp = (R)1 / (R)o;
   return launch_z<R>(c, zf, pr);
+}
+
+template <typename R>
+static int slab_back_dev(ghost_ctx *c, int o, double dt, double nu, bool prune, void *const w[3], void *const v[3],
+                         const void *const C[3], const void *const f[3]) {
+  GB_CHECK(slab_y_dev<R>(c, -1, 3, prune, w));
+  return slab_back_z_dev<R>(c, o, dt, nu, prune, w, v, C, f);
 }
 
 }  // namespace gb
@@ -3549,7 +3566,7 @@ int ghost_slab_pack(ghost_slab *s, int dir, int nf, int prune, const void *const
   const bool pr = prune != 0;
   unsigned char *dst = (unsigned char *)send;
   for (int p = 0; p < s->nranks; ++p)
-    for (int f = 0; f < nf; ++f) {
+    for (int f = 0; f < nf && !(s->self_direct && p == me); ++f) {
       const unsigned char *src = (const unsigned char *)fields[f];
       if (dir == 0) {  // my (live) kx rows, p's z planes, from a (nxh_loc, ny, nz) field
         const size_t w = (size_t)s->nzl[p] * es, h = (size_t)s->live_rows(me, pr) * ny;
@@ -3579,7 +3596,7 @@ int ghost_slab_unpack(ghost_slab *s, int dir, int nf, int prune, const void *rec
   const bool pr = prune != 0;
   const unsigned char *src = (const unsigned char *)recv;
   for (int p = 0; p < s->nranks; ++p)
-    for (int f = 0; f < nf; ++f) {
+    for (int f = 0; f < nf && !(s->self_direct && p == me); ++f) {
       unsigned char *dst = (unsigned char *)fields[f];
       if (dir == 0) {  // p's (live) kx rows of my z planes: rows ista_p.. of a (nxh, ny, nz_loc) field
         const size_t n = (size_t)s->live_rows(p, pr) * ny * s->nzl[me] * es;
@@ -3596,6 +3613,70 @@ int ghost_slab_unpack(ghost_slab *s, int dir, int nf, int prune, const void *rec
       }
     }
   return GHOST_OK;
+}
+
+int ghost_slab_set_self_direct(ghost_slab *s, int on) {
+  SLAB_CHECK(s);
+  s->self_direct = on != 0;
+  return GHOST_OK;
+}
+
+int ghost_slab_exchange_self(ghost_slab *s, int dir, int nf, int prune, const void *const *in, void *const *out) {
+  SLAB_CHECK(s);
+  if ((dir != 0 && dir != 1) || nf < 1 || nf > 16) return fail(GHOST_ERR_ARG, "exchange_self dir=%d nf=%d", dir, nf);
+  GB_CHECK(slab_dev_ptrs(in, nf));
+  GB_CHECK(slab_dev_ptrs((const void *const *)out, nf));
+  ghost_ctx *c = s->spec;
+  const size_t es = c->precision == GHOST_SINGLE ? 8 : 16;
+  const int me = s->rank, ny = c->ny, nz = c->nz_glob;
+  // my live kx rows of my z planes: (rows, ny, nz) at z offset ksta in the
+  // kx-slab, (rows, ny, nz_loc) at row ista in the z-slab
+  const size_t w = (size_t)s->nzl[me] * es, h = (size_t)s->live_rows(me, prune != 0) * ny;
+  if (h == 0) return GHOST_OK;
+  const size_t zoff = (size_t)s->ksta[me] * es, roff = (size_t)s->ista[me] * ny * w;
+  for (int f = 0; f < nf; ++f) {
+    const unsigned char *src = (const unsigned char *)in[f];
+    unsigned char *dst = (unsigned char *)out[f];
+    if (dir == 0)
+      GB_CUDA(cudaMemcpy2DAsync(dst + roff, w, src + zoff, (size_t)nz * es, w, h, cudaMemcpyDeviceToDevice, c->stream));
+    else
+      GB_CUDA(cudaMemcpy2DAsync(dst + zoff, (size_t)nz * es, src + roff, w, w, h, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return GHOST_OK;
+}
+
+int ghost_slab_hd_front_z(ghost_slab *s, const void *const v[3], void *const C[3], int copy, int prune,
+                          void *const w[6]) {
+  SLAB_CHECK(s);
+  GB_CHECK(slab_dev_ptrs(v, 3));
+  GB_CHECK(slab_dev_ptrs((const void *const *)w, 6));
+  if (copy) GB_CHECK(slab_dev_ptrs((const void *const *)C, 3));
+  ghost_ctx *c = s->spec;
+  return c->precision == GHOST_SINGLE ? slab_front_dev<float>(c, v, C, copy, prune != 0, w, false)
+                                      : slab_front_dev<double>(c, v, C, copy, prune != 0, w, false);
+}
+
+int ghost_slab_ypass(ghost_slab *s, int sign, int nf, int prune, void *const *fields) {
+  SLAB_CHECK(s);
+  if ((sign != 1 && sign != -1) || nf < 1 || nf > 9) return fail(GHOST_ERR_ARG, "ypass sign=%d nf=%d", sign, nf);
+  GB_CHECK(slab_dev_ptrs((const void *const *)fields, nf));
+  ghost_ctx *c = s->spec;
+  return c->precision == GHOST_SINGLE ? slab_y_dev<float>(c, sign, nf, prune != 0, fields)
+                                      : slab_y_dev<double>(c, sign, nf, prune != 0, fields);
+}
+
+int ghost_slab_hd_back_z(ghost_slab *s, int o, double dt, double nu, int prune, void *const w[3], void *const v[3],
+                         const void *const C[3], const void *const f[3]) {
+  SLAB_CHECK(s);
+  if (o < 1) return fail(GHOST_ERR_ARG, "substep o=%d", o);
+  GB_CHECK(slab_dev_ptrs((const void *const *)w, 3));
+  GB_CHECK(slab_dev_ptrs((const void *const *)v, 3));
+  GB_CHECK(slab_dev_ptrs(C, 3));
+  if (f && !f[0]) f = nullptr;
+  if (f) GB_CHECK(slab_dev_ptrs(f, 3));
+  ghost_ctx *c = s->spec;
+  return c->precision == GHOST_SINGLE ? slab_back_z_dev<float>(c, o, dt, nu, prune != 0, w, v, C, f)
+                                      : slab_back_z_dev<double>(c, o, dt, nu, prune != 0, w, v, C, f);
 }
 
 }  // extern "C"

@@ -456,6 +456,41 @@
          TYPE(C_PTR) :: fields(*)
          INTEGER(C_INT) :: s
        END FUNCTION
+       FUNCTION ghost_slab_set_self_direct(slab,on) BIND(C,name="ghost_slab_set_self_direct") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: on
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_exchange_self(slab,dir,nf,prune,fin,fout) BIND(C,name="ghost_slab_exchange_self") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: dir, nf, prune
+         TYPE(C_PTR) :: fin(*), fout(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_hd_front_z(slab,v,c,copy,prune,w) BIND(C,name="ghost_slab_hd_front_z") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         TYPE(C_PTR) :: v(3), c(3), w(6)
+         INTEGER(C_INT), VALUE :: copy, prune
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_ypass(slab,sgn,nf,prune,fields) BIND(C,name="ghost_slab_ypass") RESULT(s)
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: sgn, nf, prune
+         TYPE(C_PTR) :: fields(*)
+         INTEGER(C_INT) :: s
+       END FUNCTION
+       FUNCTION ghost_slab_hd_back_z(slab,o,dt,nu,prune,w,v,c,f) BIND(C,name="ghost_slab_hd_back_z") RESULT(s)
+         IMPORT :: C_INT, C_PTR, C_DOUBLE
+         TYPE(C_PTR), VALUE :: slab
+         INTEGER(C_INT), VALUE :: o, prune
+         REAL(C_DOUBLE), VALUE :: dt, nu
+         TYPE(C_PTR) :: w(3), v(3), c(3), f(3)
+         INTEGER(C_INT) :: s
+       END FUNCTION
        FUNCTION ghost_ctx_set_tile_cfg(ctx,cfg) BIND(C,name="ghost_ctx_set_tile_cfg") RESULT(s)
          IMPORT :: C_INT, C_PTR
          TYPE(C_PTR), VALUE :: ctx

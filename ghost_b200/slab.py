@@ -22,6 +22,13 @@ the device: a rank's kx-slab of a spectral field is (nxh_loc, ny, nz),
 Fortran (nz, ny, ista:iend).  Every substep after the first of a run is
 zero-pruned as in ghost_hd_run: pruned passes, and exchanges of the kx
 rows below Slab.rows only.
+
+By default (Slab(overlap=True)) the exchanges are split into field groups
+(substep(), GROUPS_OVERLAP): the all-to-all of v's three fields runs while
+curl v is transformed along y, and each product field's all-to-all back
+runs while the previous field is transformed along y; the collectives are
+asynchronous, each on its own buffer slot, and a rank's own block moves
+field to field (ghost_slab_exchange_self) instead of through the buffers.
 """
 from __future__ import annotations
 
@@ -66,35 +73,95 @@ def live_rows(ista, nxhl, rows):
     return [max(0, min(rows - a, n)) for a, n in zip(ista, nxhl)]
 
 
-def exchange_counts(nxhl, nzl, ny: int, rank: int, direction: int, nf: int):
+def exchange_counts(nxhl, nzl, ny: int, rank: int, direction: int, nf: int, self_direct: bool = False):
     """Complex values sent to and received from every peer by `rank` in one
     all-to-all of nf fields.  Direction 0 (kx-slab -> z-slab): the chunk
     for peer p is nf blocks of my kx rows x ny x p's z planes; the chunk
     from p is nf blocks of p's rows x ny x my planes.  Direction 1 is the
-    reverse.  For a pruned exchange nxhl is the ranks' live rows."""
+    reverse.  For a pruned exchange nxhl is the ranks' live rows.  With
+    self_direct the rank's own chunk is empty (it moves field to field)."""
     n = len(nxhl)
     mine = [nf * nxhl[rank] * ny * nzl[p] for p in range(n)]
     theirs = [nf * nxhl[p] * ny * nzl[rank] for p in range(n)]
+    if self_direct:
+        mine[rank] = theirs[rank] = 0
     return (mine, theirs) if direction == 0 else (theirs, mine)
 
 
-def all_to_all(recv, send, recv_counts, send_counts, group=None):
+# Field groups of the two exchanges of a substep.  Plain: one all-to-all of
+# the six front fields, one of the three x-pass products.  Overlapped: the
+# front's fields go in two groups (v, then curl v), so that the first
+# group's all-to-all runs while the second group is transformed along y;
+# the products go one field at a time, so that field q's Y forward runs
+# while the later fields are still in flight.
+GROUPS_PLAIN = (((0, 1, 2, 3, 4, 5),), ((0, 1, 2),))
+GROUPS_OVERLAP = (((0, 1, 2), (3, 4, 5)), ((0,), (1,), (2,)))
+
+
+def substep(ops, o, dt, nu, v, f, copy, prune, groups, self_direct):
+    """One HD substep of a slab-decomposed run (include/hd_rkstep2.f90) as
+    a schedule of phases over field groups.  ops provides the phases for one
+    rank (Slab) or for all ranks in lockstep (run_local):
+      front_z(v, copy, prune); ypass(sign, idx, prune);
+      pack(d, idx, prune, g); exchange(d, g, nf, prune) -> handle;
+      wait(handle); unpack(d, idx, prune, g); exchange_self(d, idx, prune);
+      xpass(prune); back_z(o, dt, nu, v, f, prune).
+    Group g of direction d has its own buffer slot, so that no pack or
+    unpack touches the buffers of an all-to-all in flight.  The results do
+    not depend on the grouping (a line's arithmetic is the same), nor on
+    self_direct."""
+    g0, g1 = groups
+    ops.front_z(v, copy, prune)
+    hs = []
+    for g, idx in enumerate(g0):
+        ops.ypass(+1, idx, prune)
+        ops.pack(0, idx, prune, g)
+        hs.append(ops.exchange(0, g, len(idx), prune))
+    if self_direct:
+        ops.exchange_self(0, tuple(q for idx in g0 for q in idx), prune)
+    for g, idx in enumerate(g0):
+        ops.wait(hs[g])
+        ops.unpack(0, idx, prune, g)
+    ops.xpass(prune)
+    hs = []
+    for g, idx in enumerate(g1):
+        ops.pack(1, idx, prune, g)
+        hs.append(ops.exchange(1, g, len(idx), prune))
+    if self_direct:
+        ops.exchange_self(1, tuple(q for idx in g1 for q in idx), prune)
+    for g, idx in enumerate(g1):
+        ops.wait(hs[g])
+        ops.unpack(1, idx, prune, g)
+        ops.ypass(-1, idx, prune)
+    ops.back_z(o, dt, nu, v, f, prune)
+
+
+def all_to_all(recv, send, recv_counts, send_counts, group=None, async_op=False):
     """One all-to-all of complex buffers (peer-major chunks of the given
     counts) over torch.distributed; the buffers travel as their real
-    and imaginary parts."""
+    and imaginary parts.  async_op: returns the work handle, whose wait()
+    orders the caller's stream after the exchange."""
     import torch.distributed as dist
     r = torch.view_as_real(recv[:sum(recv_counts)]).reshape(-1)
     s = torch.view_as_real(send[:sum(send_counts)]).reshape(-1)
-    dist.all_to_all_single(r, s, [2 * c for c in recv_counts], [2 * c for c in send_counts], group=group)
+    return dist.all_to_all_single(r, s, [2 * c for c in recv_counts], [2 * c for c in send_counts], group=group,
+                                  async_op=async_op)
 
 
 class Slab:
     """One rank's share of a slab-decomposed HD run: the library's slab
-    context and the work arrays of the substep."""
+    context and the work arrays of the substep.
+
+    overlap (default): the exchanges go in field groups (GROUPS_OVERLAP),
+    each all-to-all asynchronous on its own buffer slot and overlapped with
+    the Y passes of the other groups, and the rank's own block moves field
+    to field (ghost_slab_exchange_self) instead of through the buffers.
+    overlap=False: one synchronous all-to-all per direction carrying every
+    block, the own block included."""
 
     def __init__(self, nx: int, ny: int | None = None, nz: int | None = None, Lx: float = 1.0, Ly: float = 1.0,
                  Lz: float = 1.0, arbsize: bool = False, precision: str = "fp64", rank: int = 0, nranks: int = 1,
-                 stream=None):
+                 stream=None, overlap: bool = True):
         ny = nx if ny is None else ny
         nz = nx if nz is None else nz
         self.lib = _lib.load()
@@ -119,14 +186,43 @@ class Slab:
         self.w = [torch.zeros(self.kshape, dtype=dt, device=dev) for _ in range(6)]   # kx-slab work fields
         self.z = [torch.zeros(self.zshape, dtype=dt, device=dev) for _ in range(6)]   # z-slab work fields
         self.C = [torch.zeros(self.kshape, dtype=dt, device=dev) for _ in range(3)]   # RK copy (hd_rkstep1)
-        # (direction, pruned) -> (send counts, receive counts)
-        self.counts = {(d, pr): exchange_counts(live_rows(self.ista, self.nxhl, self.rows if pr else None), self.nzl,
-                                                ny, rank, d, 6 if d == 0 else 3)
-                       for d in (0, 1) for pr in (False, True)}
-        nsend = max(sum(self.counts[d, False][0]) for d in (0, 1))
-        nrecv = max(sum(self.counts[d, False][1]) for d in (0, 1))
-        self.send = torch.empty(nsend, dtype=dt, device=dev)
-        self.recv = torch.empty(nrecv, dtype=dt, device=dev)
+        # buffers for either mode (the plain one's hold the most)
+        nsend = nrecv = 0
+        for ov in (False, True):
+            self.set_overlap(ov, _sizes_only=True)
+            nsend, nrecv = max(nsend, self._nsend), max(nrecv, self._nrecv)
+        self.send = torch.empty(max(nsend, 1), dtype=dt, device=dev)
+        self.recv = torch.empty(max(nrecv, 1), dtype=dt, device=dev)
+        self.group = None
+        self.exchange_events = None
+        self.set_overlap(overlap)
+
+    def set_overlap(self, on: bool, _sizes_only: bool = False):
+        """Switch between the overlapped schedule (field groups, asynchronous
+        all-to-alls, own block field to field) and the plain one; one rank
+        always runs the plain one (it has no exchange)."""
+        self.overlap = bool(on) and self.nranks > 1
+        self.self_direct = self.overlap
+        self.groups = GROUPS_OVERLAP if self.overlap else GROUPS_PLAIN
+        # buffer slots: group g of direction d at send/recv offsets soff/roff[d, g]
+        # (the two directions never have exchanges in flight together, so they share the buffers)
+        self.soff, self.roff = {}, {}
+        self._nsend = self._nrecv = 0
+        for d in (0, 1):
+            so = ro = 0
+            for g, idx in enumerate(self.groups[d]):
+                sc, rc = self.counts(d, len(idx), False)
+                self.soff[d, g], self.roff[d, g] = so, ro
+                so += sum(sc)
+                ro += sum(rc)
+            self._nsend, self._nrecv = max(self._nsend, so), max(self._nrecv, ro)
+        if not _sizes_only:
+            check(self.lib.ghost_slab_set_self_direct(self.h, int(self.self_direct)), "ghost_slab_set_self_direct")
+
+    def counts(self, d: int, nf: int, prune: bool):
+        """(send counts, receive counts) of an exchange of nf fields in direction d."""
+        return exchange_counts(live_rows(self.ista, self.nxhl, self.rows if prune else None), self.nzl, self.ny,
+                               self.rank, d, nf, self.self_direct)
 
     def close(self):
         if getattr(self, "h", None):
@@ -160,15 +256,59 @@ class Slab:
         check(self.lib.ghost_slab_hd_front(self.h, self._pp(self._fields(v)), self._pp(self.C), int(copy), int(prune),
                                            self._pp(self.w)), "ghost_slab_hd_front")
 
-    def pack(self, direction: int, prune: bool = False):
-        fields = self.w if direction == 0 else self.z[:3]
-        check(self.lib.ghost_slab_pack(self.h, direction, len(fields), int(prune), self._pp(fields),
-                                       ctypes.c_void_p(self.send.data_ptr())), "ghost_slab_pack")
+    def front_z(self, v, copy: bool, prune: bool = False):
+        check(self.lib.ghost_slab_hd_front_z(self.h, self._pp(self._fields(v)), self._pp(self.C), int(copy),
+                                             int(prune), self._pp(self.w)), "ghost_slab_hd_front_z")
 
-    def unpack(self, direction: int, prune: bool = False):
-        fields = self.z if direction == 0 else self.w[:3]
+    def ypass(self, sign: int, idx, prune: bool = False):
+        check(self.lib.ghost_slab_ypass(self.h, sign, len(idx), int(prune), self._pp([self.w[q] for q in idx])),
+              "ghost_slab_ypass")
+
+    def _slot(self, buf, off, d, g):
+        return ctypes.c_void_p(buf[off[d, g]:].data_ptr())
+
+    def pack(self, direction: int, idx=None, prune: bool = False, g: int = 0):
+        if idx is None:
+            idx = self.groups[direction][0]
+        fields = [(self.w if direction == 0 else self.z)[q] for q in idx]
+        check(self.lib.ghost_slab_pack(self.h, direction, len(fields), int(prune), self._pp(fields),
+                                       self._slot(self.send, self.soff, direction, g)), "ghost_slab_pack")
+
+    def unpack(self, direction: int, idx=None, prune: bool = False, g: int = 0):
+        if idx is None:
+            idx = self.groups[direction][0]
+        fields = [(self.z if direction == 0 else self.w)[q] for q in idx]
         check(self.lib.ghost_slab_unpack(self.h, direction, len(fields), int(prune),
-                                         ctypes.c_void_p(self.recv.data_ptr()), self._pp(fields)), "ghost_slab_unpack")
+                                         self._slot(self.recv, self.roff, direction, g), self._pp(fields)),
+              "ghost_slab_unpack")
+
+    def exchange(self, direction: int, g: int, nf: int, prune: bool = False):
+        """The all-to-all of group g: asynchronous with overlap (returns the
+        work handle), else synchronous (events around it when requested)."""
+        sc, rc = self.counts(direction, nf, prune)
+        send = self.send[self.soff[direction, g]:]
+        recv = self.recv[self.roff[direction, g]:]
+        if self.overlap:
+            return all_to_all(recv, send, rc, sc, self.group, async_op=True)
+        if self.exchange_events is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        all_to_all(recv, send, rc, sc, self.group)
+        if self.exchange_events is not None:
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record()
+            self.exchange_events.append((e0, e1))
+        return None
+
+    @staticmethod
+    def wait(handle):
+        if handle is not None:
+            handle.wait()
+
+    def exchange_self(self, direction: int, idx, prune: bool = False):
+        src, dst = (self.w, self.z) if direction == 0 else (self.z, self.w)
+        check(self.lib.ghost_slab_exchange_self(self.h, direction, len(idx), int(prune), self._pp([src[q] for q in idx]),
+                                                self._pp([dst[q] for q in idx])), "ghost_slab_exchange_self")
 
     def xpass(self, prune: bool = False):
         # one rank: the kx-slab is the whole field and the z-slab layout is the same, so the x pass
@@ -181,74 +321,107 @@ class Slab:
         check(self.lib.ghost_slab_hd_back(self.h, o, dt, nu, int(prune), self._pp(self.w[:3]),
                                           self._pp(self._fields(v)), self._pp(self.C), fp), "ghost_slab_hd_back")
 
+    def back_z(self, o: int, dt: float, nu: float, v, f=None, prune: bool = False):
+        fp = self._pp(self._fields(f)) if f is not None else None
+        check(self.lib.ghost_slab_hd_back_z(self.h, o, dt, nu, int(prune), self._pp(self.w[:3]),
+                                            self._pp(self._fields(v)), self._pp(self.C), fp), "ghost_slab_hd_back_z")
+
     # -- runs -----------------------------------------------------------
     def run(self, nsteps: int, ord: int, dt: float, nu: float, vx, vy, vz, fx=None, fy=None, fz=None, group=None,
             exchange_events=None):
         """nsteps RK steps of order ord (GHOST's RK loop, main3D.fpp:3195-3231)
         of this rank's kx-slab of v, the transposes as NCCL all-to-alls.
         Every substep after the first is zero-pruned, as in ghost_hd_run.
-        exchange_events: a list to which CUDA event pairs bracketing each
-        all-to-all (on the current stream) are appended."""
+        exchange_events (synchronous exchanges only, overlap=False): a list to
+        which CUDA event pairs bracketing each all-to-all (on the current
+        stream) are appended."""
+        if exchange_events is not None and self.overlap:
+            raise ValueError("exchange_events times synchronous exchanges: construct the Slab with overlap=False")
         v, f = [vx, vy, vz], (None if fx is None else [fx, fy, fz])
-        for t in range(nsteps):
-            for o in range(ord, 0, -1):
-                pr = not (t == 0 and o == ord)
-                self.front(v, o == ord, pr)
-                if self.nranks == 1:
-                    self.xpass(pr)
-                else:
-                    for d in (0, 1):
-                        self.pack(d, pr)
-                        if exchange_events is not None:
-                            e0 = torch.cuda.Event(enable_timing=True)
-                            e0.record()
-                        all_to_all(self.recv, self.send, self.counts[d, pr][1], self.counts[d, pr][0], group)
-                        if exchange_events is not None:
-                            e1 = torch.cuda.Event(enable_timing=True)
-                            e1.record()
-                            exchange_events.append((e0, e1))
-                        self.unpack(d, pr)
-                        if d == 0:
-                            self.xpass(pr)
-                self.back(o, dt, nu, v, f, pr)
+        self.group, self.exchange_events = group, exchange_events
+        try:
+            for t in range(nsteps):
+                for o in range(ord, 0, -1):
+                    pr = not (t == 0 and o == ord)
+                    if self.nranks == 1:
+                        self.front(v, o == ord, pr)
+                        self.xpass(pr)
+                        self.back(o, dt, nu, v, f, pr)
+                    else:
+                        substep(self, o, dt, nu, v, f, o == ord, pr, self.groups, self.self_direct)
+        finally:
+            self.group, self.exchange_events = None, None
 
 
-def _local_exchange(slabs, direction: int, prune: bool):
-    """The all-to-all among ranks held by one process: device copies from
-    every peer's send chunk for r into r's receive chunk from that peer."""
-    n = len(slabs)
-    for r, dst in enumerate(slabs):
-        roff = 0
-        rc = dst.counts[direction, prune][1]
-        for p, src in enumerate(slabs):
-            sc = src.counts[direction, prune][0]
-            soff = sum(sc[:r])
-            assert sc[r] == rc[p]
-            dst.recv[roff:roff + rc[p]].copy_(src.send[soff:soff + sc[r]])
-            roff += rc[p]
-    return n
+class _Lockstep:
+    """The phases of substep() applied to every rank that one process holds,
+    rank after rank; an exchange is the device copies from every peer's send
+    slot for r into r's receive slot from that peer, once every rank has
+    packed."""
+
+    def __init__(self, slabs):
+        self.slabs = slabs
+
+    def front_z(self, vs, copy, prune):
+        for s, v in zip(self.slabs, vs):
+            s.front_z(v, copy, prune)
+
+    def ypass(self, sign, idx, prune):
+        for s in self.slabs:
+            s.ypass(sign, idx, prune)
+
+    def pack(self, d, idx, prune, g):
+        for s in self.slabs:
+            s.pack(d, idx, prune, g)
+
+    def exchange(self, d, g, nf, prune):
+        for r, dst in enumerate(self.slabs):
+            rc = dst.counts(d, nf, prune)[1]
+            roff = dst.roff[d, g]
+            for p, src in enumerate(self.slabs):
+                sc = src.counts(d, nf, prune)[0]
+                soff = src.soff[d, g] + sum(sc[:r])
+                assert sc[r] == rc[p]
+                if rc[p]:
+                    dst.recv[roff:roff + rc[p]].copy_(src.send[soff:soff + sc[r]])
+                roff += rc[p]
+        return None
+
+    @staticmethod
+    def wait(handle):
+        pass
+
+    def unpack(self, d, idx, prune, g):
+        for s in self.slabs:
+            s.unpack(d, idx, prune, g)
+
+    def exchange_self(self, d, idx, prune):
+        for s in self.slabs:
+            s.exchange_self(d, idx, prune)
+
+    def xpass(self, prune):
+        for s in self.slabs:
+            s.xpass(prune)
+
+    def back_z(self, o, dt, nu, vs, fs, prune):
+        for r, (s, v) in enumerate(zip(self.slabs, vs)):
+            s.back_z(o, dt, nu, v, None if fs is None else fs[r], prune)
 
 
 def run_local(slabs, nsteps: int, ord: int, dt: float, nu: float, vs, fs=None):
     """RK steps of a decomposed run whose ranks this process holds (slabs
     in rank order, vs[r] / fs[r] rank r's kx-slabs of v and f): the same
-    library calls as Slab.run, phase by phase over the ranks, with the
+    schedule and library calls as Slab.run (the slabs' overlap setting
+    picks the field groups), phase by phase over the ranks, with the
     all-to-alls done by device copies on the current stream."""
+    if len(slabs) == 1:
+        s = slabs[0]
+        return s.run(nsteps, ord, dt, nu, *vs[0], *(fs[0] if fs is not None else (None, None, None)))
+    ops = _Lockstep(slabs)
+    groups, direct = slabs[0].groups, slabs[0].self_direct
+    if any(s.groups != groups or s.self_direct != direct for s in slabs):
+        raise ValueError("the ranks of a run need the same overlap setting")
     for t in range(nsteps):
         for o in range(ord, 0, -1):
             pr = not (t == 0 and o == ord)
-            for s, v in zip(slabs, vs):
-                s.front(v, o == ord, pr)
-            if len(slabs) == 1:
-                slabs[0].xpass(pr)
-            for d in (0, 1) if len(slabs) > 1 else ():
-                for s in slabs:
-                    s.pack(d, pr)
-                _local_exchange(slabs, d, pr)
-                for s in slabs:
-                    s.unpack(d, pr)
-                if d == 0:
-                    for s in slabs:
-                        s.xpass(pr)
-            for r, (s, v) in enumerate(zip(slabs, vs)):
-                s.back(o, dt, nu, v, None if fs is None else fs[r], pr)
+            substep(ops, o, dt, nu, vs, fs, o == ord, pr, groups, direct)

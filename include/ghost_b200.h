@@ -658,6 +658,29 @@ int ghost_slab_pack(ghost_slab *s, int dir, int nf, int prune, const void *const
 /* the blocks from every peer out of recv into nf fields (dir 0: z-slab
  * fields; dir 1: kx-slab fields) */
 int ghost_slab_unpack(ghost_slab *s, int dir, int nf, int prune, const void *recv, void *const *fields);
+/* on = 1: ghost_slab_pack and ghost_slab_unpack skip the rank's own block
+ * (its chunk in the send and receive buffers has size 0), and
+ * ghost_slab_exchange_self moves it from the source fields straight into
+ * the destination fields; the all-to-all then carries only the peers'
+ * blocks.  Default 0 (the own block travels through the buffers). */
+int ghost_slab_set_self_direct(ghost_slab *s, int on);
+/* the rank's own block of an exchange of nf fields, field to field: dir 0
+ * from kx-slab fields (in) into z-slab fields (out), dir 1 the reverse
+ * (the transposes' local part, fftp-3/fftp3D.fpp:158-201) */
+int ghost_slab_exchange_self(ghost_slab *s, int dir, int nf, int prune, const void *const *in, void *const *out);
+/* The front and back phases split around their Y passes, so that the
+ * exchange of some fields can run while the others are transformed:
+ * ghost_slab_hd_front = ghost_slab_hd_front_z, then ghost_slab_ypass(+1)
+ * of the six fields (in any grouping); ghost_slab_hd_back =
+ * ghost_slab_ypass(-1) of the three fields (in any grouping), then
+ * ghost_slab_hd_back_z.  A line's arithmetic does not depend on the
+ * grouping: the results are the same bits. */
+int ghost_slab_hd_front_z(ghost_slab *s, const void *const v[3], void *const C[3], int copy, int prune,
+                          void *const w[6]);
+/* the Y pass (sign +1 inverse, -1 forward) of nf <= 9 kx-slab fields */
+int ghost_slab_ypass(ghost_slab *s, int sign, int nf, int prune, void *const *fields);
+int ghost_slab_hd_back_z(ghost_slab *s, int o, double dt, double nu, int prune, void *const w[3], void *const v[3],
+                         const void *const C[3], const void *const f[3]);
 
 #ifdef __cplusplus
 }

@@ -2,7 +2,9 @@
 held by one process (ghost_b200.slab.run_local: the library's slab passes,
 packing and unpacking, with the all-to-alls done by device copies), against
 the undivided run of ghost_hd_run on the same fields.  Uneven kx slabs
-(33 rows over 2 or 4 ranks) included."""
+(33 rows over 2 or 4 ranks) included.  Both schedules: the overlapped one
+(field groups, own block copied field to field) and the plain one, which
+give the same bits."""
 import numpy as np
 import pytest
 
@@ -15,10 +17,11 @@ def _fields(g, seed):
     return v
 
 
+@pytest.mark.parametrize("overlap", [True, False])
 @pytest.mark.parametrize("prec,P,shape", [("fp64", 1, (64, 64, 64)), ("fp64", 2, (64, 64, 64)),
                                           ("fp64", 4, (64, 64, 64)), ("fp32", 2, (64, 64, 64)),
                                           ("fp64", 4, (64, 32, 128))])
-def test_slab_run_matches_undivided_run(prec, P, shape):
+def test_slab_run_matches_undivided_run(prec, P, shape, overlap):
     import torch
 
     from ghost_b200 import Ghost
@@ -30,7 +33,7 @@ def test_slab_run_matches_undivided_run(prec, P, shape):
     v0, f = _fields(g, 1000), _fields(g, 77)
     ref = [x.clone() for x in v0]
     g.hd_run(2, 4, 1e-3, 2e-3, *ref, *f)
-    slabs = [Slab(nx, ny, nz, precision=prec, rank=r, nranks=P, **kw) for r in range(P)]
+    slabs = [Slab(nx, ny, nz, precision=prec, rank=r, nranks=P, overlap=overlap, **kw) for r in range(P)]
     vs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in v0] for r, s in enumerate(slabs)]
     fs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in f] for r, s in enumerate(slabs)]
     for _ in range(2):  # two calls in a row: the work arrays carry nothing over
@@ -96,3 +99,42 @@ def test_slab_run_without_forcing_and_null_forcing_pointers():
         assert torch.equal(a, b)
     for t in slabs + [s]:
         t.close()
+
+
+@pytest.mark.parametrize("prec,P", [("fp32", 2), ("fp64", 2), ("fp32", 4), ("fp64", 4)])
+def test_overlapped_schedule_is_the_plain_one_bit_for_bit(prec, P):
+    """Field groups, asynchronous slots and the own block copied field to
+    field change no bit of the run (uneven kx slabs: 33 rows over 2 or 4
+    ranks; with 4 ranks one holds no live row)."""
+    import torch
+
+    from ghost_b200 import Ghost
+    from ghost_b200.slab import Slab, run_local
+    nz = 64
+    g = Ghost(64, 64, nz, precision=prec)
+    v0, f = _fields(g, 31), _fields(g, 32)
+    out = {}
+    for overlap in (True, False):
+        slabs = [Slab(64, 64, nz, precision=prec, rank=r, nranks=P, overlap=overlap) for r in range(P)]
+        assert all(s.overlap == overlap and s.self_direct == overlap for s in slabs)
+        vs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in v0] for r, s in enumerate(slabs)]
+        fs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in f] for r, s in enumerate(slabs)]
+        run_local(slabs, 2, 3, 1e-3, 2e-3, vs, fs)
+        torch.cuda.synchronize()
+        out[overlap] = [torch.cat([vs[r][c] for r in range(P)], dim=0) for c in range(3)]
+        for s in slabs:
+            s.close()
+    for a, b in zip(out[True], out[False]):
+        assert torch.equal(a, b)
+    # switching a slab's mode at run time gives the same bits again
+    slabs = [Slab(64, 64, nz, precision=prec, rank=r, nranks=P, overlap=False) for r in range(P)]
+    for s in slabs:
+        s.set_overlap(True)
+    vs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in v0] for r, s in enumerate(slabs)]
+    fs = [[x[s.ista[r]:s.ista[r] + s.nxhl[r]].clone() for x in f] for r, s in enumerate(slabs)]
+    run_local(slabs, 2, 3, 1e-3, 2e-3, vs, fs)
+    torch.cuda.synchronize()
+    for c in range(3):
+        assert torch.equal(torch.cat([vs[r][c] for r in range(P)], dim=0), out[False][c])
+    for s in slabs:
+        s.close()
