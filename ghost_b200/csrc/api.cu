@@ -95,7 +95,32 @@ bool is_device_ptr(const void *p) {
 
 int check_status(ghost_ctx *c);
 
+// flag |= 1 when any byte of rows [live, rows) of any run is nonzero (a
+// field of nruns runs of `rows` kx rows of row_u4 16-byte words each)
+__global__ void dead_rows_kernel(const uint4 *__restrict__ p, int nruns, int rows, int live, size_t row_u4,
+                                 int *__restrict__ flag) {
+  const size_t per_run = (size_t)(rows - live) * row_u4, total = per_run * nruns;
+  bool any = false;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = q / per_run, o = q - r * per_run;
+    const uint4 w = p[(r * rows + live) * row_u4 + o];
+    any |= (w.x | w.y | w.z | w.w) != 0u;
+  }
+  if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// Staging of host arrays for a call on device fields.  Two kinds of field
+// move only their live kx rows (rows 0..live-1 of every run, the rows that
+// hold a mode of the truncation):
+//   IN_LIVE:  an input read only at kept modes (forcing): the live rows go
+//             in, the rest of the staging buffer is never read;
+//   OUT_LIVE: an in/out field that the call leaves zero outside the kept
+//             modes (the velocity): it goes in whole, and the live rows come
+//             back when the rows beyond hold zero bits both in the input and
+//             in the result (then the host array already holds them); else
+//             the whole field comes back.
 struct Staging {
+  static constexpr int IN = 1, OUT = 2, IN_LIVE = 4, OUT_LIVE = 8;
   ghost_ctx *c;
   int used = 0;
   bool any_host = false;
@@ -103,9 +128,38 @@ struct Staging {
     void *host;
     const void *dev;
     size_t bytes;
+    bool live;
   };
   std::vector<Back> back;
+  // live rows per run and the rows of a run (0: unknown, whole fields move)
+  int live = 0, rows = 0;
+  size_t row_bytes = 0;
+  bool flag_armed = false;
   explicit Staging(ghost_ctx *ctx) : c(ctx) {}
+  void set_live(int live_rows, int run_rows, size_t bytes_per_row) {
+    live = live_rows;
+    rows = run_rows;
+    row_bytes = bytes_per_row;
+  }
+  bool live_ok(size_t bytes) const {
+    return live > 0 && live < rows && row_bytes % 16 == 0 && (size_t)rows * row_bytes * c->nruns == bytes;
+  }
+  int check_dead(const void *dev) {
+    if (!c->dead_flag) {
+      GB_CHECK(dalloc((void **)&c->dead_flag, sizeof(int)));
+      GB_CUDA(cudaMallocHost((void **)&c->dead_flag_host, sizeof(int)));
+    }
+    if (!flag_armed) {
+      GB_CUDA(cudaMemsetAsync(c->dead_flag, 0, sizeof(int), c->stream));
+      flag_armed = true;
+    }
+    const size_t total = (size_t)(rows - live) * (row_bytes / 16) * c->nruns;
+    const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
+    dead_rows_kernel<<<grid, 256, 0, c->stream>>>((const uint4 *)dev, c->nruns, rows, live, row_bytes / 16,
+                                                  c->dead_flag);
+    GB_CUDA(cudaGetLastError());
+    return GHOST_OK;
+  }
   int buffer(void **out) {
     while ((int)c->stage.size() <= used) {
       void *p;
@@ -131,8 +185,15 @@ struct Staging {
     any_host = true;
     void *d;
     GB_CHECK(buffer(&d));
-    if (dir & 1) GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
-    if (dir & 2) back.push_back({(void *)user, d, bytes});
+    const bool lv = (dir & (IN_LIVE | OUT_LIVE)) && live_ok(bytes);
+    const size_t run_b = (size_t)rows * row_bytes, live_b = (size_t)live * row_bytes;
+    if ((dir & IN_LIVE) && lv)
+      GB_CUDA(cudaMemcpy2DAsync(d, run_b, (const void *)user, run_b, live_b, c->nruns, cudaMemcpyHostToDevice,
+                                c->stream));
+    else if (dir & IN)
+      GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
+    if ((dir & OUT_LIVE) && lv) GB_CHECK(check_dead(d));  // the input's rows beyond the live ones
+    if (dir & OUT) back.push_back({(void *)user, d, bytes, (dir & OUT_LIVE) && lv});
     *dev = (T *)d;
     return GHOST_OK;
   }
@@ -140,12 +201,29 @@ struct Staging {
 };
 
 int Staging::finish() {
-  for (auto &b : back) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
-  if (any_host) {
-    GB_CUDA(cudaStreamSynchronize(c->stream));
-    return check_status(c);
+  bool any_live = false;
+  for (auto &b : back)
+    if (b.live) {
+      GB_CHECK(check_dead(b.dev));  // the result's rows beyond the live ones
+      any_live = true;
+    }
+  if (any_live) GB_CUDA(cudaMemcpyAsync(c->dead_flag_host, c->dead_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  const size_t run_b = (size_t)rows * row_bytes, live_b = (size_t)live * row_bytes;
+  for (auto &b : back) {
+    if (b.live)
+      GB_CUDA(cudaMemcpy2DAsync(b.host, run_b, b.dev, run_b, live_b, c->nruns, cudaMemcpyDeviceToHost, c->stream));
+    else
+      GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
   }
-  return GHOST_OK;
+  if (!any_host) return GHOST_OK;
+  GB_CUDA(cudaStreamSynchronize(c->stream));
+  if (any_live && *c->dead_flag_host != 0) {
+    // nonzero bits beyond the live rows in the input or the result: the whole field comes back
+    for (auto &b : back)
+      if (b.live) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+    GB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return check_status(c);
 }
 
 template <typename R> const KParams<R> &kparams(const ghost_ctx *c);
@@ -1320,6 +1398,7 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->prune_valid = c->prune_ok = false;
   c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
   c->prune_nlines = c->prune_imax = 0;
+  c->dead_flag = c->dead_flag_host = nullptr;
   for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
     c->t_ms[k] = 0.0;
     c->t_n[k] = 0;
@@ -1355,6 +1434,8 @@ int ghost_ctx_destroy(ghost_ctx *c) {
   cudaFree(c->prune_lines);
   cudaFree(c->prune_jpos);
   cudaFree(c->prune_jneg);
+  cudaFree(c->dead_flag);
+  if (c->dead_flag_host) cudaFreeHost(c->dead_flag_host);
   for (auto &p : c->ev_pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -2280,6 +2361,15 @@ int ghost_hd_rkstep2(ghost_ctx *c, int o, double dt, double nu, void *vx, void *
   return st.finish();
 }
 
+// the live kx rows of the truncation for host-array staging (none known:
+// whole fields move)
+static int staging_live_rows(ghost_ctx *c, Staging &st) {
+  if (!c->prune_valid) GB_CHECK(c->precision == GHOST_SINGLE ? build_prune<float>(c) : build_prune<double>(c));
+  if (c->prune_ok)
+    st.set_live(c->prune_imax + 1, c->nxh, (size_t)c->ny * c->nz * (c->precision == GHOST_SINGLE ? 8 : 16));
+  return GHOST_OK;
+}
+
 int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *vx, void *vy, void *vz, void *C1,
                  void *C2, void *C3, const void *fx, const void *fy, const void *fz) {
   CTX_CHECK(c);
@@ -2290,14 +2380,17 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
   if ((C1 == nullptr) != (C2 == nullptr) || (C1 == nullptr) != (C3 == nullptr))
     return fail(GHOST_ERR_ARG, "RK storage must be all given or all null");
   Staging st(c);
+  // host arrays: the forcing is read only at kept modes and the run leaves v
+  // zero outside them, so only their live kx rows need to cross the bus
+  GB_CHECK(staging_live_rows(c, st));
   void *v[3], *Cd[3];
   const void *f[3] = {nullptr, nullptr, nullptr};
   void *vu[3] = {vx, vy, vz};
   void *Cu[3] = {C1, C2, C3};
   const void *fu[3] = {fx, fy, fz};
   for (int q = 0; q < 3; ++q) {
-    GB_CHECK(st.map(vu[q], c->cbytes, 3, &v[q]));
-    if (fx) GB_CHECK(st.map(fu[q], c->cbytes, 1, &f[q]));
+    GB_CHECK(st.map(vu[q], c->cbytes, Staging::IN | Staging::OUT | Staging::OUT_LIVE, &v[q]));
+    if (fx) GB_CHECK(st.map(fu[q], c->cbytes, Staging::IN | Staging::IN_LIVE, &f[q]));
     if (C1) {
       GB_CHECK(st.map(Cu[q], c->cbytes, 3, &Cd[q]));
     } else {

@@ -133,6 +133,9 @@ struct ghost_ctx {
   bool prune_valid, prune_ok;
   int *prune_lines, *prune_jpos, *prune_jneg;
   int prune_nlines, prune_imax;
+  // host-array calls: a device flag and its pinned host copy (nonzero values
+  // beyond the live kx rows of a staged field), allocated on first use
+  int *dead_flag, *dead_flag_host;
   // per-kernel timers (ghost_ctx_enable_timers)
   bool timers_on;
   std::vector<cudaEvent_t> ev_free;

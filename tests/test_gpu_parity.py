@@ -257,6 +257,51 @@ def test_hd_host_arrays_drop_in():
     assert rel_l2(V, ref) < 1e-12
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_hd_host_arrays_move_live_rows_only(prec):
+    """Host arrays move only the kx rows that hold kept modes where that is
+    exact: the forcing's other rows are never read (garbage there changes
+    nothing), and v comes back whole when its rows beyond the live ones
+    held nonzero values on the way in (they leave as zeros).  Every case
+    against the same run on device arrays, bit for bit."""
+    o = Oracle(32, precision=prec)
+    g = ghost(32, precision=prec)
+    v0 = solenoidal_ic(o, seed=21)
+    f0, _ = o.random_solenoidal(22, 2.0, 3.0, 0, 1.0)
+    live = 32 // 3 + 1  # kx rows 0..10 hold every mode with kn2 <= kmax at 32^3
+    rng = np.random.default_rng(23)
+    junk = lambda x: (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape)).astype(x.dtype)  # noqa: E731
+
+    def device_run(v, f, nsteps=2):
+        V = [to_dev(x) for x in v]
+        g.hd_run(nsteps, 2, 1e-3, 2e-3, *V, *[to_dev(x) for x in f])
+        return [to_host(x) for x in V]
+
+    # 1: v zero beyond the live rows (every step's output), forcing with junk there
+    v1 = device_run(v0, f0, 1)
+    assert all(np.all(x[live:] == 0) for x in v1)
+    f_junk = [x.copy() for x in f0]
+    for x in f_junk:
+        x[live:] = junk(x[live:])
+    ref = device_run(v1, f0)
+    V = [x.copy() for x in v1]
+    g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f_junk])
+    assert all(np.array_equal(a, b) for a, b in zip(V, ref))
+    # 2: v with nonzero values beyond the live rows: they are zero afterwards
+    v2 = [x.copy() for x in v1]
+    for x in v2:
+        x[live + 2] = junk(x[live + 2])
+    ref = device_run(v2, f0)
+    V = [x.copy() for x in v2]
+    g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
+    assert all(np.array_equal(a, b) for a, b in zip(V, ref))
+    assert all(np.all(x[live:] == 0) for x in V)
+    # 3: no step: v comes back as it went in, nonzero rows included
+    V = [x.copy() for x in v2]
+    g.hd_run(0, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
+    assert all(np.array_equal(a, b) for a, b in zip(V, v2))
+
+
 def test_hd_anisotropic_grid():
     o = Oracle(32, 16, 64)
     g = ghost(32, 16, 64)
