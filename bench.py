@@ -363,26 +363,9 @@ def traffic_from_profiles(kernel):
 
 
 def prune_fractions(n):
-    """Exact fractions of the spectral grid the pruned passes must touch for a
-    cubic n^3 grid with the 2/3 truncation kn2 <= n^2/9 (kz = 0 decides a
-    z-line; a kx row is live if any of its lines is)."""
-    import numpy as np
-    nxh = n // 2 + 1
-    kmax = np.float32(1.0 / 9.0) * np.float32(n * n)
-    kx = np.arange(nxh, dtype=np.float64)
-    kx[-1] = -(n // 2)
-    ky = np.fft.fftfreq(n, 1.0 / n)
-    k2 = kx[:, None] ** 2 + ky[None, :] ** 2
-    live = k2 <= kmax
-    f_line = live.mean()
-    f_row = live.any(axis=1).mean()
-    kz = np.fft.fftfreq(n, 1.0 / n)
-    kept = 0
-    for i in range(nxh):
-        kk = k2[i][:, None] + kz[None, :] ** 2
-        kept += int(((kk <= kmax) & (kk >= 3.8e-7)).sum())
-    f_keep = kept / (nxh * n * n)
-    return float(f_line), float(f_row), float(f_keep)
+    """(f_line, f_row, f_keep) of the pruned passes (ghost_b200.roofline)."""
+    from ghost_b200.roofline import prune_fractions as pf
+    return pf(n)
 
 
 def fp64_vs_cpu_oracle(g64, v64, f64):

@@ -20,7 +20,9 @@ of the faster mode.
 Default workload: 128 runs at 32^3, 96 at 64^3, 32 at 128^3 (96.5M grid
 points), seeds 1000+r, nu log-uniform in [5e-4, 5e-3] from a seeded host
 RNG, the config-0 initial spectrum, RK2, dt = 1e-3.  Prints one JSON line
-with run-steps/s and grid-point-steps/s.
+with run-steps/s, grid-point-steps/s and the HBM roofline of the faster mode
+(the pruned substeps' algorithmic bytes of every class, ghost_b200.roofline,
+over the measured copy bandwidth).
 """
 from __future__ import annotations
 
@@ -116,6 +118,12 @@ def main(argv=None):
     points = sum(r * n ** 3 for n, r in zip(sizes, runs))
     best = min(timing, key=timing.get)
     wall = timing[best]
+    # HBM roofline: the pruned substep's algorithmic bytes of every class (no forcing)
+    from ghost_b200.roofline import measured_hbm_peak, pass_bytes
+    eb = 8 if a.precision == "fp32" else 16
+    step_bytes = a.ord * sum(sum(pass_bytes(n, a.ord, False, eb, r).values()) for n, r in zip(sizes, runs))
+    peak, peak_kind = measured_hbm_peak()
+    achieved = step_bytes * a.steps / wall / 1e9
     if rank == 0:
         print(json.dumps({
             "workload": f"ensemble {'+'.join(f'{r}x{n}^3' for n, r in zip(sizes, runs))}, RK{a.ord}, dt={a.dt}, "
@@ -123,6 +131,8 @@ def main(argv=None):
             "gpus": world, "steps": a.steps, "seconds": wall, "run_steps_per_s": total * a.steps / wall,
             "ensemble_steps_per_s": a.steps / wall, "gridpoint_steps_per_s": points * a.steps / wall,
             "mode": best, "autotuned_mode": tuned_mode,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "bytes_per_ensemble_step": step_bytes},
             "modes": {m: {"seconds": w, "run_steps_per_s": total * a.steps / w,
                           "gridpoint_steps_per_s": points * a.steps / w} for m, w in timing.items()},
             "tile_cfg": cfg, "setup_s": setup,

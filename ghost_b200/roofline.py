@@ -1,0 +1,61 @@
+"""Algorithmic bytes of the fused HD substep, the numerator of the HBM
+rooflines that bench.py and the ensemble bench report.
+
+For a cubic n^3 grid with the 2/3 truncation (kn2 <= n^2/9, the library's
+float32 rounding of kmax), the pruned passes touch these fractions of a
+spectral field C = (n/2+1) n^2 complex values: f_line of the (kx, ky)
+z-lines, f_row of the kx rows and f_keep of the modes.  Per substep of an
+RK step of order `ord` the five passes move (in units of C):
+    Z inverse  (9 + 3/ord) f_line    v in, v and curl v out (+ the RK copy)
+    Y inverse  6 (f_line + f_row)
+    X fused    9 f_row               six fields in, three products out
+    Y forward  3 (f_row + f_line)
+    Z forward  6 f_line + 9 f_keep   (6 f_keep without forcing)
+"""
+from __future__ import annotations
+
+import json
+import os
+
+
+def prune_fractions(n: int):
+    """(f_line, f_row, f_keep) of a cubic n^3 grid: the fractions of the
+    spectral grid the pruned passes touch (kz = 0 decides a z-line; a kx
+    row is live if any of its lines is)."""
+    import numpy as np
+    nxh = n // 2 + 1
+    kmax = np.float32(1.0 / 9.0) * np.float32(n * n)
+    kx = np.arange(nxh, dtype=np.float64)
+    kx[-1] = -(n // 2)
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    k2 = kx[:, None] ** 2 + ky[None, :] ** 2
+    live = k2 <= kmax
+    f_line = live.mean()
+    f_row = live.any(axis=1).mean()
+    kz = np.fft.fftfreq(n, 1.0 / n)
+    kept = 0
+    for i in range(nxh):
+        kk = k2[i][:, None] + kz[None, :] ** 2
+        kept += int(((kk <= kmax) & (kk >= 3.8e-7)).sum())
+    f_keep = kept / (nxh * n * n)
+    return float(f_line), float(f_row), float(f_keep)
+
+
+def pass_bytes(n: int, ord: int, forced: bool = True, elem_bytes: int = 8, runs: int = 1):
+    """Algorithmic bytes of each pass of one pruned substep (dict)."""
+    f_line, f_row, f_keep = prune_fractions(n)
+    cb = (n // 2 + 1) * n * n * elem_bytes * runs
+    return {"z_inv": (9 + 3 / ord) * f_line * cb,
+            "y_inv": 6 * (f_line + f_row) * cb,
+            "x_nl": 9 * f_row * cb,
+            "y_fwd": 3 * (f_row + f_line) * cb,
+            "z_fwd": (6 * f_line + (9 if forced else 6) * f_keep) * cb}
+
+
+def measured_hbm_peak():
+    """(GB/s, "measured" | "fallback"): MEASURED_PEAKS.json's hbm_gbs at the
+    repository root, or the fallback figure of this GPU pool."""
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
