@@ -410,6 +410,7 @@ template <typename R, int N, class Op> int launch_z_n(ghost_ctx *c, const Op &op
   constexpr int L256 = fit_lines<R, N, Op::NLOAD>(256 / T > 0 ? 256 / T : 1);
   constexpr int L128 = fit_lines<R, N, Op::NLOAD>(128 / T > 0 ? 128 / T : 1);
   if constexpr (N >= 256 && L128 != L256) {
+    if ((c->tile_cfg & 38) == 38) return launch_z_cfg<R, N, L128, 1, 4>(c, op, pr);
     if ((c->tile_cfg & 6) == 6) return launch_z_cfg<R, N, L128, 2, 3>(c, op, pr);
   }
   if ((c->tile_cfg & 2) && L128 != L256) return launch_z_cfg<R, N, L128, 3, 1>(c, op, pr);
@@ -2413,12 +2414,18 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
 
 // Tile variants tried by the autotuners (bit 0: y tiles 16 z-lines wide;
 // bit 1: z CTAs of 128 threads; bits 1 and 2: two-stage z ring, three CTAs
-// per SM; bit 3: two-stage y ring with a second exchange buffer).
-static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30};
+// per SM; bit 3: two-stage y ring with a second exchange buffer; bit 4: y
+// passes with 16 values per thread; bits 1, 2 and 5: one-stage z ring, four
+// CTAs per SM, for lines of 256 points or more).
+static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62};
+
+// a variant with bit 5 runs the same kernels as without it on z lines
+// shorter than 256 points: the autotuners skip it there
+static bool tile_cfg_distinct(const ghost_ctx *c, int cfg) { return !(cfg & 32) || c->nz >= 256; }
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 31) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..31", cfg);
+  if (cfg < 0 || cfg > 63) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..63", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }
@@ -2455,6 +2462,7 @@ int ghost_hd_autotune(ghost_ctx *c, int ord, double dt, double nu, const void *v
   int best_cfg = c->tile_cfg;
   for (int cfg : kTileCfgs) {
     if (st) break;
+    if (!tile_cfg_distinct(c, cfg)) continue;
     c->tile_cfg = cfg;
     float tot = 0.f;
     for (int rep = 0; rep < 3 && !st; ++rep) {
@@ -3280,6 +3288,7 @@ int ghost_ensemble_autotune(ghost_ensemble *e, int ord, double dt, int *cfg_out)
     int st = GHOST_OK;
     for (int cfg : kTileCfgs) {
       if (st != GHOST_OK) break;
+      if (!tile_cfg_distinct(c, cfg)) continue;
       c->tile_cfg = cfg;
       float tot = 0.f;
       for (int rep = 0; rep < 3 && st == GHOST_OK; ++rep) {
