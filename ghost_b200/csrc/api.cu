@@ -491,6 +491,9 @@ template <typename R, int N, int S> int launch_y_n(ghost_ctx *c, const Fields<R>
   // radix-8 butterflies per stage, half the threads per line
   if constexpr (sizeof(R) == 4 && N >= 256) {
     if (c->tile_cfg & 16) {
+      // bit 6 with bit 3: the inverse pass in tiles of 4 z-lines, four CTAs per SM
+      if constexpr (S > 0)
+        if ((c->tile_cfg & 72) == 72) return launch_y_cfg<R, N, S, 4, true, 16>(c, f, nf, pr);
       if (c->tile_cfg & 8) return launch_y_cfg<R, N, S, 8, true, 16>(c, f, nf, pr);
       return launch_y_cfg<R, N, S, 8, false, 16>(c, f, nf, pr);
     }
@@ -2416,16 +2419,20 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
 // bit 1: z CTAs of 128 threads; bits 1 and 2: two-stage z ring, three CTAs
 // per SM; bit 3: two-stage y ring with a second exchange buffer; bit 4: y
 // passes with 16 values per thread; bits 1, 2 and 5: one-stage z ring, four
-// CTAs per SM, for lines of 256 points or more).
-static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62};
+// CTAs per SM, for lines of 256 points or more; bits 3, 4 and 6: the FP32 y
+// inverse in tiles of 4 z-lines, four CTAs per SM).
+static const int kTileCfgs[] = {0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62, 126};
 
 // a variant with bit 5 runs the same kernels as without it on z lines
-// shorter than 256 points: the autotuners skip it there
-static bool tile_cfg_distinct(const ghost_ctx *c, int cfg) { return !(cfg & 32) || c->nz >= 256; }
+// shorter than 256 points, and one with bit 6 the same as without it on FP64
+// or y lines shorter than 256 points: the autotuners skip those
+static bool tile_cfg_distinct(const ghost_ctx *c, int cfg) {
+  return (!(cfg & 32) || c->nz >= 256) && (!(cfg & 64) || (c->precision == GHOST_SINGLE && c->ny >= 256));
+}
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 63) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..63", cfg);
+  if (cfg < 0 || cfg > 127) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..127", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }

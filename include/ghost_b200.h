@@ -96,8 +96,9 @@ int ghost_ctx_set_kmax(ghost_ctx *ctx, double kmax);
  * 1 and 2 together a two-stage z ring with three CTAs per SM; bit 3 a
  * two-stage y ring with a second exchange buffer; bit 4 (FP32, y lines of
  * 256 points or more) y passes with 16 values per thread; bits 1, 2 and 5
- * (z lines of 256 points or more) a one-stage z ring with four CTAs per SM.
- * Results do not depend on the variant. */
+ * (z lines of 256 points or more) a one-stage z ring with four CTAs per SM;
+ * bits 3, 4 and 6 the FP32 y inverse in tiles of 4 z-lines (four CTAs per
+ * SM).  Results do not depend on the variant (0..127). */
 int ghost_ctx_set_tile_cfg(ghost_ctx *ctx, int cfg);
 int ghost_ctx_get_tile_cfg(const ghost_ctx *ctx, int *cfg);
 /* Times one RK step of every tile variant on a copy of v (device arrays;

@@ -441,7 +441,7 @@ def test_ensemble_graph_steps_match_oracle(prec):
     ens = Ensemble(sizes, nruns, precision=prec)
     ens.init(seeds, nus)
     cfg = ens.autotune(2, 1e-3)
-    assert len(cfg) == 2 and all(c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62) for c in cfg)
+    assert len(cfg) == 2 and all(c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62, 126) for c in cfg)
     ens.run(4, 2, 1e-3)
     e = ens.energy(1)
     tol = 1e-12 if prec == "fp64" else 1e-5
@@ -472,10 +472,10 @@ def test_tile_variants_are_bitwise_identical(prec):
     g.init_random_solenoidal(2000, 2.0, 3.0, 0, 1.0, *F)
     keep = [x.clone() for x in V0]
     cfg = g.hd_autotune(4, 5e-4, 1e-3, *V0, *F)
-    assert cfg in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62)
+    assert cfg in (0, 1, 2, 3, 6, 7, 8, 14, 16, 22, 24, 30, 38, 46, 62, 126)
     assert all(torch.equal(a, b) for a, b in zip(V0, keep))
     ref = None
-    for c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 30, 38, 62):
+    for c in (0, 1, 2, 3, 6, 7, 8, 14, 16, 30, 38, 62, 126):
         g.set_tile_cfg(c)
         V = [x.clone() for x in keep]
         g.hd_run(2, 4, 5e-4, 1e-3, *V, *F)
@@ -665,16 +665,17 @@ def test_phaseshift(prec, shape):
 # Shapes whose lines along one axis (or two) have 512 points run the same
 # kernel instantiations as the 512^3 benchmark step: xpipe_nl_kernel<*, 512,
 # ...> for nx = 512, ypipe_kernel<*, 512, ...> for ny = 512 and
-# zpipe_kernel<*, 512, ...> for nz = 512.  Tile variants 30 and 62 are the
-# FP32 benchmark's (y passes with 16 values per thread and a second exchange
-# buffer; a two-stage z ring with three CTAs per SM, or a one-stage z ring
-# with four); FP64 runs the variants the autotuner picks at 512^3 (22, 6),
-# the one-stage z ring (38) and the default.
+# zpipe_kernel<*, 512, ...> for nz = 512.  Tile variants 30, 62 and 126 are
+# the FP32 benchmark's (y passes with 16 values per thread and a second
+# exchange buffer; a two-stage z ring with three CTAs per SM, or a one-stage
+# z ring with four; 126 also runs the y inverse in 4-line tiles); FP64 runs
+# the variants the autotuner picks at 512^3 (22, 6), the one-stage z ring
+# (38) and the default.
 LINE512 = [(512, 16, 16), (16, 512, 16), (16, 16, 512), (512, 512, 16)]
 
 
 @pytest.mark.parametrize("shape", LINE512)
-@pytest.mark.parametrize("prec,cfgs,tol", [("fp64", (0, 6, 22, 38), 1e-12), ("fp32", (0, 1, 30, 62), 1e-5)])
+@pytest.mark.parametrize("prec,cfgs,tol", [("fp64", (0, 6, 22, 38), 1e-12), ("fp32", (0, 1, 30, 62, 126), 1e-5)])
 def test_forced_rk4_with_512_point_lines(shape, prec, cfgs, tol):
     """Config 1's step (forced on 2 <= |k| <= 3, nu = 1e-3, dt = 5e-4, RK4)
     for two steps (the second zero-pruned) against the FP64 oracle; every
@@ -714,7 +715,7 @@ def test_bouss_fp32_with_512_point_x_lines(shape):
     ref_v, ref_th = o.bouss_run(2, *args, v0, th0)
     g = ghost(*shape, Lx=1, Ly=1, Lz=0.25, arbsize=True, precision="fp32")
     first = None
-    for cfg in (0, 30, 62):
+    for cfg in (0, 30, 62, 126):
         g.set_tile_cfg(cfg)
         V = [to_dev(x.astype(np.complex64)) for x in v0]
         TH = to_dev(th0.astype(np.complex64))
