@@ -316,9 +316,10 @@ def e2e_host(n, steps, rank):
     """Through the public C ABI with pinned host arrays: every step copies
     the velocity and forcing in and the velocity out (GHOST's host-array
     calling convention).  The library moves the whole velocity in, the
-    forcing's live kx rows in (the rest is never read) and the velocity's
-    live kx rows out (the rest is zero in the input and the result, which
-    the library checks on the device); the byte counts are those moves."""
+    forcing's live box in (the kx rows and y-lines that hold kept modes; the
+    rest is never read) and the velocity's live box out (the rest is zero in
+    the input and the result, which the library checks on the device); the
+    byte counts are those moves."""
     import torch
     from ghost_b200 import Ghost
     g, v, f = setup_run(n, "fp32", rank)
@@ -338,13 +339,15 @@ def e2e_host(n, steps, rank):
     for _ in range(steps):
         g.hd_run(1, ORD, DT, NU, *nv, *nf)
     dt = time.perf_counter() - t0
-    rb = g.ny * g.nz * 8  # bytes of one kx row
-    live = int(round(prune_fractions(n)[1] * g.nxh))
-    dead = [int((x[live:] != 0).any()) for x in nv]  # the result's rows beyond the live ones: zero
+    from ghost_b200.roofline import live_box
+    lb = g.nz * 8  # bytes of one y-line
+    live, jt, jb = live_box(n)
+    dead = [int((x[live:] != 0).any() or (x[:live, jt:g.ny - jb] != 0).any()) for x in nv]
     g.close()
     if any(dead):
-        raise RuntimeError("the velocity holds values beyond the live kx rows")
-    return steps / dt, 3 * g.nxh * rb + 3 * live * rb, 3 * live * rb
+        raise RuntimeError("the velocity holds values outside the live box")
+    box = live * (jt + jb) * lb
+    return steps / dt, 3 * g.nxh * g.ny * lb + 3 * box, 3 * box
 
 
 def traffic_from_profiles(kernel):

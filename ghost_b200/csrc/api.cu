@@ -95,30 +95,47 @@ bool is_device_ptr(const void *p) {
 
 int check_status(ghost_ctx *c);
 
-// flag |= 1 when any byte of rows [live, rows) of any run is nonzero (a
-// field of nruns runs of `rows` kx rows of row_u4 16-byte words each)
-__global__ void dead_rows_kernel(const uint4 *__restrict__ p, int nruns, int rows, int live, size_t row_u4,
-                                 int *__restrict__ flag) {
-  const size_t per_run = (size_t)(rows - live) * row_u4, total = per_run * nruns;
+// The live box of a spectral field: kx rows [0, live) and, in each, the
+// y-lines [0, jt) and [ny - jb, ny) (a field of nruns runs of `rows` kx
+// rows of ny lines of line_u4 16-byte words).  flag |= 1 when any word
+// outside the box is nonzero.
+struct LiveBox {
+  int rows, live, ny, jt, jb;
+  size_t line_u4;
+};
+__global__ void dead_box_kernel(const uint4 *__restrict__ p, int nruns, LiveBox b, int *__restrict__ flag) {
+  const int mid = b.ny - b.jt - b.jb;  // lines between the two live blocks of a live row
+  const size_t part_a = (size_t)(b.rows - b.live) * b.ny * b.line_u4;  // the rows beyond the live ones
+  const size_t part_b = (size_t)b.live * mid * b.line_u4;               // the middle lines of the live rows
+  const size_t per_run = part_a + part_b, total = per_run * nruns;
   bool any = false;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-    const size_t r = q / per_run, o = q - r * per_run;
-    const uint4 w = p[(r * rows + live) * row_u4 + o];
-    any |= (w.x | w.y | w.z | w.w) != 0u;
+    const size_t r = q / per_run;
+    size_t o = q - r * per_run, idx;
+    if (o < part_a) {
+      idx = ((size_t)r * b.rows + b.live) * b.ny * b.line_u4 + o;
+    } else {
+      o -= part_a;
+      const size_t per_row = (size_t)mid * b.line_u4, row = o / per_row, rem = o - row * per_row;
+      const size_t line = b.jt + rem / b.line_u4, w = rem % b.line_u4;
+      idx = (((size_t)r * b.rows + row) * b.ny + line) * b.line_u4 + w;
+    }
+    const uint4 v = p[idx];
+    any |= (v.x | v.y | v.z | v.w) != 0u;
   }
   if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // Staging of host arrays for a call on device fields.  Two kinds of field
-// move only their live kx rows (rows 0..live-1 of every run, the rows that
-// hold a mode of the truncation):
-//   IN_LIVE:  an input read only at kept modes (forcing): the live rows go
-//             in, the rest of the staging buffer is never read;
+// move only their live box (LiveBox: the kx rows that hold a mode of the
+// truncation and, in them, the two blocks of y-lines that do):
+//   IN_LIVE:  an input read only at kept modes (forcing): the box goes in,
+//             the rest of the staging buffer is never read;
 //   OUT_LIVE: an in/out field that the call leaves zero outside the kept
-//             modes (the velocity): it goes in whole, and the live rows come
-//             back when the rows beyond hold zero bits both in the input and
-//             in the result (then the host array already holds them); else
-//             the whole field comes back.
+//             modes (the velocity): it goes in whole, and the box comes back
+//             when the rest holds zero bits both in the input and in the
+//             result (then the host array already holds them); else the
+//             whole field comes back.
 struct Staging {
   static constexpr int IN = 1, OUT = 2, IN_LIVE = 4, OUT_LIVE = 8;
   ghost_ctx *c;
@@ -131,18 +148,35 @@ struct Staging {
     bool live;
   };
   std::vector<Back> back;
-  // live rows per run and the rows of a run (0: unknown, whole fields move)
-  int live = 0, rows = 0;
-  size_t row_bytes = 0;
+  // the live box (live = 0: unknown, whole fields move)
+  LiveBox box{0, 0, 0, 0, 0, 0};
+  size_t line_bytes = 0;
   bool flag_armed = false;
   explicit Staging(ghost_ctx *ctx) : c(ctx) {}
-  void set_live(int live_rows, int run_rows, size_t bytes_per_row) {
-    live = live_rows;
-    rows = run_rows;
-    row_bytes = bytes_per_row;
+  void set_live(int live_rows, int run_rows, int ny, int jt, int jb, size_t bytes_per_line) {
+    box = LiveBox{run_rows, live_rows, ny, jt, jb, bytes_per_line / 16};
+    line_bytes = bytes_per_line;
   }
   bool live_ok(size_t bytes) const {
-    return live > 0 && live < rows && row_bytes % 16 == 0 && (size_t)rows * row_bytes * c->nruns == bytes;
+    return box.live > 0 && line_bytes % 16 == 0 && box.jt + box.jb <= box.ny &&
+           (box.live < box.rows || box.jt + box.jb < box.ny) &&
+           (size_t)box.rows * box.ny * line_bytes * c->nruns == bytes;
+  }
+  // the two blocks of the box of every run, host <-> device
+  int copy_box(void *dst, const void *src, cudaMemcpyKind kind) {
+    const size_t pitch = (size_t)box.ny * line_bytes, run_b = (size_t)box.rows * pitch;
+    for (int r = 0; r < c->nruns; ++r) {
+      const size_t o = (size_t)r * run_b;
+      if (box.jt > 0)
+        GB_CUDA(cudaMemcpy2DAsync((char *)dst + o, pitch, (const char *)src + o, pitch, (size_t)box.jt * line_bytes,
+                                  box.live, kind, c->stream));
+      if (box.jb > 0) {
+        const size_t ob = o + (size_t)(box.ny - box.jb) * line_bytes;
+        GB_CUDA(cudaMemcpy2DAsync((char *)dst + ob, pitch, (const char *)src + ob, pitch, (size_t)box.jb * line_bytes,
+                                  box.live, kind, c->stream));
+      }
+    }
+    return GHOST_OK;
   }
   int check_dead(const void *dev) {
     if (!c->dead_flag) {
@@ -153,10 +187,10 @@ struct Staging {
       GB_CUDA(cudaMemsetAsync(c->dead_flag, 0, sizeof(int), c->stream));
       flag_armed = true;
     }
-    const size_t total = (size_t)(rows - live) * (row_bytes / 16) * c->nruns;
-    const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
-    dead_rows_kernel<<<grid, 256, 0, c->stream>>>((const uint4 *)dev, c->nruns, rows, live, row_bytes / 16,
-                                                  c->dead_flag);
+    const size_t total = ((size_t)(box.rows - box.live) * box.ny + (size_t)box.live * (box.ny - box.jt - box.jb)) *
+                         box.line_u4 * c->nruns;
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, 148 * 8));
+    dead_box_kernel<<<grid, 256, 0, c->stream>>>((const uint4 *)dev, c->nruns, box, c->dead_flag);
     GB_CUDA(cudaGetLastError());
     return GHOST_OK;
   }
@@ -186,10 +220,8 @@ struct Staging {
     void *d;
     GB_CHECK(buffer(&d));
     const bool lv = (dir & (IN_LIVE | OUT_LIVE)) && live_ok(bytes);
-    const size_t run_b = (size_t)rows * row_bytes, live_b = (size_t)live * row_bytes;
     if ((dir & IN_LIVE) && lv)
-      GB_CUDA(cudaMemcpy2DAsync(d, run_b, (const void *)user, run_b, live_b, c->nruns, cudaMemcpyHostToDevice,
-                                c->stream));
+      GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));
     else if (dir & IN)
       GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
     if ((dir & OUT_LIVE) && lv) GB_CHECK(check_dead(d));  // the input's rows beyond the live ones
@@ -208,17 +240,16 @@ int Staging::finish() {
       any_live = true;
     }
   if (any_live) GB_CUDA(cudaMemcpyAsync(c->dead_flag_host, c->dead_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  const size_t run_b = (size_t)rows * row_bytes, live_b = (size_t)live * row_bytes;
   for (auto &b : back) {
     if (b.live)
-      GB_CUDA(cudaMemcpy2DAsync(b.host, run_b, b.dev, run_b, live_b, c->nruns, cudaMemcpyDeviceToHost, c->stream));
+      GB_CHECK(copy_box(b.host, b.dev, cudaMemcpyDeviceToHost));
     else
       GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
   }
   if (!any_host) return GHOST_OK;
   GB_CUDA(cudaStreamSynchronize(c->stream));
   if (any_live && *c->dead_flag_host != 0) {
-    // nonzero bits beyond the live rows in the input or the result: the whole field comes back
+    // nonzero bits outside the live box in the input or the result: the whole field comes back
     for (auto &b : back)
       if (b.live) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
     GB_CUDA(cudaStreamSynchronize(c->stream));
@@ -734,6 +765,8 @@ template <typename R> int build_prune(ghost_ctx *c) {
   GB_CUDA(cudaMemcpy(c->prune_jneg, jneg.data(), sizeof(int) * nxh, cudaMemcpyHostToDevice));
   c->prune_nlines = n;
   c->prune_imax = imax;
+  c->prune_jtop = *std::max_element(jpos.begin(), jpos.end());
+  c->prune_jbot = *std::max_element(jneg.begin(), jneg.end());
   return GHOST_OK;
 }
 
@@ -1402,6 +1435,7 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->prune_valid = c->prune_ok = false;
   c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
   c->prune_nlines = c->prune_imax = 0;
+  c->prune_jtop = c->prune_jbot = 0;
   c->dead_flag = c->dead_flag_host = nullptr;
   for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
     c->t_ms[k] = 0.0;
@@ -2365,12 +2399,13 @@ int ghost_hd_rkstep2(ghost_ctx *c, int o, double dt, double nu, void *vx, void *
   return st.finish();
 }
 
-// the live kx rows of the truncation for host-array staging (none known:
+// the live box of the truncation for host-array staging (none known:
 // whole fields move)
 static int staging_live_rows(ghost_ctx *c, Staging &st) {
   if (!c->prune_valid) GB_CHECK(c->precision == GHOST_SINGLE ? build_prune<float>(c) : build_prune<double>(c));
   if (c->prune_ok)
-    st.set_live(c->prune_imax + 1, c->nxh, (size_t)c->ny * c->nz * (c->precision == GHOST_SINGLE ? 8 : 16));
+    st.set_live(c->prune_imax + 1, c->nxh, c->ny, c->prune_jtop, c->prune_jbot,
+                (size_t)c->nz * (c->precision == GHOST_SINGLE ? 8 : 16));
   return GHOST_OK;
 }
 

@@ -59,3 +59,21 @@ def measured_hbm_peak():
     if os.path.exists(path):
         return float(json.load(open(path))["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def live_box(n: int):
+    """(live kx rows, y-lines from the top, y-lines from the bottom) of a cubic
+    n^3 grid's truncation: the box of the spectral field that holds every
+    kept mode (the host-array staging of ghost_hd_run moves only this box of
+    the forcing in and of the velocity out)."""
+    import numpy as np
+    kmax = np.float32(1.0 / 9.0) * np.float32(n * n)
+    nxh = n // 2 + 1
+    kx = np.arange(nxh, dtype=np.float64)
+    kx[-1] = -(n // 2)
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    live = (kx[:, None] ** 2 + ky[None, :] ** 2) <= kmax
+    rows = int(np.nonzero(live.any(axis=1))[0].max()) + 1
+    jt = int(live[:, : n // 2].sum(axis=1).max())
+    jb = int(live[:, n // 2:].sum(axis=1).max())
+    return rows, jt, jb

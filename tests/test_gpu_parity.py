@@ -259,16 +259,18 @@ def test_hd_host_arrays_drop_in():
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_hd_host_arrays_move_live_rows_only(prec):
-    """Host arrays move only the kx rows that hold kept modes where that is
-    exact: the forcing's other rows are never read (garbage there changes
-    nothing), and v comes back whole when its rows beyond the live ones
-    held nonzero values on the way in (they leave as zeros).  Every case
-    against the same run on device arrays, bit for bit."""
+    """Host arrays move only the live box (the kx rows that hold kept modes,
+    and in them the two blocks of y-lines that do) where that is exact: the
+    forcing outside it is never read (garbage there changes nothing), and v
+    comes back whole when it held nonzero values outside the box on the way
+    in (they leave as zeros).  Every case against the same run on device
+    arrays, bit for bit."""
     o = Oracle(32, precision=prec)
     g = ghost(32, precision=prec)
     v0 = solenoidal_ic(o, seed=21)
     f0, _ = o.random_solenoidal(22, 2.0, 3.0, 0, 1.0)
     live = 32 // 3 + 1  # kx rows 0..10 hold every mode with kn2 <= kmax at 32^3
+    jt, jb = 11, 10      # and in them the y-lines ky = 0..10 and -10..-1
     rng = np.random.default_rng(23)
     junk = lambda x: (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape)).astype(x.dtype)  # noqa: E731
 
@@ -279,10 +281,11 @@ def test_hd_host_arrays_move_live_rows_only(prec):
 
     # 1: v zero beyond the live rows (every step's output), forcing with junk there
     v1 = device_run(v0, f0, 1)
-    assert all(np.all(x[live:] == 0) for x in v1)
+    assert all(np.all(x[live:] == 0) and np.all(x[:, jt:32 - jb] == 0) for x in v1)
     f_junk = [x.copy() for x in f0]
     for x in f_junk:
         x[live:] = junk(x[live:])
+        x[:live, jt:32 - jb] = junk(x[:live, jt:32 - jb])
     ref = device_run(v1, f0)
     V = [x.copy() for x in v1]
     g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f_junk])
@@ -296,6 +299,15 @@ def test_hd_host_arrays_move_live_rows_only(prec):
     g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
     assert all(np.array_equal(a, b) for a, b in zip(V, ref))
     assert all(np.all(x[live:] == 0) for x in V)
+    # 2b: nonzero values in the middle y-lines of a live row only
+    v2b = [x.copy() for x in v1]
+    for x in v2b:
+        x[0, 16] = junk(x[0, 16])
+    ref = device_run(v2b, f0)
+    V = [x.copy() for x in v2b]
+    g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
+    assert all(np.array_equal(a, b) for a, b in zip(V, ref))
+    assert all(np.all(x[0, 16] == 0) for x in V)
     # 3: no step: v comes back as it went in, nonzero rows included
     V = [x.copy() for x in v2]
     g.hd_run(0, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
