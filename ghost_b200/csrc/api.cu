@@ -6,8 +6,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -132,10 +134,12 @@ __global__ void dead_box_kernel(const uint4 *__restrict__ p, int nruns, LiveBox 
 //   IN_LIVE:  an input read only at kept modes (forcing): the box goes in,
 //             the rest of the staging buffer is never read;
 //   OUT_LIVE: an in/out field that the call leaves zero outside the kept
-//             modes (the velocity): it goes in whole, and the box comes back
-//             when the rest holds zero bits both in the input and in the
-//             result (then the host array already holds them); else the
-//             whole field comes back.
+//             modes (the velocity).  The box goes in while host threads scan
+//             the rest of the host array: if it holds only zero bits, the
+//             device copy is zeroed there, else the whole field goes in.  The
+//             box comes back when the result also holds zero bits outside it
+//             (a device check; then the host array already holds them), else
+//             the whole field comes back.
 struct Staging {
   static constexpr int IN = 1, OUT = 2, IN_LIVE = 4, OUT_LIVE = 8;
   ghost_ctx *c;
@@ -145,7 +149,8 @@ struct Staging {
     void *host;
     const void *dev;
     size_t bytes;
-    bool live;
+    bool live;   // the box comes back unless the result check finds bits outside it
+    bool whole;  // the input held nonzero bits outside the box: the whole field comes back
   };
   std::vector<Back> back;
   // the live box (live = 0: unknown, whole fields move)
@@ -161,6 +166,44 @@ struct Staging {
     return box.live > 0 && line_bytes % 16 == 0 && box.jt + box.jb <= box.ny &&
            (box.live < box.rows || box.jt + box.jb < box.ny) &&
            (size_t)box.rows * box.ny * line_bytes * c->nruns == bytes;
+  }
+  // nonzero bits in a host array outside the box (up to 16 host threads,
+  // rows dealt round robin; an array not 8-byte aligned counts as nonzero)
+  bool host_outside_nonzero(const void *host) const {
+    if (((uintptr_t)host & 7u) != 0) return true;
+    const size_t row_b = (size_t)box.ny * line_bytes, nrows = (size_t)box.rows * c->nruns;
+    const size_t mid_lo = (size_t)box.jt * line_bytes, mid_hi = (size_t)(box.ny - box.jb) * line_bytes;
+    std::atomic<bool> found(false);
+    auto scan = [&](int tid, int nth) {
+      for (size_t q = tid; q < nrows && !found.load(std::memory_order_relaxed); q += nth) {
+        const size_t row = q % box.rows;
+        const uint64_t *w = (const uint64_t *)((const unsigned char *)host + q * row_b + (row < (size_t)box.live ? mid_lo : 0));
+        const size_t n = (row < (size_t)box.live ? mid_hi - mid_lo : row_b) / 8;
+        uint64_t acc = 0;
+        for (size_t k = 0; k < n; ++k) acc |= w[k];
+        if (acc) found.store(true, std::memory_order_relaxed);
+      }
+    };
+    const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; ++t) pool.emplace_back(scan, t, nth);
+    scan(0, nth);
+    for (auto &th : pool) th.join();
+    return found.load();
+  }
+  // zero a device field outside the box
+  int zero_outside(void *dev) {
+    const size_t pitch = (size_t)box.ny * line_bytes, run_b = (size_t)box.rows * pitch;
+    for (int r = 0; r < c->nruns; ++r) {
+      unsigned char *base = (unsigned char *)dev + (size_t)r * run_b;
+      if (box.rows > box.live)
+        GB_CUDA(cudaMemsetAsync(base + (size_t)box.live * pitch, 0, (size_t)(box.rows - box.live) * pitch, c->stream));
+      const int mid = box.ny - box.jt - box.jb;
+      if (mid > 0)
+        GB_CUDA(cudaMemset2DAsync(base + (size_t)box.jt * line_bytes, pitch, 0, (size_t)mid * line_bytes, box.live,
+                                  c->stream));
+    }
+    return GHOST_OK;
   }
   // the two blocks of the box of every run, host <-> device
   int copy_box(void *dst, const void *src, cudaMemcpyKind kind) {
@@ -220,12 +263,20 @@ struct Staging {
     void *d;
     GB_CHECK(buffer(&d));
     const bool lv = (dir & (IN_LIVE | OUT_LIVE)) && live_ok(bytes);
-    if ((dir & IN_LIVE) && lv)
+    bool whole = false;
+    if ((dir & IN_LIVE) && lv) {
       GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));
-    else if (dir & IN)
+    } else if ((dir & IN) && (dir & OUT_LIVE) && lv) {
+      GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));  // in flight while the host scans
+      whole = host_outside_nonzero((const void *)user);
+      if (whole)
+        GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
+      else
+        GB_CHECK(zero_outside(d));
+    } else if (dir & IN) {
       GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
-    if ((dir & OUT_LIVE) && lv) GB_CHECK(check_dead(d));  // the input's rows beyond the live ones
-    if (dir & OUT) back.push_back({(void *)user, d, bytes, (dir & OUT_LIVE) && lv});
+    }
+    if (dir & OUT) back.push_back({(void *)user, d, bytes, (dir & OUT_LIVE) && lv && !whole, whole});
     *dev = (T *)d;
     return GHOST_OK;
   }
@@ -236,7 +287,7 @@ int Staging::finish() {
   bool any_live = false;
   for (auto &b : back)
     if (b.live) {
-      GB_CHECK(check_dead(b.dev));  // the result's rows beyond the live ones
+      GB_CHECK(check_dead(b.dev));  // the result outside the live box
       any_live = true;
     }
   if (any_live) GB_CUDA(cudaMemcpyAsync(c->dead_flag_host, c->dead_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -244,12 +295,12 @@ int Staging::finish() {
     if (b.live)
       GB_CHECK(copy_box(b.host, b.dev, cudaMemcpyDeviceToHost));
     else
-      GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+      GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));  // whole field
   }
   if (!any_host) return GHOST_OK;
   GB_CUDA(cudaStreamSynchronize(c->stream));
   if (any_live && *c->dead_flag_host != 0) {
-    // nonzero bits outside the live box in the input or the result: the whole field comes back
+    // nonzero bits outside the live box in a result: the whole field comes back
     for (auto &b : back)
       if (b.live) GB_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
     GB_CUDA(cudaStreamSynchronize(c->stream));
