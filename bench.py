@@ -342,13 +342,15 @@ def e2e_host(n, steps, rank):
         g.hd_run(1, ORD, DT, NU, *nv, *nf)
     dt = time.perf_counter() - t0
     from ghost_b200.roofline import live_box
-    lb = g.nz * 8  # bytes of one y-line
-    live, jt, jb = live_box(n)
-    dead = [int((x[live:] != 0).any() or (x[:live, jt:g.ny - jb] != 0).any()) for x in nv]
+    live, jt, jb, kt, kb = live_box(n)
+    zt, zb = (kt * 8 + 15) // 16 * 2, (kb * 8 + 15) // 16 * 2  # z blocks rounded out to 16-byte words
+    dead = [int((x[live:] != 0).any() or (x[:live, jt:g.ny - jb] != 0).any()
+                or (x[:live, :jt, zt:g.nz - zb] != 0).any() or (x[:live, g.ny - jb:, zt:g.nz - zb] != 0).any())
+            for x in nv]
     g.close()
     if any(dead):
         raise RuntimeError("the velocity holds values outside the live box")
-    box = live * (jt + jb) * lb
+    box = live * (jt + jb) * (zt + zb) * 8
     return steps / dt, 6 * box, 3 * box
 
 

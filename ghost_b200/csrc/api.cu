@@ -97,30 +97,40 @@ bool is_device_ptr(const void *p) {
 
 int check_status(ghost_ctx *c);
 
-// The live box of a spectral field: kx rows [0, live) and, in each, the
-// y-lines [0, jt) and [ny - jb, ny) (a field of nruns runs of `rows` kx
-// rows of ny lines of line_u4 16-byte words).  flag |= 1 when any word
-// outside the box is nonzero.
+// The live box of a spectral field: kx rows [0, live), in each the y-lines
+// [0, jt) and [ny - jb, ny), and in each of those the 16-byte words
+// [0, kt) and [line - kb, line) of the z-line (a field of nruns runs of
+// `rows` kx rows of ny lines of line_u4 16-byte words; the z bounds are
+// rounded out to whole words).  flag |= 1 when any word outside the box is
+// nonzero.
 struct LiveBox {
   int rows, live, ny, jt, jb;
-  size_t line_u4;
+  size_t line_u4, kt, kb;
 };
 __global__ void dead_box_kernel(const uint4 *__restrict__ p, int nruns, LiveBox b, int *__restrict__ flag) {
-  const int mid = b.ny - b.jt - b.jb;  // lines between the two live blocks of a live row
+  const int mid = b.ny - b.jt - b.jb;                // lines between the two live blocks of a live row
+  const size_t midz = b.line_u4 - b.kt - b.kb;       // words between the two live z-blocks of a box line
   const size_t part_a = (size_t)(b.rows - b.live) * b.ny * b.line_u4;  // the rows beyond the live ones
   const size_t part_b = (size_t)b.live * mid * b.line_u4;               // the middle lines of the live rows
-  const size_t per_run = part_a + part_b, total = per_run * nruns;
+  const size_t part_c = (size_t)b.live * (b.jt + b.jb) * midz;         // the middle words of the box lines
+  const size_t per_run = part_a + part_b + part_c, total = per_run * nruns;
   bool any = false;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
     const size_t r = q / per_run;
     size_t o = q - r * per_run, idx;
     if (o < part_a) {
       idx = ((size_t)r * b.rows + b.live) * b.ny * b.line_u4 + o;
-    } else {
+    } else if (o < part_a + part_b) {
       o -= part_a;
       const size_t per_row = (size_t)mid * b.line_u4, row = o / per_row, rem = o - row * per_row;
       const size_t line = b.jt + rem / b.line_u4, w = rem % b.line_u4;
       idx = (((size_t)r * b.rows + row) * b.ny + line) * b.line_u4 + w;
+    } else {
+      o -= part_a + part_b;
+      const size_t per_row = (size_t)(b.jt + b.jb) * midz, row = o / per_row, rem = o - row * per_row;
+      const size_t lb = rem / midz, w = rem % midz;
+      const size_t line = lb < (size_t)b.jt ? lb : (size_t)(b.ny - b.jb) + (lb - b.jt);
+      idx = (((size_t)r * b.rows + row) * b.ny + line) * b.line_u4 + b.kt + w;
     }
     const uint4 v = p[idx];
     any |= (v.x | v.y | v.z | v.w) != 0u;
@@ -154,17 +164,22 @@ struct Staging {
   };
   std::vector<Back> back;
   // the live box (live = 0: unknown, whole fields move)
-  LiveBox box{0, 0, 0, 0, 0, 0};
+  LiveBox box{0, 0, 0, 0, 0, 0, 0, 0};
   size_t line_bytes = 0;
   bool flag_armed = false;
   explicit Staging(ghost_ctx *ctx) : c(ctx) {}
-  void set_live(int live_rows, int run_rows, int ny, int jt, int jb, size_t bytes_per_line) {
-    box = LiveBox{run_rows, live_rows, ny, jt, jb, bytes_per_line / 16};
-    line_bytes = bytes_per_line;
+  // kt, kb: live values from the top and the bottom of a z-line of `elem`
+  // bytes each (rounded out to 16-byte words)
+  void set_live(int live_rows, int run_rows, int ny, int jt, int jb, int nz, int kt, int kb, size_t elem) {
+    const size_t line_u4 = (size_t)nz * elem / 16;
+    const size_t kt_u4 = std::min(line_u4, ((size_t)kt * elem + 15) / 16);
+    const size_t kb_u4 = std::min(line_u4 - kt_u4, ((size_t)kb * elem + 15) / 16);
+    box = LiveBox{run_rows, live_rows, ny, jt, jb, line_u4, kt_u4, kb_u4};
+    line_bytes = (size_t)nz * elem;
   }
   bool live_ok(size_t bytes) const {
     return box.live > 0 && line_bytes % 16 == 0 && box.jt + box.jb <= box.ny &&
-           (box.live < box.rows || box.jt + box.jb < box.ny) &&
+           box.kt + box.kb <= box.line_u4 &&
            (size_t)box.rows * box.ny * line_bytes * c->nruns == bytes;
   }
   // nonzero bits in a host array outside the box (up to 16 host threads,
@@ -172,16 +187,29 @@ struct Staging {
   bool host_outside_nonzero(const void *host) const {
     if (((uintptr_t)host & 7u) != 0) return true;
     const size_t row_b = (size_t)box.ny * line_bytes, nrows = (size_t)box.rows * c->nruns;
-    const size_t mid_lo = (size_t)box.jt * line_bytes, mid_hi = (size_t)(box.ny - box.jb) * line_bytes;
+    const size_t z_lo = box.kt * 16, z_hi = line_bytes - box.kb * 16;  // the middle bytes of a box line
     std::atomic<bool> found(false);
+    auto any_bits = [](const unsigned char *p, size_t n) {
+      const uint64_t *w = (const uint64_t *)p;
+      uint64_t acc = 0;
+      for (size_t k = 0; k < n / 8; ++k) acc |= w[k];
+      return acc != 0;
+    };
     auto scan = [&](int tid, int nth) {
       for (size_t q = tid; q < nrows && !found.load(std::memory_order_relaxed); q += nth) {
         const size_t row = q % box.rows;
-        const uint64_t *w = (const uint64_t *)((const unsigned char *)host + q * row_b + (row < (size_t)box.live ? mid_lo : 0));
-        const size_t n = (row < (size_t)box.live ? mid_hi - mid_lo : row_b) / 8;
-        uint64_t acc = 0;
-        for (size_t k = 0; k < n; ++k) acc |= w[k];
-        if (acc) found.store(true, std::memory_order_relaxed);
+        const unsigned char *base = (const unsigned char *)host + q * row_b;
+        bool hit = false;
+        if (row >= (size_t)box.live) {
+          hit = any_bits(base, row_b);
+        } else {
+          for (int j = 0; j < box.ny && !hit; ++j) {
+            const unsigned char *line = base + (size_t)j * line_bytes;
+            hit = (j >= box.jt && j < box.ny - box.jb) ? any_bits(line, line_bytes)
+                                                        : (z_hi > z_lo && any_bits(line + z_lo, z_hi - z_lo));
+          }
+        }
+        if (hit) found.store(true, std::memory_order_relaxed);
       }
     };
     const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -194,6 +222,7 @@ struct Staging {
   // zero a device field outside the box
   int zero_outside(void *dev) {
     const size_t pitch = (size_t)box.ny * line_bytes, run_b = (size_t)box.rows * pitch;
+    const size_t midz = (box.line_u4 - box.kt - box.kb) * 16;
     for (int r = 0; r < c->nruns; ++r) {
       unsigned char *base = (unsigned char *)dev + (size_t)r * run_b;
       if (box.rows > box.live)
@@ -202,23 +231,36 @@ struct Staging {
       if (mid > 0)
         GB_CUDA(cudaMemset2DAsync(base + (size_t)box.jt * line_bytes, pitch, 0, (size_t)mid * line_bytes, box.live,
                                   c->stream));
+      // the middle of the box lines: a 3D block (z bytes, lines, rows) per line block
+      const int j0[2] = {0, box.ny - box.jb}, nj[2] = {box.jt, box.jb};
+      for (int q = 0; q < 2 && midz > 0; ++q) {
+        if (nj[q] == 0) continue;
+        cudaPitchedPtr pp = make_cudaPitchedPtr(base, line_bytes, line_bytes, box.ny);
+        pp.ptr = base + (size_t)j0[q] * line_bytes + box.kt * 16;
+        GB_CUDA(cudaMemset3DAsync(pp, 0, make_cudaExtent(midz, nj[q], box.live), c->stream));
+      }
     }
     return GHOST_OK;
   }
-  // the two blocks of the box of every run, host <-> device
+  // the four blocks of the box of every run (two line blocks times two z
+  // blocks, each a 3D copy of z bytes x lines x rows), host <-> device
   int copy_box(void *dst, const void *src, cudaMemcpyKind kind) {
     const size_t pitch = (size_t)box.ny * line_bytes, run_b = (size_t)box.rows * pitch;
-    for (int r = 0; r < c->nruns; ++r) {
-      const size_t o = (size_t)r * run_b;
-      if (box.jt > 0)
-        GB_CUDA(cudaMemcpy2DAsync((char *)dst + o, pitch, (const char *)src + o, pitch, (size_t)box.jt * line_bytes,
-                                  box.live, kind, c->stream));
-      if (box.jb > 0) {
-        const size_t ob = o + (size_t)(box.ny - box.jb) * line_bytes;
-        GB_CUDA(cudaMemcpy2DAsync((char *)dst + ob, pitch, (const char *)src + ob, pitch, (size_t)box.jb * line_bytes,
-                                  box.live, kind, c->stream));
-      }
-    }
+    const int j0[2] = {0, box.ny - box.jb}, nj[2] = {box.jt, box.jb};
+    const size_t z0[2] = {0, line_bytes - box.kb * 16}, nz[2] = {box.kt * 16, box.kb * 16};
+    for (int r = 0; r < c->nruns; ++r)
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          if (nj[a] == 0 || nz[b] == 0) continue;
+          cudaMemcpy3DParms prm = {};
+          prm.srcPtr = make_cudaPitchedPtr(const_cast<void *>(src), line_bytes, line_bytes, box.ny);
+          prm.dstPtr = make_cudaPitchedPtr(dst, line_bytes, line_bytes, box.ny);
+          prm.srcPos = prm.dstPos = make_cudaPos(z0[b], (size_t)j0[a], (size_t)r * box.rows);
+          prm.extent = make_cudaExtent(nz[b], nj[a], box.live);
+          prm.kind = kind;
+          GB_CUDA(cudaMemcpy3DAsync(&prm, c->stream));
+        }
+    (void)run_b;
     return GHOST_OK;
   }
   int check_dead(const void *dev) {
@@ -230,8 +272,10 @@ struct Staging {
       GB_CUDA(cudaMemsetAsync(c->dead_flag, 0, sizeof(int), c->stream));
       flag_armed = true;
     }
-    const size_t total = ((size_t)(box.rows - box.live) * box.ny + (size_t)box.live * (box.ny - box.jt - box.jb)) *
-                         box.line_u4 * c->nruns;
+    const size_t total = (((size_t)(box.rows - box.live) * box.ny + (size_t)box.live * (box.ny - box.jt - box.jb)) *
+                              box.line_u4 +
+                          (size_t)box.live * (box.jt + box.jb) * (box.line_u4 - box.kt - box.kb)) *
+                         c->nruns;
     const int grid = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, 148 * 8));
     dead_box_kernel<<<grid, 256, 0, c->stream>>>((const uint4 *)dev, c->nruns, box, c->dead_flag);
     GB_CUDA(cudaGetLastError());
@@ -818,6 +862,22 @@ template <typename R> int build_prune(ghost_ctx *c) {
   c->prune_imax = imax;
   c->prune_jtop = *std::max_element(jpos.begin(), jpos.end());
   c->prune_jbot = *std::max_element(jneg.begin(), jneg.end());
+  // kz values that can be kept: kn2 >= its kz term (every term is >= 0 and
+  // the sums round monotonically), so |kz| beyond those is never kept
+  auto kz_term = [&](int k) -> R {
+    const R cz = (R)(k < kp.nz / 2 ? k : k - kp.nz);
+    volatile R cc = cz * cz;
+    if (kp.anis) {
+      volatile R z = kp.rms * cc;
+      return z + (R)0;
+    }
+    return cc + (R)0;
+  };
+  int kt = 0, kb = 0;
+  while (kt < kp.nz / 2 && kz_term(kt) <= kp.kmax) ++kt;
+  while (kb < kp.nz - kp.nz / 2 && kz_term(kp.nz - 1 - kb) <= kp.kmax) ++kb;
+  c->prune_ktop = kt;
+  c->prune_kbot = kb;
   return GHOST_OK;
 }
 
@@ -1487,6 +1547,7 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->prune_lines = c->prune_jpos = c->prune_jneg = nullptr;
   c->prune_nlines = c->prune_imax = 0;
   c->prune_jtop = c->prune_jbot = 0;
+  c->prune_ktop = c->prune_kbot = 0;
   c->dead_flag = c->dead_flag_host = nullptr;
   for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
     c->t_ms[k] = 0.0;
@@ -2455,8 +2516,8 @@ int ghost_hd_rkstep2(ghost_ctx *c, int o, double dt, double nu, void *vx, void *
 static int staging_live_rows(ghost_ctx *c, Staging &st) {
   if (!c->prune_valid) GB_CHECK(c->precision == GHOST_SINGLE ? build_prune<float>(c) : build_prune<double>(c));
   if (c->prune_ok)
-    st.set_live(c->prune_imax + 1, c->nxh, c->ny, c->prune_jtop, c->prune_jbot,
-                (size_t)c->nz * (c->precision == GHOST_SINGLE ? 8 : 16));
+    st.set_live(c->prune_imax + 1, c->nxh, c->ny, c->prune_jtop, c->prune_jbot, c->nz, c->prune_ktop, c->prune_kbot,
+                c->precision == GHOST_SINGLE ? 8 : 16);
   return GHOST_OK;
 }
 

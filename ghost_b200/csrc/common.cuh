@@ -134,6 +134,7 @@ struct ghost_ctx {
   int *prune_lines, *prune_jpos, *prune_jneg;
   int prune_nlines, prune_imax;
   int prune_jtop, prune_jbot;  // largest live y-line counts from the top and the bottom over the kx rows
+  int prune_ktop, prune_kbot;  // live kz counts from the top and the bottom of a z-line
   // host-array calls: a device flag and its pinned host copy (nonzero values
   // beyond the live kx rows of a staged field), allocated on first use
   int *dead_flag, *dead_flag_host;

@@ -62,10 +62,11 @@ def measured_hbm_peak():
 
 
 def live_box(n: int):
-    """(live kx rows, y-lines from the top, y-lines from the bottom) of a cubic
-    n^3 grid's truncation: the box of the spectral field that holds every
-    kept mode (the host-array staging of ghost_hd_run moves only this box of
-    the forcing in and of the velocity out)."""
+    """(live kx rows, y-lines from the top, y-lines from the bottom, kz values
+    from the top, kz values from the bottom) of a cubic n^3 grid's
+    truncation: the box of the spectral field that holds every kept mode
+    (the host-array staging of ghost_hd_run moves only this box, its z
+    blocks rounded out to 16-byte words)."""
     import numpy as np
     kmax = np.float32(1.0 / 9.0) * np.float32(n * n)
     nxh = n // 2 + 1
@@ -76,4 +77,8 @@ def live_box(n: int):
     rows = int(np.nonzero(live.any(axis=1))[0].max()) + 1
     jt = int(live[:, : n // 2].sum(axis=1).max())
     jb = int(live[:, n // 2:].sum(axis=1).max())
-    return rows, jt, jb
+    kz = np.fft.fftfreq(n, 1.0 / n)
+    zl = kz ** 2 <= kmax
+    kt = int(zl[: n // 2].sum())
+    kb = int(zl[n // 2:].sum())
+    return rows, jt, jb, kt, kb

@@ -353,8 +353,8 @@ int ghost_hd_rkstep2(ghost_ctx *ctx, int o, double dt, double nu, void *vx, void
 /* nsteps steps of the loop main3D.fpp:3195-3231 (RK1 then DO o=ord,1,-1
  * RK2), the copy of RK1 fused into the first substep.  C1..C3 are the
  * RK storage (device, or NULL: context-owned).  f may be NULL.  With host
- * arrays, only the live box of f and v crosses the bus (the kx rows and
- * y-lines that hold a mode of the truncation), as long as v holds only zero
+ * arrays, only the live box of f and v crosses the bus (the kx rows, y-lines
+ * and kz values that can hold a mode of the truncation), as long as v holds only zero
  * bits outside it, on the way in (scanned by up to 16 host threads during
  * the copy) and in the result (checked on the device); otherwise the whole
  * of v moves.  The results are the same bits either way. */

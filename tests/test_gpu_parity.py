@@ -270,7 +270,8 @@ def test_hd_host_arrays_move_live_rows_only(prec):
     v0 = solenoidal_ic(o, seed=21)
     f0, _ = o.random_solenoidal(22, 2.0, 3.0, 0, 1.0)
     live = 32 // 3 + 1  # kx rows 0..10 hold every mode with kn2 <= kmax at 32^3
-    jt, jb = 11, 10      # and in them the y-lines ky = 0..10 and -10..-1
+    jt, jb = 11, 10      # and in them the y-lines ky = 0..10 and -10..-1, and the kz values 0..10, -10..-1
+    zt, zb = (12, 10) if prec == "fp32" else (11, 10)  # the z blocks in whole 16-byte words
     rng = np.random.default_rng(23)
     junk = lambda x: (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape)).astype(x.dtype)  # noqa: E731
 
@@ -281,11 +282,13 @@ def test_hd_host_arrays_move_live_rows_only(prec):
 
     # 1: v zero beyond the live rows (every step's output), forcing with junk there
     v1 = device_run(v0, f0, 1)
-    assert all(np.all(x[live:] == 0) and np.all(x[:, jt:32 - jb] == 0) for x in v1)
+    assert all(np.all(x[live:] == 0) and np.all(x[:, jt:32 - jb] == 0) and np.all(x[:, :, zt:32 - zb] == 0)
+               for x in v1)
     f_junk = [x.copy() for x in f0]
     for x in f_junk:
         x[live:] = junk(x[live:])
         x[:live, jt:32 - jb] = junk(x[:live, jt:32 - jb])
+        x[:live, :, zt:32 - zb] = junk(x[:live, :, zt:32 - zb])
     ref = device_run(v1, f0)
     V = [x.copy() for x in v1]
     g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f_junk])
@@ -308,6 +311,15 @@ def test_hd_host_arrays_move_live_rows_only(prec):
     g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
     assert all(np.array_equal(a, b) for a, b in zip(V, ref))
     assert all(np.all(x[0, 16] == 0) for x in V)
+    # 2c: nonzero values in the middle kz of a box line only
+    v2c = [x.copy() for x in v1]
+    for x in v2c:
+        x[1, 2, 16] = 1.5 + 0.5j
+    ref = device_run(v2c, f0)
+    V = [x.copy() for x in v2c]
+    g.hd_run(2, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
+    assert all(np.array_equal(a, b) for a, b in zip(V, ref))
+    assert all(x[1, 2, 16] == 0 for x in V)
     # 3: no step: v comes back as it went in, nonzero rows included
     V = [x.copy() for x in v2]
     g.hd_run(0, 2, 1e-3, 2e-3, *V, *[x.copy() for x in f0])
