@@ -307,27 +307,49 @@ struct Staging {
     void *d;
     GB_CHECK(buffer(&d));
     const bool lv = (dir & (IN_LIVE | OUT_LIVE)) && live_ok(bytes);
-    bool whole = false;
     if ((dir & IN_LIVE) && lv) {
       GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));
     } else if ((dir & IN) && (dir & OUT_LIVE) && lv) {
-      GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));  // in flight while the host scans
-      whole = host_outside_nonzero((const void *)user);
-      if (whole)
-        GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
-      else
-        GB_CHECK(zero_outside(d));
+      GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));  // in flight while resolve() scans
+      pending.push_back({(const void *)user, d, bytes, back.size()});
     } else if (dir & IN) {
       GB_CUDA(cudaMemcpyAsync(d, (const void *)user, bytes, cudaMemcpyHostToDevice, c->stream));
     }
-    if (dir & OUT) back.push_back({(void *)user, d, bytes, (dir & OUT_LIVE) && lv && !whole, whole});
+    if (dir & OUT) back.push_back({(void *)user, d, bytes, (dir & OUT_LIVE) && lv, false});
     *dev = (T *)d;
+    return GHOST_OK;
+  }
+  // OUT_LIVE inputs whose boxes are in flight: the host scans the rest of
+  // each while the copies run, then zeroes the device copy there or sends
+  // the whole field (call after the last map, before the work)
+  struct Pending {
+    const void *host;
+    void *dev;
+    size_t bytes;
+    size_t back_index;  // the field's entry in back, or back.size() for an input only
+  };
+  std::vector<Pending> pending;
+  int resolve() {
+    for (auto &p : pending) {
+      const bool whole = host_outside_nonzero(p.host);
+      if (whole) {
+        GB_CUDA(cudaMemcpyAsync(p.dev, p.host, p.bytes, cudaMemcpyHostToDevice, c->stream));
+        if (p.back_index < back.size()) {
+          back[p.back_index].live = false;
+          back[p.back_index].whole = true;
+        }
+      } else {
+        GB_CHECK(zero_outside(p.dev));
+      }
+    }
+    pending.clear();
     return GHOST_OK;
   }
   int finish();
 };
 
 int Staging::finish() {
+  if (!pending.empty()) return fail(GHOST_ERR_STATE, "staged inputs left unresolved");
   bool any_live = false;
   for (auto &b : back)
     if (b.live) {
@@ -2549,6 +2571,7 @@ int ghost_hd_run(ghost_ctx *c, int nsteps, int ord, double dt, double nu, void *
       Cd[q] = c->rk[q];
     }
   }
+  GB_CHECK(st.resolve());  // every box is queued: the host scans v while they copy
   // The first substep of a call reads v on the whole grid (it may hold
   // modes outside the truncation); its update leaves v zero there, so the
   // later substeps skip the known zeros.
