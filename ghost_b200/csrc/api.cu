@@ -138,11 +138,22 @@ __global__ void dead_box_kernel(const uint4 *__restrict__ p, int nruns, LiveBox 
   if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
+// the context stream waits for late inputs still in flight (ghost_ctx::late_pending)
+static int late_wait(ghost_ctx *c) {
+  if (c->late_pending) {
+    GB_CUDA(cudaStreamWaitEvent(c->stream, c->ev_late, 0));
+    c->late_pending = false;
+  }
+  return GHOST_OK;
+}
+
 // Staging of host arrays for a call on device fields.  Two kinds of field
 // move only their live box (LiveBox: the kx rows that hold a mode of the
 // truncation and, in them, the two blocks of y-lines that do):
-//   IN_LIVE:  an input read only at kept modes (forcing): the box goes in,
-//             the rest of the staging buffer is never read;
+//   IN_LIVE:  an input read only at kept modes and only late in a substep
+//             (the forcing): the box goes in on a side stream after the
+//             early inputs, while the work starts, and the read waits for it
+//             (late_wait); the rest of the staging buffer is never read;
 //   OUT_LIVE: an in/out field that the call leaves zero outside the kept
 //             modes (the velocity).  The box goes in while host threads scan
 //             the rest of the host array: if it holds only zero bits, the
@@ -244,7 +255,8 @@ struct Staging {
   }
   // the four blocks of the box of every run (two line blocks times two z
   // blocks, each a 3D copy of z bytes x lines x rows), host <-> device
-  int copy_box(void *dst, const void *src, cudaMemcpyKind kind) {
+  int copy_box(void *dst, const void *src, cudaMemcpyKind kind, cudaStream_t stream = nullptr) {
+    if (!stream) stream = c->stream;
     const size_t pitch = (size_t)box.ny * line_bytes, run_b = (size_t)box.rows * pitch;
     const int j0[2] = {0, box.ny - box.jb}, nj[2] = {box.jt, box.jb};
     const size_t z0[2] = {0, line_bytes - box.kb * 16}, nz[2] = {box.kt * 16, box.kb * 16};
@@ -258,7 +270,7 @@ struct Staging {
           prm.srcPos = prm.dstPos = make_cudaPos(z0[b], (size_t)j0[a], (size_t)r * box.rows);
           prm.extent = make_cudaExtent(nz[b], nj[a], box.live);
           prm.kind = kind;
-          GB_CUDA(cudaMemcpy3DAsync(&prm, c->stream));
+          GB_CUDA(cudaMemcpy3DAsync(&prm, stream));
         }
     (void)run_b;
     return GHOST_OK;
@@ -308,7 +320,7 @@ struct Staging {
     GB_CHECK(buffer(&d));
     const bool lv = (dir & (IN_LIVE | OUT_LIVE)) && live_ok(bytes);
     if ((dir & IN_LIVE) && lv) {
-      GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));
+      late.push_back({(const void *)user, d});  // copied by resolve() on the side stream
     } else if ((dir & IN) && (dir & OUT_LIVE) && lv) {
       GB_CHECK(copy_box(d, (const void *)user, cudaMemcpyHostToDevice));  // in flight while resolve() scans
       pending.push_back({(const void *)user, d, bytes, back.size()});
@@ -329,7 +341,31 @@ struct Staging {
     size_t back_index;  // the field's entry in back, or back.size() for an input only
   };
   std::vector<Pending> pending;
+  // IN_LIVE inputs (read late in a substep): their boxes go on the side
+  // stream after the early inputs, while the work starts; the first read
+  // waits on ev_late (late_wait)
+  struct Late {
+    const void *host;
+    void *dev;
+  };
+  std::vector<Late> late;
   int resolve() {
+    // the late boxes first, on the side stream after the early boxes (and
+    // after the last call's reads of these buffers), so that the copies run
+    // back to back while the host scans
+    if (!late.empty()) {
+      if (!c->side) {
+        GB_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        GB_CUDA(cudaEventCreateWithFlags(&c->ev_early, cudaEventDisableTiming));
+        GB_CUDA(cudaEventCreateWithFlags(&c->ev_late, cudaEventDisableTiming));
+      }
+      GB_CUDA(cudaEventRecord(c->ev_early, c->stream));
+      GB_CUDA(cudaStreamWaitEvent(c->side, c->ev_early, 0));
+      for (auto &l : late) GB_CHECK(copy_box(l.dev, l.host, cudaMemcpyHostToDevice, c->side));
+      GB_CUDA(cudaEventRecord(c->ev_late, c->side));
+      c->late_pending = true;
+      late.clear();
+    }
     for (auto &p : pending) {
       const bool whole = host_outside_nonzero(p.host);
       if (whole) {
@@ -349,7 +385,8 @@ struct Staging {
 };
 
 int Staging::finish() {
-  if (!pending.empty()) return fail(GHOST_ERR_STATE, "staged inputs left unresolved");
+  if (!pending.empty() || !late.empty()) return fail(GHOST_ERR_STATE, "staged inputs left unresolved");
+  GB_CHECK(late_wait(c));  // a call with no step still orders the late copies before returning
   bool any_live = false;
   for (auto &b : back)
     if (b.live) {
@@ -1052,6 +1089,7 @@ int hd_substep_dev(ghost_ctx *c, int o, double dt, double nu, void *const v[3], 
   GB_CHECK((launch_y<R, +1>(c, fy, 6, pr)));
   GB_CHECK((launch_x<R, X_HD>(c, nullptr, nullptr, (const void *const *)w, (void *const *)w, pr.rows)));
   GB_CHECK((launch_y<R, -1>(c, fy, 3, pr)));
+  GB_CHECK(late_wait(c));  // a staged forcing may still be on its way
   ZFwdHD<R> zf{};
   for (int q = 0; q < 3; ++q) {
     zf.nl.p[q] = (const cx<R> *)w[q];
@@ -1571,6 +1609,9 @@ int ghost_ctx_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, in
   c->prune_jtop = c->prune_jbot = 0;
   c->prune_ktop = c->prune_kbot = 0;
   c->dead_flag = c->dead_flag_host = nullptr;
+  c->side = nullptr;
+  c->ev_early = c->ev_late = nullptr;
+  c->late_pending = false;
   for (int k = 0; k < GHOST_TIMER_KINDS; ++k) {
     c->t_ms[k] = 0.0;
     c->t_n[k] = 0;
@@ -1608,6 +1649,12 @@ int ghost_ctx_destroy(ghost_ctx *c) {
   cudaFree(c->prune_jneg);
   cudaFree(c->dead_flag);
   if (c->dead_flag_host) cudaFreeHost(c->dead_flag_host);
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
+  }
+  if (c->ev_early) cudaEventDestroy(c->ev_early);
+  if (c->ev_late) cudaEventDestroy(c->ev_late);
   for (auto &p : c->ev_pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);

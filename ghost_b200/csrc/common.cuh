@@ -138,6 +138,12 @@ struct ghost_ctx {
   // host-array calls: a device flag and its pinned host copy (nonzero values
   // beyond the live kx rows of a staged field), allocated on first use
   int *dead_flag, *dead_flag_host;
+  // host-array calls: a second stream for inputs needed late in a substep
+  // (the forcing), the event after the early inputs, the event the next
+  // forcing read waits on (f_pending), all created on first use
+  cudaStream_t side;
+  cudaEvent_t ev_early, ev_late;
+  bool late_pending;
   // per-kernel timers (ghost_ctx_enable_timers)
   bool timers_on;
   std::vector<cudaEvent_t> ev_free;
