@@ -227,12 +227,14 @@ __global__ void spec_features_kernel(const double *__restrict__ E, int kc, float
 
 // tve(k) of the spectral network: the first output of row k-1 times
 // out_scale sqrt(E(kc)/kc) (Kraichnan's scaling of a spectral eddy
-// viscosity at the cutoff) for k <= kc, zero beyond
+// viscosity at the cutoff) for k <= kc, zero beyond, and never negative: a
+// negative eddy viscosity (backscatter) would feed its shell without
+// bound once the molecular viscosity is below it
 __global__ void spec_tve_kernel(const float *__restrict__ y, const double *__restrict__ E, int kc, int nb,
                                 double out_scale, double *__restrict__ tve) {
   const double s = out_scale * sqrt(fmax(E[kc - 1], 0.0) / (double)kc);
   for (int k = 1 + (int)threadIdx.x; k <= nb; k += (int)blockDim.x)
-    tve[k - 1] = k <= kc ? (double)y[(size_t)(k - 1) * GHOST_MLP_NOUT] * s : 0.0;
+    tve[k - 1] = k <= kc ? fmax((double)y[(size_t)(k - 1) * GHOST_MLP_NOUT] * s, 0.0) : 0.0;
 }
 
 // ---------------------------------------------------------------------

@@ -50,7 +50,7 @@ def spectrum_errors(E_les, E_dns, kc):
 def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_ratio=4, ord=4, spinup=4000,
         nsnap=40, snap_every=100, val_snaps=4, train_steps=4000, batch=65536, lr=2e-3, seed=7, kolmo=1.4,
         models=("none", "edqnm", "mlp", "mlp_cal", "mlp_spectral"), deviatoric=True, spec_train_steps=3000,
-        spec_lr=3e-3, log=print):
+        spec_lr=3e-3, fallback=False, log=print):
     import numpy as np
     import torch
 
@@ -69,7 +69,7 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
                           les_dt=dt * les_dt_ratio, ord=ord, spinup=spinup, nsnap=nsnap, snap_every=snap_every,
                           val_snaps=val_snaps, train_steps=train_steps, batch=batch, lr=lr, seed=seed,
                           kolmo=kolmo, deviatoric=deviatoric, spec_train_steps=spec_train_steps, spec_lr=spec_lr,
-                          precision="fp32")}
+                          fallback=fallback, precision="fp32")}
 
     # ---- 1. DNS
     g = Ghost(dns_n, precision="fp32")
@@ -240,11 +240,13 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     for model in models:
         vl = [x.clone() for x in v0]
         if model == "mlp":
-            les.set_model("mlp", mlp, grad_scale=gs, tau_scale=1.0 / ts, delta=1.0)
+            les.set_model("mlp", mlp, grad_scale=gs, tau_scale=1.0 / ts, delta=1.0, kolmo=kolmo)
         elif model == "mlp_cal":
-            les.set_model("mlp", mlp, grad_scale=gs, tau_scale=cal / ts, delta=1.0)
+            les.set_model("mlp", mlp, grad_scale=gs, tau_scale=cal / ts, delta=1.0, kolmo=kolmo)
         elif model == "mlp_spectral":
-            les.set_model("mlp_spectral", mlp_s, tau_scale=1.0 / so)
+            les.set_model("mlp_spectral", mlp_s, tau_scale=1.0 / so, kolmo=kolmo)
+        if model.startswith("mlp"):
+            les.set_fallback(fallback)  # a learned closure that blows up hands over to EDQNM
         elif model == "edqnm":
             les.set_model("edqnm", kolmo=kolmo)
         else:
@@ -267,6 +269,8 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
         steps = (len(spectra) - 1) * sub
         res = {"finite": ok, "steps": steps, "ms": ms, "ms_per_step": ms / max(1, steps),
                "energy_final": float(np.sum(spectra[-1]))}
+        if model.startswith("mlp") and fallback:
+            res["closure_at_end"], res["fell_back_at_step"] = les.status()
         if ok:
             res["error_time_avg"] = spectrum_errors(spectra[1:].mean(0), E_dns[1:].mean(0), kc)
             res["error_final"] = spectrum_errors(spectra[-1], E_dns[-1], kc)
@@ -327,13 +331,14 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--val-snaps", type=int, default=4)
     ap.add_argument("--full-stress", action="store_true", help="train on tau with its trace")
+    ap.add_argument("--fallback", action="store_true", help="learned closures hand over to EDQNM on a blow-up")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     t = time.time()
     res = run(dns_n=a.dns_n, les_n=a.les_n, kc=a.kc, nu_dns=a.nu_dns, nu_les=a.nu_les, dt=a.dt,
               les_dt_ratio=a.les_dt_ratio, spinup=a.spinup, nsnap=a.nsnap, snap_every=a.snap_every,
               train_steps=a.train_steps, batch=a.batch, lr=a.lr, val_snaps=a.val_snaps,
-              deviatoric=not a.full_stress)
+              deviatoric=not a.full_stress, fallback=a.fallback)
     res["wall_s"] = time.time() - t
     summary = {k: res[k] for k in ("config", "dns", "cost")}
     summary["training"] = {k: v for k, v in res["training"].items() if k != "history"}

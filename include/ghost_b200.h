@@ -496,9 +496,10 @@ int ghost_mlp_train_step(ghost_mlp *mlp, const float *x, const float *t, int B, 
  *                    the force -P div tau (P the Leray projection);
  *   GHOST_LES_MLP_SPECTRAL  a learned spectral eddy viscosity: the network
  *                    maps each resolved shell's inputs (ghost_les_spectral_features,
- *                    from the current kinetic spectrum) to tve(k) = y0
- *                    tau_scale sqrt(E(kc)/kc), applied as EDQNM's tve is
- *                    (the update uses nu + tve(k)), without vcorrect. */
+ *                    from the current kinetic spectrum) to tve(k) =
+ *                    max(y0 tau_scale sqrt(E(kc)/kc), 0), applied as
+ *                    EDQNM's tve is (the update uses nu + tve(k)), without
+ *                    vcorrect. */
 #define GHOST_LES_NONE 0
 #define GHOST_LES_EDQNM 1
 #define GHOST_LES_MLP 2

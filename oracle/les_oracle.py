@@ -123,8 +123,9 @@ def spectral_features(E, kc):
 
 
 def spectral_tve(y0, E, kc, nb, out_scale):
-    """tve of the spectral closure: y0[k-1] out_scale sqrt(E(kc)/kc) for k <= kc, 0 beyond."""
+    """tve of the spectral closure: max(y0[k-1] out_scale sqrt(E(kc)/kc), 0)
+    for k <= kc, 0 beyond."""
     s = out_scale * np.sqrt(max(float(E[kc - 1]), 0.0) / kc)
     t = np.zeros(nb)
-    t[:kc] = np.asarray(y0, dtype=np.float64)[:kc] * s
+    t[:kc] = np.maximum(np.asarray(y0, dtype=np.float64)[:kc] * s, 0.0)
     return t
