@@ -18,7 +18,8 @@
    snapshot's filtered spectrum (ghost_les_spectral_features) to the
    a-priori nu_t(k) = -S(k)/D(k) of that snapshot, S the subgrid energy
    transfer of shell k and D its sum of k^2 |ubar|^2, in units of
-   sqrt(E(kc)/kc).
+   sqrt(E(kc)/kc); for an LES at a lower viscosity than the DNS the
+   difference nu_dns - nu_les joins the target.
 4. LES: from the filtered first snapshot, the coarse grid is advanced over
    the same time window with no closure, GHOST's EDQNM eddy viscosity, and
    the trained networks; spectra at the snapshot times.
@@ -203,8 +204,10 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
 
     # ---- 3b. the spectral network: shell inputs of each snapshot's filtered
     # spectrum -> nu_t(k) / sqrt(E(kc)/kc), trained on the a-priori eddy
-    # viscosity of the training snapshots
-    nu_ap = -S_sgs[:, :kc] / D_sgs[:, :kc]
+    # viscosity of the training snapshots.  An LES at a lower viscosity than
+    # the DNS must also dissipate what the DNS's extra viscosity did on the
+    # resolved shells: nu_t(k) = -S(k)/D(k) + (nu_dns - nu_les)
+    nu_ap = -S_sgs[:, :kc] / D_sgs[:, :kc] + (nu_dns - nu_les)
     vel = np.sqrt(np.maximum(E_dns[:, kc - 1], 0.0) / kc)
     xs = torch.cat([les.spectral_features(torch.tensor(E_dns[q], device=dev)) for q in range(nsnap)])
     ys0 = nu_ap / vel[:, None]
