@@ -51,7 +51,7 @@ def spectrum_errors(E_les, E_dns, kc):
 def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_ratio=4, ord=4, spinup=4000,
         nsnap=40, snap_every=100, val_snaps=4, train_steps=4000, batch=65536, lr=2e-3, seed=7, kolmo=1.4,
         models=("none", "edqnm", "mlp", "mlp_cal", "mlp_spectral"), deviatoric=True, spec_train_steps=3000,
-        spec_lr=3e-3, fallback=False, log=print):
+        spec_lr=3e-3, fallback=False, spectral_from=None, log=print):
     import numpy as np
     import torch
 
@@ -218,6 +218,15 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
     xs_va, ys_va = xs[ntr * kc:].contiguous(), ys[ntr * kc:].contiguous()
     mlp_s = MLP(seed + 1)
     e0.record(stream)
+    if spectral_from is not None:
+        # a spectral network trained elsewhere (another cutoff or grid): its
+        # inputs and output are in units of kc and sqrt(E(kc)/kc), so it is
+        # used as it is, with its own output scale
+        mlp_s.params = np.asarray(spectral_from["params"], dtype=np.float32)
+        so = 1.0 / float(spectral_from["out_scale"])
+        ys[:, 0] = torch.tensor((ys0 * so).ravel(), dtype=torch.float32, device=dev)
+        xs_va, ys_va = xs[ntr * kc:].contiguous(), ys[ntr * kc:].contiguous()
+        spec_train_steps = 0
     for step in range(spec_train_steps):
         lr_s = spec_lr * 0.5 * (1.0 + np.cos(np.pi * step / spec_train_steps))
         mlp_s.train_step(xs_tr, ys_tr, lr_s, want_loss=False)
@@ -310,6 +319,8 @@ def run(dns_n=512, les_n=128, kc=42, nu_dns=1e-3, nu_les=None, dt=5e-4, les_dt_r
         out["cost"][f"{model}_speedup_vs_dns"] = dns_per_t / les_per_t if les_per_t > 0 else None
     out["mlp_params"] = mlp.params.tolist()
     out["mlp_spectral_params"] = mlp_s.params.tolist()
+    if spectral_from is not None:
+        out["training_spectral"]["trained_on"] = spectral_from.get("from")
     les.close()
     c.close()
     mlp.close()
@@ -335,13 +346,20 @@ def main(argv=None):
     ap.add_argument("--val-snaps", type=int, default=4)
     ap.add_argument("--full-stress", action="store_true", help="train on tau with its trace")
     ap.add_argument("--fallback", action="store_true", help="learned closures hand over to EDQNM on a blow-up")
+    ap.add_argument("--spectral-from", default=None,
+                    help="a result file (--out) whose spectral network is used instead of training one")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    spec = None
+    if a.spectral_from:
+        r0 = json.load(open(a.spectral_from))
+        spec = {"params": r0["mlp_spectral_params"], "out_scale": r0["training_spectral"]["out_scale"],
+                "from": r0["config"]}
     t = time.time()
     res = run(dns_n=a.dns_n, les_n=a.les_n, kc=a.kc, nu_dns=a.nu_dns, nu_les=a.nu_les, dt=a.dt,
               les_dt_ratio=a.les_dt_ratio, spinup=a.spinup, nsnap=a.nsnap, snap_every=a.snap_every,
               train_steps=a.train_steps, batch=a.batch, lr=a.lr, val_snaps=a.val_snaps,
-              deviatoric=not a.full_stress, fallback=a.fallback)
+              deviatoric=not a.full_stress, fallback=a.fallback, spectral_from=spec)
     res["wall_s"] = time.time() - t
     summary = {k: res[k] for k in ("config", "dns", "cost")}
     summary["training"] = {k: v for k, v in res["training"].items() if k != "history"}
