@@ -819,6 +819,16 @@ template <typename R, int NX, int KIND> int launch_x_n(ghost_ctx *c, const void 
         return post_launch(c);
       }
     }
+    // FP32 1024-point lines: tiles of 8 z-values (64-byte rows instead of
+    // 32, one CTA of 512 threads per SM) where nz allows (bit 8 of the tile
+    // variant asks for the 4-value tiles)
+    if constexpr (sizeof(R) == 4 && NX == 1024 && BZ == 4) {
+      if (c->nz % 8 == 0 && !(c->tile_cfg & 256)) {
+        GB_CHECK((launch_x_fused<R, NX, KIND, 8, 1>(c, ins, outs, rows)));
+        timer_end(c, ts);
+        return post_launch(c);
+      }
+    }
     GB_CHECK((launch_x_fused<R, NX, KIND, BZ, 2>(c, ins, outs, rows)));
   } else if (KIND == X_C2R && xw_plain_ok(c)) {
     GB_CHECK(launch_xw_c2r(c, in, out));
@@ -2649,7 +2659,7 @@ static bool tile_cfg_distinct(const ghost_ctx *c, int cfg) {
 
 int ghost_ctx_set_tile_cfg(ghost_ctx *c, int cfg) {
   CTX_CHECK(c);
-  if (cfg < 0 || cfg > 127) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..127", cfg);
+  if (cfg < 0 || cfg > 511) return fail(GHOST_ERR_ARG, "tile variant %d not in 0..511", cfg);
   c->tile_cfg = cfg;
   return GHOST_OK;
 }
