@@ -15,8 +15,14 @@ library FFT, as GHOST's FFTW/OpenMP build runs them (GHOST itself needs
 Fortran, MPI and FFTW, none of which exist here).  Each of its steps is a
 bounded sample, one RK substep, so that the run ends within minutes.
 With torchrun (N > 1) the ranks advance ONE 512^3 run split into GHOST's
-kx-slabs / z-slabs, with an NCCL all-to-all per transform direction
-(strong scaling); N = 1 runs the undivided fused step.
+kx-slabs / z-slabs, with NCCL all-to-alls in field groups overlapped with the
+Y passes (strong scaling; the plain schedule of one all-to-all per transform
+direction is timed beside it); N = 1 runs the undivided fused step.
+
+The e2e figure calls ghost_hd_run with pinned host arrays every step: the
+library moves each array's live box (the kx rows, y-lines and kz values that
+can hold a kept mode) and checks, on the host for the input and on the
+device for the result, that the rest holds only zero bits.
 """
 from __future__ import annotations
 
