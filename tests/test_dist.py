@@ -58,6 +58,10 @@ def test_reference_arm_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+    # --steps 2 substeps round up to one whole RK4 step, and the line's
+    # steps, ms_per_step and value describe the same timed seconds
+    assert d["steps"] == 1 and d["substeps_timed"] == 4 and d["steps_requested"] == 2
+    assert abs(d["steps"] * d["ms_per_step"] * 1e-3 - d["steps"] / d["value"]) < 1e-9
 
 
 def test_ensemble_shards_partition_the_runs():
