@@ -530,6 +530,7 @@ def run_slab(args, ws, rank, local):
     import torch
 
     from ghost_b200 import Ghost
+    from ghost_b200.roofline import slab_roofline
     from ghost_b200.slab import Slab
     n = args.grid
     clocks = Clocks(local)
@@ -627,6 +628,7 @@ def run_slab(args, ws, rank, local):
             "schedule": "overlapped: v and curl v exchanged as two asynchronous all-to-alls, the products one field "
                         "at a time, each behind the Y passes of the others; own block copied field to field",
             "plain_schedule_ms_per_step": ms32_plain / args.steps,
+            "roofline": slab_roofline(n, ws, ms32 / args.steps, xch, ORD),
             "e2e": {"value": args.e2e_steps / (ms_e2e * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches * ws,

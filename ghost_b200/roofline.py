@@ -82,3 +82,42 @@ def live_box(n: int):
     kt = int(zl[: n // 2].sum())
     kb = int(zl[n // 2:].sum())
     return rows, jt, jb, kt, kb
+
+
+def slab_exchange_bytes(n: int, nranks: int, elem_bytes: int = 8):
+    """Bytes that must cross the links in one pruned substep of the slab run
+    (ghost_b200.slab) of a cubic n^3 grid over nranks ranks: the six front
+    fields (v, curl v) kx-slab -> z-slab and the three products back, the
+    live kx rows only, each rank's own block excluded.  Returns the largest
+    over the ranks of max(bytes sent, bytes received), the per-direction
+    load of the busiest GPU."""
+    from .slab import exchange_counts, live_rows, slab_layout
+    ista, nxhl, _, nzl = slab_layout(n, n, nranks)
+    lr = live_rows(ista, nxhl, live_box(n)[0])
+    worst = 0
+    for r in range(nranks):
+        s0, r0 = exchange_counts(lr, nzl, n, r, 0, 6, self_direct=True)
+        s1, r1 = exchange_counts(lr, nzl, n, r, 1, 3, self_direct=True)
+        worst = max(worst, sum(s0) + sum(s1), sum(r0) + sum(r1))
+    return worst * elem_bytes
+
+
+def slab_roofline(n: int, nranks: int, ms_per_step: float, xch_ms_per_substep: float, ord: int = 4,
+                  elem_bytes: int = 8, link_gbs: float = 770.0):
+    """Roofline of the slab-decomposed run (no per-pass timers there): each
+    rank's share of the pruned step's algorithmic bytes (pass_bytes x ord /
+    nranks) over the measured step time, against the HBM peak, and the
+    exchange's link bytes per substep (slab_exchange_bytes) over the
+    measured exchange time, against the peer copy bandwidth link_gbs (GB/s
+    per direction, measured on this kind of machine)."""
+    peak, kind = measured_hbm_peak()
+    step_bytes = ord * sum(pass_bytes(n, ord, True, elem_bytes).values()) / nranks
+    ach = step_bytes / (ms_per_step * 1e-3) / 1e9
+    xb = slab_exchange_bytes(n, nranks, elem_bytes)
+    xach = xb / (xch_ms_per_substep * 1e-3) / 1e9 if xch_ms_per_substep > 0 else None
+    return {"bound": "hbm", "kernel": f"whole RK{ord} step, one rank's share of the pruned passes",
+            "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": kind,
+            "bytes_per_rank_per_step": step_bytes, "traffic": None,
+            "exchange": {"bytes_per_substep": xb, "achieved": xach, "peak": link_gbs, "unit": "GB/s",
+                         "frac": None if xach is None else xach / link_gbs,
+                         "peak_kind": "measured peer copy per direction"}}

@@ -68,6 +68,27 @@ def test_exchange_counts_match_between_peers(nx, nz, p):
     assert sum(sum(x[0]) for x in c) == 6 * rows * ny * nz
 
 
+def test_slab_roofline_counts_the_busiest_ranks_link_bytes():
+    """The roofline of the slab line: 64^3 over 2 ranks holds kx rows 17/16,
+    of which 17/5 are live (kx <= 21).  Rank 0 sends v and curl v of its 17
+    live rows for rank 1's 32 planes and the three products of rank 1's 5
+    live rows back: 6*17*64*32 + 3*5*64*32 complex values, the largest load
+    of either rank in either direction.  The HBM share is the undivided
+    run's pruned bytes over the ranks."""
+    from ghost_b200.roofline import pass_bytes, slab_exchange_bytes, slab_roofline
+    assert slab_exchange_bytes(64, 2) == (6 * 17 * 64 * 32 + 3 * 5 * 64 * 32) * 8
+    assert slab_exchange_bytes(64, 2, elem_bytes=16) == 2 * slab_exchange_bytes(64, 2)
+    r = slab_roofline(64, 2, ms_per_step=2.0, xch_ms_per_substep=0.5)
+    step_bytes = 4 * sum(pass_bytes(64, 4).values()) / 2
+    assert r["bytes_per_rank_per_step"] == pytest.approx(step_bytes)
+    assert r["achieved"] == pytest.approx(step_bytes / 2e-3 / 1e9)
+    assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    assert r["exchange"]["achieved"] == pytest.approx(slab_exchange_bytes(64, 2) / 0.5e-3 / 1e9)
+    assert r["exchange"]["frac"] == pytest.approx(r["exchange"]["achieved"] / 770.0)
+    # one rank exchanges nothing
+    assert slab_exchange_bytes(64, 1) == 0
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
